@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the per-frame voxel diffuse-GI path on B200.
+
+Workload (one "step" = one frame): the seeded fBm terrain of 512x256x512
+voxels (4 octaves, base frequency 1/64, lacunarity 2, gain 0.5, height bias),
+8 albedo materials U[0.2, 0.8], a sun of radiance 3 towards (0.4, 0.8, 0.3),
+256 emissive voxels of radiance U[1, 10]; the faces turned towards a
+cube-map camera at (256, 200, 256) (six 90-degree frusta) form the world
+cache; every frame traces 8 paths per face with 2 diffuse hits, terminating
+at cached faces, and accumulates the result (prepare, trace, accumulate).
+
+Printed metric: rays/s (one ray = one trace_domain_limited call, counted by
+the library's counting pass over the same frame). ``e2e`` is the same metric
+through the C ABI with pinned host task/result buffers copied every frame.
+``--impl reference`` times the CPU oracle (the restatement of the
+reference's algorithm; the reference itself is Rust/WGSL and has no CPU
+path) on the box's host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "global-illumination_b200"))
+
+EYE = (256.0, 200.0, 256.0)
+SPP = 8
+BOUNCES = 2
+METRIC = "rays/s and ms/frame at equal relMSE vs FP64 ref: MLP cache vs plain, 1 B200"
+WORKLOAD = "terrain 512x256x512 fBm, sun + 256 emissive voxels, faces facing a cube-map camera at (256,200,256), 8 spp, 2 bounces via world cache, FP32"
+
+
+def make_scene(seed):
+    import vgi
+
+    coords, vox = vgi.terrain(32, 16, 32, seed=seed, octaves=4, period=64.0, base_height=128.0, falloff=400.0, emitters=256)
+    rng = np.random.default_rng(seed)
+    m = vgi.VoxelGiMaterials()
+    for k in range(8):
+        m.set(k, vgi.MaterialTransport(diffuse=tuple(rng.uniform(0.2, 0.8, 3))))
+    for k in range(248):
+        r = float(rng.uniform(1.0, 10.0))
+        m.set(8 + k, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5), emission=(r, r, r)))
+    sun = vgi.DirectionalTransportLight((0.4, 0.8, 0.3), (3.0, 3.0, 3.0))
+    faces = vgi.exposed_faces(coords, vox, facing=EYE)
+    transport = vgi.TransportSettings(bounces=BOUNCES, path_steps=2048)
+    return coords, vox, m.words(), sun.words(), faces, transport
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per trace launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "trace_faces_terrain.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clocks and throttle reasons during timing."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=lambda: self.lines.extend(iter(self.proc.stdout.readline, "")), daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total, budget_s=20.0):
+    """The oracle on a bounded face sample with the GPU's warm cache state."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    n = faces.shape[0]
+    state = g.read_state()
+    index = O.face_index(faces[:, :4])
+    rng = np.random.default_rng(7)
+    sample = np.sort(rng.choice(n, size=min(n, 2048), replace=False))
+    tasks = np.zeros((sample.size, 8), np.uint32)
+    tasks[:, 0:3] = faces[sample, 0:3].view(np.uint32)
+    tasks[:, 3] = faces[sample, 3]
+    tasks[:, 4] = state[sample, 6]
+    d = geometry[0]
+    params = O.params_words(sample.size, SPP, d.size // 4, 1, geometry[3], 1, (0, 0, 0), total, n_emit)
+    threads = os.cpu_count() or 1
+    pipe = O.Pipeline(BOUNCES, 0, 2048, 0, SPP)
+    rays = 0
+    start = time.perf_counter()
+    chunks = 0
+    while True:
+        _, cnt = O.trace_faces(geometry, params, words, lights, emitters, tasks, pipe, state, index, threads)
+        rays += cnt["rays"]
+        chunks += 1
+        if time.perf_counter() - start > budget_s or chunks >= 8:
+            break
+    elapsed = time.perf_counter() - start
+    return {"value": rays / elapsed, "unit": "rays/s", "cores": threads, "kind": "port",
+            "sample": f"{chunks} x {sample.size} of {n} faces (seeded), {SPP} spp, the GPU's warm cache state, {threads} threads, {elapsed:.1f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU oracle (restatement of the reference's
+    algorithm) on bounded samples of the same workload, all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    import vgi
+
+    coords, vox, words, lights, faces, transport = make_scene(2)
+    scene = O.Scene(coords, vox, top_mode=0)
+    geometry = scene.arrays()
+    emitters, n_emit, total = O.emitters(coords, vox, words)
+    n = faces.shape[0]
+    # Warm-cache equivalent of the GPU's steady state: every slot holds 16+
+    # samples (the ray work depends only on which faces are cached, not on
+    # their values), sequences advanced as after the warm-up frames.
+    state = np.zeros((n, 36), np.uint32)
+    state[:, 5] = 16
+    state[:, 6] = SPP * 2
+    index = O.face_index(faces[:, :4])
+    threads = os.cpu_count() or 1
+    pipe = O.Pipeline(BOUNCES, 0, 2048, 0, SPP)
+    rng = np.random.default_rng(11)
+    per_step = 2048
+
+    def step(k):
+        sample = np.sort(rng.choice(n, size=per_step, replace=False))
+        tasks = np.zeros((per_step, 8), np.uint32)
+        tasks[:, 0:3] = faces[sample, 0:3].view(np.uint32)
+        tasks[:, 3] = faces[sample, 3]
+        tasks[:, 4] = SPP * (2 + k)
+        params = O.params_words(per_step, SPP, geometry[0].size // 4, 1, geometry[3], 1, (0, 0, 0), total, n_emit)
+        t0 = time.perf_counter()
+        _, cnt = O.trace_faces(geometry, params, words, lights, emitters, tasks, pipe, state, index, threads)
+        return cnt["rays"], time.perf_counter() - t0
+
+    for k in range(args.warmup):
+        step(k)
+    rays, secs = 0, 0.0
+    for k in range(args.steps):
+        r, s = step(args.warmup + k)
+        rays += r
+        secs += s
+    value = rays / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "faces": int(n), "spp": SPP, "bounces": BOUNCES,
+                   "step": f"oracle trace of {per_step} seeded faces of {n} per step (bounded CPU sample)"},
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} steps x {per_step} of {n} faces, warm-cache counts, {threads} threads"},
+        "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["vgi", "reference"], default="vgi")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import vgi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    # Weak scaling: every rank traces its own terrain (seed 2 + rank); no
+    # data-path collective, only the timing reduction.
+    coords, vox, words, lights, faces, transport = make_scene(2 + rank)
+    g = vgi.GpuTracer(local)
+    g.upload_regions(coords, vox)
+    g.set_materials(words)
+    g.set_lights(lights, 1)
+    g.set_environment((0.0, 0.0, 0.0))
+    g.build_emitters()
+    g.set_transport(transport)
+    g.set_faces(faces)
+    g.set_timing(True)
+    n = faces.shape[0]
+    stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    clock = 0
+    for _ in range(args.warmup):
+        g.frame(SPP, clock)
+        clock += 16
+    g.sync()
+    before = g.census(SPP)
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    start_ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    end_ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kernel_ms = []
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))  # L2 flush: 256 MB written between frames, outside the timed pair
+            start_ev[k].record(stream)
+        g.frame(SPP, clock)
+        clock += 16
+        with torch.cuda.stream(stream):
+            end_ev[k].record(stream)
+        kernel_ms.append(g.frame_times())
+    torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(start_ev, end_ev)]
+    clocks = sampler.stop()
+    after = g.census(SPP)
+    rays_per_frame = 0.5 * (before["rays"] + after["rays"])
+    bytes_per_frame = 0.5 * (before["bytes"] + after["bytes"])
+    paths_per_frame = before["paths"]
+    total_ms = float(sum(step_ms))
+
+    # End to end through the C ABI: pinned host tasks in, results out, every frame.
+    tasks_host = torch.empty((n, 8), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    tasks_host[:] = vgi.tasks_for(faces)
+    results_host = torch.empty((n, 24), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    e2e_ms = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        g.trace_batch(tasks_host, SPP, clock, out=results_host)
+        e2e_ms.append(1000.0 * (time.perf_counter() - t0))
+        clock += 16
+    e2e_total = float(sum(e2e_ms))
+
+    stats = torch.tensor([total_ms, e2e_total, rays_per_frame * args.steps, float(n)], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        mx = stats.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = stats.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        total_ms, e2e_total = float(mx[0]), float(mx[1])
+        total_rays, total_faces = float(sm[2]), float(sm[3])
+    else:
+        total_rays, total_faces = float(stats[2]), float(stats[3])
+
+    trace_ms = float(np.mean([t[1] for t in kernel_ms]))
+    peak, peak_kind = measured_peak()
+    achieved = bytes_per_frame / (trace_ms * 1e-3) / 1e9
+    traffic = profiled_traffic()
+    if rank == 0:
+        base = None
+        if world == 1 and not args.no_cpu_baseline:
+            geometry = g.geometry()
+            emitters, n_emit, total = vgi.host_emitters(coords, vox, words)
+            base = cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total)
+        line = {
+            "metric": METRIC,
+            "value": total_rays / (total_ms * 1e-3),
+            "unit": "rays/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "faces": int(n), "spp": SPP, "bounces": BOUNCES, "parallelism": f"independent scene per GPU x{world}",
+                       "paths_per_frame": int(paths_per_frame), "rays_per_frame": rays_per_frame,
+                       "l2": "256 MB buffer written between timed frames (outside the event pair)",
+                       "kernel_ms": {"prepare": float(np.mean([t[0] for t in kernel_ms])), "trace": trace_ms,
+                                     "accumulate": float(np.mean([t[2] for t in kernel_ms]))},
+                       "paths_per_s": paths_per_frame * world / (total_ms * 1e-3 / args.steps),
+                       "frames_per_s": 1000.0 * args.steps / total_ms},
+            "e2e": {"value": total_rays / (e2e_total * 1e-3), "unit": "rays/s", "h2d_bytes_per_step": int(n * 32), "d2h_bytes_per_step": int(n * 96)},
+            "gpu_launches": 3 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "note": "trace kernel: algorithmic bytes per launch (counting pass) / CUDA-event trace time"},
+            "clocks": clocks,
+        }
+        if base:
+            line["cpu_baseline"] = base
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,322 @@
+// Resident face-cache maintenance around the trace: begin_trace and
+// mark_changed before it, accumulate (discounted running mean, display EMA,
+// stability) after it, and apply_events for retention events.
+//
+// Behaviour follows (paths within nathanaelneveux/global-illumination,
+// crates/bevy_voxel_gi/shaders/):
+//   voxel_accumulate.wgsl:130-133  begin_trace
+//   voxel_accumulate.wgsl:135-262  accumulate, record_stability, settled_flag
+//   voxel_accumulate.wgsl:264-286  sample_noise, required_samples, refinement_error
+//   voxel_accumulate.wgsl:295-344  apply_events, binds
+//   voxel_accumulate.wgsl:432-446  mark_changed
+//   voxel_retention.wgsl:1-96      curve_limit, box_distance2, resolve_retention
+//
+// Layout: the reference's slot records (9 uint4 state, 3 uint4 metadata,
+// 3 uint4 checkpoint) are kept as arrays of uint4 so each thread moves whole
+// 16-byte words and a warp covers contiguous lines. Beside them each slot
+// has a 16-byte gather record (mean rgb, count word) that the trace reads for
+// the world-cache gather instead of two state words; every kernel that
+// changes a slot's mean or count rewrites it.
+#include "vgi_device.cuh"
+#include "vgi_types.cuh"
+
+namespace vgi {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr uint32_t kNoLimit = 0xffffffffu;
+constexpr uint32_t kUrgent = 0x40000000u;
+constexpr uint32_t kMirrorStale = 0x20000000u;
+
+__device__ __forceinline__ float u2f(uint32_t u) { return __uint_as_float(u); }
+__device__ __forceinline__ uint32_t f2b(float f) { return __float_as_uint(f); }
+__device__ __forceinline__ float lum3(float r, float g, float b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
+}
+__device__ __forceinline__ float max3(float a, float b, float c) { return wmax(a, wmax(b, c)); }
+__device__ __forceinline__ float var1(float s, float m) { return wmax(__fsub_rn(s, __fmul_rn(m, m)), 0.0f); }
+
+__device__ __forceinline__ void write_record(float4* cache, uint32_t slot, const uint4& mean, uint32_t count) {
+    cache[slot] = make_float4(u2f(mean.x), u2f(mean.y), u2f(mean.z), u2f(count));
+}
+
+// binds (voxel_accumulate.wgsl:336-344)
+__device__ bool binds(const uint4* state, uint32_t slot, float change, float physical) {
+    uint4 m = state[slot * 9u], s = state[slot * 9u + 2u];
+    uint32_t count = state[slot * 9u + 1u].y;
+    float mr = u2f(m.x), mg = u2f(m.y), mb = u2f(m.z);
+    float variance = lum3(var1(u2f(s.x), mr), var1(u2f(s.y), mg), var1(u2f(s.z), mb));
+    bool lit = lum3(mr, mg, mb) >= __fmul_rn(0.05f, change);
+    float keep = __fdiv_rn(__fmul_rn(physical, variance), wmax(__fmul_rn(change, change), 1e-30f));
+    return !lit || keep < (float)(count & 0x7fffffffu);
+}
+
+// prepare's begin_trace and batch stamp (voxel_accumulate.wgsl:114-121),
+// then mark_changed (:432-446), one thread per task. With slot_meta null only
+// the task's sequence is written (the counting pass's copy of the tasks).
+__global__ void __launch_bounds__(kBlock) prepare_kernel(AccumArgs a) {
+    uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= a.n) return;
+    uint32_t slot = a.slots ? a.slots[i] : i;
+    if (slot == kNoIndex) return;
+    uint4 meta1 = a.state[slot * 9u + 1u];
+    a.tasks[i * 2u + 1u].x = meta1.z;  // begin_trace: the task takes the slot's sequence
+    if (a.slot_meta == nullptr) return;
+    uint4* sm = a.slot_meta + slot * 3u + 1u;
+    uint4 sched = *sm;
+    sched.y = (sched.y & 0xfu) | (a.controls[25] << 4);
+    sm->y = sched.y;
+    float pending = u2f(sched.x);
+    if (pending <= 0.0f) return;
+    if (binds(a.state, slot, pending, u2f(a.controls[11]))) {
+        meta1.y |= 0x80000000u;
+        a.state[slot * 9u + 1u].y = meta1.y;
+        a.cache[slot].w = u2f(meta1.y);
+    } else {
+        sm->x = 0u;
+    }
+}
+
+__device__ float refinement_error(uint4 m, uint4 s, uint32_t count) {
+    if (count < 2u) return 1.0f;
+    float c = (float)count;
+    float ex = __fdiv_rn(__fsqrt_rn(__fdiv_rn(var1(u2f(s.x), u2f(m.x)), c)), __fadd_rn(0.002f, fabsf(u2f(m.x))));
+    float ey = __fdiv_rn(__fsqrt_rn(__fdiv_rn(var1(u2f(s.y), u2f(m.y)), c)), __fadd_rn(0.002f, fabsf(u2f(m.y))));
+    float ez = __fdiv_rn(__fsqrt_rn(__fdiv_rn(var1(u2f(s.z), u2f(m.z)), c)), __fadd_rn(0.002f, fabsf(u2f(m.z))));
+    return wmin(max3(ex, ey, ez), 8.0f);
+}
+__device__ float sample_noise(uint4 m, uint4 s) {
+    float ex = __fdiv_rn(__fsqrt_rn(var1(u2f(s.x), u2f(m.x))), __fadd_rn(0.002f, fabsf(u2f(m.x))));
+    float ey = __fdiv_rn(__fsqrt_rn(var1(u2f(s.y), u2f(m.y))), __fadd_rn(0.002f, fabsf(u2f(m.y))));
+    float ez = __fdiv_rn(__fsqrt_rn(var1(u2f(s.z), u2f(m.z))), __fadd_rn(0.002f, fabsf(u2f(m.z))));
+    return max3(ex, ey, ez);
+}
+
+__device__ __forceinline__ float lerp_alpha(float p, float m, float alpha) { return __fadd_rn(p, __fmul_rn(__fsub_rn(m, p), alpha)); }
+__device__ __forceinline__ float mix_w(float a, float b, float t) {
+    return __fadd_rn(__fmul_rn(a, __fsub_rn(1.0f, t)), __fmul_rn(b, t));
+}
+
+// accumulate + record_stability + settled_flag for CPU-owned faces (no GPU picks).
+__global__ void __launch_bounds__(kBlock) accumulate_kernel(AccumArgs a) {
+    const uint32_t* ctl = a.controls;
+    uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= a.n || i >= ctl[0]) return;
+    uint32_t slot = a.slots ? a.slots[i] : i;
+    if (slot == kNoIndex) return;
+    uint4* st = a.state + slot * 9u;
+    uint4* out = a.outputs + (size_t)i * 6u;
+    uint4* cp = a.checkpoint + slot * 3u;
+    uint4 s0 = st[0], s1 = st[1], s2 = st[2], s3 = st[3], s6 = st[6], s7 = st[7];
+    cp[0] = s0;
+    cp[1] = s2;
+    uint4 cp2 = make_uint4(s1.x, s1.y & 0x7fffffffu, s3.x, 0u);
+    uint4 o0 = out[0], o1 = out[1], o2 = out[2], o4 = out[4], o5 = out[5];
+    uint32_t fresh = f2u(u2f(o1.y));
+    uint4* sched_p = a.slot_meta + slot * 3u + 1u;
+    uint4 sched = *sched_p;
+    float pending = u2f(sched.x);
+    if (fresh > 0u) sched.x = 0u;
+    uint32_t previous_count = s1.y & 0x7fffffffu;
+    float physical = u2f(ctl[11]);
+    float change = (s1.y & 0x80000000u) != 0u ? pending : 0.0f;
+    if (physical > 0.0f && fresh > 0u && change > 0.0f) {
+        float om = lum3(u2f(s0.x), u2f(s0.y), u2f(s0.z));
+        float ov = lum3(var1(u2f(s2.x), u2f(s0.x)), var1(u2f(s2.y), u2f(s0.y)), var1(u2f(s2.z), u2f(s0.z)));
+        float fv = lum3(var1(u2f(o2.x), u2f(o0.x)), var1(u2f(o2.y), u2f(o0.y)), var1(u2f(o2.z), u2f(o0.z)));
+        float variance = om < __fmul_rn(0.05f, change) ? fv : ov;
+        float keep = __fdiv_rn(__fmul_rn(physical, variance), __fmul_rn(change, change));
+        uint32_t k = f2u(wmin(keep, 65536.0f));
+        previous_count = previous_count < k ? previous_count : k;
+        cp2.y = cp2.y < previous_count ? cp2.y : previous_count;
+    }
+    cp[2] = cp2;
+    uint32_t count = previous_count + fresh;
+    count = count < ctl[3] ? count : ctl[3];
+    float recency = u2f(ctl[10]);
+    float alpha = fresh > 0u ? wmin(__fdiv_rn(__fmul_rn(recency, (float)fresh), (float)(count > 1u ? count : 1u)), 1.0f) : 0.0f;
+    uint4 nm = make_uint4(f2b(lerp_alpha(u2f(s0.x), u2f(o0.x), alpha)), f2b(lerp_alpha(u2f(s0.y), u2f(o0.y), alpha)),
+                          f2b(lerp_alpha(u2f(s0.z), u2f(o0.z), alpha)), f2b(lerp_alpha(u2f(s0.w), u2f(o0.w), alpha)));
+    uint4 ns = make_uint4(f2b(lerp_alpha(u2f(s2.x), u2f(o2.x), alpha)), f2b(lerp_alpha(u2f(s2.y), u2f(o2.y), alpha)),
+                          f2b(lerp_alpha(u2f(s2.z), u2f(o2.z), alpha)), f2b(lerp_alpha(u2f(s2.w), u2f(o2.w), alpha)));
+    s1.y = count;
+    s1.z += ctl[1];
+    float rr = u2f(nm.x), rg = u2f(nm.y), rb = u2f(nm.z);
+    float mr = u2f(ns.x), mg = u2f(ns.y), mb = u2f(ns.z);
+    float cnt = wmax((float)count, 1.0f);
+    float er = __fsqrt_rn(__fdiv_rn(var1(mr, rr), cnt)), eg = __fsqrt_rn(__fdiv_rn(var1(mg, rg), cnt)), eb = __fsqrt_rn(__fdiv_rn(var1(mb, rb), cnt));
+    float uncertainty = count < 2u ? 1.0f
+                                   : wmin(8.0f, max3(__fdiv_rn(er, __fadd_rn(0.02f, fabsf(rr))), __fdiv_rn(eg, __fadd_rn(0.02f, fabsf(rg))),
+                                                     __fdiv_rn(eb, __fadd_rn(0.02f, fabsf(rb)))));
+    float noise = count < 2u ? 1.0f
+                             : wmin(8.0f, max3(__fdiv_rn(er, __fadd_rn(0.002f, fabsf(rr))), __fdiv_rn(eg, __fadd_rn(0.002f, fabsf(rg))),
+                                               __fdiv_rn(eb, __fadd_rn(0.002f, fabsf(rb)))));
+    float elapsed = s7.z != 0u ? __fmul_rn((float)(ctl[2] - s7.y), 0.001f) : __fdiv_rn(1.0f, 60.0f);
+    float time_alpha = __fsub_rn(1.0f, own_exp(__fdiv_rn(-elapsed, u2f(ctl[4]))));
+    float evidence = __fdiv_rn((float)count, __fadd_rn((float)count, 32.0f));
+    float blend = wmin(time_alpha, __fdiv_rn(evidence, __fadd_rn(1.0f, __fmul_rn(__fmul_rn(16.0f, noise), noise))));
+    float pr = u2f(s6.x), pg = u2f(s6.y), pb = u2f(s6.z), pw = u2f(s6.w);
+    float old_weight = __fdiv_rn(__fsub_rn(1.0f, blend), __fadd_rn(0.25f, max3(pr, pg, pb)));
+    float new_weight = __fdiv_rn(blend, __fadd_rn(0.25f, max3(rr, rg, rb)));
+    float alpha_display = wmin(blend, __fdiv_rn(new_weight, wmax(__fadd_rn(old_weight, new_weight), 0.0000001f)));
+    float confidence = wclamp(__fdiv_rn(__fdiv_rn((float)count, __fadd_rn((float)count, 8.0f)), __fadd_rn(1.0f, uncertainty)), 0.125f, 1.0f);
+    uint4 disp = make_uint4(f2b(mix_w(pr, rr, alpha_display)), f2b(mix_w(pg, rg, alpha_display)), f2b(mix_w(pb, rb, alpha_display)),
+                            f2b(mix_w(pw, confidence, blend)));
+    s7.y = ctl[2];
+    s7.z = 0xffffffffu;
+    s1.w = disp.x;
+    s3 = make_uint4(s3.x, disp.y, disp.z, disp.w);
+    st[0] = nm;
+    st[1] = s1;
+    st[2] = ns;
+    st[3] = s3;
+    st[4] = o4;
+    st[5] = o5;
+    st[6] = disp;
+    st[7] = s7;
+    write_record(a.cache, slot, nm, count);
+    // record_stability (picked = false)
+    uint4* rank_p = a.slot_meta + slot * 3u + 2u;
+    bool same_revision = (sched.y & 8u) != 0u && sched.w == ctl[16];
+    uint32_t scount = count & 0x7fffffffu;
+    float tolerance = u2f(ctl[17]);
+    float bx = u2f(s0.x), by = u2f(s0.y), bz = u2f(s0.z);
+    float dx = __fdiv_rn(fabsf(__fsub_rn(bx, rr)), __fadd_rn(0.002f, wmax(fabsf(bx), fabsf(rr))));
+    float dy = __fdiv_rn(fabsf(__fsub_rn(by, rg)), __fadd_rn(0.002f, wmax(fabsf(by), fabsf(rg))));
+    float dz = __fdiv_rn(fabsf(__fsub_rn(bz, rb)), __fadd_rn(0.002f, wmax(fabsf(bz), fabsf(rb))));
+    float drift = max3(dx, dy, dz);
+    float dispr = u2f(disp.x), dispg = u2f(disp.y), dispb = u2f(disp.z);
+    bool settled = max3(fabsf(__fsub_rn(dispr, rr)), fabsf(__fsub_rn(dispg, rg)), fabsf(__fsub_rn(dispb, rb))) <=
+                   __fadd_rn(0.001f, __fmul_rn(__fmul_rn(max3(rr, rg, rb), tolerance), 0.5f));
+    uint32_t required = max3(rr, rg, rb) < 0.02f ? (ctl[18] > 256u ? ctl[18] : 256u) : ctl[18];
+    bool stable_now = same_revision && settled && scount >= required && refinement_error(nm, ns, scount) <= tolerance &&
+                      drift <= __fmul_rn(tolerance, 0.5f);
+    uint32_t stable = stable_now ? (((sched.y & 7u) + 1u) < 4u ? (sched.y & 7u) + 1u : 4u) : 0u;
+    sched.y = (sched.y & 0xfffffff0u) | 8u | stable;
+    sched.w = ctl[16];
+    *sched_p = sched;
+    uint4 rank = *rank_p;
+    *rank_p = make_uint4(f2b(sample_noise(nm, ns)), ctl[2], f2b(max3(rr, rg, rb)), 0x80000000u | scount | (rank.w & kMirrorStale));
+    uint4 w1 = s1;
+    if ((sched.y & 15u) == 12u) w1.y |= 0x80000000u;
+    out[0] = nm;
+    out[1] = w1;
+    out[2] = ns;
+    out[3] = s3;
+    out[4] = o4;
+    out[5] = o5;
+}
+
+// curve_limit / box_distance2 / load_height (voxel_retention.wgsl:9-22)
+__device__ __forceinline__ uint32_t curve_limit(uint32_t d2) {
+    if (d2 >= 36864u) return kNoLimit;
+    return (d2 * d2 + 10368u) / 20736u;
+}
+__device__ __forceinline__ uint32_t box_distance2(int lx, int ly, int lz, int hx, int hy, int hz, int px, int py, int pz) {
+    int sx = min(max(max(lx - px, px - hx), 0), 4096);
+    int sy = min(max(max(ly - py, py - hy), 0), 4096);
+    int sz = min(max(max(lz - pz, pz - hz), 0), 4096);
+    return (uint32_t)sx * (uint32_t)sx + (uint32_t)sy * (uint32_t)sy + (uint32_t)sz * (uint32_t)sz;
+}
+
+__global__ void __launch_bounds__(kBlock) apply_events_kernel(AccumArgs a, const uint4* events, uint32_t n_slots) {
+    const uint32_t* ctl = a.controls;
+    uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
+    if (slot >= n_slots) return;
+    uint4 identity = a.slot_meta[slot * 3u];
+    if ((identity.w & 8u) == 0u) return;
+    int px = (int)identity.x, py = (int)identity.y, pz = (int)identity.z;
+    const uint32_t event_count = ctl[13], reach = ctl[15];
+    const float physical = u2f(ctl[11]);
+    const bool measured_mode = physical > 0.0f;
+    // resolve_retention (voxel_retention.wgsl:29-96)
+    uint32_t cap = kNoLimit, source_cap = kNoLimit;
+    float change = 0.0f;
+    bool known = true, woken = false, urgent_if_binding = false, urgent = false;
+    for (uint32_t e = 0; e < event_count; ++e) {
+        uint4 h0 = events[e * 3u], h1 = events[e * 3u + 1u], h2 = events[e * 3u + 2u];
+        if ((h0.w & 2u) != 0u) {
+            uint32_t limit = h2.x;
+            for (uint32_t b = 0; b < h2.w; ++b) {
+                uint4 sp = events[event_count * 3u + (h2.z + b) * 2u];
+                float dx = __fsub_rn((float)px, u2f(sp.x)), dy = __fsub_rn((float)py, u2f(sp.y)), dz = __fsub_rn((float)pz, u2f(sp.z));
+                float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+                if (d2 <= u2f(sp.w)) limit = limit < 4u ? limit : 4u;
+            }
+            source_cap = source_cap < limit ? source_cap : limit;
+            woken = true;
+            continue;
+        }
+        uint32_t outside = box_distance2((int)h0.x, (int)h0.y, (int)h0.z, (int)h1.x, (int)h1.y, (int)h1.z, px, py, pz);
+        if (outside > reach) continue;
+        woken = true;
+        bool exact = known;
+        uint32_t nearest = kNoLimit;
+        for (uint32_t b = 0; b < h2.w; ++b) {
+            uint32_t record = event_count * 3u + (h2.z + b) * 2u;
+            uint4 b0 = events[record], b1 = events[record + 1u];
+            uint32_t d = box_distance2((int)b0.x, (int)b0.y, (int)b0.z, (int)b1.x, (int)b1.y, (int)b1.z, px, py, pz);
+            if (d > reach) continue;
+            nearest = nearest < d ? nearest : d;
+            uint32_t edit_kind = b1.w & 7u;
+            if ((b1.w & 8u) != 0u && (edit_kind == 0u || edit_kind == 3u)) {
+                if (edit_kind == 3u && measured_mode) urgent_if_binding = urgent_if_binding || d <= ctl[30];
+                else urgent = urgent || d <= ctl[31];
+            }
+            if (exact) {
+                uint32_t kind = b1.w & 7u;
+                if (kind == 0u) {
+                    known = false;
+                    exact = false;
+                } else if (kind != 1u) {
+                    float area = 1.0f;
+                    if (kind == 2u) area = (float)min(max(((int)b1.w >> 3) + 1 - py, 0), 16);
+                    change = __fadd_rn(change, __fdiv_rn(__fmul_rn(u2f(b0.w), area), __fmul_rn(3.14159265358979f, (float)(d > 1u ? d : 1u))));
+                }
+            }
+        }
+        if (nearest != kNoLimit) {
+            uint32_t c = curve_limit(nearest);
+            cap = cap < c ? cap : c;
+        }
+    }
+    bool measured = measured_mode && known;
+    uint32_t other = measured ? kNoLimit : cap;
+    uint32_t limit = source_cap < other ? source_cap : other;
+    if (limit != kNoLimit) {
+        uint4* s1p = a.state + slot * 9u + 1u;
+        uint32_t y = s1p->y;
+        y = y < limit ? y : limit;
+        s1p->y = y;
+        uint4* rank = a.slot_meta + slot * 3u + 2u;
+        rank->w = (rank->w & 0xe0000000u) | (y & 0x1fffffffu);
+        uint4* cp2 = a.checkpoint + slot * 3u + 2u;
+        cp2->y = cp2->y < limit ? cp2->y : limit;
+        a.cache[slot].w = u2f(y);
+    }
+    uint4* sched = a.slot_meta + slot * 3u + 1u;
+    if (measured && change > 0.0f) sched->x = f2b(__fadd_rn(u2f(sched->x), change));
+    if (urgent_if_binding) {
+        float p = u2f(sched->x);
+        urgent = urgent || !measured || (p > 0.0f && binds(a.state, slot, p, physical));
+    }
+    if (woken || urgent) sched->y &= 0xfffffff0u;
+    if (urgent) a.slot_meta[slot * 3u + 2u].w |= kUrgent;
+}
+
+}  // namespace
+
+void launch_prepare(const AccumArgs& a, cudaStream_t s) {
+    if (a.n == 0) return;
+    prepare_kernel<<<(a.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(a);
+}
+void launch_accumulate(const AccumArgs& a, cudaStream_t s) {
+    if (a.n == 0) return;
+    accumulate_kernel<<<(a.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(a);
+}
+void launch_apply_events(const AccumArgs& a, const uint4* events, uint32_t n_slots, cudaStream_t s) {
+    if (n_slots == 0) return;
+    apply_events_kernel<<<(n_slots + kBlock - 1) / kBlock, kBlock, 0, s>>>(a, events, n_slots);
+}
+
+}  // namespace vgi

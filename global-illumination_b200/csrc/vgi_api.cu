@@ -1,0 +1,829 @@
+// libvgi C ABI (include/vgi.h): context, device buffers and the per-frame
+// sequence. One CUDA stream per context; all device memory is owned here.
+#include "../../include/vgi.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "vgi_runtime.h"
+#include "vgi_types.cuh"
+
+namespace vgi {
+void launch_classify_pack(const uint16_t* voxels, const uint32_t* regions, uint32_t grid, uint32_t n, uint4* headers, uint32_t* cells,
+                          unsigned long long* alloc, unsigned long long capacity, uint32_t* error, cudaStream_t s);
+void launch_scatter_edits(const uint2* edits, uint32_t n, uint16_t* voxels, cudaStream_t s);
+void launch_set_header_extents(uint4* headers, const uint2* zw, uint32_t n, cudaStream_t s);
+}  // namespace vgi
+
+namespace {
+
+using namespace vgi;
+
+template <class T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t count = 0;  // elements allocated
+    cudaError_t reserve(size_t n) {
+        if (n <= count && ptr) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+        if (n == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&ptr, n * sizeof(T));
+        if (e == cudaSuccess) count = n;
+        return e;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+};
+
+constexpr uint32_t kHistoryLimit = 65536;
+constexpr float kMaxPathDistance = 768.0f;
+
+}  // namespace
+
+struct vgi_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+
+    // geometry
+    std::vector<RegionKey> keys;
+    std::unordered_map<RegionKey, uint32_t, RegionKeyHash> where;
+    std::vector<uint16_t> host_voxels;
+    std::vector<uint8_t> strides;
+    std::vector<uint4> host_headers;
+    TopLevelField top;
+    int32_t bounds[6] = {0, 0, 0, 0, 0, 0};
+    uint64_t dir_slots = 0;
+    uint64_t cells_used = 0;
+    bool geometry = false;
+    DevBuf<int4> directory;
+    DevBuf<uint4> headers;
+    DevBuf<uint32_t> cells;
+    DevBuf<uint16_t> voxels;
+    DevBuf<unsigned long long> alloc;
+    DevBuf<uint32_t> pack_error;
+    DevBuf<uint2> edit_buf;
+    DevBuf<uint2> zw;
+    DevBuf<uint32_t> region_list;
+
+    // model
+    std::vector<float> host_materials = std::vector<float>(256 * 16, 0.0f);
+    DevBuf<float4> materials;
+    DevBuf<float4> lights;
+    uint32_t n_lights = 0, n_directional = 0;
+    float env[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    DevBuf<uint4> emitters;
+    float emitter_count = 0.0f, emitter_total = 0.0f;
+    vgi_transport transport{};
+
+    // face cache
+    uint32_t n_slots = 0;
+    DevBuf<uint4> tasks, results, state, slot_meta, checkpoint, face_index;
+    DevBuf<float4> cache;
+    DevBuf<uint4> scratch_tasks, scratch_results;
+    DevBuf<uint4> events;
+    uint32_t n_events = 0;
+    DevBuf<unsigned long long> counters;
+    uint32_t batch_id = 1;
+
+    // frame timing
+    bool timing = false;
+    cudaEvent_t marks[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+int fail(vgi_ctx* c, int code, const std::string& what) {
+    if (c) c->error = what;
+    return code;
+}
+#define VGI_CUDA(c, call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail((c), VGI_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+uint32_t fbits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+vgi_transport default_transport() {
+    vgi_transport t{};
+    t.reach = kMaxPathDistance;
+    t.bounces = 3;
+    t.path_steps = 2048;
+    t.budgeted = 0;
+    t.history_limit = 0;
+    t.recency = 1.0f;
+    t.measured_retention = 1.0f;
+    t.response_seconds = 0.075f;
+    t.lanes = 0;
+    t.transport_revision = 0;
+    t.stable_error = 0.12f;
+    t.stable_samples = 32;
+    return t;
+}
+
+// TransportSettings::normalized (src/settings.rs:413-426)
+float norm_reach(float r) { return std::isfinite(r) ? std::min(std::max(r, 1.0f), kMaxPathDistance) : kMaxPathDistance; }
+uint32_t norm_bounces(uint32_t b) { return std::min(std::max(b, 1u), 3u); }
+
+uint32_t lanes_log2(const vgi_transport& t, uint32_t samples) {
+    uint32_t lanes = t.lanes;
+    if (lanes == 0) {
+        // One thread per sample for small sample counts; cap at 32.
+        lanes = 1;
+        while (lanes < samples && lanes < 32) lanes <<= 1;
+        if (lanes > samples && lanes > 1) lanes >>= 1;
+    }
+    uint32_t l = 0;
+    while ((1u << (l + 1)) <= lanes && l < 5) ++l;
+    return l;
+}
+
+// The Controls uniform of shaders/voxel_accumulate.wgsl:11-15 as
+// src/gpu/resident.rs:708-760 fills it, for a batch of CPU-owned faces.
+void fill_controls(const vgi_ctx* c, uint32_t samples, uint32_t clock_ms, uint32_t* w) {
+    std::memset(w, 0, 36 * 4);
+    const vgi_transport& t = c->transport;
+    w[0] = c->n_slots;
+    w[1] = samples;
+    w[2] = clock_ms;
+    w[3] = t.history_limit == 0 ? kHistoryLimit : std::min(t.history_limit, kHistoryLimit);
+    w[4] = fbits(std::max(t.response_seconds, 0.001f));
+    w[5] = c->n_slots;
+    w[10] = fbits(t.recency >= 1.0f ? t.recency : 1.0f);
+    w[11] = fbits(std::max(t.measured_retention, 0.0f));
+    w[13] = c->n_events;
+    w[14] = c->n_slots;
+    w[15] = 192u * 192u;  // INFLUENCE_RADIUS^2 (src/retention.rs:33-40)
+    w[16] = t.transport_revision;
+    w[17] = fbits(t.stable_error);
+    w[18] = t.stable_samples;
+    w[24] = c->n_slots;
+    w[25] = c->batch_id;
+    w[30] = 64u * 64u;  // MEASURED_RELIGHT_RADIUS^2 (src/geometry.rs:19)
+    w[31] = 48u * 48u;  // RELIGHT_RADIUS^2 (src/geometry.rs:15)
+}
+
+TraceArgs trace_args(vgi_ctx* c, const uint4* tasks, uint4* results, uint32_t n, uint32_t samples, bool with_cache) {
+    TraceArgs a{};
+    a.directory = c->directory.ptr;
+    a.headers = c->headers.ptr;
+    a.cells = c->cells.ptr;
+    a.dir_mask = (uint32_t)(c->dir_slots - 1);
+    for (int k = 0; k < 3; ++k) {
+        a.mn[k] = c->bounds[k];
+        a.mx[k] = c->bounds[3 + k];
+    }
+    a.materials = c->materials.ptr;
+    a.emitters = c->emitters.ptr;
+    a.emitter_count = c->emitter_count;
+    a.emitter_total = c->emitter_total;
+    a.max_distance = kMaxPathDistance;
+    a.reach = norm_reach(c->transport.reach);
+    for (int k = 0; k < 4; ++k) a.env[k] = c->env[k];
+    a.light_count = c->n_lights;
+    a.lights = c->lights.ptr;
+    a.face_index = with_cache ? c->face_index.ptr : nullptr;
+    a.cache = with_cache ? c->cache.ptr : nullptr;
+    a.tasks = tasks;
+    a.results = results;
+    a.n_tasks = n;
+    a.samples = samples;
+    a.path_steps = c->transport.path_steps;
+    a.lanes_log2 = lanes_log2(c->transport, samples);
+    a.counters = c->counters.ptr;
+    return a;
+}
+
+AccumArgs accum_args(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
+    AccumArgs a{};
+    a.state = c->state.ptr;
+    a.slot_meta = c->slot_meta.ptr;
+    a.checkpoint = c->checkpoint.ptr;
+    a.outputs = c->results.ptr;
+    a.tasks = c->tasks.ptr;
+    a.cache = c->cache.ptr;
+    a.slots = nullptr;
+    a.n = c->n_slots;
+    fill_controls(c, samples, clock_ms, a.controls);
+    return a;
+}
+
+int check_ready(vgi_ctx* c, bool need_faces) {
+    if (!c) return VGI_ERR_INVALID;
+    if (!c->geometry) return fail(c, VGI_ERR_STATE, "no geometry uploaded");
+    if (!c->materials.ptr || !c->lights.ptr || !c->emitters.ptr) return fail(c, VGI_ERR_STATE, "model not set");
+    if (need_faces && c->n_slots == 0) return fail(c, VGI_ERR_STATE, "no faces set");
+    return VGI_OK;
+}
+
+bool transport_limited(const vgi_ctx* c) { return norm_reach(c->transport.reach) < kMaxPathDistance; }
+
+int read_counters(vgi_ctx* c, vgi_counters* out) {
+    unsigned long long h[10];
+    VGI_CUDA(c, cudaMemcpyAsync(h, c->counters.ptr, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (out) {
+        out->rays = h[0];
+        out->paths = h[1];
+        out->steps = h[2];
+        out->bytes = h[3];
+        out->unknown = h[4];
+        out->cache_hits = h[5];
+        for (int k = 0; k < 4; ++k) out->status[k] = h[6 + k];
+    }
+    return VGI_OK;
+}
+
+// Headers z/w from the top-level field and strides; uploads them.
+int finish_headers(vgi_ctx* c) {
+    const uint32_t n = (uint32_t)c->keys.size();
+    std::vector<uint2> zw(n);
+    for (uint32_t r = 0; r < n; ++r) {
+        Extents e = c->top.at(c->keys[r].x, c->keys[r].y, c->keys[r].z);
+        uint32_t neg = (uint32_t)e[0] | ((uint32_t)e[2] << 8) | ((uint32_t)e[4] << 16);
+        uint32_t pos = (uint32_t)e[1] | ((uint32_t)e[3] << 8) | ((uint32_t)e[5] << 16);
+        pos |= (uint32_t)c->strides[r] << 28;
+        zw[r] = make_uint2(neg, pos);
+        c->host_headers[r].z = neg;
+        c->host_headers[r].w = pos;
+    }
+    VGI_CUDA(c, c->zw.reserve(std::max<size_t>(n, 1)));
+    VGI_CUDA(c, cudaMemcpyAsync(c->zw.ptr, zw.data(), n * sizeof(uint2), cudaMemcpyHostToDevice, c->stream));
+    launch_set_header_extents(c->headers.ptr, c->zw.ptr, n, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    return VGI_OK;
+}
+
+bool region_blocked(const vgi_ctx* c, int32_t x, int32_t y, int32_t z) {
+    auto it = c->where.find(RegionKey{x, y, z});
+    if (it == c->where.end()) return true;
+    return c->host_headers[it->second].x != 1u;
+}
+
+// Runs classify_pack over `list` (region indices; null = all) and reads back
+// the headers' kind/payload words.
+int pack_regions(vgi_ctx* c, const std::vector<uint32_t>* list) {
+    const uint32_t n = (uint32_t)c->keys.size();
+    uint32_t grid = n;
+    const uint32_t* dlist = nullptr;
+    if (list) {
+        grid = (uint32_t)list->size();
+        VGI_CUDA(c, c->region_list.reserve(std::max<size_t>(grid, 1)));
+        VGI_CUDA(c, cudaMemcpyAsync(c->region_list.ptr, list->data(), grid * 4, cudaMemcpyHostToDevice, c->stream));
+        dlist = c->region_list.ptr;
+    }
+    VGI_CUDA(c, cudaMemcpyAsync(c->alloc.ptr, &c->cells_used, 8, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->pack_error.ptr, 0, 4, c->stream));
+    launch_classify_pack(c->voxels.ptr, dlist, grid, n, c->headers.ptr, c->cells.ptr, c->alloc.ptr, c->cells.count, c->pack_error.ptr,
+                         c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    uint32_t err = 0;
+    unsigned long long used = 0;
+    VGI_CUDA(c, cudaMemcpyAsync(&err, c->pack_error.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(&used, c->alloc.ptr, 8, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(c->host_headers.data(), c->headers.ptr, n * sizeof(uint4), cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err) return fail(c, VGI_ERR_CAPACITY, "cell arena exhausted");
+    c->cells_used = used;
+    return VGI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vgi_create(const vgi_config* config, vgi_ctx** out) {
+    if (!out) return VGI_ERR_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return VGI_UNAVAILABLE;
+    int device = config ? config->device : 0;
+    if (device < 0 || device >= count) return VGI_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return VGI_UNAVAILABLE;
+    auto* c = new vgi_ctx();
+    c->device = device;
+    c->transport = default_transport();
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        c->counters.reserve(16) != cudaSuccess || c->alloc.reserve(1) != cudaSuccess || c->pack_error.reserve(1) != cudaSuccess) {
+        delete c;
+        return VGI_ERR_CUDA;
+    }
+    *out = c;
+    return VGI_OK;
+}
+
+int vgi_destroy(vgi_ctx* c) {
+    if (!c) return VGI_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->directory.release(); c->headers.release(); c->cells.release(); c->voxels.release(); c->alloc.release();
+    c->pack_error.release(); c->edit_buf.release(); c->zw.release(); c->region_list.release();
+    c->materials.release(); c->lights.release(); c->emitters.release();
+    c->tasks.release(); c->results.release(); c->state.release(); c->slot_meta.release(); c->checkpoint.release();
+    c->face_index.release(); c->cache.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
+    c->counters.release();
+    for (auto& e : c->marks)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return VGI_OK;
+}
+
+const char* vgi_last_error(const vgi_ctx* c) { return c ? c->error.c_str() : "null context"; }
+
+int vgi_stream(vgi_ctx* c, void** stream) {
+    if (!c || !stream) return VGI_ERR_INVALID;
+    *stream = (void*)c->stream;
+    return VGI_OK;
+}
+
+int vgi_sync(vgi_ctx* c) {
+    if (!c) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides) {
+    if (!c || (n && (!coords || !voxels))) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    c->keys.assign(n, RegionKey{0, 0, 0});
+    c->where.clear();
+    for (uint32_t r = 0; r < n; ++r) {
+        c->keys[r] = RegionKey{coords[r * 3], coords[r * 3 + 1], coords[r * 3 + 2]};
+        if (!c->where.emplace(c->keys[r], r).second) return fail(c, VGI_ERR_INVALID, "duplicate region coordinate");
+    }
+    for (size_t i = 0; i < (size_t)n * 4096; ++i)
+        if (voxels[i] > 256) return fail(c, VGI_ERR_INVALID, "voxel value above 256 (materials are 0..255, 256 is air)");
+    c->host_voxels.assign(voxels, voxels + (size_t)n * 4096);
+    c->strides.assign(n, 0);
+    if (strides) std::copy(strides, strides + n, c->strides.begin());
+    c->host_headers.assign(n, make_uint4(0, 0, 0, 0));
+    // Worst case: every region mixed with 64 mixed bricks (64 + 64 * 32 words);
+    // brick pointers are 30-bit word offsets.
+    unsigned long long capacity = std::min<unsigned long long>((unsigned long long)n * (64 + 64 * 32) + 64, 1ull << 30);
+    VGI_CUDA(c, c->voxels.reserve((size_t)std::max<uint32_t>(n, 1) * 4096));
+    VGI_CUDA(c, c->headers.reserve(std::max<uint32_t>(n, 1)));
+    VGI_CUDA(c, c->cells.reserve(capacity));
+    c->cells.count = capacity;
+    if (n) VGI_CUDA(c, cudaMemcpyAsync(c->voxels.ptr, voxels, (size_t)n * 8192, cudaMemcpyHostToDevice, c->stream));
+    c->cells_used = 0;
+    int rc = pack_regions(c, nullptr);
+    if (rc != VGI_OK) return rc;
+    // Region bounds and the top-level field grown from an empty scene
+    // (TransportScene::with_page_contents from the default scene).
+    int32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    if (n) {
+        lo[0] = hi[0] = c->keys[0].x; lo[1] = hi[1] = c->keys[0].y; lo[2] = hi[2] = c->keys[0].z;
+        for (const RegionKey& k : c->keys) {
+            lo[0] = std::min(lo[0], k.x); lo[1] = std::min(lo[1], k.y); lo[2] = std::min(lo[2], k.z);
+            hi[0] = std::max(hi[0], k.x); hi[1] = std::max(hi[1], k.y); hi[2] = std::max(hi[2], k.z);
+        }
+    }
+    for (int a = 0; a < 3; ++a) { c->bounds[a] = lo[a]; c->bounds[3 + a] = hi[a]; }
+    c->top = TopLevelField{}.updated(lo, hi, n > 0, [c](int32_t x, int32_t y, int32_t z) { return region_blocked(c, x, y, z); }, {});
+    rc = finish_headers(c);
+    if (rc != VGI_OK) return rc;
+    std::vector<int32_t> dir = build_directory(c->keys);
+    c->dir_slots = dir.size() / 4;
+    VGI_CUDA(c, c->directory.reserve(c->dir_slots));
+    VGI_CUDA(c, cudaMemcpyAsync(c->directory.ptr, dir.data(), dir.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->geometry = true;
+    return VGI_OK;
+}
+
+int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, const uint32_t* headers, uint32_t n_headers,
+                      const uint32_t* cells, uint64_t n_cells, const int32_t* bounds6) {
+    if (!c || !directory || !headers || !bounds6 || slots == 0 || (slots & (slots - 1))) return VGI_ERR_INVALID;
+    if (n_cells && !cells) return VGI_ERR_INVALID;
+    // Every index the traversal follows must stay inside the arrays.
+    for (uint64_t s = 0; s < slots; ++s) {
+        int32_t w = directory[s * 4 + 3];
+        if (w < -1 || (w >= 0 && (uint32_t)w >= n_headers)) return fail(c, VGI_ERR_INVALID, "directory entry names no header");
+    }
+    for (uint32_t h = 0; h < n_headers; ++h) {
+        const uint32_t kind = headers[h * 4], payload = headers[h * 4 + 1];
+        if (kind == 2 && payload > 255) return fail(c, VGI_ERR_INVALID, "uniform region material above 255");
+        if (kind != 3) continue;
+        if ((uint64_t)payload + 64 > n_cells) return fail(c, VGI_ERR_INVALID, "brick table outside the cells");
+        for (uint32_t b = 0; b < 64; ++b) {
+            const uint32_t word = cells[payload + b];
+            if ((word & 3u) == 1u && (word >> 2) > 255) return fail(c, VGI_ERR_INVALID, "uniform brick material above 255");
+            if ((word & 3u) == 3u) return fail(c, VGI_ERR_INVALID, "brick word state 3");
+            if ((word & 3u) != 2u) continue;
+            const uint64_t ptr = word >> 2;
+            if (ptr + 32 > n_cells) return fail(c, VGI_ERR_INVALID, "brick payload outside the cells");
+            for (uint32_t k = 0; k < 32; ++k)
+                for (uint32_t half = 0; half < 2; ++half) {
+                    const uint32_t cell = (cells[ptr + k] >> (16 * half)) & 0xffffu;
+                    if ((cell & 1u) && (cell >> 1) > 255) return fail(c, VGI_ERR_INVALID, "voxel material above 255");
+                }
+        }
+    }
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, c->directory.reserve(slots));
+    VGI_CUDA(c, c->headers.reserve(std::max<uint32_t>(n_headers, 1)));
+    VGI_CUDA(c, c->cells.reserve(std::max<uint64_t>(n_cells, 1)));
+    VGI_CUDA(c, cudaMemcpyAsync(c->directory.ptr, directory, slots * 16, cudaMemcpyHostToDevice, c->stream));
+    if (n_headers) VGI_CUDA(c, cudaMemcpyAsync(c->headers.ptr, headers, (size_t)n_headers * 16, cudaMemcpyHostToDevice, c->stream));
+    if (n_cells) VGI_CUDA(c, cudaMemcpyAsync(c->cells.ptr, cells, n_cells * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->dir_slots = slots;
+    c->cells_used = n_cells;
+    for (int k = 0; k < 6; ++k) c->bounds[k] = bounds6[k];
+    c->keys.clear();
+    c->where.clear();
+    c->host_voxels.clear();
+    c->host_headers.clear();
+    c->geometry = true;
+    return VGI_OK;
+}
+
+int vgi_edit_voxels(vgi_ctx* c, const int32_t* edits, uint32_t n) {
+    if (!c || (n && !edits)) return VGI_ERR_INVALID;
+    if (!c->geometry || c->keys.empty()) return fail(c, VGI_ERR_STATE, "edits need geometry uploaded as regions");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    std::vector<uint2> packed;
+    packed.reserve(n);
+    std::vector<uint32_t> dirty;
+    std::vector<uint8_t> was_blocked(c->keys.size(), 2);
+    for (uint32_t e = 0; e < n; ++e) {
+        int32_t x = edits[e * 4], y = edits[e * 4 + 1], z = edits[e * 4 + 2];
+        int32_t value = edits[e * 4 + 3];
+        if (value < 0 || value > 256) return fail(c, VGI_ERR_INVALID, "voxel value outside 0..256");
+        auto it = c->where.find(RegionKey{x >> 4, y >> 4, z >> 4});
+        if (it == c->where.end()) continue;
+        uint32_t r = it->second;
+        uint32_t local = (uint32_t)((x & 15) + 16 * ((y & 15) + 16 * (z & 15)));
+        c->host_voxels[(size_t)r * 4096 + local] = (uint16_t)value;
+        packed.push_back(make_uint2(r, (local << 16) | (uint32_t)value));
+        if (was_blocked[r] == 2) {
+            was_blocked[r] = c->host_headers[r].x != 1u ? 1 : 0;
+            dirty.push_back(r);
+        }
+    }
+    if (packed.empty()) return VGI_OK;
+    VGI_CUDA(c, c->edit_buf.reserve(packed.size()));
+    VGI_CUDA(c, cudaMemcpyAsync(c->edit_buf.ptr, packed.data(), packed.size() * sizeof(uint2), cudaMemcpyHostToDevice, c->stream));
+    launch_scatter_edits(c->edit_buf.ptr, (uint32_t)packed.size(), c->voxels.ptr, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    // Repack only the edited regions into fresh cell space; a full repack
+    // reclaims space once the arena passes three quarters.
+    bool full = c->cells_used + (unsigned long long)dirty.size() * (64 + 64 * 32) > c->cells.count * 3 / 4;
+    if (full) c->cells_used = 0;
+    int rc = pack_regions(c, full ? nullptr : &dirty);
+    if (rc != VGI_OK) return rc;
+    std::vector<RegionKey> changed;
+    for (uint32_t r : dirty) {
+        uint8_t now = c->host_headers[r].x != 1u ? 1 : 0;
+        if (now != was_blocked[r]) changed.push_back(c->keys[r]);
+    }
+    if (!changed.empty()) {
+        std::sort(changed.begin(), changed.end(), [](const RegionKey& a, const RegionKey& b) {
+            if (a.z != b.z) return a.z < b.z;
+            if (a.y != b.y) return a.y < b.y;
+            return a.x < b.x;
+        });
+        c->top = c->top.updated(c->bounds, c->bounds + 3, true,
+                                [c](int32_t x, int32_t y, int32_t z) { return region_blocked(c, x, y, z); }, changed);
+    }
+    rc = finish_headers(c);
+    if (rc != VGI_OK) return rc;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_geometry_info(vgi_ctx* c, uint64_t* sizes3, int32_t* bounds6) {
+    if (!c || !sizes3 || !bounds6) return VGI_ERR_INVALID;
+    if (!c->geometry) return fail(c, VGI_ERR_STATE, "no geometry uploaded");
+    sizes3[0] = c->dir_slots;
+    sizes3[1] = c->keys.empty() ? c->headers.count : c->keys.size();
+    sizes3[2] = c->cells_used;
+    for (int k = 0; k < 6; ++k) bounds6[k] = c->bounds[k];
+    return VGI_OK;
+}
+
+int vgi_read_geometry(vgi_ctx* c, int32_t* directory, uint32_t* headers, uint32_t* cells) {
+    uint64_t sizes[3];
+    int32_t b[6];
+    int rc = vgi_geometry_info(c, sizes, b);
+    if (rc != VGI_OK) return rc;
+    if (directory) VGI_CUDA(c, cudaMemcpyAsync(directory, c->directory.ptr, sizes[0] * 16, cudaMemcpyDeviceToHost, c->stream));
+    if (headers) VGI_CUDA(c, cudaMemcpyAsync(headers, c->headers.ptr, sizes[1] * 16, cudaMemcpyDeviceToHost, c->stream));
+    if (cells && sizes[2]) VGI_CUDA(c, cudaMemcpyAsync(cells, c->cells.ptr, sizes[2] * 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_set_materials(vgi_ctx* c, const float* m) {
+    if (!c || !m) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    c->host_materials.assign(m, m + 256 * 16);
+    VGI_CUDA(c, c->materials.reserve(256 * 4));
+    VGI_CUDA(c, cudaMemcpyAsync(c->materials.ptr, m, 256 * 64, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_set_lights(vgi_ctx* c, const float* lights, uint32_t n, uint32_t n_directional) {
+    if (!c || (n && !lights) || n_directional > n || n > 4096) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    // An empty light list still uploads one default record (src/gpu.rs:757-759).
+    std::vector<float> words(std::max<uint32_t>(n, 1) * 12, 0.0f);
+    if (n) std::copy(lights, lights + n * 12, words.begin());
+    VGI_CUDA(c, c->lights.reserve(words.size() / 4));
+    VGI_CUDA(c, cudaMemcpyAsync(c->lights.ptr, words.data(), words.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->n_lights = n;
+    c->n_directional = n_directional;
+    return VGI_OK;
+}
+
+int vgi_set_environment(vgi_ctx* c, const float* rgb3) {
+    if (!c || !rgb3) return VGI_ERR_INVALID;
+    c->env[0] = rgb3[0];
+    c->env[1] = rgb3[1];
+    c->env[2] = rgb3[2];
+    c->env[3] = 0.0f;
+    return VGI_OK;
+}
+
+int vgi_set_emitters(vgi_ctx* c, const uint32_t* words, uint64_t n_words, uint32_t n_faces, float total_weight) {
+    if (!c || !words || n_words < 8 || (n_words & 3)) return VGI_ERR_INVALID;
+    // Layout check (src/gpu.rs:686-711, src/emission/tree.rs:173-195): face
+    // records, then light-tree nodes whose children follow their parent.
+    const uint64_t records = n_faces == 0 ? 1 : n_faces;
+    if (n_words < records * 8) return fail(c, VGI_ERR_INVALID, "emitter words shorter than the face records");
+    if (n_faces > 0) {
+        float tree_len_f;
+        std::memcpy(&tree_len_f, &words[7], 4);
+        if (!(tree_len_f >= 0.0f) || tree_len_f > 4.0e9f) return fail(c, VGI_ERR_INVALID, "bad light-tree length");
+        const uint64_t nodes = (uint64_t)tree_len_f;
+        if (n_words != records * 8 + nodes * 16) return fail(c, VGI_ERR_INVALID, "emitter word count does not match the tree");
+        for (uint64_t f = 0; f < n_faces; ++f) {
+            float m;
+            std::memcpy(&m, &words[f * 8 + 6], 4);
+            if (!(m >= 0.0f && m < 256.0f)) return fail(c, VGI_ERR_INVALID, "emitter material outside 0..255");
+        }
+        for (uint64_t i = 0; i < nodes; ++i) {
+            const uint32_t* w = words + records * 8 + i * 16;
+            const uint32_t left = w[12], right = w[13];
+            if (left == 0xffffffffu) {
+                if (right >= n_faces) return fail(c, VGI_ERR_INVALID, "light-tree leaf names no face");
+            } else if (left <= i || right <= i || left >= nodes || right >= nodes) {
+                return fail(c, VGI_ERR_INVALID, "light-tree children must follow their parent");
+            }
+        }
+    }
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, c->emitters.reserve(n_words / 4));
+    VGI_CUDA(c, cudaMemcpyAsync(c->emitters.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->emitter_count = (float)n_faces;
+    c->emitter_total = total_weight;
+    return VGI_OK;
+}
+
+int vgi_build_emitters(vgi_ctx* c) {
+    if (!c) return VGI_ERR_INVALID;
+    if (c->keys.empty() && c->geometry) return fail(c, VGI_ERR_STATE, "emitters need geometry uploaded as regions");
+    EmitterWords e = build_emitters(c->keys, c->host_voxels.data(), c->host_materials.data());
+    return vgi_set_emitters(c, e.words.data(), e.words.size(), e.faces, e.total_weight);
+}
+
+int vgi_set_transport(vgi_ctx* c, const vgi_transport* t) {
+    if (!c || !t) return VGI_ERR_INVALID;
+    vgi_transport n = *t;
+    n.reach = norm_reach(n.reach);
+    n.bounces = norm_bounces(n.bounces);
+    if (n.path_steps == 0) n.path_steps = 2048;
+    if (n.lanes && (n.lanes & (n.lanes - 1))) return fail(c, VGI_ERR_INVALID, "lanes must be a power of two");
+    if (n.lanes > 32) return fail(c, VGI_ERR_INVALID, "lanes above 32");
+    c->transport = n;
+    return VGI_OK;
+}
+
+int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
+    if (!c || (n && !faces)) return VGI_ERR_INVALID;
+    if (n >= (1u << 29)) return fail(c, VGI_ERR_CAPACITY, "slot index exceeds 29 bits");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    std::vector<std::array<int32_t, 4>> keys(n);
+    std::vector<uint4> tasks((size_t)n * 2), meta((size_t)n * 3, make_uint4(0, 0, 0, 0));
+    for (uint32_t s = 0; s < n; ++s) {
+        if (faces[s].face > 5 || faces[s].material > 255) return fail(c, VGI_ERR_INVALID, "face or material out of range");
+        keys[s] = {faces[s].voxel[0], faces[s].voxel[1], faces[s].voxel[2], (int32_t)faces[s].face};
+        tasks[s * 2] = make_uint4((uint32_t)faces[s].voxel[0], (uint32_t)faces[s].voxel[1], (uint32_t)faces[s].voxel[2], faces[s].face);
+        tasks[s * 2 + 1] = make_uint4(0, 0, 0, 0);
+        // Slot identity: voxel, face | LIVE (8) | material << 16.
+        meta[s * 3] = make_uint4((uint32_t)faces[s].voxel[0], (uint32_t)faces[s].voxel[1], (uint32_t)faces[s].voxel[2],
+                                 faces[s].face | 8u | (faces[s].material << 16));
+    }
+    std::vector<uint32_t> index = build_face_index(keys);
+    size_t m = std::max<uint32_t>(n, 1);
+    VGI_CUDA(c, c->tasks.reserve(m * 2));
+    VGI_CUDA(c, c->results.reserve(m * 6));
+    VGI_CUDA(c, c->state.reserve(m * 9));
+    VGI_CUDA(c, c->slot_meta.reserve(m * 3));
+    VGI_CUDA(c, c->checkpoint.reserve(m * 3));
+    VGI_CUDA(c, c->cache.reserve(m));
+    VGI_CUDA(c, c->face_index.reserve(index.size() / 4));
+    VGI_CUDA(c, cudaMemcpyAsync(c->tasks.ptr, tasks.data(), (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->results.ptr, 0, m * 96, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->state.ptr, 0, m * 144, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(c->slot_meta.ptr, meta.data(), (size_t)n * 48, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->checkpoint.ptr, 0, m * 48, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->cache.ptr, 0, m * 16, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(c->face_index.ptr, index.data(), index.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->n_slots = n;
+    return VGI_OK;
+}
+
+int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
+    int rc = check_ready(c, true);
+    if (rc != VGI_OK) return rc;
+    if (samples == 0) return fail(c, VGI_ERR_INVALID, "samples must be positive");
+    AccumArgs acc = accum_args(c, samples, clock_ms);
+    if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[0], c->stream));
+    launch_prepare(acc, c->stream);
+    if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[1], c->stream));
+    TraceArgs tr = trace_args(c, c->tasks.ptr, c->results.ptr, c->n_slots, samples, true);
+    launch_trace(tr, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, false, c->stream);
+    if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[2], c->stream));
+    launch_accumulate(acc, c->stream);
+    if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[3], c->stream));
+    VGI_CUDA(c, cudaGetLastError());
+    c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
+    if (c->batch_id == 0) c->batch_id = 1;
+    return VGI_OK;
+}
+
+int vgi_set_timing(vgi_ctx* c, int enable) {
+    if (!c) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    if (enable && !c->marks[0])
+        for (auto& e : c->marks) VGI_CUDA(c, cudaEventCreate(&e));
+    c->timing = enable != 0;
+    return VGI_OK;
+}
+
+int vgi_frame_times(vgi_ctx* c, float* ms3) {
+    if (!c || !ms3) return VGI_ERR_INVALID;
+    if (!c->timing) return fail(c, VGI_ERR_STATE, "timing not enabled");
+    VGI_CUDA(c, cudaEventSynchronize(c->marks[3]));
+    for (int k = 0; k < 3; ++k) VGI_CUDA(c, cudaEventElapsedTime(&ms3[k], c->marks[k], c->marks[k + 1]));
+    return VGI_OK;
+}
+
+int vgi_trace_batch(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samples, uint32_t clock_ms, uint32_t* results) {
+    int rc = check_ready(c, true);
+    if (rc != VGI_OK) return rc;
+    if (!tasks || !results || n != c->n_slots) return fail(c, VGI_ERR_INVALID, "one task per slot expected");
+    VGI_CUDA(c, cudaMemcpyAsync(c->tasks.ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    rc = vgi_frame(c, samples, clock_ms);
+    if (rc != VGI_OK) return rc;
+    VGI_CUDA(c, cudaMemcpyAsync(results, c->results.ptr, (size_t)n * 96, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_census(vgi_ctx* c, uint32_t samples, vgi_counters* counters) {
+    int rc = check_ready(c, true);
+    if (rc != VGI_OK) return rc;
+    VGI_CUDA(c, c->scratch_tasks.reserve((size_t)c->n_slots * 2));
+    VGI_CUDA(c, c->scratch_results.reserve((size_t)c->n_slots * 6));
+    // The next frame's tasks: the slot tasks with each slot's sequence.
+    VGI_CUDA(c, cudaMemcpyAsync(c->scratch_tasks.ptr, c->tasks.ptr, (size_t)c->n_slots * 32, cudaMemcpyDeviceToDevice, c->stream));
+    AccumArgs acc = accum_args(c, samples, 0);
+    acc.tasks = c->scratch_tasks.ptr;
+    acc.slot_meta = nullptr;  // begin_trace only
+    launch_prepare(acc, c->stream);
+    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 10 * 8, c->stream));
+    TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, c->n_slots, samples, true);
+    launch_trace(tr, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, true, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    return read_counters(c, counters);
+}
+
+int vgi_trace_tasks(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samples, uint32_t* results, vgi_counters* counters) {
+    int rc = check_ready(c, false);
+    if (rc != VGI_OK) return rc;
+    if (!tasks || !results) return VGI_ERR_INVALID;
+    if (n == 0) return VGI_OK;
+    VGI_CUDA(c, c->scratch_tasks.reserve((size_t)n * 2));
+    VGI_CUDA(c, c->scratch_results.reserve((size_t)n * 6));
+    VGI_CUDA(c, cudaMemcpyAsync(c->scratch_tasks.ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 10 * 8, c->stream));
+    bool with_cache = c->n_slots > 0;
+    TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, n, samples, with_cache);
+    launch_trace(tr, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, counters != nullptr, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    VGI_CUDA(c, cudaMemcpyAsync(results, c->scratch_results.ptr, (size_t)n * 96, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (counters) return read_counters(c, counters);
+    return VGI_OK;
+}
+
+int vgi_apply_events(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint64_t n_words) {
+    if (!c || (n_words && !words) || (n_words & 3) || (uint64_t)n_events * 12 > n_words) return VGI_ERR_INVALID;
+    if (c->n_slots == 0) return VGI_OK;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, c->events.reserve(std::max<uint64_t>(n_words / 4, 1)));
+    if (n_words) VGI_CUDA(c, cudaMemcpyAsync(c->events.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    c->n_events = n_events;
+    AccumArgs acc = accum_args(c, 0, 0);
+    launch_apply_events(acc, c->events.ptr, c->n_slots, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    c->n_events = 0;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_read_results(vgi_ctx* c, uint32_t first, uint32_t n, uint32_t* words24) {
+    if (!c || !words24 || (uint64_t)first + n > c->n_slots) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaMemcpyAsync(words24, c->results.ptr + (size_t)first * 6, (size_t)n * 96, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_read_state(vgi_ctx* c, uint32_t first, uint32_t n, uint32_t* words36) {
+    if (!c || !words36 || (uint64_t)first + n > c->n_slots) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaMemcpyAsync(words36, c->state.ptr + (size_t)first * 9, (size_t)n * 144, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_write_state(vgi_ctx* c, uint32_t first, uint32_t n, const uint32_t* words36) {
+    if (!c || !words36 || (uint64_t)first + n > c->n_slots) return VGI_ERR_INVALID;
+    std::vector<float4> rec(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t* s = words36 + (size_t)i * 36;
+        float r, g, b, w;
+        std::memcpy(&r, s + 0, 4);
+        std::memcpy(&g, s + 1, 4);
+        std::memcpy(&b, s + 2, 4);
+        std::memcpy(&w, s + 5, 4);
+        rec[i] = make_float4(r, g, b, w);
+    }
+    VGI_CUDA(c, cudaMemcpyAsync(c->state.ptr + (size_t)first * 9, words36, (size_t)n * 144, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(c->cache.ptr + first, rec.data(), (size_t)n * 16, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_read_slot_meta(vgi_ctx* c, uint32_t first, uint32_t n, uint32_t* words12) {
+    if (!c || !words12 || (uint64_t)first + n > c->n_slots) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaMemcpyAsync(words12, c->slot_meta.ptr + (size_t)first * 3, (size_t)n * 48, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+void vgi_material_record(const float* diffuse3, const float* emission3, float* out16) {
+    // VoxelGiMaterials::bounded (src/world.rs:166-173) then GpuMaterial
+    // (src/gpu.rs:713-723): diffuse clamped to [0, 1], emission to [0, 1e12].
+    auto bounded = [](float v, float hi) { return std::isfinite(v) ? std::min(std::max(v, 0.0f), hi) : 0.0f; };
+    std::memset(out16, 0, 64);
+    float emax = 0.0f;
+    for (int k = 0; k < 3; ++k) {
+        out16[k] = bounded(diffuse3[k], 1.0f);
+        out16[8 + k] = bounded(emission3[k], 1.0e12f);
+    }
+    emax = std::max(out16[8], std::max(out16[9], out16[10]));
+    out16[13] = emax;
+}
+
+void vgi_directional_light_record(const float* d, const float* radiance3, const float* custom3, float* out12) {
+    // GpuLight for a directional source (src/gpu.rs:733-744): glam's
+    // normalize_or_zero (v * (1 / length)), range -1.
+    std::memset(out12, 0, 48);
+    float len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    float rcp = 1.0f / len;
+    if (std::isfinite(rcp) && rcp > 0.0f) {
+        out12[0] = d[0] * rcp;
+        out12[1] = d[1] * rcp;
+        out12[2] = d[2] * rcp;
+    }
+    out12[3] = -1.0f;
+    for (int k = 0; k < 3; ++k) {
+        out12[4 + k] = radiance3[k];
+        out12[9 + k] = custom3 ? custom3[k] : 0.0f;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,247 @@
+// NAADF upload path on the GPU: region classification, brick-level and
+// voxel-level AADF construction and cell packing, one CTA per 16^3 region.
+//
+// Behaviour follows (paths within nathanaelneveux/global-illumination,
+// crates/bevy_voxel_gi/src/):
+//   world.rs:243-319      NaadfRegion::build (Empty / Uniform / mixed)
+//   world.rs:352-384      brick_voxel_bounds / brick_bounds
+//   naadf.rs:37-148       build_aadf / try_grow (Jacobi sweeps, max(size)-1 rounds)
+//   gpu_scene.rs:174-239  header kinds, 64-word brick tables, 32-word bricks
+//   gpu_scene.rs:458-467  pack_bytes / pack_extents
+//
+// B200 layout: a CTA stages its region's 8 KB of voxels in shared memory with
+// 16-byte loads, classifies it with block votes, builds the 4^3 brick field and
+// then each warp builds the 4^3 voxel field of one mixed brick at a time
+// (two cells per lane, __syncwarp between sweeps). Cell space is reserved
+// with one atomic per mixed region, so the whole pack is a single streaming
+// pass over the voxels. Identical brick payloads are not interned here:
+// every mixed brick owns its 32 words (the reference deduplicates them on the
+// CPU; traversal reads the same values either way).
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace vgi {
+namespace {
+
+constexpr int kThreads = 128;
+constexpr uint16_t kAir = 256;
+
+// An AADF as six 4-bit extents (NEG_X, POS_X, NEG_Y, POS_Y, NEG_Z, POS_Z).
+__device__ __forceinline__ uint32_t ext_get(uint32_t a, int d) { return (a >> (d * 4)) & 15u; }
+__device__ __forceinline__ uint32_t ext_inc(uint32_t a, int d) { return a + (1u << (d * 4)); }
+
+// try_grow on a 4x4x4 grid (naadf.rs:117-148): `cur` grows one step in
+// direction d towards neighbour n if n is in the grid, unblocked, and covers
+// every other extent of cur.
+__device__ __forceinline__ uint32_t try_grow4(uint32_t cur, int nx, int ny, int nz, int d, uint64_t blocked, const uint32_t* src) {
+    if (nx < 0 || ny < 0 || nz < 0 || nx > 3 || ny > 3 || nz > 3) return cur;
+    if (ext_get(cur, d) == 255u) return cur;
+    int ni = nx + 4 * (ny + 4 * nz);
+    if ((blocked >> ni) & 1ull) return cur;
+    uint32_t nb = src[ni];
+    int opposite = d ^ 1;
+#pragma unroll
+    for (int b = 0; b < 6; ++b)
+        if (b != opposite && ext_get(nb, b) < ext_get(cur, b)) return cur;
+    return ext_inc(cur, d);
+}
+
+// build_aadf over a 4^3 grid by one warp: buf holds 2 x 64 words; returns
+// with the result in buf[0..63]. Not called for an all-empty grid.
+__device__ void build_aadf4_warp(uint64_t blocked, uint32_t* buf, int lane) {
+    uint32_t* src = buf;
+    uint32_t* dst = buf + 64;
+    src[lane] = 0u;
+    src[lane + 32] = 0u;
+    __syncwarp();
+    if (blocked == ~0ull) return;
+    for (int round = 0; round < 3; ++round) {
+        for (int axis = 0; axis < 3; ++axis) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                int i = lane + 32 * h;
+                int x = i & 3, y = (i >> 2) & 3, z = i >> 4;
+                uint32_t cur = 0u;
+                if (!((blocked >> i) & 1ull)) {
+                    cur = src[i];
+                    int dx = axis == 0, dy = axis == 1, dz = axis == 2;
+                    cur = try_grow4(cur, x - dx, y - dy, z - dz, axis * 2, blocked, src);
+                    cur = try_grow4(cur, x + dx, y + dy, z + dz, axis * 2 + 1, blocked, src);
+                }
+                dst[i] = cur;
+            }
+            __syncwarp();
+            uint32_t* t = src;
+            src = dst;
+            dst = t;
+        }
+    }
+    // 9 sweeps: the result is in the buffer that started as `dst`; move it.
+    uint32_t a = src[lane], b = src[lane + 32];
+    __syncwarp();
+    buf[lane] = a;
+    buf[lane + 32] = b;
+    __syncwarp();
+}
+
+__device__ __forceinline__ uint32_t pack_extents(uint32_t a) {
+    uint32_t bits = 0;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) bits |= (ext_get(a, d) & 3u) << (d * 2);
+    return bits;
+}
+
+// One CTA per region. headers[r] receives (kind, material or cell offset);
+// z and w (top-level extents, stride) are written by the host runtime.
+__global__ void __launch_bounds__(kThreads) classify_pack_kernel(const uint16_t* __restrict__ voxels, const uint32_t* __restrict__ regions,
+                                                                 uint32_t n, uint4* __restrict__ headers, uint32_t* __restrict__ cells,
+                                                                 unsigned long long* __restrict__ alloc, unsigned long long capacity,
+                                                                 uint32_t* __restrict__ error) {
+    __shared__ __align__(16) uint16_t vox[4096];
+    __shared__ uint32_t brick_info[64];   // bit 0 uniform, bit 1 occupied, bits 16.. first material
+    __shared__ uint32_t table[64];
+    __shared__ uint32_t scratch[4][128];
+    __shared__ uint32_t mixed_list[64];
+    __shared__ uint32_t n_mixed;
+    __shared__ unsigned long long base;
+    const uint32_t r = regions ? regions[blockIdx.x] : blockIdx.x;
+    if (r >= n) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(voxels + (size_t)r * 4096);
+        uint4* dst = reinterpret_cast<uint4*>(vox);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dst[tid + k * kThreads] = __ldg(src + tid + k * kThreads);
+    }
+    if (tid == 0) n_mixed = 0;
+    __syncthreads();
+    const uint16_t v0 = vox[0];
+    bool air = true, same = true;
+    for (int i = tid; i < 4096; i += kThreads) {
+        air = air && vox[i] == kAir;
+        same = same && vox[i] == v0;
+    }
+    const bool all_air = __syncthreads_and(air);
+    const bool all_same = __syncthreads_and(same);
+    if (all_air || all_same) {
+        if (tid == 0) headers[r] = make_uint4(all_air ? 1u : 2u, (uint32_t)(all_air ? kAir : v0), 0u, 0u);
+        return;
+    }
+    // Per-brick uniformity and occupancy.
+    if (tid < 64) {
+        int bx = tid & 3, by = (tid >> 2) & 3, bz = tid >> 4;
+        uint16_t first = vox[(bx * 4) + 16 * ((by * 4) + 16 * (bz * 4))];
+        bool uniform = true, occupied = false;
+        for (int v = 0; v < 64; ++v) {
+            uint16_t m = vox[(bx * 4 + (v & 3)) + 16 * ((by * 4 + ((v >> 2) & 3)) + 16 * (bz * 4 + (v >> 4)))];
+            uniform = uniform && m == first;
+            occupied = occupied || m != kAir;
+        }
+        brick_info[tid] = (uniform ? 1u : 0u) | (occupied ? 2u : 0u) | ((uint32_t)first << 16);
+    }
+    __syncthreads();
+    // Brick-level field (brick_bounds) by warp 0; the mixed-brick list by warp 1.
+    if (warp == 0) {
+        uint64_t occ = 0;
+        for (int b = 0; b < 64; ++b) occ |= (uint64_t)((brick_info[b] >> 1) & 1u) << b;
+        build_aadf4_warp(occ, scratch[0], lane);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            int b = lane + 32 * h;
+            uint32_t info = brick_info[b];
+            uint32_t first = info >> 16;
+            if ((info & 1u) && first == kAir) table[b] = pack_extents(scratch[0][b]) << 2;
+            else if (info & 1u) table[b] = (first << 2) | 1u;
+            else table[b] = 2u;
+        }
+    } else if (warp == 1) {
+        // Mixed bricks in table order (ballot + popc keeps the order stable).
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            int b = lane + 32 * h;
+            bool mixed = !(brick_info[b] & 1u);
+            unsigned ballot = __ballot_sync(0xffffffffu, mixed);
+            uint32_t before = h == 0 ? 0u : (uint32_t)__popc(__ballot_sync(0xffffffffu, !(brick_info[lane] & 1u)));
+            if (mixed) mixed_list[before + __popc(ballot & ((1u << lane) - 1u))] = (uint32_t)b;
+            if (h == 1 && lane == 0) n_mixed = before + __popc(ballot);
+        }
+    }
+    __syncthreads();
+    const uint32_t words = 64u + 32u * n_mixed;
+    if (tid == 0) {
+        unsigned long long at = atomicAdd(alloc, (unsigned long long)words);
+        if (at + words > capacity) {
+            atomicOr(error, 1u);
+            base = ~0ull;
+        } else {
+            base = at;
+        }
+    }
+    __syncthreads();
+    if (base == ~0ull) return;
+    // Voxel-level fields and payloads: one mixed brick per warp at a time.
+    for (uint32_t k = warp; k < n_mixed; k += kThreads / 32) {
+        const uint32_t b = mixed_list[k];
+        const int bx = b & 3, by = (b >> 2) & 3, bz = b >> 4;
+        uint16_t m0, m1;
+        {
+            int v = lane, w = lane + 32;
+            m0 = vox[(bx * 4 + (v & 3)) + 16 * ((by * 4 + ((v >> 2) & 3)) + 16 * (bz * 4 + (v >> 4)))];
+            m1 = vox[(bx * 4 + (w & 3)) + 16 * ((by * 4 + ((w >> 2) & 3)) + 16 * (bz * 4 + (w >> 4)))];
+        }
+        uint64_t blocked = (uint64_t)__ballot_sync(0xffffffffu, m0 != kAir) | ((uint64_t)__ballot_sync(0xffffffffu, m1 != kAir) << 32);
+        build_aadf4_warp(blocked, scratch[warp], lane);
+        uint32_t c0 = m0 == kAir ? (pack_extents(scratch[warp][lane]) << 1) : (((uint32_t)m0 << 1) | 1u);
+        uint32_t c1 = m1 == kAir ? (pack_extents(scratch[warp][lane + 32]) << 1) : (((uint32_t)m1 << 1) | 1u);
+        // Cells 2j and 2j+1 share word j: lane l owns cells l and l+32, so
+        // word j (j < 16) takes cells 2j, 2j+1 from lanes 2j, 2j+1 (first half)
+        // and word 16 + j from their second halves.
+        uint32_t lo0 = __shfl_sync(0xffffffffu, c0, (lane & 15) * 2), hi0 = __shfl_sync(0xffffffffu, c0, (lane & 15) * 2 + 1);
+        uint32_t lo1 = __shfl_sync(0xffffffffu, c1, (lane & 15) * 2), hi1 = __shfl_sync(0xffffffffu, c1, (lane & 15) * 2 + 1);
+        uint32_t word = lane < 16 ? (lo0 | (hi0 << 16)) : (lo1 | (hi1 << 16));
+        const unsigned long long ptr = base + 64u + 32u * k;
+        cells[ptr + (lane < 16 ? lane : lane)] = word;
+        if (lane == 0) table[b] = ((uint32_t)ptr << 2) | 2u;
+        __syncwarp();
+    }
+    __syncthreads();
+    if (tid < 64) cells[base + tid] = table[tid];
+    if (tid == 0) headers[r] = make_uint4(3u, (uint32_t)base, 0u, 0u);
+}
+
+// Voxel edits: 2 words per edit (region index, local index << 16 | value).
+__global__ void scatter_edits_kernel(const uint2* __restrict__ edits, uint32_t n, uint16_t* __restrict__ voxels) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint2 e = edits[i];
+    voxels[(size_t)e.x * 4096 + (e.y >> 16)] = (uint16_t)(e.y & 0xffffu);
+}
+
+// Top-level extents and stride into header words z, w: 2 words per region.
+__global__ void set_header_extents_kernel(uint4* __restrict__ headers, const uint2* __restrict__ zw, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint2 v = zw[i];
+    headers[i].z = v.x;
+    headers[i].w = v.y;
+}
+
+}  // namespace
+
+void launch_classify_pack(const uint16_t* voxels, const uint32_t* regions, uint32_t grid, uint32_t n, uint4* headers, uint32_t* cells,
+                          unsigned long long* alloc, unsigned long long capacity, uint32_t* error, cudaStream_t s) {
+    if (grid == 0) return;
+    classify_pack_kernel<<<grid, kThreads, 0, s>>>(voxels, regions, n, headers, cells, alloc, capacity, error);
+}
+
+void launch_scatter_edits(const uint2* edits, uint32_t n, uint16_t* voxels, cudaStream_t s) {
+    if (n == 0) return;
+    scatter_edits_kernel<<<(n + 255) / 256, 256, 0, s>>>(edits, n, voxels);
+}
+
+void launch_set_header_extents(uint4* headers, const uint2* zw, uint32_t n, cudaStream_t s) {
+    if (n == 0) return;
+    set_header_extents_kernel<<<(n + 255) / 256, 256, 0, s>>>(headers, zw, n);
+}
+
+}  // namespace vgi

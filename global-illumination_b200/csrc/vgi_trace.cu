@@ -1,0 +1,830 @@
+// Face trace: the distance-skip DDA over NAADF geometry, the cosine-hemisphere
+// path estimator with emitter NEE and MIS, the world-cache gather, and the
+// per-face moment reduction.
+//
+// Behaviour follows the reference shaders line for line (paths within
+// nathanaelneveux/global-illumination, crates/bevy_voxel_gi/shaders/):
+//   voxel_traversal.wgsl:17-219  face_index_of, lookup_region, advance_box,
+//                                geometry_ahead, trace_domain_limited
+//   voxel_path.wgsl:63-520       cached_energy, emitter selection and light
+//                                tree, QMC sampler, hemisphere, direct_at,
+//                                sample_emitter, sample_terminal_emission,
+//                                advance_path, trace_receiver
+//   voxel_trace.wgsl:25-92       trace_moments, write_result,
+//                                trace_faces_parallel
+//
+// Layout on B200: one thread per (face, lane); the lanes of a face are
+// adjacent in a warp and trace the strided subsequences i = lane, lane + L, ...
+// (PATH_LANES = L). Lane 0 sums the lanes in order with warp shuffles, which
+// gives exactly the cooperative kernel's summation order. The material table
+// is staged in shared memory; geometry, face index, cache records and emitter
+// words are read through the read-only path (they stay resident in the 126 MB
+// L2 for the configurations this targets).
+#include "vgi_device.cuh"
+#include "vgi_types.cuh"
+
+namespace vgi {
+namespace {
+
+constexpr int kBlock = 256;
+
+template <bool C>
+struct Cnt {
+    __device__ void ray() {}
+    __device__ void step() {}
+    __device__ void bytes(uint32_t) {}
+    __device__ void status(uint32_t) {}
+    __device__ void path() {}
+    __device__ void unknown() {}
+    __device__ void cache_hit() {}
+};
+template <>
+struct Cnt<true> {
+    uint32_t rays = 0, steps = 0, paths = 0, unk = 0, hits = 0, st[4] = {0, 0, 0, 0};
+    unsigned long long b = 0;
+    __device__ void ray() { rays++; }
+    __device__ void step() { steps++; }
+    __device__ void bytes(uint32_t n) { b += n; }
+    __device__ void status(uint32_t s) { st[s & 3]++; }
+    __device__ void path() { paths++; }
+    __device__ void unknown() { unk++; }
+    __device__ void cache_hit() { hits++; }
+};
+
+struct Ray {
+    I3 voxel;
+    uint32_t material;
+    V3 position;
+    uint32_t status;
+    V3 normal;
+};
+
+struct Mat {
+    float4 diffuse;    // rgb, w unused (0)
+    float4 emission;   // rgb, w unused (0)
+    float weight;      // emission_extra.y
+};
+
+__device__ __forceinline__ uint32_t face_index_of(V3 n) {
+    if (n.x != 0.0f) return n.x < 0.0f ? 1u : 0u;
+    if (n.y != 0.0f) return n.y < 0.0f ? 3u : 2u;
+    if (n.z != 0.0f) return n.z < 0.0f ? 5u : 4u;
+    return 6u;
+}
+__device__ __forceinline__ V3 face_normal(uint32_t face) {
+    float s = (face & 1u) != 0u ? -1.0f : 1.0f;
+    uint32_t a = face >> 1;
+    return V3{a == 0 ? s : 0.0f, a == 1 ? s : 0.0f, a == 2 ? s : 0.0f};
+}
+
+template <bool C>
+__device__ __forceinline__ uint32_t lookup_region(const TraceArgs& A, int x, int y, int z, Cnt<C>& cnt) {
+    uint32_t slot = hash_voxel(x, y, z) & A.dir_mask;
+#pragma unroll 1
+    for (uint32_t attempt = 0; attempt < 32u; ++attempt) {
+        int4 e = __ldg(A.directory + slot);
+        cnt.bytes(16);
+        if (e.w == -1) return kNoIndex;
+        if (e.x == x && e.y == y && e.z == z) return (uint32_t)e.w;
+        slot = (slot + 1u) & A.dir_mask;
+    }
+    return kNoIndex;
+}
+
+__device__ __forceinline__ bool in_bounds(const TraceArgs& A, int x, int y, int z) {
+    return x >= A.mn[0] && y >= A.mn[1] && z >= A.mn[2] && x <= A.mx[0] && y <= A.mx[1] && z <= A.mx[2];
+}
+
+// advance_box (voxel_traversal.wgsl:90-107): exit normal and distance of the
+// ray from the box (cell - neg, cell + pos + 1) * size.
+__device__ __forceinline__ float4 advance_box(V3 p, V3 d, I3 cell, I3 ng, I3 ps, float size) {
+    float tx, ty, tz;
+    {
+        bool moving = fabsf(d.x) > 1e-8f;
+        float plane = d.x > 0.0f ? __fmul_rn((float)(cell.x + ps.x + 1), size) : __fmul_rn((float)(cell.x - ng.x), size);
+        float raw = __fdiv_rn(__fsub_rn(plane, p.x), moving ? d.x : 1.0f);
+        tx = (moving && raw >= -0.001f && raw < 1e30f) ? raw : 1e30f;
+    }
+    {
+        bool moving = fabsf(d.y) > 1e-8f;
+        float plane = d.y > 0.0f ? __fmul_rn((float)(cell.y + ps.y + 1), size) : __fmul_rn((float)(cell.y - ng.y), size);
+        float raw = __fdiv_rn(__fsub_rn(plane, p.y), moving ? d.y : 1.0f);
+        ty = (moving && raw >= -0.001f && raw < 1e30f) ? raw : 1e30f;
+    }
+    {
+        bool moving = fabsf(d.z) > 1e-8f;
+        float plane = d.z > 0.0f ? __fmul_rn((float)(cell.z + ps.z + 1), size) : __fmul_rn((float)(cell.z - ng.z), size);
+        float raw = __fdiv_rn(__fsub_rn(plane, p.z), moving ? d.z : 1.0f);
+        tz = (moving && raw >= -0.001f && raw < 1e30f) ? raw : 1e30f;
+    }
+    bool choose_y = ty < wmax(tx, 0.0f);
+    float dxy = wmax(choose_y ? ty : tx, 0.0f);
+    bool choose_z = tz < dxy;
+    float dist = wmax(choose_z ? tz : dxy, 0.0f);
+    float ax = (!choose_z && !choose_y) ? 1.0f : 0.0f;
+    float ay = (!choose_z && choose_y) ? 1.0f : 0.0f;
+    float az = choose_z ? 1.0f : 0.0f;
+    bool hit = dist < 1e30f;
+    float4 r;
+    r.x = hit ? __fmul_rn(ax, d.x > 0.0f ? -1.0f : 1.0f) : 0.0f;
+    r.y = hit ? __fmul_rn(ay, d.y > 0.0f ? -1.0f : 1.0f) : 0.0f;
+    r.z = hit ? __fmul_rn(az, d.z > 0.0f ? -1.0f : 1.0f) : 0.0f;
+    r.w = wmax(__fadd_rn(dist, 0.001f), 0.001f);
+    return r;
+}
+
+__device__ __forceinline__ I3 unpack_bytes(uint32_t v) { return I3{(int)(v & 255u), (int)((v >> 8) & 255u), (int)((v >> 16) & 255u)}; }
+__device__ __forceinline__ I3 neg_ext(uint32_t b) { return I3{(int)(b & 3u), (int)((b >> 4) & 3u), (int)((b >> 8) & 3u)}; }
+__device__ __forceinline__ I3 pos_ext(uint32_t b) { return I3{(int)((b >> 2) & 3u), (int)((b >> 6) & 3u), (int)((b >> 10) & 3u)}; }
+
+__device__ __forceinline__ I3 floor_div16(V3 p) {
+    return I3{f2i(floorf(__fdiv_rn(p.x, 16.0f))), f2i(floorf(__fdiv_rn(p.y, 16.0f))), f2i(floorf(__fdiv_rn(p.z, 16.0f)))};
+}
+
+// geometry_ahead (voxel_traversal.wgsl:108-121)
+template <bool C>
+__device__ bool geometry_ahead(const TraceArgs& A, V3 position, V3 dir, float remaining, Cnt<C>& cnt) {
+#pragma unroll 1
+    for (uint32_t step = 0; step < 2048u; ++step) {
+        cnt.step();
+        I3 r = floor_div16(position);
+        if (remaining < 0.0f || !in_bounds(A, r.x, r.y, r.z)) return false;
+        uint32_t index = lookup_region(A, r.x, r.y, r.z, cnt);
+        if (index != kNoIndex) {
+            cnt.bytes(16);
+            if (__ldg(&A.headers[index].x) != 1u) return true;
+        }
+        float travel = advance_box(position, dir, r, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f).w;
+        position = position + dir * travel;
+        remaining = __fsub_rn(remaining, travel);
+    }
+    return true;
+}
+
+// trace_domain_limited (voxel_traversal.wgsl:126-219)
+template <bool C>
+__device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_distance, bool visible_geometry, uint32_t max_steps,
+                            Cnt<C>& cnt) {
+    cnt.ray();
+    Ray res;
+    res.voxel = I3{0, 0, 0};
+    res.material = 0u;
+    res.position = V3{0.0f, 0.0f, 0.0f};
+    res.status = 0u;
+    res.normal = V3{0.0f, 0.0f, 0.0f};
+    float nearv = -1e30f, farv = 1e30f;
+    V3 normal{0.0f, 0.0f, 0.0f};
+    const float mnx = __fmul_rn((float)A.mn[0], 16.0f), mny = __fmul_rn((float)A.mn[1], 16.0f), mnz = __fmul_rn((float)A.mn[2], 16.0f);
+    const float mxx = __fmul_rn((float)(A.mx[0] + 1), 16.0f), mxy = __fmul_rn((float)(A.mx[1] + 1), 16.0f),
+                mxz = __fmul_rn((float)(A.mx[2] + 1), 16.0f);
+#define VGI_SLAB(AX, O, D, MN, MX)                                              \
+    if (fabsf(D) <= 1e-8f) {                                                    \
+        if (O < MN || O > MX) { cnt.status(0); return res; }                    \
+    } else {                                                                    \
+        float first = __fdiv_rn(__fsub_rn(MN, O), D);                           \
+        float second = __fdiv_rn(__fsub_rn(MX, O), D);                          \
+        if (wmin(first, second) > nearv) {                                      \
+            nearv = wmin(first, second);                                        \
+            float s = first < second ? -1.0f : 1.0f;                            \
+            normal = V3{AX == 0 ? s : 0.0f, AX == 1 ? s : 0.0f, AX == 2 ? s : 0.0f}; \
+        }                                                                       \
+        farv = wmin(farv, wmax(first, second));                                 \
+    }
+    VGI_SLAB(0, origin.x, dir.x, mnx, mxx)
+    VGI_SLAB(1, origin.y, dir.y, mny, mxy)
+    VGI_SLAB(2, origin.z, dir.z, mnz, mxz)
+#undef VGI_SLAB
+    if (farv < wmax(nearv, 0.0f)) { cnt.status(0); return res; }
+    float distance = __fadd_rn(wmax(nearv, 0.0f), 0.001f);
+    V3 position = origin + dir * distance;
+    int lrx = 0x7fffffff, lry = 0x7fffffff, lrz = 0x7fffffff;
+    uint4 meta = make_uint4(0, 0, 0, 0);
+#pragma unroll 1
+    for (uint32_t step = 0; step < max_steps; ++step) {
+        cnt.step();
+        if (distance > max_distance) { cnt.status(0); return res; }
+        I3 voxel{f2i(floorf(position.x)), f2i(floorf(position.y)), f2i(floorf(position.z))};
+        int rx = voxel.x >> 4, ry = voxel.y >> 4, rz = voxel.z >> 4;
+        if (!in_bounds(A, rx, ry, rz)) { cnt.status(0); return res; }
+        if (lrx != rx || lry != ry || lrz != rz) {
+            uint32_t index = lookup_region(A, rx, ry, rz, cnt);
+            if (index == kNoIndex) {
+                if (visible_geometry) {
+                    float4 adv = advance_box(position, dir, I3{rx, ry, rz}, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f);
+                    distance = __fadd_rn(distance, adv.w);
+                    position = position + dir * adv.w;
+                    normal = V3{adv.x, adv.y, adv.z};
+                    continue;
+                }
+                res.status = geometry_ahead(A, position, dir, __fsub_rn(max_distance, distance), cnt) ? 2u : 0u;
+                cnt.status(res.status);
+                return res;
+            }
+            cnt.bytes(16);
+            meta = __ldg(A.headers + index);
+            lrx = rx; lry = ry; lrz = rz;
+        }
+        float4 adv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (meta.x == 1u) {
+            adv = advance_box(position, dir, I3{rx, ry, rz}, unpack_bytes(meta.z), unpack_bytes(meta.w), 16.0f);
+        } else {
+            uint32_t material = meta.y;
+            if (meta.x == 3u) {
+                uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
+                uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
+                uint32_t brick = __ldg(A.cells + meta.y + (bz * 4u + by) * 4u + bx);
+                cnt.bytes(4);
+                uint32_t state = brick & 3u;
+                if (state == 0u) {
+                    uint32_t ext = brick >> 2u;
+                    adv = advance_box(position, dir, I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz}, neg_ext(ext), pos_ext(ext), 4.0f);
+                    material = 256u;
+                } else if (state == 1u) {
+                    material = brick >> 2u;
+                } else {
+                    uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
+                    uint32_t word = __ldg(A.cells + (brick >> 2u) + (idx >> 1));
+                    cnt.bytes(4);
+                    uint32_t cell = (word >> ((idx & 1u) * 16u)) & 65535u;
+                    material = (cell & 1u) != 0u ? (cell >> 1u) : 256u;
+                    if (material == 256u) {
+                        uint32_t ext = cell >> 1u;
+                        adv = advance_box(position, dir, voxel, neg_ext(ext), pos_ext(ext), 1.0f);
+                    }
+                }
+            }
+            if (material != 256u) {
+                res.voxel = voxel;
+                res.material = material;
+                res.position = position;
+                res.normal = normal;
+                res.status = 1u;
+                cnt.status(1);
+                return res;
+            }
+        }
+        distance = __fadd_rn(distance, adv.w);
+        position = position + dir * adv.w;
+        normal = V3{adv.x, adv.y, adv.z};
+    }
+    res.status = 2u;
+    res.material = 0xffffffffu;
+    cnt.status(2);
+    return res;
+}
+
+// ---- estimator ---------------------------------------------------------------
+struct Emissive {
+    I3 voxel;
+    uint32_t face;
+    float4 sampling;
+};
+
+template <bool C>
+__device__ __forceinline__ Emissive load_emitter(const TraceArgs& A, uint32_t index, Cnt<C>& cnt) {
+    cnt.bytes(32);
+    uint4 a = __ldg(A.emitters + index * 2u);
+    uint4 b = __ldg(A.emitters + index * 2u + 1u);
+    return Emissive{I3{(int)a.x, (int)a.y, (int)a.z}, a.w,
+                    make_float4(__uint_as_float(b.x), __uint_as_float(b.y), __uint_as_float(b.z), __uint_as_float(b.w))};
+}
+
+struct Node {
+    float4 mp;       // minimum xyz, power
+    V3 mx;
+    uint32_t normals;
+    I3 pivot;
+    uint32_t face;
+    uint4 children;  // left, right, axis, 0
+};
+
+template <bool C>
+__device__ __forceinline__ Node load_node(const TraceArgs& A, uint32_t index, Cnt<C>& cnt) {
+    cnt.bytes(64);
+    uint32_t offset = f2u(A.emitter_count) * 2u + index * 4u;
+    uint4 w0 = __ldg(A.emitters + offset), w1 = __ldg(A.emitters + offset + 1u), w2 = __ldg(A.emitters + offset + 2u),
+          w3 = __ldg(A.emitters + offset + 3u);
+    Node n;
+    n.mp = make_float4(__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z), __uint_as_float(w0.w));
+    n.mx = V3{__uint_as_float(w1.x), __uint_as_float(w1.y), __uint_as_float(w1.z)};
+    n.normals = w1.w;
+    n.pivot = I3{(int)w2.x, (int)w2.y, (int)w2.z};
+    n.face = w2.w;
+    n.children = w3;
+    return n;
+}
+
+// voxel_path.wgsl:108-122
+__device__ float node_importance(const Node& node, V3 position, V3 normal) {
+    V3 mn{node.mp.x, node.mp.y, node.mp.z};
+    V3 delta = (mn + node.mx) * 0.5f - position;
+    float radius = __fmul_rn(len3(node.mx - mn), 0.5f);
+    float distance = wmax(len3(delta), 1e-5f);
+    V3 direction = delta / distance;
+    float spread = wmin(__fdiv_rn(radius, distance), 1.0f);
+    float receiver = wclamp(__fadd_rn(dot3(normal, direction), spread), 0.0f, 1.0f);
+    float px = (node.normals & 1u) ? -direction.x : -1.0f;
+    float py = (node.normals & 4u) ? -direction.y : -1.0f;
+    float pz = (node.normals & 16u) ? -direction.z : -1.0f;
+    float nx = (node.normals & 2u) ? direction.x : -1.0f;
+    float ny = (node.normals & 8u) ? direction.y : -1.0f;
+    float nz = (node.normals & 32u) ? direction.z : -1.0f;
+    float qx = wmax(px, nx), qy = wmax(py, ny), qz = wmax(pz, nz);
+    float emitter = wclamp(__fadd_rn(wmax(wmax(qx, qy), qz), spread), 0.0f, 1.0f);
+    float num = __fmul_rn(__fmul_rn(node.mp.w, receiver), emitter);
+    float den = __fadd_rn(__fadd_rn(__fmul_rn(distance, distance), __fmul_rn(radius, radius)), 0.25f);
+    return __fdiv_rn(num, den);
+}
+
+template <bool C>
+__device__ float node_left_probability(const TraceArgs& A, const Node& node, V3 position, V3 normal, Cnt<C>& cnt) {
+    Node left = load_node(A, node.children.x, cnt);
+    Node right = load_node(A, node.children.y, cnt);
+    float power = __fdiv_rn(left.mp.w, __fadd_rn(left.mp.w, right.mp.w));
+    float a = node_importance(left, position, normal);
+    float b = node_importance(right, position, normal);
+    if (__fadd_rn(a, b) <= 1e-20f) return wclamp(power, 1e-6f, 0.999999f);
+    return wclamp(__fadd_rn(__fmul_rn(0.05f, power), __fdiv_rn(__fmul_rn(0.95f, a), __fadd_rn(a, b))), 1e-6f, 0.999999f);
+}
+
+template <bool C>
+__device__ Emissive tree_emitter(const TraceArgs& A, V3 position, V3 normal, float choice, Cnt<C>& cnt) {
+    uint32_t index = 0;
+    float u = choice, probability = 1.0f;
+    // Median splits keep the hierarchy balanced (depth <= 33); the host
+    // checks that children follow their parent, so the walk ends. The bound
+    // only guards malformed words: a zero-probability emitter contributes 0.
+#pragma unroll 1
+    for (uint32_t depth = 0; depth < 64u; ++depth) {
+        Node node = load_node(A, index, cnt);
+        if (node.children.x == 0xffffffffu) {
+            Emissive e = load_emitter(A, node.children.y, cnt);
+            e.sampling.y = probability;
+            return e;
+        }
+        float p = node_left_probability(A, node, position, normal, cnt);
+        if (u < p) {
+            probability = __fmul_rn(probability, p);
+            u = __fdiv_rn(u, p);
+            index = node.children.x;
+        } else {
+            probability = __fmul_rn(probability, __fsub_rn(1.0f, p));
+            u = __fdiv_rn(__fsub_rn(u, p), __fsub_rn(1.0f, p));
+            index = node.children.y;
+        }
+        u = wmin(u, __uint_as_float(0x3f7fffffu));
+    }
+    return Emissive{I3{0, 0, 0}, 0u, make_float4(0.0f, 0.0f, 0.0f, 0.0f)};
+}
+
+__device__ __forceinline__ int comp(I3 v, uint32_t i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+
+__device__ __forceinline__ bool key_less(I3 voxel, uint32_t face, const Node& node) {
+    uint32_t axis = node.children.z;
+#pragma unroll
+    for (uint32_t j = 0; j < 3u; ++j) {
+        uint32_t i = (axis + j) % 3u;
+        int a = comp(voxel, i), b = comp(node.pivot, i);
+        if (a != b) return a < b;
+    }
+    return face < node.face;
+}
+
+template <bool C>
+__device__ float tree_probability(const TraceArgs& A, V3 position, V3 normal, I3 voxel, V3 hit_normal, Cnt<C>& cnt) {
+    uint32_t face = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < 6u; ++i) {
+        V3 fn = face_normal(i);
+        if (fn.x == hit_normal.x && fn.y == hit_normal.y && fn.z == hit_normal.z) face = i;
+    }
+    uint32_t index = 0;
+    float probability = 1.0f;
+#pragma unroll 1
+    for (uint32_t depth = 0; depth < 64u; ++depth) {
+        Node node = load_node(A, index, cnt);
+        if (node.children.x == 0xffffffffu) {
+            Emissive found = load_emitter(A, node.children.y, cnt);
+            bool same = found.voxel.x == voxel.x && found.voxel.y == voxel.y && found.voxel.z == voxel.z && found.face == face;
+            return same ? probability : 0.0f;
+        }
+        float p = node_left_probability(A, node, position, normal, cnt);
+        if (key_less(voxel, face, node)) {
+            probability = __fmul_rn(probability, p);
+            index = node.children.x;
+        } else {
+            probability = __fmul_rn(probability, __fsub_rn(1.0f, p));
+            index = node.children.y;
+        }
+    }
+    return 0.0f;
+}
+
+// voxel_path.wgsl:178-213 (the Owen scramble is sobol_burley's hash)
+__device__ __forceinline__ uint32_t scramble_reverse(uint32_t v, uint32_t seed) {
+    v ^= v * 0x3d20adeau;
+    v += seed;
+    v *= (seed >> 16u) | 1u;
+    v ^= v * 0x05526c56u;
+    v ^= v * 0x53a22864u;
+    return v;
+}
+
+__device__ float sample_1d(uint32_t stream, uint32_t sequence, uint32_t dimension) {
+    if (dimension < 12u) {
+        // primes 2..37
+        const uint32_t base = dimension < 6u ? (dimension < 3u ? (dimension == 0u ? 2u : (dimension == 1u ? 3u : 5u))
+                                                              : (dimension == 3u ? 7u : (dimension == 4u ? 11u : 13u)))
+                                            : (dimension < 9u ? (dimension == 6u ? 17u : (dimension == 7u ? 19u : 23u))
+                                                              : (dimension == 9u ? 29u : (dimension == 10u ? 31u : 37u)));
+        const float fbase = (float)base;
+        uint32_t index = (sequence & 0x00ffffffu) + 1u;
+        float scale = 1.0f, value = 0.0f;
+#pragma unroll 1
+        while (index != 0u) {
+            scale = __fdiv_rn(scale, fbase);
+            uint32_t q = index / base;
+            value = __fadd_rn(value, __fmul_rn((float)(index - q * base), scale));
+            index = q;
+        }
+        float rotation = __fdiv_rn((float)(pcg(stream ^ pcg(dimension)) >> 9u), 8388608.0f);
+        float t = __fadd_rn(value, rotation);
+        return __fsub_rn(t, floorf(t));
+    }
+    uint32_t seed = pcg(stream ^ pcg(dimension / 2u));
+    uint32_t index = __brev(scramble_reverse(__brev(sequence), pcg(seed ^ 0x79c68e4au)));
+    if ((dimension & 1u) != 0u) {
+        index ^= (index >> 1u) & 0x55555555u;
+        index ^= (index >> 2u) & 0x33333333u;
+        index ^= (index >> 4u) & 0x0f0f0f0fu;
+        index ^= (index >> 8u) & 0x00ff00ffu;
+        index ^= (index >> 16u) & 0x0000ffffu;
+    }
+    uint32_t value = __brev(scramble_reverse(index, pcg(seed ^ pcg(dimension))));
+    return __fdiv_rn((float)(value >> 9u), 8388608.0f);
+}
+
+__device__ __forceinline__ float continuation_sample(uint32_t stream, uint32_t sequence, uint32_t bounce, uint32_t dimension) {
+    if (bounce < 3u) {
+        uint32_t legacy = dimension == 2u ? 8u + bounce : 2u + bounce * 2u + dimension;
+        return sample_1d(stream, sequence, legacy);
+    }
+    return sample_1d(stream, sequence, 16u + (bounce - 3u) * 3u + dimension);
+}
+
+// voxel_path.wgsl:231-238
+__device__ V3 hemisphere(V3 n, float u, float v) {
+    V3 tangent = fabsf(n.z) < 0.999f ? normalize3(cross3(n, V3{0.0f, 0.0f, 1.0f})) : normalize3(cross3(n, V3{0.0f, 1.0f, 0.0f}));
+    V3 bitangent = cross3(n, tangent);
+    float phi = __fmul_rn(6.28318530718f, u);
+    float s, c;
+    own_sincos(phi, &s, &c);
+    float sv = __fsqrt_rn(v);
+    return (tangent * __fmul_rn(c, sv) + bitangent * __fmul_rn(s, sv)) + n * __fsqrt_rn(__fsub_rn(1.0f, v));
+}
+
+__device__ __forceinline__ float cosine_pdf(V3 n, V3 d) { return __fdiv_rn(wmax(dot3(n, d), 0.0f), 3.14159265359f); }
+
+template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
+struct Tracer {
+    const TraceArgs& A;
+    const float4* smat;   // shared material table, 2 float4 per material
+    Cnt<C>& cnt;
+
+    __device__ Mat material(uint32_t m) {
+        cnt.bytes(64);
+        // Material ids are below 256 for every geometry the host accepts.
+        m &= 255u;
+        float4 d = smat[m * 2u], e = smat[m * 2u + 1u];
+        return Mat{make_float4(d.x, d.y, d.z, 0.0f), make_float4(e.x, e.y, e.z, 0.0f), d.w};
+    }
+    __device__ float reach() const { return LIMITED ? A.reach : A.max_distance; }
+
+    // voxel_path.wgsl:239-243
+    __device__ Ray trace(V3 origin, V3 dir, float max_distance) {
+        Ray r = trace_domain(A, origin, dir, max_distance, BUDGETED, A.path_steps, cnt);
+        if (BUDGETED && r.status == 2u && r.material == 0xffffffffu) r.status = 0u;
+        return r;
+    }
+    // voxel_path.wgsl:271-282
+    __device__ Ray trace_diffuse(V3 origin, V3 dir) {
+        float r = reach();
+        Ray hit = trace(origin, dir, r);
+        if (LIMITED && hit.status == 0u && geometry_ahead(A, origin + dir * r, dir, __fsub_rn(A.max_distance, r), cnt)) hit.status = 3u;
+        return hit;
+    }
+    // voxel_path.wgsl:283-307 (value rgb; custom_visible only at the face centre)
+    template <bool CUSTOM>
+    __device__ void direct_at(V3 position, V3 normal, V3& value, V3& custom, float* value_w = nullptr) {
+        value = V3{0.0f, 0.0f, 0.0f};
+        custom = V3{0.0f, 0.0f, 0.0f};
+        float w = 0.0f;
+        V3 origin = position + normal * 0.002f;
+#pragma unroll 1
+        for (uint32_t i = 0; i < A.light_count; ++i) {
+            const float4 Lp = __ldg(A.lights + i * 3u), Le = __ldg(A.lights + i * 3u + 1u), Lx = __ldg(A.lights + i * 3u + 2u);
+            cnt.bytes(48);
+            V3 pos{Lp.x, Lp.y, Lp.z};
+            float distance = A.max_distance;
+            float attenuation = 1.0f;
+            V3 direction;
+            if (Lp.w >= 0.0f) {
+                V3 delta = pos - position;
+                float d2 = dot3(delta, delta);
+                if (d2 <= 0.0000001f || d2 > __fmul_rn(Lp.w, Lp.w)) continue;
+                distance = __fsqrt_rn(d2);
+                direction = delta / distance;
+                distance = __fsub_rn(distance, 0.004f);
+                attenuation = __fdiv_rn(1.0f, wmax(d2, 1.0f));
+            } else {
+                direction = normalize3(pos);
+            }
+            float cosine = wmax(dot3(normal, direction), 0.0f);
+            if (cosine > 0.0f && trace(origin, direction, distance).status == 0u) {
+                float k = __fmul_rn(cosine, attenuation);
+                value = value + V3{Le.x, Le.y, Le.z} * k;
+                if (CUSTOM) {
+                    custom = custom + V3{Lx.y, Lx.z, Lx.w} * k;
+                    w = __fadd_rn(w, __fmul_rn(Le.w, k));
+                }
+            }
+        }
+        if (CUSTOM && value_w) *value_w = w;
+    }
+    // voxel_path.wgsl:309-324
+    __device__ Emissive choose_emitter(V3 position, V3 normal, float choice) {
+        uint32_t count = f2u(A.emitter_count);
+        if (load_emitter(A, 0u, cnt).sampling.w > 0.0f) return tree_emitter(A, position, normal, choice, cnt);
+        uint32_t low = 0, high = count;
+#pragma unroll 1
+        while (low < high) {
+            uint32_t middle = (low + high) / 2u;
+            if (load_emitter(A, middle, cnt).sampling.x <= choice) low = middle + 1u;
+            else high = middle;
+        }
+        return load_emitter(A, low < count - 1u ? low : count - 1u, cnt);
+    }
+    // voxel_path.wgsl:332-364
+    __device__ V3 sample_emitter(V3 position, V3 normal, uint32_t source_stream, uint32_t sequence, uint32_t bounce) {
+        V3 zero{0.0f, 0.0f, 0.0f};
+        if (A.emitter_count == 0.0f) return zero;
+        uint32_t stream = source_stream ^ pcg(bounce + 0xa341316cu);
+        Emissive em = choose_emitter(position, normal, sample_1d(stream, sequence, 12u));
+        V3 en = face_normal(em.face);
+        uint32_t axis = em.face / 2u;
+        V3 tangent = axis == 0u ? V3{0.0f, 1.0f, 0.0f} : V3{1.0f, 0.0f, 0.0f};
+        V3 bitangent = axis == 2u ? V3{0.0f, 1.0f, 0.0f} : V3{0.0f, 0.0f, 1.0f};
+        float s13 = __fsub_rn(sample_1d(stream, sequence, 13u), 0.5f);
+        float s14 = __fsub_rn(sample_1d(stream, sequence, 14u), 0.5f);
+        V3 lp = ((add_s(itof(em.voxel), 0.5f) + en * 0.5f) + tangent * s13) + bitangent * s14;
+        V3 delta = lp - position;
+        float d2 = dot3(delta, delta);
+        float r = reach();
+        if (d2 < 0.0001f || d2 > __fmul_rn(r, r)) return zero;
+        float distance = __fsqrt_rn(d2);
+        V3 direction = delta / distance;
+        float rc = wmax(dot3(normal, direction), 0.0f);
+        float ec = wmax(dot3(en, -direction), 0.0f);
+        if (rc <= 0.0f || ec <= 0.0f || em.sampling.y <= 0.0f) return zero;
+        float light_pdf = __fdiv_rn(__fmul_rn(em.sampling.y, d2), ec);
+        float directional_pdf = __fdiv_rn(rc, 3.14159265359f);
+        V3 so = position + normal * 0.002f;
+        V3 sd = (lp + en * 0.002f) - so;
+        float sdist = len3(sd);
+        if (trace(so, sd / sdist, sdist).status != 0u) return zero;
+        Mat m = material(f2u(em.sampling.z));
+        float factor = __fdiv_rn(directional_pdf, __fadd_rn(light_pdf, directional_pdf));
+        return V3{m.emission.x, m.emission.y, m.emission.z} * factor;
+    }
+    // voxel_path.wgsl:368-394
+    __device__ V3 sample_terminal_emission(V3 position, V3 normal, uint32_t stream, uint32_t sequence, uint32_t bounce) {
+        V3 zero{0.0f, 0.0f, 0.0f};
+        if (A.emitter_count == 0.0f) return zero;
+        if (continuation_sample(stream, sequence, bounce, 2u) < 0.5f) return sample_emitter(position, normal, stream, sequence, bounce + 1u) * 2.0f;
+        V3 direction = hemisphere(normal, continuation_sample(stream, sequence, bounce, 0u), continuation_sample(stream, sequence, bounce, 1u));
+        if (dot3(normal, direction) <= 0.0f) return zero;
+        float r = reach();
+        Ray hit = trace(position + normal * 0.002f, direction, r);
+        if (hit.status != 1u) return zero;
+        Mat m = material(hit.material);
+        float power = m.weight;
+        V3 delta = hit.position - position;
+        float d2 = dot3(delta, delta);
+        if (power == 0.0f || d2 < 0.0001f || d2 > __fmul_rn(r, r)) return zero;
+        float selection_pdf = __fdiv_rn(power, wmax(A.emitter_total, 1e-20f));
+        if (load_emitter(A, 0u, cnt).sampling.w > 0.0f) selection_pdf = tree_probability(A, position, normal, hit.voxel, hit.normal, cnt);
+        float light_pdf = __fdiv_rn(__fmul_rn(selection_pdf, d2), wmax(dot3(hit.normal, -direction), 1e-8f));
+        float directional_pdf = cosine_pdf(normal, direction);
+        float factor = __fdiv_rn(__fmul_rn(2.0f, directional_pdf), __fadd_rn(directional_pdf, light_pdf));
+        return V3{m.emission.x, m.emission.y, m.emission.z} * factor;
+    }
+    // voxel_path.wgsl:66-87; the slot's record holds (mean rgb, count word).
+    __device__ bool cached_energy(I3 voxel, uint32_t face, V3& value) {
+        if (face > 5u || A.face_index == nullptr) return false;
+        uint4 header = __ldg(A.face_index);
+        uint32_t mask = header.x;
+        uint32_t slot = (hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(face + 1u)) & mask;
+#pragma unroll 1
+        for (uint32_t attempt = 0; attempt < header.y; ++attempt) {
+            uint4 e = __ldg(A.face_index + slot + 1u);
+            cnt.bytes(16);
+            if (e.w == 0xffffffffu) return false;
+            if ((int)e.x == voxel.x && (int)e.y == voxel.y && (int)e.z == voxel.z && (e.w >> 29u) == face) {
+                float4 rec = __ldg(A.cache + (e.w & 0x1fffffffu));
+                cnt.bytes(16);
+                uint32_t count = __float_as_uint(rec.w);
+                if (count < 16u || (count & 0x80000000u) != 0u) return false;
+                value = V3{rec.x, rec.y, rec.z};
+                return true;
+            }
+            slot = (slot + 1u) & mask;
+        }
+        return false;
+    }
+    // voxel_path.wgsl:418-496: begin_path + advance_path with DIFFUSE_HITS steps
+    // and the terminal mixture; returns the continuation's energy.
+    __device__ V3 trace_path(V3 start, V3 direction, V3 normal, uint32_t stream, uint32_t sequence, bool& unknown) {
+        V3 energy{0.0f, 0.0f, 0.0f};
+        V3 tp{1.0f, 1.0f, 1.0f};
+        V3 origin = start;
+        float previous_pdf = cosine_pdf(normal, direction);
+        V3 previous_position = start - normal * 0.001f;
+        V3 previous_normal = normal;
+        if (previous_pdf <= 0.0f) return energy;
+#pragma unroll 1
+        for (uint32_t step = 0; step < HITS; ++step) {
+            uint32_t bounce = step;
+            Ray hit = trace_diffuse(origin, direction);
+            if (hit.status == 0u) {
+                float horizon = wclamp(__fadd_rn(__fmul_rn(direction.y, 0.35f), 0.65f), 0.15f, 1.0f);
+                energy = energy + (tp * V3{A.env[0], A.env[1], A.env[2]}) * horizon;
+                break;
+            }
+            if (hit.status == 2u) { unknown = true; break; }
+            if (hit.status == 3u) break;
+            Mat m = material(hit.material);
+            V3 direct, unused;
+            direct_at<false>(hit.position, hit.normal, direct, unused);
+            float emission_weight = m.weight;
+            V3 delta = hit.position - origin;
+            float selection_pdf = __fdiv_rn(emission_weight, wmax(A.emitter_total, 1e-20f));
+            if (emission_weight > 0.0f && A.emitter_count > 0.0f && load_emitter(A, 0u, cnt).sampling.w > 0.0f)
+                selection_pdf = tree_probability(A, previous_position, previous_normal, hit.voxel, hit.normal, cnt);
+            float light_pdf = __fdiv_rn(__fmul_rn(selection_pdf, dot3(delta, delta)), wmax(dot3(hit.normal, -direction), 1e-8f));
+            float mis = 1.0f;
+            if (light_pdf > 0.0f) mis = __fdiv_rn(previous_pdf, __fadd_rn(previous_pdf, light_pdf));
+            V3 emission{m.emission.x, m.emission.y, m.emission.z};
+            V3 diffuse{m.diffuse.x, m.diffuse.y, m.diffuse.z};
+            V3 cached;
+            if (cached_energy(hit.voxel, face_index_of(hit.normal), cached)) {
+                cnt.cache_hit();
+                energy = energy + tp * (emission * mis + diffuse * (direct + cached));
+                break;
+            }
+            bool last = step + 1u == HITS;
+            V3 nee = last ? sample_terminal_emission(hit.position, hit.normal, stream, sequence, bounce)
+                          : sample_emitter(hit.position, hit.normal, stream, sequence, bounce + 1u);
+            energy = energy + tp * (emission * mis + diffuse * (direct + nee));
+            if (last) break;
+            tp = tp * diffuse;
+            float maximum = wmax(tp.x, wmax(tp.y, tp.z));
+            if (maximum == 0.0f) break;
+            if (bounce >= 1u) {
+                float survival = wclamp(maximum, 0.1f, 0.95f);
+                if (continuation_sample(stream, sequence, bounce, 2u) > survival) break;
+                tp = tp / survival;
+            }
+            origin = hit.position + hit.normal * 0.002f;
+            previous_position = hit.position;
+            previous_normal = hit.normal;
+            direction = hemisphere(hit.normal, continuation_sample(stream, sequence, bounce, 0u), continuation_sample(stream, sequence, bounce, 1u));
+            previous_pdf = cosine_pdf(hit.normal, direction);
+            if (previous_pdf <= 0.0f) break;
+        }
+        return energy;
+    }
+};
+
+template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
+__global__ void __launch_bounds__(kBlock) trace_faces_kernel(const TraceArgs A) {
+    __shared__ float4 smat[512];
+    for (int i = threadIdx.x; i < 256; i += kBlock) {
+        float4 d = __ldg(A.materials + i * 4), e = __ldg(A.materials + i * 4 + 2), x = __ldg(A.materials + i * 4 + 3);
+        smat[i * 2] = make_float4(d.x, d.y, d.z, x.y);
+        smat[i * 2 + 1] = make_float4(e.x, e.y, e.z, 0.0f);
+    }
+    __syncthreads();
+    Cnt<C> cnt;
+    Tracer<HITS, LIMITED, BUDGETED, C> T{A, smat, cnt};
+    const uint32_t lanes = 1u << A.lanes_log2;
+    const uint32_t gid = blockIdx.x * kBlock + threadIdx.x;
+    const uint32_t face = gid >> A.lanes_log2;
+    const uint32_t lane = gid & (lanes - 1u);
+    uint4 t0 = make_uint4(0, 0, 0, 0xffffffffu), t1 = make_uint4(0, 0, 0, 0);
+    if (face < A.n_tasks) {
+        t0 = __ldg(A.tasks + face * 2u);
+        t1 = __ldg(A.tasks + face * 2u + 1u);
+    }
+    const bool valid = face < A.n_tasks && t0.w != 0xffffffffu;
+    V3 mean{0.0f, 0.0f, 0.0f}, second{0.0f, 0.0f, 0.0f};
+    uint32_t known = 0;
+    V3 normal = face_normal(valid ? t0.w : 0u);
+    I3 voxel{(int)t0.x, (int)t0.y, (int)t0.z};
+    V3 surface = add_s(itof(voxel), 0.5f) + normal * 0.5f;
+    if (valid) {
+        if (lane == 0) cnt.bytes(32 + 96);
+        const uint32_t stream = hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(t0.w + 1u);
+#pragma unroll 1
+        for (uint32_t i = lane; i < A.samples; i += lanes) {
+            const uint32_t sequence = t1.x + i;
+            cnt.path();
+            // voxel_path.wgsl:504-520 (sample_receiver_path + trace_receiver)
+            V3 direction = hemisphere(normal, sample_1d(stream, sequence, 0u), sample_1d(stream, sequence, 1u));
+            V3 value = T.sample_emitter(surface, normal, stream, sequence, 0u);
+            bool unknown = false;
+            if (dot3(normal, direction) > 0.0f) {
+                V3 cont = T.trace_path(surface + normal * 0.001f, direction, normal, stream, sequence, unknown);
+                value = value + cont;
+            }
+            if (unknown) { cnt.unknown(); continue; }
+            mean = mean + value;
+            second = second + value * value;
+            known += 1u;
+        }
+    }
+    // Lane 0 sums lanes 0..L-1 in order (trace_faces_parallel's reduction);
+    // with one lane this is the serial kernel's 0 + sum.
+    V3 tm{0.0f, 0.0f, 0.0f}, ts{0.0f, 0.0f, 0.0f};
+    uint32_t tk = 0;
+    {
+        const uint32_t base = (threadIdx.x & 31u) & ~(lanes - 1u);
+        for (uint32_t i = 0; i < lanes; ++i) {
+            float mx = __shfl_sync(0xffffffffu, mean.x, base + i), my = __shfl_sync(0xffffffffu, mean.y, base + i),
+                  mz = __shfl_sync(0xffffffffu, mean.z, base + i);
+            float sx = __shfl_sync(0xffffffffu, second.x, base + i), sy = __shfl_sync(0xffffffffu, second.y, base + i),
+                  sz = __shfl_sync(0xffffffffu, second.z, base + i);
+            uint32_t k = __shfl_sync(0xffffffffu, known, base + i);
+            tm = tm + V3{mx, my, mz};
+            ts = ts + V3{sx, sy, sz};
+            tk += k;
+        }
+    }
+    if (valid && lane == 0) {
+        // write_result (voxel_trace.wgsl:25-37)
+        V3 dv, dc;
+        float dw = 0.0f;
+        T.template direct_at<true>(surface, normal, dv, dc, &dw);
+        float inverse = __fdiv_rn(1.0f, (float)(tk > 1u ? tk : 1u));
+        V3 m = tm * inverse, s = ts * inverse;
+        uint4* out = A.results + (size_t)face * 6u;
+        out[0] = make_uint4(__float_as_uint(m.x), __float_as_uint(m.y), __float_as_uint(m.z), 0u);
+        out[1] = make_uint4(0u, __float_as_uint((float)tk), 0u, 0u);
+        out[2] = make_uint4(__float_as_uint(s.x), __float_as_uint(s.y), __float_as_uint(s.z), 0u);
+        out[3] = make_uint4(0u, 0u, 0u, 0u);
+        out[4] = make_uint4(__float_as_uint(dv.x), __float_as_uint(dv.y), __float_as_uint(dv.z), __float_as_uint(dw));
+        out[5] = make_uint4(0u, __float_as_uint(dc.x), __float_as_uint(dc.y), __float_as_uint(dc.z));
+    }
+    if constexpr (C) {
+        // Warp-aggregate the counters, one atomic per counter per warp.
+        unsigned long long v[10];
+        const Cnt<true>& c = cnt;
+        v[0] = c.rays; v[1] = c.paths; v[2] = c.steps; v[3] = c.b; v[4] = c.unk; v[5] = c.hits;
+        v[6] = c.st[0]; v[7] = c.st[1]; v[8] = c.st[2]; v[9] = c.st[3];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+            unsigned long long x = v[k];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if ((threadIdx.x & 31u) == 0u && x) atomicAdd(A.counters + k, x);
+        }
+    }
+}
+
+template <uint32_t H, bool L, bool B>
+void launch_variant(const TraceArgs& a, bool count, cudaStream_t s) {
+    uint64_t threads = (uint64_t)a.n_tasks << a.lanes_log2;
+    uint32_t blocks = (uint32_t)((threads + kBlock - 1) / kBlock);
+    if (blocks == 0) return;
+    if (count) trace_faces_kernel<H, L, B, true><<<blocks, kBlock, 0, s>>>(a);
+    else trace_faces_kernel<H, L, B, false><<<blocks, kBlock, 0, s>>>(a);
+}
+
+template <uint32_t H>
+void launch_hits(const TraceArgs& a, bool limited, bool budgeted, bool count, cudaStream_t s) {
+    if (limited) {
+        if (budgeted) launch_variant<H, true, true>(a, count, s);
+        else launch_variant<H, true, false>(a, count, s);
+    } else {
+        if (budgeted) launch_variant<H, false, true>(a, count, s);
+        else launch_variant<H, false, false>(a, count, s);
+    }
+}
+
+}  // namespace
+
+void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t s) {
+    if (hits <= 1) launch_hits<1>(a, limited, budgeted, count, s);
+    else if (hits == 2) launch_hits<2>(a, limited, budgeted, count, s);
+    else launch_hits<3>(a, limited, budgeted, count, s);
+}
+
+}  // namespace vgi

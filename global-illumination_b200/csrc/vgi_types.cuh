@@ -1,0 +1,59 @@
+// Launch records shared by the host API and the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vgi {
+
+constexpr uint32_t kNoIndex = 0xffffffffu;
+
+// Everything the face trace reads. Geometry and cache arrays are read-only
+// for the kernel's lifetime and are loaded through the non-coherent path.
+struct TraceArgs {
+    // NAADF geometry (binding 1-3 of the reference's layout)
+    const int4* directory;
+    const uint4* headers;
+    const uint32_t* cells;
+    uint32_t dir_mask;
+    int mn[3], mx[3];
+    // model
+    const float4* materials;   // 4 float4 per material (GpuMaterial)
+    const uint4* emitters;     // GpuEmitter records then light-tree nodes
+    float emitter_count;       // params.extra.w
+    float emitter_total;       // params.extra.z
+    float max_distance;        // params.extra.y (768)
+    float reach;               // params.transport.x
+    float env[4];
+    uint32_t light_count;      // counts.w
+    const float4* lights;      // 3 float4 per light (GpuLight)
+    // world cache
+    const uint4* face_index;   // [0] = (mask, probes, 0, 0), entries from 1
+    const float4* cache;       // per slot: mean rgb, count word (bits)
+    // faces
+    const uint4* tasks;        // 2 uint4 per task (FaceTask)
+    uint4* results;            // 6 uint4 per task (FaceResult)
+    uint32_t n_tasks;
+    uint32_t samples;          // counts.y
+    uint32_t path_steps;       // PATH_STEPS
+    uint32_t lanes_log2;       // threads per face = 1 << lanes_log2
+    unsigned long long* counters;  // 10 counters (counting variant only)
+};
+
+struct AccumArgs {
+    uint4* state;         // 9 uint4 per slot
+    uint4* slot_meta;     // 3 uint4 per slot
+    uint4* checkpoint;    // 3 uint4 per slot
+    uint4* outputs;       // 6 uint4 per task
+    uint4* tasks;         // 2 uint4 per task
+    float4* cache;        // per slot gather record
+    const uint32_t* slots;  // task -> slot (null: identity)
+    uint32_t n;
+    uint32_t controls[36];
+};
+
+void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
+void launch_prepare(const AccumArgs& a, cudaStream_t stream);
+void launch_accumulate(const AccumArgs& a, cudaStream_t stream);
+void launch_apply_events(const AccumArgs& a, const uint4* events, uint32_t n_slots, cudaStream_t stream);
+
+}  // namespace vgi

@@ -1,0 +1,528 @@
+"""Python binding of libvgi (include/vgi.h) for tests, benchmarks and tools.
+
+The host-side names mirror bevy_voxel_gi's interface for this path
+(crates/bevy_voxel_gi/src/): ``MaterialTransport`` / ``VoxelGiMaterials``
+(world.rs:59-175), ``TransportSettings`` (settings.rs:393-428),
+``DirectionalTransportLight`` (sources.rs:38-45) and ``GpuTracer``
+(gpu.rs:309-1240), whose methods map one-to-one onto the C ABI. Every call
+goes through the CUDA library; there is no CPU fallback, and loading fails
+loudly when libvgi.so has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(os.path.dirname(_HERE), "libvgi.so")
+
+OK = 0
+UNAVAILABLE = 1
+ERR_INVALID = -1
+ERR_CUDA = -2
+ERR_STATE = -3
+ERR_CAPACITY = -4
+
+AIR = 256
+FACE_OFFSETS = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
+
+
+class VgiError(RuntimeError):
+    """A libvgi call returned a failure status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"libvgi status {status}: {message}")
+        self.status = status
+
+
+class TransportUnavailable(VgiError):
+    """No usable CUDA device: the reference idles transport in this case
+    (src/lib.rs:355-357); it never falls back to the CPU."""
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [
+        ("rays", ctypes.c_uint64),
+        ("paths", ctypes.c_uint64),
+        ("steps", ctypes.c_uint64),
+        ("bytes", ctypes.c_uint64),
+        ("unknown", ctypes.c_uint64),
+        ("cache_hits", ctypes.c_uint64),
+        ("status", ctypes.c_uint64 * 4),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "status"}
+        d["status"] = [int(v) for v in self.status]
+        return d
+
+
+class _Transport(ctypes.Structure):
+    _fields_ = [
+        ("reach", ctypes.c_float),
+        ("bounces", ctypes.c_uint32),
+        ("path_steps", ctypes.c_uint32),
+        ("budgeted", ctypes.c_uint32),
+        ("history_limit", ctypes.c_uint32),
+        ("recency", ctypes.c_float),
+        ("measured_retention", ctypes.c_float),
+        ("response_seconds", ctypes.c_float),
+        ("lanes", ctypes.c_uint32),
+        ("transport_revision", ctypes.c_uint32),
+        ("stable_error", ctypes.c_float),
+        ("stable_samples", ctypes.c_uint32),
+    ]
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("flags", ctypes.c_uint32)]
+
+
+class TerrainParams(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint32),
+        ("octaves", ctypes.c_uint32),
+        ("period", ctypes.c_float),
+        ("base_height", ctypes.c_float),
+        ("falloff", ctypes.c_float),
+        ("emitters", ctypes.c_uint32),
+    ]
+
+
+class FaceFilter(ctypes.Structure):
+    _fields_ = [
+        ("use_frustum", ctypes.c_uint32),
+        ("eye", ctypes.c_float * 3),
+        ("forward", ctypes.c_float * 3),
+        ("tan_half", ctypes.c_float),
+        ("use_box", ctypes.c_uint32),
+        ("box_min", ctypes.c_int32 * 3),
+        ("box_max", ctypes.c_int32 * 3),
+        ("use_facing", ctypes.c_uint32),
+    ]
+
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+_I64 = ctypes.c_int64
+_INT = ctypes.c_int
+_F = ctypes.c_float
+
+_SIGNATURES = {
+    "vgi_create": (_INT, [_P, _P]),
+    "vgi_destroy": (_INT, [_P]),
+    "vgi_last_error": (ctypes.c_char_p, [_P]),
+    "vgi_stream": (_INT, [_P, _P]),
+    "vgi_sync": (_INT, [_P]),
+    "vgi_upload_regions": (_INT, [_P, _P, _U32, _P, _P]),
+    "vgi_upload_packed": (_INT, [_P, _P, _U64, _P, _U32, _P, _U64, _P]),
+    "vgi_edit_voxels": (_INT, [_P, _P, _U32]),
+    "vgi_geometry_info": (_INT, [_P, _P, _P]),
+    "vgi_read_geometry": (_INT, [_P, _P, _P, _P]),
+    "vgi_set_materials": (_INT, [_P, _P]),
+    "vgi_set_lights": (_INT, [_P, _P, _U32, _U32]),
+    "vgi_set_environment": (_INT, [_P, _P]),
+    "vgi_set_emitters": (_INT, [_P, _P, _U64, _U32, _F]),
+    "vgi_build_emitters": (_INT, [_P]),
+    "vgi_set_transport": (_INT, [_P, _P]),
+    "vgi_set_faces": (_INT, [_P, _P, _U32]),
+    "vgi_frame": (_INT, [_P, _U32, _U32]),
+    "vgi_set_timing": (_INT, [_P, _INT]),
+    "vgi_frame_times": (_INT, [_P, _P]),
+    "vgi_trace_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P]),
+    "vgi_census": (_INT, [_P, _U32, _P]),
+    "vgi_trace_tasks": (_INT, [_P, _P, _U32, _U32, _P, _P]),
+    "vgi_apply_events": (_INT, [_P, _P, _U32, _U64]),
+    "vgi_read_results": (_INT, [_P, _U32, _U32, _P]),
+    "vgi_read_state": (_INT, [_P, _U32, _U32, _P]),
+    "vgi_write_state": (_INT, [_P, _U32, _U32, _P]),
+    "vgi_read_slot_meta": (_INT, [_P, _U32, _U32, _P]),
+    "vgi_material_record": (None, [_P, _P, _P]),
+    "vgi_directional_light_record": (None, [_P, _P, _P, _P]),
+    "vgi_host_emitters": (_I64, [_P, _U32, _P, _P, _P, _U64, _P]),
+    "vgi_host_face_index": (_I64, [_P, _U32, _P, _U64]),
+    "vgi_host_top_level": (_INT, [_P, _P, _U32, _P, _U64]),
+    "vgi_scene_grid_coords": (_U32, [_U32, _U32, _U32, _P]),
+    "vgi_scene_stone_room": (None, [_P]),
+    "vgi_scene_furnace": (None, [_P]),
+    "vgi_scene_terrain": (None, [_P, _U32, _U32, _U32, _P]),
+    "vgi_scene_faces": (_U64, [_P, _U32, _P, _P, _P, _U64]),
+}
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """Loads libvgi.so (built in-tree by ``make -C global-illumination_b200``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY_PATH):
+            raise FileNotFoundError(f"{LIBRARY_PATH} is missing: build it with make -C {os.path.dirname(LIBRARY_PATH)}")
+        lib = ctypes.CDLL(LIBRARY_PATH)
+        for name, (restype, argtypes) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays passed to libvgi must be contiguous"
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c(a, dtype) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype))
+
+
+# ---- host-side mirror of the reference's model types --------------------------
+
+@dataclasses.dataclass
+class MaterialTransport:
+    """A transport material's optics (src/world.rs:59-79)."""
+
+    diffuse: Sequence[float] = (0.45, 0.45, 0.45)
+    emission: Sequence[float] = (0.0, 0.0, 0.0)
+
+
+class VoxelGiMaterials:
+    """The 256 transport materials (src/world.rs:90-175); unassigned ones keep
+    the default optics. ``words()`` is the GpuMaterial table the GPU reads."""
+
+    def __init__(self):
+        self.entries = [MaterialTransport() for _ in range(256)]
+        self.assigned = [False] * 256
+
+    def set(self, material: int, transport: MaterialTransport) -> None:
+        self.entries[material] = transport
+        self.assigned[material] = True
+
+    def get(self, material: int) -> MaterialTransport:
+        return self.entries[material]
+
+    def insert(self, transport: MaterialTransport) -> int:
+        for m in range(256):
+            if self.assigned[m] and self.words_of(self.entries[m]).tobytes() == self.words_of(transport).tobytes():
+                return m
+        for m in range(256):
+            if not self.assigned[m]:
+                self.set(m, transport)
+                return m
+        raise ValueError("MaterialsFull: all 256 materials are assigned")
+
+    @staticmethod
+    def words_of(t: MaterialTransport) -> np.ndarray:
+        out = np.zeros(16, np.float32)
+        library().vgi_material_record(_ptr(_c(t.diffuse, np.float32)), _ptr(_c(t.emission, np.float32)), _ptr(out))
+        return out
+
+    def words(self) -> np.ndarray:
+        return np.concatenate([self.words_of(e) for e in self.entries]).astype(np.float32)
+
+
+@dataclasses.dataclass
+class DirectionalTransportLight:
+    """A directional source (src/sources.rs:38-45): direction towards the light."""
+
+    direction: Sequence[float]
+    radiance: Sequence[float]
+    custom_visible: Sequence[float] = (0.0, 0.0, 0.0)
+
+    def words(self) -> np.ndarray:
+        out = np.zeros(12, np.float32)
+        library().vgi_directional_light_record(_ptr(_c(self.direction, np.float32)), _ptr(_c(self.radiance, np.float32)),
+                                               _ptr(_c(self.custom_visible, np.float32)), _ptr(out))
+        return out
+
+
+@dataclasses.dataclass
+class TransportSettings:
+    """TransportSettings (src/settings.rs:393-428) plus the accumulation
+    fields of TraceWork (src/work.rs:11-47) and the shader overrides."""
+
+    reach: float = 768.0
+    bounces: int = 3
+    path_steps: int = 2048
+    budgeted: bool = False
+    history_limit: int = 0
+    recency: float = 1.0
+    measured_retention: float = 1.0
+    response_seconds: float = 0.075
+    lanes: int = 0
+    transport_revision: int = 0
+    stable_error: float = 0.12
+    stable_samples: int = 32
+
+    def _c(self) -> _Transport:
+        return _Transport(self.reach, self.bounces, self.path_steps, int(self.budgeted), self.history_limit, self.recency,
+                          self.measured_retention, self.response_seconds, self.lanes, self.transport_revision,
+                          self.stable_error, self.stable_samples)
+
+
+class GpuTracer:
+    """One libvgi context: the B200 counterpart of the reference's GpuTracer."""
+
+    def __init__(self, device: int = 0):
+        lib = library()
+        handle = ctypes.c_void_p()
+        cfg = _Config(device, 0)
+        rc = lib.vgi_create(ctypes.byref(cfg), ctypes.byref(handle))
+        if rc == UNAVAILABLE:
+            raise TransportUnavailable(rc, "no CUDA device")
+        if rc != OK:
+            raise VgiError(rc, "vgi_create failed")
+        self._h = handle
+        self._lib = lib
+        self.n_slots = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.vgi_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        if rc != OK:
+            raise VgiError(rc, self._lib.vgi_last_error(self._h).decode())
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self._lib.vgi_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def sync(self) -> None:
+        self._check(self._lib.vgi_sync(self._h))
+
+    # geometry
+    def upload_regions(self, coords: np.ndarray, voxels: np.ndarray, strides: Optional[np.ndarray] = None) -> None:
+        coords = _c(coords, np.int32).reshape(-1, 3)
+        voxels = _c(voxels, np.uint16).reshape(-1)
+        assert voxels.size == coords.shape[0] * 4096
+        st = None if strides is None else _c(strides, np.uint8)
+        self._check(self._lib.vgi_upload_regions(self._h, _ptr(coords), coords.shape[0], _ptr(voxels), _ptr(st)))
+
+    def upload_packed(self, directory, headers, cells, bounds) -> None:
+        d = _c(directory, np.int32).reshape(-1)
+        h = _c(headers, np.uint32).reshape(-1)
+        c = _c(cells, np.uint32).reshape(-1)
+        b = _c(bounds, np.int32).reshape(-1)
+        self._check(self._lib.vgi_upload_packed(self._h, _ptr(d), d.size // 4, _ptr(h), h.size // 4, _ptr(c), c.size, _ptr(b)))
+
+    def edit_voxels(self, edits: np.ndarray) -> None:
+        e = _c(edits, np.int32).reshape(-1, 4)
+        self._check(self._lib.vgi_edit_voxels(self._h, _ptr(e), e.shape[0]))
+
+    def geometry(self):
+        sizes = np.zeros(3, np.uint64)
+        bounds = np.zeros(6, np.int32)
+        self._check(self._lib.vgi_geometry_info(self._h, _ptr(sizes), _ptr(bounds)))
+        d = np.zeros(int(sizes[0]) * 4, np.int32)
+        h = np.zeros(int(sizes[1]) * 4, np.uint32)
+        c = np.zeros(max(int(sizes[2]), 1), np.uint32)
+        self._check(self._lib.vgi_read_geometry(self._h, _ptr(d), _ptr(h), _ptr(c)))
+        return d, h, c[: int(sizes[2])], bounds
+
+    # model
+    def set_materials(self, words: np.ndarray) -> None:
+        w = _c(words, np.float32).reshape(-1)
+        assert w.size == 256 * 16
+        self._check(self._lib.vgi_set_materials(self._h, _ptr(w)))
+
+    def set_lights(self, words: np.ndarray, n_directional: int) -> None:
+        w = _c(words, np.float32).reshape(-1)
+        self._check(self._lib.vgi_set_lights(self._h, _ptr(w), w.size // 12, n_directional))
+
+    def set_environment(self, rgb) -> None:
+        self._check(self._lib.vgi_set_environment(self._h, _ptr(_c(rgb, np.float32))))
+
+    def set_emitters(self, words: np.ndarray, n_faces: int, total_weight: float) -> None:
+        w = _c(words, np.uint32).reshape(-1)
+        self._check(self._lib.vgi_set_emitters(self._h, _ptr(w), w.size, n_faces, total_weight))
+
+    def build_emitters(self) -> None:
+        self._check(self._lib.vgi_build_emitters(self._h))
+
+    def set_transport(self, t: TransportSettings) -> None:
+        tc = t._c()
+        self._check(self._lib.vgi_set_transport(self._h, ctypes.byref(tc)))
+
+    # face cache
+    def set_faces(self, faces: np.ndarray) -> None:
+        f = _c(faces, np.int32).reshape(-1, 5)
+        self._check(self._lib.vgi_set_faces(self._h, _ptr(f), f.shape[0]))
+        self.n_slots = f.shape[0]
+
+    def frame(self, samples: int, clock_ms: int = 0) -> None:
+        self._check(self._lib.vgi_frame(self._h, samples, clock_ms))
+
+    def set_timing(self, enable: bool) -> None:
+        self._check(self._lib.vgi_set_timing(self._h, int(enable)))
+
+    def frame_times(self) -> np.ndarray:
+        """Device ms of the last frame's prepare, trace and accumulate."""
+        out = np.zeros(3, np.float32)
+        self._check(self._lib.vgi_frame_times(self._h, _ptr(out)))
+        return out
+
+    def trace_batch(self, tasks: np.ndarray, samples: int, clock_ms: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        t = _c(tasks, np.uint32).reshape(-1, 8)
+        if out is None:
+            out = np.zeros((t.shape[0], 24), np.uint32)
+        self._check(self._lib.vgi_trace_batch(self._h, _ptr(t), t.shape[0], samples, clock_ms, _ptr(out)))
+        return out
+
+    def census(self, samples: int) -> dict:
+        c = Counters()
+        self._check(self._lib.vgi_census(self._h, samples, ctypes.byref(c)))
+        return c.as_dict()
+
+    def trace_tasks(self, tasks: np.ndarray, samples: int, count: bool = False):
+        t = _c(tasks, np.uint32).reshape(-1, 8)
+        out = np.zeros((t.shape[0], 24), np.uint32)
+        c = Counters()
+        self._check(self._lib.vgi_trace_tasks(self._h, _ptr(t), t.shape[0], samples, _ptr(out), ctypes.byref(c) if count else None))
+        return (out, c.as_dict()) if count else out
+
+    def apply_events(self, words: np.ndarray, n_events: int) -> None:
+        w = _c(words, np.uint32).reshape(-1)
+        self._check(self._lib.vgi_apply_events(self._h, _ptr(w), n_events, w.size))
+
+    def read_results(self, first: int = 0, n: Optional[int] = None) -> np.ndarray:
+        n = self.n_slots - first if n is None else n
+        out = np.zeros((n, 24), np.uint32)
+        self._check(self._lib.vgi_read_results(self._h, first, n, _ptr(out)))
+        return out
+
+    def read_state(self, first: int = 0, n: Optional[int] = None) -> np.ndarray:
+        n = self.n_slots - first if n is None else n
+        out = np.zeros((n, 36), np.uint32)
+        self._check(self._lib.vgi_read_state(self._h, first, n, _ptr(out)))
+        return out
+
+    def write_state(self, words: np.ndarray, first: int = 0) -> None:
+        w = _c(words, np.uint32).reshape(-1, 36)
+        self._check(self._lib.vgi_write_state(self._h, first, w.shape[0], _ptr(w)))
+
+    def read_slot_meta(self, first: int = 0, n: Optional[int] = None) -> np.ndarray:
+        n = self.n_slots - first if n is None else n
+        out = np.zeros((n, 12), np.uint32)
+        self._check(self._lib.vgi_read_slot_meta(self._h, first, n, _ptr(out)))
+        return out
+
+
+# ---- synthetic workloads and host-runtime helpers ----------------------------
+
+def grid_coords(nx: int, ny: int, nz: int) -> np.ndarray:
+    out = np.zeros((nx * ny * nz, 3), np.int32)
+    library().vgi_scene_grid_coords(nx, ny, nz, _ptr(out))
+    return out
+
+
+def stone_room():
+    vox = np.zeros(8 * 4096, np.uint16)
+    library().vgi_scene_stone_room(_ptr(vox))
+    return grid_coords(2, 2, 2), vox
+
+
+def furnace():
+    vox = np.zeros(8 * 4096, np.uint16)
+    library().vgi_scene_furnace(_ptr(vox))
+    return grid_coords(2, 2, 2), vox
+
+
+def terrain(nx: int, ny: int, nz: int, seed: int = 2, octaves: int = 4, period: float = 64.0, base_height: float = 96.0,
+            falloff: float = 48.0, emitters: int = 256):
+    p = TerrainParams(seed, octaves, period, base_height, falloff, emitters)
+    vox = np.zeros(nx * ny * nz * 4096, np.uint16)
+    library().vgi_scene_terrain(ctypes.byref(p), nx, ny, nz, _ptr(vox))
+    return grid_coords(nx, ny, nz), vox
+
+
+def exposed_faces(coords, voxels, frustum=None, box=None, facing=None) -> np.ndarray:
+    """Exposed faces as (voxel xyz, face, material) rows. ``frustum`` =
+    (eye, forward, tan_half); ``box`` = (min xyz, max xyz) on the air cell;
+    ``facing`` = an eye position: faces turned towards it (a cube-map camera)."""
+    coords = _c(coords, np.int32).reshape(-1, 3)
+    voxels = _c(voxels, np.uint16).reshape(-1)
+    flt = FaceFilter()
+    if facing is not None:
+        flt.use_facing = 1
+        flt.eye[:] = list(map(float, facing))
+    if frustum is not None:
+        eye, fwd, tan_half = frustum
+        fwd = np.asarray(fwd, np.float64)
+        fwd = fwd / np.linalg.norm(fwd)
+        flt.use_frustum = 1
+        flt.eye[:] = list(map(float, eye))
+        flt.forward[:] = list(map(float, fwd))
+        flt.tan_half = tan_half
+    if box is not None:
+        flt.use_box = 1
+        flt.box_min[:] = list(map(int, box[0]))
+        flt.box_max[:] = list(map(int, box[1]))
+    lib = library()
+    n = lib.vgi_scene_faces(_ptr(coords), coords.shape[0], _ptr(voxels), ctypes.byref(flt), None, 0)
+    out = np.zeros((max(n, 1), 5), np.int32)
+    lib.vgi_scene_faces(_ptr(coords), coords.shape[0], _ptr(voxels), ctypes.byref(flt), _ptr(out), n)
+    return out[:n]
+
+
+def host_emitters(coords, voxels, material_words):
+    coords = _c(coords, np.int32).reshape(-1, 3)
+    voxels = _c(voxels, np.uint16).reshape(-1)
+    m = _c(material_words, np.float32).reshape(-1)
+    info = np.zeros(2, np.uint32)
+    lib = library()
+    n = lib.vgi_host_emitters(_ptr(coords), coords.shape[0], _ptr(voxels), _ptr(m), None, 0, _ptr(info))
+    out = np.zeros(n, np.uint32)
+    lib.vgi_host_emitters(_ptr(coords), coords.shape[0], _ptr(voxels), _ptr(m), _ptr(out), n, _ptr(info))
+    return out, int(info[0]), float(info[1:2].view(np.float32)[0])
+
+
+def host_face_index(faces) -> np.ndarray:
+    f = _c(faces, np.int32).reshape(-1, 4)
+    lib = library()
+    n = lib.vgi_host_face_index(_ptr(f), f.shape[0], None, 0)
+    out = np.zeros((n, 4), np.uint32)
+    lib.vgi_host_face_index(_ptr(f), f.shape[0], _ptr(out), n)
+    return out
+
+
+def host_top_level(coords, solid) -> Optional[np.ndarray]:
+    coords = _c(coords, np.int32).reshape(-1, 3)
+    s = _c(solid, np.uint8)
+    lo, hi = coords.min(0), coords.max(0)
+    cells = int(np.prod(hi - lo + 1))
+    out = np.zeros(cells * 6, np.uint8)
+    rc = library().vgi_host_top_level(_ptr(coords), _ptr(s), coords.shape[0], _ptr(out), out.size)
+    return None if rc == 1 else out.reshape(-1, 6)
+
+
+def tasks_for(faces: np.ndarray, sequence: int = 0) -> np.ndarray:
+    """FaceTask words (voxel xyz, face, sequence, 0, 0, 0) for face rows."""
+    f = np.asarray(faces, np.int32).reshape(-1, 5)
+    t = np.zeros((f.shape[0], 8), np.uint32)
+    t[:, 0:3] = f[:, 0:3].astype(np.int64).astype(np.uint32)
+    t[:, 3] = f[:, 3]
+    t[:, 4] = sequence
+    return t

@@ -1,0 +1,185 @@
+/*
+ * vgi.h -- C ABI of the B200-native voxel diffuse-GI path (libvgi.so).
+ *
+ * This is the drop-in boundary for bevy_voxel_gi's per-frame GPU transport:
+ * NAADF geometry upload and edits, distance-skip DDA traversal, the
+ * visible-face cosine-hemisphere trace into the face cache, the world-cache
+ * gather and the temporal accumulation with proportional edit discount.
+ * Each entry point names the reference interface it replaces (paths within
+ * nathanaelneveux/global-illumination, crates/bevy_voxel_gi/).
+ *
+ * Conventions
+ *  - Every function returns an int status: VGI_OK (0), > 0 recoverable,
+ *    < 0 fatal for the context. vgi_last_error() describes the last failure.
+ *  - A context is owned by one thread at a time (the reference's single trace
+ *    worker, src/dispatch.rs:167-275); it is not thread-safe.
+ *  - Host buffers passed in are copied before the call returns. Device
+ *    buffers belong to the library. Work is enqueued on the context's CUDA
+ *    stream; read-back calls synchronise that stream.
+ *  - Word layouts are the reference's GPU records (little-endian u32/f32):
+ *    GpuMaterial 16 floats, GpuLight 12 floats, FaceTask 8 words,
+ *    FaceResult 24 words, resident state 36 words (src/gpu.rs:118-184,
+ *    shaders/voxel_trace.wgsl:5-20, shaders/voxel_accumulate.wgsl:1-3).
+ */
+#ifndef VGI_H
+#define VGI_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VGI_OK 0
+#define VGI_UNAVAILABLE 1       /* no usable CUDA device: transport idles (src/lib.rs:355-357) */
+#define VGI_ERR_INVALID (-1)    /* bad argument or size */
+#define VGI_ERR_CUDA (-2)       /* a CUDA call failed */
+#define VGI_ERR_STATE (-3)      /* call out of order (e.g. frame before geometry) */
+#define VGI_ERR_CAPACITY (-4)   /* a size limit was exceeded */
+
+typedef struct vgi_ctx vgi_ctx;
+
+typedef struct {
+    int32_t device;   /* CUDA ordinal */
+    uint32_t flags;   /* reserved, 0 */
+} vgi_config;
+
+/* Transport and accumulation settings (src/settings.rs:393-428 TransportSettings,
+ * src/work.rs:11-47 TraceWork history fields, shader override constants
+ * shaders/voxel_path.wgsl:4-14 and shaders/voxel_trace.wgsl:3). */
+typedef struct {
+    float reach;              /* diffuse reach, clamped to [1, 768]; < 768 selects LIMITED_REACH */
+    uint32_t bounces;         /* DIFFUSE_HITS, clamped to [1, 3] */
+    uint32_t path_steps;      /* PATH_STEPS (default 2048) */
+    uint32_t budgeted;        /* BUDGETED_RAYS (0/1) */
+    uint32_t history_limit;   /* 0 = 65536 */
+    float recency;            /* >= 1; other values select 1 */
+    float measured_retention; /* c of the measured discount; 0 = distance curve */
+    float response_seconds;   /* display response time constant */
+    uint32_t lanes;           /* threads per face (1,2,4,8,16,32); 0 = automatic */
+    uint32_t transport_revision;
+    float stable_error;
+    uint32_t stable_samples;
+} vgi_transport;
+
+/* One face-cache slot: the exposed face (voxel, face 0..5 in +X,-X,+Y,-Y,+Z,-Z
+ * order) and its voxel's material (slot identity, shaders/voxel_accumulate.wgsl:37-42). */
+typedef struct {
+    int32_t voxel[3];
+    uint32_t face;
+    uint32_t material;
+} vgi_face;
+
+/* Per-frame work counters (filled by the counting pass, vgi_census). */
+typedef struct {
+    uint64_t rays;        /* trace_domain_limited calls */
+    uint64_t paths;       /* receiver samples */
+    uint64_t steps;       /* DDA iterations, including geometry_ahead */
+    uint64_t bytes;       /* algorithmic bytes of the trace */
+    uint64_t unknown;     /* paths that reached unloaded space */
+    uint64_t cache_hits;  /* paths ended by the world-cache gather */
+    uint64_t status[4];   /* rays by status: escaped, hit, unknown, reach */
+} vgi_counters;
+
+/* ---- lifecycle: GpuTracer::new / drop (src/gpu.rs:448-595) ---------------- */
+int vgi_create(const vgi_config* config, vgi_ctx** out);
+int vgi_destroy(vgi_ctx* ctx);
+const char* vgi_last_error(const vgi_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work. */
+int vgi_stream(vgi_ctx* ctx, void** stream);
+int vgi_sync(vgi_ctx* ctx);
+
+/* ---- geometry: NaadfRegion::build + PackedScene::update + synchronize_geometry
+ * (src/world.rs:243-384, src/gpu_scene.rs:72-309, src/gpu/geometry.rs:19-124).
+ * `coords` holds 3 region coordinates per region (16^3 voxels each), `voxels`
+ * 4096 u16 per region (x fastest; 0..255 solid material, 256 air),
+ * `strides` the optional per-region stride log2 (header bits 28-30). The GPU
+ * classifies regions, builds brick and voxel AADFs and packs the cells; the
+ * host runtime grows the top-level field and the directory. */
+int vgi_upload_regions(vgi_ctx* ctx, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides);
+/* Parity path: arrays exactly as PackedScene holds them (directory 4 ints per
+ * slot, headers 4 words per region, cells) and region bounds min xyz, max xyz. */
+int vgi_upload_packed(vgi_ctx* ctx, const int32_t* directory, uint64_t slots, const uint32_t* headers, uint32_t n_headers,
+                      const uint32_t* cells, uint64_t n_cells, const int32_t* bounds6);
+/* VoxelGiInput::edit_voxel batch (src/input.rs:90-93): 4 ints per edit
+ * (x, y, z, value). Voxels outside uploaded regions are ignored. The edited
+ * regions are repacked on the GPU and the top-level field is updated
+ * incrementally (TransportScene::with_page_contents, src/world.rs:982-1046). */
+int vgi_edit_voxels(vgi_ctx* ctx, const int32_t* edits, uint32_t n);
+/* sizes: directory slots, headers, cells; bounds: min xyz, max xyz. */
+int vgi_geometry_info(vgi_ctx* ctx, uint64_t* sizes3, int32_t* bounds6);
+int vgi_read_geometry(vgi_ctx* ctx, int32_t* directory, uint32_t* headers, uint32_t* cells);
+
+/* ---- model: GpuTracer's material/light/emitter uploads (src/gpu.rs:680-800) --- */
+int vgi_set_materials(vgi_ctx* ctx, const float* materials /* 256 x 16 */);
+/* `lights`: n GpuLight records, directional ones first. */
+int vgi_set_lights(vgi_ctx* ctx, const float* lights /* n x 12 */, uint32_t n, uint32_t n_directional);
+int vgi_set_environment(vgi_ctx* ctx, const float* rgb3);
+/* Emitter buffer as the shader reads it (GpuEmitter records then light-tree words). */
+int vgi_set_emitters(vgi_ctx* ctx, const uint32_t* words, uint64_t n_words, uint32_t n_faces, float total_weight);
+/* EmissionDistribution::build (src/emission.rs:91-165) from the uploaded
+ * regions and the current materials, done by the host runtime. */
+int vgi_build_emitters(vgi_ctx* ctx);
+
+/* ---- transport settings: select_quality_pipeline (src/gpu.rs:1172-1229) --- */
+int vgi_set_transport(vgi_ctx* ctx, const vgi_transport* transport);
+
+/* ---- face cache: resident slots and the face index (src/gpu/resident.rs,
+ * src/gpu/face_index.rs). Slots 0..n-1 start empty (sequence 0). */
+int vgi_set_faces(vgi_ctx* ctx, const vgi_face* faces, uint32_t n);
+
+/* One frame over every slot: prepare (begin_trace), mark_changed, the face
+ * trace with cache gather, then accumulate (submit_compact's resident batch,
+ * src/gpu.rs:647-1022). `clock_ms` is the accumulation clock. Enqueued only. */
+int vgi_frame(vgi_ctx* ctx, uint32_t samples, uint32_t clock_ms);
+/* Device timing of vgi_frame (the reference's timestamp query pairs,
+ * src/gpu.rs:488-500): with timing enabled each frame records CUDA events on
+ * the context's stream around prepare, trace and accumulate, and
+ * vgi_frame_times returns the last frame's three durations in ms
+ * (synchronises the stream). */
+int vgi_set_timing(vgi_ctx* ctx, int enable);
+int vgi_frame_times(vgi_ctx* ctx, float* ms3);
+/* The same frame through host buffers (submit_compact + complete_readback):
+ * 8-word tasks in (one per slot, in slot order; their sequence words are
+ * replaced by the slot's), 24-word results out. Synchronous. */
+int vgi_trace_batch(vgi_ctx* ctx, const uint32_t* tasks, uint32_t n, uint32_t samples, uint32_t clock_ms, uint32_t* results);
+/* A counting trace of the next frame's work (no state change): rays, paths,
+ * steps and algorithmic bytes. Synchronous. */
+int vgi_census(vgi_ctx* ctx, uint32_t samples, vgi_counters* counters);
+/* Trace explicit tasks against the current cache without accumulating
+ * (trace_faces_parallel alone). Synchronous; counters may be null. */
+int vgi_trace_tasks(vgi_ctx* ctx, const uint32_t* tasks, uint32_t n, uint32_t samples, uint32_t* results, vgi_counters* counters);
+
+/* Retention events in the encode_events layout (src/gpu/resident.rs:1326-1414):
+ * n_events headers of three uint4, then bound records of two uint4.
+ * Applied by apply_events to every live slot (shaders/voxel_accumulate.wgsl:295-332). */
+int vgi_apply_events(vgi_ctx* ctx, const uint32_t* words, uint32_t n_events, uint64_t n_words);
+
+/* ---- read-back: bounded snapshots (complete_readback, src/gpu.rs:1024-1170) --- */
+int vgi_read_results(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words24);
+int vgi_read_state(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words36);
+int vgi_write_state(vgi_ctx* ctx, uint32_t first, uint32_t n, const uint32_t* words36);
+int vgi_read_slot_meta(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words12);
+
+/* ---- host runtime (no device needed) -------------------------------------- */
+/* Record builders with the host-side conventions of src/gpu.rs:717-760
+ * (directional: glam normalize_or_zero of the direction, range -1). */
+void vgi_material_record(const float* diffuse3, const float* emission3, float* out16);
+void vgi_directional_light_record(const float* direction3, const float* radiance3, const float* custom3, float* out12);
+/* The emitter words vgi_build_emitters uploads, for a region list and a
+ * material table: returns the word count, writes when `capacity` suffices;
+ * info = [faces, total_weight bits]. */
+int64_t vgi_host_emitters(const int32_t* coords, uint32_t n, const uint16_t* voxels, const float* materials, uint32_t* out,
+                          uint64_t capacity, uint32_t* info2);
+/* The face index vgi_set_faces uploads (4 ints per face: voxel xyz, face):
+ * returns the uint4 count (capacity + 1), writes when `capacity4` suffices. */
+int64_t vgi_host_face_index(const int32_t* faces, uint32_t n, uint32_t* out, uint64_t capacity4);
+/* The top-level field vgi_upload_regions grows from an empty scene: 6 bytes
+ * per cell over the region bounds (x fastest); returns 1 when the field is
+ * disabled by its size limits, 0 when written. `solid` holds 1 per region
+ * with any solid voxel. */
+int vgi_host_top_level(const int32_t* coords, const uint8_t* solid, uint32_t n, uint8_t* out6, uint64_t capacity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VGI_H */

@@ -1,0 +1,1159 @@
+// TEST INFRASTRUCTURE ONLY (the oracle). CPU restatement of the reference's
+// WGSL transport: traversal, path estimator, world-space face trace, cache
+// gather, accumulation and the proportional edit discount. tests/ compare the
+// CUDA kernels with it; bench.py times it as the CPU baseline. The product
+// never links it.
+//
+// Follows (paths within nathanaelneveux/global-illumination):
+//   crates/bevy_voxel_gi/shaders/voxel_traversal.wgsl:17-219   traversal
+//   crates/bevy_voxel_gi/shaders/voxel_path.wgsl:63-520         estimator
+//   crates/bevy_voxel_gi/shaders/voxel_trace.wgsl:25-92         face trace
+//   crates/bevy_voxel_gi/shaders/voxel_accumulate.wgsl:83-446   prepare/accumulate/events
+//   crates/bevy_voxel_gi/shaders/voxel_retention.wgsl:1-96      resolve_retention
+//   crates/bevy_voxel_gi/src/gpu/face_index.rs:22-145           face index
+//   crates/bevy_voxel_gi/src/emission.rs:91-165                 emitter distribution
+//   crates/bevy_voxel_gi/src/emission/tree.rs:28-75, 173-195    light tree and its words
+//
+// Every float expression keeps the shader's operation order; see
+// oracle_math.h for the builtin semantics.
+#include "oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <map>
+#include <atomic>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+struct Geometry {
+    const int32_t* directory;
+    const uint32_t* headers;
+    const uint32_t* cells;
+    uint32_t mask;
+    int32_t mn[3], mx[3];
+};
+
+struct Model {
+    const float* params;      // 24 words (GpuParams)
+    const float* materials;   // 16 floats per material
+    const float* lights;      // 12 floats per light
+    const uint32_t* emitters; // uint4 words
+    const uint32_t* state;    // 36 words per slot (9 uint4)
+    const uint32_t* index;    // uint4 words; [0] = (mask, probes, 0, 0)
+    orc_pipeline pipe;
+};
+
+struct Counters {
+    uint64_t rays = 0, paths = 0, steps = 0, bytes = 0, unknown = 0, cache_hits = 0;
+    uint64_t status[4] = {0, 0, 0, 0};
+};
+
+struct Ctx {
+    Geometry g;
+    Model m;
+    Counters c;
+    uint32_t pcount(int i) const { return fbits(m.params[i]); }   // counts.*
+    int32_t pmin(int i) const { return (int32_t)fbits(m.params[4 + i]); }
+    int32_t pmax(int i) const { return (int32_t)fbits(m.params[8 + i]); }
+    float env(int i) const { return m.params[12 + i]; }
+    float extra(int i) const { return m.params[16 + i]; }
+    float transport(int i) const { return m.params[20 + i]; }
+};
+
+struct RayResult {
+    i3 voxel{0, 0, 0};
+    uint32_t material = 0;
+    f3 position{0, 0, 0};
+    uint32_t status = 0;
+    f3 normal{0, 0, 0};
+};
+
+// ---- voxel_traversal.wgsl ------------------------------------------------
+static uint32_t face_index_of(f3 n) {
+    if (n.x != 0.0f) return n.x < 0.0f ? 1u : 0u;
+    if (n.y != 0.0f) return n.y < 0.0f ? 3u : 2u;
+    if (n.z != 0.0f) return n.z < 0.0f ? 5u : 4u;
+    return 6u;
+}
+
+static uint32_t lookup_region(Ctx& x, i3 c) {
+    uint32_t slot = hash_voxel(c.x, c.y, c.z) & x.g.mask;
+    for (uint32_t attempt = 0; attempt < 32u; ++attempt) {
+        const int32_t* e = x.g.directory + (size_t)slot * 4;
+        x.c.bytes += 16;
+        if (e[3] == -1) return 0xffffffffu;
+        if (e[0] == c.x && e[1] == c.y && e[2] == c.z) return (uint32_t)e[3];
+        slot = (slot + 1u) & x.g.mask;
+    }
+    return 0xffffffffu;
+}
+
+static bool in_bounds(const Ctx& x, i3 r) {
+    return r.x >= x.g.mn[0] && r.y >= x.g.mn[1] && r.z >= x.g.mn[2] && r.x <= x.g.mx[0] && r.y <= x.g.mx[1] &&
+           r.z <= x.g.mx[2];
+}
+
+static i3 unpack_bytes(uint32_t v) { return i3{(int32_t)(v & 255u), (int32_t)((v >> 8) & 255u), (int32_t)((v >> 16) & 255u)}; }
+static i3 negative_extents(uint32_t b) { return i3{(int32_t)(b & 3u), (int32_t)((b >> 4) & 3u), (int32_t)((b >> 8) & 3u)}; }
+static i3 positive_extents(uint32_t b) { return i3{(int32_t)((b >> 2) & 3u), (int32_t)((b >> 6) & 3u), (int32_t)((b >> 10) & 3u)}; }
+
+struct F4 { float x, y, z, w; };
+
+// voxel_traversal.wgsl:90-107
+static F4 advance_box(f3 p, f3 d, i3 cell, i3 ng, i3 ps, float size) {
+    float mnv[3] = {(float)(cell.x - ng.x) * size, (float)(cell.y - ng.y) * size, (float)(cell.z - ng.z) * size};
+    float mxv[3] = {(float)(cell.x + ps.x + 1) * size, (float)(cell.y + ps.y + 1) * size, (float)(cell.z + ps.z + 1) * size};
+    float pp[3] = {p.x, p.y, p.z}, dd[3] = {d.x, d.y, d.z};
+    float travel[3];
+    for (int a = 0; a < 3; ++a) {
+        bool moving = std::fabs(dd[a]) > 1e-8f;
+        float plane = dd[a] > 0.0f ? mxv[a] : mnv[a];
+        float raw = (plane - pp[a]) / (moving ? dd[a] : 1.0f);
+        travel[a] = (moving && raw >= -0.001f && raw < 1e30f) ? raw : 1e30f;
+    }
+    bool choose_y = travel[1] < wmax(travel[0], 0.0f);
+    float distance_xy = wmax(choose_y ? travel[1] : travel[0], 0.0f);
+    bool choose_z = travel[2] < distance_xy;
+    float distance = wmax(choose_z ? travel[2] : distance_xy, 0.0f);
+    float axis[3] = {0.0f, 0.0f, 0.0f};
+    if (choose_z) axis[2] = 1.0f; else if (choose_y) axis[1] = 1.0f; else axis[0] = 1.0f;
+    float nrm[3];
+    for (int a = 0; a < 3; ++a) nrm[a] = distance < 1e30f ? axis[a] * (dd[a] > 0.0f ? -1.0f : 1.0f) : 0.0f;
+    return F4{nrm[0], nrm[1], nrm[2], wmax(distance + 0.001f, 0.001f)};
+}
+
+// voxel_traversal.wgsl:108-121
+static bool geometry_ahead(Ctx& x, f3 start, f3 dir, float max_distance) {
+    f3 position = start;
+    float remaining = max_distance;
+    for (uint32_t step = 0; step < 2048u; ++step) {
+        x.c.steps += 1;
+        f3 q = divs(position, 16.0f);
+        i3 region{f2i(std::floor(q.x)), f2i(std::floor(q.y)), f2i(std::floor(q.z))};
+        if (remaining < 0.0f || !in_bounds(x, region)) return false;
+        uint32_t index = lookup_region(x, region);
+        if (index != 0xffffffffu) {
+            x.c.bytes += 16;
+            if (x.g.headers[(size_t)index * 4] != 1u) return true;
+        }
+        float travel = advance_box(position, dir, region, i3{0, 0, 0}, i3{0, 0, 0}, 16.0f).w;
+        position = add(position, muls(dir, travel));
+        remaining = remaining - travel;
+    }
+    return true;
+}
+
+// voxel_traversal.wgsl:126-219
+static RayResult trace_domain_limited(Ctx& x, f3 origin, f3 dir, float max_distance, bool visible_geometry,
+                                      uint32_t max_steps) {
+    x.c.rays += 1;
+    RayResult result;
+    float nearv = -1e30f, farv = 1e30f;
+    f3 normal{0.0f, 0.0f, 0.0f};
+    float mnv[3] = {(float)x.pmin(0) * 16.0f, (float)x.pmin(1) * 16.0f, (float)x.pmin(2) * 16.0f};
+    float mxv[3] = {(float)(x.pmax(0) + 1) * 16.0f, (float)(x.pmax(1) + 1) * 16.0f, (float)(x.pmax(2) + 1) * 16.0f};
+    float oo[3] = {origin.x, origin.y, origin.z}, dd[3] = {dir.x, dir.y, dir.z};
+    for (int a = 0; a < 3; ++a) {
+        if (std::fabs(dd[a]) <= 1e-8f) {
+            if (oo[a] < mnv[a] || oo[a] > mxv[a]) { x.c.status[0] += 1; return result; }
+            continue;
+        }
+        float first = (mnv[a] - oo[a]) / dd[a];
+        float second = (mxv[a] - oo[a]) / dd[a];
+        if (wmin(first, second) > nearv) {
+            nearv = wmin(first, second);
+            normal = f3{0.0f, 0.0f, 0.0f};
+            setc(normal, a, first < second ? -1.0f : 1.0f);
+        }
+        farv = wmin(farv, wmax(first, second));
+    }
+    if (farv < wmax(nearv, 0.0f)) { x.c.status[0] += 1; return result; }
+    float distance = wmax(nearv, 0.0f) + 0.001f;
+    f3 position = add(origin, muls(dir, distance));
+    i3 last_region{0x7fffffff, 0x7fffffff, 0x7fffffff};
+    uint32_t meta[4] = {0, 0, 0, 0};
+    for (uint32_t step = 0; step < max_steps; ++step) {
+        x.c.steps += 1;
+        if (distance > max_distance) { x.c.status[0] += 1; return result; }
+        i3 voxel{f2i(std::floor(position.x)), f2i(std::floor(position.y)), f2i(std::floor(position.z))};
+        i3 region{voxel.x >> 4, voxel.y >> 4, voxel.z >> 4};
+        if (!in_bounds(x, region)) { x.c.status[0] += 1; return result; }
+        if (last_region.x != region.x || last_region.y != region.y || last_region.z != region.z) {
+            uint32_t index = lookup_region(x, region);
+            if (index == 0xffffffffu) {
+                if (visible_geometry) {
+                    F4 adv = advance_box(position, dir, region, i3{0, 0, 0}, i3{0, 0, 0}, 16.0f);
+                    distance = distance + adv.w;
+                    position = add(position, muls(dir, adv.w));
+                    normal = f3{adv.x, adv.y, adv.z};
+                    continue;
+                }
+                result.status = geometry_ahead(x, position, dir, max_distance - distance) ? 2u : 0u;
+                x.c.status[result.status] += 1;
+                return result;
+            }
+            x.c.bytes += 16;
+            const uint32_t* h = x.g.headers + (size_t)index * 4;
+            meta[0] = h[0]; meta[1] = h[1]; meta[2] = h[2]; meta[3] = h[3];
+            last_region = region;
+        }
+        F4 adv{0.0f, 0.0f, 0.0f, 0.0f};
+        if (meta[0] == 1u) {
+            adv = advance_box(position, dir, region, unpack_bytes(meta[2]), unpack_bytes(meta[3]), 16.0f);
+        } else {
+            uint32_t material = meta[1];
+            if (meta[0] == 3u) {
+                uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
+                uint32_t bx = lx / 4u, by = ly / 4u, bz = lz / 4u;
+                uint32_t brick_data = x.g.cells[meta[1] + (bz * 4u + by) * 4u + bx];
+                x.c.bytes += 4;
+                uint32_t state = brick_data & 3u;
+                if (state == 0u) {
+                    uint32_t ext = brick_data >> 2u;
+                    adv = advance_box(position, dir, i3{region.x * 4 + (int32_t)bx, region.y * 4 + (int32_t)by, region.z * 4 + (int32_t)bz},
+                                      negative_extents(ext), positive_extents(ext), 4.0f);
+                    material = 256u;
+                } else if (state == 1u) {
+                    material = brick_data >> 2u;
+                } else {
+                    uint32_t ix = lx & 3u, iy = ly & 3u, iz = lz & 3u;
+                    uint32_t idx = (iz * 4u + iy) * 4u + ix;
+                    uint32_t word = x.g.cells[(brick_data >> 2u) + idx / 2u];
+                    x.c.bytes += 4;
+                    uint32_t cell = (word >> ((idx & 1u) * 16u)) & 65535u;
+                    material = (cell & 1u) != 0u ? (cell >> 1u) : 256u;
+                    if (material == 256u) {
+                        uint32_t ext = cell >> 1u;
+                        adv = advance_box(position, dir, voxel, negative_extents(ext), positive_extents(ext), 1.0f);
+                    }
+                }
+            }
+            if (material != 256u) {
+                result.voxel = voxel;
+                result.material = material;
+                result.position = position;
+                result.normal = normal;
+                result.status = 1u;
+                x.c.status[1] += 1;
+                return result;
+            }
+        }
+        distance = distance + adv.w;
+        position = add(position, muls(dir, adv.w));
+        normal = f3{adv.x, adv.y, adv.z};
+    }
+    result.status = 2u;
+    result.material = 0xffffffffu;
+    x.c.status[2] += 1;
+    return result;
+}
+
+// ---- voxel_path.wgsl -------------------------------------------------------
+struct Energy { F4 value{0, 0, 0, 0}; f3 custom{0, 0, 0}; };
+
+static F4 f4add(F4 a, F4 b) { return F4{a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
+static F4 f4mul(F4 a, F4 b) { return F4{a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w}; }
+static F4 f4muls(F4 a, float s) { return F4{a.x * s, a.y * s, a.z * s, a.w * s}; }
+static F4 f4divs(F4 a, float s) { return F4{a.x / s, a.y / s, a.z / s, a.w / s}; }
+static F4 ld4(const float* p) { return F4{p[0], p[1], p[2], p[3]}; }
+
+static F4 material_diffuse(Ctx& x, uint32_t m) { x.c.bytes += 64; return ld4(x.m.materials + (size_t)m * 16); }
+static const float* material(Ctx& x, uint32_t m) { x.c.bytes += 64; return x.m.materials + (size_t)m * 16; }
+
+struct Emissive { i3 voxel; uint32_t face; F4 sampling; };
+static Emissive load_emitter(Ctx& x, uint32_t index) {
+    x.c.bytes += 32;
+    const uint32_t* a = x.m.emitters + (size_t)index * 8;
+    return Emissive{i3{(int32_t)a[0], (int32_t)a[1], (int32_t)a[2]}, a[3], F4{bitsf(a[4]), bitsf(a[5]), bitsf(a[6]), bitsf(a[7])}};
+}
+struct LightNode { F4 minimum_power; f3 maximum; uint32_t normals; i3 pivot; uint32_t face; uint32_t children[4]; };
+static LightNode load_node(Ctx& x, uint32_t index) {
+    x.c.bytes += 64;
+    uint32_t offset = f2u(x.extra(3)) * 2u + index * 4u;
+    const uint32_t* w = x.m.emitters + (size_t)offset * 4;
+    LightNode n;
+    n.minimum_power = F4{bitsf(w[0]), bitsf(w[1]), bitsf(w[2]), bitsf(w[3])};
+    n.maximum = f3{bitsf(w[4]), bitsf(w[5]), bitsf(w[6])};
+    n.normals = w[7];
+    n.pivot = i3{(int32_t)w[8], (int32_t)w[9], (int32_t)w[10]};
+    n.face = w[11];
+    for (int i = 0; i < 4; ++i) n.children[i] = w[12 + i];
+    return n;
+}
+
+static f3 face_normal(uint32_t face) {
+    f3 n{0.0f, 0.0f, 0.0f};
+    setc(n, (int)(face / 2u), (face & 1u) != 0u ? -1.0f : 1.0f);
+    return n;
+}
+
+// voxel_path.wgsl:108-122
+static float node_importance(const LightNode& node, f3 position, f3 normal) {
+    f3 mnp{node.minimum_power.x, node.minimum_power.y, node.minimum_power.z};
+    f3 delta = sub(muls(add(mnp, node.maximum), 0.5f), position);
+    float radius = length(sub(node.maximum, mnp)) * 0.5f;
+    float distance = wmax(length(delta), 1e-5f);
+    f3 direction = divs(delta, distance);
+    float spread = wmin(radius / distance, 1.0f);
+    float receiver = wclamp(dot(normal, direction) + spread, 0.0f, 1.0f);
+    f3 nd = neg(direction);
+    float positive[3] = {(node.normals & 1u) ? nd.x : -1.0f, (node.normals & 4u) ? nd.y : -1.0f, (node.normals & 16u) ? nd.z : -1.0f};
+    float negative[3] = {(node.normals & 2u) ? direction.x : -1.0f, (node.normals & 8u) ? direction.y : -1.0f,
+                         (node.normals & 32u) ? direction.z : -1.0f};
+    float projected[3];
+    for (int a = 0; a < 3; ++a) projected[a] = wmax(positive[a], negative[a]);
+    float emitter = wclamp(wmax(wmax(projected[0], projected[1]), projected[2]) + spread, 0.0f, 1.0f);
+    return node.minimum_power.w * receiver * emitter / (distance * distance + radius * radius + 0.25f);
+}
+
+// voxel_path.wgsl:123-131
+static float node_left_probability(Ctx& x, const LightNode& node, f3 position, f3 normal) {
+    LightNode left = load_node(x, node.children[0]);
+    LightNode right = load_node(x, node.children[1]);
+    float power = left.minimum_power.w / (left.minimum_power.w + right.minimum_power.w);
+    float a = node_importance(left, position, normal);
+    float b = node_importance(right, position, normal);
+    if (a + b <= 1e-20f) return wclamp(power, 1e-6f, 0.999999f);
+    return wclamp(0.05f * power + 0.95f * a / (a + b), 1e-6f, 0.999999f);
+}
+
+// voxel_path.wgsl:132-149
+static Emissive tree_emitter(Ctx& x, f3 position, f3 normal, float choice) {
+    uint32_t index = 0;
+    float uniform = choice;
+    float probability = 1.0f;
+    for (;;) {
+        LightNode node = load_node(x, index);
+        if (node.children[0] == 0xffffffffu) {
+            Emissive e = load_emitter(x, node.children[1]);
+            e.sampling.y = probability;
+            return e;
+        }
+        float p = node_left_probability(x, node, position, normal);
+        if (uniform < p) { probability = probability * p; uniform = uniform / p; index = node.children[0]; }
+        else { probability = probability * (1.0f - p); uniform = (uniform - p) / (1.0f - p); index = node.children[1]; }
+        uniform = wmin(uniform, bitsf(0x3f7fffffu));
+    }
+}
+
+// voxel_path.wgsl:150-174
+static bool key_less(i3 voxel, uint32_t face, const LightNode& node) {
+    uint32_t axis = node.children[2];
+    for (uint32_t j = 0; j < 3u; ++j) {
+        int i = (int)((axis + j) % 3u);
+        if (compi(voxel, i) != compi(node.pivot, i)) return compi(voxel, i) < compi(node.pivot, i);
+    }
+    return face < node.face;
+}
+static float tree_probability(Ctx& x, f3 position, f3 normal, i3 voxel, f3 hit_normal) {
+    uint32_t face = 0;
+    for (uint32_t i = 0; i < 6u; ++i) {
+        f3 fn = face_normal(i);
+        if (fn.x == hit_normal.x && fn.y == hit_normal.y && fn.z == hit_normal.z) face = i;
+    }
+    uint32_t index = 0;
+    float probability = 1.0f;
+    for (;;) {
+        LightNode node = load_node(x, index);
+        if (node.children[0] == 0xffffffffu) {
+            Emissive found = load_emitter(x, node.children[1]);
+            bool same = found.voxel.x == voxel.x && found.voxel.y == voxel.y && found.voxel.z == voxel.z && found.face == face;
+            return same ? probability : 0.0f;
+        }
+        float p = node_left_probability(x, node, position, normal);
+        if (key_less(voxel, face, node)) { probability = probability * p; index = node.children[0]; }
+        else { probability = probability * (1.0f - p); index = node.children[1]; }
+    }
+}
+
+// voxel_path.wgsl:178-213
+static uint32_t scramble_reverse(uint32_t input, uint32_t seed) {
+    uint32_t v = input;
+    v ^= v * 0x3d20adeau;
+    v += seed;
+    v *= (seed >> 16u) | 1u;
+    v ^= v * 0x05526c56u;
+    v ^= v * 0x53a22864u;
+    return v;
+}
+static float sample_1d(uint32_t stream, uint32_t sequence, uint32_t dimension) {
+    if (dimension < 12u) {
+        static const uint32_t primes[12] = {2u, 3u, 5u, 7u, 11u, 13u, 17u, 19u, 23u, 29u, 31u, 37u};
+        uint32_t base = primes[dimension];
+        uint32_t index = (sequence & 0x00ffffffu) + 1u;
+        float scale = 1.0f, value = 0.0f;
+        while (index != 0u) {
+            scale = scale / (float)base;
+            value = value + (float)(index % base) * scale;
+            index = index / base;
+        }
+        float rotation = (float)(pcg(stream ^ pcg(dimension)) >> 9u) / 8388608.0f;
+        return fract(value + rotation);
+    }
+    uint32_t seed = pcg(stream ^ pcg(dimension / 2u));
+    uint32_t index = reverse_bits(scramble_reverse(reverse_bits(sequence), pcg(seed ^ 0x79c68e4au)));
+    if ((dimension & 1u) != 0u) {
+        index ^= (index >> 1u) & 0x55555555u;
+        index ^= (index >> 2u) & 0x33333333u;
+        index ^= (index >> 4u) & 0x0f0f0f0fu;
+        index ^= (index >> 8u) & 0x00ff00ffu;
+        index ^= (index >> 16u) & 0x0000ffffu;
+    }
+    uint32_t value = reverse_bits(scramble_reverse(index, pcg(seed ^ pcg(dimension))));
+    return (float)(value >> 9u) / 8388608.0f;
+}
+// voxel_path.wgsl:218-224
+static float continuation_sample(uint32_t stream, uint32_t sequence, uint32_t bounce, uint32_t dimension) {
+    if (bounce < 3u) {
+        uint32_t legacy = dimension == 2u ? 8u + bounce : 2u + bounce * 2u + dimension;
+        return sample_1d(stream, sequence, legacy);
+    }
+    return sample_1d(stream, sequence, 16u + (bounce - 3u) * 3u + dimension);
+}
+
+// voxel_path.wgsl:231-238
+static f3 hemisphere(f3 n, float u, float v) {
+    f3 tangent;
+    if (std::fabs(n.z) < 0.999f) tangent = normalize(cross(n, f3{0.0f, 0.0f, 1.0f}));
+    else tangent = normalize(cross(n, f3{0.0f, 1.0f, 0.0f}));
+    f3 bitangent = cross(n, tangent);
+    float phi = 6.28318530718f * u;
+    float s, c;
+    own_sincos(phi, &s, &c);
+    return add(add(muls(tangent, c * std::sqrt(v)), muls(bitangent, s * std::sqrt(v))), muls(n, std::sqrt(1.0f - v)));
+}
+
+// voxel_path.wgsl:239-243
+static RayResult trace(Ctx& x, f3 origin, f3 dir, float max_distance) {
+    RayResult r = trace_domain_limited(x, origin, dir, max_distance, x.m.pipe.budgeted != 0, x.m.pipe.path_steps);
+    if (x.m.pipe.budgeted && r.status == 2u && r.material == 0xffffffffu) r.status = 0u;
+    return r;
+}
+static float connection_reach(const Ctx& x) { return x.m.pipe.limited_reach ? x.transport(0) : x.extra(1); }
+
+// voxel_path.wgsl:271-282
+static RayResult trace_diffuse(Ctx& x, f3 origin, f3 dir) {
+    float reach = connection_reach(x);
+    RayResult r = trace(x, origin, dir, reach);
+    if (x.m.pipe.limited_reach && r.status == 0u &&
+        geometry_ahead(x, add(origin, muls(dir, reach)), dir, x.extra(1) - reach))
+        r.status = 3u;
+    return r;
+}
+
+// voxel_path.wgsl:283-307
+static Energy direct_at(Ctx& x, f3 position, f3 normal) {
+    Energy e;
+    f3 origin = add(position, muls(normal, 0.002f));
+    uint32_t count = x.pcount(3);
+    for (uint32_t i = 0; i < count; ++i) {
+        const float* L = x.m.lights + (size_t)i * 12;
+        x.c.bytes += 48;
+        f3 pos{L[0], L[1], L[2]};
+        float distance = x.extra(1);
+        float attenuation = 1.0f;
+        f3 direction;
+        if (L[3] >= 0.0f) {
+            f3 delta = sub(pos, position);
+            float d2 = dot(delta, delta);
+            if (d2 <= 0.0000001f || d2 > L[3] * L[3]) continue;
+            distance = std::sqrt(d2);
+            direction = divs(delta, distance);
+            distance = distance - 0.004f;
+            attenuation = 1.0f / wmax(d2, 1.0f);
+        } else {
+            direction = normalize(pos);
+        }
+        float cosine = wmax(dot(normal, direction), 0.0f);
+        if (cosine > 0.0f && trace(x, origin, direction, distance).status == 0u) {
+            float k = cosine * attenuation;
+            e.value = f4add(e.value, F4{L[4] * k, L[5] * k, L[6] * k, L[7] * k});
+            e.custom = add(e.custom, f3{L[9] * k, L[10] * k, L[11] * k});
+        }
+    }
+    return e;
+}
+
+// voxel_path.wgsl:309-324
+static Emissive choose_emitter(Ctx& x, f3 position, f3 normal, float choice) {
+    uint32_t count = f2u(x.extra(3));
+    if (load_emitter(x, 0).sampling.w > 0.0f) return tree_emitter(x, position, normal, choice);
+    uint32_t low = 0, high = count;
+    while (low < high) {
+        uint32_t middle = (low + high) / 2u;
+        if (load_emitter(x, middle).sampling.x <= choice) low = middle + 1u;
+        else high = middle;
+    }
+    return load_emitter(x, umin(low, count - 1u));
+}
+
+static float cosine_pdf(f3 n, f3 d) { return wmax(dot(n, d), 0.0f) / 3.14159265359f; }
+
+// voxel_path.wgsl:332-364
+static Energy sample_emitter(Ctx& x, f3 position, f3 normal, uint32_t source_stream, uint32_t sequence, uint32_t bounce) {
+    Energy result;
+    if (x.extra(3) == 0.0f) return result;
+    uint32_t stream = source_stream ^ pcg(bounce + 0xa341316cu);
+    Emissive em = choose_emitter(x, position, normal, sample_1d(stream, sequence, 12u));
+    f3 en = face_normal(em.face);
+    uint32_t axis = em.face / 2u;
+    f3 tangent = axis == 0u ? f3{0.0f, 1.0f, 0.0f} : f3{1.0f, 0.0f, 0.0f};
+    f3 bitangent = axis == 2u ? f3{0.0f, 1.0f, 0.0f} : f3{0.0f, 0.0f, 1.0f};
+    f3 lp = add(add(add(adds(tof(em.voxel), 0.5f), muls(en, 0.5f)), muls(tangent, sample_1d(stream, sequence, 13u) - 0.5f)),
+                muls(bitangent, sample_1d(stream, sequence, 14u) - 0.5f));
+    f3 delta = sub(lp, position);
+    float d2 = dot(delta, delta);
+    float reach = connection_reach(x);
+    if (d2 < 0.0001f || d2 > reach * reach) return result;
+    float distance = std::sqrt(d2);
+    f3 direction = divs(delta, distance);
+    float receiver_cosine = wmax(dot(normal, direction), 0.0f);
+    float emitter_cosine = wmax(dot(en, neg(direction)), 0.0f);
+    if (receiver_cosine <= 0.0f || emitter_cosine <= 0.0f || em.sampling.y <= 0.0f) return result;
+    float light_pdf = em.sampling.y * d2 / emitter_cosine;
+    float directional_pdf = receiver_cosine / 3.14159265359f;
+    f3 shadow_origin = add(position, muls(normal, 0.002f));
+    f3 shadow_delta = sub(add(lp, muls(en, 0.002f)), shadow_origin);
+    float shadow_distance = length(shadow_delta);
+    if (trace(x, shadow_origin, divs(shadow_delta, shadow_distance), shadow_distance).status != 0u) return result;
+    const float* mat = material(x, f2u(em.sampling.z));
+    float factor = directional_pdf / (light_pdf + directional_pdf);
+    result.value = f4muls(ld4(mat + 8), factor);
+    return result;
+}
+
+// voxel_path.wgsl:368-394
+static Energy sample_terminal_emission(Ctx& x, f3 position, f3 normal, uint32_t stream, uint32_t sequence, uint32_t bounce) {
+    Energy result;
+    if (x.extra(3) == 0.0f) return result;
+    if (continuation_sample(stream, sequence, bounce, 2u) < 0.5f) {
+        result = sample_emitter(x, position, normal, stream, sequence, bounce + 1u);
+        result.value = f4muls(result.value, 2.0f);
+        return result;
+    }
+    f3 direction = hemisphere(normal, continuation_sample(stream, sequence, bounce, 0u), continuation_sample(stream, sequence, bounce, 1u));
+    if (dot(normal, direction) <= 0.0f) return result;
+    RayResult hit = trace(x, add(position, muls(normal, 0.002f)), direction, connection_reach(x));
+    if (hit.status != 1u) return result;
+    const float* mat = material(x, hit.material);
+    float power = mat[13];
+    f3 delta = sub(hit.position, position);
+    float d2 = dot(delta, delta);
+    float reach = connection_reach(x);
+    if (power == 0.0f || d2 < 0.0001f || d2 > reach * reach) return result;
+    float selection_pdf = power / wmax(x.extra(2), 1e-20f);
+    if (load_emitter(x, 0).sampling.w > 0.0f) selection_pdf = tree_probability(x, position, normal, hit.voxel, hit.normal);
+    float light_pdf = selection_pdf * d2 / wmax(dot(hit.normal, neg(direction)), 1e-8f);
+    float directional_pdf = cosine_pdf(normal, direction);
+    float factor = 2.0f * directional_pdf / (directional_pdf + light_pdf);
+    result.value = f4muls(ld4(mat + 8), factor);
+    return result;
+}
+
+// voxel_path.wgsl:63-87, with the gather reading the slot's 16-byte cache
+// record (mean rgb, count word) instead of two state words.
+struct Cached { bool found; F4 value; };
+static Cached cached_energy(Ctx& x, i3 voxel, uint32_t face) {
+    Cached c{false, F4{0, 0, 0, 0}};
+    if (face > 5u || !x.m.index) return c;
+    const uint32_t* header = x.m.index;
+    uint32_t mask = header[0];
+    uint32_t slot = (hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(face + 1u)) & mask;
+    for (uint32_t attempt = 0; attempt < header[1]; ++attempt) {
+        const uint32_t* e = x.m.index + (size_t)(slot + 1u) * 4;
+        x.c.bytes += 16;
+        if (e[3] == 0xffffffffu) return c;
+        if ((int32_t)e[0] == voxel.x && (int32_t)e[1] == voxel.y && (int32_t)e[2] == voxel.z && (e[3] >> 29u) == face) {
+            uint32_t base = (e[3] & 0x1fffffffu) * 9u;
+            const uint32_t* words = x.m.state + (size_t)(base + 1u) * 4;
+            x.c.bytes += 16;
+            if (words[1] < 16u || (words[1] & 0x80000000u) != 0u) return c;
+            const uint32_t* m = x.m.state + (size_t)base * 4;
+            c.found = true;
+            c.value = F4{bitsf(m[0]), bitsf(m[1]), bitsf(m[2]), bitsf(m[3])};
+            return c;
+        }
+        slot = (slot + 1u) & mask;
+    }
+    return c;
+}
+
+struct PathEnergy { Energy energy; bool unknown = false; };
+struct PathState {
+    PathEnergy result;
+    F4 throughput{1.0f, 1.0f, 1.0f, 1.0f};
+    f3 origin, direction, previous_position, previous_normal;
+    float previous_pdf = 0.0f;
+    uint32_t bounce = 0;
+    bool done = false;
+};
+
+// voxel_path.wgsl:418-428
+static PathState begin_path(f3 start, f3 direction, f3 normal) {
+    PathState s;
+    s.origin = start;
+    s.direction = direction;
+    s.previous_normal = normal;
+    s.previous_pdf = cosine_pdf(normal, direction);
+    s.previous_position = sub(start, muls(normal, 0.001f));
+    s.done = s.previous_pdf <= 0.0f;
+    return s;
+}
+
+// voxel_path.wgsl:429-492
+static PathState advance_path(Ctx& x, PathState state, uint32_t stream, uint32_t sequence, uint32_t steps, bool terminal) {
+    if (state.done) return state;
+    for (uint32_t step = 0; step < steps; ++step) {
+        uint32_t bounce = state.bounce;
+        state.done = true;
+        RayResult hit = trace_diffuse(x, state.origin, state.direction);
+        if (hit.status == 0u) {
+            float horizon = wclamp(state.direction.y * 0.35f + 0.65f, 0.15f, 1.0f);
+            F4 env{x.env(0), x.env(1), x.env(2), x.env(3)};
+            state.result.energy.value = f4add(state.result.energy.value, f4muls(f4mul(state.throughput, env), horizon));
+            break;
+        }
+        if (hit.status == 2u) { state.result.unknown = true; break; }
+        if (hit.status == 3u) break;
+        const float* mat = material(x, hit.material);
+        F4 diffuse = ld4(mat), emission = ld4(mat + 8);
+        Energy direct = direct_at(x, hit.position, hit.normal);
+        float emission_weight = mat[13];
+        f3 delta = sub(hit.position, state.origin);
+        float selection_pdf = emission_weight / wmax(x.extra(2), 1e-20f);
+        if (emission_weight > 0.0f && x.extra(3) > 0.0f && load_emitter(x, 0).sampling.w > 0.0f)
+            selection_pdf = tree_probability(x, state.previous_position, state.previous_normal, hit.voxel, hit.normal);
+        float light_pdf = selection_pdf * dot(delta, delta) / wmax(dot(hit.normal, neg(state.direction)), 1e-8f);
+        float mis = 1.0f;
+        if (light_pdf > 0.0f) mis = state.previous_pdf / (state.previous_pdf + light_pdf);
+        Cached cached = cached_energy(x, hit.voxel, face_index_of(hit.normal));
+        if (cached.found) {
+            x.c.cache_hits += 1;
+            F4 term = f4add(f4muls(emission, mis), f4mul(diffuse, f4add(direct.value, cached.value)));
+            state.result.energy.value = f4add(state.result.energy.value, f4mul(state.throughput, term));
+            break;
+        }
+        Energy nee;
+        if (terminal && step + 1u == steps) nee = sample_terminal_emission(x, hit.position, hit.normal, stream, sequence, bounce);
+        else nee = sample_emitter(x, hit.position, hit.normal, stream, sequence, bounce + 1u);
+        F4 term = f4add(f4muls(emission, mis), f4mul(diffuse, f4add(direct.value, nee.value)));
+        state.result.energy.value = f4add(state.result.energy.value, f4mul(state.throughput, term));
+        if (terminal && step + 1u == steps) break;
+        state.throughput = f4mul(state.throughput, diffuse);
+        float maximum = wmax(state.throughput.x, wmax(state.throughput.y, state.throughput.z));
+        if (maximum == 0.0f) break;
+        if (bounce >= 1u) {
+            float survival = wclamp(maximum, 0.1f, 0.95f);
+            if (continuation_sample(stream, sequence, bounce, 2u) > survival) break;
+            state.throughput = f4divs(state.throughput, survival);
+        }
+        state.origin = add(hit.position, muls(hit.normal, 0.002f));
+        state.previous_position = hit.position;
+        state.previous_normal = hit.normal;
+        state.direction = hemisphere(hit.normal, continuation_sample(stream, sequence, bounce, 0u), continuation_sample(stream, sequence, bounce, 1u));
+        state.previous_pdf = cosine_pdf(hit.normal, state.direction);
+        if (state.previous_pdf <= 0.0f) break;
+        state.bounce += 1u;
+        state.done = false;
+    }
+    return state;
+}
+
+// voxel_path.wgsl:504-520
+struct ReceiverSample { F4 energy; bool known; };
+static ReceiverSample trace_receiver(Ctx& x, f3 surface, f3 normal, uint32_t stream, uint32_t sequence) {
+    x.c.paths += 1;
+    f3 direction = hemisphere(normal, sample_1d(stream, sequence, 0u), sample_1d(stream, sequence, 1u));
+    Energy emitter = sample_emitter(x, surface, normal, stream, sequence, 0u);
+    PathEnergy continuation;
+    if (dot(normal, direction) > 0.0f) {
+        PathState st = begin_path(add(surface, muls(normal, 0.001f)), direction, normal);
+        continuation = advance_path(x, st, stream, sequence, x.m.pipe.diffuse_hits, true).result;
+    }
+    ReceiverSample r;
+    r.known = !continuation.unknown;
+    r.energy = f4add(emitter.value, continuation.energy.value);
+    if (continuation.unknown) x.c.unknown += 1;
+    return r;
+}
+
+// voxel_trace.wgsl:44-59 (one lane's strided subsequence)
+struct Moments { F4 mean{0, 0, 0, 0}; F4 second{0, 0, 0, 0}; uint32_t known = 0; };
+static Moments trace_moments(Ctx& x, const uint32_t* task, uint32_t first, uint32_t step) {
+    Moments m;
+    i3 voxel{(int32_t)task[0], (int32_t)task[1], (int32_t)task[2]};
+    f3 normal = face_normal(task[3]);
+    f3 surface = add(adds(tof(voxel), 0.5f), muls(normal, 0.5f));
+    uint32_t stream = hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(task[3] + 1u);
+    for (uint32_t i = first; i < x.pcount(1); i += step) {
+        ReceiverSample s = trace_receiver(x, surface, normal, stream, task[4] + i);
+        if (!s.known) continue;
+        m.mean = f4add(m.mean, s.energy);
+        m.second = f4add(m.second, f4mul(s.energy, s.energy));
+        m.known += 1u;
+    }
+    return m;
+}
+
+// voxel_trace.wgsl:25-37
+static void write_result(Ctx& x, const uint32_t* task, const Moments& m, uint32_t* out) {
+    f3 normal = face_normal(task[3]);
+    i3 voxel{(int32_t)task[0], (int32_t)task[1], (int32_t)task[2]};
+    Energy direct = direct_at(x, add(adds(tof(voxel), 0.5f), muls(normal, 0.5f)), normal);
+    float inverse = 1.0f / (float)umax(m.known, 1u);
+    F4 mean = f4muls(m.mean, inverse), second = f4muls(m.second, inverse);
+    float vals[24] = {mean.x, mean.y, mean.z, mean.w, 0.0f, (float)m.known, 0.0f, 0.0f,
+                      second.x, second.y, second.z, second.w, 0.0f, 0.0f, 0.0f, 0.0f,
+                      direct.value.x, direct.value.y, direct.value.z, direct.value.w,
+                      0.0f, direct.custom.x, direct.custom.y, direct.custom.z};
+    for (int i = 0; i < 24; ++i) out[i] = fbits(vals[i]);
+    out[12] = out[13] = out[14] = out[15] = 0u;
+    x.c.bytes += 96 + 32;
+}
+
+static void add_counters(Counters& a, const Counters& b) {
+    a.rays += b.rays; a.paths += b.paths; a.steps += b.steps; a.bytes += b.bytes;
+    a.unknown += b.unknown; a.cache_hits += b.cache_hits;
+    for (int i = 0; i < 4; ++i) a.status[i] += b.status[i];
+}
+
+// ---- voxel_retention.wgsl / voxel_accumulate.wgsl ----------------------------
+static const uint32_t NO_LIMIT = 0xffffffffu;
+static uint32_t curve_limit(uint32_t d2) {
+    if (d2 >= 36864u) return NO_LIMIT;
+    return (d2 * d2 + 10368u) / 20736u;
+}
+static uint32_t box_distance2(const int32_t lo[3], const int32_t hi[3], const int32_t p[3]) {
+    uint32_t s = 0;
+    for (int a = 0; a < 3; ++a) {
+        int32_t v = imax(imax(lo[a] - p[a], p[a] - hi[a]), 0);
+        v = imin(v, 4096);
+        s += (uint32_t)v * (uint32_t)v;
+    }
+    return s;
+}
+static float load_height(int32_t top, int32_t y) {
+    int32_t v = top + 1 - y;
+    v = v < 0 ? 0 : (v > 16 ? 16 : v);
+    return (float)v;
+}
+struct Retention { uint32_t limit; float change; bool measured, woken, urgent, urgent_if_binding; };
+
+// voxel_retention.wgsl:29-96
+static Retention resolve_retention(const uint32_t* events, const int32_t p[3], uint32_t event_count, uint32_t reach,
+                                   bool measured_mode, uint32_t urgent_measured, uint32_t urgent_curve) {
+    uint32_t cap = NO_LIMIT;
+    float change = 0.0f;
+    bool known = true;
+    uint32_t source_cap = NO_LIMIT;
+    bool woken = false, urgent_if_binding = false, urgent = false;
+    const float PI = 3.14159265358979f;
+    for (uint32_t e = 0; e < event_count; ++e) {
+        const uint32_t* h0 = events + (size_t)(e * 3u) * 4;
+        const uint32_t* h1 = h0 + 4;
+        const uint32_t* h2 = h0 + 8;
+        if ((h0[3] & 2u) != 0u) {
+            uint32_t limit = h2[0];
+            for (uint32_t b = 0; b < h2[3]; ++b) {
+                const uint32_t* s = events + (size_t)(event_count * 3u + (h2[2] + b) * 2u) * 4;
+                f3 d = sub(f3{(float)p[0], (float)p[1], (float)p[2]}, f3{bitsf(s[0]), bitsf(s[1]), bitsf(s[2])});
+                if (dot(d, d) <= bitsf(s[3])) limit = umin(limit, 4u);
+            }
+            source_cap = umin(source_cap, limit);
+            woken = true;
+            continue;
+        }
+        int32_t lo[3] = {(int32_t)h0[0], (int32_t)h0[1], (int32_t)h0[2]};
+        int32_t hi[3] = {(int32_t)h1[0], (int32_t)h1[1], (int32_t)h1[2]};
+        uint32_t outside = box_distance2(lo, hi, p);
+        if (outside > reach) continue;
+        woken = true;
+        bool exact = known;
+        uint32_t nearest = NO_LIMIT;
+        for (uint32_t b = 0; b < h2[3]; ++b) {
+            size_t record = (size_t)event_count * 3u + (h2[2] + b) * 2u;
+            const uint32_t* b0 = events + record * 4;
+            const uint32_t* b1 = b0 + 4;
+            int32_t blo[3] = {(int32_t)b0[0], (int32_t)b0[1], (int32_t)b0[2]};
+            int32_t bhi[3] = {(int32_t)b1[0], (int32_t)b1[1], (int32_t)b1[2]};
+            uint32_t d = box_distance2(blo, bhi, p);
+            if (d > reach) continue;
+            nearest = umin(nearest, d);
+            uint32_t edit_kind = b1[3] & 7u;
+            if ((b1[3] & 8u) != 0u && (edit_kind == 0u || edit_kind == 3u)) {
+                if (edit_kind == 3u && measured_mode) urgent_if_binding = urgent_if_binding || d <= urgent_measured;
+                else urgent = urgent || d <= urgent_curve;
+            }
+            if (exact) {
+                uint32_t kind = b1[3] & 7u;
+                if (kind == 0u) { known = false; exact = false; }
+                else if (kind != 1u) {
+                    float area = kind == 2u ? load_height(((int32_t)b1[3]) >> 3, p[1]) : 1.0f;
+                    change = change + bitsf(b0[3]) * area / (PI * (float)umax(d, 1u));
+                }
+            }
+        }
+        if (nearest != NO_LIMIT) cap = umin(cap, curve_limit(nearest));
+    }
+    bool measured = measured_mode && known;
+    uint32_t limit = umin(source_cap, measured ? NO_LIMIT : cap);
+    return Retention{limit, change, measured, woken, urgent, urgent_if_binding};
+}
+
+static inline float lum(F4 v) { return 0.2126f * v.x + 0.7152f * v.y + 0.0722f * v.z; }
+static inline float max3(float a, float b, float c) { return wmax(a, wmax(b, c)); }
+static F4 stF4(const uint32_t* s) { return F4{bitsf(s[0]), bitsf(s[1]), bitsf(s[2]), bitsf(s[3])}; }
+static void putF4(uint32_t* s, F4 v) { s[0] = fbits(v.x); s[1] = fbits(v.y); s[2] = fbits(v.z); s[3] = fbits(v.w); }
+
+// voxel_accumulate.wgsl:336-344 (controls: display.w = c)
+static bool binds(const uint32_t* state, uint32_t slot, float change, float physical) {
+    const uint32_t* base = state + (size_t)slot * 36;
+    F4 mean = stF4(base);
+    F4 second = stF4(base + 8);
+    F4 variance{wmax(second.x - mean.x * mean.x, 0.0f), wmax(second.y - mean.y * mean.y, 0.0f), wmax(second.z - mean.z * mean.z, 0.0f), 0};
+    bool lit = lum(mean) >= 0.05f * change;
+    float keep = physical * lum(variance) / wmax(change * change, 1e-30f);
+    return !lit || keep < (float)(base[5] & 0x7fffffffu);
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+static Geometry make_geometry(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells,
+                              const float* params) {
+    Geometry g;
+    g.directory = directory; g.headers = headers; g.cells = cells;
+    g.mask = (uint32_t)(slots - 1);
+    for (int a = 0; a < 3; ++a) { g.mn[a] = (int32_t)fbits(params[4 + a]); g.mx[a] = (int32_t)fbits(params[8 + a]); }
+    return g;
+}
+
+extern "C" {
+
+// trace_faces / trace_faces_parallel (voxel_trace.wgsl:62-92): `tasks` holds
+// 8 words per face (voxel xyz, face, sequence, padding); `results` receives 24
+// words per face (FaceResult). With pipe->lanes = L, lane l of a face traces
+// samples l, l+L, ... and lane 0 sums the lanes in order, as the cooperative
+// kernel does; L = 1 is the serial kernel. `state` (36 words per slot) and
+// `index` (face index words) may be null for a cacheless trace.
+int orc_trace_faces(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells,
+                    const float* params, const float* materials, const float* lights, const uint32_t* emitters,
+                    const uint32_t* state, const uint32_t* index, const uint32_t* tasks, uint32_t n_tasks,
+                    const orc_pipeline* pipe, uint32_t* results, orc_counters* counters, int threads) {
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, materials, lights, emitters, state, index, *pipe};
+    uint32_t lanes = pipe->lanes == 0 ? 1 : pipe->lanes;
+    Counters total;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::vector<Counters> per((size_t)threads);
+    std::atomic<uint64_t> next{0};
+    auto worker = [&](int tid) {
+        for (;;) {
+            uint64_t first = next.fetch_add(16);
+            if (first >= n_tasks) break;
+            uint64_t last = std::min<uint64_t>(first + 16, n_tasks);
+            for (uint64_t t = first; t < last; ++t) {
+                Ctx x{g, m, Counters{}};
+                const uint32_t* task = tasks + (size_t)t * 8;
+                if (task[3] == 0xffffffffu) continue;
+                Moments total_m;
+                for (uint32_t l = 0; l < lanes; ++l) {
+                    Moments lm = trace_moments(x, task, l, lanes);
+                    total_m.mean = f4add(total_m.mean, lm.mean);
+                    total_m.second = f4add(total_m.second, lm.second);
+                    total_m.known += lm.known;
+                }
+                write_result(x, task, total_m, results + (size_t)t * 24);
+                add_counters(per[(size_t)tid], x.c);
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker, t);
+    worker(0);
+    for (auto& th : pool) th.join();
+    for (auto& c : per) add_counters(total, c);
+    if (counters) {
+        counters->rays = total.rays; counters->paths = total.paths; counters->steps = total.steps;
+        counters->bytes = total.bytes; counters->unknown = total.unknown; counters->cache_hits = total.cache_hits;
+        for (int i = 0; i < 4; ++i) counters->status[i] = total.status[i];
+    }
+    return 0;
+}
+
+// One ray through trace_domain_limited (for traversal parity tests):
+// out = [voxel xyz, material, position xyz (bits), status, normal xyz (bits), steps].
+int orc_trace_ray(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells,
+                  const float* params, const float* ray, uint32_t visible_geometry, uint32_t max_steps, uint32_t* out) {
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, nullptr, nullptr, nullptr, nullptr, nullptr, orc_pipeline{1, 0, max_steps, 0, 1}};
+    Ctx x{g, m, Counters{}};
+    RayResult r = trace_domain_limited(x, f3{ray[0], ray[1], ray[2]}, f3{ray[3], ray[4], ray[5]}, ray[6], visible_geometry != 0, max_steps);
+    uint32_t v[12] = {(uint32_t)r.voxel.x, (uint32_t)r.voxel.y, (uint32_t)r.voxel.z, r.material, fbits(r.position.x), fbits(r.position.y),
+                      fbits(r.position.z), r.status, fbits(r.normal.x), fbits(r.normal.y), fbits(r.normal.z), (uint32_t)x.c.steps};
+    for (int i = 0; i < 12; ++i) out[i] = v[i];
+    return 0;
+}
+
+// advance_box (voxel_traversal.wgsl:90-107) on one case:
+// in = [position xyz, size, direction xyz, cell xyz (as int bits), negative xyz, positive xyz]
+int orc_advance_box(const float* in, float* out) {
+    const uint32_t* u = (const uint32_t*)in;
+    F4 r = advance_box(f3{in[0], in[1], in[2]}, f3{in[4], in[5], in[6]}, i3{(int32_t)u[7], (int32_t)u[8], (int32_t)u[9]},
+                       i3{(int32_t)u[10], (int32_t)u[11], (int32_t)u[12]}, i3{(int32_t)u[13], (int32_t)u[14], (int32_t)u[15]}, in[3]);
+    out[0] = r.x; out[1] = r.y; out[2] = r.z; out[3] = r.w;
+    return 0;
+}
+
+float orc_sample_1d(uint32_t stream, uint32_t sequence, uint32_t dimension) { return sample_1d(stream, sequence, dimension); }
+void orc_hemisphere(const float* n, float u, float v, float* out) {
+    f3 r = hemisphere(f3{n[0], n[1], n[2]}, u, v);
+    out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+void orc_sincos(float x, float* s, float* c) { own_sincos(x, s, c); }
+float orc_exp(float x) { return own_exp(x); }
+uint32_t orc_pcg(uint32_t v) { return pcg(v); }
+uint32_t orc_curve_limit(uint32_t d2) { return curve_limit(d2); }
+
+// prepare for every traced CPU-owned slot (voxel_accumulate.wgsl:114-133):
+// the task takes the slot's current sequence (begin_trace) and the slot's
+// schedule word records the batch id (controls batch.y). slot_meta may be null.
+int orc_begin_trace(const uint32_t* state, uint32_t* slot_meta, uint32_t* tasks, const uint32_t* slots, uint32_t n,
+                    const uint32_t* controls) {
+    for (uint32_t i = 0; i < n; ++i) {
+        tasks[(size_t)i * 8 + 4] = state[(size_t)slots[i] * 36 + 6];
+        if (slot_meta) {
+            uint32_t* sched = slot_meta + ((size_t)slots[i] * 3 + 1) * 4;
+            sched[1] = (sched[1] & 0xfu) | (controls[25] << 4);
+        }
+    }
+    return 0;
+}
+
+// mark_changed (voxel_accumulate.wgsl:432-446); controls = 36 words.
+int orc_mark_changed(uint32_t* state, uint32_t* slot_meta, const uint32_t* slots, uint32_t n, const uint32_t* controls) {
+    float physical = bitsf(controls[11]);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t slot = slots[i];
+        if (slot == 0xffffffffu) continue;
+        uint32_t* meta = slot_meta + ((size_t)slot * 3 + 1) * 4;
+        float pending = bitsf(meta[0]);
+        if (pending <= 0.0f) continue;
+        if (binds(state, slot, pending, physical)) state[(size_t)slot * 36 + 5] |= 0x80000000u;
+        else meta[0] = 0u;
+    }
+    return 0;
+}
+
+static uint32_t required_samples(const uint32_t* controls, F4 mean) {
+    uint32_t s = controls[18];
+    return max3(mean.x, mean.y, mean.z) < 0.02f ? umax(s, 256u) : s;
+}
+static float refinement_error(const uint32_t* base, uint32_t count) {
+    if (count < 2u) return 1.0f;
+    F4 mean = stF4(base), second = stF4(base + 8);
+    float c = (float)count;
+    float e[3];
+    float mv[3] = {mean.x, mean.y, mean.z}, sv[3] = {second.x, second.y, second.z};
+    for (int a = 0; a < 3; ++a) e[a] = std::sqrt(wmax(sv[a] - mv[a] * mv[a], 0.0f) / c) / (0.002f + std::fabs(mv[a]));
+    return wmin(max3(e[0], e[1], e[2]), 8.0f);
+}
+static float sample_noise(const uint32_t* base) {
+    F4 mean = stF4(base), second = stF4(base + 8);
+    float mv[3] = {mean.x, mean.y, mean.z}, sv[3] = {second.x, second.y, second.z}, e[3];
+    for (int a = 0; a < 3; ++a) e[a] = std::sqrt(wmax(sv[a] - mv[a] * mv[a], 0.0f)) / (0.002f + std::fabs(mv[a]));
+    return max3(e[0], e[1], e[2]);
+}
+
+// accumulate (voxel_accumulate.wgsl:135-227) with record_stability (:237-262)
+// for batches of CPU-owned faces only (no GPU picks: batch.x = n).
+// outputs: 24 words per task (FaceResult in, state words 0..5 out).
+int orc_accumulate(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint, uint32_t* outputs, const uint32_t* slots,
+                   uint32_t n, const uint32_t* controls) {
+    const uint32_t MIRROR_STALE = 0x20000000u;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t slot = slots[i];
+        if (i >= controls[0] || slot == 0xffffffffu) continue;
+        uint32_t* base = state + (size_t)slot * 36;
+        uint32_t* out = outputs + (size_t)i * 24;
+        uint32_t* cp = checkpoint + (size_t)slot * 12;
+        for (int k = 0; k < 4; ++k) { cp[k] = base[k]; cp[4 + k] = base[8 + k]; }
+        cp[8] = base[4]; cp[9] = base[5] & 0x7fffffffu; cp[10] = base[12]; cp[11] = 0u;
+        uint32_t fresh = f2u(bitsf(out[5]));
+        uint32_t* meta = slot_meta + ((size_t)slot * 3 + 1) * 4;
+        float pending = bitsf(meta[0]);
+        if (fresh > 0u) meta[0] = 0u;
+        uint32_t previous_count = base[5] & 0x7fffffffu;
+        float physical = bitsf(controls[11]);
+        float change = (base[5] & 0x80000000u) != 0u ? pending : 0.0f;
+        if (physical > 0.0f && fresh > 0u && change > 0.0f) {
+            F4 om = stF4(base), os = stF4(base + 8), fm = stF4(out), fs = stF4(out + 8);
+            F4 ov{wmax(os.x - om.x * om.x, 0.0f), wmax(os.y - om.y * om.y, 0.0f), wmax(os.z - om.z * om.z, 0.0f), 0};
+            F4 fv{wmax(fs.x - fm.x * fm.x, 0.0f), wmax(fs.y - fm.y * fm.y, 0.0f), wmax(fs.z - fm.z * fm.z, 0.0f), 0};
+            float variance = lum(om) < 0.05f * change ? lum(fv) : lum(ov);
+            float keep = physical * variance / (change * change);
+            previous_count = umin(previous_count, f2u(wmin(keep, 65536.0f)));
+            cp[9] = umin(cp[9], previous_count);
+        }
+        uint32_t count = umin(previous_count + fresh, controls[3]);
+        float recency = bitsf(controls[10]);
+        float alpha = fresh > 0u ? wmin(recency * (float)fresh / (float)umax(count, 1u), 1.0f) : 0.0f;
+        F4 mean = stF4(out), second = stF4(out + 8), pm = stF4(base), ps = stF4(base + 8);
+        F4 nm{pm.x + (mean.x - pm.x) * alpha, pm.y + (mean.y - pm.y) * alpha, pm.z + (mean.z - pm.z) * alpha, pm.w + (mean.w - pm.w) * alpha};
+        F4 ns{ps.x + (second.x - ps.x) * alpha, ps.y + (second.y - ps.y) * alpha, ps.z + (second.z - ps.z) * alpha, ps.w + (second.w - ps.w) * alpha};
+        putF4(base, nm);
+        putF4(base + 8, ns);
+        base[5] = count;
+        base[6] += controls[1];
+        for (int k = 0; k < 4; ++k) { base[16 + k] = out[16 + k]; base[20 + k] = out[20 + k]; }
+        F4 radiance = stF4(base), moment = stF4(base + 8);
+        float rv[3] = {radiance.x, radiance.y, radiance.z}, mv[3] = {moment.x, moment.y, moment.z};
+        float cnt = wmax((float)count, 1.0f), u[3], nz[3];
+        for (int a = 0; a < 3; ++a) {
+            float err = std::sqrt(wmax(mv[a] - rv[a] * rv[a], 0.0f) / cnt);
+            u[a] = err / (0.02f + std::fabs(rv[a]));
+            nz[a] = err / (0.002f + std::fabs(rv[a]));
+        }
+        float uncertainty = count < 2u ? 1.0f : wmin(8.0f, max3(u[0], u[1], u[2]));
+        float noise = count < 2u ? 1.0f : wmin(8.0f, max3(nz[0], nz[1], nz[2]));
+        float elapsed = base[30] != 0u ? (float)(controls[2] - base[29]) * 0.001f : 1.0f / 60.0f;
+        float time_alpha = 1.0f - own_exp(-elapsed / bitsf(controls[4]));
+        float evidence = (float)count / ((float)count + 32.0f);
+        float blend = wmin(time_alpha, evidence / (1.0f + 16.0f * noise * noise));
+        F4 previous = stF4(base + 24);
+        float old_weight = (1.0f - blend) / (0.25f + max3(previous.x, previous.y, previous.z));
+        float new_weight = blend / (0.25f + max3(radiance.x, radiance.y, radiance.z));
+        float alpha_display = wmin(blend, new_weight / wmax(old_weight + new_weight, 0.0000001f));
+        float confidence = wclamp((float)count / ((float)count + 8.0f) / (1.0f + uncertainty), 0.125f, 1.0f);
+        // mix(a, b, t) = a * (1 - t) + b * t
+        F4 disp{previous.x * (1.0f - alpha_display) + radiance.x * alpha_display,
+                previous.y * (1.0f - alpha_display) + radiance.y * alpha_display,
+                previous.z * (1.0f - alpha_display) + radiance.z * alpha_display,
+                previous.w * (1.0f - blend) + confidence * blend};
+        putF4(base + 24, disp);
+        base[29] = controls[2];
+        base[30] = 0xffffffffu;
+        base[7] = base[24];
+        base[13] = base[25]; base[14] = base[26]; base[15] = base[27];
+        for (int k = 0; k < 24; ++k) out[k] = base[k];
+        // record_stability (picked = false: batch.x == n)
+        uint32_t* sched = slot_meta + ((size_t)slot * 3 + 1) * 4;
+        uint32_t* rank = slot_meta + ((size_t)slot * 3 + 2) * 4;
+        uint32_t sy = sched[1], sw = sched[3];
+        bool same_revision = (sy & 8u) != 0u && sw == controls[16];
+        uint32_t scount = base[5] & 0x7fffffffu;
+        F4 after = stF4(base);
+        float tolerance = bitsf(controls[17]);
+        float bv[3] = {pm.x, pm.y, pm.z}, av[3] = {after.x, after.y, after.z}, dr[3];
+        for (int a = 0; a < 3; ++a) dr[a] = std::fabs(bv[a] - av[a]) / (0.002f + wmax(std::fabs(bv[a]), std::fabs(av[a])));
+        float drift = max3(dr[0], dr[1], dr[2]);
+        F4 display = stF4(base + 24);
+        bool settled = max3(std::fabs(display.x - after.x), std::fabs(display.y - after.y), std::fabs(display.z - after.z)) <=
+                       0.001f + max3(after.x, after.y, after.z) * tolerance * 0.5f;
+        uint32_t stable = (same_revision && settled && scount >= required_samples(controls, after) &&
+                           refinement_error(base, scount) <= tolerance && drift <= tolerance * 0.5f)
+                              ? umin((sy & 7u) + 1u, 4u)
+                              : 0u;
+        sched[1] = (sy & 0xfffffff0u) | 8u | stable;
+        sched[3] = controls[16];
+        uint32_t old_rank_w = rank[3];
+        rank[0] = fbits(sample_noise(base));
+        rank[1] = controls[2];
+        rank[2] = fbits(max3(after.x, after.y, after.z));
+        rank[3] = 0x80000000u | scount | (old_rank_w & MIRROR_STALE);
+        // settled_flag
+        if ((sched[1] & 15u) == 12u) out[5] |= 0x80000000u;
+    }
+    return 0;
+}
+
+// apply_events (voxel_accumulate.wgsl:295-332) over slots [0, n_slots).
+int orc_apply_events(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint, const uint32_t* events, uint32_t n_slots,
+                     const uint32_t* controls) {
+    const uint32_t URGENT = 0x40000000u;
+    float physical = bitsf(controls[11]);
+    for (uint32_t slot = 0; slot < n_slots; ++slot) {
+        uint32_t* identity = slot_meta + (size_t)slot * 12;
+        if ((identity[3] & 8u) == 0u) continue;
+        int32_t p[3] = {(int32_t)identity[0], (int32_t)identity[1], (int32_t)identity[2]};
+        Retention r = resolve_retention(events, p, controls[13], controls[15], physical > 0.0f, controls[30], controls[31]);
+        bool urgent = r.urgent;
+        if (r.limit != NO_LIMIT) {
+            uint32_t* base = state + (size_t)slot * 36;
+            base[5] = umin(base[5], r.limit);
+            uint32_t* rank = slot_meta + ((size_t)slot * 3 + 2) * 4;
+            rank[3] = (rank[3] & 0xe0000000u) | (base[5] & 0x1fffffffu);
+            checkpoint[(size_t)slot * 12 + 9] = umin(checkpoint[(size_t)slot * 12 + 9], r.limit);
+        }
+        uint32_t* sched = slot_meta + ((size_t)slot * 3 + 1) * 4;
+        if (r.measured && r.change > 0.0f) sched[0] = fbits(bitsf(sched[0]) + r.change);
+        if (r.urgent_if_binding) {
+            float pending = bitsf(sched[0]);
+            urgent = urgent || !r.measured || (pending > 0.0f && binds(state, slot, pending, physical));
+        }
+        if (r.woken || urgent) sched[1] &= 0xfffffff0u;
+        if (urgent) slot_meta[((size_t)slot * 3 + 2) * 4 + 3] |= URGENT;
+    }
+    return 0;
+}
+
+// The (voxel, face) -> slot index as the worker builds it (face_index.rs:36-97):
+// capacity 1024, doubled before an insert would exceed half load; faces
+// inserted in slot order. out: words of [mask, 64, 0, 0] then entries;
+// returns the number of uint4 words written (capacity + 1), or -1 if
+// `out_capacity` is too small.
+namespace {
+struct FaceTable {
+    std::vector<uint32_t> e;
+    uint64_t len = 0;
+    explicit FaceTable(uint64_t cap) : e(cap * 4, 0) { for (uint64_t i = 0; i < cap; ++i) e[i * 4 + 3] = 0xffffffffu; }
+    uint64_t cap() const { return e.size() / 4; }
+    void insert(int32_t x, int32_t y, int32_t z, uint32_t face, uint32_t slot) {
+        uint64_t mask = cap() - 1;
+        uint64_t home = (hash_voxel(x, y, z) ^ pcg(face + 1u)) & mask;
+        for (uint64_t j = home;; j = (j + 1) & mask) {
+            if (e[j * 4 + 3] == 0xffffffffu) break;
+            if ((int32_t)e[j * 4] == x && (int32_t)e[j * 4 + 1] == y && (int32_t)e[j * 4 + 2] == z && (e[j * 4 + 3] >> 29) == face) {
+                e[j * 4 + 3] = (face << 29) | slot;
+                return;
+            }
+        }
+        if ((len + 1) * 2 > cap()) { grow(); mask = cap() - 1; home = (hash_voxel(x, y, z) ^ pcg(face + 1u)) & mask; }
+        uint64_t idx = home;
+        while (e[idx * 4 + 3] != 0xffffffffu) idx = (idx + 1) & mask;
+        e[idx * 4] = (uint32_t)x; e[idx * 4 + 1] = (uint32_t)y; e[idx * 4 + 2] = (uint32_t)z;
+        e[idx * 4 + 3] = (face << 29) | slot;
+        len += 1;
+    }
+    void grow() {
+        std::vector<uint32_t> old;
+        old.swap(e);
+        uint64_t old_cap = old.size() / 4;
+        e.assign(old_cap * 2 * 4, 0);
+        for (uint64_t i = 0; i < old_cap * 2; ++i) e[i * 4 + 3] = 0xffffffffu;
+        len = 0;
+        for (uint64_t i = 0; i < old_cap; ++i)
+            if (old[i * 4 + 3] != 0xffffffffu)
+                insert((int32_t)old[i * 4], (int32_t)old[i * 4 + 1], (int32_t)old[i * 4 + 2], old[i * 4 + 3] >> 29,
+                       old[i * 4 + 3] & 0x1fffffffu);
+    }
+};
+}  // namespace
+
+int64_t orc_face_index(const int32_t* faces /*4 per face: xyz, face*/, uint32_t n, uint32_t* out, uint64_t out_capacity) {
+    FaceTable t(1024);
+    for (uint32_t s = 0; s < n; ++s) {
+        const int32_t* f = faces + (size_t)s * 4;
+        t.insert(f[0], f[1], f[2], (uint32_t)f[3], s);
+    }
+    uint64_t cap = t.cap();
+    if (cap + 1 > out_capacity) return -1;
+    out[0] = (uint32_t)(cap - 1); out[1] = 64; out[2] = 0; out[3] = 0;
+    std::copy(t.e.begin(), t.e.end(), out + 4);
+    return (int64_t)(cap + 1);
+}
+
+}  // extern "C"

@@ -1,0 +1,300 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+Test infrastructure only: the oracle is the checker the CUDA path is compared
+with; nothing in the product imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_PATH = os.path.join(ORACLE_DIR, "liboracle.so")
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+_I64 = ctypes.c_int64
+_INT = ctypes.c_int
+_F = ctypes.c_float
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [("rays", _U64), ("paths", _U64), ("steps", _U64), ("bytes", _U64), ("unknown", _U64),
+                ("cache_hits", _U64), ("status", _U64 * 4)]
+
+    def as_dict(self):
+        d = {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "status"}
+        d["status"] = [int(v) for v in self.status]
+        return d
+
+
+class Pipeline(ctypes.Structure):
+    _fields_ = [("diffuse_hits", _U32), ("limited_reach", _U32), ("path_steps", _U32), ("budgeted", _U32), ("lanes", _U32)]
+
+
+_SIG = {
+    "orc_build_aadf": (_INT, [_U32, _U32, _U32, _P, _P]),
+    "orc_scene_create": (_INT, [_P, _U32, _P, _P, _INT, _P]),
+    "orc_scene_free": (None, [_P]),
+    "orc_scene_edit": (_INT, [_P, _P, _U32]),
+    "orc_scene_info": (_INT, [_P, _P, _P]),
+    "orc_scene_copy": (_INT, [_P, _P, _P, _P]),
+    "orc_scene_top_level": (_INT, [_P, _P]),
+    "orc_canonical": (_INT, [_P, _U64, _P, _P, _U64, _P, _U32, _P]),
+    "orc_trace_faces": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _INT]),
+    "orc_trace_ray": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P]),
+    "orc_advance_box": (_INT, [_P, _P]),
+    "orc_sample_1d": (_F, [_U32, _U32, _U32]),
+    "orc_hemisphere": (None, [_P, _F, _F, _P]),
+    "orc_sincos": (None, [_F, _P, _P]),
+    "orc_exp": (_F, [_F]),
+    "orc_pcg": (_U32, [_U32]),
+    "orc_curve_limit": (_U32, [_U32]),
+    "orc_begin_trace": (_INT, [_P, _P, _P, _P, _U32, _P]),
+    "orc_mark_changed": (_INT, [_P, _P, _P, _U32, _P]),
+    "orc_accumulate": (_INT, [_P, _P, _P, _P, _P, _U32, _P]),
+    "orc_apply_events": (_INT, [_P, _P, _P, _P, _U32, _P]),
+    "orc_face_index": (_I64, [_P, _U32, _P, _U64]),
+    "orc_emitters": (_I64, [_P, _U32, _P, _P, _P, _U64, _P]),
+}
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_PATH):
+            build()
+        l = ctypes.CDLL(ORACLE_PATH)
+        for name, (res, args) in _SIG.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def ptr(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def c(a, dtype):
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype))
+
+
+def f2u(x: float) -> int:
+    return struct.unpack("<I", struct.pack("<f", x))[0]
+
+
+# ---- geometry -------------------------------------------------------------
+
+def build_aadf(size, blocked):
+    sx, sy, sz = size
+    b = c(blocked, np.uint8).reshape(-1)
+    out = np.zeros(b.size * 6, np.uint8)
+    lib().orc_build_aadf(sx, sy, sz, ptr(b), ptr(out))
+    return out.reshape(-1, 6)
+
+
+class Scene:
+    """The reference's packing of a region list (PackedScene over a scene
+    built from nothing): directory, headers, cells and region bounds."""
+
+    def __init__(self, coords, voxels, top_mode: int = 0, strides=None):
+        coords = c(coords, np.int32).reshape(-1, 3)
+        voxels = c(voxels, np.uint16).reshape(-1)
+        st = None if strides is None else c(strides, np.uint8)
+        h = ctypes.c_void_p()
+        rc = lib().orc_scene_create(ptr(coords), coords.shape[0], ptr(voxels), ptr(st), top_mode, ctypes.byref(h))
+        assert rc == 0, rc
+        self._h = h
+        self.coords = coords
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_scene_free(self._h)
+            self._h = None
+
+    def edit(self, edits) -> None:
+        e = c(edits, np.int32).reshape(-1, 4)
+        assert lib().orc_scene_edit(self._h, ptr(e), e.shape[0]) == 0
+
+    def arrays(self):
+        sizes = np.zeros(3, np.uint64)
+        bounds = np.zeros(6, np.int32)
+        lib().orc_scene_info(self._h, ptr(sizes), ptr(bounds))
+        d = np.zeros(int(sizes[0]) * 4, np.int32)
+        h = np.zeros(int(sizes[1]) * 4, np.uint32)
+        cl = np.zeros(max(int(sizes[2]), 1), np.uint32)
+        lib().orc_scene_copy(self._h, ptr(d), ptr(h), ptr(cl))
+        return d, h, cl[: int(sizes[2])], bounds
+
+    def top_level(self):
+        bounds = self.arrays()[3]
+        n = int(np.prod(bounds[3:] - bounds[:3] + 1))
+        out = np.zeros(n * 6, np.uint8)
+        rc = lib().orc_scene_top_level(self._h, ptr(out))
+        return None if rc == 1 else out.reshape(-1, 6)
+
+
+def canonical(directory, headers, cells, coords):
+    d = c(directory, np.int32).reshape(-1)
+    h = c(headers, np.uint32).reshape(-1)
+    cl = c(cells, np.uint32).reshape(-1)
+    if cl.size == 0:
+        cl = np.zeros(1, np.uint32)
+    co = c(coords, np.int32).reshape(-1, 3)
+    out = np.zeros((co.shape[0], 4 + 64 * 33), np.uint32)
+    rc = lib().orc_canonical(ptr(d), d.size // 4, ptr(h), ptr(cl), cells.size, ptr(co), co.shape[0], ptr(out))
+    assert rc == 0, rc
+    return out
+
+
+# ---- model words ------------------------------------------------------------
+
+def params_words(n_tasks, samples, dir_slots, n_lights, bounds, n_directional, environment=(0, 0, 0), emitter_total=0.0,
+                 emitter_count=0, reach=768.0):
+    """GpuParams (src/gpu.rs:771-791) as 24 little-endian words in a float32 array."""
+    w = np.zeros(24, np.uint32)
+    w[0:4] = [n_tasks, samples, dir_slots - 1, n_lights]
+    w[4:7] = np.asarray(bounds[:3], np.int32).view(np.uint32)
+    w[8:11] = np.asarray(bounds[3:6], np.int32).view(np.uint32)
+    w[11] = n_directional
+    f = w.view(np.float32)
+    f[12:15] = environment
+    f[15] = 0.0
+    f[16] = 0.0
+    f[17] = 768.0
+    f[18] = emitter_total
+    f[19] = float(emitter_count)
+    f[20] = min(max(reach, 1.0), 768.0)
+    return f
+
+
+def emitters(coords, voxels, materials):
+    co = c(coords, np.int32).reshape(-1, 3)
+    vx = c(voxels, np.uint16).reshape(-1)
+    m = c(materials, np.float32).reshape(-1)
+    info = np.zeros(3, np.uint32)
+    n = lib().orc_emitters(ptr(co), co.shape[0], ptr(vx), ptr(m), None, 0, ptr(info))
+    out = np.zeros(n, np.uint32)
+    lib().orc_emitters(ptr(co), co.shape[0], ptr(vx), ptr(m), ptr(out), n, ptr(info))
+    return out, int(info[0]), float(info[2:3].view(np.float32)[0])
+
+
+def face_index(faces):
+    f = c(faces, np.int32).reshape(-1, 4)
+    cap = 1024
+    while f.shape[0] * 2 > cap:
+        cap *= 2
+    out = np.zeros((cap * 4 + 1) * 4, np.uint32)
+    n = lib().orc_face_index(ptr(f), f.shape[0], ptr(out), out.size // 4)
+    assert n > 0
+    return out[: n * 4].reshape(-1, 4)
+
+
+def trace_faces(geometry, params, materials, lights, emitter_words, tasks, pipe: Pipeline, state=None, index=None, threads=0):
+    d, h, cl, _ = geometry
+    d = c(d, np.int32)
+    h = c(h, np.uint32)
+    cl = c(cl, np.uint32) if len(cl) else np.zeros(1, np.uint32)
+    t = c(tasks, np.uint32).reshape(-1, 8)
+    out = np.zeros((t.shape[0], 24), np.uint32)
+    cnt = Counters()
+    lights = c(lights, np.float32).reshape(-1)
+    if lights.size == 0:
+        lights = np.zeros(12, np.float32)
+    rc = lib().orc_trace_faces(ptr(d), d.size // 4, ptr(h), ptr(cl), ptr(c(params, np.float32)), ptr(c(materials, np.float32)),
+                               ptr(lights), ptr(c(emitter_words, np.uint32)),
+                               ptr(None if state is None else c(state, np.uint32)), ptr(None if index is None else c(index, np.uint32)),
+                               ptr(t), t.shape[0], ctypes.byref(pipe), ptr(out), ctypes.byref(cnt), threads)
+    assert rc == 0
+    return out, cnt.as_dict()
+
+
+def controls_words(n, samples, clock_ms, transport, batch_id=1, n_events=0):
+    """The Controls words the product's frame uses (src/gpu/resident.rs:708-760)."""
+    w = np.zeros(36, np.uint32)
+    w[0] = n
+    w[1] = samples
+    w[2] = clock_ms
+    hl = transport.history_limit
+    w[3] = 65536 if hl == 0 else min(hl, 65536)
+    w[4] = f2u(max(transport.response_seconds, 0.001))
+    w[5] = n
+    w[10] = f2u(transport.recency if transport.recency >= 1.0 else 1.0)
+    w[11] = f2u(max(transport.measured_retention, 0.0))
+    w[13] = n_events
+    w[14] = n
+    w[15] = 192 * 192
+    w[16] = transport.transport_revision
+    w[17] = f2u(transport.stable_error)
+    w[18] = transport.stable_samples
+    w[24] = n
+    w[25] = batch_id
+    w[30] = 64 * 64
+    w[31] = 48 * 48
+    return w
+
+
+class Frames:
+    """The product's per-frame sequence on the CPU: begin_trace, mark_changed,
+    trace (with cache gather), accumulate; state laid out as the reference's
+    resident records."""
+
+    def __init__(self, geometry, params_fn, materials, lights, emitter_words, faces, transport, pipe: Pipeline, threads=0):
+        self.geometry = geometry
+        self.params_fn = params_fn
+        self.materials = materials
+        self.lights = lights
+        self.emitter_words = emitter_words
+        self.faces = np.asarray(faces, np.int32).reshape(-1, 5)
+        n = self.faces.shape[0]
+        self.n = n
+        self.transport = transport
+        self.pipe = pipe
+        self.threads = threads
+        self.state = np.zeros((n, 36), np.uint32)
+        self.meta = np.zeros((n, 12), np.uint32)
+        self.meta[:, 0:3] = self.faces[:, 0:3].view(np.uint32)
+        self.meta[:, 3] = self.faces[:, 3].astype(np.uint32) | 8 | (self.faces[:, 4].astype(np.uint32) << 16)
+        self.checkpoint = np.zeros((n, 12), np.uint32)
+        self.index = face_index(self.faces[:, :4])
+        self.tasks = np.zeros((n, 8), np.uint32)
+        self.tasks[:, 0:3] = self.faces[:, 0:3].view(np.uint32)
+        self.tasks[:, 3] = self.faces[:, 3]
+        self.slots = np.arange(n, dtype=np.uint32)
+        self.batch_id = 1
+        self.results = np.zeros((n, 24), np.uint32)
+
+    def frame(self, samples, clock_ms=0):
+        ctl = controls_words(self.n, samples, clock_ms, self.transport, self.batch_id)
+        L = lib()
+        L.orc_begin_trace(ptr(self.state), ptr(self.meta), ptr(self.tasks), ptr(self.slots), self.n, ptr(ctl))
+        L.orc_mark_changed(ptr(self.state), ptr(self.meta), ptr(self.slots), self.n, ptr(ctl))
+        params = self.params_fn(self.n, samples)
+        out, cnt = trace_faces(self.geometry, params, self.materials, self.lights, self.emitter_words, self.tasks, self.pipe,
+                               self.state, self.index, self.threads)
+        L.orc_accumulate(ptr(self.state), ptr(self.meta), ptr(self.checkpoint), ptr(out), ptr(self.slots), self.n, ptr(ctl))
+        self.results = out
+        self.batch_id = (self.batch_id + 1) & 0x0FFFFFFF or 1
+        return cnt
+
+    def apply_events(self, words, n_events):
+        ctl = controls_words(self.n, 0, 0, self.transport, self.batch_id, n_events)
+        w = c(words, np.uint32)
+        lib().orc_apply_events(ptr(self.state), ptr(self.meta), ptr(self.checkpoint), ptr(w), self.n, ptr(ctl))
