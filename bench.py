@@ -125,7 +125,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total, budget_s=20.0):
+def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total, budget_s=15.0):
     """The oracle on a bounded face sample with the GPU's warm cache state."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
@@ -147,10 +147,12 @@ def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit,
     start = time.perf_counter()
     chunks = 0
     while True:
+        # Successive chunks trace the sample's next frames (sequence + spp).
         _, cnt = O.trace_faces(geometry, params, words, lights, emitters, tasks, pipe, state, index, threads)
+        tasks[:, 4] += SPP
         rays += cnt["rays"]
         chunks += 1
-        if time.perf_counter() - start > budget_s or chunks >= 8:
+        if time.perf_counter() - start > budget_s or chunks >= 1000:
             break
     elapsed = time.perf_counter() - start
     return {"value": rays / elapsed, "unit": "rays/s", "cores": threads, "kind": "port",
@@ -342,6 +344,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "faces": int(n), "spp": SPP, "bounces": BOUNCES, "parallelism": f"independent scene per GPU x{world}",
                        "paths_per_frame": int(paths_per_frame), "rays_per_frame": rays_per_frame,
+                       "census": {"steps": before["steps"], "bytes": before["bytes"], "cache_hits": before["cache_hits"],
+                                  "unknown": before["unknown"], "status": before["status"]},
                        "l2": "256 MB buffer written between timed frames (outside the event pair)",
                        "kernel_ms": {"prepare": float(np.mean([t[0] for t in kernel_ms])), "trace": trace_ms,
                                      "accumulate": float(np.mean([t[2] for t in kernel_ms]))},

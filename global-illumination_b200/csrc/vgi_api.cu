@@ -652,6 +652,7 @@ int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, cudaMemcpyAsync(c->face_index.ptr, index.data(), index.size() * 4, cudaMemcpyHostToDevice, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->n_slots = n;
+    c->batch_id = 1;  // a new face set starts a new batch sequence
     return VGI_OK;
 }
 
