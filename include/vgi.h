@@ -160,6 +160,37 @@ int vgi_read_state(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words36);
 int vgi_write_state(vgi_ctx* ctx, uint32_t first, uint32_t n, const uint32_t* words36);
 int vgi_read_slot_meta(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words12);
 
+/* ---- region packing without allocation -------------------------------------
+ * No counterpart in the reference. This is for callers that must not allocate
+ * device memory. One example is an engine that has reserved all of its GPU
+ * memory through its own allocator and forbids libraries from taking more.
+ * Another is a frame-critical thread, where cudaMalloc's implicit device
+ * synchronisation would stall rendering.
+ *
+ * It packs `n` regions on the calling thread's current device, on `stream`
+ * (a cudaStream_t, 0 for the legacy default stream). The regions are n x 4096
+ * u16 voxels in the caller's device memory, 16-byte aligned, values 0..256.
+ * Outputs, also in the caller's device memory:
+ *   headers: n x 4 u32, 16-byte aligned, (kind, material or cell offset, 0, 0)
+ *            as vgi_upload_regions' packer writes them;
+ *   cells:   `cells_capacity` u32 words.
+ * On success, *cells_used is the number of cell words written. Cells are laid
+ * out in region order, so the layout depends only on the input.
+ *
+ * The call allocates nothing. Its scratch is a static device array sized for
+ * VGI_STATIC_PACK_MAX_REGIONS regions (about 256 KiB per GPU, held until the
+ * process exits). The first call on each device looks up that array's device
+ * address; make it before any stream capture. The call synchronises `stream`.
+ * Every call shares the array, so two calls whose work overlaps on the GPU
+ * race; serialise them on one stream.
+ *
+ * Returns VGI_ERR_CAPACITY for n above the maximum or when cells_capacity is
+ * too small, and VGI_ERR_INVALID for null or misaligned pointers or voxel
+ * values above 256. */
+#define VGI_STATIC_PACK_MAX_REGIONS 65536
+int vgi_pack_regions_static(const uint16_t* voxels, uint32_t n, uint32_t* headers, uint32_t* cells, uint64_t cells_capacity,
+                            uint64_t* cells_used, void* stream);
+
 /* ---- host runtime (no device needed) -------------------------------------- */
 /* Record builders with the host-side conventions of src/gpu.rs:717-760
  * (directional: glam normalize_or_zero of the direction, range -1). */
