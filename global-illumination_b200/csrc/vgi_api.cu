@@ -84,6 +84,7 @@ struct vgi_ctx {
     uint32_t n_lights = 0, n_directional = 0;
     float env[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     DevBuf<uint4> emitters;
+    DevBuf<float4> node_aux;
     float emitter_count = 0.0f, emitter_total = 0.0f;
     vgi_transport transport{};
 
@@ -191,6 +192,7 @@ TraceArgs trace_args(vgi_ctx* c, const uint4* tasks, uint4* results, uint32_t n,
     }
     a.materials = c->materials.ptr;
     a.emitters = c->emitters.ptr;
+    a.node_aux = c->node_aux.ptr;
     a.emitter_count = c->emitter_count;
     a.emitter_total = c->emitter_total;
     a.max_distance = kMaxPathDistance;
@@ -316,6 +318,7 @@ int vgi_create(const vgi_config* config, vgi_ctx** out) {
     int device = config ? config->device : 0;
     if (device < 0 || device >= count) return VGI_ERR_INVALID;
     if (cudaSetDevice(device) != cudaSuccess) return VGI_UNAVAILABLE;
+    if (init_trace_constants() != cudaSuccess) return VGI_ERR_CUDA;
     auto* c = new vgi_ctx();
     c->device = device;
     c->transport = default_transport();
@@ -334,7 +337,7 @@ int vgi_destroy(vgi_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->directory.release(); c->headers.release(); c->cells.release(); c->voxels.release(); c->alloc.release();
     c->pack_error.release(); c->edit_buf.release(); c->zw.release(); c->region_list.release();
-    c->materials.release(); c->lights.release(); c->emitters.release();
+    c->materials.release(); c->lights.release(); c->emitters.release(); c->node_aux.release();
     c->tasks.release(); c->results.release(); c->state.release(); c->slot_meta.release(); c->checkpoint.release();
     c->face_index.release(); c->cache.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
     c->counters.release();
@@ -594,6 +597,10 @@ int vgi_set_emitters(vgi_ctx* c, const uint32_t* words, uint64_t n_words, uint32
     VGI_CUDA(c, cudaSetDevice(c->device));
     VGI_CUDA(c, c->emitters.reserve(n_words / 4));
     VGI_CUDA(c, cudaMemcpyAsync(c->emitters.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    const uint32_t nodes = (uint32_t)((n_words - records * 8) / 16);
+    VGI_CUDA(c, c->node_aux.reserve(2 * (size_t)std::max<uint32_t>(nodes, 1)));
+    launch_node_aux(c->emitters.ptr, (uint32_t)(records * 2), nodes, c->node_aux.ptr, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->emitter_count = (float)n_faces;
     c->emitter_total = total_weight;

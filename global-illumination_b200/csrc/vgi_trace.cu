@@ -24,6 +24,11 @@
 #include "vgi_types.cuh"
 
 namespace vgi {
+
+// Halton scales per dimension: entry k is the reference's `scale` after k + 1
+// divisions by the base (index < 2^24 + 1 has at most 25 base-2 digits).
+__constant__ float c_halton_scale[12][25];
+
 namespace {
 
 constexpr int kBlock = 256;
@@ -137,8 +142,10 @@ __device__ __forceinline__ I3 unpack_bytes(uint32_t v) { return I3{(int)(v & 255
 __device__ __forceinline__ I3 neg_ext(uint32_t b) { return I3{(int)(b & 3u), (int)((b >> 4) & 3u), (int)((b >> 8) & 3u)}; }
 __device__ __forceinline__ I3 pos_ext(uint32_t b) { return I3{(int)((b >> 2) & 3u), (int)((b >> 6) & 3u), (int)((b >> 10) & 3u)}; }
 
+// floor(position / 16.0): dividing by a power of two is exact, so multiplying
+// by 1/16 rounds to the same value.
 __device__ __forceinline__ I3 floor_div16(V3 p) {
-    return I3{f2i(floorf(__fdiv_rn(p.x, 16.0f))), f2i(floorf(__fdiv_rn(p.y, 16.0f))), f2i(floorf(__fdiv_rn(p.z, 16.0f)))};
+    return I3{f2i(floorf(__fmul_rn(p.x, 0.0625f))), f2i(floorf(__fmul_rn(p.y, 0.0625f))), f2i(floorf(__fmul_rn(p.z, 0.0625f)))};
 }
 
 // geometry_ahead (voxel_traversal.wgsl:108-121)
@@ -289,58 +296,53 @@ __device__ __forceinline__ Emissive load_emitter(const TraceArgs& A, uint32_t in
                     make_float4(__uint_as_float(b.x), __uint_as_float(b.y), __uint_as_float(b.z), __uint_as_float(b.w))};
 }
 
-struct Node {
-    float4 mp;       // minimum xyz, power
-    V3 mx;
-    uint32_t normals;
-    I3 pivot;
-    uint32_t face;
-    uint4 children;  // left, right, axis, 0
+// Light-tree nodes (LightNode, voxel_path.wgsl:93-107) are read through a
+// companion record per node, built once per emitter upload by node_aux_kernel:
+//   aux[2i]     = (centre xyz, radius): (min + max) * 0.5 and
+//                 length(max - min) * 0.5, the values node_importance derives
+//                 on every visit, computed with the same operations;
+//   aux[2i + 1] = (power, normals, left, right) as raw words.
+// The walk then moves 16-32 bytes per node instead of 64. The algorithmic
+// byte count still charges the node records the shader loads.
+struct NodeLite {
+    float4 geo;   // centre xyz, radius
+    uint4 link;   // power bits, normals, left, right
 };
 
-template <bool C>
-__device__ __forceinline__ Node load_node(const TraceArgs& A, uint32_t index, Cnt<C>& cnt) {
-    cnt.bytes(64);
-    uint32_t offset = f2u(A.emitter_count) * 2u + index * 4u;
-    uint4 w0 = __ldg(A.emitters + offset), w1 = __ldg(A.emitters + offset + 1u), w2 = __ldg(A.emitters + offset + 2u),
-          w3 = __ldg(A.emitters + offset + 3u);
-    Node n;
-    n.mp = make_float4(__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z), __uint_as_float(w0.w));
-    n.mx = V3{__uint_as_float(w1.x), __uint_as_float(w1.y), __uint_as_float(w1.z)};
-    n.normals = w1.w;
-    n.pivot = I3{(int)w2.x, (int)w2.y, (int)w2.z};
-    n.face = w2.w;
-    n.children = w3;
-    return n;
+__device__ __forceinline__ NodeLite load_lite(const TraceArgs& A, uint32_t index) {
+    return NodeLite{__ldg(A.node_aux + 2u * index), __ldg(reinterpret_cast<const uint4*>(A.node_aux) + 2u * index + 1u)};
 }
 
 // voxel_path.wgsl:108-122
-__device__ float node_importance(const Node& node, V3 position, V3 normal) {
-    V3 mn{node.mp.x, node.mp.y, node.mp.z};
-    V3 delta = (mn + node.mx) * 0.5f - position;
-    float radius = __fmul_rn(len3(node.mx - mn), 0.5f);
+__device__ float node_importance(const NodeLite& node, V3 position, V3 normal) {
+    V3 delta = V3{node.geo.x, node.geo.y, node.geo.z} - position;
+    float radius = node.geo.w;
     float distance = wmax(len3(delta), 1e-5f);
     V3 direction = delta / distance;
     float spread = wmin(__fdiv_rn(radius, distance), 1.0f);
     float receiver = wclamp(__fadd_rn(dot3(normal, direction), spread), 0.0f, 1.0f);
-    float px = (node.normals & 1u) ? -direction.x : -1.0f;
-    float py = (node.normals & 4u) ? -direction.y : -1.0f;
-    float pz = (node.normals & 16u) ? -direction.z : -1.0f;
-    float nx = (node.normals & 2u) ? direction.x : -1.0f;
-    float ny = (node.normals & 8u) ? direction.y : -1.0f;
-    float nz = (node.normals & 32u) ? direction.z : -1.0f;
+    const uint32_t normals = node.link.y;
+    float px = (normals & 1u) ? -direction.x : -1.0f;
+    float py = (normals & 4u) ? -direction.y : -1.0f;
+    float pz = (normals & 16u) ? -direction.z : -1.0f;
+    float nx = (normals & 2u) ? direction.x : -1.0f;
+    float ny = (normals & 8u) ? direction.y : -1.0f;
+    float nz = (normals & 32u) ? direction.z : -1.0f;
     float qx = wmax(px, nx), qy = wmax(py, ny), qz = wmax(pz, nz);
     float emitter = wclamp(__fadd_rn(wmax(wmax(qx, qy), qz), spread), 0.0f, 1.0f);
-    float num = __fmul_rn(__fmul_rn(node.mp.w, receiver), emitter);
+    float num = __fmul_rn(__fmul_rn(__uint_as_float(node.link.x), receiver), emitter);
     float den = __fadd_rn(__fadd_rn(__fmul_rn(distance, distance), __fmul_rn(radius, radius)), 0.25f);
     return __fdiv_rn(num, den);
 }
 
+// voxel_path.wgsl:123-131, given the node's children.
 template <bool C>
-__device__ float node_left_probability(const TraceArgs& A, const Node& node, V3 position, V3 normal, Cnt<C>& cnt) {
-    Node left = load_node(A, node.children.x, cnt);
-    Node right = load_node(A, node.children.y, cnt);
-    float power = __fdiv_rn(left.mp.w, __fadd_rn(left.mp.w, right.mp.w));
+__device__ float node_left_probability(const TraceArgs& A, uint32_t left_index, uint32_t right_index, V3 position, V3 normal, Cnt<C>& cnt) {
+    cnt.bytes(128);  // load_node(left) + load_node(right)
+    const NodeLite left = load_lite(A, left_index);
+    const NodeLite right = load_lite(A, right_index);
+    const float lp = __uint_as_float(left.link.x), rp = __uint_as_float(right.link.x);
+    float power = __fdiv_rn(lp, __fadd_rn(lp, rp));
     float a = node_importance(left, position, normal);
     float b = node_importance(right, position, normal);
     if (__fadd_rn(a, b) <= 1e-20f) return wclamp(power, 1e-6f, 0.999999f);
@@ -356,21 +358,22 @@ __device__ Emissive tree_emitter(const TraceArgs& A, V3 position, V3 normal, flo
     // only guards malformed words: a zero-probability emitter contributes 0.
 #pragma unroll 1
     for (uint32_t depth = 0; depth < 64u; ++depth) {
-        Node node = load_node(A, index, cnt);
-        if (node.children.x == 0xffffffffu) {
-            Emissive e = load_emitter(A, node.children.y, cnt);
+        cnt.bytes(64);  // load_node(index)
+        const uint4 link = __ldg(reinterpret_cast<const uint4*>(A.node_aux) + 2u * index + 1u);
+        if (link.z == 0xffffffffu) {
+            Emissive e = load_emitter(A, link.w, cnt);
             e.sampling.y = probability;
             return e;
         }
-        float p = node_left_probability(A, node, position, normal, cnt);
+        float p = node_left_probability(A, link.z, link.w, position, normal, cnt);
         if (u < p) {
             probability = __fmul_rn(probability, p);
             u = __fdiv_rn(u, p);
-            index = node.children.x;
+            index = link.z;
         } else {
             probability = __fmul_rn(probability, __fsub_rn(1.0f, p));
             u = __fdiv_rn(__fsub_rn(u, p), __fsub_rn(1.0f, p));
-            index = node.children.y;
+            index = link.w;
         }
         u = wmin(u, __uint_as_float(0x3f7fffffu));
     }
@@ -379,15 +382,17 @@ __device__ Emissive tree_emitter(const TraceArgs& A, V3 position, V3 normal, flo
 
 __device__ __forceinline__ int comp(I3 v, uint32_t i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
 
-__device__ __forceinline__ bool key_less(I3 voxel, uint32_t face, const Node& node) {
-    uint32_t axis = node.children.z;
+// key_less (voxel_path.wgsl:150-157) against the node's pivot word (voxel
+// xyz, face) and link word (left, right, axis).
+__device__ __forceinline__ bool key_less(I3 voxel, uint32_t face, uint4 pivot, uint32_t axis) {
+    const I3 p{(int)pivot.x, (int)pivot.y, (int)pivot.z};
 #pragma unroll
     for (uint32_t j = 0; j < 3u; ++j) {
         uint32_t i = (axis + j) % 3u;
-        int a = comp(voxel, i), b = comp(node.pivot, i);
+        int a = comp(voxel, i), b = comp(p, i);
         if (a != b) return a < b;
     }
-    return face < node.face;
+    return face < pivot.w;
 }
 
 template <bool C>
@@ -401,20 +406,23 @@ __device__ float tree_probability(const TraceArgs& A, V3 position, V3 normal, I3
     uint32_t index = 0;
     float probability = 1.0f;
 #pragma unroll 1
+    const uint32_t first_node = f2u(A.emitter_count) * 2u;
     for (uint32_t depth = 0; depth < 64u; ++depth) {
-        Node node = load_node(A, index, cnt);
-        if (node.children.x == 0xffffffffu) {
-            Emissive found = load_emitter(A, node.children.y, cnt);
+        cnt.bytes(64);  // load_node(index)
+        const uint4 pivot = __ldg(A.emitters + first_node + index * 4u + 2u);
+        const uint4 link = __ldg(A.emitters + first_node + index * 4u + 3u);  // left, right, axis
+        if (link.x == 0xffffffffu) {
+            Emissive found = load_emitter(A, link.y, cnt);
             bool same = found.voxel.x == voxel.x && found.voxel.y == voxel.y && found.voxel.z == voxel.z && found.face == face;
             return same ? probability : 0.0f;
         }
-        float p = node_left_probability(A, node, position, normal, cnt);
-        if (key_less(voxel, face, node)) {
+        float p = node_left_probability(A, link.x, link.y, position, normal, cnt);
+        if (key_less(voxel, face, pivot, link.z)) {
             probability = __fmul_rn(probability, p);
-            index = node.children.x;
+            index = link.x;
         } else {
             probability = __fmul_rn(probability, __fsub_rn(1.0f, p));
-            index = node.children.y;
+            index = link.y;
         }
     }
     return 0.0f;
@@ -430,24 +438,45 @@ __device__ __forceinline__ uint32_t scramble_reverse(uint32_t v, uint32_t seed) 
     return v;
 }
 
+// The radical inverse of voxel_path.wgsl:191-198: digit k of `index` in base
+// BASE times scale_k, where scale_k is the k-th value of the reference's
+// running `scale /= f32(base)`. The scales are precomputed with the same IEEE
+// divisions (c_halton_scale), and BASE is a compile-time constant, so each
+// digit costs a multiply-high instead of an integer and a float division.
+template <uint32_t BASE>
+__device__ __forceinline__ float radical_inverse(uint32_t index, const float* scale) {
+    float value = 0.0f;
+    uint32_t k = 0;
+#pragma unroll 1
+    while (index != 0u) {
+        const uint32_t q = index / BASE;
+        value = __fadd_rn(value, __fmul_rn((float)(index - q * BASE), scale[k]));
+        index = q;
+        ++k;
+    }
+    return value;
+}
+
 __device__ float sample_1d(uint32_t stream, uint32_t sequence, uint32_t dimension) {
     if (dimension < 12u) {
-        // primes 2..37
-        const uint32_t base = dimension < 6u ? (dimension < 3u ? (dimension == 0u ? 2u : (dimension == 1u ? 3u : 5u))
-                                                              : (dimension == 3u ? 7u : (dimension == 4u ? 11u : 13u)))
-                                            : (dimension < 9u ? (dimension == 6u ? 17u : (dimension == 7u ? 19u : 23u))
-                                                              : (dimension == 9u ? 29u : (dimension == 10u ? 31u : 37u)));
-        const float fbase = (float)base;
-        uint32_t index = (sequence & 0x00ffffffu) + 1u;
-        float scale = 1.0f, value = 0.0f;
-#pragma unroll 1
-        while (index != 0u) {
-            scale = __fdiv_rn(scale, fbase);
-            uint32_t q = index / base;
-            value = __fadd_rn(value, __fmul_rn((float)(index - q * base), scale));
-            index = q;
+        const uint32_t index = (sequence & 0x00ffffffu) + 1u;
+        float value;
+        switch (dimension) {
+            case 0: value = radical_inverse<2>(index, c_halton_scale[0]); break;
+            case 1: value = radical_inverse<3>(index, c_halton_scale[1]); break;
+            case 2: value = radical_inverse<5>(index, c_halton_scale[2]); break;
+            case 3: value = radical_inverse<7>(index, c_halton_scale[3]); break;
+            case 4: value = radical_inverse<11>(index, c_halton_scale[4]); break;
+            case 5: value = radical_inverse<13>(index, c_halton_scale[5]); break;
+            case 6: value = radical_inverse<17>(index, c_halton_scale[6]); break;
+            case 7: value = radical_inverse<19>(index, c_halton_scale[7]); break;
+            case 8: value = radical_inverse<23>(index, c_halton_scale[8]); break;
+            case 9: value = radical_inverse<29>(index, c_halton_scale[9]); break;
+            case 10: value = radical_inverse<31>(index, c_halton_scale[10]); break;
+            default: value = radical_inverse<37>(index, c_halton_scale[11]); break;
         }
-        float rotation = __fdiv_rn((float)(pcg(stream ^ pcg(dimension)) >> 9u), 8388608.0f);
+        // x / 2^23 is exact, so the multiply gives the same bits.
+        float rotation = __fmul_rn((float)(pcg(stream ^ pcg(dimension)) >> 9u), 0x1p-23f);
         float t = __fadd_rn(value, rotation);
         return __fsub_rn(t, floorf(t));
     }
@@ -461,7 +490,7 @@ __device__ float sample_1d(uint32_t stream, uint32_t sequence, uint32_t dimensio
         index ^= (index >> 16u) & 0x0000ffffu;
     }
     uint32_t value = __brev(scramble_reverse(index, pcg(seed ^ pcg(dimension))));
-    return __fdiv_rn((float)(value >> 9u), 8388608.0f);
+    return __fmul_rn((float)(value >> 9u), 0x1p-23f);
 }
 
 __device__ __forceinline__ float continuation_sample(uint32_t stream, uint32_t sequence, uint32_t bounce, uint32_t dimension) {
@@ -825,6 +854,48 @@ void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted
     if (hits <= 1) launch_hits<1>(a, limited, budgeted, count, s);
     else if (hits == 2) launch_hits<2>(a, limited, budgeted, count, s);
     else launch_hits<3>(a, limited, budgeted, count, s);
+}
+
+}  // namespace vgi
+
+namespace vgi {
+namespace {
+
+// Companion light-tree records (see NodeLite): one thread per node.
+__global__ void node_aux_kernel(const uint4* __restrict__ emitters, uint32_t first_node, uint32_t nodes, float4* __restrict__ aux) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    const uint4 w0 = emitters[first_node + i * 4u], w1 = emitters[first_node + i * 4u + 1u], w3 = emitters[first_node + i * 4u + 3u];
+    const V3 mn{__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z)};
+    const V3 mx{__uint_as_float(w1.x), __uint_as_float(w1.y), __uint_as_float(w1.z)};
+    const V3 centre = (mn + mx) * 0.5f;
+    const float radius = __fmul_rn(len3(mx - mn), 0.5f);
+    aux[2u * i] = make_float4(centre.x, centre.y, centre.z, radius);
+    reinterpret_cast<uint4*>(aux)[2u * i + 1u] = make_uint4(w0.w, w1.w, w3.x, w3.y);
+}
+
+}  // namespace
+
+void launch_node_aux(const uint4* emitters, uint32_t first_node, uint32_t nodes, float4* aux, cudaStream_t s) {
+    if (nodes == 0) return;
+    node_aux_kernel<<<(nodes + 255) / 256, 256, 0, s>>>(emitters, first_node, nodes, aux);
+}
+
+cudaError_t init_trace_constants() {
+    // The reference's running `scale /= f32(base)` (voxel_path.wgsl:195),
+    // for as many digits as an index up to 2^24 has in each base.
+    static const uint32_t primes[12] = {2u, 3u, 5u, 7u, 11u, 13u, 17u, 19u, 23u, 29u, 31u, 37u};
+    float table[12][25] = {};
+    for (int d = 0; d < 12; ++d) {
+        uint32_t digits = 0;
+        for (uint32_t m = 0x1000000u; m != 0u; m /= primes[d]) ++digits;
+        float scale = 1.0f;
+        for (uint32_t k = 0; k < digits && k < 25; ++k) {
+            scale = scale / (float)primes[d];
+            table[d][k] = scale;
+        }
+    }
+    return cudaMemcpyToSymbol(c_halton_scale, table, sizeof(table));
 }
 
 }  // namespace vgi

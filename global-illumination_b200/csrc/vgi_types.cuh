@@ -19,6 +19,7 @@ struct TraceArgs {
     // model
     const float4* materials;   // 4 float4 per material (GpuMaterial)
     const uint4* emitters;     // GpuEmitter records then light-tree nodes
+    const float4* node_aux;    // 2 records per light-tree node (see vgi_trace.cu)
     float emitter_count;       // params.extra.w
     float emitter_total;       // params.extra.z
     float max_distance;        // params.extra.y (768)
@@ -52,6 +53,8 @@ struct AccumArgs {
 };
 
 void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
+void launch_node_aux(const uint4* emitters, uint32_t first_node, uint32_t nodes, float4* aux, cudaStream_t stream);
+cudaError_t init_trace_constants();
 void launch_prepare(const AccumArgs& a, cudaStream_t stream);
 void launch_accumulate(const AccumArgs& a, cudaStream_t stream);
 void launch_apply_events(const AccumArgs& a, const uint4* events, uint32_t n_slots, cudaStream_t stream);
