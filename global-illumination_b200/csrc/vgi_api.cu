@@ -101,6 +101,14 @@ struct vgi_ctx {
     // frame timing
     bool timing = false;
     cudaEvent_t marks[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    // trace layout and the wavefront's buffers
+    uint32_t layout = VGI_LAYOUT_WAVEFRONT;
+    uint32_t traverse_blocks = 0;
+    uint32_t refill_min = 8;
+    DevBuf<float4> w_state, w_ray;
+    DevBuf<uint4> w_hit;
+    DevBuf<uint32_t> w_status, w_queue0, w_queue1, w_counters;
 };
 
 namespace {
@@ -236,6 +244,38 @@ int check_ready(vgi_ctx* c, bool need_faces) {
 
 bool transport_limited(const vgi_ctx* c) { return norm_reach(c->transport.reach) < kMaxPathDistance; }
 
+// Enqueues the face trace for `a` in the context's layout.
+int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
+    if (c->layout == VGI_LAYOUT_SINGLE_KERNEL) {
+        launch_trace(a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
+        VGI_CUDA(c, cudaGetLastError());
+        return VGI_OK;
+    }
+    const size_t paths = (size_t)a.n_tasks * a.samples;
+    const size_t slots = paths * (2 + a.light_count) + (size_t)a.n_tasks * a.light_count;
+    if (paths > 0xffffffffull || slots > 0xffffffffull) return fail(c, VGI_ERR_CAPACITY, "too many paths for the wavefront layout");
+    VGI_CUDA(c, c->w_state.reserve(std::max<size_t>(paths, 1) * 9));
+    VGI_CUDA(c, c->w_ray.reserve(std::max<size_t>(slots, 1) * 2));
+    VGI_CUDA(c, c->w_hit.reserve(std::max<size_t>(paths, 1) * 6));
+    VGI_CUDA(c, c->w_status.reserve(std::max<size_t>(slots, 1)));
+    VGI_CUDA(c, c->w_queue0.reserve(std::max<size_t>(slots, 1)));
+    VGI_CUDA(c, c->w_queue1.reserve(std::max<size_t>(slots, 1)));
+    VGI_CUDA(c, c->w_counters.reserve(4));
+    WaveBuffers b{};
+    b.state = c->w_state.ptr;
+    b.ray = c->w_ray.ptr;
+    b.hit = c->w_hit.ptr;
+    b.status = c->w_status.ptr;
+    b.queue[0] = c->w_queue0.ptr;
+    b.queue[1] = c->w_queue1.ptr;
+    b.counters = c->w_counters.ptr;
+    b.traverse_blocks = c->traverse_blocks;
+    b.refill_min = c->refill_min;
+    launch_wave(b, a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    return VGI_OK;
+}
+
 int read_counters(vgi_ctx* c, vgi_counters* out) {
     unsigned long long h[10];
     VGI_CUDA(c, cudaMemcpyAsync(h, c->counters.ptr, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
@@ -322,6 +362,9 @@ int vgi_create(const vgi_config* config, vgi_ctx** out) {
     auto* c = new vgi_ctx();
     c->device = device;
     c->transport = default_transport();
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0) sms = 1;
+    c->traverse_blocks = (uint32_t)sms * wave_traverse_blocks_per_sm();
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         c->counters.reserve(16) != cudaSuccess || c->alloc.reserve(1) != cudaSuccess || c->pack_error.reserve(1) != cudaSuccess) {
         delete c;
@@ -341,6 +384,8 @@ int vgi_destroy(vgi_ctx* c) {
     c->tasks.release(); c->results.release(); c->state.release(); c->slot_meta.release(); c->checkpoint.release();
     c->face_index.release(); c->cache.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
     c->counters.release();
+    c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
+    c->w_queue0.release(); c->w_queue1.release(); c->w_counters.release();
     for (auto& e : c->marks)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -672,13 +717,23 @@ int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
     launch_prepare(acc, c->stream);
     if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[1], c->stream));
     TraceArgs tr = trace_args(c, c->tasks.ptr, c->results.ptr, c->n_slots, samples, true);
-    launch_trace(tr, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, false, c->stream);
+    rc = run_trace(c, tr, false);
+    if (rc != VGI_OK) return rc;
     if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[2], c->stream));
     launch_accumulate(acc, c->stream);
     if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[3], c->stream));
     VGI_CUDA(c, cudaGetLastError());
     c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
     if (c->batch_id == 0) c->batch_id = 1;
+    return VGI_OK;
+}
+
+int vgi_set_layout(vgi_ctx* c, uint32_t layout, uint32_t refill_min) {
+    if (!c) return VGI_ERR_INVALID;
+    if (layout != VGI_LAYOUT_WAVEFRONT && layout != VGI_LAYOUT_SINGLE_KERNEL) return fail(c, VGI_ERR_INVALID, "unknown layout");
+    if (refill_min < 1 || refill_min > 32) return fail(c, VGI_ERR_INVALID, "refill_min outside 1..32");
+    c->layout = layout;
+    c->refill_min = refill_min;
     return VGI_OK;
 }
 
@@ -724,8 +779,8 @@ int vgi_census(vgi_ctx* c, uint32_t samples, vgi_counters* counters) {
     launch_prepare(acc, c->stream);
     VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 10 * 8, c->stream));
     TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, c->n_slots, samples, true);
-    launch_trace(tr, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, true, c->stream);
-    VGI_CUDA(c, cudaGetLastError());
+    rc = run_trace(c, tr, true);
+    if (rc != VGI_OK) return rc;
     return read_counters(c, counters);
 }
 
@@ -740,8 +795,8 @@ int vgi_trace_tasks(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samp
     VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 10 * 8, c->stream));
     bool with_cache = c->n_slots > 0;
     TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, n, samples, with_cache);
-    launch_trace(tr, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, counters != nullptr, c->stream);
-    VGI_CUDA(c, cudaGetLastError());
+    rc = run_trace(c, tr, counters != nullptr);
+    if (rc != VGI_OK) return rc;
     VGI_CUDA(c, cudaMemcpyAsync(results, c->scratch_results.ptr, (size_t)n * 96, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     if (counters) return read_counters(c, counters);

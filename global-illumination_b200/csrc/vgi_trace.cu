@@ -899,3 +899,6 @@ cudaError_t init_trace_constants() {
 }
 
 }  // namespace vgi
+
+// The wavefront layout shares this translation unit's helpers and constants.
+#include "vgi_wave.cuh"

@@ -52,7 +52,22 @@ struct AccumArgs {
     uint32_t controls[36];
 };
 
+// Device buffers of the wavefront layout (vgi_wave.cuh) for P = tasks x
+// samples paths and S = P * (2 + lights) + tasks * lights ray slots.
+struct WaveBuffers {
+    float4* state;            // 9 * P path-state words
+    float4* ray;              // 2 * S
+    uint32_t* status;         // S
+    uint4* hit;               // 6 * P (full results of slots 0 and 1)
+    uint32_t* queue[2];       // S each
+    uint32_t* counters;       // queue counts [0], [1]; traversal head [2]
+    uint32_t traverse_blocks; // persistent traversal grid
+    uint32_t refill_min;      // idle lanes that trigger a refill
+};
+
 void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
+void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
+uint32_t wave_traverse_blocks_per_sm();
 void launch_node_aux(const uint4* emitters, uint32_t first_node, uint32_t nodes, float4* aux, cudaStream_t stream);
 cudaError_t init_trace_constants();
 void launch_prepare(const AccumArgs& a, cudaStream_t stream);

@@ -1,0 +1,898 @@
+// Wavefront layout of the face trace (included by vgi_trace.cu, so it shares
+// the estimator helpers and the Halton table).
+//
+// The per-path work of trace_receiver / advance_path (voxel_path.wgsl:418-520)
+// runs as stages. At each stage a path emits every ray it can launch
+// independently: its continuation, one shadow ray per light for direct_at,
+// and its emitter NEE or terminal connection. One persistent traversal
+// kernel then runs all queued rays. Its lanes refill from the queue as their
+// rays finish, so warps stay full whatever the step counts. The next shade
+// stage first completes the previous hit's contribution in the shader's
+// operation order:
+//     energy + tp * (emission * mis + diffuse * (direct + nee))
+// then processes the new hit. Every path performs the same float operations
+// as the single-kernel layout, so results are bit-identical to it and to the
+// oracle.
+//
+// Launch sequence per frame with DIFFUSE_HITS = H:
+//     begin, (traverse, shade) x H, traverse, finalize.
+// Ray slots per path and stage: 0 continuation, 1 NEE shadow or terminal ray,
+// 2.. one shadow ray per light. Face-centre direct rays follow all path slots.
+
+namespace vgi {
+namespace {
+
+constexpr int kWaveBlock = 256;
+
+// Path-state fields, each an array of n_paths float4 (SoA for coalescing).
+enum : uint32_t {
+    kE = 0,    // continuation energy rgb, previous_pdf
+    kTP = 1,   // throughput for the next hit rgb, bounce (bits)
+    kPP = 2,   // previous position xyz (the last hit point), flags (bits)
+    kPN = 3,   // previous normal xyz
+    kTH = 4,   // throughput at the pending hit rgb, pending kind (bits)
+    kEM = 5,   // emission * mis of the pending hit rgb
+    kDF = 6,   // diffuse of the pending hit rgb
+    kX = 7,    // cached energy or pending emitter value rgb
+    kN0 = 8,   // receiver NEE (pending, then final) rgb
+    kFields = 9,
+};
+
+// Path flags (kPP.w).
+constexpr uint32_t kFlagContinue = 1u;   // slot 0 holds this stage's continuation ray
+constexpr uint32_t kFlagUnknown = 2u;    // reached unloaded space
+constexpr uint32_t kFlagRan = 4u;        // the receiver's continuation was traced
+constexpr uint32_t kFlagS0 = 8u;         // slot 1 holds the receiver's NEE shadow ray
+constexpr uint32_t kFlagN = 16u;         // slot 1 holds the pending hit's NEE or terminal ray
+constexpr uint32_t kFlagValid = 32u;     // a traced sample of a valid task
+
+// Pending-contribution kinds (kTH.w).
+constexpr uint32_t kKindNone = 0u, kKindCached = 1u, kKindNee = 2u, kKindTermEmitter = 3u, kKindTermCosine = 4u;
+
+struct WaveArgs {
+    TraceArgs t;
+    uint32_t n_paths;
+    uint32_t slots;          // ray slots per path: 2 + lights
+    float4* state;           // kFields * n_paths
+    float4* ray;             // 2 float4 per ray slot: origin xyz + max distance, direction xyz + (full bit)
+    uint32_t* status;        // per ray slot
+    uint4* hit;              // 3 uint4 per path for slots 0 and 1 (full results): [p*2 + slot]
+    uint32_t* queue_in;      // ray slot indices to traverse
+    const uint32_t* count_in;
+    uint32_t* queue_out;     // rays emitted by this stage
+    uint32_t* count_out;
+    uint32_t* queue_head;    // traversal cursor
+};
+
+__device__ __forceinline__ float4& field(const WaveArgs& W, uint32_t f, uint32_t p) { return W.state[(size_t)f * W.n_paths + p]; }
+__device__ __forceinline__ uint32_t bits(float f) { return __float_as_uint(f); }
+__device__ __forceinline__ float fl(uint32_t u) { return __uint_as_float(u); }
+
+// Appends `slot` to the output queue (one atomic per warp).
+__device__ __forceinline__ void enqueue(const WaveArgs& W, bool want, uint32_t slot) {
+    const unsigned mask = __ballot_sync(0xffffffffu, want);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(W.count_out, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) W.queue_out[base + __popc(mask & ((1u << lane) - 1u))] = slot;
+}
+
+__device__ __forceinline__ void put_ray(const WaveArgs& W, uint32_t slot, V3 o, V3 d, float maxd, bool full) {
+    W.ray[2u * slot] = make_float4(o.x, o.y, o.z, maxd);
+    W.ray[2u * slot + 1u] = make_float4(d.x, d.y, d.z, fl(full ? 1u : 0u));
+}
+
+template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
+struct WaveTracer {
+    const WaveArgs& W;
+    const TraceArgs& A;
+    const float4* smat;
+    Cnt<C>& cnt;
+
+    __device__ Mat material_nocount(uint32_t m) const {
+        m &= 255u;
+        float4 d = smat[m * 2u], e = smat[m * 2u + 1u];
+        return Mat{make_float4(d.x, d.y, d.z, 0.0f), make_float4(e.x, e.y, e.z, 0.0f), d.w};
+    }
+    __device__ float reach() const { return LIMITED ? A.reach : A.max_distance; }
+
+    // sample_emitter up to its shadow ray (voxel_path.wgsl:332-358). Returns
+    // true with the ray and the value it would add (emission * factor) when a
+    // ray is needed; the material is counted when the ray turns out visible.
+    __device__ bool prepare_nee(V3 position, V3 normal, uint32_t source_stream, uint32_t sequence, uint32_t bounce, V3& so, V3& sdir,
+                                float& sdist, V3& pending) {
+        if (A.emitter_count == 0.0f) return false;
+        uint32_t stream = source_stream ^ pcg(bounce + 0xa341316cu);
+        // choose_emitter (voxel_path.wgsl:309-324)
+        Emissive em;
+        {
+            const float choice = sample_1d(stream, sequence, 12u);
+            uint32_t count = f2u(A.emitter_count);
+            if (load_emitter(A, 0u, cnt).sampling.w > 0.0f) {
+                em = tree_emitter(A, position, normal, choice, cnt);
+            } else {
+                uint32_t low = 0, high = count;
+#pragma unroll 1
+                while (low < high) {
+                    uint32_t middle = (low + high) / 2u;
+                    if (load_emitter(A, middle, cnt).sampling.x <= choice) low = middle + 1u;
+                    else high = middle;
+                }
+                em = load_emitter(A, low < count - 1u ? low : count - 1u, cnt);
+            }
+        }
+        V3 en = face_normal(em.face);
+        uint32_t axis = em.face / 2u;
+        V3 tangent = axis == 0u ? V3{0.0f, 1.0f, 0.0f} : V3{1.0f, 0.0f, 0.0f};
+        V3 bitangent = axis == 2u ? V3{0.0f, 1.0f, 0.0f} : V3{0.0f, 0.0f, 1.0f};
+        float s13 = __fsub_rn(sample_1d(stream, sequence, 13u), 0.5f);
+        float s14 = __fsub_rn(sample_1d(stream, sequence, 14u), 0.5f);
+        V3 lp = ((add_s(itof(em.voxel), 0.5f) + en * 0.5f) + tangent * s13) + bitangent * s14;
+        V3 delta = lp - position;
+        float d2 = dot3(delta, delta);
+        float r = reach();
+        if (d2 < 0.0001f || d2 > __fmul_rn(r, r)) return false;
+        float distance = __fsqrt_rn(d2);
+        V3 direction = delta / distance;
+        float rc = wmax(dot3(normal, direction), 0.0f);
+        float ec = wmax(dot3(en, -direction), 0.0f);
+        if (rc <= 0.0f || ec <= 0.0f || em.sampling.y <= 0.0f) return false;
+        float light_pdf = __fdiv_rn(__fmul_rn(em.sampling.y, d2), ec);
+        float directional_pdf = __fdiv_rn(rc, 3.14159265359f);
+        so = position + normal * 0.002f;
+        V3 sd = (lp + en * 0.002f) - so;
+        sdist = len3(sd);
+        sdir = sd / sdist;
+        Mat m = material_nocount(f2u(em.sampling.z));
+        float factor = __fdiv_rn(directional_pdf, __fadd_rn(light_pdf, directional_pdf));
+        pending = V3{m.emission.x, m.emission.y, m.emission.z} * factor;
+        // The material index rides in the ray's spare word for the count.
+        return true;
+    }
+
+    // direct_at's rays (voxel_path.wgsl:283-307): one per light that faces the point.
+    __device__ void emit_direct(V3 position, V3 normal, uint32_t first_slot, bool want) {
+        V3 origin = position + normal * 0.002f;
+#pragma unroll 1
+        for (uint32_t i = 0; i < A.light_count; ++i) {
+            bool emit = false;
+            V3 direction{0.0f, 0.0f, 0.0f};
+            float distance = A.max_distance;
+            if (want) {
+                const float4 Lp = __ldg(A.lights + i * 3u);
+                cnt.bytes(48);
+                V3 pos{Lp.x, Lp.y, Lp.z};
+                bool skip = false;
+                if (Lp.w >= 0.0f) {
+                    V3 delta = pos - position;
+                    float d2 = dot3(delta, delta);
+                    if (d2 <= 0.0000001f || d2 > __fmul_rn(Lp.w, Lp.w)) skip = true;
+                    else {
+                        distance = __fsqrt_rn(d2);
+                        direction = delta / distance;
+                        distance = __fsub_rn(distance, 0.004f);
+                    }
+                } else {
+                    direction = normalize3(pos);
+                }
+                emit = !skip && wmax(dot3(normal, direction), 0.0f) > 0.0f;
+                if (emit) put_ray(W, first_slot + i, origin, direction, distance, false);
+            }
+            enqueue(W, emit, first_slot + i);
+        }
+    }
+
+    // direct_at's value from the shadow rays' statuses, in light order.
+    template <bool CUSTOM>
+    __device__ V3 gather_direct(V3 position, V3 normal, uint32_t first_slot, V3* custom, float* value_w) {
+        V3 value{0.0f, 0.0f, 0.0f}, cv{0.0f, 0.0f, 0.0f};
+        float w = 0.0f;
+#pragma unroll 1
+        for (uint32_t i = 0; i < A.light_count; ++i) {
+            const float4 Lp = __ldg(A.lights + i * 3u), Le = __ldg(A.lights + i * 3u + 1u);
+            V3 pos{Lp.x, Lp.y, Lp.z};
+            float attenuation = 1.0f;
+            V3 direction;
+            if (Lp.w >= 0.0f) {
+                V3 delta = pos - position;
+                float d2 = dot3(delta, delta);
+                if (d2 <= 0.0000001f || d2 > __fmul_rn(Lp.w, Lp.w)) continue;
+                float distance = __fsqrt_rn(d2);
+                direction = delta / distance;
+                attenuation = __fdiv_rn(1.0f, wmax(d2, 1.0f));
+            } else {
+                direction = normalize3(pos);
+            }
+            float cosine = wmax(dot3(normal, direction), 0.0f);
+            if (cosine > 0.0f && W.status[first_slot + i] == 0u) {
+                float k = __fmul_rn(cosine, attenuation);
+                value = value + V3{Le.x, Le.y, Le.z} * k;
+                if (CUSTOM) {
+                    const float4 Lx = __ldg(A.lights + i * 3u + 2u);
+                    cv = cv + V3{Lx.y, Lx.z, Lx.w} * k;
+                    w = __fadd_rn(w, __fmul_rn(Le.w, k));
+                }
+            }
+        }
+        if (CUSTOM) {
+            *custom = cv;
+            *value_w = w;
+        }
+        return value;
+    }
+
+    // The status a shadow/continuation ray reports through trace() (BUDGETED fix).
+    __device__ uint32_t traced_status(uint32_t slot) const { return W.status[slot]; }
+
+    // Completes the pending hit of path p: energy += tp * (em*mis + diffuse * (direct + X)).
+    __device__ void combine(uint32_t p, uint32_t kind, uint32_t flags, float4& e) {
+        const float4 th = field(W, kTH, p), em = field(W, kEM, p), df = field(W, kDF, p), xv = field(W, kX, p);
+        const float4 pp = field(W, kPP, p), pn = field(W, kPN, p);
+        const V3 position{pp.x, pp.y, pp.z}, normal{pn.x, pn.y, pn.z};
+        const uint32_t base = p * W.slots;
+        V3 unused;
+        float unused_w;
+        V3 direct = gather_direct<false>(position, normal, base + 2u, &unused, &unused_w);
+        V3 x{0.0f, 0.0f, 0.0f};
+        if (kind == kKindCached) {
+            x = V3{xv.x, xv.y, xv.z};
+        } else if (kind == kKindNee || kind == kKindTermEmitter) {
+            if ((flags & kFlagN) && traced_status(base + 1u) == 0u) {
+                cnt.bytes(64);  // sample_emitter's material read
+                x = V3{xv.x, xv.y, xv.z};
+            }
+            if (kind == kKindTermEmitter) x = x * 2.0f;
+        } else if (kind == kKindTermCosine && (flags & kFlagN)) {
+            // sample_terminal_emission's cosine branch (voxel_path.wgsl:376-393).
+            const uint4 h0 = W.hit[((size_t)p * 2u + 1u) * 3u], h1 = W.hit[((size_t)p * 2u + 1u) * 3u + 1u],
+                        h2 = W.hit[((size_t)p * 2u + 1u) * 3u + 2u];
+            if (h0.x == 1u) {
+                const float4 rd = W.ray[2u * (base + 1u) + 1u];
+                const V3 direction{rd.x, rd.y, rd.z};
+                cnt.bytes(64);
+                Mat m = material_nocount(h0.y);
+                const V3 hp{fl(h1.y), fl(h1.z), fl(h1.w)}, hn{fl(h2.x), fl(h2.y), fl(h2.z)};
+                const I3 hv{(int)h0.z, (int)h0.w, (int)h1.x};
+                float power = m.weight;
+                V3 delta = hp - position;
+                float d2 = dot3(delta, delta);
+                float r = reach();
+                if (!(power == 0.0f || d2 < 0.0001f || d2 > __fmul_rn(r, r))) {
+                    float selection_pdf = __fdiv_rn(power, wmax(A.emitter_total, 1e-20f));
+                    if (load_emitter(A, 0u, cnt).sampling.w > 0.0f) selection_pdf = tree_probability(A, position, normal, hv, hn, cnt);
+                    float light_pdf = __fdiv_rn(__fmul_rn(selection_pdf, d2), wmax(dot3(hn, -direction), 1e-8f));
+                    float directional_pdf = cosine_pdf(normal, direction);
+                    float factor = __fdiv_rn(__fmul_rn(2.0f, directional_pdf), __fadd_rn(directional_pdf, light_pdf));
+                    x = V3{m.emission.x, m.emission.y, m.emission.z} * factor;
+                }
+            }
+        }
+        const V3 tp{th.x, th.y, th.z};
+        const V3 t = V3{em.x, em.y, em.z} + V3{df.x, df.y, df.z} * (direct + x);
+        const V3 energy = V3{e.x, e.y, e.z} + tp * t;
+        e.x = energy.x;
+        e.y = energy.y;
+        e.z = energy.z;
+    }
+};
+
+template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
+__device__ __forceinline__ void stage_materials(const TraceArgs& A, float4* smat) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        float4 d = __ldg(A.materials + i * 4), e = __ldg(A.materials + i * 4 + 2), x = __ldg(A.materials + i * 4 + 3);
+        smat[i * 2] = make_float4(d.x, d.y, d.z, x.y);
+        smat[i * 2 + 1] = make_float4(e.x, e.y, e.z, 0.0f);
+    }
+    __syncthreads();
+}
+
+template <bool C>
+__device__ __forceinline__ void flush_counters(const TraceArgs& A, Cnt<C>& cnt) {
+    if constexpr (C) {
+        unsigned long long v[10];
+        v[0] = cnt.rays; v[1] = cnt.paths; v[2] = cnt.steps; v[3] = cnt.b; v[4] = cnt.unk; v[5] = cnt.hits;
+        v[6] = cnt.st[0]; v[7] = cnt.st[1]; v[8] = cnt.st[2]; v[9] = cnt.st[3];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+            unsigned long long x = v[k];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if ((threadIdx.x & 31u) == 0u && x) atomicAdd(A.counters + k, x);
+        }
+    }
+}
+
+// Stage 0: the receiver sample (voxel_path.wgsl:504-513) of every path, and
+// the face-centre direct rays of write_result (voxel_trace.wgsl:28).
+template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
+__global__ void __launch_bounds__(kWaveBlock) wave_begin_kernel(const WaveArgs W) {
+    __shared__ float4 smat[512];
+    const TraceArgs& A = W.t;
+    stage_materials<HITS, LIMITED, BUDGETED, C>(A, smat);
+    Cnt<C> cnt;
+    WaveTracer<HITS, LIMITED, BUDGETED, C> T{W, A, smat, cnt};
+    const uint32_t p = blockIdx.x * kWaveBlock + threadIdx.x;
+    const bool in = p < W.n_paths;
+    const uint32_t face = in ? p / A.samples : 0u;
+    const uint32_t sample = in ? p - face * A.samples : 0u;
+    uint4 t0 = make_uint4(0, 0, 0, 0xffffffffu), t1 = make_uint4(0, 0, 0, 0);
+    if (in) {
+        t0 = __ldg(A.tasks + face * 2u);
+        t1 = __ldg(A.tasks + face * 2u + 1u);
+    }
+    const bool valid = in && t0.w != 0xffffffffu;
+    const V3 normal = face_normal(valid ? t0.w : 0u);
+    const I3 voxel{(int)t0.x, (int)t0.y, (int)t0.z};
+    const V3 surface = add_s(itof(voxel), 0.5f) + normal * 0.5f;
+    const uint32_t stream = hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(t0.w + 1u);
+    const uint32_t sequence = t1.x + sample;
+    const uint32_t base = p * W.slots;
+    uint32_t flags = valid ? kFlagValid : 0u;
+    bool s0 = false, c0 = false;
+    if (valid) {
+        cnt.path();
+        if (sample == 0u) cnt.bytes(32 + 96);
+        V3 direction = hemisphere(normal, sample_1d(stream, sequence, 0u), sample_1d(stream, sequence, 1u));
+        V3 so, sd, pending;
+        float sdist;
+        s0 = T.prepare_nee(surface, normal, stream, sequence, 0u, so, sd, sdist, pending);
+        if (s0) {
+            put_ray(W, base + 1u, so, sd, sdist, false);
+            flags |= kFlagS0;
+            field(W, kN0, p) = make_float4(pending.x, pending.y, pending.z, 0.0f);
+        } else {
+            field(W, kN0, p) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        if (dot3(normal, direction) > 0.0f) {
+            flags |= kFlagRan;
+            const V3 start = surface + normal * 0.001f;
+            const float previous_pdf = cosine_pdf(normal, direction);
+            const V3 previous_position = start - normal * 0.001f;
+            field(W, kE, p) = make_float4(0.0f, 0.0f, 0.0f, previous_pdf);
+            field(W, kTP, p) = make_float4(1.0f, 1.0f, 1.0f, fl(0u));
+            field(W, kPN, p) = make_float4(normal.x, normal.y, normal.z, 0.0f);
+            if (previous_pdf > 0.0f) {
+                c0 = true;
+                flags |= kFlagContinue;
+                put_ray(W, base, start, direction, T.reach(), true);
+            }
+            field(W, kPP, p) = make_float4(previous_position.x, previous_position.y, previous_position.z, fl(flags));
+        } else {
+            field(W, kE, p) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            field(W, kPP, p) = make_float4(0.0f, 0.0f, 0.0f, fl(flags));
+        }
+        field(W, kTH, p) = make_float4(0.0f, 0.0f, 0.0f, fl(kKindNone));
+    } else if (in) {
+        field(W, kPP, p) = make_float4(0.0f, 0.0f, 0.0f, fl(0u));
+        field(W, kTH, p) = make_float4(0.0f, 0.0f, 0.0f, fl(kKindNone));
+    }
+    enqueue(W, s0, base + 1u);
+    enqueue(W, c0, base);
+    // Face-centre direct rays, one thread per face.
+    const uint32_t face_slots = W.n_paths * W.slots;
+    T.emit_direct(surface, normal, face_slots + face * A.light_count, valid && sample == 0u);
+    flush_counters<C>(A, cnt);
+}
+
+// One lane's ray in flight: trace_domain_limited's loop variables.
+struct RayRun {
+    V3 dir, pos, nrm;
+    float dist, maxd;
+    int lrx, lry, lrz;
+    uint4 meta;
+    uint32_t step, slot;
+    bool full;
+};
+
+template <bool BUDGETED>
+__device__ __forceinline__ void finish_ray(const WaveArgs& W, RayRun& s, uint32_t status, uint32_t material, I3 voxel, V3 position, V3 normal) {
+    if (BUDGETED && status == 2u && material == 0xffffffffu) status = 0u;  // trace()'s budget rule
+    W.status[s.slot] = status;
+    if (s.full) {
+        const uint32_t p = s.slot / W.slots, k = s.slot - p * W.slots;
+        uint4* h = W.hit + ((size_t)p * 2u + k) * 3u;
+        h[0] = make_uint4(status, material, (uint32_t)voxel.x, (uint32_t)voxel.y);
+        h[1] = make_uint4((uint32_t)voxel.z, bits(position.x), bits(position.y), bits(position.z));
+        h[2] = make_uint4(bits(normal.x), bits(normal.y), bits(normal.z), 0u);
+    }
+    s.slot = kNoIndex;
+}
+
+// trace_domain_limited's set-up (voxel_traversal.wgsl:127-151): the slab
+// clip against the scene bounds. A ray that misses finishes at once.
+template <bool BUDGETED, bool C>
+__device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t slot, Cnt<C>& cnt) {
+    const TraceArgs& A = W.t;
+    const float4 ro = W.ray[2u * slot], rd = W.ray[2u * slot + 1u];
+    s.slot = slot;
+    s.full = (bits(rd.w) & 1u) != 0u;
+    s.dir = V3{rd.x, rd.y, rd.z};
+    s.maxd = ro.w;
+    cnt.ray();
+    const V3 origin{ro.x, ro.y, ro.z}, dir = s.dir;
+    float nearv = -1e30f, farv = 1e30f;
+    V3 normal{0.0f, 0.0f, 0.0f};
+    const float mnx = __fmul_rn((float)A.mn[0], 16.0f), mny = __fmul_rn((float)A.mn[1], 16.0f), mnz = __fmul_rn((float)A.mn[2], 16.0f);
+    const float mxx = __fmul_rn((float)(A.mx[0] + 1), 16.0f), mxy = __fmul_rn((float)(A.mx[1] + 1), 16.0f),
+                mxz = __fmul_rn((float)(A.mx[2] + 1), 16.0f);
+    const I3 zi{0, 0, 0};
+    const V3 zv{0.0f, 0.0f, 0.0f};
+#define VGI_SLAB(AX, O, D, MN, MX)                                                      \
+    if (fabsf(D) <= 1e-8f) {                                                            \
+        if (O < MN || O > MX) { cnt.status(0); finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv); return; } \
+    } else {                                                                            \
+        float first = __fdiv_rn(__fsub_rn(MN, O), D);                                   \
+        float second = __fdiv_rn(__fsub_rn(MX, O), D);                                  \
+        if (wmin(first, second) > nearv) {                                              \
+            nearv = wmin(first, second);                                                \
+            float sg = first < second ? -1.0f : 1.0f;                                   \
+            normal = V3{AX == 0 ? sg : 0.0f, AX == 1 ? sg : 0.0f, AX == 2 ? sg : 0.0f}; \
+        }                                                                               \
+        farv = wmin(farv, wmax(first, second));                                         \
+    }
+    VGI_SLAB(0, origin.x, dir.x, mnx, mxx)
+    VGI_SLAB(1, origin.y, dir.y, mny, mxy)
+    VGI_SLAB(2, origin.z, dir.z, mnz, mxz)
+#undef VGI_SLAB
+    if (farv < wmax(nearv, 0.0f)) {
+        cnt.status(0);
+        finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv);
+        return;
+    }
+    s.dist = __fadd_rn(wmax(nearv, 0.0f), 0.001f);
+    s.pos = origin + dir * s.dist;
+    s.nrm = normal;
+    s.lrx = s.lry = s.lrz = 0x7fffffff;
+    s.meta = make_uint4(0, 0, 0, 0);
+    s.step = 0;
+}
+
+// One iteration of trace_domain_limited's loop (voxel_traversal.wgsl:152-213),
+// including the out-of-steps exit (:214-218).
+template <bool BUDGETED, bool C>
+__device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& cnt) {
+    const TraceArgs& A = W.t;
+    const I3 zi{0, 0, 0};
+    const V3 zv{0.0f, 0.0f, 0.0f};
+    if (s.step >= A.path_steps) {
+        cnt.status(2);
+        finish_ray<BUDGETED>(W, s, 2u, 0xffffffffu, zi, zv, zv);
+        return;
+    }
+    cnt.step();
+    if (s.dist > s.maxd) {
+        cnt.status(0);
+        finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv);
+        return;
+    }
+    const I3 voxel{f2i(floorf(s.pos.x)), f2i(floorf(s.pos.y)), f2i(floorf(s.pos.z))};
+    const int rx = voxel.x >> 4, ry = voxel.y >> 4, rz = voxel.z >> 4;
+    if (!in_bounds(A, rx, ry, rz)) {
+        cnt.status(0);
+        finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv);
+        return;
+    }
+    if (s.lrx != rx || s.lry != ry || s.lrz != rz) {
+        const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
+        if (index == kNoIndex) {
+            if (BUDGETED) {  // visible_geometry: cross the missing region
+                const float4 adv = advance_box(s.pos, s.dir, I3{rx, ry, rz}, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f);
+                s.dist = __fadd_rn(s.dist, adv.w);
+                s.pos = s.pos + s.dir * adv.w;
+                s.nrm = V3{adv.x, adv.y, adv.z};
+                s.step += 1u;
+                return;
+            }
+            const uint32_t st = geometry_ahead(A, s.pos, s.dir, __fsub_rn(s.maxd, s.dist), cnt) ? 2u : 0u;
+            cnt.status(st);
+            finish_ray<BUDGETED>(W, s, st, 0u, zi, zv, zv);
+            return;
+        }
+        cnt.bytes(16);
+        s.meta = __ldg(A.headers + index);
+        s.lrx = rx;
+        s.lry = ry;
+        s.lrz = rz;
+    }
+    float4 adv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (s.meta.x == 1u) {
+        adv = advance_box(s.pos, s.dir, I3{rx, ry, rz}, unpack_bytes(s.meta.z), unpack_bytes(s.meta.w), 16.0f);
+    } else {
+        uint32_t material = s.meta.y;
+        if (s.meta.x == 3u) {
+            const uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
+            const uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
+            const uint32_t brick = __ldg(A.cells + s.meta.y + (bz * 4u + by) * 4u + bx);
+            cnt.bytes(4);
+            const uint32_t state = brick & 3u;
+            if (state == 0u) {
+                const uint32_t ext = brick >> 2u;
+                adv = advance_box(s.pos, s.dir, I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz}, neg_ext(ext), pos_ext(ext), 4.0f);
+                material = 256u;
+            } else if (state == 1u) {
+                material = brick >> 2u;
+            } else {
+                const uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
+                const uint32_t word = __ldg(A.cells + (brick >> 2u) + (idx >> 1));
+                cnt.bytes(4);
+                const uint32_t cell = (word >> ((idx & 1u) * 16u)) & 65535u;
+                material = (cell & 1u) != 0u ? (cell >> 1u) : 256u;
+                if (material == 256u) {
+                    const uint32_t ext = cell >> 1u;
+                    adv = advance_box(s.pos, s.dir, voxel, neg_ext(ext), pos_ext(ext), 1.0f);
+                }
+            }
+        }
+        if (material != 256u) {
+            cnt.status(1);
+            finish_ray<BUDGETED>(W, s, 1u, material, voxel, s.pos, s.nrm);
+            return;
+        }
+    }
+    s.dist = __fadd_rn(s.dist, adv.w);
+    s.pos = s.pos + s.dir * adv.w;
+    s.nrm = V3{adv.x, adv.y, adv.z};
+    s.step += 1u;
+}
+
+// trace() (voxel_path.wgsl:239-243) for every queued ray. Persistent warps
+// keep one ray per lane and advance all lanes one DDA step per pass; when
+// enough lanes have finished, they take the next rays from the queue (one
+// atomic per warp), so a warp is not held by its longest ray.
+template <bool BUDGETED, bool C>
+__global__ void __launch_bounds__(kWaveBlock) wave_traverse_kernel(const WaveArgs W, uint32_t refill_min) {
+    const TraceArgs& A = W.t;
+    Cnt<C> cnt;
+    const uint32_t total = *W.count_in;
+    const int lane = threadIdx.x & 31;
+    RayRun s;
+    s.slot = kNoIndex;
+    bool exhausted = false;
+    for (;;) {
+        const bool need = s.slot == kNoIndex;
+        const unsigned want = __ballot_sync(0xffffffffu, need);
+        if (!exhausted && (uint32_t)__popc(want) >= (want == 0xffffffffu ? 1u : refill_min)) {
+            const int leader = __ffs(want) - 1;
+            uint32_t first = 0;
+            if (lane == leader) first = atomicAdd(W.queue_head, (uint32_t)__popc(want));
+            first = __shfl_sync(0xffffffffu, first, leader);
+            const uint32_t mine = first + __popc(want & ((1u << lane) - 1u));
+            if (first + __popc(want) >= total) exhausted = true;
+            if (need && mine < total) start_ray<BUDGETED, C>(W, s, W.queue_in[mine], cnt);
+        }
+        const bool idle = s.slot == kNoIndex;
+        if (__all_sync(0xffffffffu, idle)) {
+            if (exhausted) break;
+            continue;
+        }
+        if (!idle) step_ray<BUDGETED, C>(W, s, cnt);
+    }
+    flush_counters<C>(A, cnt);
+}
+
+// Stage s >= 1: complete the pending hit, then the continuation's new hit
+// (one iteration of advance_path, voxel_path.wgsl:432-490).
+template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
+__global__ void __launch_bounds__(kWaveBlock) wave_shade_kernel(const WaveArgs W, uint32_t stage) {
+    __shared__ float4 smat[512];
+    const TraceArgs& A = W.t;
+    stage_materials<HITS, LIMITED, BUDGETED, C>(A, smat);
+    Cnt<C> cnt;
+    WaveTracer<HITS, LIMITED, BUDGETED, C> T{W, A, smat, cnt};
+    const uint32_t p = blockIdx.x * kWaveBlock + threadIdx.x;
+    const bool in = p < W.n_paths;
+    float4 pp = in ? field(W, kPP, p) : make_float4(0, 0, 0, 0);
+    uint32_t flags = bits(pp.w);
+    const uint32_t base = p * W.slots;
+    bool emit_c = false, emit_n = false, emit_d = false;
+    V3 dpos{0.0f, 0.0f, 0.0f}, dnrm{0.0f, 0.0f, 0.0f};
+    if (in && (flags & kFlagValid)) {
+        float4 e = field(W, kE, p);
+        // The receiver's NEE from stage 0.
+        if (stage == 1u && (flags & kFlagS0)) {
+            float4 n0 = field(W, kN0, p);
+            if (W.status[base + 1u] == 0u) cnt.bytes(64);
+            else n0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            field(W, kN0, p) = n0;
+        }
+        const uint32_t kind = bits(field(W, kTH, p).w);
+        if (kind != kKindNone) T.combine(p, kind, flags, e);
+        flags &= ~(kFlagS0 | kFlagN);
+        uint32_t pending_kind = kKindNone;
+        if (flags & kFlagContinue) {
+            flags &= ~kFlagContinue;
+            const float4 tpw = field(W, kTP, p);
+            const uint32_t bounce = bits(tpw.w);
+            const V3 tp{tpw.x, tpw.y, tpw.z};
+            const float4 ro = W.ray[2u * base], rd = W.ray[2u * base + 1u];
+            const V3 origin{ro.x, ro.y, ro.z}, direction{rd.x, rd.y, rd.z};
+            const uint4 h0 = W.hit[(size_t)p * 6u], h1 = W.hit[(size_t)p * 6u + 1u], h2 = W.hit[(size_t)p * 6u + 2u];
+            uint32_t status = h0.x;
+            if (LIMITED && status == 0u &&
+                geometry_ahead(A, origin + direction * T.reach(), direction, __fsub_rn(A.max_distance, T.reach()), cnt))
+                status = 3u;
+            if (status == 0u) {
+                float horizon = wclamp(__fadd_rn(__fmul_rn(direction.y, 0.35f), 0.65f), 0.15f, 1.0f);
+                V3 en = V3{e.x, e.y, e.z} + (tp * V3{A.env[0], A.env[1], A.env[2]}) * horizon;
+                e.x = en.x;
+                e.y = en.y;
+                e.z = en.z;
+            } else if (status == 2u) {
+                flags |= kFlagUnknown;
+            } else if (status == 1u) {
+                const V3 hp{fl(h1.y), fl(h1.z), fl(h1.w)}, hn{fl(h2.x), fl(h2.y), fl(h2.z)};
+                const I3 hv{(int)h0.z, (int)h0.w, (int)h1.x};
+                cnt.bytes(64);
+                const Mat m = T.material_nocount(h0.y);
+                const float4 ppos = pp, pnrm = field(W, kPN, p);
+                const V3 previous_position{ppos.x, ppos.y, ppos.z}, previous_normal{pnrm.x, pnrm.y, pnrm.z};
+                const float previous_pdf = e.w;
+                // direct_at's rays from the hit.
+                emit_d = true;
+                const float emission_weight = m.weight;
+                const V3 delta = hp - origin;
+                float selection_pdf = __fdiv_rn(emission_weight, wmax(A.emitter_total, 1e-20f));
+                if (emission_weight > 0.0f && A.emitter_count > 0.0f && load_emitter(A, 0u, cnt).sampling.w > 0.0f)
+                    selection_pdf = tree_probability(A, previous_position, previous_normal, hv, hn, cnt);
+                const float light_pdf = __fdiv_rn(__fmul_rn(selection_pdf, dot3(delta, delta)), wmax(dot3(hn, -direction), 1e-8f));
+                float mis = 1.0f;
+                if (light_pdf > 0.0f) mis = __fdiv_rn(previous_pdf, __fadd_rn(previous_pdf, light_pdf));
+                const V3 emission{m.emission.x, m.emission.y, m.emission.z};
+                const V3 diffuse{m.diffuse.x, m.diffuse.y, m.diffuse.z};
+                const V3 em_mis = emission * mis;
+                // Task identity for the sampler.
+                const uint32_t face = p / A.samples, sample = p - face * A.samples;
+                const uint4 t0 = __ldg(A.tasks + face * 2u), t1 = __ldg(A.tasks + face * 2u + 1u);
+                const uint32_t pstream = hash_voxel((int)t0.x, (int)t0.y, (int)t0.z) ^ pcg(t0.w + 1u);
+                const uint32_t sequence = t1.x + sample;
+                V3 cached;
+                V3 xval{0.0f, 0.0f, 0.0f};
+                bool have_cache = false;
+                {
+                    // cached_energy (voxel_path.wgsl:66-87)
+                    const uint32_t f = face_index_of(hn);
+                    if (f <= 5u && A.face_index != nullptr) {
+                        const uint4 header = __ldg(A.face_index);
+                        uint32_t s = (hash_voxel(hv.x, hv.y, hv.z) ^ pcg(f + 1u)) & header.x;
+#pragma unroll 1
+                        for (uint32_t attempt = 0; attempt < header.y; ++attempt) {
+                            const uint4 ent = __ldg(A.face_index + s + 1u);
+                            cnt.bytes(16);
+                            if (ent.w == 0xffffffffu) break;
+                            if ((int)ent.x == hv.x && (int)ent.y == hv.y && (int)ent.z == hv.z && (ent.w >> 29u) == f) {
+                                const float4 rec = __ldg(A.cache + (ent.w & 0x1fffffffu));
+                                cnt.bytes(16);
+                                const uint32_t count = __float_as_uint(rec.w);
+                                if (!(count < 16u || (count & 0x80000000u) != 0u)) {
+                                    cached = V3{rec.x, rec.y, rec.z};
+                                    have_cache = true;
+                                }
+                                break;
+                            }
+                            s = (s + 1u) & header.x;
+                        }
+                    }
+                }
+                if (have_cache) {
+                    cnt.cache_hit();
+                    pending_kind = kKindCached;
+                    xval = cached;
+                } else {
+                    const bool last = bounce + 1u == HITS;
+                    V3 so, sd, pend{0.0f, 0.0f, 0.0f};
+                    float sdist = 0.0f;
+                    if (last) {
+                        // sample_terminal_emission (voxel_path.wgsl:368-394)
+                        if (A.emitter_count != 0.0f) {
+                            if (continuation_sample(pstream, sequence, bounce, 2u) < 0.5f) {
+                                pending_kind = kKindTermEmitter;
+                                emit_n = T.prepare_nee(hp, hn, pstream, sequence, bounce + 1u, so, sd, sdist, pend);
+                                if (emit_n) put_ray(W, base + 1u, so, sd, sdist, false);
+                            } else {
+                                pending_kind = kKindTermCosine;
+                                const V3 tdir = hemisphere(hn, continuation_sample(pstream, sequence, bounce, 0u),
+                                                           continuation_sample(pstream, sequence, bounce, 1u));
+                                if (dot3(hn, tdir) > 0.0f) {
+                                    emit_n = true;
+                                    put_ray(W, base + 1u, hp + hn * 0.002f, tdir, T.reach(), true);
+                                }
+                            }
+                        } else {
+                            pending_kind = kKindNee;  // zero emitter value
+                        }
+                    } else {
+                        pending_kind = kKindNee;
+                        emit_n = T.prepare_nee(hp, hn, pstream, sequence, bounce + 1u, so, sd, sdist, pend);
+                        if (emit_n) put_ray(W, base + 1u, so, sd, sdist, false);
+                    }
+                    xval = pend;
+                    if (!last) {
+                        // The continuation (voxel_path.wgsl:472-489).
+                        V3 tn = tp * diffuse;
+                        const float maximum = wmax(tn.x, wmax(tn.y, tn.z));
+                        bool go = maximum != 0.0f;
+                        if (go && bounce >= 1u) {
+                            const float survival = wclamp(maximum, 0.1f, 0.95f);
+                            if (continuation_sample(pstream, sequence, bounce, 2u) > survival) go = false;
+                            else tn = tn / survival;
+                        }
+                        if (go) {
+                            const V3 ndir = hemisphere(hn, continuation_sample(pstream, sequence, bounce, 0u),
+                                                       continuation_sample(pstream, sequence, bounce, 1u));
+                            const float npdf = cosine_pdf(hn, ndir);
+                            e.w = npdf;
+                            if (npdf > 0.0f) {
+                                emit_c = true;
+                                flags |= kFlagContinue;
+                                put_ray(W, base, hp + hn * 0.002f, ndir, T.reach(), true);
+                                field(W, kTP, p) = make_float4(tn.x, tn.y, tn.z, fl(bounce + 1u));
+                            }
+                        }
+                    }
+                }
+                if (emit_n) flags |= kFlagN;
+                field(W, kTH, p) = make_float4(tp.x, tp.y, tp.z, fl(pending_kind));
+                field(W, kEM, p) = make_float4(em_mis.x, em_mis.y, em_mis.z, 0.0f);
+                field(W, kDF, p) = make_float4(diffuse.x, diffuse.y, diffuse.z, 0.0f);
+                field(W, kX, p) = make_float4(xval.x, xval.y, xval.z, 0.0f);
+                field(W, kPN, p) = make_float4(hn.x, hn.y, hn.z, 0.0f);
+                pp = make_float4(hp.x, hp.y, hp.z, 0.0f);
+                dpos = hp;
+                dnrm = hn;
+            }
+        }
+        if (pending_kind == kKindNone) field(W, kTH, p) = make_float4(0.0f, 0.0f, 0.0f, fl(kKindNone));
+        field(W, kE, p) = e;
+        pp.w = fl(flags);
+        field(W, kPP, p) = pp;
+    }
+    // Warp-collective from here on: every thread takes part.
+    T.emit_direct(dpos, dnrm, base + 2u, emit_d);  // direct_at's rays from the hit point
+    enqueue(W, emit_n, base + 1u);
+    enqueue(W, emit_c, base);
+    flush_counters<C>(A, cnt);
+}
+
+// Completes each path's last pending hit, then trace_moments + write_result
+// (voxel_trace.wgsl:25-92) with the same lane layout as trace_faces_kernel:
+// one thread per (face, lane), lanes summing strided samples, lane 0 summing
+// the lanes in order.
+template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
+__global__ void __launch_bounds__(kWaveBlock) wave_finalize_kernel(const WaveArgs W) {
+    __shared__ float4 smat[512];
+    const TraceArgs& A = W.t;
+    stage_materials<HITS, LIMITED, BUDGETED, C>(A, smat);
+    Cnt<C> cnt;
+    WaveTracer<HITS, LIMITED, BUDGETED, C> T{W, A, smat, cnt};
+    const uint32_t lanes = 1u << A.lanes_log2;
+    const uint32_t gid = blockIdx.x * kWaveBlock + threadIdx.x;
+    const uint32_t face = gid >> A.lanes_log2;
+    const uint32_t lane = gid & (lanes - 1u);
+    uint4 t0 = make_uint4(0, 0, 0, 0xffffffffu);
+    if (face < A.n_tasks) t0 = __ldg(A.tasks + face * 2u);
+    const bool valid = face < A.n_tasks && t0.w != 0xffffffffu;
+    V3 mean{0.0f, 0.0f, 0.0f}, second{0.0f, 0.0f, 0.0f};
+    uint32_t known = 0;
+    if (valid) {
+#pragma unroll 1
+        for (uint32_t i = lane; i < A.samples; i += lanes) {
+            const uint32_t p = face * A.samples + i;
+            const uint32_t flags = bits(field(W, kPP, p).w);
+            float4 e = field(W, kE, p);
+            const uint32_t kind = bits(field(W, kTH, p).w);
+            if (kind != kKindNone) T.combine(p, kind, flags, e);
+            if (flags & kFlagUnknown) {
+                cnt.unknown();
+                continue;
+            }
+            const float4 n0 = field(W, kN0, p);
+            V3 value{n0.x, n0.y, n0.z};
+            if (flags & kFlagRan) value = value + V3{e.x, e.y, e.z};
+            mean = mean + value;
+            second = second + value * value;
+            known += 1u;
+        }
+    }
+    V3 tm{0.0f, 0.0f, 0.0f}, ts{0.0f, 0.0f, 0.0f};
+    uint32_t tk = 0;
+    {
+        const uint32_t base = (threadIdx.x & 31u) & ~(lanes - 1u);
+        for (uint32_t i = 0; i < lanes; ++i) {
+            float mx = __shfl_sync(0xffffffffu, mean.x, base + i), my = __shfl_sync(0xffffffffu, mean.y, base + i),
+                  mz = __shfl_sync(0xffffffffu, mean.z, base + i);
+            float sx = __shfl_sync(0xffffffffu, second.x, base + i), sy = __shfl_sync(0xffffffffu, second.y, base + i),
+                  sz = __shfl_sync(0xffffffffu, second.z, base + i);
+            uint32_t k = __shfl_sync(0xffffffffu, known, base + i);
+            tm = tm + V3{mx, my, mz};
+            ts = ts + V3{sx, sy, sz};
+            tk += k;
+        }
+    }
+    if (valid && lane == 0) {
+        const V3 normal = face_normal(t0.w);
+        const V3 surface = add_s(itof(I3{(int)t0.x, (int)t0.y, (int)t0.z}), 0.5f) + normal * 0.5f;
+        V3 dc;
+        float dw = 0.0f;
+        const V3 dv = T.template gather_direct<true>(surface, normal, W.n_paths * W.slots + face * A.light_count, &dc, &dw);
+        float inverse = __fdiv_rn(1.0f, (float)(tk > 1u ? tk : 1u));
+        V3 m = tm * inverse, s = ts * inverse;
+        uint4* out = A.results + (size_t)face * 6u;
+        out[0] = make_uint4(__float_as_uint(m.x), __float_as_uint(m.y), __float_as_uint(m.z), 0u);
+        out[1] = make_uint4(0u, __float_as_uint((float)tk), 0u, 0u);
+        out[2] = make_uint4(__float_as_uint(s.x), __float_as_uint(s.y), __float_as_uint(s.z), 0u);
+        out[3] = make_uint4(0u, 0u, 0u, 0u);
+        out[4] = make_uint4(__float_as_uint(dv.x), __float_as_uint(dv.y), __float_as_uint(dv.z), __float_as_uint(dw));
+        out[5] = make_uint4(0u, __float_as_uint(dc.x), __float_as_uint(dc.y), __float_as_uint(dc.z));
+    }
+    flush_counters<C>(A, cnt);
+}
+
+template <uint32_t H, bool L, bool B, bool C>
+void wave_run(const WaveBuffers& b, const TraceArgs& a, cudaStream_t s) {
+    WaveArgs W{};
+    W.t = a;
+    W.n_paths = a.n_tasks * a.samples;
+    W.slots = 2u + a.light_count;
+    W.state = b.state;
+    W.ray = b.ray;
+    W.status = b.status;
+    W.hit = b.hit;
+    W.queue_head = b.counters + 2;
+    const uint32_t path_blocks = (W.n_paths + kWaveBlock - 1) / kWaveBlock;
+    const uint32_t face_blocks = (uint32_t)((((uint64_t)a.n_tasks << a.lanes_log2) + kWaveBlock - 1) / kWaveBlock);
+    uint32_t* qa = b.queue[0];
+    uint32_t* qb = b.queue[1];
+    uint32_t* ca = b.counters + 0;
+    uint32_t* cb = b.counters + 1;
+    cudaMemsetAsync(ca, 0, sizeof(uint32_t), s);
+    W.queue_out = qa;
+    W.count_out = ca;
+    wave_begin_kernel<H, L, B, C><<<path_blocks, kWaveBlock, 0, s>>>(W);
+    for (uint32_t stage = 1; stage <= H + 1u; ++stage) {
+        // Traverse what the previous stage queued.
+        W.queue_in = qa;
+        W.count_in = ca;
+        cudaMemsetAsync(W.queue_head, 0, sizeof(uint32_t), s);
+        wave_traverse_kernel<B, C><<<b.traverse_blocks, kWaveBlock, 0, s>>>(W, b.refill_min);
+        if (stage == H + 1u) break;
+        cudaMemsetAsync(cb, 0, sizeof(uint32_t), s);
+        W.queue_out = qb;
+        W.count_out = cb;
+        wave_shade_kernel<H, L, B, C><<<path_blocks, kWaveBlock, 0, s>>>(W, stage);
+        uint32_t* t = qa; qa = qb; qb = t;
+        t = ca; ca = cb; cb = t;
+    }
+    wave_finalize_kernel<H, L, B, C><<<face_blocks, kWaveBlock, 0, s>>>(W);
+}
+
+template <uint32_t H>
+void wave_hits(const WaveBuffers& b, const TraceArgs& a, bool limited, bool budgeted, bool count, cudaStream_t s) {
+#define VGI_WAVE(LL, BB)                                      \
+    if (count) wave_run<H, LL, BB, true>(b, a, s);            \
+    else wave_run<H, LL, BB, false>(b, a, s);
+    if (limited) {
+        if (budgeted) { VGI_WAVE(true, true) } else { VGI_WAVE(true, false) }
+    } else {
+        if (budgeted) { VGI_WAVE(false, true) } else { VGI_WAVE(false, false) }
+    }
+#undef VGI_WAVE
+}
+
+}  // namespace
+
+void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t s) {
+    if (a.n_tasks == 0 || a.samples == 0) return;
+    if (hits <= 1) wave_hits<1>(b, a, limited, budgeted, count, s);
+    else if (hits == 2) wave_hits<2>(b, a, limited, budgeted, count, s);
+    else wave_hits<3>(b, a, limited, budgeted, count, s);
+}
+
+uint32_t wave_traverse_blocks_per_sm() {
+    int blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, wave_traverse_kernel<false, false>, kWaveBlock, 0);
+    return blocks > 0 ? (uint32_t)blocks : 1u;
+}
+
+}  // namespace vgi

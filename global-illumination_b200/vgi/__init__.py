@@ -133,6 +133,8 @@ _SIGNATURES = {
     "vgi_set_faces": (_INT, [_P, _P, _U32]),
     "vgi_frame": (_INT, [_P, _U32, _U32]),
     "vgi_set_timing": (_INT, [_P, _INT]),
+    "vgi_set_layout": (_INT, [_P, _U32, _U32]),
+    "vgi_pack_regions_static": (_INT, [_P, _U32, _P, _P, _U64, _P, _P]),
     "vgi_frame_times": (_INT, [_P, _P]),
     "vgi_trace_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P]),
     "vgi_census": (_INT, [_P, _U32, _P]),
@@ -374,6 +376,13 @@ class GpuTracer:
 
     def frame(self, samples: int, clock_ms: int = 0) -> None:
         self._check(self._lib.vgi_frame(self._h, samples, clock_ms))
+
+    WAVEFRONT = 0
+    SINGLE_KERNEL = 1
+
+    def set_layout(self, layout: int, refill_min: int = 8) -> None:
+        """Trace layout: GpuTracer.WAVEFRONT (default) or GpuTracer.SINGLE_KERNEL."""
+        self._check(self._lib.vgi_set_layout(self._h, layout, refill_min))
 
     def set_timing(self, enable: bool) -> None:
         self._check(self._lib.vgi_set_timing(self._h, int(enable)))

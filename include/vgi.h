@@ -131,6 +131,16 @@ int vgi_set_faces(vgi_ctx* ctx, const vgi_face* faces, uint32_t n);
  * trace with cache gather, then accumulate (submit_compact's resident batch,
  * src/gpu.rs:647-1022). `clock_ms` is the accumulation clock. Enqueued only. */
 int vgi_frame(vgi_ctx* ctx, uint32_t samples, uint32_t clock_ms);
+/* Layout of the face trace. Both layouts compute bit-identical results.
+ * VGI_LAYOUT_WAVEFRONT (default): paths advance in stages whose rays a
+ *   persistent traversal kernel runs from a queue.
+ * VGI_LAYOUT_SINGLE_KERNEL: one thread per (face, lane) runs whole paths, the
+ *   reference's trace_faces_parallel layout (shaders/voxel_trace.wgsl:70-92).
+ * `refill_min` (1..32, default 8) is how many idle lanes make a traversal
+ * warp take new rays from the queue. */
+#define VGI_LAYOUT_WAVEFRONT 0u
+#define VGI_LAYOUT_SINGLE_KERNEL 1u
+int vgi_set_layout(vgi_ctx* ctx, uint32_t layout, uint32_t refill_min);
 /* Device timing of vgi_frame (the reference's timestamp query pairs,
  * src/gpu.rs:488-500): with timing enabled each frame records CUDA events on
  * the context's stream around prepare, trace and accumulate, and

@@ -26,7 +26,8 @@ class Case:
         self.faces = vgi.exposed_faces(self.coords, self.vox) if faces is None else faces
         self.emitters, self.n_emit, self.total = vgi.host_emitters(self.coords, self.vox, self.materials)
 
-    def load(self, g: vgi.GpuTracer, with_faces=True):
+    def load(self, g: vgi.GpuTracer, with_faces=True, layout=vgi.GpuTracer.WAVEFRONT):
+        g.set_layout(layout)
         g.upload_regions(self.coords, self.vox)
         g.set_materials(self.materials)
         g.set_lights(self.lights, self.n_directional)
@@ -115,8 +116,11 @@ def test_gpu_packing_matches_oracle(gpu, make):
     assert_words_equal(O.canonical(d, h, cl, case.coords), O.canonical(rd, rh, rcl, case.coords), "canonical geometry")
 
 
-def trace_pair(gpu, case, samples, lanes, sequence=0):
-    case.load(gpu, with_faces=False)
+LAYOUTS = [vgi.GpuTracer.WAVEFRONT, vgi.GpuTracer.SINGLE_KERNEL]
+
+
+def trace_pair(gpu, case, samples, lanes, sequence=0, layout=vgi.GpuTracer.WAVEFRONT):
+    case.load(gpu, with_faces=False, layout=layout)
     geometry = gpu.geometry()
     tasks = vgi.tasks_for(case.faces, sequence)
     got, gcnt = gpu.trace_tasks(tasks, samples, count=True)
@@ -133,17 +137,18 @@ def trace_pair(gpu, case, samples, lanes, sequence=0):
     (terrain_case, 8, {"bounces": 3, "reach": 24.0}),
     (terrain_case, 4, {"bounces": 2, "budgeted": True, "path_steps": 48, "env": (0.16, 0.24, 0.38)}),
 ])
-def test_trace_matches_oracle_bit_exact(gpu, make, samples, kw):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_trace_matches_oracle_bit_exact(gpu, make, samples, kw, layout):
     case = make(**kw)
     lanes = lanes_for(case.transport, samples)
-    got, want, gcnt, wcnt = trace_pair(gpu, case, samples, lanes, sequence=12345)
+    got, want, gcnt, wcnt = trace_pair(gpu, case, samples, lanes, sequence=12345, layout=layout)
     assert_words_equal(got, want, "face results")
     assert gcnt == wcnt
     assert wcnt["rays"] > 0 and wcnt["paths"] == case.faces.shape[0] * samples
 
 
-def run_frames(gpu, case, frames, samples):
-    case.load(gpu)
+def run_frames(gpu, case, frames, samples, layout=vgi.GpuTracer.WAVEFRONT):
+    case.load(gpu, layout=layout)
     geometry = gpu.geometry()
     lanes = lanes_for(case.transport, samples)
     ref = O.Frames(geometry, case.params_fn(geometry), case.materials, case.lights, case.emitters, case.faces, case.transport,
@@ -154,18 +159,20 @@ def run_frames(gpu, case, frames, samples):
     return ref
 
 
-def test_stone_room_frames_match_oracle(gpu):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_stone_room_frames_match_oracle(gpu, layout):
     # Config 1 shape: 4 spp, 1 bounce via the cache, 64 DDA steps, history 64.
     case = stone_room_case()
-    ref = run_frames(gpu, case, 24, 4)
+    ref = run_frames(gpu, case, 24, 4, layout)
     assert_words_equal(gpu.read_results(), ref.results, "frame results")
     assert_words_equal(gpu.read_state(), ref.state, "resident state")
     assert_words_equal(gpu.read_slot_meta(), ref.meta, "slot metadata")
 
 
-def test_terrain_frames_with_cache_match_oracle(gpu):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_terrain_frames_with_cache_match_oracle(gpu, layout):
     case = terrain_case(bounces=2)
-    ref = run_frames(gpu, case, 6, 8)
+    ref = run_frames(gpu, case, 6, 8, layout)
     assert_words_equal(gpu.read_results(), ref.results, "frame results")
     assert_words_equal(gpu.read_state(), ref.state, "resident state")
     # The cache served paths once faces reached 16 samples.
@@ -173,9 +180,10 @@ def test_terrain_frames_with_cache_match_oracle(gpu):
     assert cnt["cache_hits"] > 0
 
 
-def test_census_counts_match_oracle(gpu):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_census_counts_match_oracle(gpu, layout):
     case = terrain_case(bounces=2)
-    ref = run_frames(gpu, case, 3, 8)
+    ref = run_frames(gpu, case, 3, 8, layout)
     got = gpu.census(8)
     geometry = gpu.geometry()
     ctl = O.controls_words(ref.n, 8, 0, case.transport)
