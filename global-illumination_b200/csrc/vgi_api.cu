@@ -108,7 +108,7 @@ struct vgi_ctx {
     uint32_t refill_min = 8;
     DevBuf<float4> w_state, w_ray;
     DevBuf<uint4> w_hit;
-    DevBuf<uint32_t> w_status, w_queue0, w_queue1, w_counters;
+    DevBuf<uint32_t> w_status, w_queue0, w_queue1, w_scatter, w_counters;
 };
 
 namespace {
@@ -253,13 +253,14 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
     }
     const size_t paths = (size_t)a.n_tasks * a.samples;
     const size_t slots = paths * (2 + a.light_count) + (size_t)a.n_tasks * a.light_count;
-    if (paths > 0xffffffffull || slots > 0xffffffffull) return fail(c, VGI_ERR_CAPACITY, "too many paths for the wavefront layout");
+    if (paths >= (1ull << 30) || slots > 0xffffffffull) return fail(c, VGI_ERR_CAPACITY, "too many paths for the wavefront layout");
     VGI_CUDA(c, c->w_state.reserve(std::max<size_t>(paths, 1) * 9));
     VGI_CUDA(c, c->w_ray.reserve(std::max<size_t>(slots, 1) * 2));
     VGI_CUDA(c, c->w_hit.reserve(std::max<size_t>(paths, 1) * 6));
     VGI_CUDA(c, c->w_status.reserve(std::max<size_t>(slots, 1)));
     VGI_CUDA(c, c->w_queue0.reserve(std::max<size_t>(slots, 1)));
     VGI_CUDA(c, c->w_queue1.reserve(std::max<size_t>(slots, 1)));
+    VGI_CUDA(c, c->w_scatter.reserve(std::max<size_t>(paths, 1)));
     VGI_CUDA(c, c->w_counters.reserve(4));
     WaveBuffers b{};
     b.state = c->w_state.ptr;
@@ -268,6 +269,7 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
     b.status = c->w_status.ptr;
     b.queue[0] = c->w_queue0.ptr;
     b.queue[1] = c->w_queue1.ptr;
+    b.scatter = c->w_scatter.ptr;
     b.counters = c->w_counters.ptr;
     b.traverse_blocks = c->traverse_blocks;
     b.refill_min = c->refill_min;
@@ -385,7 +387,7 @@ int vgi_destroy(vgi_ctx* c) {
     c->face_index.release(); c->cache.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
     c->counters.release();
     c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
-    c->w_queue0.release(); c->w_queue1.release(); c->w_counters.release();
+    c->w_queue0.release(); c->w_queue1.release(); c->w_scatter.release(); c->w_counters.release();
     for (auto& e : c->marks)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -467,6 +469,7 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
     }
     for (uint32_t h = 0; h < n_headers; ++h) {
         const uint32_t kind = headers[h * 4], payload = headers[h * 4 + 1];
+        if (kind < 1 || kind > 3) return fail(c, VGI_ERR_INVALID, "region kind outside 1..3");
         if (kind == 2 && payload > 255) return fail(c, VGI_ERR_INVALID, "uniform region material above 255");
         if (kind != 3) continue;
         if ((uint64_t)payload + 64 > n_cells) return fail(c, VGI_ERR_INVALID, "brick table outside the cells");

@@ -60,7 +60,8 @@ struct WaveBuffers {
     uint32_t* status;         // S
     uint4* hit;               // 6 * P (full results of slots 0 and 1)
     uint32_t* queue[2];       // S each
-    uint32_t* counters;       // queue counts [0], [1]; traversal head [2]
+    uint32_t* scatter;        // P: uncached hits awaiting NEE and continuation
+    uint32_t* counters;       // queue counts [0], [1]; traversal head [2]; scatter count [3]
     uint32_t traverse_blocks; // persistent traversal grid
     uint32_t refill_min;      // idle lanes that trigger a refill
 };

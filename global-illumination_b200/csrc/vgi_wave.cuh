@@ -62,6 +62,8 @@ struct WaveArgs {
     uint32_t* queue_out;     // rays emitted by this stage
     uint32_t* count_out;
     uint32_t* queue_head;    // traversal cursor
+    uint32_t* scatter_queue; // uncached hits: path | bounce << 30
+    uint32_t* scatter_count;
 };
 
 __device__ __forceinline__ float4& field(const WaveArgs& W, uint32_t f, uint32_t p) { return W.state[(size_t)f * W.n_paths + p]; }
@@ -450,87 +452,95 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
 }
 
 // One iteration of trace_domain_limited's loop (voxel_traversal.wgsl:152-213),
-// including the out-of-steps exit (:214-218).
+// including the out-of-steps exit (:214-218). The branches only decide the
+// outcome: either the ray ends (one finish below) or it skips a box, whose
+// cell, extents and size they choose for the single advance_box call. The
+// lanes of a warp take different branches, but none of them runs the box
+// step on its own.
 template <bool BUDGETED, bool C>
 __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& cnt) {
     const TraceArgs& A = W.t;
-    const I3 zi{0, 0, 0};
-    const V3 zv{0.0f, 0.0f, 0.0f};
+    constexpr uint32_t kGo = 0xffffffffu;
+    uint32_t status = kGo, material = 0u;
+    I3 voxel{0, 0, 0};
+    I3 cell{0, 0, 0}, ng{0, 0, 0}, ps{0, 0, 0};
+    float size = 16.0f;
     if (s.step >= A.path_steps) {
-        cnt.status(2);
-        finish_ray<BUDGETED>(W, s, 2u, 0xffffffffu, zi, zv, zv);
-        return;
-    }
-    cnt.step();
-    if (s.dist > s.maxd) {
-        cnt.status(0);
-        finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv);
-        return;
-    }
-    const I3 voxel{f2i(floorf(s.pos.x)), f2i(floorf(s.pos.y)), f2i(floorf(s.pos.z))};
-    const int rx = voxel.x >> 4, ry = voxel.y >> 4, rz = voxel.z >> 4;
-    if (!in_bounds(A, rx, ry, rz)) {
-        cnt.status(0);
-        finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv);
-        return;
-    }
-    if (s.lrx != rx || s.lry != ry || s.lrz != rz) {
-        const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
-        if (index == kNoIndex) {
-            if (BUDGETED) {  // visible_geometry: cross the missing region
-                const float4 adv = advance_box(s.pos, s.dir, I3{rx, ry, rz}, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f);
-                s.dist = __fadd_rn(s.dist, adv.w);
-                s.pos = s.pos + s.dir * adv.w;
-                s.nrm = V3{adv.x, adv.y, adv.z};
-                s.step += 1u;
-                return;
-            }
-            const uint32_t st = geometry_ahead(A, s.pos, s.dir, __fsub_rn(s.maxd, s.dist), cnt) ? 2u : 0u;
-            cnt.status(st);
-            finish_ray<BUDGETED>(W, s, st, 0u, zi, zv, zv);
-            return;
-        }
-        cnt.bytes(16);
-        s.meta = __ldg(A.headers + index);
-        s.lrx = rx;
-        s.lry = ry;
-        s.lrz = rz;
-    }
-    float4 adv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (s.meta.x == 1u) {
-        adv = advance_box(s.pos, s.dir, I3{rx, ry, rz}, unpack_bytes(s.meta.z), unpack_bytes(s.meta.w), 16.0f);
+        status = 2u;
+        material = 0xffffffffu;
     } else {
-        uint32_t material = s.meta.y;
-        if (s.meta.x == 3u) {
-            const uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
-            const uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
-            const uint32_t brick = __ldg(A.cells + s.meta.y + (bz * 4u + by) * 4u + bx);
-            cnt.bytes(4);
-            const uint32_t state = brick & 3u;
-            if (state == 0u) {
-                const uint32_t ext = brick >> 2u;
-                adv = advance_box(s.pos, s.dir, I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz}, neg_ext(ext), pos_ext(ext), 4.0f);
-                material = 256u;
-            } else if (state == 1u) {
-                material = brick >> 2u;
+        cnt.step();
+        voxel = I3{f2i(floorf(s.pos.x)), f2i(floorf(s.pos.y)), f2i(floorf(s.pos.z))};
+        const int rx = voxel.x >> 4, ry = voxel.y >> 4, rz = voxel.z >> 4;
+        if (s.dist > s.maxd || !in_bounds(A, rx, ry, rz)) {
+            status = 0u;
+        } else {
+            bool missing = false;
+            if (s.lrx != rx || s.lry != ry || s.lrz != rz) {
+                const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
+                if (index == kNoIndex) {
+                    missing = true;
+                } else {
+                    cnt.bytes(16);
+                    s.meta = __ldg(A.headers + index);
+                    s.lrx = rx;
+                    s.lry = ry;
+                    s.lrz = rz;
+                }
+            }
+            cell = I3{rx, ry, rz};
+            if (missing) {
+                // visible_geometry crosses a missing region; otherwise the ray
+                // ends as unknown or escaped by geometry_ahead.
+                if (!BUDGETED) status = geometry_ahead(A, s.pos, s.dir, __fsub_rn(s.maxd, s.dist), cnt) ? 2u : 0u;
+            } else if (s.meta.x == 1u) {
+                ng = unpack_bytes(s.meta.z);
+                ps = unpack_bytes(s.meta.w);
+            } else if (s.meta.x != 3u) {
+                status = 1u;
+                material = s.meta.y;
             } else {
-                const uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
-                const uint32_t word = __ldg(A.cells + (brick >> 2u) + (idx >> 1));
+                const uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
+                const uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
+                const uint32_t brick = __ldg(A.cells + s.meta.y + (bz * 4u + by) * 4u + bx);
                 cnt.bytes(4);
-                const uint32_t cell = (word >> ((idx & 1u) * 16u)) & 65535u;
-                material = (cell & 1u) != 0u ? (cell >> 1u) : 256u;
-                if (material == 256u) {
-                    const uint32_t ext = cell >> 1u;
-                    adv = advance_box(s.pos, s.dir, voxel, neg_ext(ext), pos_ext(ext), 1.0f);
+                const uint32_t state = brick & 3u;
+                if (state == 0u) {
+                    const uint32_t ext = brick >> 2u;
+                    cell = I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz};
+                    ng = neg_ext(ext);
+                    ps = pos_ext(ext);
+                    size = 4.0f;
+                } else if (state == 1u) {
+                    status = 1u;
+                    material = brick >> 2u;
+                } else {
+                    const uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
+                    const uint32_t word = __ldg(A.cells + (brick >> 2u) + (idx >> 1));
+                    cnt.bytes(4);
+                    const uint32_t c = (word >> ((idx & 1u) * 16u)) & 65535u;
+                    if ((c & 1u) != 0u) {
+                        status = 1u;
+                        material = c >> 1u;
+                    } else {
+                        const uint32_t ext = c >> 1u;
+                        cell = voxel;
+                        ng = neg_ext(ext);
+                        ps = pos_ext(ext);
+                        size = 1.0f;
+                    }
                 }
             }
         }
-        if (material != 256u) {
-            cnt.status(1);
-            finish_ray<BUDGETED>(W, s, 1u, material, voxel, s.pos, s.nrm);
-            return;
-        }
     }
+    if (status != kGo) {
+        cnt.status(status);
+        const bool hit = status == 1u;
+        const V3 zv{0.0f, 0.0f, 0.0f};
+        finish_ray<BUDGETED>(W, s, status, material, hit ? voxel : I3{0, 0, 0}, hit ? s.pos : zv, hit ? s.nrm : zv);
+        return;
+    }
+    const float4 adv = advance_box(s.pos, s.dir, cell, ng, ps, size);
     s.dist = __fadd_rn(s.dist, adv.w);
     s.pos = s.pos + s.dir * adv.w;
     s.nrm = V3{adv.x, adv.y, adv.z};
@@ -586,7 +596,8 @@ __global__ void __launch_bounds__(kWaveBlock) wave_shade_kernel(const WaveArgs W
     float4 pp = in ? field(W, kPP, p) : make_float4(0, 0, 0, 0);
     uint32_t flags = bits(pp.w);
     const uint32_t base = p * W.slots;
-    bool emit_c = false, emit_n = false, emit_d = false;
+    bool emit_c = false, emit_n = false, emit_d = false, scatter = false;
+    uint32_t scatter_entry = 0;
     V3 dpos{0.0f, 0.0f, 0.0f}, dnrm{0.0f, 0.0f, 0.0f};
     if (in && (flags & kFlagValid)) {
         float4 e = field(W, kE, p);
@@ -680,59 +691,14 @@ __global__ void __launch_bounds__(kWaveBlock) wave_shade_kernel(const WaveArgs W
                     pending_kind = kKindCached;
                     xval = cached;
                 } else {
-                    const bool last = bounce + 1u == HITS;
-                    V3 so, sd, pend{0.0f, 0.0f, 0.0f};
-                    float sdist = 0.0f;
-                    if (last) {
-                        // sample_terminal_emission (voxel_path.wgsl:368-394)
-                        if (A.emitter_count != 0.0f) {
-                            if (continuation_sample(pstream, sequence, bounce, 2u) < 0.5f) {
-                                pending_kind = kKindTermEmitter;
-                                emit_n = T.prepare_nee(hp, hn, pstream, sequence, bounce + 1u, so, sd, sdist, pend);
-                                if (emit_n) put_ray(W, base + 1u, so, sd, sdist, false);
-                            } else {
-                                pending_kind = kKindTermCosine;
-                                const V3 tdir = hemisphere(hn, continuation_sample(pstream, sequence, bounce, 0u),
-                                                           continuation_sample(pstream, sequence, bounce, 1u));
-                                if (dot3(hn, tdir) > 0.0f) {
-                                    emit_n = true;
-                                    put_ray(W, base + 1u, hp + hn * 0.002f, tdir, T.reach(), true);
-                                }
-                            }
-                        } else {
-                            pending_kind = kKindNee;  // zero emitter value
-                        }
-                    } else {
-                        pending_kind = kKindNee;
-                        emit_n = T.prepare_nee(hp, hn, pstream, sequence, bounce + 1u, so, sd, sdist, pend);
-                        if (emit_n) put_ray(W, base + 1u, so, sd, sdist, false);
-                    }
-                    xval = pend;
-                    if (!last) {
-                        // The continuation (voxel_path.wgsl:472-489).
-                        V3 tn = tp * diffuse;
-                        const float maximum = wmax(tn.x, wmax(tn.y, tn.z));
-                        bool go = maximum != 0.0f;
-                        if (go && bounce >= 1u) {
-                            const float survival = wclamp(maximum, 0.1f, 0.95f);
-                            if (continuation_sample(pstream, sequence, bounce, 2u) > survival) go = false;
-                            else tn = tn / survival;
-                        }
-                        if (go) {
-                            const V3 ndir = hemisphere(hn, continuation_sample(pstream, sequence, bounce, 0u),
-                                                       continuation_sample(pstream, sequence, bounce, 1u));
-                            const float npdf = cosine_pdf(hn, ndir);
-                            e.w = npdf;
-                            if (npdf > 0.0f) {
-                                emit_c = true;
-                                flags |= kFlagContinue;
-                                put_ray(W, base, hp + hn * 0.002f, ndir, T.reach(), true);
-                                field(W, kTP, p) = make_float4(tn.x, tn.y, tn.z, fl(bounce + 1u));
-                            }
-                        }
-                    }
+                    // NEE or the terminal connection, and the continuation,
+                    // run in wave_scatter_kernel over the paths queued here.
+                    pending_kind = kKindNee;
+                    scatter = true;
+                    scatter_entry = p | (bounce << 30);
                 }
-                if (emit_n) flags |= kFlagN;
+                (void)pstream;
+                (void)sequence;
                 field(W, kTH, p) = make_float4(tp.x, tp.y, tp.z, fl(pending_kind));
                 field(W, kEM, p) = make_float4(em_mis.x, em_mis.y, em_mis.z, 0.0f);
                 field(W, kDF, p) = make_float4(diffuse.x, diffuse.y, diffuse.z, 0.0f);
@@ -752,6 +718,103 @@ __global__ void __launch_bounds__(kWaveBlock) wave_shade_kernel(const WaveArgs W
     T.emit_direct(dpos, dnrm, base + 2u, emit_d);  // direct_at's rays from the hit point
     enqueue(W, emit_n, base + 1u);
     enqueue(W, emit_c, base);
+    {
+        const unsigned mask = __ballot_sync(0xffffffffu, scatter);
+        if (mask) {
+            const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+            uint32_t first = 0;
+            if (lane == leader) first = atomicAdd(W.scatter_count, (uint32_t)__popc(mask));
+            first = __shfl_sync(0xffffffffu, first, leader);
+            if (scatter) W.scatter_queue[first + __popc(mask & ((1u << lane) - 1u))] = scatter_entry;
+        }
+    }
+    flush_counters<C>(A, cnt);
+}
+
+// The rest of an uncached hit (advance_path, voxel_path.wgsl:464-489) for the
+// paths wave_shade_kernel queued: the emitter NEE, or on the last hit
+// sample_terminal_emission's connection, then roulette and the continuation.
+// Queue entries are path | bounce << 30; warps stride over the queue.
+template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
+__global__ void __launch_bounds__(kWaveBlock) wave_scatter_kernel(const WaveArgs W) {
+    __shared__ float4 smat[512];
+    const TraceArgs& A = W.t;
+    stage_materials<HITS, LIMITED, BUDGETED, C>(A, smat);
+    Cnt<C> cnt;
+    WaveTracer<HITS, LIMITED, BUDGETED, C> T{W, A, smat, cnt};
+    const uint32_t total = *W.scatter_count;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (kWaveBlock / 32);
+    for (uint32_t first = (blockIdx.x * kWaveBlock + threadIdx.x) - lane; first < total; first += warps * 32u) {
+        const uint32_t k = first + lane;
+        const bool active = k < total;
+        const uint32_t entry = active ? W.scatter_queue[k] : 0u;
+        const uint32_t p = entry & 0x3fffffffu, bounce = entry >> 30;
+        const uint32_t base = p * W.slots;
+        bool emit_n = false, emit_c = false;
+        if (active) {
+            const float4 pp = field(W, kPP, p), pn = field(W, kPN, p), th = field(W, kTH, p), df = field(W, kDF, p);
+            const V3 hp{pp.x, pp.y, pp.z}, hn{pn.x, pn.y, pn.z}, tp{th.x, th.y, th.z}, diffuse{df.x, df.y, df.z};
+            uint32_t flags = bits(pp.w);
+            const uint32_t face = p / A.samples, sample = p - face * A.samples;
+            const uint4 t0 = __ldg(A.tasks + face * 2u), t1 = __ldg(A.tasks + face * 2u + 1u);
+            const uint32_t pstream = hash_voxel((int)t0.x, (int)t0.y, (int)t0.z) ^ pcg(t0.w + 1u);
+            const uint32_t sequence = t1.x + sample;
+            const bool last = bounce + 1u == HITS;
+            uint32_t kind = kKindNee;
+            V3 so, sd, pend{0.0f, 0.0f, 0.0f};
+            float sdist = 0.0f;
+            if (last) {
+                // sample_terminal_emission (voxel_path.wgsl:368-394)
+                if (A.emitter_count != 0.0f) {
+                    if (continuation_sample(pstream, sequence, bounce, 2u) < 0.5f) {
+                        kind = kKindTermEmitter;
+                        emit_n = T.prepare_nee(hp, hn, pstream, sequence, bounce + 1u, so, sd, sdist, pend);
+                        if (emit_n) put_ray(W, base + 1u, so, sd, sdist, false);
+                    } else {
+                        kind = kKindTermCosine;
+                        const V3 tdir =
+                            hemisphere(hn, continuation_sample(pstream, sequence, bounce, 0u), continuation_sample(pstream, sequence, bounce, 1u));
+                        if (dot3(hn, tdir) > 0.0f) {
+                            emit_n = true;
+                            put_ray(W, base + 1u, hp + hn * 0.002f, tdir, T.reach(), true);
+                        }
+                    }
+                }
+            } else {
+                emit_n = T.prepare_nee(hp, hn, pstream, sequence, bounce + 1u, so, sd, sdist, pend);
+                if (emit_n) put_ray(W, base + 1u, so, sd, sdist, false);
+                // The continuation (voxel_path.wgsl:472-489).
+                V3 tn = tp * diffuse;
+                const float maximum = wmax(tn.x, wmax(tn.y, tn.z));
+                bool go = maximum != 0.0f;
+                if (go && bounce >= 1u) {
+                    const float survival = wclamp(maximum, 0.1f, 0.95f);
+                    if (continuation_sample(pstream, sequence, bounce, 2u) > survival) go = false;
+                    else tn = tn / survival;
+                }
+                if (go) {
+                    const V3 ndir = hemisphere(hn, continuation_sample(pstream, sequence, bounce, 0u), continuation_sample(pstream, sequence, bounce, 1u));
+                    const float npdf = cosine_pdf(hn, ndir);
+                    float4 e = field(W, kE, p);
+                    e.w = npdf;
+                    field(W, kE, p) = e;
+                    if (npdf > 0.0f) {
+                        emit_c = true;
+                        flags |= kFlagContinue;
+                        put_ray(W, base, hp + hn * 0.002f, ndir, T.reach(), true);
+                        field(W, kTP, p) = make_float4(tn.x, tn.y, tn.z, fl(bounce + 1u));
+                    }
+                }
+            }
+            if (emit_n) flags |= kFlagN;
+            field(W, kTH, p) = make_float4(tp.x, tp.y, tp.z, fl(kind));
+            field(W, kX, p) = make_float4(pend.x, pend.y, pend.z, 0.0f);
+            field(W, kPP, p) = make_float4(pp.x, pp.y, pp.z, fl(flags));
+        }
+        enqueue(W, emit_n, base + 1u);
+        enqueue(W, emit_c, base);
+    }
     flush_counters<C>(A, cnt);
 }
 
@@ -840,6 +903,8 @@ void wave_run(const WaveBuffers& b, const TraceArgs& a, cudaStream_t s) {
     W.status = b.status;
     W.hit = b.hit;
     W.queue_head = b.counters + 2;
+    W.scatter_queue = b.scatter;
+    W.scatter_count = b.counters + 3;
     const uint32_t path_blocks = (W.n_paths + kWaveBlock - 1) / kWaveBlock;
     const uint32_t face_blocks = (uint32_t)((((uint64_t)a.n_tasks << a.lanes_log2) + kWaveBlock - 1) / kWaveBlock);
     uint32_t* qa = b.queue[0];
@@ -858,9 +923,11 @@ void wave_run(const WaveBuffers& b, const TraceArgs& a, cudaStream_t s) {
         wave_traverse_kernel<B, C><<<b.traverse_blocks, kWaveBlock, 0, s>>>(W, b.refill_min);
         if (stage == H + 1u) break;
         cudaMemsetAsync(cb, 0, sizeof(uint32_t), s);
+        cudaMemsetAsync(W.scatter_count, 0, sizeof(uint32_t), s);
         W.queue_out = qb;
         W.count_out = cb;
         wave_shade_kernel<H, L, B, C><<<path_blocks, kWaveBlock, 0, s>>>(W, stage);
+        wave_scatter_kernel<H, L, B, C><<<b.traverse_blocks, kWaveBlock, 0, s>>>(W);
         uint32_t* t = qa; qa = qb; qb = t;
         t = ca; ca = cb; cb = t;
     }
