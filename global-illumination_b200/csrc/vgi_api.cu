@@ -19,6 +19,8 @@ void launch_classify_pack(const uint16_t* voxels, const uint32_t* regions, uint3
                           unsigned long long* alloc, unsigned long long capacity, uint32_t* error, cudaStream_t s);
 void launch_scatter_edits(const uint2* edits, uint32_t n, uint16_t* voxels, cudaStream_t s);
 void launch_set_header_extents(uint4* headers, const uint2* zw, uint32_t n, cudaStream_t s);
+void launch_dedup_bricks(const uint4* headers, uint32_t n, uint32_t* cells, uint32_t* table, uint32_t mask, uint32_t* error,
+                         cudaStream_t s);
 }  // namespace vgi
 
 namespace {
@@ -76,6 +78,7 @@ struct vgi_ctx {
     DevBuf<uint2> edit_buf;
     DevBuf<uint2> zw;
     DevBuf<uint32_t> region_list;
+    DevBuf<uint32_t> dedup_table;
 
     // model
     std::vector<float> host_materials = std::vector<float>(256 * 16, 0.0f);
@@ -101,6 +104,8 @@ struct vgi_ctx {
     // frame timing
     bool timing = false;
     cudaEvent_t marks[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t traverse_marks[8] = {};
+    uint32_t traverse_launches = 0;  // traversal launches of the last timed wavefront frame
 
     // trace layout and the wavefront's buffers
     uint32_t layout = VGI_LAYOUT_WAVEFRONT;
@@ -247,6 +252,7 @@ bool transport_limited(const vgi_ctx* c) { return norm_reach(c->transport.reach)
 // Enqueues the face trace for `a` in the context's layout.
 int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
     if (c->layout == VGI_LAYOUT_SINGLE_KERNEL) {
+        if (c->timing && !count) c->traverse_launches = 0;
         launch_trace(a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
         VGI_CUDA(c, cudaGetLastError());
         return VGI_OK;
@@ -273,13 +279,15 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
     b.counters = c->w_counters.ptr;
     b.traverse_blocks = c->traverse_blocks;
     b.refill_min = c->refill_min;
+    b.traverse_marks = (c->timing && !count) ? c->traverse_marks : nullptr;
+    if (b.traverse_marks) c->traverse_launches = std::min<uint32_t>(c->transport.bounces + 1u, 4u);
     launch_wave(b, a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     return VGI_OK;
 }
 
 int read_counters(vgi_ctx* c, vgi_counters* out) {
-    unsigned long long h[10];
+    unsigned long long h[11];
     VGI_CUDA(c, cudaMemcpyAsync(h, c->counters.ptr, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     if (out) {
@@ -290,6 +298,7 @@ int read_counters(vgi_ctx* c, vgi_counters* out) {
         out->unknown = h[4];
         out->cache_hits = h[5];
         for (int k = 0; k < 4; ++k) out->status[k] = h[6 + k];
+        out->traverse_bytes = h[10];
     }
     return VGI_OK;
 }
@@ -337,13 +346,21 @@ int pack_regions(vgi_ctx* c, const std::vector<uint32_t>* list) {
     launch_classify_pack(c->voxels.ptr, dlist, grid, n, c->headers.ptr, c->cells.ptr, c->alloc.ptr, c->cells.count, c->pack_error.ptr,
                          c->stream);
     VGI_CUDA(c, cudaGetLastError());
+    // Share identical brick payloads across every region (sized for all
+    // bricks mixed, at most half full).
+    size_t slots = 1;
+    while (slots < (size_t)n * 128) slots <<= 1;
+    VGI_CUDA(c, c->dedup_table.reserve(slots));
+    VGI_CUDA(c, cudaMemsetAsync(c->dedup_table.ptr, 0xff, slots * 4, c->stream));
+    launch_dedup_bricks(c->headers.ptr, n, c->cells.ptr, c->dedup_table.ptr, (uint32_t)(slots - 1), c->pack_error.ptr, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
     uint32_t err = 0;
     unsigned long long used = 0;
     VGI_CUDA(c, cudaMemcpyAsync(&err, c->pack_error.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaMemcpyAsync(&used, c->alloc.ptr, 8, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaMemcpyAsync(c->host_headers.data(), c->headers.ptr, n * sizeof(uint4), cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (err) return fail(c, VGI_ERR_CAPACITY, "cell arena exhausted");
+    if (err & 1u) return fail(c, VGI_ERR_CAPACITY, "cell arena exhausted");
     c->cells_used = used;
     return VGI_OK;
 }
@@ -381,7 +398,7 @@ int vgi_destroy(vgi_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->directory.release(); c->headers.release(); c->cells.release(); c->voxels.release(); c->alloc.release();
-    c->pack_error.release(); c->edit_buf.release(); c->zw.release(); c->region_list.release();
+    c->pack_error.release(); c->edit_buf.release(); c->zw.release(); c->region_list.release(); c->dedup_table.release();
     c->materials.release(); c->lights.release(); c->emitters.release(); c->node_aux.release();
     c->tasks.release(); c->results.release(); c->state.release(); c->slot_meta.release(); c->checkpoint.release();
     c->face_index.release(); c->cache.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
@@ -389,6 +406,8 @@ int vgi_destroy(vgi_ctx* c) {
     c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
     c->w_queue0.release(); c->w_queue1.release(); c->w_scatter.release(); c->w_counters.release();
     for (auto& e : c->marks)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->traverse_marks)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -743,17 +762,25 @@ int vgi_set_layout(vgi_ctx* c, uint32_t layout, uint32_t refill_min) {
 int vgi_set_timing(vgi_ctx* c, int enable) {
     if (!c) return VGI_ERR_INVALID;
     VGI_CUDA(c, cudaSetDevice(c->device));
-    if (enable && !c->marks[0])
+    if (enable && !c->marks[0]) {
         for (auto& e : c->marks) VGI_CUDA(c, cudaEventCreate(&e));
+        for (auto& e : c->traverse_marks) VGI_CUDA(c, cudaEventCreate(&e));
+    }
     c->timing = enable != 0;
     return VGI_OK;
 }
 
-int vgi_frame_times(vgi_ctx* c, float* ms3) {
-    if (!c || !ms3) return VGI_ERR_INVALID;
+int vgi_frame_times(vgi_ctx* c, float* ms4) {
+    if (!c || !ms4) return VGI_ERR_INVALID;
     if (!c->timing) return fail(c, VGI_ERR_STATE, "timing not enabled");
     VGI_CUDA(c, cudaEventSynchronize(c->marks[3]));
-    for (int k = 0; k < 3; ++k) VGI_CUDA(c, cudaEventElapsedTime(&ms3[k], c->marks[k], c->marks[k + 1]));
+    for (int k = 0; k < 3; ++k) VGI_CUDA(c, cudaEventElapsedTime(&ms4[k], c->marks[k], c->marks[k + 1]));
+    ms4[3] = 0.0f;
+    for (uint32_t k = 0; k < c->traverse_launches; ++k) {
+        float ms = 0.0f;
+        VGI_CUDA(c, cudaEventElapsedTime(&ms, c->traverse_marks[2 * k], c->traverse_marks[2 * k + 1]));
+        ms4[3] += ms;
+    }
     return VGI_OK;
 }
 
@@ -780,7 +807,7 @@ int vgi_census(vgi_ctx* c, uint32_t samples, vgi_counters* counters) {
     acc.tasks = c->scratch_tasks.ptr;
     acc.slot_meta = nullptr;  // begin_trace only
     launch_prepare(acc, c->stream);
-    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 10 * 8, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 11 * 8, c->stream));
     TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, c->n_slots, samples, true);
     rc = run_trace(c, tr, true);
     if (rc != VGI_OK) return rc;
@@ -795,7 +822,7 @@ int vgi_trace_tasks(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samp
     VGI_CUDA(c, c->scratch_tasks.reserve((size_t)n * 2));
     VGI_CUDA(c, c->scratch_results.reserve((size_t)n * 6));
     VGI_CUDA(c, cudaMemcpyAsync(c->scratch_tasks.ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
-    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 10 * 8, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 11 * 8, c->stream));
     bool with_cache = c->n_slots > 0;
     TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, n, samples, with_cache);
     rc = run_trace(c, tr, counters != nullptr);

@@ -149,6 +149,50 @@ __global__ void __launch_bounds__(kThreads) classify_pack_kernel(const uint16_t*
     if (tid == 0) headers[r] = make_uint4(3u, (uint32_t)base, 0u, 0u);
 }
 
+// Brick payload deduplication (the reference's intern_brick,
+// gpu_scene.rs:311-335): one thread per brick word of every mixed region.
+// Each mixed brick's 32-word payload is hashed into an open-addressing table
+// of payload pointers; equal payloads (compared word for word, never by hash
+// alone) share the first pointer to claim a slot, and the brick word is
+// repointed to it. Traversal reads the same values; the payloads it touches
+// shrink to one copy each.
+__device__ __forceinline__ uint32_t payload_hash(const uint32_t* p) {
+    uint32_t h = 0x9e3779b9u;
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+        h ^= p[k] + 0x7f4a7c15u + (h << 6) + (h >> 2);
+        h *= 0x85ebca6bu;
+    }
+    return h ^ (h >> 16);
+}
+
+__global__ void dedup_bricks_kernel(const uint4* __restrict__ headers, uint32_t n, uint32_t* __restrict__ cells,
+                                    uint32_t* __restrict__ table, uint32_t mask, uint32_t* __restrict__ error) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = i >> 6, b = i & 63u;
+    if (r >= n) return;
+    const uint4 h = headers[r];
+    if (h.x != 3u) return;
+    const uint32_t word = cells[h.y + b];
+    if ((word & 3u) != 2u) return;
+    const uint32_t mine = word >> 2;
+    const uint32_t* payload = cells + mine;
+    uint32_t slot = payload_hash(payload) & mask;
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+        const uint32_t held = atomicCAS(table + slot, 0xffffffffu, mine);
+        if (held == 0xffffffffu) return;  // first copy: stays canonical
+        bool same = true;
+        const uint32_t* other = cells + held;
+        for (int k = 0; k < 32 && same; ++k) same = other[k] == payload[k];
+        if (same) {
+            cells[h.y + b] = (held << 2) | 2u;
+            return;
+        }
+        slot = (slot + 1u) & mask;
+    }
+    atomicOr(error, 4u);  // table full: the brick keeps its own payload
+}
+
 // Voxel edits: 2 words per edit (region index, local index << 16 | value).
 __global__ void scatter_edits_kernel(const uint2* __restrict__ edits, uint32_t n, uint16_t* __restrict__ voxels) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,6 +216,13 @@ void launch_classify_pack(const uint16_t* voxels, const uint32_t* regions, uint3
                           unsigned long long* alloc, unsigned long long capacity, uint32_t* error, cudaStream_t s) {
     if (grid == 0) return;
     classify_pack_kernel<<<grid, kThreads, 0, s>>>(voxels, regions, n, headers, cells, alloc, capacity, error);
+}
+
+void launch_dedup_bricks(const uint4* headers, uint32_t n, uint32_t* cells, uint32_t* table, uint32_t mask, uint32_t* error,
+                         cudaStream_t s) {
+    if (n == 0) return;
+    const uint64_t threads = (uint64_t)n * 64;
+    dedup_bricks_kernel<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(headers, n, cells, table, mask, error);
 }
 
 void launch_scatter_edits(const uint2* edits, uint32_t n, uint16_t* voxels, cudaStream_t s) {

@@ -38,18 +38,25 @@ struct Cnt {
     __device__ void ray() {}
     __device__ void step() {}
     __device__ void bytes(uint32_t) {}
+    __device__ void tbytes(uint32_t) {}
     __device__ void status(uint32_t) {}
     __device__ void path() {}
     __device__ void unknown() {}
     __device__ void cache_hit() {}
 };
+// Counters of the counting variant. `tb` is the traversal's share of the
+// algorithmic bytes: directory probes, region headers, brick and cell words.
 template <>
 struct Cnt<true> {
     uint32_t rays = 0, steps = 0, paths = 0, unk = 0, hits = 0, st[4] = {0, 0, 0, 0};
-    unsigned long long b = 0;
+    unsigned long long b = 0, tb = 0;
     __device__ void ray() { rays++; }
     __device__ void step() { steps++; }
     __device__ void bytes(uint32_t n) { b += n; }
+    __device__ void tbytes(uint32_t n) {
+        b += n;
+        tb += n;
+    }
     __device__ void status(uint32_t s) { st[s & 3]++; }
     __device__ void path() { paths++; }
     __device__ void unknown() { unk++; }
@@ -88,7 +95,7 @@ __device__ __forceinline__ uint32_t lookup_region(const TraceArgs& A, int x, int
 #pragma unroll 1
     for (uint32_t attempt = 0; attempt < 32u; ++attempt) {
         int4 e = __ldg(A.directory + slot);
-        cnt.bytes(16);
+        cnt.tbytes(16);
         if (e.w == -1) return kNoIndex;
         if (e.x == x && e.y == y && e.z == z) return (uint32_t)e.w;
         slot = (slot + 1u) & A.dir_mask;
@@ -158,7 +165,7 @@ __device__ bool geometry_ahead(const TraceArgs& A, V3 position, V3 dir, float re
         if (remaining < 0.0f || !in_bounds(A, r.x, r.y, r.z)) return false;
         uint32_t index = lookup_region(A, r.x, r.y, r.z, cnt);
         if (index != kNoIndex) {
-            cnt.bytes(16);
+            cnt.tbytes(16);
             if (__ldg(&A.headers[index].x) != 1u) return true;
         }
         float travel = advance_box(position, dir, r, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f).w;
@@ -227,7 +234,7 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
                 cnt.status(res.status);
                 return res;
             }
-            cnt.bytes(16);
+            cnt.tbytes(16);
             meta = __ldg(A.headers + index);
             lrx = rx; lry = ry; lrz = rz;
         }
@@ -240,7 +247,7 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
                 uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
                 uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
                 uint32_t brick = __ldg(A.cells + meta.y + (bz * 4u + by) * 4u + bx);
-                cnt.bytes(4);
+                cnt.tbytes(4);
                 uint32_t state = brick & 3u;
                 if (state == 0u) {
                     uint32_t ext = brick >> 2u;
@@ -251,7 +258,7 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
                 } else {
                     uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
                     uint32_t word = __ldg(A.cells + (brick >> 2u) + (idx >> 1));
-                    cnt.bytes(4);
+                    cnt.tbytes(4);
                     uint32_t cell = (word >> ((idx & 1u) * 16u)) & 65535u;
                     material = (cell & 1u) != 0u ? (cell >> 1u) : 256u;
                     if (material == 256u) {
@@ -815,12 +822,12 @@ __global__ void __launch_bounds__(kBlock) trace_faces_kernel(const TraceArgs A) 
     }
     if constexpr (C) {
         // Warp-aggregate the counters, one atomic per counter per warp.
-        unsigned long long v[10];
+        unsigned long long v[11];
         const Cnt<true>& c = cnt;
         v[0] = c.rays; v[1] = c.paths; v[2] = c.steps; v[3] = c.b; v[4] = c.unk; v[5] = c.hits;
-        v[6] = c.st[0]; v[7] = c.st[1]; v[8] = c.st[2]; v[9] = c.st[3];
+        v[6] = c.st[0]; v[7] = c.st[1]; v[8] = c.st[2]; v[9] = c.st[3]; v[10] = c.tb;
 #pragma unroll
-        for (int k = 0; k < 10; ++k) {
+        for (int k = 0; k < 11; ++k) {
             unsigned long long x = v[k];
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
             if ((threadIdx.x & 31u) == 0u && x) atomicAdd(A.counters + k, x);

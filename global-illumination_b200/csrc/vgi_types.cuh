@@ -64,6 +64,7 @@ struct WaveBuffers {
     uint32_t* counters;       // queue counts [0], [1]; traversal head [2]; scatter count [3]
     uint32_t traverse_blocks; // persistent traversal grid
     uint32_t refill_min;      // idle lanes that trigger a refill
+    cudaEvent_t* traverse_marks;  // optional: start/end events of up to 4 traversal launches
 };
 
 void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);

@@ -294,11 +294,11 @@ __device__ __forceinline__ void stage_materials(const TraceArgs& A, float4* smat
 template <bool C>
 __device__ __forceinline__ void flush_counters(const TraceArgs& A, Cnt<C>& cnt) {
     if constexpr (C) {
-        unsigned long long v[10];
+        unsigned long long v[11];
         v[0] = cnt.rays; v[1] = cnt.paths; v[2] = cnt.steps; v[3] = cnt.b; v[4] = cnt.unk; v[5] = cnt.hits;
-        v[6] = cnt.st[0]; v[7] = cnt.st[1]; v[8] = cnt.st[2]; v[9] = cnt.st[3];
+        v[6] = cnt.st[0]; v[7] = cnt.st[1]; v[8] = cnt.st[2]; v[9] = cnt.st[3]; v[10] = cnt.tb;
 #pragma unroll
-        for (int k = 0; k < 10; ++k) {
+        for (int k = 0; k < 11; ++k) {
             unsigned long long x = v[k];
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
             if ((threadIdx.x & 31u) == 0u && x) atomicAdd(A.counters + k, x);
@@ -481,7 +481,7 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
                 if (index == kNoIndex) {
                     missing = true;
                 } else {
-                    cnt.bytes(16);
+                    cnt.tbytes(16);
                     s.meta = __ldg(A.headers + index);
                     s.lrx = rx;
                     s.lry = ry;
@@ -503,7 +503,7 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
                 const uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
                 const uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
                 const uint32_t brick = __ldg(A.cells + s.meta.y + (bz * 4u + by) * 4u + bx);
-                cnt.bytes(4);
+                cnt.tbytes(4);
                 const uint32_t state = brick & 3u;
                 if (state == 0u) {
                     const uint32_t ext = brick >> 2u;
@@ -517,7 +517,7 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
                 } else {
                     const uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
                     const uint32_t word = __ldg(A.cells + (brick >> 2u) + (idx >> 1));
-                    cnt.bytes(4);
+                    cnt.tbytes(4);
                     const uint32_t c = (word >> ((idx & 1u) * 16u)) & 65535u;
                     if ((c & 1u) != 0u) {
                         status = 1u;
@@ -920,7 +920,9 @@ void wave_run(const WaveBuffers& b, const TraceArgs& a, cudaStream_t s) {
         W.queue_in = qa;
         W.count_in = ca;
         cudaMemsetAsync(W.queue_head, 0, sizeof(uint32_t), s);
+        if (b.traverse_marks && stage <= 4u) cudaEventRecord(b.traverse_marks[2u * (stage - 1u)], s);
         wave_traverse_kernel<B, C><<<b.traverse_blocks, kWaveBlock, 0, s>>>(W, b.refill_min);
+        if (b.traverse_marks && stage <= 4u) cudaEventRecord(b.traverse_marks[2u * (stage - 1u) + 1u], s);
         if (stage == H + 1u) break;
         cudaMemsetAsync(cb, 0, sizeof(uint32_t), s);
         cudaMemsetAsync(W.scatter_count, 0, sizeof(uint32_t), s);

@@ -53,6 +53,7 @@ class Counters(ctypes.Structure):
         ("unknown", ctypes.c_uint64),
         ("cache_hits", ctypes.c_uint64),
         ("status", ctypes.c_uint64 * 4),
+        ("traverse_bytes", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -388,8 +389,9 @@ class GpuTracer:
         self._check(self._lib.vgi_set_timing(self._h, int(enable)))
 
     def frame_times(self) -> np.ndarray:
-        """Device ms of the last frame's prepare, trace and accumulate."""
-        out = np.zeros(3, np.float32)
+        """Device ms of the last frame's prepare, trace and accumulate, and the
+        summed traversal launches of the wavefront layout."""
+        out = np.zeros(4, np.float32)
         self._check(self._lib.vgi_frame_times(self._h, _ptr(out)))
         return out
 

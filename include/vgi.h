@@ -78,6 +78,8 @@ typedef struct {
     uint64_t unknown;     /* paths that reached unloaded space */
     uint64_t cache_hits;  /* paths ended by the world-cache gather */
     uint64_t status[4];   /* rays by status: escaped, hit, unknown, reach */
+    uint64_t traverse_bytes; /* the traversal's share of `bytes`: directory,
+                                header, brick and cell words */
 } vgi_counters;
 
 /* ---- lifecycle: GpuTracer::new / drop (src/gpu.rs:448-595) ---------------- */
@@ -143,11 +145,12 @@ int vgi_frame(vgi_ctx* ctx, uint32_t samples, uint32_t clock_ms);
 int vgi_set_layout(vgi_ctx* ctx, uint32_t layout, uint32_t refill_min);
 /* Device timing of vgi_frame (the reference's timestamp query pairs,
  * src/gpu.rs:488-500): with timing enabled each frame records CUDA events on
- * the context's stream around prepare, trace and accumulate, and
- * vgi_frame_times returns the last frame's three durations in ms
- * (synchronises the stream). */
+ * the context's stream around prepare, trace and accumulate, and around each
+ * traversal launch of the wavefront layout. vgi_frame_times returns the last
+ * frame's prepare, trace and accumulate durations and the summed traversal
+ * time (0 for the single-kernel layout), in ms; it synchronises the stream. */
 int vgi_set_timing(vgi_ctx* ctx, int enable);
-int vgi_frame_times(vgi_ctx* ctx, float* ms3);
+int vgi_frame_times(vgi_ctx* ctx, float* ms4);
 /* The same frame through host buffers (submit_compact + complete_readback):
  * 8-word tasks in (one per slot, in slot order; their sequence words are
  * replaced by the slot's), 24-word results out. Synchronous. */

@@ -24,6 +24,7 @@ typedef struct orc_scene orc_scene;
 typedef struct {
     uint64_t rays, paths, steps, bytes, unknown, cache_hits;
     uint64_t status[4];
+    uint64_t traverse_bytes;  // the traversal's share of bytes (directory, header, brick, cell)
 } orc_counters;
 
 typedef struct {

@@ -48,6 +48,12 @@ struct Model {
 struct Counters {
     uint64_t rays = 0, paths = 0, steps = 0, bytes = 0, unknown = 0, cache_hits = 0;
     uint64_t status[4] = {0, 0, 0, 0};
+    uint64_t traverse_bytes = 0;
+    // Bytes the traversal reads (directory probes, headers, brick and cell words).
+    void tbytes(uint64_t n) {
+        bytes += n;
+        traverse_bytes += n;
+    }
 };
 
 struct Ctx {
@@ -82,7 +88,7 @@ static uint32_t lookup_region(Ctx& x, i3 c) {
     uint32_t slot = hash_voxel(c.x, c.y, c.z) & x.g.mask;
     for (uint32_t attempt = 0; attempt < 32u; ++attempt) {
         const int32_t* e = x.g.directory + (size_t)slot * 4;
-        x.c.bytes += 16;
+        x.c.tbytes(16);
         if (e[3] == -1) return 0xffffffffu;
         if (e[0] == c.x && e[1] == c.y && e[2] == c.z) return (uint32_t)e[3];
         slot = (slot + 1u) & x.g.mask;
@@ -135,7 +141,7 @@ static bool geometry_ahead(Ctx& x, f3 start, f3 dir, float max_distance) {
         if (remaining < 0.0f || !in_bounds(x, region)) return false;
         uint32_t index = lookup_region(x, region);
         if (index != 0xffffffffu) {
-            x.c.bytes += 16;
+            x.c.tbytes(16);
             if (x.g.headers[(size_t)index * 4] != 1u) return true;
         }
         float travel = advance_box(position, dir, region, i3{0, 0, 0}, i3{0, 0, 0}, 16.0f).w;
@@ -194,7 +200,7 @@ static RayResult trace_domain_limited(Ctx& x, f3 origin, f3 dir, float max_dista
                 x.c.status[result.status] += 1;
                 return result;
             }
-            x.c.bytes += 16;
+            x.c.tbytes(16);
             const uint32_t* h = x.g.headers + (size_t)index * 4;
             meta[0] = h[0]; meta[1] = h[1]; meta[2] = h[2]; meta[3] = h[3];
             last_region = region;
@@ -208,7 +214,7 @@ static RayResult trace_domain_limited(Ctx& x, f3 origin, f3 dir, float max_dista
                 uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
                 uint32_t bx = lx / 4u, by = ly / 4u, bz = lz / 4u;
                 uint32_t brick_data = x.g.cells[meta[1] + (bz * 4u + by) * 4u + bx];
-                x.c.bytes += 4;
+                x.c.tbytes(4);
                 uint32_t state = brick_data & 3u;
                 if (state == 0u) {
                     uint32_t ext = brick_data >> 2u;
@@ -221,7 +227,7 @@ static RayResult trace_domain_limited(Ctx& x, f3 origin, f3 dir, float max_dista
                     uint32_t ix = lx & 3u, iy = ly & 3u, iz = lz & 3u;
                     uint32_t idx = (iz * 4u + iy) * 4u + ix;
                     uint32_t word = x.g.cells[(brick_data >> 2u) + idx / 2u];
-                    x.c.bytes += 4;
+                    x.c.tbytes(4);
                     uint32_t cell = (word >> ((idx & 1u) * 16u)) & 65535u;
                     material = (cell & 1u) != 0u ? (cell >> 1u) : 256u;
                     if (material == 256u) {
@@ -717,6 +723,7 @@ static void add_counters(Counters& a, const Counters& b) {
     a.rays += b.rays; a.paths += b.paths; a.steps += b.steps; a.bytes += b.bytes;
     a.unknown += b.unknown; a.cache_hits += b.cache_hits;
     for (int i = 0; i < 4; ++i) a.status[i] += b.status[i];
+    a.traverse_bytes += b.traverse_bytes;
 }
 
 // ---- voxel_retention.wgsl / voxel_accumulate.wgsl ----------------------------
@@ -880,6 +887,7 @@ int orc_trace_faces(const int32_t* directory, uint64_t slots, const uint32_t* he
         counters->rays = total.rays; counters->paths = total.paths; counters->steps = total.steps;
         counters->bytes = total.bytes; counters->unknown = total.unknown; counters->cache_hits = total.cache_hits;
         for (int i = 0; i < 4; ++i) counters->status[i] = total.status[i];
+        counters->traverse_bytes = total.traverse_bytes;
     }
     return 0;
 }

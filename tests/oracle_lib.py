@@ -26,7 +26,7 @@ _F = ctypes.c_float
 
 class Counters(ctypes.Structure):
     _fields_ = [("rays", _U64), ("paths", _U64), ("steps", _U64), ("bytes", _U64), ("unknown", _U64),
-                ("cache_hits", _U64), ("status", _U64 * 4)]
+                ("cache_hits", _U64), ("status", _U64 * 4), ("traverse_bytes", _U64)]
 
     def as_dict(self):
         d = {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "status"}
