@@ -33,6 +33,10 @@ sys.path.insert(0, os.path.join(ROOT, "global-illumination_b200"))
 EYE = (256.0, 200.0, 256.0)
 SPP = 8
 BOUNCES = 2
+# Kernels vgi_frame launches in the wavefront layout: prepare, begin,
+# (traverse, shade, scatter) per diffuse hit, the last traverse, finalize and
+# accumulate.
+LAUNCHES_PER_FRAME = 2 + 3 * BOUNCES + 1 + 2
 METRIC = "rays/s and ms/frame at equal relMSE vs FP64 ref: MLP cache vs plain, 1 B200"
 WORKLOAD = "terrain 512x256x512 fBm, sun + 256 emissive voxels, faces facing a cube-map camera at (256,200,256), 8 spp, 2 bounces via world cache, FP32"
 
@@ -125,6 +129,14 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def lane_use(census):
+    """Rays in flight per warp pass of the traversal loop, while rays remained
+    queued and after the queue ran out, and the drain's share of passes."""
+    wp, lp = census["warp_passes"], census["lane_passes"]
+    total = max(wp[0] + wp[1], 1)
+    return {"queued": lp[0] / max(wp[0], 1), "drain": lp[1] / max(wp[1], 1), "drain_pass_share": wp[1] / total}
+
+
 def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total, budget_s=15.0):
     """The oracle on a bounded face sample with the GPU's warm cache state."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -152,7 +164,7 @@ def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit,
         tasks[:, 4] += SPP
         rays += cnt["rays"]
         chunks += 1
-        if time.perf_counter() - start > budget_s or chunks >= 1000:
+        if time.perf_counter() - start > budget_s or chunks >= 100000:
             break
     elapsed = time.perf_counter() - start
     return {"value": rays / elapsed, "unit": "rays/s", "cores": threads, "kind": "port",
@@ -351,6 +363,7 @@ def main():
                        "census": {"steps": before["steps"], "bytes": before["bytes"], "traverse_bytes": before["traverse_bytes"],
                                   "cache_hits": before["cache_hits"],
                                   "unknown": before["unknown"], "status": before["status"]},
+                       "traverse_lanes": lane_use(before),
                        "l2": "256 MB buffer written between timed frames (outside the event pair)",
                        "kernel_ms": {"prepare": float(np.mean([t[0] for t in kernel_ms])), "trace": trace_ms,
                                      "traverse": traverse_ms, "accumulate": float(np.mean([t[2] for t in kernel_ms]))},
@@ -358,7 +371,7 @@ def main():
                        "paths_per_s": paths_per_frame * world / (total_ms * 1e-3 / args.steps),
                        "frames_per_s": 1000.0 * args.steps / total_ms},
             "e2e": {"value": total_rays / (e2e_total * 1e-3), "unit": "rays/s", "h2d_bytes_per_step": int(n * 32), "d2h_bytes_per_step": int(n * 96)},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": LAUNCHES_PER_FRAME * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_source": peak_kind, "kernel": "wave_traverse_kernel",
                          "launches_per_frame": traverse_launches,

@@ -287,7 +287,7 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
 }
 
 int read_counters(vgi_ctx* c, vgi_counters* out) {
-    unsigned long long h[11];
+    unsigned long long h[kCounterWords];
     VGI_CUDA(c, cudaMemcpyAsync(h, c->counters.ptr, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     if (out) {
@@ -299,6 +299,10 @@ int read_counters(vgi_ctx* c, vgi_counters* out) {
         out->cache_hits = h[5];
         for (int k = 0; k < 4; ++k) out->status[k] = h[6 + k];
         out->traverse_bytes = h[10];
+        for (int k = 0; k < 2; ++k) {
+            out->warp_passes[k] = h[11 + k];
+            out->lane_passes[k] = h[13 + k];
+        }
     }
     return VGI_OK;
 }
@@ -807,7 +811,7 @@ int vgi_census(vgi_ctx* c, uint32_t samples, vgi_counters* counters) {
     acc.tasks = c->scratch_tasks.ptr;
     acc.slot_meta = nullptr;  // begin_trace only
     launch_prepare(acc, c->stream);
-    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 11 * 8, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, kCounterWords * 8, c->stream));
     TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, c->n_slots, samples, true);
     rc = run_trace(c, tr, true);
     if (rc != VGI_OK) return rc;
@@ -822,7 +826,7 @@ int vgi_trace_tasks(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samp
     VGI_CUDA(c, c->scratch_tasks.reserve((size_t)n * 2));
     VGI_CUDA(c, c->scratch_results.reserve((size_t)n * 6));
     VGI_CUDA(c, cudaMemcpyAsync(c->scratch_tasks.ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
-    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, 11 * 8, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, kCounterWords * 8, c->stream));
     bool with_cache = c->n_slots > 0;
     TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, n, samples, with_cache);
     rc = run_trace(c, tr, counters != nullptr);

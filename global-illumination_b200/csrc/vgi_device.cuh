@@ -41,6 +41,28 @@ __device__ __forceinline__ float len3(V3 a) { return __fsqrt_rn(dot3(a, a)); }
 __device__ __forceinline__ V3 normalize3(V3 a) { return a / len3(a); }
 __device__ __forceinline__ V3 itof(I3 a) { return V3{(float)a.x, (float)a.y, (float)a.z}; }
 
+// a / b rounded to nearest, from y = RN(1/b), for a ray's repeated divisions
+// by its direction components. Two Markstein corrections of q = RN(a y)
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990): the first brings q within
+// one ulp of a / b, so the remainder a - b q is exact in the fma, and the
+// second then rounds correctly since y is within half an ulp of 1 / b. The
+// traversal calls it with b a direction component, 1e-8 < |b| <= 1 (or
+// b = y = 1, where it is exact), and a a difference of positions, so no step
+// overflows or underflows and the result equals the IEEE quotient.
+__device__ __forceinline__ float div_recip(float a, float b, float y) {
+    float q = __fmul_rn(a, y);
+    float r = __fmaf_rn(-b, q, a);
+    q = __fmaf_rn(r, y, q);
+    r = __fmaf_rn(-b, q, a);
+    return __fmaf_rn(r, y, q);
+}
+// The reciprocals div_recip needs for a direction, with 1 for the axes the
+// traversal treats as not moving (|d| <= 1e-8), which it divides by 1.
+__device__ __forceinline__ V3 direction_recip(V3 d) {
+    return V3{fabsf(d.x) > 1e-8f ? __frcp_rn(d.x) : 1.0f, fabsf(d.y) > 1e-8f ? __frcp_rn(d.y) : 1.0f,
+              fabsf(d.z) > 1e-8f ? __frcp_rn(d.z) : 1.0f};
+}
+
 // WGSL i32(f32) / u32(f32): truncate, saturate, NaN -> 0.
 __device__ __forceinline__ int f2i(float x) { return __float2int_rz(x); }
 __device__ __forceinline__ uint32_t f2u(float x) { return __float2uint_rz(x); }

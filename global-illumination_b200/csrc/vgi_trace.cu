@@ -49,6 +49,7 @@ struct Cnt {
 template <>
 struct Cnt<true> {
     uint32_t rays = 0, steps = 0, paths = 0, unk = 0, hits = 0, st[4] = {0, 0, 0, 0};
+    uint32_t wp[2] = {0, 0}, lp[2] = {0, 0};
     unsigned long long b = 0, tb = 0;
     __device__ void ray() { rays++; }
     __device__ void step() { steps++; }
@@ -108,25 +109,31 @@ __device__ __forceinline__ bool in_bounds(const TraceArgs& A, int x, int y, int 
 }
 
 // advance_box (voxel_traversal.wgsl:90-107): exit normal and distance of the
-// ray from the box (cell - neg, cell + pos + 1) * size.
-__device__ __forceinline__ float4 advance_box(V3 p, V3 d, I3 cell, I3 ng, I3 ps, float size) {
+// ray from the box (cell - neg, cell + pos + 1) * size. It is split in two:
+// box_planes picks the exit plane per axis from the direction's sign, and
+// advance_planes runs the rest, so a ray that stays in one box can reuse its
+// planes. `inv` holds the direction's reciprocals (direction_recip), so each
+// division is div_recip.
+__device__ __forceinline__ V3 box_planes(V3 d, I3 cell, I3 ng, I3 ps, float size) {
+    return V3{d.x > 0.0f ? __fmul_rn((float)(cell.x + ps.x + 1), size) : __fmul_rn((float)(cell.x - ng.x), size),
+              d.y > 0.0f ? __fmul_rn((float)(cell.y + ps.y + 1), size) : __fmul_rn((float)(cell.y - ng.y), size),
+              d.z > 0.0f ? __fmul_rn((float)(cell.z + ps.z + 1), size) : __fmul_rn((float)(cell.z - ng.z), size)};
+}
+__device__ __forceinline__ float4 advance_planes(V3 p, V3 d, V3 inv, V3 plane) {
     float tx, ty, tz;
     {
         bool moving = fabsf(d.x) > 1e-8f;
-        float plane = d.x > 0.0f ? __fmul_rn((float)(cell.x + ps.x + 1), size) : __fmul_rn((float)(cell.x - ng.x), size);
-        float raw = __fdiv_rn(__fsub_rn(plane, p.x), moving ? d.x : 1.0f);
+        float raw = div_recip(__fsub_rn(plane.x, p.x), moving ? d.x : 1.0f, inv.x);
         tx = (moving && raw >= -0.001f && raw < 1e30f) ? raw : 1e30f;
     }
     {
         bool moving = fabsf(d.y) > 1e-8f;
-        float plane = d.y > 0.0f ? __fmul_rn((float)(cell.y + ps.y + 1), size) : __fmul_rn((float)(cell.y - ng.y), size);
-        float raw = __fdiv_rn(__fsub_rn(plane, p.y), moving ? d.y : 1.0f);
+        float raw = div_recip(__fsub_rn(plane.y, p.y), moving ? d.y : 1.0f, inv.y);
         ty = (moving && raw >= -0.001f && raw < 1e30f) ? raw : 1e30f;
     }
     {
         bool moving = fabsf(d.z) > 1e-8f;
-        float plane = d.z > 0.0f ? __fmul_rn((float)(cell.z + ps.z + 1), size) : __fmul_rn((float)(cell.z - ng.z), size);
-        float raw = __fdiv_rn(__fsub_rn(plane, p.z), moving ? d.z : 1.0f);
+        float raw = div_recip(__fsub_rn(plane.z, p.z), moving ? d.z : 1.0f, inv.z);
         tz = (moving && raw >= -0.001f && raw < 1e30f) ? raw : 1e30f;
     }
     bool choose_y = ty < wmax(tx, 0.0f);
@@ -144,6 +151,9 @@ __device__ __forceinline__ float4 advance_box(V3 p, V3 d, I3 cell, I3 ng, I3 ps,
     r.w = wmax(__fadd_rn(dist, 0.001f), 0.001f);
     return r;
 }
+__device__ __forceinline__ float4 advance_box(V3 p, V3 d, V3 inv, I3 cell, I3 ng, I3 ps, float size) {
+    return advance_planes(p, d, inv, box_planes(d, cell, ng, ps, size));
+}
 
 __device__ __forceinline__ I3 unpack_bytes(uint32_t v) { return I3{(int)(v & 255u), (int)((v >> 8) & 255u), (int)((v >> 16) & 255u)}; }
 __device__ __forceinline__ I3 neg_ext(uint32_t b) { return I3{(int)(b & 3u), (int)((b >> 4) & 3u), (int)((b >> 8) & 3u)}; }
@@ -157,7 +167,7 @@ __device__ __forceinline__ I3 floor_div16(V3 p) {
 
 // geometry_ahead (voxel_traversal.wgsl:108-121)
 template <bool C>
-__device__ bool geometry_ahead(const TraceArgs& A, V3 position, V3 dir, float remaining, Cnt<C>& cnt) {
+__device__ bool geometry_ahead(const TraceArgs& A, V3 position, V3 dir, V3 inv, float remaining, Cnt<C>& cnt) {
 #pragma unroll 1
     for (uint32_t step = 0; step < 2048u; ++step) {
         cnt.step();
@@ -168,7 +178,7 @@ __device__ bool geometry_ahead(const TraceArgs& A, V3 position, V3 dir, float re
             cnt.tbytes(16);
             if (__ldg(&A.headers[index].x) != 1u) return true;
         }
-        float travel = advance_box(position, dir, r, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f).w;
+        float travel = advance_box(position, dir, inv, r, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f).w;
         position = position + dir * travel;
         remaining = __fsub_rn(remaining, travel);
     }
@@ -188,15 +198,16 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
     res.normal = V3{0.0f, 0.0f, 0.0f};
     float nearv = -1e30f, farv = 1e30f;
     V3 normal{0.0f, 0.0f, 0.0f};
+    const V3 inv = direction_recip(dir);
     const float mnx = __fmul_rn((float)A.mn[0], 16.0f), mny = __fmul_rn((float)A.mn[1], 16.0f), mnz = __fmul_rn((float)A.mn[2], 16.0f);
     const float mxx = __fmul_rn((float)(A.mx[0] + 1), 16.0f), mxy = __fmul_rn((float)(A.mx[1] + 1), 16.0f),
                 mxz = __fmul_rn((float)(A.mx[2] + 1), 16.0f);
-#define VGI_SLAB(AX, O, D, MN, MX)                                              \
+#define VGI_SLAB(AX, O, D, Y, MN, MX)                                           \
     if (fabsf(D) <= 1e-8f) {                                                    \
         if (O < MN || O > MX) { cnt.status(0); return res; }                    \
     } else {                                                                    \
-        float first = __fdiv_rn(__fsub_rn(MN, O), D);                           \
-        float second = __fdiv_rn(__fsub_rn(MX, O), D);                          \
+        float first = div_recip(__fsub_rn(MN, O), D, Y);                        \
+        float second = div_recip(__fsub_rn(MX, O), D, Y);                       \
         if (wmin(first, second) > nearv) {                                      \
             nearv = wmin(first, second);                                        \
             float s = first < second ? -1.0f : 1.0f;                            \
@@ -204,9 +215,9 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
         }                                                                       \
         farv = wmin(farv, wmax(first, second));                                 \
     }
-    VGI_SLAB(0, origin.x, dir.x, mnx, mxx)
-    VGI_SLAB(1, origin.y, dir.y, mny, mxy)
-    VGI_SLAB(2, origin.z, dir.z, mnz, mxz)
+    VGI_SLAB(0, origin.x, dir.x, inv.x, mnx, mxx)
+    VGI_SLAB(1, origin.y, dir.y, inv.y, mny, mxy)
+    VGI_SLAB(2, origin.z, dir.z, inv.z, mnz, mxz)
 #undef VGI_SLAB
     if (farv < wmax(nearv, 0.0f)) { cnt.status(0); return res; }
     float distance = __fadd_rn(wmax(nearv, 0.0f), 0.001f);
@@ -224,13 +235,13 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
             uint32_t index = lookup_region(A, rx, ry, rz, cnt);
             if (index == kNoIndex) {
                 if (visible_geometry) {
-                    float4 adv = advance_box(position, dir, I3{rx, ry, rz}, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f);
+                    float4 adv = advance_box(position, dir, inv, I3{rx, ry, rz}, I3{0, 0, 0}, I3{0, 0, 0}, 16.0f);
                     distance = __fadd_rn(distance, adv.w);
                     position = position + dir * adv.w;
                     normal = V3{adv.x, adv.y, adv.z};
                     continue;
                 }
-                res.status = geometry_ahead(A, position, dir, __fsub_rn(max_distance, distance), cnt) ? 2u : 0u;
+                res.status = geometry_ahead(A, position, dir, inv, __fsub_rn(max_distance, distance), cnt) ? 2u : 0u;
                 cnt.status(res.status);
                 return res;
             }
@@ -240,7 +251,7 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
         }
         float4 adv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (meta.x == 1u) {
-            adv = advance_box(position, dir, I3{rx, ry, rz}, unpack_bytes(meta.z), unpack_bytes(meta.w), 16.0f);
+            adv = advance_box(position, dir, inv, I3{rx, ry, rz}, unpack_bytes(meta.z), unpack_bytes(meta.w), 16.0f);
         } else {
             uint32_t material = meta.y;
             if (meta.x == 3u) {
@@ -251,7 +262,7 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
                 uint32_t state = brick & 3u;
                 if (state == 0u) {
                     uint32_t ext = brick >> 2u;
-                    adv = advance_box(position, dir, I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz}, neg_ext(ext), pos_ext(ext), 4.0f);
+                    adv = advance_box(position, dir, inv, I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz}, neg_ext(ext), pos_ext(ext), 4.0f);
                     material = 256u;
                 } else if (state == 1u) {
                     material = brick >> 2u;
@@ -263,7 +274,7 @@ __device__ Ray trace_domain(const TraceArgs& A, V3 origin, V3 dir, float max_dis
                     material = (cell & 1u) != 0u ? (cell >> 1u) : 256u;
                     if (material == 256u) {
                         uint32_t ext = cell >> 1u;
-                        adv = advance_box(position, dir, voxel, neg_ext(ext), pos_ext(ext), 1.0f);
+                        adv = advance_box(position, dir, inv, voxel, neg_ext(ext), pos_ext(ext), 1.0f);
                     }
                 }
             }
@@ -546,7 +557,7 @@ struct Tracer {
     __device__ Ray trace_diffuse(V3 origin, V3 dir) {
         float r = reach();
         Ray hit = trace(origin, dir, r);
-        if (LIMITED && hit.status == 0u && geometry_ahead(A, origin + dir * r, dir, __fsub_rn(A.max_distance, r), cnt)) hit.status = 3u;
+        if (LIMITED && hit.status == 0u && geometry_ahead(A, origin + dir * r, dir, direction_recip(dir), __fsub_rn(A.max_distance, r), cnt)) hit.status = 3u;
         return hit;
     }
     // voxel_path.wgsl:283-307 (value rgb; custom_visible only at the face centre)

@@ -6,6 +6,8 @@
 namespace vgi {
 
 constexpr uint32_t kNoIndex = 0xffffffffu;
+// Counter words of the counting variants, in vgi_counters order.
+constexpr int kCounterWords = 15;
 
 // Everything the face trace reads. Geometry and cache arrays are read-only
 // for the kernel's lifetime and are loaded through the non-coherent path.

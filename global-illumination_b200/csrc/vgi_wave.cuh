@@ -294,11 +294,12 @@ __device__ __forceinline__ void stage_materials(const TraceArgs& A, float4* smat
 template <bool C>
 __device__ __forceinline__ void flush_counters(const TraceArgs& A, Cnt<C>& cnt) {
     if constexpr (C) {
-        unsigned long long v[11];
+        unsigned long long v[kCounterWords];
         v[0] = cnt.rays; v[1] = cnt.paths; v[2] = cnt.steps; v[3] = cnt.b; v[4] = cnt.unk; v[5] = cnt.hits;
         v[6] = cnt.st[0]; v[7] = cnt.st[1]; v[8] = cnt.st[2]; v[9] = cnt.st[3]; v[10] = cnt.tb;
+        v[11] = cnt.wp[0]; v[12] = cnt.wp[1]; v[13] = cnt.lp[0]; v[14] = cnt.lp[1];
 #pragma unroll
-        for (int k = 0; k < 11; ++k) {
+        for (int k = 0; k < kCounterWords; ++k) {
             unsigned long long x = v[k];
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
             if ((threadIdx.x & 31u) == 0u && x) atomicAdd(A.counters + k, x);
@@ -380,11 +381,19 @@ __global__ void __launch_bounds__(kWaveBlock) wave_begin_kernel(const WaveArgs W
 
 // One lane's ray in flight: trace_domain_limited's loop variables.
 struct RayRun {
-    V3 dir, pos, nrm;
+    V3 dir, inv, pos, nrm;
     float dist, maxd;
     int lrx, lry, lrz;
     uint4 meta;
     uint32_t step, slot;
+    // The box of the last step: its exit planes, and the voxel position
+    // shifted by the level it was found at (4 region, 2 brick, 0 voxel). A
+    // step whose voxel has the same key looks up the same box, so it reuses
+    // the planes. Rays that graze a face, where the move across the face is
+    // lost to rounding, take up to the step budget inside one box this way.
+    V3 plane;
+    int kx, ky, kz;
+    uint32_t shift;  // kNoIndex: no box cached
     bool full;
 };
 
@@ -411,6 +420,7 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
     s.slot = slot;
     s.full = (bits(rd.w) & 1u) != 0u;
     s.dir = V3{rd.x, rd.y, rd.z};
+    s.inv = direction_recip(s.dir);
     s.maxd = ro.w;
     cnt.ray();
     const V3 origin{ro.x, ro.y, ro.z}, dir = s.dir;
@@ -421,12 +431,12 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
                 mxz = __fmul_rn((float)(A.mx[2] + 1), 16.0f);
     const I3 zi{0, 0, 0};
     const V3 zv{0.0f, 0.0f, 0.0f};
-#define VGI_SLAB(AX, O, D, MN, MX)                                                      \
+#define VGI_SLAB(AX, O, D, Y, MN, MX)                                                   \
     if (fabsf(D) <= 1e-8f) {                                                            \
         if (O < MN || O > MX) { cnt.status(0); finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv); return; } \
     } else {                                                                            \
-        float first = __fdiv_rn(__fsub_rn(MN, O), D);                                   \
-        float second = __fdiv_rn(__fsub_rn(MX, O), D);                                  \
+        float first = div_recip(__fsub_rn(MN, O), D, Y);                                \
+        float second = div_recip(__fsub_rn(MX, O), D, Y);                               \
         if (wmin(first, second) > nearv) {                                              \
             nearv = wmin(first, second);                                                \
             float sg = first < second ? -1.0f : 1.0f;                                   \
@@ -434,9 +444,9 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
         }                                                                               \
         farv = wmin(farv, wmax(first, second));                                         \
     }
-    VGI_SLAB(0, origin.x, dir.x, mnx, mxx)
-    VGI_SLAB(1, origin.y, dir.y, mny, mxy)
-    VGI_SLAB(2, origin.z, dir.z, mnz, mxz)
+    VGI_SLAB(0, origin.x, dir.x, s.inv.x, mnx, mxx)
+    VGI_SLAB(1, origin.y, dir.y, s.inv.y, mny, mxy)
+    VGI_SLAB(2, origin.z, dir.z, s.inv.z, mnz, mxz)
 #undef VGI_SLAB
     if (farv < wmax(nearv, 0.0f)) {
         cnt.status(0);
@@ -448,23 +458,69 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
     s.nrm = normal;
     s.lrx = s.lry = s.lrz = 0x7fffffff;
     s.meta = make_uint4(0, 0, 0, 0);
+    s.shift = kNoIndex;
     s.step = 0;
 }
 
 // One iteration of trace_domain_limited's loop (voxel_traversal.wgsl:152-213),
 // including the out-of-steps exit (:214-218). The branches only decide the
 // outcome: either the ray ends (one finish below) or it skips a box, whose
-// cell, extents and size they choose for the single advance_box call. The
-// lanes of a warp take different branches, but none of them runs the box
-// step on its own.
+// cell, extents and size they choose for the single box step. The lanes of a
+// warp take different branches, but none of them runs the box step on its
+// own. A step inside the box of the previous step skips the lookups (see
+// RayRun) and counts the words the lookup would have read.
+// Steps of a ray that grazes a face of its box. If some moving axis's exit
+// distance lies in [-0.001, 0] and adding dir * 0.001 cannot change that
+// coordinate (the move rounds away), then every later step in the same box
+// exits at distance 0: advance_box returns exactly 0.001 (any exit distance
+// <= 0 makes its selected distance 0), the coordinate stays, and so does the
+// exit distance. Those steps are replayed here as what they are, four
+// additions each, while the voxel keeps the box's key, and only the last
+// one's normal is computed in full. Every value equals the general step's.
+// `limit` bounds the replayed step count (it is the step budget once the
+// queue is empty, so a lane then finishes its creep in one pass).
+template <bool C>
+__device__ __forceinline__ void creep(const TraceArgs& A, RayRun& s, Cnt<C>& cnt, uint32_t limit) {
+    const V3 c = s.dir * 0.001f;
+    bool stuck = false;
+#define VGI_STUCK(AX)                                                                                              \
+    if (fabsf(s.dir.AX) > 1e-8f) {                                                                                 \
+        const float raw = div_recip(__fsub_rn(s.plane.AX, s.pos.AX), s.dir.AX, s.inv.AX);                           \
+        if (raw >= -0.001f && raw <= 0.0f && __fadd_rn(s.pos.AX, c.AX) == s.pos.AX) stuck = true;                  \
+    }
+    VGI_STUCK(x)
+    VGI_STUCK(y)
+    VGI_STUCK(z)
+#undef VGI_STUCK
+    if (!stuck) return;
+    const uint32_t bytes = s.shift == 4u ? 0u : (s.shift == 2u ? 4u : 8u);
+    const uint32_t end = limit < A.path_steps ? limit : A.path_steps;
+    V3 last = s.pos;
+    bool ran = false;
+#pragma unroll 1
+    while (s.step < end && !(s.dist > s.maxd)) {
+        const int vx = f2i(floorf(s.pos.x)), vy = f2i(floorf(s.pos.y)), vz = f2i(floorf(s.pos.z));
+        if ((vx >> s.shift) != s.kx || (vy >> s.shift) != s.ky || (vz >> s.shift) != s.kz) break;
+        cnt.step();
+        cnt.tbytes(bytes);
+        last = s.pos;
+        ran = true;
+        s.dist = __fadd_rn(s.dist, 0.001f);
+        s.pos = s.pos + c;
+        s.step += 1u;
+    }
+    if (ran) {
+        const float4 a = advance_planes(last, s.dir, s.inv, s.plane);
+        s.nrm = V3{a.x, a.y, a.z};
+    }
+}
+
 template <bool BUDGETED, bool C>
-__device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& cnt) {
+__device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& cnt, uint32_t creep_limit) {
     const TraceArgs& A = W.t;
     constexpr uint32_t kGo = 0xffffffffu;
     uint32_t status = kGo, material = 0u;
     I3 voxel{0, 0, 0};
-    I3 cell{0, 0, 0}, ng{0, 0, 0}, ps{0, 0, 0};
-    float size = 16.0f;
     if (s.step >= A.path_steps) {
         status = 2u;
         material = 0xffffffffu;
@@ -472,9 +528,18 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
         cnt.step();
         voxel = I3{f2i(floorf(s.pos.x)), f2i(floorf(s.pos.y)), f2i(floorf(s.pos.z))};
         const int rx = voxel.x >> 4, ry = voxel.y >> 4, rz = voxel.z >> 4;
-        if (s.dist > s.maxd || !in_bounds(A, rx, ry, rz)) {
+        const bool same = s.shift != kNoIndex && (voxel.x >> s.shift) == s.kx && (voxel.y >> s.shift) == s.ky &&
+                          (voxel.z >> s.shift) == s.kz;
+        if (same) {
+            // Same region (so in bounds), same brick or voxel: the same box.
+            if (s.dist > s.maxd) status = 0u;
+            else cnt.tbytes(s.shift == 4u ? 0u : (s.shift == 2u ? 4u : 8u));
+        } else if (s.dist > s.maxd || !in_bounds(A, rx, ry, rz)) {
             status = 0u;
         } else {
+            I3 cell{0, 0, 0}, ng{0, 0, 0}, ps{0, 0, 0};
+            float size = 16.0f;
+            uint32_t shift = 4u;
             bool missing = false;
             if (s.lrx != rx || s.lry != ry || s.lrz != rz) {
                 const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
@@ -492,7 +557,8 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
             if (missing) {
                 // visible_geometry crosses a missing region; otherwise the ray
                 // ends as unknown or escaped by geometry_ahead.
-                if (!BUDGETED) status = geometry_ahead(A, s.pos, s.dir, __fsub_rn(s.maxd, s.dist), cnt) ? 2u : 0u;
+                if (!BUDGETED) status = geometry_ahead(A, s.pos, s.dir, s.inv, __fsub_rn(s.maxd, s.dist), cnt) ? 2u : 0u;
+                shift = kNoIndex;
             } else if (s.meta.x == 1u) {
                 ng = unpack_bytes(s.meta.z);
                 ps = unpack_bytes(s.meta.w);
@@ -511,6 +577,7 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
                     ng = neg_ext(ext);
                     ps = pos_ext(ext);
                     size = 4.0f;
+                    shift = 2u;
                 } else if (state == 1u) {
                     status = 1u;
                     material = brick >> 2u;
@@ -528,7 +595,19 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
                         ng = neg_ext(ext);
                         ps = pos_ext(ext);
                         size = 1.0f;
+                        shift = 0u;
                     }
+                }
+            }
+            if (status == kGo) {
+                // A missing region crossed under the budget rule is looked up
+                // again at every step, so its box is not kept.
+                s.plane = box_planes(s.dir, cell, ng, ps, size);
+                s.shift = shift;
+                if (shift != kNoIndex) {
+                    s.kx = voxel.x >> shift;
+                    s.ky = voxel.y >> shift;
+                    s.kz = voxel.z >> shift;
                 }
             }
         }
@@ -540,11 +619,12 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
         finish_ray<BUDGETED>(W, s, status, material, hit ? voxel : I3{0, 0, 0}, hit ? s.pos : zv, hit ? s.nrm : zv);
         return;
     }
-    const float4 adv = advance_box(s.pos, s.dir, cell, ng, ps, size);
+    const float4 adv = advance_planes(s.pos, s.dir, s.inv, s.plane);
     s.dist = __fadd_rn(s.dist, adv.w);
     s.pos = s.pos + s.dir * adv.w;
     s.nrm = V3{adv.x, adv.y, adv.z};
     s.step += 1u;
+    if (adv.w == 0.001f && s.shift != kNoIndex) creep<C>(A, s, cnt, creep_limit);
 }
 
 // trace() (voxel_path.wgsl:239-243) for every queued ray. Persistent warps
@@ -573,11 +653,20 @@ __global__ void __launch_bounds__(kWaveBlock) wave_traverse_kernel(const WaveArg
             if (need && mine < total) start_ray<BUDGETED, C>(W, s, W.queue_in[mine], cnt);
         }
         const bool idle = s.slot == kNoIndex;
-        if (__all_sync(0xffffffffu, idle)) {
+        const unsigned busy = __ballot_sync(0xffffffffu, !idle);
+        if (!busy) {
             if (exhausted) break;
             continue;
         }
-        if (!idle) step_ray<BUDGETED, C>(W, s, cnt);
+        if constexpr (C) {
+            if (lane == 0) {
+                cnt.wp[exhausted ? 1 : 0] += 1u;
+                cnt.lp[exhausted ? 1 : 0] += (uint32_t)__popc(busy);
+            }
+        }
+        // While rays remain queued a grazing lane replays at most 64 steps per
+        // pass, so it holds up the warp's other lanes only briefly.
+        if (!idle) step_ray<BUDGETED, C>(W, s, cnt, exhausted ? 0xffffffffu : s.step + 64u);
     }
     flush_counters<C>(A, cnt);
 }
@@ -622,7 +711,7 @@ __global__ void __launch_bounds__(kWaveBlock) wave_shade_kernel(const WaveArgs W
             const uint4 h0 = W.hit[(size_t)p * 6u], h1 = W.hit[(size_t)p * 6u + 1u], h2 = W.hit[(size_t)p * 6u + 2u];
             uint32_t status = h0.x;
             if (LIMITED && status == 0u &&
-                geometry_ahead(A, origin + direction * T.reach(), direction, __fsub_rn(A.max_distance, T.reach()), cnt))
+                geometry_ahead(A, origin + direction * T.reach(), direction, direction_recip(direction), __fsub_rn(A.max_distance, T.reach()), cnt))
                 status = 3u;
             if (status == 0u) {
                 float horizon = wclamp(__fadd_rn(__fmul_rn(direction.y, 0.35f), 0.65f), 0.15f, 1.0f);

@@ -54,11 +54,15 @@ class Counters(ctypes.Structure):
         ("cache_hits", ctypes.c_uint64),
         ("status", ctypes.c_uint64 * 4),
         ("traverse_bytes", ctypes.c_uint64),
+        ("warp_passes", ctypes.c_uint64 * 2),
+        ("lane_passes", ctypes.c_uint64 * 2),
     ]
 
     def as_dict(self) -> dict:
-        d = {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "status"}
-        d["status"] = [int(v) for v in self.status]
+        d = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            d[k] = int(v) if isinstance(v, int) else [int(x) for x in v]
         return d
 
 

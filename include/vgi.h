@@ -80,6 +80,12 @@ typedef struct {
     uint64_t status[4];   /* rays by status: escaped, hit, unknown, reach */
     uint64_t traverse_bytes; /* the traversal's share of `bytes`: directory,
                                 header, brick and cell words */
+    /* Lane use of the wavefront traversal: passes of its loop made by warps
+     * with a ray in flight, and the rays in flight summed over those passes,
+     * while rays remained queued [0] and after the queue ran out [1]. Zero in
+     * the single-kernel layout. */
+    uint64_t warp_passes[2];
+    uint64_t lane_passes[2];
 } vgi_counters;
 
 /* ---- lifecycle: GpuTracer::new / drop (src/gpu.rs:448-595) ---------------- */
