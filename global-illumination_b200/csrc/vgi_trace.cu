@@ -423,8 +423,8 @@ __device__ float tree_probability(const TraceArgs& A, V3 position, V3 normal, I3
     }
     uint32_t index = 0;
     float probability = 1.0f;
-#pragma unroll 1
     const uint32_t first_node = f2u(A.emitter_count) * 2u;
+#pragma unroll 1
     for (uint32_t depth = 0; depth < 64u; ++depth) {
         cnt.bytes(64);  // load_node(index)
         const uint4 pivot = __ldg(A.emitters + first_node + index * 4u + 2u);
