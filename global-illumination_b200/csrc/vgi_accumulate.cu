@@ -8,6 +8,7 @@
 //   voxel_accumulate.wgsl:135-262  accumulate, record_stability, settled_flag
 //   voxel_accumulate.wgsl:264-286  sample_noise, required_samples, refinement_error
 //   voxel_accumulate.wgsl:295-344  apply_events, binds
+//   voxel_accumulate.wgsl:357-425  face_slot, measure_edits, finish_edits
 //   voxel_accumulate.wgsl:432-446  mark_changed
 //   voxel_retention.wgsl:1-96      curve_limit, box_distance2, resolve_retention
 //
@@ -304,7 +305,94 @@ __global__ void __launch_bounds__(kBlock) apply_events_kernel(AccumArgs a, const
     if (urgent) a.slot_meta[slot * 3u + 2u].w |= kUrgent;
 }
 
+// face_slot (voxel_accumulate.wgsl:357-370): the face index's slot for
+// (voxel, face), or kNoLimit.
+__device__ uint32_t face_slot(const uint4* index, int x, int y, int z, uint32_t face) {
+    const uint4 header = index[0];
+    uint32_t probe = (hash_voxel(x, y, z) ^ pcg(face + 1u)) & header.x;
+#pragma unroll 1
+    for (uint32_t attempt = 0; attempt < header.y; ++attempt) {
+        const uint4 e = index[probe + 1u];
+        if (e.w == 0xffffffffu) return kNoLimit;
+        if ((int)e.x == x && (int)e.y == y && (int)e.z == z && (e.w >> 29u) == face) return e.w & 0x1fffffffu;
+        probe = (probe + 1u) & header.x;
+    }
+    return kNoLimit;
+}
+
+// measure_edits (voxel_accumulate.wgsl:375-403), one thread per scan
+// position: the brightest outgoing luminance (albedo times incident mean and
+// direct luminance, plus emission) of the position's traced faces, folded
+// into its entry with an atomic max of the float bits (non-negative values
+// order like their bits) tagged by the high bit as "observed". Entries are
+// laid out by first position, so a binary search finds a position's entry.
+__global__ void __launch_bounds__(kBlock) measure_edits_kernel(const uint4* state, const uint4* slot_meta, const uint4* index,
+                                                               const float2* material_light, const uint4* measures,
+                                                               uint32_t n_entries, uint32_t n_positions, uint32_t* measure_max) {
+    const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
+    if (t >= n_positions) return;
+    uint32_t lo = 0, hi = n_entries;
+#pragma unroll 1
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) / 2u;
+        if (measures[mid * 3u].y <= t) lo = mid;
+        else hi = mid;
+    }
+    const uint4 a = measures[lo * 3u], b = measures[lo * 3u + 1u], size = measures[lo * 3u + 2u];
+    if (t < a.y || t >= a.y + a.z) return;
+    const uint32_t local = t - a.y;
+    const int x = (int)b.x + (int)(local % size.x), y = (int)b.y + (int)((local / size.x) % size.y),
+              z = (int)b.z + (int)(local / (size.x * size.y));
+    float brightest = 0.0f;
+    bool observed = false;
+#pragma unroll 1
+    for (uint32_t face = 0; face < 6u; ++face) {
+        const uint32_t slot = face_slot(index, x, y, z, face);
+        if (slot == kNoLimit) continue;
+        const uint4 identity = slot_meta[slot * 3u];
+        if ((identity.w & 8u) == 0u) continue;
+        if ((state[slot * 9u + 1u].y & 0x7fffffffu) == 0u) continue;
+        observed = true;
+        const uint4 m = state[slot * 9u], d = state[slot * 9u + 4u];
+        const float incident = __fadd_rn(lum3(u2f(m.x), u2f(m.y), u2f(m.z)), lum3(u2f(d.x), u2f(d.y), u2f(d.z)));
+        const float2 light = material_light[identity.w >> 16u];
+        brightest = wmax(brightest, __fadd_rn(__fmul_rn(light.x, incident), light.y));
+    }
+    if (observed) atomicMax(measure_max + lo, f2b(brightest) | 0x80000000u);
+}
+
+// finish_edits (voxel_accumulate.wgsl:407-423), one thread per entry: the
+// bound's flux becomes its own emission plus the brightest outgoing
+// luminance times two faces per changed voxel, and its kind a measured edit
+// (3); an edit with no traced face in its scan becomes unknown (0).
+__global__ void __launch_bounds__(kBlock) finish_edits_kernel(const uint4* measures, uint32_t n_entries, const uint32_t* measure_max,
+                                                              uint4* events) {
+    const uint32_t e = blockIdx.x * kBlock + threadIdx.x;
+    if (e >= n_entries) return;
+    const uint4 a = measures[e * 3u];
+    const float base_flux = u2f(measures[e * 3u + 1u].w);
+    const uint32_t observation = measure_max[e];
+    if ((observation & 0x80000000u) == 0u) {
+        events[a.x + 1u].w &= 0xfffffff8u;
+        return;
+    }
+    const float brightest = u2f(observation & 0x7fffffffu);
+    events[a.x].w = f2b(__fadd_rn(base_flux, __fmul_rn(__fmul_rn(brightest, 2.0f), (float)a.w)));
+    events[a.x + 1u].w = (events[a.x + 1u].w & 0xfffffff8u) | 3u;
+}
+
 }  // namespace
+
+void launch_measure_edits(const uint4* state, const uint4* slot_meta, const uint4* index, const float2* material_light,
+                          const uint4* measures, uint32_t n_entries, uint32_t n_positions, uint32_t* measure_max, uint4* events,
+                          cudaStream_t s) {
+    if (n_entries == 0) return;
+    cudaMemsetAsync(measure_max, 0, (size_t)n_entries * 4, s);
+    if (n_positions)
+        measure_edits_kernel<<<(n_positions + kBlock - 1) / kBlock, kBlock, 0, s>>>(state, slot_meta, index, material_light, measures,
+                                                                                   n_entries, n_positions, measure_max);
+    finish_edits_kernel<<<(n_entries + kBlock - 1) / kBlock, kBlock, 0, s>>>(measures, n_entries, measure_max, events);
+}
 
 void launch_prepare(const AccumArgs& a, cudaStream_t s) {
     if (a.n == 0) return;

@@ -83,6 +83,9 @@ struct vgi_ctx {
     // model
     std::vector<float> host_materials = std::vector<float>(256 * 16, 0.0f);
     DevBuf<float4> materials;
+    DevBuf<float2> material_light;  // (albedo, emission) luminance per material
+    DevBuf<uint4> measures;
+    DevBuf<uint32_t> measure_max;
     DevBuf<float4> lights;
     uint32_t n_lights = 0, n_directional = 0;
     float env[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -98,6 +101,7 @@ struct vgi_ctx {
     DevBuf<uint4> scratch_tasks, scratch_results;
     DevBuf<uint4> events;
     uint32_t n_events = 0;
+    uint64_t n_events_read = 0;  // uint4 words of the last measured event list, readable back
     DevBuf<unsigned long long> counters;
     uint32_t batch_id = 1;
 
@@ -406,6 +410,7 @@ int vgi_destroy(vgi_ctx* c) {
     c->materials.release(); c->lights.release(); c->emitters.release(); c->node_aux.release();
     c->tasks.release(); c->results.release(); c->state.release(); c->slot_meta.release(); c->checkpoint.release();
     c->face_index.release(); c->cache.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
+    c->material_light.release(); c->measures.release(); c->measure_max.release();
     c->counters.release();
     c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
     c->w_queue0.release(); c->w_queue1.release(); c->w_scatter.release(); c->w_counters.release();
@@ -611,6 +616,16 @@ int vgi_set_materials(vgi_ctx* c, const float* m) {
     c->host_materials.assign(m, m + 256 * 16);
     VGI_CUDA(c, c->materials.reserve(256 * 4));
     VGI_CUDA(c, cudaMemcpyAsync(c->materials.ptr, m, 256 * 64, cudaMemcpyHostToDevice, c->stream));
+    // The luminance of each material's albedo and emission, for measuring
+    // edits (ResidentCache::set_materials, src/gpu/resident.rs:816-838).
+    std::vector<float2> light(256);
+    for (int i = 0; i < 256; ++i) {
+        const float* d = m + i * 16;
+        const float* e = m + i * 16 + 8;
+        light[i] = make_float2(0.2126f * d[0] + 0.7152f * d[1] + 0.0722f * d[2], 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2]);
+    }
+    VGI_CUDA(c, c->material_light.reserve(256));
+    VGI_CUDA(c, cudaMemcpyAsync(c->material_light.ptr, light.data(), 256 * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }
@@ -848,6 +863,53 @@ int vgi_apply_events(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint6
     launch_apply_events(acc, c->events.ptr, c->n_slots, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     c->n_events = 0;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_apply_events_measured(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint64_t n_words, const uint32_t* measures,
+                              uint32_t n_entries) {
+    if (!c || (n_words && !words) || (n_words & 3) || (uint64_t)n_events * 12 > n_words || (n_entries && !measures))
+        return VGI_ERR_INVALID;
+    // Entries must tile their positions in order and name a bound record.
+    uint64_t positions = 0;
+    for (uint32_t e = 0; e < n_entries; ++e) {
+        const uint32_t* a = measures + (size_t)e * 12;
+        const uint32_t* size = a + 8;
+        const uint64_t count = (uint64_t)size[0] * size[1] * size[2];
+        if (a[1] != positions || a[2] != count || count == 0 || (uint64_t)a[0] + 2 > n_words / 4 ||
+            (uint64_t)a[0] < (uint64_t)n_events * 3)
+            return fail(c, VGI_ERR_INVALID, "measured edit entries must tile their scan positions and name a bound record");
+        positions += count;
+        if (positions > 0x7fffffffull) return fail(c, VGI_ERR_CAPACITY, "too many measured edit positions");
+    }
+    c->n_events_read = 0;
+    if (c->n_slots == 0) return VGI_OK;
+    if (n_entries && !c->material_light.ptr) return fail(c, VGI_ERR_STATE, "measured edits need the material table");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, c->events.reserve(std::max<uint64_t>(n_words / 4, 1)));
+    if (n_words) VGI_CUDA(c, cudaMemcpyAsync(c->events.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    if (n_entries) {
+        VGI_CUDA(c, c->measures.reserve((size_t)n_entries * 3));
+        VGI_CUDA(c, c->measure_max.reserve(n_entries));
+        VGI_CUDA(c, cudaMemcpyAsync(c->measures.ptr, measures, (size_t)n_entries * 48, cudaMemcpyHostToDevice, c->stream));
+        launch_measure_edits(c->state.ptr, c->slot_meta.ptr, c->face_index.ptr, c->material_light.ptr, c->measures.ptr, n_entries,
+                             (uint32_t)positions, c->measure_max.ptr, c->events.ptr, c->stream);
+        VGI_CUDA(c, cudaGetLastError());
+    }
+    c->n_events = n_events;
+    AccumArgs acc = accum_args(c, 0, 0);
+    launch_apply_events(acc, c->events.ptr, c->n_slots, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    c->n_events = 0;
+    c->n_events_read = n_words / 4;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_read_events(vgi_ctx* c, uint32_t* words, uint64_t n_words) {
+    if (!c || (n_words && !words) || n_words > c->n_events_read * 4) return VGI_ERR_INVALID;
+    if (n_words) VGI_CUDA(c, cudaMemcpyAsync(words, c->events.ptr, n_words * 4, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }

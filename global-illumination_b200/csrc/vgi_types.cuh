@@ -72,6 +72,9 @@ struct WaveBuffers {
 void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
 void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
 uint32_t wave_traverse_blocks_per_sm();
+void launch_measure_edits(const uint4* state, const uint4* slot_meta, const uint4* index, const float2* material_light,
+                          const uint4* measures, uint32_t n_entries, uint32_t n_positions, uint32_t* measure_max, uint4* events,
+                          cudaStream_t s);
 void launch_node_aux(const uint4* emitters, uint32_t first_node, uint32_t nodes, float4* aux, cudaStream_t stream);
 cudaError_t init_trace_constants();
 void launch_prepare(const AccumArgs& a, cudaStream_t stream);

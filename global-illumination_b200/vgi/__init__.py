@@ -145,6 +145,8 @@ _SIGNATURES = {
     "vgi_census": (_INT, [_P, _U32, _P]),
     "vgi_trace_tasks": (_INT, [_P, _P, _U32, _U32, _P, _P]),
     "vgi_apply_events": (_INT, [_P, _P, _U32, _U64]),
+    "vgi_apply_events_measured": (_INT, [_P, _P, _U32, _U64, _P, _U32]),
+    "vgi_read_events": (_INT, [_P, _P, _U64]),
     "vgi_read_results": (_INT, [_P, _U32, _U32, _P]),
     "vgi_read_state": (_INT, [_P, _U32, _U32, _P]),
     "vgi_write_state": (_INT, [_P, _U32, _U32, _P]),
@@ -421,6 +423,17 @@ class GpuTracer:
     def apply_events(self, words: np.ndarray, n_events: int) -> None:
         w = _c(words, np.uint32).reshape(-1)
         self._check(self._lib.vgi_apply_events(self._h, _ptr(w), n_events, w.size))
+
+    def apply_events_measured(self, words: np.ndarray, n_events: int, measures: np.ndarray) -> np.ndarray:
+        """Retention events whose measured edits take their flux from the
+        cache first; returns the event words as apply_events read them."""
+        w = _c(words, np.uint32).reshape(-1)
+        m = _c(measures, np.uint32).reshape(-1, 12)
+        self._check(self._lib.vgi_apply_events_measured(self._h, _ptr(w), n_events, w.size, _ptr(m), m.shape[0]))
+        out = np.zeros_like(w)
+        if self.n_slots:
+            self._check(self._lib.vgi_read_events(self._h, _ptr(out), out.size))
+        return out
 
     def read_results(self, first: int = 0, n: Optional[int] = None) -> np.ndarray:
         n = self.n_slots - first if n is None else n

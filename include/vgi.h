@@ -172,6 +172,20 @@ int vgi_trace_tasks(vgi_ctx* ctx, const uint32_t* tasks, uint32_t n, uint32_t sa
  * n_events headers of three uint4, then bound records of two uint4.
  * Applied by apply_events to every live slot (shaders/voxel_accumulate.wgsl:295-332). */
 int vgi_apply_events(vgi_ctx* ctx, const uint32_t* words, uint32_t n_events, uint64_t n_words);
+/* The same with measured edits (the resident batch's measure_edits and
+ * finish_edits passes before apply_events, src/gpu/resident.rs:1004-1050;
+ * shaders/voxel_accumulate.wgsl:375-425). `measures` holds 12 words per
+ * measured edit bound (encode_events' measure records): (bound record index,
+ * first scan position, positions, changed voxels), (scan min xyz, own flux
+ * bits), (scan size xyz, 0); entries tile the positions in order. Each such
+ * bound's flux becomes its own flux plus twice the changed voxels times the
+ * brightest outgoing luminance of the traced faces in its scan box, and its
+ * kind a measured edit (3), or unknown (0) when no traced face was seen.
+ * Needs the material table. The rewritten words stay readable through
+ * vgi_read_events until the next call. */
+int vgi_apply_events_measured(vgi_ctx* ctx, const uint32_t* words, uint32_t n_events, uint64_t n_words, const uint32_t* measures,
+                              uint32_t n_entries);
+int vgi_read_events(vgi_ctx* ctx, uint32_t* words, uint64_t n_words);
 
 /* ---- read-back: bounded snapshots (complete_readback, src/gpu.rs:1024-1170) --- */
 int vgi_read_results(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words24);

@@ -1108,6 +1108,63 @@ int orc_apply_events(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint,
     return 0;
 }
 
+// measure_edits + finish_edits (voxel_accumulate.wgsl:375-425) for the
+// measured edit bounds of an encoded event list (encode_events,
+// src/gpu/resident.rs:1326-1414). `measures` holds 3 uint4 per entry:
+// (bound record, first position, positions, changed voxels),
+// (scan min xyz, own flux bits), (scan size xyz, 0). `material_light` holds
+// (albedo luminance, emission luminance) per material. For every position of
+// an entry's scan box, the brightest outgoing luminance of its traced faces
+// (albedo * (mean + direct luminance) + emission) is taken; the bound then
+// gets flux = own + brightest * 2 * voxels and kind 3 (measured edit), or
+// kind 0 (unknown) when no traced face was seen. Rewrites `events` in place.
+int orc_measure_edits(const uint32_t* state, const uint32_t* slot_meta, const uint32_t* index, const float* material_light,
+                      const uint32_t* measures, uint32_t n_entries, uint32_t* events) {
+    const uint32_t mask = index[0], probes = index[1];
+    for (uint32_t e = 0; e < n_entries; ++e) {
+        const uint32_t* a = measures + (size_t)e * 12;
+        const uint32_t* b = a + 4;
+        const uint32_t* c = a + 8;
+        float brightest = 0.0f;
+        bool observed = false;
+        for (uint32_t local = 0; local < a[2]; ++local) {
+            const uint32_t off[3] = {local % c[0], (local / c[0]) % c[1], local / (c[0] * c[1])};
+            const int32_t p[3] = {(int32_t)b[0] + (int32_t)off[0], (int32_t)b[1] + (int32_t)off[1], (int32_t)b[2] + (int32_t)off[2]};
+            for (uint32_t face = 0; face < 6u; ++face) {
+                // face_slot (voxel_accumulate.wgsl:357-370)
+                uint32_t slot = NO_LIMIT;
+                uint32_t probe = (hash_voxel(p[0], p[1], p[2]) ^ pcg(face + 1u)) & mask;
+                for (uint32_t attempt = 0; attempt < probes; ++attempt) {
+                    const uint32_t* entry = index + ((size_t)probe + 1) * 4;
+                    if (entry[3] == 0xffffffffu) break;
+                    if ((int32_t)entry[0] == p[0] && (int32_t)entry[1] == p[1] && (int32_t)entry[2] == p[2] && (entry[3] >> 29u) == face) {
+                        slot = entry[3] & 0x1fffffffu;
+                        break;
+                    }
+                    probe = (probe + 1u) & mask;
+                }
+                if (slot == NO_LIMIT) continue;
+                const uint32_t* identity = slot_meta + (size_t)slot * 12;
+                if ((identity[3] & 8u) == 0u) continue;
+                const uint32_t* base = state + (size_t)slot * 36;
+                if ((base[5] & 0x7fffffffu) == 0u) continue;
+                observed = true;
+                const float incident = lum(stF4(base)) + lum(stF4(base + 16));
+                const float* light = material_light + (size_t)(identity[3] >> 16) * 2;
+                brightest = wmax(brightest, light[0] * incident + light[1]);
+            }
+        }
+        uint32_t* record = events + (size_t)a[0] * 4;
+        if (!observed) {
+            record[7] &= 0xfffffff8u;
+            continue;
+        }
+        record[3] = fbits(bitsf(b[3]) + brightest * 2.0f * (float)a[3]);
+        record[7] = (record[7] & 0xfffffff8u) | 3u;
+    }
+    return 0;
+}
+
 // The (voxel, face) -> slot index as the worker builds it (face_index.rs:36-97):
 // capacity 1024, doubled before an insert would exceed half load; faces
 // inserted in slot order. out: words of [mask, 64, 0, 0] then entries;

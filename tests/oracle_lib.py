@@ -60,6 +60,7 @@ _SIG = {
     "orc_mark_changed": (_INT, [_P, _P, _P, _U32, _P]),
     "orc_accumulate": (_INT, [_P, _P, _P, _P, _P, _U32, _P]),
     "orc_apply_events": (_INT, [_P, _P, _P, _P, _U32, _P]),
+    "orc_measure_edits": (_INT, [_P, _P, _P, _P, _P, _U32, _P]),
     "orc_face_index": (_I64, [_P, _U32, _P, _U64]),
     "orc_emitters": (_I64, [_P, _U32, _P, _P, _P, _U64, _P]),
 }
@@ -293,6 +294,14 @@ class Frames:
         self.results = out
         self.batch_id = (self.batch_id + 1) & 0x0FFFFFFF or 1
         return cnt
+
+    def measure_edits(self, words, measures, n_entries, material_light):
+        """measure_edits + finish_edits on a copy of the event words."""
+        w = c(words, np.uint32).copy()
+        m = c(measures, np.uint32)
+        ml = c(material_light, np.float32)
+        lib().orc_measure_edits(ptr(self.state), ptr(self.meta), ptr(self.index), ptr(ml), ptr(m), n_entries, ptr(w))
+        return w
 
     def apply_events(self, words, n_events):
         ctl = controls_words(self.n, 0, 0, self.transport, self.batch_id, n_events)

@@ -230,6 +230,51 @@ def test_events_and_discount_match_oracle(gpu):
     assert_words_equal(gpu.read_results(), ref.results, "results after discounted frames")
 
 
+def material_light(words):
+    """(albedo, emission) luminance per material, as the host builds it for
+    edit measurement (src/gpu/resident.rs:816-838)."""
+    m = np.asarray(words, np.float32).reshape(256, 16)
+    w = [np.float32(0.2126), np.float32(0.7152), np.float32(0.0722)]
+    out = np.zeros((256, 2), np.float32)
+    for col, first in ((0, 0), (1, 8)):
+        out[:, col] = (w[0] * m[:, first] + w[1] * m[:, first + 1]) + w[2] * m[:, first + 2]
+    return out
+
+
+def test_measured_edits_match_oracle(gpu):
+    # measure_edits + finish_edits (voxel_accumulate.wgsl:375-425) ahead of
+    # apply_events: two edits next to traced faces take their flux from the
+    # cache; one in open air above the terrain sees no face and turns unknown.
+    case = terrain_case(bounces=2, measured_retention=1.0)
+    ref = run_frames(gpu, case, 4, 8)
+    a = case.faces[len(case.faces) // 2, :3]
+    b = case.faces[len(case.faces) // 5, :3]
+    sky = np.array([a[0], 120, a[2]], np.int32)
+    bounds = [(a, a, 2.0, 1), (b - 1, b, 0.5, 8), (sky, sky + 1, 1.0, 8)]
+    events = [(np.minimum(a, b - 1) - 1, np.maximum(a, b) + 1, [(lo, hi, flux, 6 | 8) for lo, hi, flux, _ in bounds[:2]]),
+              (sky - 1, sky + 2, [(sky, sky + 1, 1.0, 6)])]
+    words, n = encode_events(events)
+    measures, first = [], 0
+    for k, (lo, hi, flux, voxels) in enumerate(bounds):
+        size = (hi - lo) + 3
+        count = int(np.prod(size))
+        measures += [[n * 3 + 2 * k, first, count, voxels], [*(lo - 1), int(np.float32(flux).view(np.uint32))], [*size, 0]]
+        first += count
+    measures = np.array(measures, np.int64).astype(np.uint32)
+    got = gpu.apply_events_measured(words, n, measures)
+    want = ref.measure_edits(words, measures, len(bounds), material_light(case.materials))
+    assert_words_equal(got.reshape(-1, 4), want.reshape(-1, 4), "event words after measurement")
+    kinds = want.reshape(-1, 4)[n * 3 + 1::2, 3] & 7
+    assert list(kinds) == [3, 3, 0], kinds
+    ref.apply_events(want, n)
+    assert_words_equal(gpu.read_state(), ref.state, "state after measured events")
+    assert_words_equal(gpu.read_slot_meta(), ref.meta, "slot metadata after measured events")
+    for f in range(2):
+        gpu.frame(8, clock_ms=100 + f)
+        ref.frame(8, clock_ms=100 + f)
+    assert_words_equal(gpu.read_results(), ref.results, "results after measured events")
+
+
 def test_edits_match_oracle(gpu):
     case = terrain_case()
     case.load(gpu, with_faces=False)

@@ -296,3 +296,43 @@ def test_hemisphere_directions_are_unit_and_upper():
             O.lib().orc_hemisphere(O.ptr(n), float(u), float(v), O.ptr(out))
             assert abs(np.linalg.norm(out) - 1.0) < 1e-5
             assert float(np.dot(out, n)) >= -1e-6
+
+
+def test_measured_edit_flux_is_own_plus_brightest_neighbour_light_twice_per_voxel():
+    # finish_edits (voxel_accumulate.wgsl:407-423): flux = own + brightest * 2 * voxels,
+    # brightest = albedo_lum * (mean_lum + direct_lum) + emission_lum over the scan's
+    # traced faces; a scan with no traced face marks the bound unknown (kind 0).
+    faces = np.array([[4, 5, 6, 2], [4, 5, 6, 3], [9, 9, 9, 0]], np.int32)
+    index = O.face_index(faces)
+    state = np.zeros((3, 36), np.uint32)
+    meta = np.zeros((3, 12), np.uint32)
+    meta[:, 0:3] = faces[:, 0:3].view(np.uint32)
+    meta[:, 3] = faces[:, 3].astype(np.uint32) | 8 | (np.array([7, 7, 9], np.uint32) << 16)
+    sf = state.view(np.float32)
+    sf[0, 0:3] = [1.0, 1.0, 1.0]   # mean
+    sf[0, 16:19] = [0.5, 0.5, 0.5]  # direct
+    state[0, 5] = 20                 # count
+    sf[1, 0:3] = [4.0, 4.0, 4.0]
+    state[1, 5] = 0                  # never traced: ignored
+    sf[2, 0:3] = [9.0, 9.0, 9.0]
+    state[2, 5] = 3                  # outside both scans
+    light = np.zeros((256, 2), np.float32)
+    light[7] = [0.5, 0.25]
+    light[9] = [1.0, 1.0]
+    # Two bounds: the first scans the 3^3 voxels around (4, 5, 6), which hold
+    # one traced and one untraced face; the second scans empty space.
+    words = np.zeros((3 + 4) * 4, np.uint32)
+    words[0:12] = [0, 0, 0, 0, 8, 8, 8, 0, 0, 0, 0, 2]
+    words[12:16] = [4, 5, 6, np.float32(2.0).view(np.uint32)]
+    words[16:20] = [4, 5, 6, 6 | 8]
+    words[20:24] = [50, 50, 50, np.float32(1.0).view(np.uint32)]
+    words[24:28] = [50, 50, 50, 6]
+    measures = np.array([[3, 0, 27, 2], [3, 4, 5, np.float32(2.0).view(np.uint32)], [3, 3, 3, 0],
+                         [5, 27, 27, 1], [49, 49, 49, np.float32(1.0).view(np.uint32)], [3, 3, 3, 0]], np.uint32)
+    out = words.copy()
+    O.lib().orc_measure_edits(O.ptr(state), O.ptr(meta), O.ptr(index), O.ptr(light), O.ptr(measures), 2, O.ptr(out))
+    lum = lambda v: (np.float32(0.2126) * np.float32(v) + np.float32(0.7152) * np.float32(v)) + np.float32(0.0722) * np.float32(v)
+    brightest = np.float32(0.5) * (lum(1.0) + lum(0.5)) + np.float32(0.25)
+    assert out[15] == (np.float32(2.0) + brightest * np.float32(2.0) * np.float32(2.0)).view(np.uint32)
+    assert out[19] == 3 | 8
+    assert out[23] == words[23] and out[27] == 0
