@@ -1108,6 +1108,41 @@ int orc_apply_events(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint,
     return 0;
 }
 
+// choose_emitter (voxel_path.wgsl:309-324) for n uniforms at one receiver:
+// out gets (voxel xyz, face, selection probability bits) per choice. The
+// emitter words are GpuEmitter records then light-tree nodes, as uploaded.
+int orc_choose_emitters(const uint32_t* emitters, uint32_t n_emitters, float total, const float* position, const float* normal,
+                        const float* choices, uint32_t n, uint32_t* out) {
+    float params[24] = {0};
+    params[18] = total;
+    params[19] = (float)n_emitters;
+    Geometry g{};
+    Model m{params, nullptr, nullptr, emitters, nullptr, nullptr, orc_pipeline{1, 0, 64, 0, 1}};
+    Ctx x{g, m, Counters{}};
+    const f3 p{position[0], position[1], position[2]}, nn{normal[0], normal[1], normal[2]};
+    for (uint32_t i = 0; i < n; ++i) {
+        Emissive e = choose_emitter(x, p, nn, choices[i]);
+        uint32_t* o = out + (size_t)i * 5;
+        o[0] = (uint32_t)e.voxel.x; o[1] = (uint32_t)e.voxel.y; o[2] = (uint32_t)e.voxel.z; o[3] = e.face;
+        o[4] = fbits(e.sampling.y);
+    }
+    return 0;
+}
+
+// The light tree's probability of selecting the emitter face (voxel, face)
+// from a receiver (tree_probability, voxel_path.wgsl:159-174).
+float orc_emitter_probability(const uint32_t* emitters, uint32_t n_emitters, float total, const float* position, const float* normal,
+                              const int32_t* voxel, uint32_t face) {
+    float params[24] = {0};
+    params[18] = total;
+    params[19] = (float)n_emitters;
+    Geometry g{};
+    Model m{params, nullptr, nullptr, emitters, nullptr, nullptr, orc_pipeline{1, 0, 64, 0, 1}};
+    Ctx x{g, m, Counters{}};
+    return tree_probability(x, f3{position[0], position[1], position[2]}, f3{normal[0], normal[1], normal[2]},
+                            i3{voxel[0], voxel[1], voxel[2]}, face_normal(face));
+}
+
 // measure_edits + finish_edits (voxel_accumulate.wgsl:375-425) for the
 // measured edit bounds of an encoded event list (encode_events,
 // src/gpu/resident.rs:1326-1414). `measures` holds 3 uint4 per entry:

@@ -34,8 +34,9 @@ class Case:
         g.set_environment(self.env)
         g.build_emitters()
         g.set_transport(self.transport)
-        if with_faces:
-            g.set_faces(self.faces)
+        # Without faces the context's cache is emptied, so a trace never
+        # gathers from an earlier test's faces (the context is shared).
+        g.set_faces(self.faces if with_faces else np.zeros((0, 5), np.int32))
 
     def pipe(self, lanes):
         t = self.transport

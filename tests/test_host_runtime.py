@@ -2,6 +2,7 @@
 every symbol the public headers declare, and its host runtime (top-level
 growth, face index, emitter distribution and light tree) matches the oracle
 word for word."""
+import ctypes
 import os
 import re
 
@@ -128,3 +129,62 @@ def test_stone_room_faces():
     faces = vgi.exposed_faces(coords, vox)
     # 6 * 30^2 interior shell faces, the emitter's 5 exposed faces, minus the floor face it covers.
     assert faces.shape[0] == 6 * 30 * 30 + 5 - 1
+
+
+def test_light_selection_frequencies_match_reported_probabilities():
+    # Restates emission/tree.rs:199-262 on the oracle's light-tree walk (the
+    # shader's choose_emitter and tree_probability): at a few receivers, the
+    # frequencies of 262,144 independent uniforms' choices, pooled into 64
+    # bins by emitter index, pass the reference's Pearson gate against the
+    # reported probabilities, which sum to one.
+    O.lib().orc_choose_emitters.restype = ctypes.c_int
+    O.lib().orc_choose_emitters.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
+    O.lib().orc_emitter_probability.restype = ctypes.c_float
+    O.lib().orc_emitter_probability.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_uint32]
+    coords, vox = vgi.terrain(6, 4, 6, seed=5, base_height=30.0, falloff=18.0, emitters=200)
+    words, n_emit, total = O.emitters(coords, vox, materials_with_emitters().words())
+    assert n_emit >= 32  # the tree, not the CDF
+    records = words[: n_emit * 8].reshape(n_emit, 8)
+    lookup = {(int(r[0]), int(r[1]), int(r[2]), int(r[3])): i for i, r in enumerate(records.view(np.int32))}
+    faces = vgi.exposed_faces(coords, vox)
+    normals = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], np.float32)
+    N = 262144
+    state = np.uint64(0x243F6A8885A308D3)
+    with np.errstate(over="ignore"):
+        steps = np.arange(1, N + 1, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15) + state
+        w = steps
+        w = (w ^ (w >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        w = (w ^ (w >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        w ^= w >> np.uint64(31)
+    uniforms = ((w >> np.uint64(40)).astype(np.float32) / np.float32(16777216.0)).astype(np.float32)
+    for probe in faces[::max(1, len(faces) // 3)][:3]:
+        n = normals[probe[3]]
+        position = (probe[:3].view(np.int32).astype(np.float32) + np.float32(0.5) + n * np.float32(0.5)).astype(np.float32)
+        expected = np.zeros(64)
+        for i, r in enumerate(records.view(np.int32)):
+            expected[i % 64] += O.lib().orc_emitter_probability(O.ptr(words), n_emit, total, O.ptr(position), O.ptr(n), O.ptr(r[:3].copy()),
+                                                                int(r[3]))
+        assert abs(expected.sum() - 1.0) < 2e-5
+        out = np.zeros((N, 5), np.uint32)
+        O.lib().orc_choose_emitters(O.ptr(words), n_emit, total, O.ptr(position), O.ptr(n), O.ptr(uniforms), N, O.ptr(out))
+        observed = np.zeros(64)
+        for row in out.view(np.int32)[:, :4]:
+            observed[lookup[tuple(int(v) for v in row)] % 64] += 1
+        bins, rare_o, rare_e = [], 0.0, 0.0
+        for o, p in zip(observed, expected):
+            e = p * N
+            if e >= 8.0:
+                bins.append([o, e])
+            else:
+                rare_o += o
+                rare_e += e
+        if rare_e >= 8.0:
+            bins.append([rare_o, rare_e])
+        else:
+            bins[0][0] += rare_o
+            bins[0][1] += rare_e
+        df = len(bins) - 1
+        chi2 = sum((o - e) ** 2 / e for o, e in bins)
+        assert chi2 < df + 10.0 * (2.0 * df) ** 0.5 + 50.0, (chi2, df, position)
