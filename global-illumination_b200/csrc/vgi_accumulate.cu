@@ -20,6 +20,7 @@
 // changes a slot's mean or count rewrites it.
 #include "vgi_device.cuh"
 #include "vgi_types.cuh"
+#include "vgi_retention.cuh"
 
 namespace vgi {
 namespace {
@@ -208,18 +209,8 @@ __global__ void __launch_bounds__(kBlock) accumulate_kernel(AccumArgs a) {
     out[5] = o5;
 }
 
-// curve_limit / box_distance2 / load_height (voxel_retention.wgsl:9-22)
-__device__ __forceinline__ uint32_t curve_limit(uint32_t d2) {
-    if (d2 >= 36864u) return kNoLimit;
-    return (d2 * d2 + 10368u) / 20736u;
-}
-__device__ __forceinline__ uint32_t box_distance2(int lx, int ly, int lz, int hx, int hy, int hz, int px, int py, int pz) {
-    int sx = min(max(max(lx - px, px - hx), 0), 4096);
-    int sy = min(max(max(ly - py, py - hy), 0), 4096);
-    int sz = min(max(max(lz - pz, pz - hz), 0), 4096);
-    return (uint32_t)sx * (uint32_t)sx + (uint32_t)sy * (uint32_t)sy + (uint32_t)sz * (uint32_t)sz;
-}
-
+// apply_events (voxel_accumulate.wgsl:295-332) with resolve_retention
+// (vgi_retention.cuh), one thread per slot.
 __global__ void __launch_bounds__(kBlock) apply_events_kernel(AccumArgs a, const uint4* events, uint32_t n_slots) {
     const uint32_t* ctl = a.controls;
     uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
@@ -230,60 +221,11 @@ __global__ void __launch_bounds__(kBlock) apply_events_kernel(AccumArgs a, const
     const uint32_t event_count = ctl[13], reach = ctl[15];
     const float physical = u2f(ctl[11]);
     const bool measured_mode = physical > 0.0f;
-    // resolve_retention (voxel_retention.wgsl:29-96)
-    uint32_t cap = kNoLimit, source_cap = kNoLimit;
-    float change = 0.0f;
-    bool known = true, woken = false, urgent_if_binding = false, urgent = false;
-    for (uint32_t e = 0; e < event_count; ++e) {
-        uint4 h0 = events[e * 3u], h1 = events[e * 3u + 1u], h2 = events[e * 3u + 2u];
-        if ((h0.w & 2u) != 0u) {
-            uint32_t limit = h2.x;
-            for (uint32_t b = 0; b < h2.w; ++b) {
-                uint4 sp = events[event_count * 3u + (h2.z + b) * 2u];
-                float dx = __fsub_rn((float)px, u2f(sp.x)), dy = __fsub_rn((float)py, u2f(sp.y)), dz = __fsub_rn((float)pz, u2f(sp.z));
-                float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                if (d2 <= u2f(sp.w)) limit = limit < 4u ? limit : 4u;
-            }
-            source_cap = source_cap < limit ? source_cap : limit;
-            woken = true;
-            continue;
-        }
-        uint32_t outside = box_distance2((int)h0.x, (int)h0.y, (int)h0.z, (int)h1.x, (int)h1.y, (int)h1.z, px, py, pz);
-        if (outside > reach) continue;
-        woken = true;
-        bool exact = known;
-        uint32_t nearest = kNoLimit;
-        for (uint32_t b = 0; b < h2.w; ++b) {
-            uint32_t record = event_count * 3u + (h2.z + b) * 2u;
-            uint4 b0 = events[record], b1 = events[record + 1u];
-            uint32_t d = box_distance2((int)b0.x, (int)b0.y, (int)b0.z, (int)b1.x, (int)b1.y, (int)b1.z, px, py, pz);
-            if (d > reach) continue;
-            nearest = nearest < d ? nearest : d;
-            uint32_t edit_kind = b1.w & 7u;
-            if ((b1.w & 8u) != 0u && (edit_kind == 0u || edit_kind == 3u)) {
-                if (edit_kind == 3u && measured_mode) urgent_if_binding = urgent_if_binding || d <= ctl[30];
-                else urgent = urgent || d <= ctl[31];
-            }
-            if (exact) {
-                uint32_t kind = b1.w & 7u;
-                if (kind == 0u) {
-                    known = false;
-                    exact = false;
-                } else if (kind != 1u) {
-                    float area = 1.0f;
-                    if (kind == 2u) area = (float)min(max(((int)b1.w >> 3) + 1 - py, 0), 16);
-                    change = __fadd_rn(change, __fdiv_rn(__fmul_rn(u2f(b0.w), area), __fmul_rn(3.14159265358979f, (float)(d > 1u ? d : 1u))));
-                }
-            }
-        }
-        if (nearest != kNoLimit) {
-            uint32_t c = curve_limit(nearest);
-            cap = cap < c ? cap : c;
-        }
-    }
-    bool measured = measured_mode && known;
-    uint32_t other = measured ? kNoLimit : cap;
-    uint32_t limit = source_cap < other ? source_cap : other;
+    const RetentionResult r = resolve_retention(events, event_count, reach, px, py, pz, measured_mode, ctl[30], ctl[31]);
+    const bool measured = r.measured, woken = r.woken, urgent_if_binding = r.urgent_if_binding;
+    const uint32_t limit = r.limit;
+    const float change = r.change;
+    bool urgent = r.urgent;
     if (limit != kNoLimit) {
         uint4* s1p = a.state + slot * 9u + 1u;
         uint32_t y = s1p->y;
@@ -381,7 +323,18 @@ __global__ void __launch_bounds__(kBlock) finish_edits_kernel(const uint4* measu
     events[a.x + 1u].w = (events[a.x + 1u].w & 0xfffffff8u) | 3u;
 }
 
+// A new slot's incarnation (state word 28): the resident allocator numbers
+// slots from 1 as it creates them (src/gpu/resident.rs:457-468).
+__global__ void __launch_bounds__(kBlock) seed_incarnations_kernel(uint4* state, uint32_t n) {
+    const uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
+    if (slot < n) state[slot * 9u + 7u].x = slot + 1u;
+}
+
 }  // namespace
+
+void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s) {
+    if (n) seed_incarnations_kernel<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(state, n);
+}
 
 void launch_measure_edits(const uint4* state, const uint4* slot_meta, const uint4* index, const float2* material_light,
                           const uint4* measures, uint32_t n_entries, uint32_t n_positions, uint32_t* measure_max, uint4* events,

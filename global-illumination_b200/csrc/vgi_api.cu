@@ -99,6 +99,10 @@ struct vgi_ctx {
     DevBuf<uint4> tasks, results, state, slot_meta, checkpoint, face_index;
     DevBuf<float4> cache;
     DevBuf<uint4> scratch_tasks, scratch_results;
+    // view tier: receivers, paths, continuations, estimates, owner queue, events
+    DevBuf<uint4> v_receivers, v_paths, v_conts, v_estimates, v_events, v_scratch;
+    DevBuf<uint32_t> v_queue;
+    uint32_t n_view = 0;
     DevBuf<uint4> events;
     uint32_t n_events = 0;
     uint64_t n_events_read = 0;  // uint4 words of the last measured event list, readable back
@@ -411,6 +415,8 @@ int vgi_destroy(vgi_ctx* c) {
     c->tasks.release(); c->results.release(); c->state.release(); c->slot_meta.release(); c->checkpoint.release();
     c->face_index.release(); c->cache.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
     c->material_light.release(); c->measures.release(); c->measure_max.release();
+    c->v_receivers.release(); c->v_paths.release(); c->v_conts.release(); c->v_estimates.release(); c->v_events.release();
+    c->v_scratch.release(); c->v_queue.release();
     c->counters.release();
     c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
     c->w_queue0.release(); c->w_queue1.release(); c->w_scatter.release(); c->w_counters.release();
@@ -739,6 +745,7 @@ int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, cudaMemcpyAsync(c->tasks.ptr, tasks.data(), (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->results.ptr, 0, m * 96, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->state.ptr, 0, m * 144, c->stream));
+    launch_seed_incarnations(c->state.ptr, n, c->stream);
     VGI_CUDA(c, cudaMemcpyAsync(c->slot_meta.ptr, meta.data(), (size_t)n * 48, cudaMemcpyHostToDevice, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->checkpoint.ptr, 0, m * 48, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->cache.ptr, 0, m * 16, c->stream));
@@ -903,6 +910,121 @@ int vgi_apply_events_measured(vgi_ctx* c, const uint32_t* words, uint32_t n_even
     VGI_CUDA(c, cudaGetLastError());
     c->n_events = 0;
     c->n_events_read = n_words / 4;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+// ---- view tier (vgi_view.cuh) --------------------------------------------
+namespace {
+ViewArgs view_args(vgi_ctx* c) {
+    ViewArgs v{};
+    v.t = trace_args(c, nullptr, nullptr, 0, 1, c->n_slots > 0);
+    v.receivers = c->v_receivers.ptr;
+    v.paths = c->v_paths.ptr;
+    v.conts = c->v_conts.ptr;
+    v.estimates = c->v_estimates.ptr;
+    v.queue = c->v_queue.ptr;
+    v.shared_state = c->state.ptr;
+    v.shared_meta = c->slot_meta.ptr;
+    v.shared_cache = c->cache.ptr;
+    v.n = c->n_view;
+    v.reach = 192u * 192u;  // INFLUENCE_RADIUS^2 (src/retention.rs:33-40)
+    v.physical = std::max(c->transport.measured_retention, 0.0f);
+    v.hits = c->transport.bounces;
+    return v;
+}
+bool view_ready(vgi_ctx* c) { return c->directory.ptr && c->materials.ptr && c->lights.ptr && c->emitters.ptr; }
+}  // namespace
+
+int vgi_view_set_receivers(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
+    if (!c || (n && !faces)) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    std::vector<uint4> receivers((size_t)n * 2), estimates((size_t)n * 4, make_uint4(0, 0, 0, 0));
+    for (uint32_t i = 0; i < n; ++i) {
+        const vgi_face& f = faces[i];
+        if (f.face > 5 || f.material > 255) return fail(c, VGI_ERR_INVALID, "receiver face or material out of range");
+        // The receiver's surface point: the face centre, voxel + 0.5 + normal * 0.5.
+        float s[3];
+        for (int a = 0; a < 3; ++a) {
+            const float n_a = (int)(f.face >> 1) == a ? ((f.face & 1u) ? -1.0f : 1.0f) : 0.0f;
+            s[a] = ((float)f.voxel[a] + 0.5f) + n_a * 0.5f;
+        }
+        uint32_t bits[3];
+        std::memcpy(bits, s, 12);
+        receivers[(size_t)i * 2] = make_uint4(bits[0], bits[1], bits[2], f.face);
+        receivers[(size_t)i * 2 + 1] = make_uint4((uint32_t)f.voxel[0], (uint32_t)f.voxel[1], (uint32_t)f.voxel[2], 0u);
+        estimates[(size_t)i * 4 + 3] = make_uint4(0u, f.material, 0u, 0u);
+    }
+    const size_t m = std::max<uint32_t>(n, 1);
+    VGI_CUDA(c, c->v_receivers.reserve(m * 2));
+    VGI_CUDA(c, c->v_paths.reserve(m * 8));
+    VGI_CUDA(c, c->v_conts.reserve(m * 8));
+    VGI_CUDA(c, c->v_estimates.reserve(m * 4));
+    VGI_CUDA(c, c->v_queue.reserve(12 + 2 * m));
+    if (n) {
+        VGI_CUDA(c, cudaMemcpyAsync(c->v_receivers.ptr, receivers.data(), (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, cudaMemcpyAsync(c->v_estimates.ptr, estimates.data(), (size_t)n * 64, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, cudaMemsetAsync(c->v_paths.ptr, 0, (size_t)n * 128, c->stream));
+        VGI_CUDA(c, cudaMemsetAsync(c->v_conts.ptr, 0, (size_t)n * 128, c->stream));
+    }
+    VGI_CUDA(c, cudaMemsetAsync(c->v_queue.ptr, 0, (12 + 2 * m) * 4, c->stream));
+    c->n_view = n;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events, uint32_t n_events, uint64_t n_words) {
+    if (!c || !wave || (n_words && !events) || (n_words & 3) || (uint64_t)n_events * 12 > n_words) return VGI_ERR_INVALID;
+    if (!view_ready(c)) return fail(c, VGI_ERR_STATE, "the view tier needs geometry, materials, lights and emitters");
+    if (c->n_view == 0) return VGI_OK;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    ViewArgs v = view_args(c);
+    v.range[0] = wave->first;
+    v.range[1] = wave->invocations == 0 ? c->n_view : wave->invocations;
+    v.range[2] = wave->max_hits;
+    v.range[3] = wave->depth;
+    for (int k = 0; k < 4; ++k) v.ticket[k] = wave->ticket[k];
+    v.view_first = wave->view_first != 0;
+    v.shared = wave->shared != 0 && c->n_slots > 0;
+    v.clock = wave->clock_ms;
+    if (n_events) {
+        VGI_CUDA(c, c->v_events.reserve(n_words / 4));
+        VGI_CUDA(c, cudaMemcpyAsync(c->v_events.ptr, events, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    }
+    v.events = c->v_events.ptr;
+    v.n_events = n_events;
+    launch_view_frame(v, transport_limited(c), c->transport.budgeted != 0, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_view_read(vgi_ctx* c, uint32_t* receivers8, uint32_t* paths32, uint32_t* conts32, uint32_t* estimates16, uint32_t* queue) {
+    if (!c) return VGI_ERR_INVALID;
+    const size_t n = c->n_view;
+    if (n) {
+        if (receivers8) VGI_CUDA(c, cudaMemcpyAsync(receivers8, c->v_receivers.ptr, n * 32, cudaMemcpyDeviceToHost, c->stream));
+        if (paths32) VGI_CUDA(c, cudaMemcpyAsync(paths32, c->v_paths.ptr, n * 128, cudaMemcpyDeviceToHost, c->stream));
+        if (conts32) VGI_CUDA(c, cudaMemcpyAsync(conts32, c->v_conts.ptr, n * 128, cudaMemcpyDeviceToHost, c->stream));
+        if (estimates16) VGI_CUDA(c, cudaMemcpyAsync(estimates16, c->v_estimates.ptr, n * 64, cudaMemcpyDeviceToHost, c->stream));
+        if (queue) VGI_CUDA(c, cudaMemcpyAsync(queue, c->v_queue.ptr, (12 + 2 * n) * 4, cudaMemcpyDeviceToHost, c->stream));
+    }
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_view_trace_paths(vgi_ctx* c, uint32_t samples, uint32_t* paths32) {
+    if (!c || (c->n_view && samples && !paths32)) return VGI_ERR_INVALID;
+    if (!view_ready(c)) return fail(c, VGI_ERR_STATE, "the view tier needs geometry, materials, lights and emitters");
+    const uint64_t total = (uint64_t)c->n_view * samples;
+    if (total == 0) return VGI_OK;
+    if (total > (1ull << 26)) return fail(c, VGI_ERR_CAPACITY, "at most 2^26 view path records per call");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, c->v_scratch.reserve(total * 8));
+    ViewArgs v = view_args(c);
+    launch_view_trace_paths(v, samples, c->v_scratch.ptr, transport_limited(c), c->transport.budgeted != 0, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    VGI_CUDA(c, cudaMemcpyAsync(paths32, c->v_scratch.ptr, total * 128, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }

@@ -920,3 +920,5 @@ cudaError_t init_trace_constants() {
 
 // The wavefront layout shares this translation unit's helpers and constants.
 #include "vgi_wave.cuh"
+#include "vgi_retention.cuh"
+#include "vgi_view.cuh"

@@ -69,9 +69,33 @@ struct WaveBuffers {
     cudaEvent_t* traverse_marks;  // optional: start/end events of up to 4 traversal launches
 };
 
+// The view tier's buffers and controls (vgi_view.cuh) for n receivers.
+struct ViewArgs {
+    TraceArgs t;
+    uint4* receivers;      // 2 per receiver: surface xyz, face | voxel xyz, sequence
+    uint4* paths;          // 8 per receiver (ViewPath)
+    uint4* conts;          // 8 per receiver (ViewContinuation)
+    uint4* estimates;      // 4 per receiver (ViewEstimate)
+    uint32_t* queue;       // 12 counters, owners (n), cursor words (n)
+    uint4* shared_state;   // the world cache's slots (9 uint4 each)
+    uint4* shared_meta;    // 3 uint4 per slot
+    float4* shared_cache;  // the slots' gather records
+    const uint4* events;
+    uint32_t n_events, reach;
+    uint32_t n;
+    uint32_t range[4];     // ViewWave.range: first owner, invocations, hits per visit, finite depth
+    uint32_t ticket[4];
+    uint32_t view_first, shared, clock;
+    float physical;        // measured retention c
+    uint32_t hits;         // DIFFUSE_HITS for trace_view_paths
+};
+
 void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
+void launch_view_frame(const ViewArgs& v, bool limited, bool budgeted, cudaStream_t stream);
+void launch_view_trace_paths(const ViewArgs& v, uint32_t samples, uint4* out, bool limited, bool budgeted, cudaStream_t stream);
 void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
 uint32_t wave_traverse_blocks_per_sm();
+void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s);
 void launch_measure_edits(const uint4* state, const uint4* slot_meta, const uint4* index, const float2* material_light,
                           const uint4* measures, uint32_t n_entries, uint32_t n_positions, uint32_t* measure_max, uint4* events,
                           cudaStream_t s);

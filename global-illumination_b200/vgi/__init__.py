@@ -66,6 +66,20 @@ class Counters(ctypes.Structure):
         return d
 
 
+class ViewWave(ctypes.Structure):
+    """vgi_view_wave: one view frame's ViewWave range, ticket and view controls."""
+    _fields_ = [
+        ("first", ctypes.c_uint32),
+        ("invocations", ctypes.c_uint32),
+        ("max_hits", ctypes.c_uint32),
+        ("depth", ctypes.c_uint32),
+        ("ticket", ctypes.c_uint32 * 4),
+        ("view_first", ctypes.c_uint32),
+        ("shared", ctypes.c_uint32),
+        ("clock_ms", ctypes.c_uint32),
+    ]
+
+
 class _Transport(ctypes.Structure):
     _fields_ = [
         ("reach", ctypes.c_float),
@@ -147,6 +161,10 @@ _SIGNATURES = {
     "vgi_apply_events": (_INT, [_P, _P, _U32, _U64]),
     "vgi_apply_events_measured": (_INT, [_P, _P, _U32, _U64, _P, _U32]),
     "vgi_read_events": (_INT, [_P, _P, _U64]),
+    "vgi_view_set_receivers": (_INT, [_P, _P, _U32]),
+    "vgi_view_frame": (_INT, [_P, _P, _P, _U32, _U64]),
+    "vgi_view_read": (_INT, [_P, _P, _P, _P, _P, _P]),
+    "vgi_view_trace_paths": (_INT, [_P, _U32, _P]),
     "vgi_read_results": (_INT, [_P, _U32, _U32, _P]),
     "vgi_read_state": (_INT, [_P, _U32, _U32, _P]),
     "vgi_write_state": (_INT, [_P, _U32, _U32, _P]),
@@ -433,6 +451,34 @@ class GpuTracer:
         out = np.zeros_like(w)
         if self.n_slots:
             self._check(self._lib.vgi_read_events(self._h, _ptr(out), out.size))
+        return out
+
+    # ---- view tier -----------------------------------------------------------
+    def view_set_receivers(self, faces: np.ndarray) -> None:
+        """Visible unit faces (voxel xyz, face, material rows) as view receivers."""
+        f = _c(faces, np.int32).reshape(-1, 5)
+        self._check(self._lib.vgi_view_set_receivers(self._h, _ptr(f), f.shape[0]))
+        self.n_view = f.shape[0]
+
+    def view_frame(self, first: int = 0, invocations: int = 0, max_hits: int = 8, depth: int = 0, ticket=(0, 0, 0, 0),
+                   view_first: bool = False, shared: bool = True, clock_ms: int = 0, events=None, n_events: int = 0) -> None:
+        w = ViewWave(first, invocations, max_hits, depth, (ctypes.c_uint32 * 4)(*ticket), int(view_first), int(shared), clock_ms)
+        ev = np.zeros(0, np.uint32) if events is None else _c(events, np.uint32).reshape(-1)
+        self._check(self._lib.vgi_view_frame(self._h, ctypes.byref(w), _ptr(ev), n_events, ev.size))
+
+    def view_read(self) -> dict:
+        n = getattr(self, "n_view", 0)
+        out = {"receivers": np.zeros((n, 8), np.uint32), "paths": np.zeros((n, 32), np.uint32),
+               "continuations": np.zeros((n, 32), np.uint32), "estimates": np.zeros((n, 16), np.uint32),
+               "queue": np.zeros(12 + 2 * n, np.uint32)}
+        self._check(self._lib.vgi_view_read(self._h, _ptr(out["receivers"]), _ptr(out["paths"]), _ptr(out["continuations"]),
+                                            _ptr(out["estimates"]), _ptr(out["queue"])))
+        return out
+
+    def view_trace_paths(self, samples: int) -> np.ndarray:
+        n = getattr(self, "n_view", 0)
+        out = np.zeros((n * samples, 32), np.uint32)
+        self._check(self._lib.vgi_view_trace_paths(self._h, samples, _ptr(out)))
         return out
 
     def read_results(self, first: int = 0, n: Optional[int] = None) -> np.ndarray:

@@ -187,6 +187,39 @@ int vgi_apply_events_measured(vgi_ctx* ctx, const uint32_t* words, uint32_t n_ev
                               uint32_t n_entries);
 int vgi_read_events(vgi_ctx* ctx, uint32_t* words, uint64_t n_words);
 
+/* ---- view tier: the visible-face path history of the view renderer -----------
+ * (shaders/voxel_view_trace.wgsl, voxel_view_runtime.wgsl:272-349,
+ * voxel_view_cache.wgsl; src/gpu/view/runtime.rs Stage::ORDER). The caller
+ * gives the receivers: one per visible unit face (voxel, face, material),
+ * each its own owner; raster discovery, reprojection between views, the
+ * topology prior of new faces and sun-corner records are outside this path.
+ * Records keep the shaders' layouts: ViewReceiver 8 words, ViewPath 32,
+ * ViewContinuation 32, ViewEstimate 16; the queue holds 12 counters, the
+ * owner list and one cursor word per receiver. */
+typedef struct vgi_view_wave {
+    uint32_t first;        /* ViewWave.range.x: first owner of the rotation */
+    uint32_t invocations;  /* range.y: owner invocations this frame (0: one per receiver) */
+    uint32_t max_hits;     /* range.z: hits a path advances per visit, 1..8 (0: no tracing) */
+    uint32_t depth;        /* range.w: finite path depth, 0 for unbiased roulette */
+    uint32_t ticket[4];    /* owner generations: a change restarts paused paths */
+    uint32_t view_first;   /* view.history.w: up to 32 visits per owner instead of 1 */
+    uint32_t shared;       /* view.cache.z: hand faces to and from the world cache */
+    uint32_t clock_ms;     /* view.cache.y: worker clock for the cache's rank records */
+} vgi_view_wave;
+/* Replaces the receiver list; estimates, paths and continuations start empty. */
+int vgi_view_set_receivers(vgi_ctx* ctx, const vgi_face* faces, uint32_t n);
+/* One view frame: reproject (sequence from the estimate, owner queue),
+ * retain_view_history for `n_events` encoded events (vgi_apply_events'
+ * layout), load_shared_faces, trace_visible_paths, store_shared_faces.
+ * Synchronous. */
+int vgi_view_frame(vgi_ctx* ctx, const vgi_view_wave* wave, const uint32_t* events, uint32_t n_events, uint64_t n_words);
+/* Snapshots of the view records; each pointer may be null. */
+int vgi_view_read(vgi_ctx* ctx, uint32_t* receivers8, uint32_t* paths32, uint32_t* continuations32, uint32_t* estimates16,
+                  uint32_t* queue);
+/* trace_view_paths: `samples` complete receiver samples per receiver
+ * (sequence + i), one ViewPath record each, in receiver-major order. */
+int vgi_view_trace_paths(vgi_ctx* ctx, uint32_t samples, uint32_t* paths32);
+
 /* ---- read-back: bounded snapshots (complete_readback, src/gpu.rs:1024-1170) --- */
 int vgi_read_results(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words24);
 int vgi_read_state(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words36);

@@ -586,7 +586,7 @@ static Cached cached_energy(Ctx& x, i3 voxel, uint32_t face) {
     return c;
 }
 
-struct PathEnergy { Energy energy; bool unknown = false; };
+struct PathEnergy { Energy energy; bool unknown = false; RayResult first_hit; };
 struct PathState {
     PathEnergy result;
     F4 throughput{1.0f, 1.0f, 1.0f, 1.0f};
@@ -615,6 +615,7 @@ static PathState advance_path(Ctx& x, PathState state, uint32_t stream, uint32_t
         uint32_t bounce = state.bounce;
         state.done = true;
         RayResult hit = trace_diffuse(x, state.origin, state.direction);
+        if (bounce == 0u) state.result.first_hit = hit;
         if (hit.status == 0u) {
             float horizon = wclamp(state.direction.y * 0.35f + 0.65f, 0.15f, 1.0f);
             F4 env{x.env(0), x.env(1), x.env(2), x.env(3)};
@@ -1254,6 +1255,374 @@ int64_t orc_face_index(const int32_t* faces /*4 per face: xyz, face*/, uint32_t 
     out[0] = (uint32_t)(cap - 1); out[1] = 64; out[2] = 0; out[3] = 0;
     std::copy(t.e.begin(), t.e.end(), out + 4);
     return (int64_t)(cap + 1);
+}
+
+}  // extern "C"
+
+// ---- view tier -------------------------------------------------------------
+// voxel_view_trace.wgsl (trace_view_paths, advance_view_path),
+// voxel_view_runtime.wgsl:272-349 (trace_visible_paths, retain_view_history)
+// and voxel_view_cache.wgsl:6-98, 188-258 (shared_slot, load_shared_face,
+// store_shared_faces), for a receiver list the caller gives (one receiver
+// per visible unit face, so every receiver owns itself). Records are the
+// shaders' layouts in 32-bit words:
+//   ViewReceiver 8       surface xyz, face | voxel xyz, sequence
+//   ViewPath 32          surface, sequence | voxel, face | direction, proposal_pdf |
+//                        hit_position, hit_status | hit_voxel, hit_face |
+//                        emitter, known | continuation, hit_material | direct, stream
+//   ViewContinuation 32  radiance | extra | throughput | origin, bounce |
+//                        direction, status | previous_position, 0 | previous_normal, 0 | ticket
+//                        (status: 0 new, 1 paused, 2 complete known, 3 complete unknown, 4 inactive)
+//   ViewEstimate 16      mean | moment | shown | identity (next sequence, material, corners, incarnation)
+// `queue` holds 12 counters, the owner list (n) and a word per receiver (n):
+// the owner's rank, replaced by its reserved sequence cursor when it loads
+// the shared face. The topology prior of new faces (bootstrap_face) and the
+// sun-corner records belong to raster discovery and are not restated.
+namespace orc {
+namespace view {
+
+constexpr uint32_t OWNERS = 0, COMPLETED = 2, KNOWN = 3, ATTEMPTED = 9, CACHE_LOADS = 10, CACHE_PROMOTIONS = 11, PREFIX = 12;
+
+static f3 rf3(const uint32_t* w) { return f3{bitsf(w[0]), bitsf(w[1]), bitsf(w[2])}; }
+static i3 ri3(const uint32_t* w) { return i3{(int32_t)w[0], (int32_t)w[1], (int32_t)w[2]}; }
+static void wf3(uint32_t* w, f3 v) { w[0] = fbits(v.x); w[1] = fbits(v.y); w[2] = fbits(v.z); }
+static void wi3(uint32_t* w, i3 v) { w[0] = (uint32_t)v.x; w[1] = (uint32_t)v.y; w[2] = (uint32_t)v.z; }
+static void wF4(uint32_t* w, F4 v) { w[0] = fbits(v.x); w[1] = fbits(v.y); w[2] = fbits(v.z); w[3] = fbits(v.w); }
+static F4 rF4(const uint32_t* w) { return F4{bitsf(w[0]), bitsf(w[1]), bitsf(w[2]), bitsf(w[3])}; }
+static f3 rgb(F4 v) { return f3{v.x, v.y, v.z}; }
+
+struct Wave { uint32_t range[4]; uint32_t ticket[4]; };
+
+// trace_view_paths (voxel_view_trace.wgsl:40-72) for path `id` of
+// receivers x samples.
+static void trace_view_path(Ctx& x, const uint32_t* receiver, uint32_t id, uint32_t samples, uint32_t* record) {
+    for (int i = 0; i < 32; ++i) record[i] = 0u;
+    if (receiver[3] >= 6u) return;
+    const f3 surface = rf3(receiver);
+    const i3 voxel = ri3(receiver + 4);
+    const uint32_t face = receiver[3];
+    const f3 normal = face_normal(face);
+    const uint32_t stream = hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(face + 1u);
+    const uint32_t sequence = receiver[7] + id % samples;
+    // sample_receiver_path (voxel_path.wgsl:504-513)
+    const f3 direction = hemisphere(normal, sample_1d(stream, sequence, 0u), sample_1d(stream, sequence, 1u));
+    const Energy emitter = sample_emitter(x, surface, normal, stream, sequence, 0u);
+    PathEnergy continuation;
+    if (dot(normal, direction) > 0.0f) {
+        PathState st = begin_path(add(surface, muls(normal, 0.001f)), direction, normal);
+        continuation = advance_path(x, st, stream, sequence, x.m.pipe.diffuse_hits, true).result;
+    }
+    const RayResult& hit = continuation.first_hit;
+    wf3(record, surface); record[3] = sequence;
+    wi3(record + 4, voxel); record[7] = face;
+    wf3(record + 8, direction); record[11] = fbits(cosine_pdf(normal, direction));
+    wf3(record + 12, hit.position); record[15] = hit.status;
+    wi3(record + 16, hit.voxel); record[19] = face_index_of(hit.normal);
+    wf3(record + 20, rgb(emitter.value)); record[23] = continuation.unknown ? 0u : 1u;
+    wf3(record + 24, rgb(continuation.energy.value)); record[27] = hit.material;
+    wf3(record + 28, rgb(direct_at(x, surface, normal).value)); record[31] = stream;
+}
+
+// advance_view_path (voxel_view_trace.wgsl:106-183) with one path per receiver.
+static void advance_view_path(Ctx& x, const uint32_t* receiver, uint32_t* record, uint32_t* stored, const Wave& wave) {
+    if (receiver[3] >= 6u) {
+        for (int i = 0; i < 32; ++i) record[i] = 0u;
+        stored[19] = 4u;
+        for (int i = 0; i < 4; ++i) stored[28 + i] = wave.ticket[i];
+        return;
+    }
+    const f3 surface = rf3(receiver);
+    const i3 voxel = ri3(receiver + 4);
+    const uint32_t face = receiver[3];
+    const f3 normal = face_normal(face);
+    const uint32_t stream = hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(face + 1u);
+    const uint32_t sequence = receiver[7];
+    const uint32_t status = stored[19];
+    bool restart = status == 0u || status == 4u;
+    for (int i = 0; i < 4; ++i) restart = restart || stored[28 + i] != wave.ticket[i];
+    const f3 rs = rf3(record);
+    restart = restart || rs.x != surface.x || rs.y != surface.y || rs.z != surface.z;
+    restart = restart || (int32_t)record[4] != voxel.x || (int32_t)record[5] != voxel.y || (int32_t)record[6] != voxel.z;
+    restart = restart || record[7] != face || record[3] != sequence;
+    PathState state;
+    if (restart) {
+        for (int i = 0; i < 32; ++i) record[i] = 0u;
+        wf3(record, surface); record[3] = sequence;
+        wi3(record + 4, voxel); record[7] = face;
+        const f3 direction = hemisphere(normal, sample_1d(stream, sequence, 0u), sample_1d(stream, sequence, 1u));
+        wf3(record + 8, direction);
+        record[11] = fbits(cosine_pdf(normal, direction));
+        wf3(record + 20, rgb(sample_emitter(x, surface, normal, stream, sequence, 0u).value));
+        wf3(record + 28, rgb(direct_at(x, surface, normal).value));
+        record[31] = stream;
+        state = begin_path(add(surface, muls(normal, 0.001f)), direction, normal);
+    } else {
+        if (status != 1u) return;
+        state.result.energy.value = rF4(stored);
+        RayResult first;
+        first.voxel = ri3(record + 16);
+        first.material = record[27];
+        first.position = rf3(record + 12);
+        first.status = record[15];
+        if (record[19] < 6u) first.normal = face_normal(record[19]);
+        state.result.first_hit = first;
+        state.throughput = rF4(stored + 8);
+        state.origin = rf3(stored + 12);
+        state.direction = rf3(stored + 16);
+        state.previous_position = rf3(stored + 20);
+        state.previous_normal = rf3(stored + 24);
+        state.previous_pdf = bitsf(stored[6]);
+        state.bounce = stored[15];
+    }
+    uint32_t steps = umin(wave.range[2], 8u);
+    bool terminal = false;
+    if (wave.range[3] != 0u) {
+        steps = umin(steps, wave.range[3] - umin(state.bounce, wave.range[3]));
+        terminal = state.bounce + steps == wave.range[3];
+    }
+    state = advance_path(x, state, stream, sequence, steps, terminal);
+    const RayResult& hit = state.result.first_hit;
+    wf3(record + 12, hit.position); record[15] = hit.status;
+    wi3(record + 16, hit.voxel); record[19] = face_index_of(hit.normal);
+    record[27] = hit.material;
+    record[23] = (state.done && !state.result.unknown) ? 1u : 0u;
+    wf3(record + 24, state.done ? rgb(state.result.energy.value) : f3{0.0f, 0.0f, 0.0f});
+    wF4(stored, state.result.energy.value);
+    wF4(stored + 4, F4{0.0f, 0.0f, state.previous_pdf, 0.0f});
+    wF4(stored + 8, state.throughput);
+    wf3(stored + 12, state.origin); stored[15] = state.bounce;
+    wf3(stored + 16, state.direction);
+    stored[19] = state.done ? (state.result.unknown ? 3u : 2u) : 1u;
+    wf3(stored + 20, state.previous_position);
+    wf3(stored + 24, state.previous_normal);
+    for (int i = 0; i < 4; ++i) stored[28 + i] = wave.ticket[i];
+}
+
+struct Shared {
+    uint32_t* state;      // world-cache slots, 36 words
+    uint32_t* meta;       // 12 words per slot
+    const uint32_t* index; // face index words
+    bool enabled;
+};
+
+// shared_slot (voxel_view_cache.wgsl:6-26) for a unit face.
+static uint32_t shared_slot(const Shared& sh, const uint32_t* receiver, uint32_t material) {
+    if (!sh.enabled) return NO_LIMIT;
+    const i3 v = ri3(receiver + 4);
+    const uint32_t face = receiver[3];
+    uint32_t bucket = (hash_voxel(v.x, v.y, v.z) ^ pcg(face + 1u)) & sh.index[0];
+    for (uint32_t attempt = 0; attempt < sh.index[1]; ++attempt) {
+        const uint32_t* e = sh.index + ((size_t)bucket + 1) * 4;
+        if (e[3] == 0xffffffffu) return NO_LIMIT;
+        if ((int32_t)e[0] == v.x && (int32_t)e[1] == v.y && (int32_t)e[2] == v.z && (e[3] >> 29u) == face) {
+            const uint32_t slot = e[3] & 0x1fffffffu;
+            const uint32_t key = sh.meta[(size_t)slot * 12 + 3];
+            if ((key & 8u) == 0u || (key >> 16u) != material) return NO_LIMIT;
+            return slot;
+        }
+        bucket = (bucket + 1u) & sh.index[0];
+    }
+    return NO_LIMIT;
+}
+
+}  // namespace view
+}  // namespace orc
+
+extern "C" {
+
+// trace_view_paths: `paths` gets 32 words per (receiver, sample).
+int orc_trace_view_paths(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
+                         const float* materials, const float* lights, const uint32_t* emitters, const uint32_t* state,
+                         const uint32_t* index, const orc_pipeline* pipe, const uint32_t* receivers, uint32_t n_receivers,
+                         uint32_t samples, uint32_t* paths) {
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, materials, lights, emitters, state, index, *pipe};
+    for (uint64_t id = 0; id < (uint64_t)n_receivers * samples; ++id) {
+        Ctx x{g, m, Counters{}};
+        view::trace_view_path(x, receivers + (id / samples) * 8, (uint32_t)id, samples, paths + id * 32);
+    }
+    return 0;
+}
+
+// One view frame over the caller's receivers, in the runtime's order
+// (runtime.rs Stage::ORDER): reproject (sequence from the estimate, owner
+// queue in receiver order), retain_view_history for one event batch,
+// load_shared_faces, trace_visible_paths, store_shared_faces.
+// `wave` = range (first, count, max hits, depth), ticket[4];
+// `view` = (view_first, shared, clock_ms, n_events, reach, measured_retention bits).
+int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
+                   const float* materials, const float* lights, const uint32_t* emitters, uint32_t* state, uint32_t* meta,
+                   const uint32_t* index, const orc_pipeline* pipe, uint32_t* receivers, uint32_t n, uint32_t* paths, uint32_t* conts,
+                   uint32_t* estimates, uint32_t* queue, const uint32_t* wave_words, const uint32_t* view_words, const uint32_t* events) {
+    using namespace view;
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, materials, lights, emitters, state, index, *pipe};
+    Wave wave;
+    for (int i = 0; i < 4; ++i) { wave.range[i] = wave_words[i]; wave.ticket[i] = wave_words[4 + i]; }
+    const bool view_first = view_words[0] != 0u;
+    Shared sh{state, meta, index, view_words[1] != 0u};
+    const uint32_t clock = view_words[2], n_events = view_words[3], reach = view_words[4];
+    const float physical = bitsf(view_words[5]);
+    for (uint32_t i = 0; i < PREFIX + 2 * n; ++i) queue[i] = 0u;
+    uint32_t* owners = queue + PREFIX;
+    uint32_t* cursor = queue + PREFIX + n;
+    // reproject_paths: the receiver's sequence is its estimate's, and every
+    // receiver is its own owner.
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t* r = receivers + (size_t)i * 8;
+        if (r[3] >= 6u) continue;
+        r[7] = estimates[(size_t)i * 16 + 12];
+        const uint32_t entry = queue[OWNERS]++;
+        owners[entry] = i;
+        cursor[i] = entry;
+    }
+    // retain_view_history
+    if (n_events) {
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t* r = receivers + (size_t)i * 8;
+            if (r[3] >= 6u) continue;
+            uint32_t* e = estimates + (size_t)i * 16;
+            const int32_t p[3] = {(int32_t)r[4], (int32_t)r[5], (int32_t)r[6]};
+            Retention change = resolve_retention(events, p, n_events, reach, physical > 0.0f, 0u, 0u);
+            if (e[15] == 0u || shared_slot(sh, r, e[13]) == NO_LIMIT) {
+                if (change.limit != NO_LIMIT) e[3] = fbits(wmin(bitsf(e[3]), (float)change.limit));
+                if (change.measured) e[7] = fbits(bitsf(e[7]) + change.change);
+            }
+            if (change.woken && conts[(size_t)i * 32 + 19] == 1u) conts[(size_t)i * 32 + 19] = 0u;
+        }
+    }
+    const uint32_t owner_count = queue[OWNERS];
+    // load_shared_faces (without the topology prior)
+    if (sh.enabled) {
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t* r = receivers + (size_t)i * 8;
+            if (r[3] >= 6u) continue;
+            uint32_t* e = estimates + (size_t)i * 16;
+            const uint32_t slot = shared_slot(sh, r, e[13]);
+            if (slot == NO_LIMIT) { e[15] = 0u; continue; }
+            const uint32_t* base = state + (size_t)slot * 36;
+            const uint32_t incarnation = base[28];
+            const uint32_t count = base[5] & 0x7fffffffu;
+            const uint32_t next = base[6];
+            queue[CACHE_LOADS] += 1;
+            if (e[15] == incarnation || bitsf(e[3]) <= (float)count) {
+                if (e[15] != incarnation) conts[(size_t)i * 32 + 19] = 0u;
+                e[0] = base[0]; e[1] = base[1]; e[2] = base[2]; e[3] = fbits((float)count);
+                e[4] = base[8]; e[5] = base[9]; e[6] = base[10]; e[7] = meta[(size_t)slot * 12 + 4];
+                e[12] = next;
+            } else {
+                queue[CACHE_PROMOTIONS] += 1;
+                e[12] = umax(e[12], next);
+            }
+            if (bitsf(e[11]) == 0.0f && count > 0u) {
+                const F4 shown = rF4(base + 24);
+                if (shown.w > 0.0f) wF4(e + 8, shown);
+                else { e[8] = e[0]; e[9] = e[1]; e[10] = e[2]; e[11] = fbits(1.0f); }
+            }
+            e[15] = incarnation;
+            const bool pending = conts[(size_t)i * 32 + 19] == 1u;
+            const uint32_t rank = cursor[i];
+            const uint32_t oc = umax(owner_count, 1u);
+            const uint32_t ordinal = (rank + owner_count - wave.range[0] % oc) % oc;
+            uint32_t visits = 0;
+            if (ordinal < umin(owner_count, wave.range[1]) && wave.range[2] > 0u)
+                visits = umin(view_first ? 32u : 1u, (wave.range[1] - ordinal + owner_count - 1u) / owner_count);
+            const uint32_t first = umax(next, e[12]);
+            const uint32_t starts = visits - ((pending && visits > 0u) ? 1u : 0u);
+            state[(size_t)slot * 36 + 6] = first + starts;
+            cursor[i] = first;
+            e[12] = pending ? paths[(size_t)i * 32 + 3] : first;
+            r[7] = e[12];
+        }
+    }
+    // trace_visible_paths
+    if (wave.range[2] != 0u) {
+        const uint32_t invocations = umin(owner_count, wave.range[1]);
+        for (uint32_t id = 0; id < invocations; ++id) {
+            const uint32_t i = owners[(wave.range[0] + id) % owner_count];
+            uint32_t* r = receivers + (size_t)i * 8;
+            uint32_t* e = estimates + (size_t)i * 16;
+            uint32_t* record = paths + (size_t)i * 32;
+            uint32_t* stored = conts + (size_t)i * 32;
+            const uint32_t visits = umin(view_first ? 32u : 1u, (wave.range[1] - id + owner_count - 1u) / owner_count);
+            const bool reserved = sh.enabled && e[15] != 0u;
+            uint32_t next = cursor[i];
+            if (stored[19] != 1u) next += 1u;
+            for (uint32_t visit = 0; visit < visits; ++visit) {
+                queue[ATTEMPTED] += 1;
+                Ctx x{g, m, Counters{}};
+                advance_view_path(x, r, record, stored, wave);
+                if (stored[19] != 2u && stored[19] != 3u) continue;
+                queue[COMPLETED] += 1;
+                if (reserved) { e[12] = next; next += 1u; }
+                else e[12] += 1u;
+                r[7] = e[12];
+                if (record[23] != 0u) {
+                    queue[KNOWN] += 1;
+                    const f3 value = add(rf3(record + 20), rf3(record + 24));
+                    F4 mean = rF4(e), moment = rF4(e + 4);
+                    if (moment.w > 0.0f) {
+                        const float change = moment.w;
+                        const f3 variance{wmax(moment.x - mean.x * mean.x, 0.0f), wmax(moment.y - mean.y * mean.y, 0.0f),
+                                          wmax(moment.z - mean.z * mean.z, 0.0f)};
+                        const float keep = physical * (0.2126f * variance.x + 0.7152f * variance.y + 0.0722f * variance.z) / (change * change);
+                        mean.w = wmin(mean.w, floorf(keep));
+                        moment.w = 0.0f;
+                    }
+                    const float count = wmin(mean.w + 1.0f, 65536.0f);
+                    const float t = 1.0f / count;
+                    // mix(a, b, t) = a * (1 - t) + b * t
+                    mean = F4{mean.x * (1.0f - t) + value.x * t, mean.y * (1.0f - t) + value.y * t, mean.z * (1.0f - t) + value.z * t, count};
+                    moment = F4{moment.x * (1.0f - t) + value.x * value.x * t, moment.y * (1.0f - t) + value.y * value.y * t,
+                                moment.z * (1.0f - t) + value.z * value.z * t, moment.w};
+                    wF4(e, mean);
+                    wF4(e + 4, moment);
+                }
+            }
+            if (reserved) {
+                const uint32_t first = cursor[i];
+                const uint32_t used = stored[19] == 1u ? record[3] + 1u : e[12];
+                cursor[i] = umax(first, used);
+            }
+        }
+    }
+    // store_shared_faces
+    if (sh.enabled) {
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t* r = receivers + (size_t)i * 8;
+            if (r[3] >= 6u) continue;
+            const uint32_t* e = estimates + (size_t)i * 16;
+            const uint32_t slot = shared_slot(sh, r, e[13]);
+            if (slot == NO_LIMIT) continue;
+            uint32_t* base = state + (size_t)slot * 36;
+            if (e[15] != base[28]) continue;
+            const uint32_t count = (uint32_t)bitsf(e[3]);
+            const bool changed_count = (base[5] & 0x7fffffffu) != count;
+            const bool changed_mean = base[0] != e[0] || base[1] != e[1] || base[2] != e[2];
+            base[0] = e[0]; base[1] = e[1]; base[2] = e[2]; base[3] = 0u;
+            base[8] = e[4]; base[9] = e[5]; base[10] = e[6]; base[11] = 0u;
+            base[4] = 0u;
+            base[12] = 0u;
+            base[5] = count | (bitsf(e[7]) > 0.0f ? 0x80000000u : 0u);
+            base[6] = cursor[i];
+            meta[(size_t)slot * 12 + 4] = e[7];
+            for (int k = 0; k < 4; ++k) base[24 + k] = e[8 + k];
+            if (e[14] != 0u) base[32] = e[14];
+            base[7] = e[8];
+            base[13] = e[9]; base[14] = e[10]; base[15] = e[11];
+            if (changed_mean || changed_count) {
+                const F4 mean = rF4(e), moment = rF4(e + 4);
+                auto noise = [](float mo, float me) { return std::sqrt(wmax(mo - me * me, 0.0f)) / (0.002f + std::fabs(me)); };
+                const float nz = wmax(noise(moment.x, mean.x), wmax(noise(moment.y, mean.y), noise(moment.z, mean.z)));
+                uint32_t* rank = meta + (size_t)slot * 12 + 8;
+                rank[0] = fbits(nz);
+                rank[1] = clock;
+                rank[2] = fbits(wmax(mean.x, wmax(mean.y, mean.z)));
+                rank[3] = 0xa0000000u | count;
+            }
+        }
+    }
+    return 0;
 }
 
 }  // extern "C"

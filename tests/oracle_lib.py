@@ -61,6 +61,8 @@ _SIG = {
     "orc_accumulate": (_INT, [_P, _P, _P, _P, _P, _U32, _P]),
     "orc_apply_events": (_INT, [_P, _P, _P, _P, _U32, _P]),
     "orc_measure_edits": (_INT, [_P, _P, _P, _P, _P, _U32, _P]),
+    "orc_trace_view_paths": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _U32, _P]),
+    "orc_view_frame": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _P, _P, _P, _P]),
     "orc_face_index": (_I64, [_P, _U32, _P, _U64]),
     "orc_emitters": (_I64, [_P, _U32, _P, _P, _P, _U64, _P]),
 }
@@ -270,6 +272,7 @@ class Frames:
         self.pipe = pipe
         self.threads = threads
         self.state = np.zeros((n, 36), np.uint32)
+        self.state[:, 28] = np.arange(1, n + 1, dtype=np.uint32)  # slot incarnations
         self.meta = np.zeros((n, 12), np.uint32)
         self.meta[:, 0:3] = self.faces[:, 0:3].view(np.uint32)
         self.meta[:, 3] = self.faces[:, 3].astype(np.uint32) | 8 | (self.faces[:, 4].astype(np.uint32) << 16)
@@ -294,6 +297,41 @@ class Frames:
         self.results = out
         self.batch_id = (self.batch_id + 1) & 0x0FFFFFFF or 1
         return cnt
+
+    def view_trace_paths(self, receivers, samples):
+        """trace_view_paths over receivers (8 words each) x samples."""
+        r = c(receivers, np.uint32).reshape(-1, 8)
+        out = np.zeros((r.shape[0] * samples, 32), np.uint32)
+        d, h, cl, _ = self.geometry
+        params = self.params_fn(self.n, samples)
+        lib().orc_trace_view_paths(ptr(d), d.size // 4, ptr(h), ptr(cl), ptr(params), ptr(self.materials), ptr(self.lights),
+                                   ptr(self.emitter_words), ptr(self.state), ptr(self.index), ctypes.byref(self.pipe), ptr(r),
+                                   r.shape[0], samples, ptr(out))
+        return out
+
+    def view_start(self, receivers, materials):
+        """A view tier over `receivers` (8 words each, as vgi_view_read
+        returns them) with empty estimates of the given materials."""
+        n = receivers.shape[0]
+        self.view = {"receivers": c(receivers, np.uint32).copy(), "paths": np.zeros((n, 32), np.uint32),
+                     "continuations": np.zeros((n, 32), np.uint32), "estimates": np.zeros((n, 16), np.uint32),
+                     "queue": np.zeros(12 + 2 * n, np.uint32)}
+        self.view["estimates"][:, 13] = materials
+
+    def view_frame(self, first=0, invocations=0, max_hits=8, depth=0, ticket=(0, 0, 0, 0), view_first=False, shared=True,
+                   clock_ms=0, events=None, n_events=0, measured_retention=1.0):
+        v = self.view
+        n = v["receivers"].shape[0]
+        wave = np.array([first, invocations or n, max_hits, depth, *ticket], np.uint32)
+        view = np.array([int(view_first), int(shared and self.n > 0), clock_ms, n_events, 192 * 192, 0], np.uint32)
+        view[5] = np.float32(max(measured_retention, 0.0)).view(np.uint32)
+        ev = np.zeros(4, np.uint32) if events is None else c(events, np.uint32)
+        d, h, cl, _ = self.geometry
+        params = self.params_fn(self.n, 1)
+        lib().orc_view_frame(ptr(d), d.size // 4, ptr(h), ptr(cl), ptr(params), ptr(self.materials), ptr(self.lights),
+                             ptr(self.emitter_words), ptr(self.state), ptr(self.meta), ptr(self.index), ctypes.byref(self.pipe),
+                             ptr(v["receivers"]), n, ptr(v["paths"]), ptr(v["continuations"]), ptr(v["estimates"]), ptr(v["queue"]),
+                             ptr(wave), ptr(view), ptr(ev))
 
     def measure_edits(self, words, measures, n_entries, material_light):
         """measure_edits + finish_edits on a copy of the event words."""

@@ -1,0 +1,101 @@
+"""View tier parity: trace_view_paths, and view frames (retain_view_history,
+load_shared_faces, trace_visible_paths with paused paths, store_shared_faces)
+interleaved with world-cache frames, bit for bit against the oracle."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+import vgi
+from test_gpu_parity import assert_words_equal, encode_events, lanes_for, terrain_case
+
+pytestmark = pytest.mark.gpu
+
+
+def world(gpu, case, frames):
+    case.load(gpu)
+    geometry = gpu.geometry()
+    lanes = lanes_for(case.transport, 8)
+    ref = O.Frames(geometry, case.params_fn(geometry), case.materials, case.lights, case.emitters, case.faces, case.transport,
+                   case.pipe(lanes))
+    for f in range(frames):
+        gpu.frame(8, clock_ms=16 * f)
+        ref.frame(8, clock_ms=16 * f)
+    return ref
+
+
+def receivers_for(faces):
+    normals = np.array(vgi.FACE_OFFSETS, np.float32)
+    r = np.zeros((faces.shape[0], 8), np.uint32)
+    surface = (faces[:, 0:3].astype(np.float32) + np.float32(0.5)) + normals[faces[:, 3]] * np.float32(0.5)
+    r[:, 0:3] = surface.astype(np.float32).view(np.uint32)
+    r[:, 3] = faces[:, 3]
+    r[:, 4:7] = faces[:, 0:3].view(np.uint32)
+    return r
+
+
+def compare_view(gpu, ref, what):
+    got = gpu.view_read()
+    for key in ("receivers", "paths", "continuations", "estimates", "queue"):
+        assert_words_equal(got[key], ref.view[key], f"{what}: view {key}")
+    assert_words_equal(gpu.read_state(), ref.state, f"{what}: world state")
+    assert_words_equal(gpu.read_slot_meta(), ref.meta, f"{what}: world slot metadata")
+
+
+def test_view_paths_match_oracle(gpu):
+    case = terrain_case(bounces=2)
+    ref = world(gpu, case, 3)
+    faces = case.faces[::7].copy()
+    gpu.view_set_receivers(faces)
+    receivers = gpu.view_read()["receivers"]
+    assert_words_equal(receivers, receivers_for(faces), "receivers")
+    got = gpu.view_trace_paths(4)
+    want = ref.view_trace_paths(receivers, 4)
+    assert_words_equal(got, want, "view paths")
+    # Some paths ended at cached faces, some traced on.
+    assert (want[:, 23] == 1).any() and (want[:, 15] == 1).any()
+
+
+@pytest.mark.parametrize("view_first", [False, True])
+def test_view_frames_with_pauses_and_handoff_match_oracle(gpu, view_first):
+    case = terrain_case(bounces=2, measured_retention=1.0)
+    ref = world(gpu, case, 3)
+    faces = case.faces[::5].copy()
+    gpu.view_set_receivers(faces)
+    ref.view_start(gpu.view_read()["receivers"], faces[:, 4])
+    n = faces.shape[0]
+    c = faces[n // 2, :3]
+    events, n_events = encode_events([(c - 3, c + 3, [(c - 3, c + 3, 30.0, 3)])])
+    plan = [
+        dict(max_hits=1, invocations=n),                       # every path pauses after one hit
+        dict(max_hits=1, invocations=n, first=7),              # resumes from a rotated owner
+        dict(max_hits=2, invocations=n // 2, first=3),         # a partial wave
+        dict(max_hits=8, invocations=2 * n, ticket=(1, 0, 0, 0)),  # a new ticket restarts paused paths
+        dict(max_hits=3, invocations=n, depth=3),              # a finite depth
+        dict(max_hits=8, invocations=n, events=events, n_events=n_events),  # retention on view history
+    ]
+    for k, wave in enumerate(plan):
+        gpu.view_frame(view_first=view_first, clock_ms=100 + k, **wave)
+        ref.view_frame(view_first=view_first, clock_ms=100 + k, measured_retention=1.0, **wave)
+        compare_view(gpu, ref, f"view frame {k}")
+        # The world cache keeps running between view frames and reads what the view stored.
+        gpu.frame(8, clock_ms=200 + k)
+        ref.frame(8, clock_ms=200 + k)
+        assert_words_equal(gpu.read_results(), ref.results, f"world results after view frame {k}")
+    q = ref.view["queue"]
+    assert q[2] > 0 and q[3] > 0 and q[10] > 0  # completed, known, cache loads
+    status = ref.view["continuations"][:, 19]
+    assert set(np.unique(status)) <= {1, 2, 3}
+
+
+def test_view_without_shared_cache_keeps_its_own_history(gpu):
+    case = terrain_case(bounces=2)
+    ref = world(gpu, case, 2)
+    faces = case.faces[::9].copy()
+    gpu.view_set_receivers(faces)
+    ref.view_start(gpu.view_read()["receivers"], faces[:, 4])
+    for k in range(3):
+        gpu.view_frame(max_hits=8, shared=False, clock_ms=k)
+        ref.view_frame(max_hits=8, shared=False, clock_ms=k)
+        compare_view(gpu, ref, f"unshared view frame {k}")
+    est = ref.view["estimates"]
+    assert (est[:, 3].view(np.float32) > 0).any() and (est[:, 15] == 0).all()
