@@ -137,6 +137,29 @@ def lane_use(census):
     return {"queued": lp[0] / max(wp[0], 1), "drain": lp[1] / max(wp[1], 1), "drain_pass_share": wp[1] / total}
 
 
+def relmse(g, faces, frames, n_faces=4096, spp=16384):
+    """Relative MSE of the world cache's accumulated face means against the
+    FP64 converged reference on a seeded face sample, in luminance:
+    mean((L - L_ref)^2 / (L_ref^2 + 0.01)). The reference's own noise floor
+    (its variance of the mean in the same units) is reported beside it."""
+    rng = np.random.default_rng(17)
+    sel = np.sort(rng.choice(faces.shape[0], size=min(n_faces, faces.shape[0]), replace=False))
+    import vgi
+
+    t0 = time.perf_counter()
+    ref, second, known = g.reference_fp64(vgi.tasks_for(faces[sel]), spp, seed=23)
+    seconds = time.perf_counter() - t0
+    w = np.array([0.2126, 0.7152, 0.0722])
+    est = g.read_state()[sel, 0:3].view(np.float32).astype(np.float64)
+    lr, le = ref @ w, est @ w
+    var_ref = (np.maximum(second - ref ** 2, 0.0) / np.maximum(known, 1)[:, None]) @ (w * w)
+    return {"value": float(np.mean((le - lr) ** 2 / (lr ** 2 + 0.01))), "faces": int(sel.size), "reference_spp": spp,
+            "frames_accumulated": frames, "reference_noise": float(np.mean(var_ref / (lr ** 2 + 0.01))),
+            "reference_seconds": round(seconds, 3),
+            "definition": "luminance, mean over faces of (L - L_ref)^2 / (L_ref^2 + 0.01); "
+                          "L = world-cache mean after the frames run, L_ref = FP64 unbiased path tracing (roulette, no cache)"}
+
+
 def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total, budget_s=15.0):
     """The oracle on a bounded face sample with the GPU's warm cache state."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -340,6 +363,7 @@ def main():
     achieved = traverse_bytes / (traverse_ms * 1e-3) / 1e9
     traffic = profiled_traffic()
     if rank == 0:
+        quality = relmse(g, faces, args.warmup + 2 * args.steps)
         base = None
         if world == 1 and not args.no_cpu_baseline:
             geometry = g.geometry()
@@ -379,6 +403,7 @@ def main():
                          "note": "traversal algorithmic bytes (directory, header, brick, cell words; counting pass) / "
                                  "CUDA-event time of the traversal launches, same frame"},
             "clocks": clocks,
+            "relmse": quality,
         }
         if base:
             line["cpu_baseline"] = base

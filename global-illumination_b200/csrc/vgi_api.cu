@@ -46,6 +46,10 @@ struct DevBuf {
         ptr = nullptr;
         count = 0;
     }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
 };
 
 constexpr uint32_t kHistoryLimit = 65536;
@@ -82,6 +86,7 @@ struct vgi_ctx {
 
     // model
     std::vector<float> host_materials = std::vector<float>(256 * 16, 0.0f);
+    std::vector<uint32_t> host_emitter_records;  // 8 words per emitter face
     DevBuf<float4> materials;
     DevBuf<float2> material_light;  // (albedo, emission) luminance per material
     DevBuf<uint4> measures;
@@ -689,6 +694,7 @@ int vgi_set_emitters(vgi_ctx* c, const uint32_t* words, uint64_t n_words, uint32
     VGI_CUDA(c, cudaSetDevice(c->device));
     VGI_CUDA(c, c->emitters.reserve(n_words / 4));
     VGI_CUDA(c, cudaMemcpyAsync(c->emitters.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    c->host_emitter_records.assign(words, words + (size_t)n_faces * 8);
     const uint32_t nodes = (uint32_t)((n_words - records * 8) / 16);
     VGI_CUDA(c, c->node_aux.reserve(2 * (size_t)std::max<uint32_t>(nodes, 1)));
     launch_node_aux(c->emitters.ptr, (uint32_t)(records * 2), nodes, c->node_aux.ptr, c->stream);
@@ -1026,6 +1032,60 @@ int vgi_view_trace_paths(vgi_ctx* c, uint32_t samples, uint32_t* paths32) {
     VGI_CUDA(c, cudaGetLastError());
     VGI_CUDA(c, cudaMemcpyAsync(paths32, c->v_scratch.ptr, total * 128, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_reference_fp64(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samples, uint64_t seed, double* mean3, double* second3,
+                       uint32_t* known) {
+    if (!c || (n && (!tasks || !mean3))) return VGI_ERR_INVALID;
+    if (!view_ready(c)) return fail(c, VGI_ERR_STATE, "the reference needs geometry, materials, lights and emitters");
+    if (n == 0) return VGI_OK;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    // Emitters chosen in proportion to their material's emission weight.
+    const size_t ne = c->host_emitter_records.size() / 8;
+    std::vector<double> cdf(ne + 1, 0.0);
+    std::vector<int4> recs(std::max<size_t>(ne, 1));
+    for (size_t i = 0; i < ne; ++i) {
+        const uint32_t* w = c->host_emitter_records.data() + i * 8;
+        float mf;
+        std::memcpy(&mf, &w[6], 4);
+        const uint32_t m = (uint32_t)mf & 255u;
+        const double weight = (double)c->host_materials[(size_t)m * 16 + 13];
+        cdf[i + 1] = cdf[i] + weight;
+        recs[i] = make_int4((int)w[0], (int)w[1], (int)w[2], (int)((w[3] & 7u) | (m << 3)));
+    }
+    DevBuf<double> d_cdf, d_sum, d_second;
+    DevBuf<int4> d_recs;
+    DevBuf<uint4> d_tasks;
+    DevBuf<uint32_t> d_known;
+    VGI_CUDA(c, d_cdf.reserve(ne + 1));
+    VGI_CUDA(c, d_recs.reserve(recs.size()));
+    VGI_CUDA(c, d_tasks.reserve((size_t)n * 2));
+    VGI_CUDA(c, d_sum.reserve((size_t)n * 3));
+    VGI_CUDA(c, d_second.reserve((size_t)n * 3));
+    VGI_CUDA(c, d_known.reserve(n));
+    VGI_CUDA(c, cudaMemcpyAsync(d_cdf.ptr, cdf.data(), cdf.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(d_recs.ptr, recs.data(), recs.size() * 16, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(d_tasks.ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    TraceArgs a = trace_args(c, nullptr, nullptr, 0, 1, false);
+    launch_reference64(a, d_cdf.ptr, d_recs.ptr, (uint32_t)ne, cdf[ne], d_tasks.ptr, n, samples, seed, d_sum.ptr, d_second.ptr, d_known.ptr,
+                       c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    std::vector<double> sum((size_t)n * 3), second((size_t)n * 3);
+    std::vector<uint32_t> cnt(n);
+    VGI_CUDA(c, cudaMemcpyAsync(sum.data(), d_sum.ptr, sum.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(second.data(), d_second.ptr, second.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(cnt.data(), d_known.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    d_cdf.release(); d_recs.release(); d_tasks.release(); d_sum.release(); d_second.release(); d_known.release();
+    for (uint32_t i = 0; i < n; ++i) {
+        const double k = cnt[i] ? (double)cnt[i] : 1.0;
+        for (int j = 0; j < 3; ++j) {
+            mean3[(size_t)i * 3 + j] = sum[(size_t)i * 3 + j] / k;
+            if (second3) second3[(size_t)i * 3 + j] = second[(size_t)i * 3 + j] / k;
+        }
+        if (known) known[i] = cnt[i];
+    }
     return VGI_OK;
 }
 

@@ -95,6 +95,9 @@ void launch_view_frame(const ViewArgs& v, bool limited, bool budgeted, cudaStrea
 void launch_view_trace_paths(const ViewArgs& v, uint32_t samples, uint4* out, bool limited, bool budgeted, cudaStream_t stream);
 void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
 uint32_t wave_traverse_blocks_per_sm();
+void launch_reference64(const TraceArgs& a, const double* cdf, const int4* emitters, uint32_t n_emitters, double total,
+                        const uint4* tasks, uint32_t n_tasks, uint32_t samples, uint64_t seed, double* sum, double* second,
+                        uint32_t* known, cudaStream_t s);
 void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s);
 void launch_measure_edits(const uint4* state, const uint4* slot_meta, const uint4* index, const float2* material_light,
                           const uint4* measures, uint32_t n_entries, uint32_t n_positions, uint32_t* measure_max, uint4* events,

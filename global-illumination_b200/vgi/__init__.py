@@ -165,6 +165,7 @@ _SIGNATURES = {
     "vgi_view_frame": (_INT, [_P, _P, _P, _U32, _U64]),
     "vgi_view_read": (_INT, [_P, _P, _P, _P, _P, _P]),
     "vgi_view_trace_paths": (_INT, [_P, _U32, _P]),
+    "vgi_reference_fp64": (_INT, [_P, _P, _U32, _U32, _U64, _P, _P, _P]),
     "vgi_read_results": (_INT, [_P, _U32, _U32, _P]),
     "vgi_read_state": (_INT, [_P, _U32, _U32, _P]),
     "vgi_write_state": (_INT, [_P, _U32, _U32, _P]),
@@ -480,6 +481,16 @@ class GpuTracer:
         out = np.zeros((n * samples, 32), np.uint32)
         self._check(self._lib.vgi_view_trace_paths(self._h, samples, _ptr(out)))
         return out
+
+    def reference_fp64(self, tasks: np.ndarray, samples: int, seed: int = 1):
+        """FP64 converged reference per FaceTask: (mean rgb, mean square rgb, known)."""
+        t = _c(tasks, np.uint32).reshape(-1, 8)
+        n = t.shape[0]
+        mean = np.zeros((n, 3), np.float64)
+        second = np.zeros((n, 3), np.float64)
+        known = np.zeros(n, np.uint32)
+        self._check(self._lib.vgi_reference_fp64(self._h, _ptr(t), n, samples, seed, _ptr(mean), _ptr(second), _ptr(known)))
+        return mean, second, known
 
     def read_results(self, first: int = 0, n: Optional[int] = None) -> np.ndarray:
         n = self.n_slots - first if n is None else n

@@ -220,6 +220,18 @@ int vgi_view_read(vgi_ctx* ctx, uint32_t* receivers8, uint32_t* paths32, uint32_
  * (sequence + i), one ViewPath record each, in receiver-major order. */
 int vgi_view_trace_paths(vgi_ctx* ctx, uint32_t samples, uint32_t* paths32);
 
+/* ---- FP64 converged reference ------------------------------------------------
+ * No counterpart in the reference's GPU path: an error yardstick. For each
+ * FaceTask (8 words; voxel, face, sequence), `samples` independent unbiased
+ * samples of the quantity the world cache accumulates (cosine-averaged
+ * incident radiance without the face's own direct light), in double
+ * precision, without the cache and with Russian roulette instead of a depth
+ * cut. mean3 / second3 get the per-face mean and mean square (rgb), known the
+ * samples that did not reach unloaded space. `seed` selects the random
+ * streams. Synchronous. */
+int vgi_reference_fp64(vgi_ctx* ctx, const uint32_t* tasks, uint32_t n, uint32_t samples, uint64_t seed, double* mean3, double* second3,
+                       uint32_t* known);
+
 /* ---- read-back: bounded snapshots (complete_readback, src/gpu.rs:1024-1170) --- */
 int vgi_read_results(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words24);
 int vgi_read_state(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words36);
