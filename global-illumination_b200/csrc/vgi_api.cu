@@ -74,6 +74,8 @@ struct vgi_ctx {
     uint64_t cells_used = 0;
     bool geometry = false;
     DevBuf<int4> directory;
+    DevBuf<int32_t> grid;  // region_grid: header index per region of the bounding box
+    bool has_grid = false;
     DevBuf<uint4> headers;
     DevBuf<uint32_t> cells;
     DevBuf<uint16_t> voxels;
@@ -226,6 +228,7 @@ TraceArgs trace_args(vgi_ctx* c, const uint4* tasks, uint4* results, uint32_t n,
     for (int k = 0; k < 4; ++k) a.env[k] = c->env[k];
     a.light_count = c->n_lights;
     a.lights = c->lights.ptr;
+    a.region_grid = c->has_grid ? c->grid.ptr : nullptr;
     a.face_index = with_cache ? c->face_index.ptr : nullptr;
     a.cache = with_cache ? c->cache.ptr : nullptr;
     a.tasks = tasks;
@@ -261,6 +264,20 @@ int check_ready(vgi_ctx* c, bool need_faces) {
 }
 
 bool transport_limited(const vgi_ctx* c) { return norm_reach(c->transport.reach) < kMaxPathDistance; }
+
+// The dense region grid the timed traversal reads instead of probing the
+// directory: built when the bounding box holds at most 2^24 regions (64 MB).
+cudaError_t upload_grid(vgi_ctx* c, const int32_t* directory, uint64_t slots) {
+    const std::vector<int32_t> grid = region_grid(directory, slots, c->bounds, c->bounds + 3, 1ull << 24);
+    c->has_grid = !grid.empty();
+    if (!c->has_grid) return cudaSuccess;
+    cudaError_t e = c->grid.reserve(grid.size());
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(c->grid.ptr, grid.data(), grid.size() * 4, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return e;
+    // The staging vector dies here, so the copy completes first.
+    return cudaStreamSynchronize(c->stream);
+}
 
 // Enqueues the face trace for `a` in the context's layout.
 int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
@@ -418,7 +435,7 @@ int vgi_destroy(vgi_ctx* c) {
     c->pack_error.release(); c->edit_buf.release(); c->zw.release(); c->region_list.release(); c->dedup_table.release();
     c->materials.release(); c->lights.release(); c->emitters.release(); c->node_aux.release();
     c->tasks.release(); c->results.release(); c->state.release(); c->slot_meta.release(); c->checkpoint.release();
-    c->face_index.release(); c->cache.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
+    c->face_index.release(); c->cache.release(); c->grid.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
     c->material_light.release(); c->measures.release(); c->measure_max.release();
     c->v_receivers.release(); c->v_paths.release(); c->v_conts.release(); c->v_estimates.release(); c->v_events.release();
     c->v_scratch.release(); c->v_queue.release();
@@ -492,6 +509,7 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
     c->dir_slots = dir.size() / 4;
     VGI_CUDA(c, c->directory.reserve(c->dir_slots));
     VGI_CUDA(c, cudaMemcpyAsync(c->directory.ptr, dir.data(), dir.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, upload_grid(c, dir.data(), c->dir_slots));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->geometry = true;
     return VGI_OK;
@@ -537,6 +555,8 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
     c->dir_slots = slots;
     c->cells_used = n_cells;
     for (int k = 0; k < 6; ++k) c->bounds[k] = bounds6[k];
+    VGI_CUDA(c, upload_grid(c, directory, slots));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->keys.clear();
     c->where.clear();
     c->host_voxels.clear();

@@ -256,6 +256,35 @@ Extents TopLevelField::at(int32_t x, int32_t y, int32_t z) const {
     return cells[g.index(x - lo[0], y - lo[1], z - lo[2])];
 }
 
+std::vector<int32_t> region_grid(const int32_t* directory, uint64_t slots, const int32_t lo[3], const int32_t hi[3], uint64_t max_cells) {
+    std::vector<int32_t> grid;
+    if (slots == 0) return grid;
+    uint64_t cells = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (hi[a] < lo[a]) return grid;
+        cells *= (uint64_t)((int64_t)hi[a] - lo[a] + 1);
+        if (cells > max_cells) return grid;
+    }
+    grid.assign(cells, -1);
+    const uint64_t mask = slots - 1;
+    size_t i = 0;
+    for (int32_t z = lo[2]; z <= hi[2]; ++z)
+        for (int32_t y = lo[1]; y <= hi[1]; ++y)
+            for (int32_t x = lo[0]; x <= hi[0]; ++x, ++i) {
+                uint64_t slot = host_hash_voxel(x, y, z) & mask;
+                for (uint32_t attempt = 0; attempt < 32u; ++attempt) {
+                    const int32_t* e = directory + slot * 4;
+                    if (e[3] == -1) break;
+                    if (e[0] == x && e[1] == y && e[2] == z) {
+                        grid[i] = e[3];
+                        break;
+                    }
+                    slot = (slot + 1) & mask;
+                }
+            }
+    return grid;
+}
+
 std::vector<int32_t> build_directory(const std::vector<RegionKey>& keys) {
     size_t capacity = 1;
     while (capacity < keys.size() * 2) capacity <<= 1;

@@ -63,4 +63,10 @@ EmitterWords build_emitters(const std::vector<RegionKey>& keys, const uint16_t* 
 uint32_t host_pcg(uint32_t v);
 uint32_t host_hash_voxel(int32_t x, int32_t y, int32_t z);
 
+// What lookup_region (shaders/voxel_traversal.wgsl:32-41) returns for every
+// region of the bounding box [lo, hi] (x fastest): the header index, or -1
+// where the probe finds an empty slot or gives up after 32 probes. Empty when
+// the box holds more than `max_cells` regions.
+std::vector<int32_t> region_grid(const int32_t* directory, uint64_t slots, const int32_t lo[3], const int32_t hi[3], uint64_t max_cells);
+
 }  // namespace vgi

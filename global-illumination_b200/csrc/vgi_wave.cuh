@@ -515,12 +515,13 @@ __device__ __forceinline__ void creep(const TraceArgs& A, RayRun& s, Cnt<C>& cnt
     }
 }
 
+constexpr uint32_t kGo = 0xffffffffu;
+
+// The first half of a step: everything up to the box step. It leaves `status`
+// at kGo when the ray skips the box in s.plane, or sets the ray's outcome.
 template <bool BUDGETED, bool C>
-__device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& cnt, uint32_t creep_limit) {
+__device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<C>& cnt, uint32_t& status, uint32_t& material, I3& voxel) {
     const TraceArgs& A = W.t;
-    constexpr uint32_t kGo = 0xffffffffu;
-    uint32_t status = kGo, material = 0u;
-    I3 voxel{0, 0, 0};
     if (s.step >= A.path_steps) {
         status = 2u;
         material = 0xffffffffu;
@@ -542,7 +543,14 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
             uint32_t shift = 4u;
             bool missing = false;
             if (s.lrx != rx || s.lry != ry || s.lrz != rz) {
-                const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
+                // The timed pass reads the dense grid (the same answer as the
+                // probe); the counting pass probes, to count its words.
+                const uint32_t index =
+                    (!C && A.region_grid)
+                        ? (uint32_t)__ldg(A.region_grid + ((size_t)(rz - A.mn[2]) * (uint32_t)(A.mx[1] - A.mn[1] + 1) + (uint32_t)(ry - A.mn[1])) *
+                                                              (uint32_t)(A.mx[0] - A.mn[0] + 1) +
+                                          (uint32_t)(rx - A.mn[0]))
+                        : lookup_region(A, rx, ry, rz, cnt);
                 if (index == kNoIndex) {
                     missing = true;
                 } else {
@@ -612,6 +620,12 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
             }
         }
     }
+}
+
+// The second half: the ray ends with its outcome, or takes the box step.
+template <bool BUDGETED, bool C>
+__device__ __forceinline__ void finish_step(const WaveArgs& W, RayRun& s, Cnt<C>& cnt, uint32_t status, uint32_t material, I3 voxel,
+                                            uint32_t creep_limit) {
     if (status != kGo) {
         cnt.status(status);
         const bool hit = status == 1u;
@@ -624,15 +638,21 @@ __device__ __forceinline__ void step_ray(const WaveArgs& W, RayRun& s, Cnt<C>& c
     s.pos = s.pos + s.dir * adv.w;
     s.nrm = V3{adv.x, adv.y, adv.z};
     s.step += 1u;
-    if (adv.w == 0.001f && s.shift != kNoIndex) creep<C>(A, s, cnt, creep_limit);
+    if (adv.w == 0.001f && s.shift != kNoIndex) creep<C>(W.t, s, cnt, creep_limit);
 }
 
 // trace() (voxel_path.wgsl:239-243) for every queued ray. Persistent warps
 // keep one ray per lane and advance all lanes one DDA step per pass; when
 // enough lanes have finished, they take the next rays from the queue (one
 // atomic per warp), so a warp is not held by its longest ray.
+// Resident blocks of the persistent traversal the compiler must fit per SM
+// (its register budget follows from it).
+#ifndef VGI_TRAVERSE_MIN_BLOCKS
+#define VGI_TRAVERSE_MIN_BLOCKS 4
+#endif
+
 template <bool BUDGETED, bool C>
-__global__ void __launch_bounds__(kWaveBlock) wave_traverse_kernel(const WaveArgs W, uint32_t refill_min) {
+__global__ void __launch_bounds__(kWaveBlock, VGI_TRAVERSE_MIN_BLOCKS) wave_traverse_kernel(const WaveArgs W, uint32_t refill_min) {
     const TraceArgs& A = W.t;
     Cnt<C> cnt;
     const uint32_t total = *W.count_in;
@@ -664,9 +684,18 @@ __global__ void __launch_bounds__(kWaveBlock) wave_traverse_kernel(const WaveArg
                 cnt.lp[exhausted ? 1 : 0] += (uint32_t)__popc(busy);
             }
         }
-        // While rays remain queued a grazing lane replays at most 64 steps per
-        // pass, so it holds up the warp's other lanes only briefly.
-        if (!idle) step_ray<BUDGETED, C>(W, s, cnt, exhausted ? 0xffffffffu : s.step + 64u);
+        // One step per busy lane, in two halves. The first half branches by
+        // what the ray's position holds (region lookup, air region, brick,
+        // voxel); the warp reconverges before the second, so the box step
+        // that most lanes take runs once for all of them. While rays remain
+        // queued a grazing lane replays at most 64 steps per pass, so it
+        // holds up the warp's other lanes only briefly.
+        uint32_t status = kGo, material = 0u;
+        I3 voxel{0, 0, 0};
+        const uint32_t creep_limit = exhausted ? 0xffffffffu : s.step + 64u;
+        if (!idle) classify_step<BUDGETED, C>(W, s, cnt, status, material, voxel);
+        __syncwarp();
+        if (!idle) finish_step<BUDGETED, C>(W, s, cnt, status, material, voxel, creep_limit);
     }
     flush_counters<C>(A, cnt);
 }
