@@ -24,6 +24,23 @@ namespace {
 
 constexpr int kWaveBlock = 256;
 
+// Resident blocks per SM each kernel's register budget must allow.
+#ifndef VGI_TRAVERSE_MIN_BLOCKS
+#define VGI_TRAVERSE_MIN_BLOCKS 4
+#endif
+#ifndef VGI_BEGIN_MIN_BLOCKS
+#define VGI_BEGIN_MIN_BLOCKS 4
+#endif
+#ifndef VGI_SHADE_MIN_BLOCKS
+#define VGI_SHADE_MIN_BLOCKS 4
+#endif
+#ifndef VGI_SCATTER_MIN_BLOCKS
+#define VGI_SCATTER_MIN_BLOCKS 4
+#endif
+#ifndef VGI_FINALIZE_MIN_BLOCKS
+#define VGI_FINALIZE_MIN_BLOCKS 4
+#endif
+
 // Path-state fields, each an array of n_paths float4 (SoA for coalescing).
 enum : uint32_t {
     kE = 0,    // continuation energy rgb, previous_pdf
@@ -310,7 +327,7 @@ __device__ __forceinline__ void flush_counters(const TraceArgs& A, Cnt<C>& cnt) 
 // Stage 0: the receiver sample (voxel_path.wgsl:504-513) of every path, and
 // the face-centre direct rays of write_result (voxel_trace.wgsl:28).
 template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
-__global__ void __launch_bounds__(kWaveBlock) wave_begin_kernel(const WaveArgs W) {
+__global__ void __launch_bounds__(kWaveBlock, VGI_BEGIN_MIN_BLOCKS) wave_begin_kernel(const WaveArgs W) {
     __shared__ float4 smat[512];
     const TraceArgs& A = W.t;
     stage_materials<HITS, LIMITED, BUDGETED, C>(A, smat);
@@ -645,11 +662,6 @@ __device__ __forceinline__ void finish_step(const WaveArgs& W, RayRun& s, Cnt<C>
 // keep one ray per lane and advance all lanes one DDA step per pass; when
 // enough lanes have finished, they take the next rays from the queue (one
 // atomic per warp), so a warp is not held by its longest ray.
-// Resident blocks of the persistent traversal the compiler must fit per SM
-// (its register budget follows from it).
-#ifndef VGI_TRAVERSE_MIN_BLOCKS
-#define VGI_TRAVERSE_MIN_BLOCKS 4
-#endif
 
 template <bool BUDGETED, bool C>
 __global__ void __launch_bounds__(kWaveBlock, VGI_TRAVERSE_MIN_BLOCKS) wave_traverse_kernel(const WaveArgs W, uint32_t refill_min) {
@@ -703,7 +715,7 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_TRAVERSE_MIN_BLOCKS) wave_trav
 // Stage s >= 1: complete the pending hit, then the continuation's new hit
 // (one iteration of advance_path, voxel_path.wgsl:432-490).
 template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
-__global__ void __launch_bounds__(kWaveBlock) wave_shade_kernel(const WaveArgs W, uint32_t stage) {
+__global__ void __launch_bounds__(kWaveBlock, VGI_SHADE_MIN_BLOCKS) wave_shade_kernel(const WaveArgs W, uint32_t stage) {
     __shared__ float4 smat[512];
     const TraceArgs& A = W.t;
     stage_materials<HITS, LIMITED, BUDGETED, C>(A, smat);
@@ -854,7 +866,7 @@ __global__ void __launch_bounds__(kWaveBlock) wave_shade_kernel(const WaveArgs W
 // sample_terminal_emission's connection, then roulette and the continuation.
 // Queue entries are path | bounce << 30; warps stride over the queue.
 template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
-__global__ void __launch_bounds__(kWaveBlock) wave_scatter_kernel(const WaveArgs W) {
+__global__ void __launch_bounds__(kWaveBlock, VGI_SCATTER_MIN_BLOCKS) wave_scatter_kernel(const WaveArgs W) {
     __shared__ float4 smat[512];
     const TraceArgs& A = W.t;
     stage_materials<HITS, LIMITED, BUDGETED, C>(A, smat);
@@ -941,7 +953,7 @@ __global__ void __launch_bounds__(kWaveBlock) wave_scatter_kernel(const WaveArgs
 // one thread per (face, lane), lanes summing strided samples, lane 0 summing
 // the lanes in order.
 template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
-__global__ void __launch_bounds__(kWaveBlock) wave_finalize_kernel(const WaveArgs W) {
+__global__ void __launch_bounds__(kWaveBlock, VGI_FINALIZE_MIN_BLOCKS) wave_finalize_kernel(const WaveArgs W) {
     __shared__ float4 smat[512];
     const TraceArgs& A = W.t;
     stage_materials<HITS, LIMITED, BUDGETED, C>(A, smat);
