@@ -293,6 +293,7 @@ def main():
     g.build_emitters()
     g.set_transport(transport)
     g.set_faces(faces)
+    tuned = g.autotune(SPP)
     g.set_timing(True)
     n = faces.shape[0]
     stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
@@ -331,6 +332,24 @@ def main():
     paths_per_frame = before["paths"]
     total_ms = float(sum(step_ms))
 
+    # The same frames replayed from a captured CUDA graph (timing events off).
+    g.set_timing(False)
+    g.set_graph(True)
+    graph_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 2)]
+    for k in range(args.steps + 1):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+            graph_ev[2 * k].record(stream)
+        g.frame(SPP, clock)
+        clock += 16
+        with torch.cuda.stream(stream):
+            graph_ev[2 * k + 1].record(stream)
+    torch.cuda.synchronize()
+    # The first frame after enabling runs directly and the second is captured.
+    graph_ms = float(np.mean([graph_ev[2 * k].elapsed_time(graph_ev[2 * k + 1]) for k in range(2, args.steps + 1)]))
+    g.set_graph(False)
+    g.set_timing(True)
+
     # End to end through the C ABI: pinned host tasks in, results out, every frame.
     tasks_host = torch.empty((n, 8), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     tasks_host[:] = vgi.tasks_for(faces)
@@ -363,7 +382,7 @@ def main():
     achieved = traverse_bytes / (traverse_ms * 1e-3) / 1e9
     traffic = profiled_traffic()
     if rank == 0:
-        quality = relmse(g, faces, args.warmup + 2 * args.steps)
+        quality = relmse(g, faces, args.warmup + 3 * args.steps + 1)
         base = None
         if world == 1 and not args.no_cpu_baseline:
             geometry = g.geometry()
@@ -392,6 +411,8 @@ def main():
                        "kernel_ms": {"prepare": float(np.mean([t[0] for t in kernel_ms])), "trace": trace_ms,
                                      "traverse": traverse_ms, "accumulate": float(np.mean([t[2] for t in kernel_ms]))},
                        "trace_algorithmic_gbs": bytes_per_frame / (trace_ms * 1e-3) / 1e9,
+                       "autotune": tuned,
+                       "graph_ms_per_frame": graph_ms,
                        "paths_per_s": paths_per_frame * world / (total_ms * 1e-3 / args.steps),
                        "frames_per_s": 1000.0 * args.steps / total_ms},
             "e2e": {"value": total_rays / (e2e_total * 1e-3), "unit": "rays/s", "h2d_bytes_per_step": int(n * 32), "d2h_bytes_per_step": int(n * 96)},

@@ -347,6 +347,9 @@ void launch_measure_edits(const uint4* state, const uint4* slot_meta, const uint
     finish_edits_kernel<<<(n_entries + kBlock - 1) / kBlock, kBlock, 0, s>>>(measures, n_entries, measure_max, events);
 }
 
+const void* prepare_kernel_address() { return reinterpret_cast<const void*>(&prepare_kernel); }
+const void* accumulate_kernel_address() { return reinterpret_cast<const void*>(&accumulate_kernel); }
+
 void launch_prepare(const AccumArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
     prepare_kernel<<<(a.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(a);

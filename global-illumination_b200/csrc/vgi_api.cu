@@ -118,6 +118,15 @@ struct vgi_ctx {
 
     // frame timing
     bool timing = false;
+    // Frame graph: vgi_frame's launches captured once per face set and
+    // sample count, replayed with the prepare and accumulate arguments
+    // updated per frame. Any setter marks it stale.
+    bool use_graph = false;
+    bool graph_dirty = true;
+    uint32_t graph_samples = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaGraphNode_t graph_prepare = nullptr, graph_accumulate = nullptr;
     cudaEvent_t marks[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t traverse_marks[8] = {};
     uint32_t traverse_launches = 0;  // traversal launches of the last timed wavefront frame
@@ -265,6 +274,17 @@ int check_ready(vgi_ctx* c, bool need_faces) {
 
 bool transport_limited(const vgi_ctx* c) { return norm_reach(c->transport.reach) < kMaxPathDistance; }
 
+// Releases the frame graph; the next frames launch directly until one is
+// captured again.
+void drop_graph(vgi_ctx* c) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+    c->graph_prepare = c->graph_accumulate = nullptr;
+    c->graph_dirty = true;
+}
+
 // The dense region grid the timed traversal reads instead of probing the
 // directory: built when the bounding box holds at most 2^24 regions (64 MB).
 cudaError_t upload_grid(vgi_ctx* c, const int32_t* directory, uint64_t slots) {
@@ -290,6 +310,7 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
     const size_t paths = (size_t)a.n_tasks * a.samples;
     const size_t slots = paths * (2 + a.light_count) + (size_t)a.n_tasks * a.light_count;
     if (paths >= (1ull << 30) || slots > 0xffffffffull) return fail(c, VGI_ERR_CAPACITY, "too many paths for the wavefront layout");
+    const void* before[3] = {c->w_state.ptr, c->w_ray.ptr, c->w_status.ptr};
     VGI_CUDA(c, c->w_state.reserve(std::max<size_t>(paths, 1) * 9));
     VGI_CUDA(c, c->w_ray.reserve(std::max<size_t>(slots, 1) * 2));
     VGI_CUDA(c, c->w_hit.reserve(std::max<size_t>(paths, 1) * 6));
@@ -298,6 +319,8 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
     VGI_CUDA(c, c->w_queue1.reserve(std::max<size_t>(slots, 1)));
     VGI_CUDA(c, c->w_scatter.reserve(std::max<size_t>(paths, 1)));
     VGI_CUDA(c, c->w_counters.reserve(4));
+    // A captured frame holds the old buffers' addresses.
+    if (before[0] != c->w_state.ptr || before[1] != c->w_ray.ptr || before[2] != c->w_status.ptr) drop_graph(c);
     WaveBuffers b{};
     b.state = c->w_state.ptr;
     b.ray = c->w_ray.ptr;
@@ -431,6 +454,7 @@ int vgi_destroy(vgi_ctx* c) {
     if (!c) return VGI_ERR_INVALID;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
     c->directory.release(); c->headers.release(); c->cells.release(); c->voxels.release(); c->alloc.release();
     c->pack_error.release(); c->edit_buf.release(); c->zw.release(); c->region_list.release(); c->dedup_table.release();
     c->materials.release(); c->lights.release(); c->emitters.release(); c->node_aux.release();
@@ -466,6 +490,7 @@ int vgi_sync(vgi_ctx* c) {
 }
 
 int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || (n && (!coords || !voxels))) return VGI_ERR_INVALID;
     VGI_CUDA(c, cudaSetDevice(c->device));
     c->keys.assign(n, RegionKey{0, 0, 0});
@@ -517,6 +542,7 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
 
 int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, const uint32_t* headers, uint32_t n_headers,
                       const uint32_t* cells, uint64_t n_cells, const int32_t* bounds6) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || !directory || !headers || !bounds6 || slots == 0 || (slots & (slots - 1))) return VGI_ERR_INVALID;
     if (n_cells && !cells) return VGI_ERR_INVALID;
     // Every index the traversal follows must stay inside the arrays.
@@ -566,6 +592,7 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
 }
 
 int vgi_edit_voxels(vgi_ctx* c, const int32_t* edits, uint32_t n) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || (n && !edits)) return VGI_ERR_INVALID;
     if (!c->geometry || c->keys.empty()) return fail(c, VGI_ERR_STATE, "edits need geometry uploaded as regions");
     VGI_CUDA(c, cudaSetDevice(c->device));
@@ -642,6 +669,7 @@ int vgi_read_geometry(vgi_ctx* c, int32_t* directory, uint32_t* headers, uint32_
 }
 
 int vgi_set_materials(vgi_ctx* c, const float* m) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || !m) return VGI_ERR_INVALID;
     VGI_CUDA(c, cudaSetDevice(c->device));
     c->host_materials.assign(m, m + 256 * 16);
@@ -662,6 +690,7 @@ int vgi_set_materials(vgi_ctx* c, const float* m) {
 }
 
 int vgi_set_lights(vgi_ctx* c, const float* lights, uint32_t n, uint32_t n_directional) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || (n && !lights) || n_directional > n || n > 4096) return VGI_ERR_INVALID;
     VGI_CUDA(c, cudaSetDevice(c->device));
     // An empty light list still uploads one default record (src/gpu.rs:757-759).
@@ -676,6 +705,7 @@ int vgi_set_lights(vgi_ctx* c, const float* lights, uint32_t n, uint32_t n_direc
 }
 
 int vgi_set_environment(vgi_ctx* c, const float* rgb3) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || !rgb3) return VGI_ERR_INVALID;
     c->env[0] = rgb3[0];
     c->env[1] = rgb3[1];
@@ -685,6 +715,7 @@ int vgi_set_environment(vgi_ctx* c, const float* rgb3) {
 }
 
 int vgi_set_emitters(vgi_ctx* c, const uint32_t* words, uint64_t n_words, uint32_t n_faces, float total_weight) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || !words || n_words < 8 || (n_words & 3)) return VGI_ERR_INVALID;
     // Layout check (src/gpu.rs:686-711, src/emission/tree.rs:173-195): face
     // records, then light-tree nodes whose children follow their parent.
@@ -733,6 +764,7 @@ int vgi_build_emitters(vgi_ctx* c) {
 }
 
 int vgi_set_transport(vgi_ctx* c, const vgi_transport* t) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || !t) return VGI_ERR_INVALID;
     vgi_transport n = *t;
     n.reach = norm_reach(n.reach);
@@ -745,6 +777,7 @@ int vgi_set_transport(vgi_ctx* c, const vgi_transport* t) {
 }
 
 int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c || (n && !faces)) return VGI_ERR_INVALID;
     if (n >= (1u << 29)) return fail(c, VGI_ERR_CAPACITY, "slot index exceeds 29 bits");
     VGI_CUDA(c, cudaSetDevice(c->device));
@@ -782,11 +815,92 @@ int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     return VGI_OK;
 }
 
+namespace {
+// Sets a captured kernel node's argument (the kernel takes one AccumArgs).
+cudaError_t set_accum_node(vgi_ctx* c, cudaGraphNode_t node, const AccumArgs& acc) {
+    cudaKernelNodeParams p{};
+    cudaError_t e = cudaGraphKernelNodeGetParams(node, &p);
+    if (e != cudaSuccess) return e;
+    AccumArgs copy = acc;
+    void* args[] = {&copy};
+    p.kernelParams = args;
+    p.extra = nullptr;
+    return cudaGraphExecKernelNodeSetParams(c->graph_exec, node, &p);
+}
+
+// Captures prepare, trace and accumulate of one frame into c->graph_exec.
+int capture_frame(vgi_ctx* c, uint32_t samples, const AccumArgs& acc) {
+    VGI_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    launch_prepare(acc, c->stream);
+    TraceArgs tr = trace_args(c, c->tasks.ptr, c->results.ptr, c->n_slots, samples, true);
+    int rc = run_trace(c, tr, false);
+    launch_accumulate(acc, c->stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc != VGI_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc != VGI_OK ? rc : fail(c, VGI_ERR_CUDA, std::string("frame capture: ") + cudaGetErrorString(e));
+    }
+    c->graph = g;
+    VGI_CUDA(c, cudaGraphInstantiate(&c->graph_exec, g, 0));
+    size_t n = 0;
+    VGI_CUDA(c, cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    VGI_CUDA(c, cudaGraphGetNodes(g, nodes.data(), &n));
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        VGI_CUDA(c, cudaGraphNodeGetType(node, &type));
+        if (type != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams p{};
+        VGI_CUDA(c, cudaGraphKernelNodeGetParams(node, &p));
+        if (p.func == prepare_kernel_address()) c->graph_prepare = node;
+        if (p.func == accumulate_kernel_address()) c->graph_accumulate = node;
+    }
+    if (!c->graph_prepare || !c->graph_accumulate) {
+        drop_graph(c);
+        return fail(c, VGI_ERR_CUDA, "frame capture lost the accumulation kernels");
+    }
+    c->graph_samples = samples;
+    c->graph_dirty = false;
+    return VGI_OK;
+}
+}  // namespace
+
+int vgi_set_graph(vgi_ctx* c, int enable) {
+    if (!c) return VGI_ERR_INVALID;
+    drop_graph(c);
+    c->use_graph = enable != 0;
+    return VGI_OK;
+}
+
 int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
     int rc = check_ready(c, true);
     if (rc != VGI_OK) return rc;
     if (samples == 0) return fail(c, VGI_ERR_INVALID, "samples must be positive");
     AccumArgs acc = accum_args(c, samples, clock_ms);
+    if (c->use_graph && !c->timing && c->layout == VGI_LAYOUT_WAVEFRONT && c->n_slots > 0) {
+        if (c->graph_exec && c->graph_samples == samples && !c->graph_dirty) {
+            VGI_CUDA(c, set_accum_node(c, c->graph_prepare, acc));
+            VGI_CUDA(c, set_accum_node(c, c->graph_accumulate, acc));
+            VGI_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
+            c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
+            if (c->batch_id == 0) c->batch_id = 1;
+            return VGI_OK;
+        }
+        if (!c->graph_dirty && c->graph_samples == samples) {
+            // Buffers are sized (the last frame ran directly): capture this one.
+            rc = capture_frame(c, samples, acc);
+            if (rc != VGI_OK) return rc;
+            VGI_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
+            c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
+            if (c->batch_id == 0) c->batch_id = 1;
+            return VGI_OK;
+        }
+        drop_graph(c);
+        c->graph_dirty = false;
+        c->graph_samples = samples;
+    }
     if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[0], c->stream));
     launch_prepare(acc, c->stream);
     if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[1], c->stream));
@@ -803,6 +917,7 @@ int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
 }
 
 int vgi_set_layout(vgi_ctx* c, uint32_t layout, uint32_t refill_min) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c) return VGI_ERR_INVALID;
     if (layout != VGI_LAYOUT_WAVEFRONT && layout != VGI_LAYOUT_SINGLE_KERNEL) return fail(c, VGI_ERR_INVALID, "unknown layout");
     if (refill_min < 1 || refill_min > 32) return fail(c, VGI_ERR_INVALID, "refill_min outside 1..32");
@@ -812,6 +927,7 @@ int vgi_set_layout(vgi_ctx* c, uint32_t layout, uint32_t refill_min) {
 }
 
 int vgi_set_timing(vgi_ctx* c, int enable) {
+    if (c) drop_graph(c);  // what a frame launches may change
     if (!c) return VGI_ERR_INVALID;
     VGI_CUDA(c, cudaSetDevice(c->device));
     if (enable && !c->marks[0]) {
@@ -864,6 +980,60 @@ int vgi_census(vgi_ctx* c, uint32_t samples, vgi_counters* counters) {
     rc = run_trace(c, tr, true);
     if (rc != VGI_OK) return rc;
     return read_counters(c, counters);
+}
+
+int vgi_autotune(vgi_ctx* c, uint32_t samples, uint32_t* layout_out, uint32_t* refill_out, float* ms_out) {
+    int rc = check_ready(c, true);
+    if (rc != VGI_OK) return rc;
+    if (samples == 0) return fail(c, VGI_ERR_INVALID, "samples must be positive");
+    VGI_CUDA(c, c->scratch_tasks.reserve((size_t)c->n_slots * 2));
+    VGI_CUDA(c, c->scratch_results.reserve((size_t)c->n_slots * 6));
+    VGI_CUDA(c, cudaMemcpyAsync(c->scratch_tasks.ptr, c->tasks.ptr, (size_t)c->n_slots * 32, cudaMemcpyDeviceToDevice, c->stream));
+    AccumArgs acc = accum_args(c, samples, 0);
+    acc.tasks = c->scratch_tasks.ptr;
+    acc.slot_meta = nullptr;  // begin_trace only: no slot changes
+    launch_prepare(acc, c->stream);
+    const TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, c->n_slots, samples, true);
+    const uint32_t layout0 = c->layout, refill0 = c->refill_min;
+    const bool timing0 = c->timing;
+    c->timing = false;
+    struct Candidate { uint32_t layout, refill; };
+    const Candidate candidates[] = {{VGI_LAYOUT_WAVEFRONT, 4}, {VGI_LAYOUT_WAVEFRONT, 6}, {VGI_LAYOUT_WAVEFRONT, 8},
+                                    {VGI_LAYOUT_WAVEFRONT, 12}, {VGI_LAYOUT_WAVEFRONT, 16}, {VGI_LAYOUT_SINGLE_KERNEL, 8}};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    VGI_CUDA(c, cudaEventCreate(&e0));
+    VGI_CUDA(c, cudaEventCreate(&e1));
+    float best = 1e30f;
+    Candidate chosen{layout0, refill0};
+    for (const Candidate& k : candidates) {
+        c->layout = k.layout;
+        c->refill_min = k.refill;
+        float ms = 0.0f;
+        for (int rep = 0; rep < 2 && rc == VGI_OK; ++rep) {  // the first run warms caches and sizes buffers
+            cudaEventRecord(e0, c->stream);
+            rc = run_trace(c, tr, false);
+            cudaEventRecord(e1, c->stream);
+            cudaEventSynchronize(e1);
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (rc != VGI_OK) break;
+        if (ms < best) {
+            best = ms;
+            chosen = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->timing = timing0;
+    c->layout = rc == VGI_OK ? chosen.layout : layout0;
+    c->refill_min = rc == VGI_OK ? chosen.refill : refill0;
+    drop_graph(c);
+    if (rc != VGI_OK) return rc;
+    VGI_CUDA(c, cudaGetLastError());
+    if (layout_out) *layout_out = chosen.layout;
+    if (refill_out) *refill_out = chosen.refill;
+    if (ms_out) *ms_out = best;
+    return VGI_OK;
 }
 
 int vgi_trace_tasks(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samples, uint32_t* results, vgi_counters* counters) {

@@ -99,6 +99,9 @@ uint32_t wave_traverse_blocks_per_sm();
 void launch_reference64(const TraceArgs& a, const double* cdf, const int4* emitters, uint32_t n_emitters, double total,
                         const uint4* tasks, uint32_t n_tasks, uint32_t samples, uint64_t seed, double* sum, double* second,
                         uint32_t* known, cudaStream_t s);
+// The per-frame kernels whose arguments a captured frame graph updates.
+const void* prepare_kernel_address();
+const void* accumulate_kernel_address();
 void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s);
 void launch_measure_edits(const uint4* state, const uint4* slot_meta, const uint4* index, const float2* material_light,
                           const uint4* measures, uint32_t n_entries, uint32_t n_positions, uint32_t* measure_max, uint4* events,

@@ -152,6 +152,8 @@ _SIGNATURES = {
     "vgi_set_faces": (_INT, [_P, _P, _U32]),
     "vgi_frame": (_INT, [_P, _U32, _U32]),
     "vgi_set_timing": (_INT, [_P, _INT]),
+    "vgi_set_graph": (_INT, [_P, _INT]),
+    "vgi_autotune": (_INT, [_P, _U32, _P, _P, _P]),
     "vgi_set_layout": (_INT, [_P, _U32, _U32]),
     "vgi_pack_regions_static": (_INT, [_P, _U32, _P, _P, _U64, _P, _P]),
     "vgi_frame_times": (_INT, [_P, _P]),
@@ -399,6 +401,16 @@ class GpuTracer:
         f = _c(faces, np.int32).reshape(-1, 5)
         self._check(self._lib.vgi_set_faces(self._h, _ptr(f), f.shape[0]))
         self.n_slots = f.shape[0]
+
+    def autotune(self, samples: int) -> dict:
+        """Picks the fastest layout / refill threshold for the current faces."""
+        layout, refill, ms = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_float()
+        self._check(self._lib.vgi_autotune(self._h, samples, ctypes.byref(layout), ctypes.byref(refill), ctypes.byref(ms)))
+        return {"layout": int(layout.value), "refill_min": int(refill.value), "trace_ms": float(ms.value)}
+
+    def set_graph(self, enable: bool) -> None:
+        """Replay frames from a captured CUDA graph (see include/vgi.h)."""
+        self._check(self._lib.vgi_set_graph(self._h, int(enable)))
 
     def frame(self, samples: int, clock_ms: int = 0) -> None:
         self._check(self._lib.vgi_frame(self._h, samples, clock_ms))

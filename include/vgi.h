@@ -149,6 +149,12 @@ int vgi_frame(vgi_ctx* ctx, uint32_t samples, uint32_t clock_ms);
 #define VGI_LAYOUT_WAVEFRONT 0u
 #define VGI_LAYOUT_SINGLE_KERNEL 1u
 int vgi_set_layout(vgi_ctx* ctx, uint32_t layout, uint32_t refill_min);
+/* Autotuner (no counterpart in the reference): times a trace of the current
+ * face set at `samples` (tasks as the next frame would trace them, results
+ * discarded, no slot changes) for the wavefront layout with refill_min
+ * 4, 6, 8, 12 and 16 and for the single-kernel layout, keeps the fastest as
+ * the context's layout and reports it. Synchronous. */
+int vgi_autotune(vgi_ctx* ctx, uint32_t samples, uint32_t* layout, uint32_t* refill_min, float* trace_ms);
 /* Device timing of vgi_frame (the reference's timestamp query pairs,
  * src/gpu.rs:488-500): with timing enabled each frame records CUDA events on
  * the context's stream around prepare, trace and accumulate, and around each
@@ -156,6 +162,14 @@ int vgi_set_layout(vgi_ctx* ctx, uint32_t layout, uint32_t refill_min);
  * frame's prepare, trace and accumulate durations and the summed traversal
  * time (0 for the single-kernel layout), in ms; it synchronises the stream. */
 int vgi_set_timing(vgi_ctx* ctx, int enable);
+/* Frame graphs (no counterpart in the reference, which records wgpu command
+ * buffers per batch): with graphs enabled and timing off, the wavefront
+ * layout's frame (prepare, the traversal and stage kernels, accumulate) is
+ * captured into a CUDA graph on the second frame after any change and
+ * replayed afterwards, with each frame's clock and batch id patched into the
+ * captured prepare and accumulate nodes. Every setter, and any growth of
+ * the trace buffers, drops the graph. Results equal direct launches. */
+int vgi_set_graph(vgi_ctx* ctx, int enable);
 int vgi_frame_times(vgi_ctx* ctx, float* ms4);
 /* The same frame through host buffers (submit_compact + complete_readback):
  * 8-word tasks in (one per slot, in slot order; their sequence words are

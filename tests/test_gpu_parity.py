@@ -171,6 +171,41 @@ def test_stone_room_frames_match_oracle(gpu, layout):
     assert_words_equal(gpu.read_slot_meta(), ref.meta, "slot metadata")
 
 
+def test_autotuned_layout_keeps_results_and_state(gpu):
+    # The autotuner's trial traces change no slot; frames after it still
+    # match the oracle in whatever layout it chose.
+    case = terrain_case(bounces=2)
+    ref = run_frames(gpu, case, 3, 8)
+    state = gpu.read_state()
+    choice = gpu.autotune(8)
+    assert choice["layout"] in (0, 1) and 1 <= choice["refill_min"] <= 32 and choice["trace_ms"] > 0
+    assert_words_equal(gpu.read_state(), state, "state after autotune")
+    for f in range(3, 5):
+        gpu.frame(8, clock_ms=16 * f)
+        ref.frame(8, clock_ms=16 * f)
+    assert_words_equal(gpu.read_results(), ref.results, "frames after autotune")
+    gpu.set_layout(vgi.GpuTracer.WAVEFRONT)
+
+
+def test_graph_replayed_frames_match_oracle(gpu):
+    # Frames replayed from a captured graph, across a transport change that
+    # drops and recaptures it.
+    case = terrain_case(bounces=2)
+    gpu.set_graph(True)
+    try:
+        ref = run_frames(gpu, case, 4, 8)
+        case.transport.history_limit = 32
+        gpu.set_transport(case.transport)
+        ref.transport = case.transport
+        for f in range(4, 8):
+            gpu.frame(8, clock_ms=16 * f)
+            ref.frame(8, clock_ms=16 * f)
+        assert_words_equal(gpu.read_results(), ref.results, "graph frame results")
+        assert_words_equal(gpu.read_state(), ref.state, "graph frame state")
+    finally:
+        gpu.set_graph(False)
+
+
 @pytest.mark.parametrize("layout", LAYOUTS)
 def test_terrain_frames_with_cache_match_oracle(gpu, layout):
     case = terrain_case(bounces=2)
