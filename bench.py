@@ -260,6 +260,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["vgi", "reference"], default="vgi")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default layout (for profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -293,7 +294,7 @@ def main():
     g.build_emitters()
     g.set_transport(transport)
     g.set_faces(faces)
-    tuned = g.autotune(SPP)
+    tuned = None if args.no_autotune else g.autotune(SPP)
     g.set_timing(True)
     n = faces.shape[0]
     stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
