@@ -109,6 +109,10 @@ struct vgi_ctx {
     // view tier: receivers, paths, continuations, estimates, owner queue, events
     DevBuf<uint4> v_receivers, v_paths, v_conts, v_estimates, v_events, v_scratch;
     DevBuf<uint32_t> v_queue;
+    // MLP radiance cache: FP32 master weights, their packed BF16 image
+    DevBuf<float> mlp_master;
+    DevBuf<uint8_t> mlp_image;
+    DevBuf<uint32_t> mlp_error;
     uint32_t n_view = 0;
     DevBuf<uint4> events;
     uint32_t n_events = 0;
@@ -463,6 +467,7 @@ int vgi_destroy(vgi_ctx* c) {
     c->material_light.release(); c->measures.release(); c->measure_max.release();
     c->v_receivers.release(); c->v_paths.release(); c->v_conts.release(); c->v_estimates.release(); c->v_events.release();
     c->v_scratch.release(); c->v_queue.release();
+    c->mlp_master.release(); c->mlp_image.release(); c->mlp_error.release();
     c->counters.release();
     c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
     c->w_queue0.release(); c->w_queue1.release(); c->w_scatter.release(); c->w_counters.release();
@@ -1276,6 +1281,49 @@ int vgi_reference_fp64(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t s
         }
         if (known) known[i] = cnt[i];
     }
+    return VGI_OK;
+}
+
+int vgi_mlp_set_weights(vgi_ctx* c, const float* master, uint32_t count) {
+    if (!c || !master) return VGI_ERR_INVALID;
+    if (count != mlp_weight_count()) return fail(c, VGI_ERR_INVALID, "MLP weight count must be 19456");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, c->mlp_master.reserve(count));
+    VGI_CUDA(c, c->mlp_image.reserve(mlp_image_bytes()));
+    VGI_CUDA(c, c->mlp_error.reserve(1));
+    VGI_CUDA(c, cudaMemcpyAsync(c->mlp_master.ptr, master, (size_t)count * 4, cudaMemcpyHostToDevice, c->stream));
+    launch_mlp_pack(c->mlp_master.ptr, c->mlp_image.ptr, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_mlp_get_weights(vgi_ctx* c, float* master, uint32_t count) {
+    if (!c || !master || count != mlp_weight_count() || !c->mlp_master.ptr) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaMemcpyAsync(master, c->mlp_master.ptr, (size_t)count * 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_mlp_forward(vgi_ctx* c, const float* features, uint32_t n, float* out4) {
+    if (!c || (n && (!features || !out4))) return VGI_ERR_INVALID;
+    if (!c->mlp_image.ptr) return fail(c, VGI_ERR_STATE, "MLP weights are not set");
+    if (n == 0) return VGI_OK;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    DevBuf<float> in;
+    DevBuf<float4> out;
+    VGI_CUDA(c, in.reserve((size_t)n * 96));
+    VGI_CUDA(c, out.reserve(n));
+    VGI_CUDA(c, cudaMemcpyAsync(in.ptr, features, (size_t)n * 96 * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 4, c->stream));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    VGI_CUDA(c, launch_mlp_forward(in.ptr, c->mlp_image.ptr, out.ptr, n, c->mlp_error.ptr, (uint32_t)sms * 3u, c->stream));
+    uint32_t err = 0;
+    VGI_CUDA(c, cudaMemcpyAsync(&err, c->mlp_error.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(out4, out.ptr, (size_t)n * 16, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err) return fail(c, VGI_ERR_CUDA, "MLP forward: a tensor-core wait ran out");
     return VGI_OK;
 }
 

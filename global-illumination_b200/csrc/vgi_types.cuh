@@ -102,6 +102,12 @@ void launch_reference64(const TraceArgs& a, const double* cdf, const int4* emitt
 // The per-frame kernels whose arguments a captured frame graph updates.
 const void* prepare_kernel_address();
 const void* accumulate_kernel_address();
+// MLP radiance cache (vgi_mlp.cu).
+void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s);
+cudaError_t launch_mlp_forward(const float* features, const uint8_t* image, float4* outputs, uint32_t n, uint32_t* error, uint32_t ctas,
+                               cudaStream_t s);
+uint32_t mlp_weight_count();
+uint32_t mlp_image_bytes();
 void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s);
 void launch_measure_edits(const uint4* state, const uint4* slot_meta, const uint4* index, const float2* material_light,
                           const uint4* measures, uint32_t n_entries, uint32_t n_positions, uint32_t* measure_max, uint4* events,

@@ -168,6 +168,9 @@ _SIGNATURES = {
     "vgi_view_read": (_INT, [_P, _P, _P, _P, _P, _P]),
     "vgi_view_trace_paths": (_INT, [_P, _U32, _P]),
     "vgi_reference_fp64": (_INT, [_P, _P, _U32, _U32, _U64, _P, _P, _P]),
+    "vgi_mlp_set_weights": (_INT, [_P, _P, _U32]),
+    "vgi_mlp_get_weights": (_INT, [_P, _P, _U32]),
+    "vgi_mlp_forward": (_INT, [_P, _P, _U32, _P]),
     "vgi_read_results": (_INT, [_P, _U32, _U32, _P]),
     "vgi_read_state": (_INT, [_P, _U32, _U32, _P]),
     "vgi_write_state": (_INT, [_P, _U32, _U32, _P]),
@@ -493,6 +496,24 @@ class GpuTracer:
         out = np.zeros((n * samples, 32), np.uint32)
         self._check(self._lib.vgi_view_trace_paths(self._h, samples, _ptr(out)))
         return out
+
+    MLP_WEIGHTS = 19456
+    MLP_LAYERS = [(96, 64), (64, 64), (64, 64), (64, 64), (64, 16)]
+
+    def mlp_set_weights(self, master: np.ndarray) -> None:
+        w = _c(master, np.float32).reshape(-1)
+        self._check(self._lib.vgi_mlp_set_weights(self._h, _ptr(w), w.size))
+
+    def mlp_get_weights(self) -> np.ndarray:
+        w = np.zeros(self.MLP_WEIGHTS, np.float32)
+        self._check(self._lib.vgi_mlp_get_weights(self._h, _ptr(w), w.size))
+        return w
+
+    def mlp_forward(self, features: np.ndarray) -> np.ndarray:
+        f = _c(features, np.float32).reshape(-1, 96)
+        out = np.zeros((f.shape[0], 4), np.float32)
+        self._check(self._lib.vgi_mlp_forward(self._h, _ptr(f), f.shape[0], _ptr(out)))
+        return out[:, :3]
 
     def reference_fp64(self, tasks: np.ndarray, samples: int, seed: int = 1):
         """FP64 converged reference per FaceTask: (mean rgb, mean square rgb, known)."""

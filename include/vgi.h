@@ -246,6 +246,20 @@ int vgi_view_trace_paths(vgi_ctx* ctx, uint32_t samples, uint32_t* paths32);
 int vgi_reference_fp64(vgi_ctx* ctx, const uint32_t* tasks, uint32_t n, uint32_t samples, uint64_t seed, double* mean3, double* second3,
                        uint32_t* known);
 
+/* ---- MLP radiance cache ------------------------------------------------------
+ * No counterpart in the reference: a small network that predicts a face's
+ * incident radiance from its position, normal and albedo, run on the
+ * tcgen05 tensor cores. 96 inputs (81 features: 12 sine/cosine frequencies
+ * per position axis, the normal as one-hot, the albedo; zero padded), four
+ * hidden layers of 64 with ReLU, 16 outputs of which the first 3 pass
+ * through exp. Weights are FP32 masters, layer after layer, each [in][out]
+ * row-major (19,456 floats); the kernels use their BF16 rounding and
+ * accumulate in FP32. */
+int vgi_mlp_set_weights(vgi_ctx* ctx, const float* master, uint32_t count);
+int vgi_mlp_get_weights(vgi_ctx* ctx, float* master, uint32_t count);
+/* Forward pass over n feature rows (96 floats each): out4 = (rgb, 0) per row. */
+int vgi_mlp_forward(vgi_ctx* ctx, const float* features, uint32_t n, float* out4);
+
 /* ---- read-back: bounded snapshots (complete_readback, src/gpu.rs:1024-1170) --- */
 int vgi_read_results(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words24);
 int vgi_read_state(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words36);
