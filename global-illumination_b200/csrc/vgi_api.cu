@@ -113,6 +113,10 @@ struct vgi_ctx {
     DevBuf<float> mlp_master;
     DevBuf<uint8_t> mlp_image;
     DevBuf<uint32_t> mlp_error;
+    DevBuf<uint8_t> mlp_image_b;              // W (rows = inputs): B operand of the backward pass
+    DevBuf<float> mlp_adam;                   // Adam first and second moments, 2 x 19456
+    DevBuf<float> mlp_grads;                  // 19456 gradients + the loss
+    uint32_t mlp_step = 0;
     uint32_t n_view = 0;
     DevBuf<uint4> events;
     uint32_t n_events = 0;
@@ -468,6 +472,7 @@ int vgi_destroy(vgi_ctx* c) {
     c->v_receivers.release(); c->v_paths.release(); c->v_conts.release(); c->v_estimates.release(); c->v_events.release();
     c->v_scratch.release(); c->v_queue.release();
     c->mlp_master.release(); c->mlp_image.release(); c->mlp_error.release();
+    c->mlp_image_b.release(); c->mlp_adam.release(); c->mlp_grads.release();
     c->counters.release();
     c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
     c->w_queue0.release(); c->w_queue1.release(); c->w_scatter.release(); c->w_counters.release();
@@ -1291,8 +1296,14 @@ int vgi_mlp_set_weights(vgi_ctx* c, const float* master, uint32_t count) {
     VGI_CUDA(c, c->mlp_master.reserve(count));
     VGI_CUDA(c, c->mlp_image.reserve(mlp_image_bytes()));
     VGI_CUDA(c, c->mlp_error.reserve(1));
+    VGI_CUDA(c, c->mlp_image_b.reserve(mlp_image_bytes()));
+    VGI_CUDA(c, c->mlp_adam.reserve((size_t)count * 2));
+    VGI_CUDA(c, c->mlp_grads.reserve((size_t)count + 1));
     VGI_CUDA(c, cudaMemcpyAsync(c->mlp_master.ptr, master, (size_t)count * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_adam.ptr, 0, (size_t)count * 8, c->stream));
+    c->mlp_step = 0;
     launch_mlp_pack(c->mlp_master.ptr, c->mlp_image.ptr, c->stream);
+    launch_mlp_pack_backward(c->mlp_master.ptr, c->mlp_image_b.ptr, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
@@ -1325,6 +1336,72 @@ int vgi_mlp_forward(vgi_ctx* c, const float* features, uint32_t n, float* out4) 
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     if (err) return fail(c, VGI_ERR_CUDA, "MLP forward: a tensor-core wait ran out");
     return VGI_OK;
+}
+
+// Gradients of the relative-luminance loss over one batch already on the
+// device, into mlp_grads (19456 gradients, then the loss).
+static int mlp_batch_gradients(vgi_ctx* c, const float* features, const float4* targets, uint32_t n) {
+    const uint32_t count = mlp_weight_count();
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_grads.ptr, 0, (size_t)(count + 1) * 4, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 4, c->stream));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    VGI_CUDA(c, launch_mlp_train(features, targets, n, c->mlp_image.ptr, c->mlp_image_b.ptr, c->mlp_grads.ptr, c->mlp_grads.ptr + count,
+                                 c->mlp_error.ptr, (uint32_t)sms, c->stream));
+    return VGI_OK;
+}
+
+static int mlp_upload_batch(vgi_ctx* c, const float* features, const float* targets4, uint32_t n, DevBuf<float>& in, DevBuf<float4>& y) {
+    VGI_CUDA(c, in.reserve((size_t)n * 96));
+    VGI_CUDA(c, y.reserve(n));
+    VGI_CUDA(c, cudaMemcpyAsync(in.ptr, features, (size_t)n * 96 * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(y.ptr, targets4, (size_t)n * 16, cudaMemcpyHostToDevice, c->stream));
+    return VGI_OK;
+}
+
+static int mlp_read_status(vgi_ctx* c, float* loss) {
+    uint32_t err = 0;
+    VGI_CUDA(c, cudaMemcpyAsync(&err, c->mlp_error.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (loss) VGI_CUDA(c, cudaMemcpyAsync(loss, c->mlp_grads.ptr + mlp_weight_count(), 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err) return fail(c, VGI_ERR_CUDA, "MLP training: a tensor-core wait ran out");
+    return VGI_OK;
+}
+
+int vgi_mlp_gradients(vgi_ctx* c, const float* features, const float* targets4, uint32_t n, float* grads, float* loss) {
+    if (!c || !n || !features || !targets4 || !grads) return VGI_ERR_INVALID;
+    if (!c->mlp_image.ptr) return fail(c, VGI_ERR_STATE, "MLP weights are not set");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    DevBuf<float> in;
+    DevBuf<float4> y;
+    if (int e = mlp_upload_batch(c, features, targets4, n, in, y)) return e;
+    if (int e = mlp_batch_gradients(c, in.ptr, y.ptr, n)) return e;
+    VGI_CUDA(c, cudaMemcpyAsync(grads, c->mlp_grads.ptr, (size_t)mlp_weight_count() * 4, cudaMemcpyDeviceToHost, c->stream));
+    return mlp_read_status(c, loss);
+}
+
+// One Adam step over a device-resident batch; the images are repacked.
+static int mlp_train_step(vgi_ctx* c, const float* features, const float4* targets, uint32_t n, float lr) {
+    if (int e = mlp_batch_gradients(c, features, targets, n)) return e;
+    const uint32_t count = mlp_weight_count();
+    c->mlp_step += 1;
+    launch_mlp_adam(c->mlp_master.ptr, c->mlp_adam.ptr, c->mlp_adam.ptr + count, c->mlp_grads.ptr, lr, 0.9f, 0.99f, 1e-8f, c->mlp_step,
+                    c->stream);
+    launch_mlp_pack(c->mlp_master.ptr, c->mlp_image.ptr, c->stream);
+    launch_mlp_pack_backward(c->mlp_master.ptr, c->mlp_image_b.ptr, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    return VGI_OK;
+}
+
+int vgi_mlp_train(vgi_ctx* c, const float* features, const float* targets4, uint32_t n, float lr, float* loss) {
+    if (!c || !n || !features || !targets4 || !(lr > 0.0f)) return VGI_ERR_INVALID;
+    if (!c->mlp_image.ptr) return fail(c, VGI_ERR_STATE, "MLP weights are not set");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    DevBuf<float> in;
+    DevBuf<float4> y;
+    if (int e = mlp_upload_batch(c, features, targets4, n, in, y)) return e;
+    if (int e = mlp_train_step(c, in.ptr, y.ptr, n, lr)) return e;
+    return mlp_read_status(c, loss);
 }
 
 int vgi_read_events(vgi_ctx* c, uint32_t* words, uint64_t n_words) {

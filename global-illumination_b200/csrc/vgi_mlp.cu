@@ -231,7 +231,248 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const float* features
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns));
 }
 
+// ---- training ------------------------------------------------------------
+// One fused kernel per batch: every CTA (one per SM, 512 TMEM columns) runs
+// its 128-sample tiles forward, then backward, and accumulates the weight
+// gradients of all layers in TMEM across its tiles:
+//     dW_l += h_l^T dz_l        (M = 128 >= in_l, K = 128 samples, N = out_l)
+//     dh_l  = dz_l W_l^T        (M = 128 samples, K = out_l, N = in_l)
+//     dz_{l-1} = dh_l * (h_l > 0)
+// h_l (the input of layer l) is kept transposed (features x samples) for the
+// dW products; dz_l is kept both as the next A operand (samples x out_l) and
+// transposed (out_l x samples). The hidden h_l^T tiles hold 64 feature rows;
+// an M = 128 product also reads the 64 rows after them (the next buffer),
+// which only feed accumulator rows 64-127, never read out (the last hidden
+// tile's extra rows are the dz^T tile, the input tile's are h_1^T). The loss is the
+// relative luminance MSE sum_c (p_c - y_c)^2 / (lum(p)^2 + 0.01) / B with
+// lum(p) held constant, p = exp(z). Gradients are summed into `grads` (same
+// order as the FP32 masters) with one atomic per weight per CTA.
+constexpr int kHT0 = kIn * kRows * 2;              // 24576
+constexpr int kHT = kHidden * kRows * 2;           // 16384
+constexpr uint32_t kWF = 0, kWB = kImageBytes, kAT = 2 * kImageBytes, kH0 = kAT + kABytes;
+constexpr uint32_t kH1 = kH0 + kHT0, kDZ = kH1 + 4 * kHT, kBarT = kDZ + kHT;
+constexpr int kTrainSmem = kBarT + 64;             // 208,960 bytes
+constexpr int kTrainColumns = 512;
+__host__ __device__ constexpr uint32_t grad_column(int l) { return 64u + 64u * (uint32_t)l; }
+__host__ __device__ constexpr uint32_t ht_offset(int l) { return l == 0 ? kH0 : kH1 + (uint32_t)(l - 1) * kHT; }
+
+// FP32 master [in][out] -> BF16 image with rows = in, K = out: the B
+// operand of dh = dz W^T.
+__global__ void pack_backward_kernel(const float* master, uint8_t* image) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kWeights) return;
+    int l = 0;
+    while (l + 1 < kLayers && i >= weight_offset(l + 1)) ++l;
+    const int local = i - weight_offset(l);
+    const int k = local / out_dim(l), n = local % out_dim(l);
+    *reinterpret_cast<__nv_bfloat16*>(image + weight_offset(l) * 2 + core_offset(k, n, out_dim(l))) = __float2bfloat16_rn(master[i]);
+}
+
+__device__ __forceinline__ void store_t(uint8_t* smem, uint32_t base, uint32_t row, uint32_t col, float v) {
+    *reinterpret_cast<__nv_bfloat16*>(smem + base + core_offset(row, col, kRows)) = __float2bfloat16_rn(v);
+}
+
+__global__ void __launch_bounds__(kThreads) train_kernel(const float* features, const float4* targets, uint32_t batch,
+                                                         const uint8_t* image_f, const uint8_t* image_b, float* grads, float* loss,
+                                                         uint32_t* error) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kBarT);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kBarT + 8);
+    uint32_t* abort_flag = reinterpret_cast<uint32_t*>(smem + kBarT + 12);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    for (uint32_t i = tid; i < kImageBytes / 16; i += kThreads) {
+        reinterpret_cast<uint4*>(smem + kWF)[i] = reinterpret_cast<const uint4*>(image_f)[i];
+        reinterpret_cast<uint4*>(smem + kWB)[i] = reinterpret_cast<const uint4*>(image_b)[i];
+    }
+    // Zero the transposed tiles and the pad once: rows past a tile's real
+    // features are read by the M = 128 products.
+    for (uint32_t i = tid; i < (kBarT - kH0) / 16; i += kThreads) reinterpret_cast<uint4*>(smem + kH0)[i] = make_uint4(0, 0, 0, 0);
+    if (tid == 0) {
+        *abort_flag = 0u;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1u));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTrainColumns));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_base = tmem + ((warp * 32u) << 16);
+    const uint32_t bar_addr = smem_u32(bar), s0 = smem_u32(smem);
+    uint32_t phase = 0;
+    const uint32_t tiles = (batch + kRows - 1) / kRows;
+    bool first = true, ok = true;
+    float loss_sum = 0.0f;
+
+    // Issues nothing itself: every thread calls it; thread 0 has issued the
+    // MMAs and the commit. Returns false when the wait ran out.
+    auto finish = [&]() -> bool {
+        if (!bar_wait(bar_addr, phase)) {
+            atomicOr(abort_flag, 1u);
+            atomicOr(error, 1u);
+        }
+        phase ^= 1u;
+        __syncthreads();
+        if (*abort_flag) return false;
+        fence_after();
+        return true;
+    };
+    auto publish = [&]() {
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+    };
+
+    for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        const uint32_t row = t * kRows + tid;
+        const bool valid = row < batch;
+        // Input: A (K = 96) and h_0^T.
+        for (uint32_t c = 0; c < kIn / 8; ++c) {
+            float v[8];
+            for (int j = 0; j < 8; ++j) v[j] = valid ? features[(size_t)row * kIn + c * 8 + j] : 0.0f;
+            store8(smem + kAT, tid, c, kIn, v);
+            for (int j = 0; j < 8; ++j) store_t(smem, kH0, c * 8 + j, tid, v[j]);
+        }
+        // Forward.
+        float z[16];
+        for (int l = 0; l < kLayers && ok; ++l) {
+            const uint32_t K = in_dim(l), N = out_dim(l);
+            publish();
+            if (tid == 0) {
+                fence_after();
+                for (uint32_t kk = 0; kk < K / 16u; ++kk)
+                    mma_bf16(tmem, matrix_desc(s0 + kAT + kk * 256u, 128u, (K / 8u) * 128u),
+                             matrix_desc(s0 + kWF + weight_offset(l) * 2 + kk * 256u, 128u, (K / 8u) * 128u), instr_desc(N), kk > 0 ? 1u : 0u);
+                mma_commit(bar_addr);
+            }
+            if (!(ok = finish())) break;
+            if (l + 1 < kLayers) {
+                for (uint32_t c0 = 0; c0 < N; c0 += 16u) {
+                    float v[16];
+                    tmem_ld16(lane_base + c0, v);
+                    tmem_wait_ld();
+                    for (int j = 0; j < 16; ++j) v[j] = v[j] > 0.0f ? v[j] : 0.0f;
+                    store8(smem + kAT, tid, c0 / 8u, N, v);
+                    store8(smem + kAT, tid, c0 / 8u + 1u, N, v + 8);
+                    for (int j = 0; j < 16; ++j) store_t(smem, ht_offset(l + 1), c0 + j, tid, v[j]);
+                }
+            } else {
+                tmem_ld16(lane_base, z);
+                tmem_wait_ld();
+            }
+        }
+        if (!ok) break;
+        // Output gradient.
+        float dz[64];
+        for (int j = 0; j < 64; ++j) dz[j] = 0.0f;
+        if (valid) {
+            const float4 y = targets[row];
+            const float p0 = expf(z[0]), p1 = expf(z[1]), p2 = expf(z[2]);
+            const float lum = 0.2126f * p0 + 0.7152f * p1 + 0.0722f * p2;
+            const float inv = 1.0f / ((lum * lum + 0.01f) * (float)batch);
+            const float e0 = p0 - y.x, e1 = p1 - y.y, e2 = p2 - y.z;
+            loss_sum += (e0 * e0 + e1 * e1 + e2 * e2) * inv;
+            dz[0] = 2.0f * e0 * inv * p0;
+            dz[1] = 2.0f * e1 * inv * p1;
+            dz[2] = 2.0f * e2 * inv * p2;
+        }
+        // Backward.
+        for (int l = kLayers - 1; l >= 0 && ok; --l) {
+            const uint32_t N = out_dim(l), Kin = in_dim(l);
+            for (uint32_t c = 0; c < N / 8u; ++c) store8(smem + kAT, tid, c, N, dz + c * 8);
+            for (uint32_t o = 0; o < N; ++o) store_t(smem, kDZ, o, tid, dz[o]);
+            publish();
+            if (tid == 0) {
+                fence_after();
+                // dW_l += h_l^T dz_l
+                for (uint32_t kk = 0; kk < kRows / 16u; ++kk)
+                    mma_bf16(tmem + grad_column(l), matrix_desc(s0 + ht_offset(l) + kk * 256u, 128u, (kRows / 8u) * 128u),
+                             matrix_desc(s0 + kDZ + kk * 256u, 128u, (kRows / 8u) * 128u), instr_desc(N), (first && kk == 0) ? 0u : 1u);
+                // dh_l = dz_l W_l^T
+                if (l > 0)
+                    for (uint32_t kk = 0; kk < N / 16u; ++kk)
+                        mma_bf16(tmem, matrix_desc(s0 + kAT + kk * 256u, 128u, (N / 8u) * 128u),
+                                 matrix_desc(s0 + kWB + weight_offset(l) * 2 + kk * 256u, 128u, (N / 8u) * 128u), instr_desc(Kin),
+                                 kk > 0 ? 1u : 0u);
+                mma_commit(bar_addr);
+            }
+            if (!(ok = finish())) break;
+            if (l > 0) {
+                for (uint32_t c0 = 0; c0 < Kin; c0 += 16u) {
+                    float v[16];
+                    tmem_ld16(lane_base + c0, v);
+                    tmem_wait_ld();
+                    for (int j = 0; j < 16; ++j) {
+                        const __nv_bfloat16 h = *reinterpret_cast<const __nv_bfloat16*>(smem + ht_offset(l) + core_offset(c0 + j, tid, kRows));
+                        dz[c0 + j] = (valid && __bfloat162float(h) > 0.0f) ? v[j] : 0.0f;
+                    }
+                }
+                for (uint32_t j = Kin; j < 64; ++j) dz[j] = 0.0f;
+            }
+        }
+        first = false;
+    }
+    // Gradients: row `tid` of each layer's accumulator is input feature tid.
+    if (ok && !first) {
+        fence_before();
+        __syncthreads();
+        fence_after();
+        for (int l = 0; l < kLayers; ++l) {
+            const uint32_t N = out_dim(l);
+            for (uint32_t c0 = 0; c0 < N; c0 += 16u) {
+                float v[16];
+                tmem_ld16(lane_base + grad_column(l) + c0, v);
+                tmem_wait_ld();
+                if (tid < (uint32_t)in_dim(l))
+                    for (int j = 0; j < 16; ++j) atomicAdd(grads + weight_offset(l) + tid * N + c0 + j, v[j]);
+            }
+        }
+    }
+    if (ok) atomicAdd(loss, loss_sum);
+    fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTrainColumns));
+}
+
+// Adam (Kingma & Ba) on the FP32 masters, step `step` (1-based), then the
+// two BF16 images are repacked by the caller.
+__global__ void adam_kernel(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps,
+                            uint32_t step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kWeights) return;
+    const float g = grads[i];
+    const float mi = beta1 * m[i] + (1.0f - beta1) * g;
+    const float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    const float mh = mi / (1.0f - powf(beta1, (float)step)), vh = vi / (1.0f - powf(beta2, (float)step));
+    master[i] -= lr * mh / (sqrtf(vh) + eps);
+}
+
 }  // namespace mlp
+
+void launch_mlp_pack_backward(const float* master, uint8_t* image, cudaStream_t s) {
+    mlp::pack_backward_kernel<<<(mlp::kWeights + 255) / 256, 256, 0, s>>>(master, image);
+}
+
+cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
+                             float* grads, float* loss, uint32_t* error, uint32_t ctas, cudaStream_t s) {
+    if (batch == 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(mlp::train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
+    if (e != cudaSuccess) return e;
+    const uint32_t tiles = (batch + mlp::kRows - 1) / mlp::kRows;
+    mlp::train_kernel<<<tiles < ctas ? tiles : ctas, mlp::kThreads, mlp::kTrainSmem, s>>>(features, targets, batch, image_f, image_b, grads,
+                                                                                           loss, error);
+    return cudaGetLastError();
+}
+
+void launch_mlp_adam(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps, uint32_t step,
+                     cudaStream_t s) {
+    mlp::adam_kernel<<<(mlp::kWeights + 255) / 256, 256, 0, s>>>(master, m, v, grads, lr, beta1, beta2, eps, step);
+}
 
 void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s) {
     mlp::pack_kernel<<<(mlp::kWeights + 255) / 256, 256, 0, s>>>(master, image);

@@ -106,6 +106,11 @@ const void* accumulate_kernel_address();
 void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s);
 cudaError_t launch_mlp_forward(const float* features, const uint8_t* image, float4* outputs, uint32_t n, uint32_t* error, uint32_t ctas,
                                cudaStream_t s);
+void launch_mlp_pack_backward(const float* master, uint8_t* image, cudaStream_t s);
+cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
+                             float* grads, float* loss, uint32_t* error, uint32_t ctas, cudaStream_t s);
+void launch_mlp_adam(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps, uint32_t step,
+                     cudaStream_t s);
 uint32_t mlp_weight_count();
 uint32_t mlp_image_bytes();
 void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s);

@@ -171,6 +171,8 @@ _SIGNATURES = {
     "vgi_mlp_set_weights": (_INT, [_P, _P, _U32]),
     "vgi_mlp_get_weights": (_INT, [_P, _P, _U32]),
     "vgi_mlp_forward": (_INT, [_P, _P, _U32, _P]),
+    "vgi_mlp_gradients": (_INT, [_P, _P, _P, _U32, _P, _P]),
+    "vgi_mlp_train": (_INT, [_P, _P, _P, _U32, ctypes.c_float, _P]),
     "vgi_read_results": (_INT, [_P, _U32, _U32, _P]),
     "vgi_read_state": (_INT, [_P, _U32, _U32, _P]),
     "vgi_write_state": (_INT, [_P, _U32, _U32, _P]),
@@ -514,6 +516,28 @@ class GpuTracer:
         out = np.zeros((f.shape[0], 4), np.float32)
         self._check(self._lib.vgi_mlp_forward(self._h, _ptr(f), f.shape[0], _ptr(out)))
         return out[:, :3]
+
+    @staticmethod
+    def _mlp_batch(features, targets):
+        f = _c(features, np.float32).reshape(-1, 96)
+        y = np.zeros((f.shape[0], 4), np.float32)
+        y[:, :3] = np.asarray(targets, np.float32).reshape(-1, 3)
+        return f, y
+
+    def mlp_gradients(self, features: np.ndarray, targets: np.ndarray):
+        """(dLoss/dW in master order, loss) of the relative-luminance loss."""
+        f, y = self._mlp_batch(features, targets)
+        g = np.zeros(self.MLP_WEIGHTS, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(self._lib.vgi_mlp_gradients(self._h, _ptr(f), _ptr(y), f.shape[0], _ptr(g), _ptr(loss)))
+        return g, float(loss[0])
+
+    def mlp_train(self, features: np.ndarray, targets: np.ndarray, lr: float = 1e-2) -> float:
+        """One Adam step; returns the loss before it."""
+        f, y = self._mlp_batch(features, targets)
+        loss = np.zeros(1, np.float32)
+        self._check(self._lib.vgi_mlp_train(self._h, _ptr(f), _ptr(y), f.shape[0], float(lr), _ptr(loss)))
+        return float(loss[0])
 
     def reference_fp64(self, tasks: np.ndarray, samples: int, seed: int = 1):
         """FP64 converged reference per FaceTask: (mean rgb, mean square rgb, known)."""

@@ -259,6 +259,15 @@ int vgi_mlp_set_weights(vgi_ctx* ctx, const float* master, uint32_t count);
 int vgi_mlp_get_weights(vgi_ctx* ctx, float* master, uint32_t count);
 /* Forward pass over n feature rows (96 floats each): out4 = (rgb, 0) per row. */
 int vgi_mlp_forward(vgi_ctx* ctx, const float* features, uint32_t n, float* out4);
+/* Training loss over n rows with targets4 = (rgb, unused) per row: the
+ * relative luminance MSE  sum_rows sum_c (p_c - y_c)^2 / (lum(p)^2 + 0.01) / n,
+ * with lum(p) = 0.2126 r + 0.7152 g + 0.0722 b held constant in the gradient.
+ * vgi_mlp_gradients writes dLoss/dW (19,456 floats, the master order) and the
+ * loss without changing the weights; vgi_mlp_train takes one Adam step
+ * (beta 0.9 / 0.99, eps 1e-8, learning rate lr) on the FP32 masters and
+ * writes the loss before the step. vgi_mlp_set_weights resets Adam. */
+int vgi_mlp_gradients(vgi_ctx* ctx, const float* features, const float* targets4, uint32_t n, float* grads, float* loss);
+int vgi_mlp_train(vgi_ctx* ctx, const float* features, const float* targets4, uint32_t n, float lr, float* loss);
 
 /* ---- read-back: bounded snapshots (complete_readback, src/gpu.rs:1024-1170) --- */
 int vgi_read_results(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words24);
