@@ -112,11 +112,27 @@ struct vgi_ctx {
     // MLP radiance cache: FP32 master weights, their packed BF16 image
     DevBuf<float> mlp_master;
     DevBuf<uint8_t> mlp_image;
-    DevBuf<uint32_t> mlp_error;
+    DevBuf<uint32_t> mlp_error;               // [0] API calls and training, [1] the frames' queries
     DevBuf<uint8_t> mlp_image_b;              // W (rows = inputs): B operand of the backward pass
     DevBuf<float> mlp_adam;                   // Adam first and second moments, 2 x 19456
     DevBuf<float> mlp_grads;                  // 19456 gradients + the loss
-    uint32_t mlp_step = 0;
+    DevBuf<uint32_t> mlp_steps;               // Adam steps taken (a device word: a frame graph replays it)
+    DevBuf<float4> w_mlp_queue;               // 2 per path: the frame's network queries
+    DevBuf<float> mlp_features;               // training rows of a frame (batch x steps x 96)
+    DevBuf<float4> mlp_targets;
+    DevBuf<uint4> mlp_train_tasks;            // the frame's training faces (FaceTasks) and their traced results
+    DevBuf<uint4> mlp_train_results;
+    DevBuf<uint32_t> mlp_query_count;         // queries of the last terminating frame
+    uint32_t mlp_queue_capacity = 0;          // paths of the last terminating frame's trace
+    uint32_t mlp_ctas = 0, mlp_sms = 0;
+    // MLP termination in vgi_frame: off, or on after `mlp_warm` plain frames
+    // that train the network; `mlp_batch` rows x `mlp_train_steps` steps a frame.
+    bool mlp_cache = false;
+    uint32_t mlp_warm = 0, mlp_batch = 65536, mlp_train_steps = 1, mlp_frames = 0;
+    float mlp_lr = 1e-2f;
+    bool graph_mlp = false;                   // the captured frame's trace ends paths with the network
+    bool mlp_timed = false;                   // the last timed frame recorded mlp_marks
+    bool mlp_queried = false;                 // a frame has queried the network (counters[4] holds its count)
     uint32_t n_view = 0;
     DevBuf<uint4> events;
     uint32_t n_events = 0;
@@ -137,6 +153,7 @@ struct vgi_ctx {
     cudaGraphNode_t graph_prepare = nullptr, graph_accumulate = nullptr;
     cudaEvent_t marks[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t traverse_marks[8] = {};
+    cudaEvent_t mlp_marks[4] = {};            // network queries, then training, of the last timed frame
     uint32_t traverse_launches = 0;  // traversal launches of the last timed wavefront frame
 
     // trace layout and the wavefront's buffers
@@ -147,6 +164,10 @@ struct vgi_ctx {
     DevBuf<uint4> w_hit;
     DevBuf<uint32_t> w_status, w_queue0, w_queue1, w_scatter, w_counters;
 };
+
+extern "C" {
+static int mlp_frame_training(vgi_ctx* c);
+}
 
 namespace {
 
@@ -308,7 +329,27 @@ cudaError_t upload_grid(vgi_ctx* c, const int32_t* directory, uint64_t slots) {
 }
 
 // Enqueues the face trace for `a` in the context's layout.
-int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
+// Whether the trace ends uncached first hits with the network's prediction.
+bool mlp_terminates(const vgi_ctx* c) {
+    return c->mlp_cache && c->mlp_image.ptr && c->mlp_frames >= c->mlp_warm && c->layout == VGI_LAYOUT_WAVEFRONT;
+}
+
+// The network's position normalisation: the loaded regions' voxel box.
+MlpEncoding mlp_encoding(const vgi_ctx* c) {
+    MlpEncoding e{};
+    for (int k = 0; k < 3; ++k) {
+        const float lo = (float)c->bounds[k] * 16.0f, hi = (float)(c->bounds[3 + k] + 1) * 16.0f;
+        e.lo[k] = lo;
+        e.inv[k] = 1.0f / std::max(hi - lo, 1.0f);
+    }
+    return e;
+}
+
+// Samples per training face in an MLP-terminated frame's training trace.
+constexpr uint32_t kMlpTrainSamples = 4;
+
+// `marks`: record the frame's timing events (off for the training trace).
+int run_trace(vgi_ctx* c, const TraceArgs& a, bool count, bool marks = true) {
     if (c->layout == VGI_LAYOUT_SINGLE_KERNEL) {
         if (c->timing && !count) c->traverse_launches = 0;
         launch_trace(a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
@@ -318,17 +359,29 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
     const size_t paths = (size_t)a.n_tasks * a.samples;
     const size_t slots = paths * (2 + a.light_count) + (size_t)a.n_tasks * a.light_count;
     if (paths >= (1ull << 30) || slots > 0xffffffffull) return fail(c, VGI_ERR_CAPACITY, "too many paths for the wavefront layout");
+    const bool mlp = mlp_terminates(c);
+    // An MLP-terminated frame also traces its training faces in these
+    // buffers: size them for both, so a captured frame never reallocates.
+    size_t room_paths = paths, room_slots = slots;
+    if (mlp) {
+        const size_t rows = c->mlp_batch, tp = rows * kMlpTrainSamples;
+        room_paths = std::max(room_paths, tp);
+        room_slots = std::max(room_slots, tp * (2 + a.light_count) + rows * a.light_count);
+    }
     const void* before[3] = {c->w_state.ptr, c->w_ray.ptr, c->w_status.ptr};
-    VGI_CUDA(c, c->w_state.reserve(std::max<size_t>(paths, 1) * 9));
-    VGI_CUDA(c, c->w_ray.reserve(std::max<size_t>(slots, 1) * 2));
-    VGI_CUDA(c, c->w_hit.reserve(std::max<size_t>(paths, 1) * 6));
-    VGI_CUDA(c, c->w_status.reserve(std::max<size_t>(slots, 1)));
-    VGI_CUDA(c, c->w_queue0.reserve(std::max<size_t>(slots, 1)));
-    VGI_CUDA(c, c->w_queue1.reserve(std::max<size_t>(slots, 1)));
-    VGI_CUDA(c, c->w_scatter.reserve(std::max<size_t>(paths, 1)));
-    VGI_CUDA(c, c->w_counters.reserve(4));
+    VGI_CUDA(c, c->w_state.reserve(std::max<size_t>(room_paths, 1) * 9));
+    VGI_CUDA(c, c->w_ray.reserve(std::max<size_t>(room_slots, 1) * 2));
+    VGI_CUDA(c, c->w_hit.reserve(std::max<size_t>(room_paths, 1) * 6));
+    VGI_CUDA(c, c->w_status.reserve(std::max<size_t>(room_slots, 1)));
+    VGI_CUDA(c, c->w_queue0.reserve(std::max<size_t>(room_slots, 1)));
+    VGI_CUDA(c, c->w_queue1.reserve(std::max<size_t>(room_slots, 1)));
+    VGI_CUDA(c, c->w_scatter.reserve(std::max<size_t>(room_paths, 1)));
+    VGI_CUDA(c, c->w_counters.reserve(5));
+    const void* queue_before = c->w_mlp_queue.ptr;
+    if (mlp) VGI_CUDA(c, c->w_mlp_queue.reserve(std::max<size_t>(room_paths, 1) * 2));
     // A captured frame holds the old buffers' addresses.
-    if (before[0] != c->w_state.ptr || before[1] != c->w_ray.ptr || before[2] != c->w_status.ptr) drop_graph(c);
+    if (before[0] != c->w_state.ptr || before[1] != c->w_ray.ptr || before[2] != c->w_status.ptr || queue_before != c->w_mlp_queue.ptr)
+        drop_graph(c);
     WaveBuffers b{};
     b.state = c->w_state.ptr;
     b.ray = c->w_ray.ptr;
@@ -340,8 +393,17 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count) {
     b.counters = c->w_counters.ptr;
     b.traverse_blocks = c->traverse_blocks;
     b.refill_min = c->refill_min;
-    b.traverse_marks = (c->timing && !count) ? c->traverse_marks : nullptr;
-    if (b.traverse_marks) c->traverse_launches = std::min<uint32_t>(c->transport.bounces + 1u, 4u);
+    b.traverse_marks = (c->timing && !count && marks) ? c->traverse_marks : nullptr;
+    if (mlp) {
+        b.mlp_image = c->mlp_image.ptr;
+        b.mlp_queue = c->w_mlp_queue.ptr;
+        b.mlp_error = c->mlp_error.ptr + 1;
+        b.mlp_ctas = c->mlp_ctas;
+        b.mlp_enc = mlp_encoding(c);
+        if (c->timing && !count && marks) b.mlp_marks = c->mlp_marks;
+        if (marks) c->mlp_queue_capacity = (uint32_t)paths;
+    }
+    if (b.traverse_marks) c->traverse_launches = std::min<uint32_t>((mlp ? 1u : c->transport.bounces) + 1u, 4u);
     launch_wave(b, a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     return VGI_OK;
@@ -472,13 +534,17 @@ int vgi_destroy(vgi_ctx* c) {
     c->v_receivers.release(); c->v_paths.release(); c->v_conts.release(); c->v_estimates.release(); c->v_events.release();
     c->v_scratch.release(); c->v_queue.release();
     c->mlp_master.release(); c->mlp_image.release(); c->mlp_error.release();
-    c->mlp_image_b.release(); c->mlp_adam.release(); c->mlp_grads.release();
+    c->mlp_image_b.release(); c->mlp_adam.release(); c->mlp_grads.release(); c->mlp_steps.release();
+    c->w_mlp_queue.release(); c->mlp_features.release(); c->mlp_targets.release();
+    c->mlp_train_tasks.release(); c->mlp_train_results.release(); c->mlp_query_count.release();
     c->counters.release();
     c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
     c->w_queue0.release(); c->w_queue1.release(); c->w_scatter.release(); c->w_counters.release();
     for (auto& e : c->marks)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->traverse_marks)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->mlp_marks)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -845,6 +911,8 @@ int capture_frame(vgi_ctx* c, uint32_t samples, const AccumArgs& acc) {
     TraceArgs tr = trace_args(c, c->tasks.ptr, c->results.ptr, c->n_slots, samples, true);
     int rc = run_trace(c, tr, false);
     launch_accumulate(acc, c->stream);
+    if (rc == VGI_OK) rc = mlp_frame_training(c);
+    c->graph_mlp = mlp_terminates(c);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (rc != VGI_OK || e != cudaSuccess) {
@@ -889,6 +957,9 @@ int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
     if (rc != VGI_OK) return rc;
     if (samples == 0) return fail(c, VGI_ERR_INVALID, "samples must be positive");
     AccumArgs acc = accum_args(c, samples, clock_ms);
+    // The warm-up frames of the MLP cache trace plainly; the first frame
+    // that ends paths with the network needs a new capture.
+    if (c->graph_exec && c->graph_mlp != mlp_terminates(c)) drop_graph(c);
     if (c->use_graph && !c->timing && c->layout == VGI_LAYOUT_WAVEFRONT && c->n_slots > 0) {
         if (c->graph_exec && c->graph_samples == samples && !c->graph_dirty) {
             VGI_CUDA(c, set_accum_node(c, c->graph_prepare, acc));
@@ -896,6 +967,7 @@ int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
             VGI_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
             c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
             if (c->batch_id == 0) c->batch_id = 1;
+            if (c->mlp_cache) c->mlp_frames += 1;
             return VGI_OK;
         }
         if (!c->graph_dirty && c->graph_samples == samples) {
@@ -905,6 +977,7 @@ int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
             VGI_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
             c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
             if (c->batch_id == 0) c->batch_id = 1;
+            if (c->mlp_cache) c->mlp_frames += 1;
             return VGI_OK;
         }
         drop_graph(c);
@@ -920,9 +993,16 @@ int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
     if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[2], c->stream));
     launch_accumulate(acc, c->stream);
     if (c->timing) VGI_CUDA(c, cudaEventRecord(c->marks[3], c->stream));
+    const bool timed_mlp = c->timing && mlp_terminates(c);
+    if (timed_mlp) VGI_CUDA(c, cudaEventRecord(c->mlp_marks[2], c->stream));
+    rc = mlp_frame_training(c);
+    if (rc != VGI_OK) return rc;
+    if (timed_mlp) VGI_CUDA(c, cudaEventRecord(c->mlp_marks[3], c->stream));
+    if (c->timing) c->mlp_timed = timed_mlp;
     VGI_CUDA(c, cudaGetLastError());
     c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
     if (c->batch_id == 0) c->batch_id = 1;
+    if (c->mlp_cache) c->mlp_frames += 1;
     return VGI_OK;
 }
 
@@ -943,6 +1023,7 @@ int vgi_set_timing(vgi_ctx* c, int enable) {
     if (enable && !c->marks[0]) {
         for (auto& e : c->marks) VGI_CUDA(c, cudaEventCreate(&e));
         for (auto& e : c->traverse_marks) VGI_CUDA(c, cudaEventCreate(&e));
+        for (auto& e : c->mlp_marks) VGI_CUDA(c, cudaEventCreate(&e));
     }
     c->timing = enable != 0;
     return VGI_OK;
@@ -1295,13 +1376,20 @@ int vgi_mlp_set_weights(vgi_ctx* c, const float* master, uint32_t count) {
     VGI_CUDA(c, cudaSetDevice(c->device));
     VGI_CUDA(c, c->mlp_master.reserve(count));
     VGI_CUDA(c, c->mlp_image.reserve(mlp_image_bytes()));
-    VGI_CUDA(c, c->mlp_error.reserve(1));
+    VGI_CUDA(c, c->mlp_error.reserve(2));
+    VGI_CUDA(c, c->mlp_steps.reserve(1));
     VGI_CUDA(c, c->mlp_image_b.reserve(mlp_image_bytes()));
+    VGI_CUDA(c, mlp_set_attributes());
+    int sms = 148;
+    VGI_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    c->mlp_sms = (uint32_t)sms;
+    c->mlp_ctas = (uint32_t)sms * 3u;  // 62 KB of shared memory per forward CTA
     VGI_CUDA(c, c->mlp_adam.reserve((size_t)count * 2));
     VGI_CUDA(c, c->mlp_grads.reserve((size_t)count + 1));
     VGI_CUDA(c, cudaMemcpyAsync(c->mlp_master.ptr, master, (size_t)count * 4, cudaMemcpyHostToDevice, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_adam.ptr, 0, (size_t)count * 8, c->stream));
-    c->mlp_step = 0;
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_steps.ptr, 0, 4, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 8, c->stream));
     launch_mlp_pack(c->mlp_master.ptr, c->mlp_image.ptr, c->stream);
     launch_mlp_pack_backward(c->mlp_master.ptr, c->mlp_image_b.ptr, c->stream);
     VGI_CUDA(c, cudaGetLastError());
@@ -1327,9 +1415,7 @@ int vgi_mlp_forward(vgi_ctx* c, const float* features, uint32_t n, float* out4) 
     VGI_CUDA(c, out.reserve(n));
     VGI_CUDA(c, cudaMemcpyAsync(in.ptr, features, (size_t)n * 96 * 4, cudaMemcpyHostToDevice, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 4, c->stream));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    VGI_CUDA(c, launch_mlp_forward(in.ptr, c->mlp_image.ptr, out.ptr, n, c->mlp_error.ptr, (uint32_t)sms * 3u, c->stream));
+    VGI_CUDA(c, launch_mlp_forward(in.ptr, c->mlp_image.ptr, out.ptr, n, c->mlp_error.ptr, c->mlp_ctas, c->stream));
     uint32_t err = 0;
     VGI_CUDA(c, cudaMemcpyAsync(&err, c->mlp_error.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaMemcpyAsync(out4, out.ptr, (size_t)n * 16, cudaMemcpyDeviceToHost, c->stream));
@@ -1344,10 +1430,8 @@ static int mlp_batch_gradients(vgi_ctx* c, const float* features, const float4* 
     const uint32_t count = mlp_weight_count();
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_grads.ptr, 0, (size_t)(count + 1) * 4, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 4, c->stream));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     VGI_CUDA(c, launch_mlp_train(features, targets, n, c->mlp_image.ptr, c->mlp_image_b.ptr, c->mlp_grads.ptr, c->mlp_grads.ptr + count,
-                                 c->mlp_error.ptr, (uint32_t)sms, c->stream));
+                                 c->mlp_error.ptr, c->mlp_sms, c->stream));
     return VGI_OK;
 }
 
@@ -1384,12 +1468,115 @@ int vgi_mlp_gradients(vgi_ctx* c, const float* features, const float* targets4, 
 static int mlp_train_step(vgi_ctx* c, const float* features, const float4* targets, uint32_t n, float lr) {
     if (int e = mlp_batch_gradients(c, features, targets, n)) return e;
     const uint32_t count = mlp_weight_count();
-    c->mlp_step += 1;
-    launch_mlp_adam(c->mlp_master.ptr, c->mlp_adam.ptr, c->mlp_adam.ptr + count, c->mlp_grads.ptr, lr, 0.9f, 0.99f, 1e-8f, c->mlp_step,
+    launch_mlp_step(c->mlp_steps.ptr, c->stream);
+    launch_mlp_adam(c->mlp_master.ptr, c->mlp_adam.ptr, c->mlp_adam.ptr + count, c->mlp_grads.ptr, lr, 0.9f, 0.99f, 1e-8f, c->mlp_steps.ptr,
                     c->stream);
     launch_mlp_pack(c->mlp_master.ptr, c->mlp_image.ptr, c->stream);
     launch_mlp_pack_backward(c->mlp_master.ptr, c->mlp_image_b.ptr, c->stream);
     VGI_CUDA(c, cudaGetLastError());
+    return VGI_OK;
+}
+
+// A frame's online training: `mlp_train_steps` Adam steps, each on
+// `mlp_batch` faces drawn from the frame's results. Enqueued only.
+//
+// `mlp_batch` training samples a frame, split over `mlp_train_steps` Adam
+// steps. Plain (warm-up) frames draw them from the frame's own receivers. A
+// frame that ended paths with the network trains on the faces those paths
+// hit without a cache answer, the faces the network is asked about: that
+// many of the frame's queries, drawn by hash, are traced as faces of their
+// own (kMlpTrainSamples paths each, one diffuse hit, the network or the
+// cache at the next hit).
+static int mlp_frame_training(vgi_ctx* c) {
+    if (!c->mlp_cache || !c->mlp_image.ptr || c->n_slots == 0) return VGI_OK;
+    const MlpEncoding enc = mlp_encoding(c);
+    const uint32_t rows = c->mlp_batch, steps = c->mlp_train_steps, batch = rows / steps;
+    if (!mlp_terminates(c)) {
+        for (uint32_t k = 0; k < steps; ++k) {
+            launch_mlp_encode_training(c->slot_meta.ptr, c->results.ptr, c->materials.ptr, c->n_slots, c->mlp_steps.ptr, batch, enc,
+                                       c->mlp_features.ptr, c->mlp_targets.ptr, c->stream);
+            if (int e = mlp_train_step(c, c->mlp_features.ptr, c->mlp_targets.ptr, batch, c->mlp_lr)) return e;
+        }
+        return VGI_OK;
+    }
+    const uint32_t* queries = c->w_counters.ptr + 4;
+    VGI_CUDA(c, cudaMemcpyAsync(c->mlp_query_count.ptr, queries, 4, cudaMemcpyDeviceToDevice, c->stream));
+    launch_mlp_query_tasks(c->w_mlp_queue.ptr, queries, c->mlp_queue_capacity, c->mlp_steps.ptr, rows, kMlpTrainSamples, enc,
+                           c->mlp_train_tasks.ptr, c->mlp_features.ptr, c->stream);
+    const TraceArgs tr = trace_args(c, c->mlp_train_tasks.ptr, c->mlp_train_results.ptr, rows, kMlpTrainSamples, true);
+    if (int e = run_trace(c, tr, false, false)) return e;
+    launch_mlp_query_targets(c->mlp_train_results.ptr, rows, c->mlp_targets.ptr, c->stream);
+    for (uint32_t k = 0; k < steps; ++k)
+        if (int e = mlp_train_step(c, c->mlp_features.ptr + (size_t)k * batch * 96, c->mlp_targets.ptr + (size_t)k * batch, batch,
+                                   c->mlp_lr))
+            return e;
+    c->mlp_queried = true;
+    return VGI_OK;
+}
+
+int vgi_mlp_encode(vgi_ctx* c, const vgi_face* faces, uint32_t n, float* features) {
+    if (!c || (n && (!faces || !features))) return VGI_ERR_INVALID;
+    if (!c->materials.ptr) return fail(c, VGI_ERR_STATE, "materials are not set");
+    if (n == 0) return VGI_OK;
+    std::vector<uint4> meta(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        if (faces[k].face > 5 || faces[k].material > 255) return fail(c, VGI_ERR_INVALID, "face or material out of range");
+        meta[k] = make_uint4((uint32_t)faces[k].voxel[0], (uint32_t)faces[k].voxel[1], (uint32_t)faces[k].voxel[2],
+                             faces[k].face | (faces[k].material << 16));
+    }
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    DevBuf<uint4> m;
+    DevBuf<float> out;
+    VGI_CUDA(c, m.reserve(n));
+    VGI_CUDA(c, out.reserve((size_t)n * 96));
+    VGI_CUDA(c, cudaMemcpyAsync(m.ptr, meta.data(), (size_t)n * 16, cudaMemcpyHostToDevice, c->stream));
+    launch_mlp_encode_faces(m.ptr, n, c->materials.ptr, mlp_encoding(c), out.ptr, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    VGI_CUDA(c, cudaMemcpyAsync(features, out.ptr, (size_t)n * 96 * 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_set_mlp_cache(vgi_ctx* c, int enable, uint32_t warm_frames, uint32_t batch, uint32_t steps_per_frame, float lr) {
+    if (c) drop_graph(c);  // what a frame launches changes
+    if (!c) return VGI_ERR_INVALID;
+    if (enable && !c->mlp_image.ptr) return fail(c, VGI_ERR_STATE, "MLP weights are not set");
+    if (enable && (steps_per_frame == 0 || steps_per_frame > 64 || batch < steps_per_frame || batch > (1u << 22) || !(lr > 0.0f)))
+        return fail(c, VGI_ERR_INVALID, "MLP cache: 1..64 steps a frame, steps <= samples <= 2^22, positive learning rate");
+    c->mlp_cache = enable != 0;
+    if (!c->mlp_cache) return VGI_OK;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    const size_t rows = batch;
+    VGI_CUDA(c, c->mlp_features.reserve(rows * 96));
+    VGI_CUDA(c, c->mlp_targets.reserve(rows));
+    VGI_CUDA(c, c->mlp_train_tasks.reserve(rows * 2));
+    VGI_CUDA(c, c->mlp_train_results.reserve(rows * 6));
+    VGI_CUDA(c, c->mlp_query_count.reserve(1));
+    c->mlp_warm = warm_frames;
+    c->mlp_batch = batch;
+    c->mlp_train_steps = steps_per_frame;
+    c->mlp_lr = lr;
+    c->mlp_frames = 0;
+    return VGI_OK;
+}
+
+int vgi_mlp_stats(vgi_ctx* c, vgi_mlp_status* out) {
+    if (!c || !out) return VGI_ERR_INVALID;
+    *out = vgi_mlp_status{};
+    out->frames = c->mlp_frames;
+    out->terminating = mlp_terminates(c) ? 1u : 0u;
+    if (!c->mlp_image.ptr) return VGI_OK;
+    uint32_t err[2] = {0, 0};
+    VGI_CUDA(c, cudaMemcpyAsync(&out->steps, c->mlp_steps.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(&out->loss, c->mlp_grads.ptr + mlp_weight_count(), 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(err, c->mlp_error.ptr, 8, cudaMemcpyDeviceToHost, c->stream));
+    if (c->mlp_queried) VGI_CUDA(c, cudaMemcpyAsync(&out->queries, c->mlp_query_count.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    out->error = err[0] | err[1];
+    if (c->mlp_timed) {
+        VGI_CUDA(c, cudaEventElapsedTime(&out->query_ms, c->mlp_marks[0], c->mlp_marks[1]));
+        VGI_CUDA(c, cudaEventElapsedTime(&out->train_ms, c->mlp_marks[2], c->mlp_marks[3]));
+    }
     return VGI_OK;
 }
 

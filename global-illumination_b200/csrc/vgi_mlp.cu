@@ -22,6 +22,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "vgi_device.cuh"
 #include "vgi_types.cuh"
 
 namespace vgi {
@@ -135,9 +136,133 @@ __global__ void pack_kernel(const float* master, uint8_t* image) {
     *reinterpret_cast<__nv_bfloat16*>(image + weight_offset(l) * 2 + core_offset(n, k, in_dim(l))) = b;
 }
 
-// outputs[row][0..3] = exp(network(features[row][0..95]))[0..2], 0
-__global__ void __launch_bounds__(kThreads) forward_kernel(const float* features, const uint8_t* image, float4* outputs, uint32_t n,
-                                                           uint32_t* error) {
+// ---- input encoding --------------------------------------------------------
+// A face's 96 inputs: for each axis a of the face centre, normalised to
+// [0, 1] over the loaded volume, sin and cos of pi 2^k x for k = 0..11
+// (features 24a + 2k and 24a + 2k + 1); the normal as one-hot over the face
+// index (72..77: +x, -x, +y, -y, +z, -z); the albedo rgb (78..80); zeros
+// (81..95). sincospif gives k = 0 and k = 6; the other frequencies follow by
+// the double-angle identities sin 2t = 2 sin t cos t, cos 2t = 1 - 2 sin^2 t,
+// five doublings at most, so the error stays within a few dozen ulp.
+__device__ __forceinline__ void encode_axis(float x, float* v) {
+    for (int half = 0; half < 2; ++half) {
+        float s, c;
+        sincospif(half ? x * 64.0f : x, &s, &c);
+        for (int k = 0; k < 6; ++k) {
+            v[(half * 6 + k) * 2] = s;
+            v[(half * 6 + k) * 2 + 1] = c;
+            const float s2 = 2.0f * s * c, c2 = 1.0f - 2.0f * s * s;
+            s = s2;
+            c = c2;
+        }
+    }
+}
+
+// Writes the encoding of one face into row `row` of a K = 96 tile.
+__device__ __forceinline__ void stage_face(uint8_t* tile, uint32_t row, const float* centre, const MlpEncoding& e, uint32_t face,
+                                           float r, float g, float b) {
+    for (int a = 0; a < 3; ++a) {
+        float v[24];
+        encode_axis((centre[a] - e.lo[a]) * e.inv[a], v);
+        for (int c = 0; c < 3; ++c) store8(tile, row, (uint32_t)(a * 3 + c), kIn, v + c * 8);
+    }
+    float v[24];
+    for (int j = 0; j < 24; ++j) v[j] = 0.0f;
+    if (face < 6u) v[face] = 1.0f;
+    v[6] = r;
+    v[7] = g;
+    v[8] = b;
+    for (int c = 0; c < 3; ++c) store8(tile, row, 9u + (uint32_t)c, kIn, v + c * 8);
+}
+
+// The centre of a face (voxel xyz, face index in the low 3 bits of w), in voxels.
+__device__ __forceinline__ void face_centre(const uint4& meta, float* centre) {
+    const uint32_t face = meta.w & 7u, axis = face >> 1;
+    const float side = (face & 1u) ? -0.5f : 0.5f;
+    centre[0] = (float)(int)meta.x + 0.5f + (axis == 0 ? side : 0.0f);
+    centre[1] = (float)(int)meta.y + 0.5f + (axis == 1 ? side : 0.0f);
+    centre[2] = (float)(int)meta.z + 0.5f + (axis == 2 ? side : 0.0f);
+}
+
+// One face's 96 inputs as FP32, in the order stage_face writes them.
+__device__ __forceinline__ void encode_centre(const float* centre, uint32_t face, float r, float g, float b, const MlpEncoding& enc,
+                                              float* f) {
+    float v[24];
+    for (int a = 0; a < 3; ++a) {
+        encode_axis((centre[a] - enc.lo[a]) * enc.inv[a], v);
+        for (int j = 0; j < 24; ++j) f[a * 24 + j] = v[j];
+    }
+    for (int j = 72; j < kIn; ++j) f[j] = 0.0f;
+    if (face < 6u) f[72 + face] = 1.0f;
+    f[78] = r;
+    f[79] = g;
+    f[80] = b;
+}
+
+// The same from a slot identity word (voxel xyz, face | material << 16).
+__device__ __forceinline__ void encode_meta(const uint4& meta, const float4* materials, const MlpEncoding& enc, float* f) {
+    const uint32_t face = meta.w & 7u, material = (meta.w >> 16) & 255u;
+    const float4 d = materials[material * 4u];
+    float centre[3];
+    face_centre(meta, centre);
+    encode_centre(centre, face, d.x, d.y, d.z, enc, f);
+}
+
+// ---- forward pass -----------------------------------------------------------
+// Rows of caller-given features: outputs[row] = (exp(net)[0..2], 0).
+struct FeatureRows {
+    const float* features;
+    float4* outputs;
+    uint32_t n;
+    __device__ uint32_t count() const { return n; }
+    __device__ void stage(uint8_t* tile, uint32_t tid, uint32_t row) const {
+        float v[8];
+        for (uint32_t c = 0; c < kIn / 8; ++c) {
+            if (row < n) {
+                const float4 a = reinterpret_cast<const float4*>(features + (size_t)row * kIn)[c * 2u];
+                const float4 b = reinterpret_cast<const float4*>(features + (size_t)row * kIn)[c * 2u + 1u];
+                v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+            } else {
+                for (int j = 0; j < 8; ++j) v[j] = 0.0f;
+            }
+            store8(tile, tid, c, kIn, v);
+        }
+    }
+    __device__ void emit(uint32_t row, float r, float g, float b) const {
+        if (row < n) outputs[row] = make_float4(r, g, b, 0.0f);
+    }
+};
+
+// The trace's queued hits: two float4 per query, (face centre xyz in
+// voxels, path index bits) and (albedo rgb, face index bits); the
+// prediction goes to out[path] = (rgb, 0). The count is read on the device.
+struct PathQueries {
+    const float4* queue;
+    const uint32_t* counter;
+    uint32_t capacity;
+    MlpEncoding enc;
+    float4* out;
+    __device__ uint32_t count() const {
+        const uint32_t n = *counter;
+        return n < capacity ? n : capacity;
+    }
+    __device__ void stage(uint8_t* tile, uint32_t tid, uint32_t row) const {
+        if (row < count()) {
+            const float4 q0 = queue[2u * row], q1 = queue[2u * row + 1u];
+            const float centre[3] = {q0.x, q0.y, q0.z};
+            stage_face(tile, tid, centre, enc, __float_as_uint(q1.w), q1.x, q1.y, q1.z);
+        } else {
+            const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (uint32_t c = 0; c < kIn / 8; ++c) store8(tile, tid, c, kIn, z);
+        }
+    }
+    __device__ void emit(uint32_t row, float r, float g, float b) const {
+        if (row < count()) out[__float_as_uint(queue[2u * row].w)] = make_float4(r, g, b, 0.0f);
+    }
+};
+
+template <class Rows>
+__global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, const uint8_t* image, uint32_t* error) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* weights = smem;
     uint8_t* tile = smem + kImageBytes;
@@ -145,6 +270,9 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const float* features
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kImageBytes + kABytes + 8);
     uint32_t* abort_flag = reinterpret_cast<uint32_t*>(smem + kImageBytes + kABytes + 12);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t n = rows.count();
+    const uint32_t tiles = (n + kRows - 1) / kRows;
+    if (blockIdx.x >= tiles) return;  // uniform per CTA: nothing allocated yet
 
     for (uint32_t i = tid; i < kImageBytes / 16; i += kThreads)
         reinterpret_cast<uint4*>(weights)[i] = reinterpret_cast<const uint4*>(image)[i];
@@ -164,24 +292,10 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const float* features
     const uint32_t lane_base = tmem + ((warp * 32u) << 16);
     const uint32_t bar_addr = smem_u32(bar);
     uint32_t phase = 0;
-    const uint32_t tiles = (n + kRows - 1) / kRows;
 
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         const uint32_t row = t * kRows + tid;
-        // Layer 0 input: the row's 96 features (zeros past the end).
-        {
-            float v[8];
-            for (uint32_t c = 0; c < kIn / 8; ++c) {
-                if (row < n) {
-                    const float4 a = reinterpret_cast<const float4*>(features + (size_t)row * kIn)[c * 2u];
-                    const float4 b = reinterpret_cast<const float4*>(features + (size_t)row * kIn)[c * 2u + 1u];
-                    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-                } else {
-                    for (int j = 0; j < 8; ++j) v[j] = 0.0f;
-                }
-                store8(tile, tid, c, kIn, v);
-            }
-        }
+        rows.stage(tile, tid, row);
         bool ok = true;
         for (int l = 0; l < kLayers && ok; ++l) {
             const uint32_t K = in_dim(l), N = out_dim(l);
@@ -221,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const float* features
                 float v[16];
                 tmem_ld16(lane_base, v);
                 tmem_wait_ld();
-                if (row < n) outputs[row] = make_float4(expf(v[0]), expf(v[1]), expf(v[2]), 0.0f);
+                rows.emit(row, expf(v[0]), expf(v[1]), expf(v[2]));
             }
         }
         if (!ok) break;
@@ -230,6 +344,70 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const float* features
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns));
 }
+
+__global__ void encode_faces_kernel(const uint4* meta, uint32_t n, const float4* materials, MlpEncoding enc, float* features) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) encode_meta(meta[k], materials, enc, features + (size_t)k * kIn);
+}
+
+// Training rows from a frame's results: `batch` slots drawn by hash from
+// (step, row); features as encode_meta writes them (BF16-rounded by the
+// training kernel), target = the slot's frame mean, NaN when the slot had no
+// known sample. slot_meta[s * 3] = voxel xyz, face | material << 16;
+// results[s * 6] = mean rgb; results[s * 6 + 1].y = samples (float bits).
+__global__ void encode_training_kernel(const uint4* slot_meta, const uint4* results, const float4* materials, uint32_t n_slots,
+                                       const uint32_t* step, uint32_t batch, MlpEncoding enc, float* features, float4* targets) {
+    const uint32_t k = blockIdx.x * kThreads + threadIdx.x;
+    if (k >= batch) return;
+    const uint32_t salt = pcg(*step * 0x9e3779b9u + 0x7f4a7c15u);
+    const uint32_t slot = pcg(k ^ salt) % n_slots;
+    encode_meta(slot_meta[(size_t)slot * 3u], materials, enc, features + (size_t)k * kIn);
+    const uint4 r0 = results[(size_t)slot * 6u], r1 = results[(size_t)slot * 6u + 1u];
+    float4 target = make_float4(__int_as_float(0x7fc00000), 0.0f, 0.0f, 0.0f);
+    if (__uint_as_float(r1.y) > 0.0f) target = make_float4(__uint_as_float(r0.x), __uint_as_float(r0.y), __uint_as_float(r0.z), 0.0f);
+    targets[k] = target;
+}
+
+// Training faces from a frame's network queries (the faces its paths hit
+// without a cache answer): row k takes query hash(step, k) mod count and
+// becomes a FaceTask (voxel, face, sequence step * samples) plus the row's
+// inputs. No queries: the task is marked invalid (face 0xffffffff).
+__global__ void query_tasks_kernel(const float4* queue, const uint32_t* counter, uint32_t capacity, const uint32_t* step, uint32_t n,
+                                   uint32_t samples, MlpEncoding enc, uint4* tasks, float* features) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t available = *counter < capacity ? *counter : capacity;
+    float* f = features + (size_t)k * kIn;
+    if (available == 0u) {
+        tasks[2u * k] = make_uint4(0u, 0u, 0u, 0xffffffffu);
+        tasks[2u * k + 1u] = make_uint4(0u, 0u, 0u, 0u);
+        for (int j = 0; j < kIn; ++j) f[j] = 0.0f;
+        return;
+    }
+    const uint32_t salt = pcg(*step * 0x85ebca6bu + 0x3c6ef372u);
+    const uint32_t q = pcg(k ^ salt) % available;
+    const float4 q0 = queue[2u * q], q1 = queue[2u * q + 1u];
+    const uint32_t face = __float_as_uint(q1.w), axis = face >> 1;
+    const float side = (face & 1u) ? -0.5f : 0.5f;
+    const float centre[3] = {q0.x, q0.y, q0.z};
+    int v[3];
+    for (int a = 0; a < 3; ++a) v[a] = (int)floorf(centre[a] - 0.5f - ((uint32_t)a == axis ? side : 0.0f));
+    tasks[2u * k] = make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], face);
+    tasks[2u * k + 1u] = make_uint4(*step * samples, 0u, 0u, 0u);
+    encode_centre(centre, face, q1.x, q1.y, q1.z, enc, f);
+}
+
+// targets[k] = the traced mean of row k's face, NaN without a known sample.
+__global__ void query_targets_kernel(const uint4* results, uint32_t n, float4* targets) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint4 r0 = results[(size_t)k * 6u], r1 = results[(size_t)k * 6u + 1u];
+    float4 target = make_float4(__int_as_float(0x7fc00000), 0.0f, 0.0f, 0.0f);
+    if (__uint_as_float(r1.y) > 0.0f) target = make_float4(__uint_as_float(r0.x), __uint_as_float(r0.y), __uint_as_float(r0.z), 0.0f);
+    targets[k] = target;
+}
+
+__global__ void step_kernel(uint32_t* step) { *step += 1u; }
 
 // ---- training ------------------------------------------------------------
 // One fused kernel per batch: every CTA (one per SM, 512 TMEM columns) runs
@@ -368,8 +546,8 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
         // Output gradient.
         float dz[64];
         for (int j = 0; j < 64; ++j) dz[j] = 0.0f;
-        if (valid) {
-            const float4 y = targets[row];
+        const float4 y = valid ? targets[row] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (valid && y.x == y.x) {  // a NaN target marks a row without a sample
             const float p0 = expf(z[0]), p1 = expf(z[1]), p2 = expf(z[2]);
             const float lum = 0.2126f * p0 + 0.7152f * p1 + 0.0722f * p2;
             const float inv = 1.0f / ((lum * lum + 0.01f) * (float)batch);
@@ -440,9 +618,10 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
 // Adam (Kingma & Ba) on the FP32 masters, step `step` (1-based), then the
 // two BF16 images are repacked by the caller.
 __global__ void adam_kernel(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps,
-                            uint32_t step) {
+                            const uint32_t* steps) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kWeights) return;
+    const uint32_t step = *steps;
     const float g = grads[i];
     const float mi = beta1 * m[i] + (1.0f - beta1) * g;
     const float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
@@ -461,17 +640,56 @@ void launch_mlp_pack_backward(const float* master, uint8_t* image, cudaStream_t 
 cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
                              float* grads, float* loss, uint32_t* error, uint32_t ctas, cudaStream_t s) {
     if (batch == 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(mlp::train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
-    if (e != cudaSuccess) return e;
     const uint32_t tiles = (batch + mlp::kRows - 1) / mlp::kRows;
     mlp::train_kernel<<<tiles < ctas ? tiles : ctas, mlp::kThreads, mlp::kTrainSmem, s>>>(features, targets, batch, image_f, image_b, grads,
                                                                                            loss, error);
     return cudaGetLastError();
 }
 
-void launch_mlp_adam(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps, uint32_t step,
-                     cudaStream_t s) {
+void launch_mlp_adam(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps,
+                     const uint32_t* step, cudaStream_t s) {
     mlp::adam_kernel<<<(mlp::kWeights + 255) / 256, 256, 0, s>>>(master, m, v, grads, lr, beta1, beta2, eps, step);
+}
+
+void launch_mlp_step(uint32_t* step, cudaStream_t s) { mlp::step_kernel<<<1, 1, 0, s>>>(step); }
+
+void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,
+                        float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s) {
+    if (capacity == 0) return;
+    const mlp::PathQueries rows{queue, count, capacity, enc, out};
+    mlp::forward_kernel<mlp::PathQueries><<<ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error);
+}
+
+void launch_mlp_encode_training(const uint4* slot_meta, const uint4* results, const float4* materials, uint32_t n_slots,
+                                const uint32_t* step, uint32_t batch, const MlpEncoding& enc, float* features, float4* targets,
+                                cudaStream_t s) {
+    if (batch == 0 || n_slots == 0) return;
+    mlp::encode_training_kernel<<<(batch + mlp::kThreads - 1) / mlp::kThreads, mlp::kThreads, 0, s>>>(slot_meta, results, materials, n_slots,
+                                                                                                     step, batch, enc, features, targets);
+}
+
+void launch_mlp_encode_faces(const uint4* meta, uint32_t n, const float4* materials, const MlpEncoding& enc, float* features,
+                             cudaStream_t s) {
+    if (n) mlp::encode_faces_kernel<<<(n + 127) / 128, 128, 0, s>>>(meta, n, materials, enc, features);
+}
+
+void launch_mlp_query_tasks(const float4* queue, const uint32_t* count, uint32_t capacity, const uint32_t* step, uint32_t n,
+                            uint32_t samples, const MlpEncoding& enc, uint4* tasks, float* features, cudaStream_t s) {
+    if (n) mlp::query_tasks_kernel<<<(n + 127) / 128, 128, 0, s>>>(queue, count, capacity, step, n, samples, enc, tasks, features);
+}
+
+void launch_mlp_query_targets(const uint4* results, uint32_t n, float4* targets, cudaStream_t s) {
+    if (n) mlp::query_targets_kernel<<<(n + 127) / 128, 128, 0, s>>>(results, n, targets);
+}
+
+// Raises the dynamic shared-memory limit of the MLP kernels; called once per
+// context before their first launch (outside any stream capture).
+cudaError_t mlp_set_attributes() {
+    cudaError_t e = cudaFuncSetAttribute(mlp::forward_kernel<mlp::FeatureRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mlp::forward_kernel<mlp::PathQueries>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(mlp::train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
+    return e;
 }
 
 void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s) {
@@ -481,10 +699,9 @@ void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s) {
 cudaError_t launch_mlp_forward(const float* features, const uint8_t* image, float4* outputs, uint32_t n, uint32_t* error, uint32_t ctas,
                                cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(mlp::forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
-    if (e != cudaSuccess) return e;
     const uint32_t tiles = (n + mlp::kRows - 1) / mlp::kRows;
-    mlp::forward_kernel<<<tiles < ctas ? tiles : ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(features, image, outputs, n, error);
+    const mlp::FeatureRows rows{features, outputs, n};
+    mlp::forward_kernel<mlp::FeatureRows><<<tiles < ctas ? tiles : ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error);
     return cudaGetLastError();
 }
 

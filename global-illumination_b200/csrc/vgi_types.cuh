@@ -57,6 +57,13 @@ struct AccumArgs {
 
 // Device buffers of the wavefront layout (vgi_wave.cuh) for P = tasks x
 // samples paths and S = P * (2 + lights) + tasks * lights ray slots.
+// Maps voxel coordinates to the MLP's [0, 1] position inputs: (x - lo) * inv
+// per axis.
+struct MlpEncoding {
+    float lo[3];
+    float inv[3];
+};
+
 struct WaveBuffers {
     float4* state;            // 9 * P path-state words
     float4* ray;              // 2 * S
@@ -68,6 +75,15 @@ struct WaveBuffers {
     uint32_t traverse_blocks; // persistent traversal grid
     uint32_t refill_min;      // idle lanes that trigger a refill
     cudaEvent_t* traverse_marks;  // optional: start/end events of up to 4 traversal launches
+    // MLP termination (null image: off). Uncached first hits are queued
+    // (2 float4 each, counter at counters[4]) and take the network's
+    // prediction in place of the continuation.
+    const uint8_t* mlp_image;
+    float4* mlp_queue;        // 2 * P
+    uint32_t* mlp_error;
+    uint32_t mlp_ctas;
+    MlpEncoding mlp_enc;
+    cudaEvent_t* mlp_marks;   // optional: start/end events of the query launch
 };
 
 // The view tier's buffers and controls (vgi_view.cuh) for n receivers.
@@ -103,14 +119,26 @@ void launch_reference64(const TraceArgs& a, const double* cdf, const int4* emitt
 const void* prepare_kernel_address();
 const void* accumulate_kernel_address();
 // MLP radiance cache (vgi_mlp.cu).
+cudaError_t mlp_set_attributes();
+void launch_mlp_step(uint32_t* step, cudaStream_t s);
+void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,
+                        float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s);
+void launch_mlp_encode_training(const uint4* slot_meta, const uint4* results, const float4* materials, uint32_t n_slots,
+                                const uint32_t* step, uint32_t batch, const MlpEncoding& enc, float* features, float4* targets,
+                                cudaStream_t s);
+void launch_mlp_query_tasks(const float4* queue, const uint32_t* count, uint32_t capacity, const uint32_t* step, uint32_t n,
+                            uint32_t samples, const MlpEncoding& enc, uint4* tasks, float* features, cudaStream_t s);
+void launch_mlp_query_targets(const uint4* results, uint32_t n, float4* targets, cudaStream_t s);
+void launch_mlp_encode_faces(const uint4* meta, uint32_t n, const float4* materials, const MlpEncoding& enc, float* features,
+                             cudaStream_t s);
 void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s);
 cudaError_t launch_mlp_forward(const float* features, const uint8_t* image, float4* outputs, uint32_t n, uint32_t* error, uint32_t ctas,
                                cudaStream_t s);
 void launch_mlp_pack_backward(const float* master, uint8_t* image, cudaStream_t s);
 cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
                              float* grads, float* loss, uint32_t* error, uint32_t ctas, cudaStream_t s);
-void launch_mlp_adam(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps, uint32_t step,
-                     cudaStream_t s);
+void launch_mlp_adam(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps,
+                     const uint32_t* step, cudaStream_t s);
 uint32_t mlp_weight_count();
 uint32_t mlp_image_bytes();
 void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s);

@@ -81,6 +81,8 @@ struct WaveArgs {
     uint32_t* queue_head;    // traversal cursor
     uint32_t* scatter_queue; // uncached hits: path | bounce << 30
     uint32_t* scatter_count;
+    float4* mlp_queue;       // MLP termination (null: off): per uncached hit (face centre, path), (albedo, face)
+    uint32_t* mlp_count;
 };
 
 __device__ __forceinline__ float4& field(const WaveArgs& W, uint32_t f, uint32_t p) { return W.state[(size_t)f * W.n_paths + p]; }
@@ -726,9 +728,10 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SHADE_MIN_BLOCKS) wave_shade_k
     float4 pp = in ? field(W, kPP, p) : make_float4(0, 0, 0, 0);
     uint32_t flags = bits(pp.w);
     const uint32_t base = p * W.slots;
-    bool emit_c = false, emit_n = false, emit_d = false, scatter = false;
+    bool emit_c = false, emit_n = false, emit_d = false, scatter = false, query = false;
     uint32_t scatter_entry = 0;
     V3 dpos{0.0f, 0.0f, 0.0f}, dnrm{0.0f, 0.0f, 0.0f};
+    float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0;
     if (in && (flags & kFlagValid)) {
         float4 e = field(W, kE, p);
         // The receiver's NEE from stage 0.
@@ -820,6 +823,14 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SHADE_MIN_BLOCKS) wave_shade_k
                     cnt.cache_hit();
                     pending_kind = kKindCached;
                     xval = cached;
+                } else if (W.mlp_queue != nullptr) {
+                    // The network's prediction for the hit face replaces the
+                    // cache value; the query kernel writes it into kX.
+                    pending_kind = kKindCached;
+                    query = true;
+                    const V3 centre = add_s(itof(hv), 0.5f) + hn * 0.5f;
+                    q0 = make_float4(centre.x, centre.y, centre.z, fl(p));
+                    q1 = make_float4(diffuse.x, diffuse.y, diffuse.z, fl(face_index_of(hn)));
                 } else {
                     // NEE or the terminal connection, and the continuation,
                     // run in wave_scatter_kernel over the paths queued here.
@@ -856,6 +867,20 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SHADE_MIN_BLOCKS) wave_shade_k
             if (lane == leader) first = atomicAdd(W.scatter_count, (uint32_t)__popc(mask));
             first = __shfl_sync(0xffffffffu, first, leader);
             if (scatter) W.scatter_queue[first + __popc(mask & ((1u << lane) - 1u))] = scatter_entry;
+        }
+    }
+    if (W.mlp_queue != nullptr) {
+        const unsigned mask = __ballot_sync(0xffffffffu, query);
+        if (mask) {
+            const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+            uint32_t first = 0;
+            if (lane == leader) first = atomicAdd(W.mlp_count, (uint32_t)__popc(mask));
+            first = __shfl_sync(0xffffffffu, first, leader);
+            if (query) {
+                const uint32_t k = first + __popc(mask & ((1u << lane) - 1u));
+                W.mlp_queue[2u * k] = q0;
+                W.mlp_queue[2u * k + 1u] = q1;
+            }
         }
     }
     flush_counters<C>(A, cnt);
@@ -1035,6 +1060,8 @@ void wave_run(const WaveBuffers& b, const TraceArgs& a, cudaStream_t s) {
     W.queue_head = b.counters + 2;
     W.scatter_queue = b.scatter;
     W.scatter_count = b.counters + 3;
+    W.mlp_queue = b.mlp_image ? b.mlp_queue : nullptr;
+    W.mlp_count = b.counters + 4;
     const uint32_t path_blocks = (W.n_paths + kWaveBlock - 1) / kWaveBlock;
     const uint32_t face_blocks = (uint32_t)((((uint64_t)a.n_tasks << a.lanes_log2) + kWaveBlock - 1) / kWaveBlock);
     uint32_t* qa = b.queue[0];
@@ -1058,8 +1085,17 @@ void wave_run(const WaveBuffers& b, const TraceArgs& a, cudaStream_t s) {
         cudaMemsetAsync(W.scatter_count, 0, sizeof(uint32_t), s);
         W.queue_out = qb;
         W.count_out = cb;
+        if (W.mlp_queue) cudaMemsetAsync(W.mlp_count, 0, sizeof(uint32_t), s);
         wave_shade_kernel<H, L, B, C><<<path_blocks, kWaveBlock, 0, s>>>(W, stage);
-        wave_scatter_kernel<H, L, B, C><<<b.traverse_blocks, kWaveBlock, 0, s>>>(W);
+        if (W.mlp_queue) {
+            // One diffuse hit: the queued hits take the network's value.
+            if (b.mlp_marks) cudaEventRecord(b.mlp_marks[0], s);
+            launch_mlp_queries(W.mlp_queue, W.mlp_count, W.n_paths, b.mlp_image, b.mlp_enc, W.state + (size_t)kX * W.n_paths, b.mlp_error,
+                               b.mlp_ctas, s);
+            if (b.mlp_marks) cudaEventRecord(b.mlp_marks[1], s);
+        } else {
+            wave_scatter_kernel<H, L, B, C><<<b.traverse_blocks, kWaveBlock, 0, s>>>(W);
+        }
         uint32_t* t = qa; qa = qb; qb = t;
         t = ca; ca = cb; cb = t;
     }
@@ -1083,6 +1119,7 @@ void wave_hits(const WaveBuffers& b, const TraceArgs& a, bool limited, bool budg
 
 void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t s) {
     if (a.n_tasks == 0 || a.samples == 0) return;
+    if (b.mlp_image) hits = 1;  // the network ends paths at the first hit
     if (hits <= 1) wave_hits<1>(b, a, limited, budgeted, count, s);
     else if (hits == 2) wave_hits<2>(b, a, limited, budgeted, count, s);
     else wave_hits<3>(b, a, limited, budgeted, count, s);

@@ -44,6 +44,13 @@ class TransportUnavailable(VgiError):
     (src/lib.rs:355-357); it never falls back to the CPU."""
 
 
+class MlpStatus(ctypes.Structure):
+    """vgi_mlp_status."""
+    _fields_ = [("frames", ctypes.c_uint32), ("steps", ctypes.c_uint32), ("terminating", ctypes.c_uint32),
+                ("queries", ctypes.c_uint32), ("loss", ctypes.c_float), ("error", ctypes.c_uint32),
+                ("query_ms", ctypes.c_float), ("train_ms", ctypes.c_float)]
+
+
 class Counters(ctypes.Structure):
     _fields_ = [
         ("rays", ctypes.c_uint64),
@@ -173,6 +180,9 @@ _SIGNATURES = {
     "vgi_mlp_forward": (_INT, [_P, _P, _U32, _P]),
     "vgi_mlp_gradients": (_INT, [_P, _P, _P, _U32, _P, _P]),
     "vgi_mlp_train": (_INT, [_P, _P, _P, _U32, ctypes.c_float, _P]),
+    "vgi_mlp_encode": (_INT, [_P, _P, _U32, _P]),
+    "vgi_set_mlp_cache": (_INT, [_P, ctypes.c_int, _U32, _U32, _U32, ctypes.c_float]),
+    "vgi_mlp_stats": (_INT, [_P, _P]),
     "vgi_read_results": (_INT, [_P, _U32, _U32, _P]),
     "vgi_read_state": (_INT, [_P, _U32, _U32, _P]),
     "vgi_write_state": (_INT, [_P, _U32, _U32, _P]),
@@ -538,6 +548,25 @@ class GpuTracer:
         loss = np.zeros(1, np.float32)
         self._check(self._lib.vgi_mlp_train(self._h, _ptr(f), _ptr(y), f.shape[0], float(lr), _ptr(loss)))
         return float(loss[0])
+
+    def mlp_encode(self, faces: np.ndarray) -> np.ndarray:
+        """The network's inputs (n x 96) for face rows (voxel xyz, face, material)."""
+        f = _c(faces, np.int32).reshape(-1, 5)
+        out = np.zeros((f.shape[0], 96), np.float32)
+        self._check(self._lib.vgi_mlp_encode(self._h, _ptr(f), f.shape[0], _ptr(out)))
+        return out
+
+    def set_mlp_cache(self, enable: bool = True, warm_frames: int = 8, samples: int = 65536, steps_per_frame: int = 16,
+                      lr: float = 1e-2) -> None:
+        """MLP cache mode of frame(): online training on `samples` faces a
+        frame over `steps_per_frame` Adam steps, and after warm_frames
+        frames the network ends uncached first hits."""
+        self._check(self._lib.vgi_set_mlp_cache(self._h, 1 if enable else 0, warm_frames, samples, steps_per_frame, float(lr)))
+
+    def mlp_stats(self) -> dict:
+        st = MlpStatus()
+        self._check(self._lib.vgi_mlp_stats(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in MlpStatus._fields_}
 
     def reference_fp64(self, tasks: np.ndarray, samples: int, seed: int = 1):
         """FP64 converged reference per FaceTask: (mean rgb, mean square rgb, known)."""

@@ -268,6 +268,37 @@ int vgi_mlp_forward(vgi_ctx* ctx, const float* features, uint32_t n, float* out4
  * writes the loss before the step. vgi_mlp_set_weights resets Adam. */
 int vgi_mlp_gradients(vgi_ctx* ctx, const float* features, const float* targets4, uint32_t n, float* grads, float* loss);
 int vgi_mlp_train(vgi_ctx* ctx, const float* features, const float* targets4, uint32_t n, float lr, float* loss);
+/* The network's 96 inputs for n faces (their voxel, face and material), as
+ * the frame's queries and training rows compute them: per axis of the face
+ * centre x (voxels, normalised to [0, 1] over the loaded regions), sin and
+ * cos of pi 2^k x for k = 0..11 (24 per axis), the face one-hot (72..77),
+ * the material's diffuse albedo (78..80), zeros. Synchronous. */
+int vgi_mlp_encode(vgi_ctx* ctx, const vgi_face* faces, uint32_t n, float* features);
+/* MLP cache mode of vgi_frame. Every frame trains the network online on
+ * `samples` faces (at most 2^22), split over `steps_per_frame` Adam steps
+ * (learning rate lr) of samples / steps_per_frame faces each (input: the
+ * face's encoding; target: the frame's traced mean of the quantity the world
+ * cache accumulates; faces without a known sample are skipped). The first
+ * `warm_frames` frames trace plainly and draw the faces from their own
+ * results. Later frames end every first hit that the world cache does not
+ * answer with the network's prediction for the hit face instead of
+ * continuing the path (the wavefront layout with one diffuse hit), and
+ * train on those hit faces: `samples` of the frame's queries are traced as
+ * faces of their own, 4 paths each. In the single-kernel layout frames trace
+ * plainly. Resets the frame count; the weights and Adam state stay. */
+int vgi_set_mlp_cache(vgi_ctx* ctx, int enable, uint32_t warm_frames, uint32_t samples, uint32_t steps_per_frame, float lr);
+typedef struct vgi_mlp_status {
+    uint32_t frames;       /* frames traced since vgi_set_mlp_cache */
+    uint32_t steps;        /* Adam steps taken since vgi_mlp_set_weights */
+    uint32_t terminating;  /* the next frame ends first hits with the network */
+    uint32_t queries;      /* network queries of the last terminating frame */
+    float loss;            /* loss of the last training batch */
+    uint32_t error;        /* nonzero: a tensor-core wait ran out */
+    float query_ms;        /* with vgi_set_timing: the last terminating frame's */
+    float train_ms;        /*   query launch and its training, CUDA-event times */
+} vgi_mlp_status;
+/* Synchronous. */
+int vgi_mlp_stats(vgi_ctx* ctx, vgi_mlp_status* out);
 
 /* ---- read-back: bounded snapshots (complete_readback, src/gpu.rs:1024-1170) --- */
 int vgi_read_results(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words24);

@@ -23,6 +23,7 @@
 #include <map>
 #include <atomic>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 namespace orc {
@@ -43,6 +44,9 @@ struct Model {
     const uint32_t* state;    // 36 words per slot (9 uint4)
     const uint32_t* index;    // uint4 words; [0] = (mask, probes, 0, 0)
     orc_pipeline pipe;
+    // MLP termination: the network's value for each (voxel, face) a path may
+    // hit; an uncached hit takes it in place of the continuation.
+    const struct PredictedFaces* predicted = nullptr;
 };
 
 struct Counters {
@@ -106,6 +110,14 @@ static i3 negative_extents(uint32_t b) { return i3{(int32_t)(b & 3u), (int32_t)(
 static i3 positive_extents(uint32_t b) { return i3{(int32_t)((b >> 2) & 3u), (int32_t)((b >> 6) & 3u), (int32_t)((b >> 10) & 3u)}; }
 
 struct F4 { float x, y, z, w; };
+struct PredictedFaces {
+    std::unordered_map<uint64_t, F4> map;
+    mutable std::atomic<uint64_t> misses{0};  // hits on faces the table does not hold
+    mutable std::atomic<uint64_t> last_miss{0};
+};
+static uint64_t face_key(int32_t x, int32_t y, int32_t z, uint32_t face) {
+    return ((uint64_t)(uint16_t)x) | ((uint64_t)(uint16_t)y << 16) | ((uint64_t)(uint16_t)z << 32) | ((uint64_t)face << 48);
+}
 
 // voxel_traversal.wgsl:90-107
 static F4 advance_box(f3 p, f3 d, i3 cell, i3 ng, i3 ps, float size) {
@@ -642,6 +654,20 @@ static PathState advance_path(Ctx& x, PathState state, uint32_t stream, uint32_t
             state.result.energy.value = f4add(state.result.energy.value, f4mul(state.throughput, term));
             break;
         }
+        if (x.m.predicted) {
+            // The GPU's MLP cache mode (no reference counterpart): the
+            // network's prediction for the hit face ends the path.
+            auto it = x.m.predicted->map.find(face_key(hit.voxel.x, hit.voxel.y, hit.voxel.z, face_index_of(hit.normal)));
+            const bool missing = it == x.m.predicted->map.end();
+            if (missing) {
+                x.m.predicted->misses += 1;
+                x.m.predicted->last_miss = face_key(hit.voxel.x, hit.voxel.y, hit.voxel.z, face_index_of(hit.normal));
+            }
+            const F4 value = missing ? F4{0, 0, 0, 0} : it->second;
+            F4 term = f4add(f4muls(emission, mis), f4mul(diffuse, f4add(direct.value, value)));
+            state.result.energy.value = f4add(state.result.energy.value, f4mul(state.throughput, term));
+            break;
+        }
         Energy nee;
         if (terminal && step + 1u == steps) nee = sample_terminal_emission(x, hit.position, hit.normal, stream, sequence, bounce);
         else nee = sample_emitter(x, hit.position, hit.normal, stream, sequence, bounce + 1u);
@@ -847,12 +873,15 @@ extern "C" {
 // samples l, l+L, ... and lane 0 sums the lanes in order, as the cooperative
 // kernel does; L = 1 is the serial kernel. `state` (36 words per slot) and
 // `index` (face index words) may be null for a cacheless trace.
-int orc_trace_faces(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells,
-                    const float* params, const float* materials, const float* lights, const uint32_t* emitters,
-                    const uint32_t* state, const uint32_t* index, const uint32_t* tasks, uint32_t n_tasks,
-                    const orc_pipeline* pipe, uint32_t* results, orc_counters* counters, int threads) {
+static uint64_t g_predicted_misses = 0, g_last_miss = 0;
+
+static int trace_faces_impl(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells,
+                            const float* params, const float* materials, const float* lights, const uint32_t* emitters,
+                            const uint32_t* state, const uint32_t* index, const uint32_t* tasks, uint32_t n_tasks,
+                            const orc_pipeline* pipe, uint32_t* results, orc_counters* counters, int threads,
+                            const PredictedFaces* predicted) {
     Geometry g = make_geometry(directory, slots, headers, cells, params);
-    Model m{params, materials, lights, emitters, state, index, *pipe};
+    Model m{params, materials, lights, emitters, state, index, *pipe, predicted};
     uint32_t lanes = pipe->lanes == 0 ? 1 : pipe->lanes;
     Counters total;
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
@@ -891,6 +920,40 @@ int orc_trace_faces(const int32_t* directory, uint64_t slots, const uint32_t* he
         counters->traverse_bytes = total.traverse_bytes;
     }
     return 0;
+}
+
+int orc_trace_faces(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells,
+                    const float* params, const float* materials, const float* lights, const uint32_t* emitters,
+                    const uint32_t* state, const uint32_t* index, const uint32_t* tasks, uint32_t n_tasks,
+                    const orc_pipeline* pipe, uint32_t* results, orc_counters* counters, int threads) {
+    return trace_faces_impl(directory, slots, headers, cells, params, materials, lights, emitters, state, index, tasks, n_tasks, pipe,
+                            results, counters, threads, nullptr);
+}
+
+// orc_trace_faces with the MLP cache mode's termination: keys4 = (voxel
+// xyz, face) and values3 = the network's rgb for each face a path may hit.
+int orc_trace_faces_predicted(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells,
+                              const float* params, const float* materials, const float* lights, const uint32_t* emitters,
+                              const uint32_t* state, const uint32_t* index, const uint32_t* tasks, uint32_t n_tasks,
+                              const orc_pipeline* pipe, const int32_t* keys4, const float* values3, uint32_t n_keys, uint32_t* results,
+                              orc_counters* counters, int threads) {
+    PredictedFaces predicted;
+    predicted.map.reserve(n_keys);
+    for (uint32_t k = 0; k < n_keys; ++k)
+        predicted.map[face_key(keys4[k * 4], keys4[k * 4 + 1], keys4[k * 4 + 2], (uint32_t)keys4[k * 4 + 3])] =
+            F4{values3[k * 3], values3[k * 3 + 1], values3[k * 3 + 2], 0.0f};
+    const int rc = trace_faces_impl(directory, slots, headers, cells, params, materials, lights, emitters, state, index, tasks, n_tasks,
+                                    pipe, results, counters, threads, &predicted);
+    g_predicted_misses = predicted.misses.load();
+    g_last_miss = predicted.last_miss.load();
+    return rc;
+}
+
+// Hits of the last orc_trace_faces_predicted call on faces its table did not
+// hold (they took zero), and the key (x | y << 16 | z << 32 | face << 48) of one.
+uint64_t orc_predicted_misses(uint64_t* last_key) {
+    if (last_key) *last_key = g_last_miss;
+    return g_predicted_misses;
 }
 
 // One ray through trace_domain_limited (for traversal parity tests):

@@ -48,6 +48,8 @@ _SIG = {
     "orc_scene_top_level": (_INT, [_P, _P]),
     "orc_canonical": (_INT, [_P, _U64, _P, _P, _U64, _P, _U32, _P]),
     "orc_trace_faces": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _INT]),
+    "orc_trace_faces_predicted": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _U32, _P, _P, _INT]),
+    "orc_predicted_misses": (_U64, [_P]),
     "orc_trace_ray": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P]),
     "orc_advance_box": (_INT, [_P, _P]),
     "orc_sample_1d": (_F, [_U32, _U32, _U32]),
@@ -210,7 +212,14 @@ def face_index(faces):
     return out[: n * 4].reshape(-1, 4)
 
 
-def trace_faces(geometry, params, materials, lights, emitter_words, tasks, pipe: Pipeline, state=None, index=None, threads=0):
+def trace_faces(geometry, params, materials, lights, emitter_words, tasks, pipe: Pipeline, state=None, index=None, threads=0,
+                predicted=None):
+    """orc_trace_faces; with predicted = (keys (n, 4): voxel xyz, face;
+    values (n, 3) rgb), an uncached hit takes the predicted value and ends
+    the path (the GPU's MLP cache mode)."""
+    if predicted is not None:
+        return _trace_faces_predicted(geometry, params, materials, lights, emitter_words, tasks, pipe, state, index, threads,
+                                      predicted)
     d, h, cl, _ = geometry
     d = c(d, np.int32)
     h = c(h, np.uint32)
@@ -227,6 +236,34 @@ def trace_faces(geometry, params, materials, lights, emitter_words, tasks, pipe:
                                ptr(t), t.shape[0], ctypes.byref(pipe), ptr(out), ctypes.byref(cnt), threads)
     assert rc == 0
     return out, cnt.as_dict()
+
+
+def _trace_faces_predicted(geometry, params, materials, lights, emitter_words, tasks, pipe, state, index, threads, predicted):
+    d, h, cl, _ = geometry
+    d = c(d, np.int32)
+    h = c(h, np.uint32)
+    cl = c(cl, np.uint32) if len(cl) else np.zeros(1, np.uint32)
+    t = c(tasks, np.uint32).reshape(-1, 8)
+    keys = c(predicted[0], np.int32).reshape(-1, 4)
+    values = c(predicted[1], np.float32).reshape(-1, 3)
+    assert keys.shape[0] == values.shape[0]
+    out = np.zeros((t.shape[0], 24), np.uint32)
+    cnt = Counters()
+    lights = c(lights, np.float32).reshape(-1)
+    if lights.size == 0:
+        lights = np.zeros(12, np.float32)
+    rc = lib().orc_trace_faces_predicted(ptr(d), d.size // 4, ptr(h), ptr(cl), ptr(c(params, np.float32)),
+                                         ptr(c(materials, np.float32)), ptr(lights), ptr(c(emitter_words, np.uint32)),
+                                         ptr(None if state is None else c(state, np.uint32)),
+                                         ptr(None if index is None else c(index, np.uint32)), ptr(t), t.shape[0], ctypes.byref(pipe),
+                                         ptr(keys), ptr(values), keys.shape[0], ptr(out), ctypes.byref(cnt), threads)
+    assert rc == 0
+    d = cnt.as_dict()
+    last = ctypes.c_uint64(0)
+    d["predicted_misses"] = int(lib().orc_predicted_misses(ctypes.byref(last)))
+    k = last.value
+    d["last_miss"] = (k & 0xffff, (k >> 16) & 0xffff, (k >> 32) & 0xffff, k >> 48)
+    return out, d
 
 
 def controls_words(n, samples, clock_ms, transport, batch_id=1, n_events=0):
@@ -285,14 +322,16 @@ class Frames:
         self.batch_id = 1
         self.results = np.zeros((n, 24), np.uint32)
 
-    def frame(self, samples, clock_ms=0):
+    def frame(self, samples, clock_ms=0, predicted=None, pipe=None):
+        """One frame; `predicted` and `pipe` as trace_faces takes them (the
+        MLP cache mode's termination and its one-hit pipeline)."""
         ctl = controls_words(self.n, samples, clock_ms, self.transport, self.batch_id)
         L = lib()
         L.orc_begin_trace(ptr(self.state), ptr(self.meta), ptr(self.tasks), ptr(self.slots), self.n, ptr(ctl))
         L.orc_mark_changed(ptr(self.state), ptr(self.meta), ptr(self.slots), self.n, ptr(ctl))
         params = self.params_fn(self.n, samples)
-        out, cnt = trace_faces(self.geometry, params, self.materials, self.lights, self.emitter_words, self.tasks, self.pipe,
-                               self.state, self.index, self.threads)
+        out, cnt = trace_faces(self.geometry, params, self.materials, self.lights, self.emitter_words, self.tasks, pipe or self.pipe,
+                               self.state, self.index, self.threads, predicted)
         L.orc_accumulate(ptr(self.state), ptr(self.meta), ptr(self.checkpoint), ptr(out), ptr(self.slots), self.n, ptr(ctl))
         self.results = out
         self.batch_id = (self.batch_id + 1) & 0x0FFFFFFF or 1
