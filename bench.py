@@ -12,6 +12,13 @@ at cached faces, and accumulates the result (prepare, trace, accumulate).
 Printed metric: rays/s (one ray = one trace_domain_limited call, counted by
 the library's counting pass over the same frame). ``e2e`` is the same metric
 through the C ABI with pinned host task/result buffers copied every frame.
+``mlp_cache`` compares the MLP cache form on the same terrain: 2 paths a
+face a frame, first hits that the world cache does not answer end with the
+network's prediction, online training inside each frame; it runs from an
+empty cache and an untrained network until its relMSE against the FP64
+reference reaches the plain trace's (after the plain run's frames), and
+reports both forms' ms/frame, rays/s and time to that relMSE, with the
+query kernel's tensor-core throughput.
 ``--impl reference`` times the CPU oracle (the restatement of the
 reference's algorithm; the reference itself is Rust/WGSL and has no CPU
 path) on the box's host cores.
@@ -58,13 +65,15 @@ def make_scene(seed):
     return coords, vox, m.words(), sun.words(), faces, transport
 
 
-def measured_peak():
+def measured_peak(key="hbm_gbs", fallback=6650.0):
+    """A peak from MEASURED_PEAKS.json (HBM copy GB/s, or cuBLAS bf16 TFLOP/s
+    as a burst), else the pool's earlier measurement."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         with open(path) as f:
-            return float(json.load(f)["hbm_gbs"]), "measured"
+            return float(json.load(f)[key]), "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return fallback, "fallback"
 
 
 def profiled_traffic():
@@ -137,27 +146,131 @@ def lane_use(census):
     return {"queued": lp[0] / max(wp[0], 1), "drain": lp[1] / max(wp[1], 1), "drain_pass_share": wp[1] / total}
 
 
-def relmse(g, faces, frames, n_faces=4096, spp=16384):
-    """Relative MSE of the world cache's accumulated face means against the
-    FP64 converged reference on a seeded face sample, in luminance:
-    mean((L - L_ref)^2 / (L_ref^2 + 0.01)). The reference's own noise floor
-    (its variance of the mean in the same units) is reported beside it."""
-    rng = np.random.default_rng(17)
-    sel = np.sort(rng.choice(faces.shape[0], size=min(n_faces, faces.shape[0]), replace=False))
+LUMA = np.array([0.2126, 0.7152, 0.0722])
+
+
+def fp64_reference(g, faces, n_faces=4096, spp=16384):
+    """The FP64 converged reference (unbiased path tracing, roulette, no
+    cache) on a seeded sample of the faces; it depends on the geometry and
+    model only, so one run serves every relMSE of the same scene."""
     import vgi
 
+    rng = np.random.default_rng(17)
+    sel = np.sort(rng.choice(faces.shape[0], size=min(n_faces, faces.shape[0]), replace=False))
     t0 = time.perf_counter()
     ref, second, known = g.reference_fp64(vgi.tasks_for(faces[sel]), spp, seed=23)
     seconds = time.perf_counter() - t0
-    w = np.array([0.2126, 0.7152, 0.0722])
-    est = g.read_state()[sel, 0:3].view(np.float32).astype(np.float64)
-    lr, le = ref @ w, est @ w
-    var_ref = (np.maximum(second - ref ** 2, 0.0) / np.maximum(known, 1)[:, None]) @ (w * w)
-    return {"value": float(np.mean((le - lr) ** 2 / (lr ** 2 + 0.01))), "faces": int(sel.size), "reference_spp": spp,
-            "frames_accumulated": frames, "reference_noise": float(np.mean(var_ref / (lr ** 2 + 0.01))),
-            "reference_seconds": round(seconds, 3),
+    lr = ref @ LUMA
+    var_ref = (np.maximum(second - ref ** 2, 0.0) / np.maximum(known, 1)[:, None]) @ (LUMA * LUMA)
+    return {"sel": sel, "l_ref": lr, "spp": spp, "seconds": seconds, "noise": float(np.mean(var_ref / (lr ** 2 + 0.01)))}
+
+
+def relmse_now(g, ref):
+    """Relative MSE of the world cache's accumulated face means against the
+    reference, in luminance: mean((L - L_ref)^2 / (L_ref^2 + 0.01))."""
+    est = g.read_state()[ref["sel"], 0:3].view(np.float32).astype(np.float64)
+    return float(np.mean((est @ LUMA - ref["l_ref"]) ** 2 / (ref["l_ref"] ** 2 + 0.01)))
+
+
+def relmse(g, ref, frames):
+    return {"value": relmse_now(g, ref), "faces": int(ref["sel"].size), "reference_spp": ref["spp"], "frames_accumulated": frames,
+            "reference_noise": ref["noise"], "reference_seconds": round(ref["seconds"], 3),
             "definition": "luminance, mean over faces of (L - L_ref)^2 / (L_ref^2 + 0.01); "
                           "L = world-cache mean after the frames run, L_ref = FP64 unbiased path tracing (roulette, no cache)"}
+
+
+# MLP cache arm: spp, plain warm-up frames, training samples a frame, Adam steps a frame, learning rate.
+MLP_SPP, MLP_WARM, MLP_SAMPLES, MLP_STEPS, MLP_LR = 2, 8, 65536, 16, 1e-2
+# Inference FLOPs per query at the network's real widths (81 inputs, 3 outputs):
+# 2 (81*64 + 3*64*64 + 64*3); the kernel computes the padded 96 x 16 shape.
+MLP_QUERY_FLOP = 2 * (81 * 64 + 3 * 64 * 64 + 64 * 3)
+
+
+def mlp_comparison(g, faces, ref, stream, flush, plain, clock, max_frames):
+    """The MLP cache form against the plain trace at equal relMSE vs FP64: the
+    MLP form starts from an empty cache and an untrained network (seeded
+    init), runs graph-replayed frames (training inside them) until its relMSE
+    reaches the plain trace's, and reports its frame time, frames and total
+    time beside the plain trace's; frames are CUDA-event timed, L2 flushed
+    between them outside the timed pair."""
+    import torch
+
+    import vgi
+
+    rng = np.random.default_rng(6)
+    init = np.concatenate([(rng.normal(0.0, 1.0 / np.sqrt(i), size=(i, o)) * 0.5).astype(np.float32).reshape(-1)
+                           for i, o in vgi.GpuTracer.MLP_LAYERS])
+    g.set_faces(faces)
+    g.mlp_set_weights(init)
+    g.set_mlp_cache(True, warm_frames=MLP_WARM, samples=MLP_SAMPLES, steps_per_frame=MLP_STEPS, lr=MLP_LR)
+    g.set_timing(False)
+    g.set_graph(True)
+    target = plain["relmse"]
+    curve, frame_ms, reached = [], [], None
+    at_equal_frames = at_equal_time = None
+    total = 0.0
+    for f in range(max_frames):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(f))
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+        g.frame(MLP_SPP, clock)
+        clock += 16
+        with torch.cuda.stream(stream):
+            e.record(stream)
+        e.synchronize()
+        frame_ms.append(s.elapsed_time(e))
+        total += frame_ms[-1]
+        value = relmse_now(g, ref) if (f + 1) % 2 == 0 or f + 1 == plain["frames"] else None
+        if value is not None:
+            curve.append([f + 1, round(total, 2), round(value, 6)])
+            if f + 1 == plain["frames"]:
+                at_equal_frames = value
+            if at_equal_time is None and total >= plain["frames"] * plain["ms_per_frame"]:
+                at_equal_time = value
+            if reached is None and value <= target:
+                reached = {"frames": f + 1, "ms": total}
+        if reached is not None and f + 1 >= plain["frames"] and at_equal_time is not None:
+            break
+    g.set_graph(False)
+    stats = g.mlp_stats()
+    # One directly launched, event-marked frame for the query and training times.
+    g.set_timing(True)
+    g.frame(MLP_SPP, clock)
+    clock += 16
+    g.sync()
+    timed = g.mlp_stats()
+    census = g.census(MLP_SPP)
+    g.set_mlp_cache(False)
+    steady_ms = float(np.median(frame_ms[MLP_WARM + 2:])) if len(frame_ms) > MLP_WARM + 4 else float(np.median(frame_ms))
+    peak, peak_kind = measured_peak("bf16_tflops", 1590.0)
+    achieved = timed["queries"] * MLP_QUERY_FLOP / (timed["query_ms"] * 1e-3) / 1e12 if timed["query_ms"] > 0 else None
+    plain_total = plain["frames"] * plain["ms_per_frame"]
+    out = {
+        "config": {"spp": MLP_SPP, "warm_frames": MLP_WARM, "training_samples_per_frame": MLP_SAMPLES, "adam_steps_per_frame": MLP_STEPS,
+                   "lr": MLP_LR, "termination": "uncached first hits take the network's prediction",
+                   "network": "96 (81 used) -> 4 x 64 ReLU -> 16 (3 used, exp), BF16 tcgen05, FP32 accumulate and Adam masters"},
+        "plain": {"spp": SPP, "frames": plain["frames"], "ms_per_frame": plain["ms_per_frame"], "relmse": target,
+                  "ms_to_relmse": plain_total},
+        "mlp_ms_per_frame": steady_ms,
+        "mlp_rays_per_frame": census["rays"],
+        "mlp_rays_per_s": census["rays"] / (steady_ms * 1e-3),
+        "frames_per_s_ratio": plain["ms_per_frame"] / steady_ms,
+        "relmse_at_equal_frames": at_equal_frames,
+        "relmse_at_equal_time": at_equal_time,
+        "reached_plain_relmse": reached,
+        "speedup_at_equal_relmse": (plain_total / reached["ms"]) if reached else None,
+        "relmse_curve": curve[::4] + ([curve[-1]] if curve and (len(curve) - 1) % 4 else []),
+        "frames_run": len(frame_ms),
+        "training": {"adam_steps": stats["steps"], "last_loss": stats["loss"], "error": stats["error"]},
+        "kernel_ms": {"queries": timed["query_ms"], "training": timed["train_ms"], "queries_per_frame": timed["queries"]},
+        "tensor_roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                            "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                            "kernel": "forward_kernel<PathQueries>",
+                            "flop_per_query": MLP_QUERY_FLOP},
+    }
+    return out, clock
 
 
 def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total, budget_s=15.0):
@@ -261,6 +374,7 @@ def main():
     ap.add_argument("--impl", choices=["vgi", "reference"], default="vgi")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default layout (for profiling runs)")
+    ap.add_argument("--no-mlp", action="store_true", help="skip the MLP cache comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -300,6 +414,7 @@ def main():
     stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
+    reference = fp64_reference(g, faces) if rank == 0 else None
     clock = 0
     for _ in range(args.warmup):
         g.frame(SPP, clock)
@@ -383,12 +498,18 @@ def main():
     achieved = traverse_bytes / (traverse_ms * 1e-3) / 1e9
     traffic = profiled_traffic()
     if rank == 0:
-        quality = relmse(g, faces, args.warmup + 3 * args.steps + 1)
+        plain_frames = args.warmup + 3 * args.steps + 1
+        quality = relmse(g, reference, plain_frames)
         base = None
         if world == 1 and not args.no_cpu_baseline:
             geometry = g.geometry()
             emitters, n_emit, total = vgi.host_emitters(coords, vox, words)
             base = cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total)
+        mlp = None
+        if not args.no_mlp:
+            # After the CPU baseline, which reads the plain trace's warm state.
+            plain = {"frames": plain_frames, "ms_per_frame": graph_ms, "relmse": quality["value"]}
+            mlp, clock = mlp_comparison(g, faces, reference, stream, flush, plain, clock, max_frames=max(4 * plain_frames, 64))
         line = {
             "metric": METRIC,
             "value": total_rays / (total_ms * 1e-3),
@@ -426,6 +547,7 @@ def main():
                                  "CUDA-event time of the traversal launches, same frame"},
             "clocks": clocks,
             "relmse": quality,
+            "mlp_cache": mlp,
         }
         if base:
             line["cpu_baseline"] = base

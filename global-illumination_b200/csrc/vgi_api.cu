@@ -115,8 +115,9 @@ struct vgi_ctx {
     DevBuf<uint32_t> mlp_error;               // [0] API calls and training, [1] the frames' queries
     DevBuf<uint8_t> mlp_image_b;              // W (rows = inputs): B operand of the backward pass
     DevBuf<float> mlp_adam;                   // Adam first and second moments, 2 x 19456
-    DevBuf<float> mlp_grads;                  // 19456 gradients + the loss
-    DevBuf<uint32_t> mlp_steps;               // Adam steps taken (a device word: a frame graph replays it)
+    DevBuf<float> mlp_grads;                  // 19456 gradients + the loss of the last batch
+    DevBuf<float> mlp_partials;               // per training CTA: gradient sums + loss
+    DevBuf<uint32_t> mlp_steps;               // Adam steps taken, blocks done (device words: a frame graph replays them)
     DevBuf<float4> w_mlp_queue;               // 2 per path: the frame's network queries
     DevBuf<float> mlp_features;               // training rows of a frame (batch x steps x 96)
     DevBuf<float4> mlp_targets;
@@ -534,7 +535,7 @@ int vgi_destroy(vgi_ctx* c) {
     c->v_receivers.release(); c->v_paths.release(); c->v_conts.release(); c->v_estimates.release(); c->v_events.release();
     c->v_scratch.release(); c->v_queue.release();
     c->mlp_master.release(); c->mlp_image.release(); c->mlp_error.release();
-    c->mlp_image_b.release(); c->mlp_adam.release(); c->mlp_grads.release(); c->mlp_steps.release();
+    c->mlp_image_b.release(); c->mlp_adam.release(); c->mlp_grads.release(); c->mlp_steps.release(); c->mlp_partials.release();
     c->w_mlp_queue.release(); c->mlp_features.release(); c->mlp_targets.release();
     c->mlp_train_tasks.release(); c->mlp_train_results.release(); c->mlp_query_count.release();
     c->counters.release();
@@ -1377,18 +1378,20 @@ int vgi_mlp_set_weights(vgi_ctx* c, const float* master, uint32_t count) {
     VGI_CUDA(c, c->mlp_master.reserve(count));
     VGI_CUDA(c, c->mlp_image.reserve(mlp_image_bytes()));
     VGI_CUDA(c, c->mlp_error.reserve(2));
-    VGI_CUDA(c, c->mlp_steps.reserve(1));
+    VGI_CUDA(c, c->mlp_steps.reserve(2));
     VGI_CUDA(c, c->mlp_image_b.reserve(mlp_image_bytes()));
     VGI_CUDA(c, mlp_set_attributes());
     int sms = 148;
     VGI_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
     c->mlp_sms = (uint32_t)sms;
     c->mlp_ctas = (uint32_t)sms * 3u;  // 62 KB of shared memory per forward CTA
+    VGI_CUDA(c, c->mlp_partials.reserve((size_t)sms * mlp_partial_floats()));
     VGI_CUDA(c, c->mlp_adam.reserve((size_t)count * 2));
     VGI_CUDA(c, c->mlp_grads.reserve((size_t)count + 1));
     VGI_CUDA(c, cudaMemcpyAsync(c->mlp_master.ptr, master, (size_t)count * 4, cudaMemcpyHostToDevice, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_adam.ptr, 0, (size_t)count * 8, c->stream));
-    VGI_CUDA(c, cudaMemsetAsync(c->mlp_steps.ptr, 0, 4, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_steps.ptr, 0, 8, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_grads.ptr, 0, (size_t)(count + 1) * 4, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 8, c->stream));
     launch_mlp_pack(c->mlp_master.ptr, c->mlp_image.ptr, c->stream);
     launch_mlp_pack_backward(c->mlp_master.ptr, c->mlp_image_b.ptr, c->stream);
@@ -1426,13 +1429,14 @@ int vgi_mlp_forward(vgi_ctx* c, const float* features, uint32_t n, float* out4) 
 
 // Gradients of the relative-luminance loss over one batch already on the
 // device, into mlp_grads (19456 gradients, then the loss).
-static int mlp_batch_gradients(vgi_ctx* c, const float* features, const float4* targets, uint32_t n) {
-    const uint32_t count = mlp_weight_count();
-    VGI_CUDA(c, cudaMemsetAsync(c->mlp_grads.ptr, 0, (size_t)(count + 1) * 4, c->stream));
-    VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 4, c->stream));
-    VGI_CUDA(c, launch_mlp_train(features, targets, n, c->mlp_image.ptr, c->mlp_image_b.ptr, c->mlp_grads.ptr, c->mlp_grads.ptr + count,
-                                 c->mlp_error.ptr, c->mlp_sms, c->stream));
-    return VGI_OK;
+// The training kernel over one device-resident batch: per-CTA partial rows.
+// Returns the number of rows.
+static uint32_t mlp_batch_partials(vgi_ctx* c, const float* features, const float4* targets, uint32_t n, int* rc) {
+    *rc = VGI_OK;
+    const cudaError_t e = launch_mlp_train(features, targets, n, c->mlp_image.ptr, c->mlp_image_b.ptr, c->mlp_partials.ptr,
+                                           c->mlp_error.ptr, c->mlp_sms, c->stream);
+    if (e != cudaSuccess) *rc = fail(c, VGI_ERR_CUDA, std::string("MLP training launch: ") + cudaGetErrorString(e));
+    return mlp_train_parts(n, c->mlp_sms);
 }
 
 static int mlp_upload_batch(vgi_ctx* c, const float* features, const float* targets4, uint32_t n, DevBuf<float>& in, DevBuf<float4>& y) {
@@ -1459,20 +1463,24 @@ int vgi_mlp_gradients(vgi_ctx* c, const float* features, const float* targets4, 
     DevBuf<float> in;
     DevBuf<float4> y;
     if (int e = mlp_upload_batch(c, features, targets4, n, in, y)) return e;
-    if (int e = mlp_batch_gradients(c, in.ptr, y.ptr, n)) return e;
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 4, c->stream));
+    int rc = VGI_OK;
+    const uint32_t parts = mlp_batch_partials(c, in.ptr, y.ptr, n, &rc);
+    if (rc != VGI_OK) return rc;
+    launch_mlp_reduce(c->mlp_partials.ptr, parts, c->mlp_grads.ptr, c->mlp_grads.ptr + mlp_weight_count(), c->stream);
+    VGI_CUDA(c, cudaGetLastError());
     VGI_CUDA(c, cudaMemcpyAsync(grads, c->mlp_grads.ptr, (size_t)mlp_weight_count() * 4, cudaMemcpyDeviceToHost, c->stream));
     return mlp_read_status(c, loss);
 }
 
 // One Adam step over a device-resident batch; the images are repacked.
 static int mlp_train_step(vgi_ctx* c, const float* features, const float4* targets, uint32_t n, float lr) {
-    if (int e = mlp_batch_gradients(c, features, targets, n)) return e;
+    int rc = VGI_OK;
+    const uint32_t parts = mlp_batch_partials(c, features, targets, n, &rc);
+    if (rc != VGI_OK) return rc;
     const uint32_t count = mlp_weight_count();
-    launch_mlp_step(c->mlp_steps.ptr, c->stream);
-    launch_mlp_adam(c->mlp_master.ptr, c->mlp_adam.ptr, c->mlp_adam.ptr + count, c->mlp_grads.ptr, lr, 0.9f, 0.99f, 1e-8f, c->mlp_steps.ptr,
-                    c->stream);
-    launch_mlp_pack(c->mlp_master.ptr, c->mlp_image.ptr, c->stream);
-    launch_mlp_pack_backward(c->mlp_master.ptr, c->mlp_image_b.ptr, c->stream);
+    launch_mlp_adam(c->mlp_master.ptr, c->mlp_adam.ptr, c->mlp_adam.ptr + count, c->mlp_partials.ptr, parts, lr, 0.9f, 0.99f, 1e-8f,
+                    c->mlp_steps.ptr, c->mlp_image.ptr, c->mlp_image_b.ptr, c->mlp_grads.ptr + count, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     return VGI_OK;
 }
@@ -1587,6 +1595,7 @@ int vgi_mlp_train(vgi_ctx* c, const float* features, const float* targets4, uint
     DevBuf<float> in;
     DevBuf<float4> y;
     if (int e = mlp_upload_batch(c, features, targets4, n, in, y)) return e;
+    VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 4, c->stream));
     if (int e = mlp_train_step(c, in.ptr, y.ptr, n, lr)) return e;
     return mlp_read_status(c, loss);
 }

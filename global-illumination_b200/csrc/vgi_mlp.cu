@@ -99,6 +99,18 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t phase) {
     return false;
 }
 
+// One-dimensional bulk copy global -> this CTA's shared memory on the TMA
+// engine (no multicast); completion is counted on the mbarrier in bytes.
+// Addresses and size are multiples of 16 bytes.
+__device__ __forceinline__ void bulk_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst), "l"(src),
+                 "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
 // Reads 16 consecutive FP32 columns of this thread's TMEM lane.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     uint32_t r[16];
@@ -274,12 +286,13 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, cons
     const uint32_t tiles = (n + kRows - 1) / kRows;
     if (blockIdx.x >= tiles) return;  // uniform per CTA: nothing allocated yet
 
-    for (uint32_t i = tid; i < kImageBytes / 16; i += kThreads)
-        reinterpret_cast<uint4*>(weights)[i] = reinterpret_cast<const uint4*>(image)[i];
+    const uint32_t bar_addr = smem_u32(bar);
     if (tid == 0) {
         *abort_flag = 0u;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1u));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_addr), "r"(1u));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        bulk_expect(bar_addr, kImageBytes);
+        bulk_load(smem_u32(weights), image, kImageBytes, bar_addr);
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTmemColumns));
@@ -290,10 +303,16 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, cons
     fence_after();
     const uint32_t tmem = *tmem_slot;
     const uint32_t lane_base = tmem + ((warp * 32u) << 16);
-    const uint32_t bar_addr = smem_u32(bar);
-    uint32_t phase = 0;
+    // The weight image (phase 0 of the mbarrier), then one phase per layer.
+    if (!bar_wait(bar_addr, 0u)) {
+        atomicOr(abort_flag, 1u);
+        atomicOr(error, 1u);
+    }
+    uint32_t phase = 1;
+    __syncthreads();
+    const uint32_t first_tile = *abort_flag ? tiles : blockIdx.x;
 
-    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    for (uint32_t t = first_tile; t < tiles; t += gridDim.x) {
         const uint32_t row = t * kRows + tid;
         rows.stage(tile, tid, row);
         bool ok = true;
@@ -407,7 +426,6 @@ __global__ void query_targets_kernel(const uint4* results, uint32_t n, float4* t
     targets[k] = target;
 }
 
-__global__ void step_kernel(uint32_t* step) { *step += 1u; }
 
 // ---- training ------------------------------------------------------------
 // One fused kernel per batch: every CTA (one per SM, 512 TMEM columns) runs
@@ -418,58 +436,85 @@ __global__ void step_kernel(uint32_t* step) { *step += 1u; }
 //     dz_{l-1} = dh_l * (h_l > 0)
 // h_l (the input of layer l) is kept transposed (features x samples) for the
 // dW products; dz_l is kept both as the next A operand (samples x out_l) and
-// transposed (out_l x samples). The hidden h_l^T tiles hold 64 feature rows;
-// an M = 128 product also reads the 64 rows after them (the next buffer),
-// which only feed accumulator rows 64-127, never read out (the last hidden
-// tile's extra rows are the dz^T tile, the input tile's are h_1^T). The loss is the
-// relative luminance MSE sum_c (p_c - y_c)^2 / (lum(p)^2 + 0.01) / B with
-// lum(p) held constant, p = exp(z). Gradients are summed into `grads` (same
-// order as the FP32 masters) with one atomic per weight per CTA.
-constexpr int kHT0 = kIn * kRows * 2;              // 24576
-constexpr int kHT = kHidden * kRows * 2;           // 16384
+// transposed (out_l x samples). The transposed tiles put the K-neighbouring
+// core matrices 144 bytes apart (not 128), so the four 8-thread groups of a
+// warp that write one feature row for 32 samples land in different banks.
+// The hidden h_l^T tiles hold 64 feature rows; an M = 128 product also reads
+// the 64 rows after them (the next buffer), which only feed accumulator rows
+// 64-127, never read out (the last hidden tile's extra rows are the dz^T
+// tile, the input tile's are h_1^T). The loss is the relative luminance MSE
+// sum_c (p_c - y_c)^2 / (lum(p)^2 + 0.01) / B with lum(p) held constant,
+// p = exp(z). Each CTA writes its gradient sums and loss to its own row of
+// `partials` (19456 + 1 floats); adam_kernel / reduce_kernel sum the rows in
+// CTA order, so the result does not depend on timing.
+constexpr uint32_t kLboT = 144, kSboT = 16 * kLboT;   // transposed tiles: K = 128 samples
+constexpr uint32_t kHT0 = (kIn / 8) * kSboT;           // 27648
+constexpr uint32_t kHT = (kHidden / 8) * kSboT;        // 18432
 constexpr uint32_t kWF = 0, kWB = kImageBytes, kAT = 2 * kImageBytes, kH0 = kAT + kABytes;
 constexpr uint32_t kH1 = kH0 + kHT0, kDZ = kH1 + 4 * kHT, kBarT = kDZ + kHT;
-constexpr int kTrainSmem = kBarT + 64;             // 208,960 bytes
+constexpr int kTrainSmem = kBarT + 64;                 // 222,272 bytes
 constexpr int kTrainColumns = 512;
+// A CTA's row of partials: gradient sums, its loss at [kWeights], padded to
+// a multiple of 4 floats so that every row's float4 stores stay aligned.
+constexpr int kPartial = (kWeights + 1 + 3) / 4 * 4;
+static_assert(kPartial % 4 == 0 && kWeights % 4 == 0, "float4-aligned partial rows");
 __host__ __device__ constexpr uint32_t grad_column(int l) { return 64u + 64u * (uint32_t)l; }
 __host__ __device__ constexpr uint32_t ht_offset(int l) { return l == 0 ? kH0 : kH1 + (uint32_t)(l - 1) * kHT; }
+// Element (row, sample) of a transposed tile.
+__host__ __device__ constexpr uint32_t t_offset(uint32_t row, uint32_t col) {
+    return (row >> 3) * kSboT + (col >> 3) * kLboT + (row & 7u) * 16u + (col & 7u) * 2u;
+}
+// The M = 128 reads of the last transposed tile end at the mbarrier.
+static_assert(kH1 + 3 * kHT + 16 * kSboT == kBarT, "transposed-tile overrun leaves the tiles");
+static_assert(kH0 + 16 * kSboT <= kBarT, "input-tile overrun leaves the tiles");
+static_assert(kTrainSmem <= 232448, "shared memory per CTA");
+
+// Positions of master weight i (layer l, input k, output n) in the forward
+// image (rows = out, K = in) and the backward image (rows = in, K = out).
+__device__ __forceinline__ void image_positions(int i, uint32_t& fwd, uint32_t& bwd) {
+    int l = 0;
+    while (l + 1 < kLayers && i >= weight_offset(l + 1)) ++l;
+    const int local = i - weight_offset(l);
+    const int k = local / out_dim(l), n = local % out_dim(l);
+    fwd = (uint32_t)weight_offset(l) * 2u + core_offset(n, k, in_dim(l));
+    bwd = (uint32_t)weight_offset(l) * 2u + core_offset(k, n, out_dim(l));
+}
 
 // FP32 master [in][out] -> BF16 image with rows = in, K = out: the B
 // operand of dh = dz W^T.
 __global__ void pack_backward_kernel(const float* master, uint8_t* image) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kWeights) return;
-    int l = 0;
-    while (l + 1 < kLayers && i >= weight_offset(l + 1)) ++l;
-    const int local = i - weight_offset(l);
-    const int k = local / out_dim(l), n = local % out_dim(l);
-    *reinterpret_cast<__nv_bfloat16*>(image + weight_offset(l) * 2 + core_offset(k, n, out_dim(l))) = __float2bfloat16_rn(master[i]);
+    uint32_t fwd, bwd;
+    image_positions(i, fwd, bwd);
+    *reinterpret_cast<__nv_bfloat16*>(image + bwd) = __float2bfloat16_rn(master[i]);
 }
 
 __device__ __forceinline__ void store_t(uint8_t* smem, uint32_t base, uint32_t row, uint32_t col, float v) {
-    *reinterpret_cast<__nv_bfloat16*>(smem + base + core_offset(row, col, kRows)) = __float2bfloat16_rn(v);
+    *reinterpret_cast<__nv_bfloat16*>(smem + base + t_offset(row, col)) = __float2bfloat16_rn(v);
 }
 
 __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, const float4* targets, uint32_t batch,
-                                                         const uint8_t* image_f, const uint8_t* image_b, float* grads, float* loss,
+                                                         const uint8_t* image_f, const uint8_t* image_b, float* partials,
                                                          uint32_t* error) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kBarT);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kBarT + 8);
     uint32_t* abort_flag = reinterpret_cast<uint32_t*>(smem + kBarT + 12);
+    float* loss_warps = reinterpret_cast<float*>(smem + kBarT + 16);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    for (uint32_t i = tid; i < kImageBytes / 16; i += kThreads) {
-        reinterpret_cast<uint4*>(smem + kWF)[i] = reinterpret_cast<const uint4*>(image_f)[i];
-        reinterpret_cast<uint4*>(smem + kWB)[i] = reinterpret_cast<const uint4*>(image_b)[i];
-    }
-    // Zero the transposed tiles and the pad once: rows past a tile's real
-    // features are read by the M = 128 products.
-    for (uint32_t i = tid; i < (kBarT - kH0) / 16; i += kThreads) reinterpret_cast<uint4*>(smem + kH0)[i] = make_uint4(0, 0, 0, 0);
+    const uint32_t bar_addr = smem_u32(bar), s0 = smem_u32(smem);
     if (tid == 0) {
         *abort_flag = 0u;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1u));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_addr), "r"(1u));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        bulk_expect(bar_addr, 2u * kImageBytes);
+        bulk_load(s0 + kWF, image_f, kImageBytes, bar_addr);
+        bulk_load(s0 + kWB, image_b, kImageBytes, bar_addr);
     }
+    // Zero the transposed tiles once: rows past a tile's real features are
+    // read by the M = 128 products.
+    for (uint32_t i = tid; i < (kBarT - kH0) / 16; i += kThreads) reinterpret_cast<uint4*>(smem + kH0)[i] = make_uint4(0, 0, 0, 0);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTrainColumns));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -479,14 +524,13 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
     fence_after();
     const uint32_t tmem = *tmem_slot;
     const uint32_t lane_base = tmem + ((warp * 32u) << 16);
-    const uint32_t bar_addr = smem_u32(bar), s0 = smem_u32(smem);
-    uint32_t phase = 0;
     const uint32_t tiles = (batch + kRows - 1) / kRows;
     bool first = true, ok = true;
     float loss_sum = 0.0f;
 
-    // Issues nothing itself: every thread calls it; thread 0 has issued the
-    // MMAs and the commit. Returns false when the wait ran out.
+    // Every thread calls it; thread 0 has issued the MMAs and the commit (or
+    // the copies). Returns false when the wait ran out.
+    uint32_t phase = 0;
     auto finish = [&]() -> bool {
         if (!bar_wait(bar_addr, phase)) {
             atomicOr(abort_flag, 1u);
@@ -503,20 +547,30 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
         fence_before();
         __syncthreads();
     };
+    ok = finish();  // the weight images
 
     for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
         const uint32_t row = t * kRows + tid;
         const bool valid = row < batch;
-        // Input: A (K = 96) and h_0^T.
-        for (uint32_t c = 0; c < kIn / 8; ++c) {
-            float v[8];
-            for (int j = 0; j < 8; ++j) v[j] = valid ? features[(size_t)row * kIn + c * 8 + j] : 0.0f;
-            store8(smem + kAT, tid, c, kIn, v);
-            for (int j = 0; j < 8; ++j) store_t(smem, kH0, c * 8 + j, tid, v[j]);
+        // Input: A (K = 96) and h_0^T, all 24 loads in flight first.
+        {
+            float4 in[kIn / 4];
+            const float4* src = reinterpret_cast<const float4*>(features + (size_t)row * kIn);
+#pragma unroll
+            for (int q = 0; q < kIn / 4; ++q) in[q] = valid ? src[q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+            for (uint32_t c = 0; c < kIn / 8; ++c) {
+                const float v[8] = {in[2 * c].x, in[2 * c].y, in[2 * c].z, in[2 * c].w,
+                                    in[2 * c + 1].x, in[2 * c + 1].y, in[2 * c + 1].z, in[2 * c + 1].w};
+                store8(smem + kAT, tid, c, kIn, v);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) store_t(smem, kH0, c * 8 + j, tid, v[j]);
+            }
         }
         // Forward.
         float z[16];
-        for (int l = 0; l < kLayers && ok; ++l) {
+#pragma unroll
+        for (int l = 0; l < kLayers; ++l) {
             const uint32_t K = in_dim(l), N = out_dim(l);
             publish();
             if (tid == 0) {
@@ -528,13 +582,16 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
             }
             if (!(ok = finish())) break;
             if (l + 1 < kLayers) {
+#pragma unroll
                 for (uint32_t c0 = 0; c0 < N; c0 += 16u) {
                     float v[16];
                     tmem_ld16(lane_base + c0, v);
                     tmem_wait_ld();
+#pragma unroll
                     for (int j = 0; j < 16; ++j) v[j] = v[j] > 0.0f ? v[j] : 0.0f;
                     store8(smem + kAT, tid, c0 / 8u, N, v);
                     store8(smem + kAT, tid, c0 / 8u + 1u, N, v + 8);
+#pragma unroll
                     for (int j = 0; j < 16; ++j) store_t(smem, ht_offset(l + 1), c0 + j, tid, v[j]);
                 }
             } else {
@@ -545,6 +602,7 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
         if (!ok) break;
         // Output gradient.
         float dz[64];
+#pragma unroll
         for (int j = 0; j < 64; ++j) dz[j] = 0.0f;
         const float4 y = valid ? targets[row] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (valid && y.x == y.x) {  // a NaN target marks a row without a sample
@@ -558,17 +616,20 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
             dz[2] = 2.0f * e2 * inv * p2;
         }
         // Backward.
-        for (int l = kLayers - 1; l >= 0 && ok; --l) {
+#pragma unroll
+        for (int l = kLayers - 1; l >= 0; --l) {
             const uint32_t N = out_dim(l), Kin = in_dim(l);
+#pragma unroll
             for (uint32_t c = 0; c < N / 8u; ++c) store8(smem + kAT, tid, c, N, dz + c * 8);
+#pragma unroll
             for (uint32_t o = 0; o < N; ++o) store_t(smem, kDZ, o, tid, dz[o]);
             publish();
             if (tid == 0) {
                 fence_after();
                 // dW_l += h_l^T dz_l
                 for (uint32_t kk = 0; kk < kRows / 16u; ++kk)
-                    mma_bf16(tmem + grad_column(l), matrix_desc(s0 + ht_offset(l) + kk * 256u, 128u, (kRows / 8u) * 128u),
-                             matrix_desc(s0 + kDZ + kk * 256u, 128u, (kRows / 8u) * 128u), instr_desc(N), (first && kk == 0) ? 0u : 1u);
+                    mma_bf16(tmem + grad_column(l), matrix_desc(s0 + ht_offset(l) + kk * 2u * kLboT, kLboT, kSboT),
+                             matrix_desc(s0 + kDZ + kk * 2u * kLboT, kLboT, kSboT), instr_desc(N), (first && kk == 0) ? 0u : 1u);
                 // dh_l = dz_l W_l^T
                 if (l > 0)
                     for (uint32_t kk = 0; kk < N / 16u; ++kk)
@@ -579,56 +640,105 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
             }
             if (!(ok = finish())) break;
             if (l > 0) {
+#pragma unroll
                 for (uint32_t c0 = 0; c0 < Kin; c0 += 16u) {
                     float v[16];
                     tmem_ld16(lane_base + c0, v);
                     tmem_wait_ld();
+#pragma unroll
                     for (int j = 0; j < 16; ++j) {
-                        const __nv_bfloat16 h = *reinterpret_cast<const __nv_bfloat16*>(smem + ht_offset(l) + core_offset(c0 + j, tid, kRows));
+                        const __nv_bfloat16 h = *reinterpret_cast<const __nv_bfloat16*>(smem + ht_offset(l) + t_offset(c0 + j, tid));
                         dz[c0 + j] = (valid && __bfloat162float(h) > 0.0f) ? v[j] : 0.0f;
                     }
                 }
+#pragma unroll
                 for (uint32_t j = Kin; j < 64; ++j) dz[j] = 0.0f;
             }
         }
+        if (!ok) break;
         first = false;
     }
-    // Gradients: row `tid` of each layer's accumulator is input feature tid.
+    // This CTA's gradient sums: row `tid` of each layer's accumulator is
+    // input feature tid.
+    float* out = partials + (size_t)blockIdx.x * kPartial;
     if (ok && !first) {
         fence_before();
         __syncthreads();
         fence_after();
+#pragma unroll
         for (int l = 0; l < kLayers; ++l) {
             const uint32_t N = out_dim(l);
+#pragma unroll
             for (uint32_t c0 = 0; c0 < N; c0 += 16u) {
                 float v[16];
                 tmem_ld16(lane_base + grad_column(l) + c0, v);
                 tmem_wait_ld();
-                if (tid < (uint32_t)in_dim(l))
-                    for (int j = 0; j < 16; ++j) atomicAdd(grads + weight_offset(l) + tid * N + c0 + j, v[j]);
+                if (tid < (uint32_t)in_dim(l)) {
+                    float4* dst = reinterpret_cast<float4*>(out + weight_offset(l) + tid * N + c0);
+                    dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+                    dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+                    dst[2] = make_float4(v[8], v[9], v[10], v[11]);
+                    dst[3] = make_float4(v[12], v[13], v[14], v[15]);
+                }
             }
         }
     }
-    if (ok) atomicAdd(loss, loss_sum);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) loss_sum += __shfl_xor_sync(0xffffffffu, loss_sum, o);
+    if ((tid & 31u) == 0) loss_warps[warp] = loss_sum;
     fence_before();
     __syncthreads();
+    if (tid == 0) out[kWeights] = (loss_warps[0] + loss_warps[1]) + (loss_warps[2] + loss_warps[3]);
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTrainColumns));
 }
 
-// Adam (Kingma & Ba) on the FP32 masters, step `step` (1-based), then the
-// two BF16 images are repacked by the caller.
-__global__ void adam_kernel(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps,
-                            const uint32_t* steps) {
+// Sums the CTAs' partial rows in order: grads[i] and the loss.
+__global__ void reduce_kernel(const float* partials, uint32_t parts, float* grads, float* loss) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kWeights) return;
-    const uint32_t step = *steps;
-    const float g = grads[i];
-    const float mi = beta1 * m[i] + (1.0f - beta1) * g;
-    const float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
-    m[i] = mi;
-    v[i] = vi;
-    const float mh = mi / (1.0f - powf(beta1, (float)step)), vh = vi / (1.0f - powf(beta2, (float)step));
-    master[i] -= lr * mh / (sqrtf(vh) + eps);
+    if (i <= kWeights) {
+        float g = 0.0f;
+        for (uint32_t c = 0; c < parts; ++c) g += partials[(size_t)c * kPartial + i];
+        if (i < kWeights) grads[i] = g;
+        else *loss = g;
+    }
+}
+
+// One Adam step (Kingma & Ba) on the FP32 masters from the CTAs' partial
+// gradient rows, then both BF16 images. The step count lives on the device
+// (frames replay from a graph): every thread reads it first, and the last
+// block to finish stores it advanced by one.
+__global__ void adam_kernel(float* master, float* m, float* v, const float* partials, uint32_t parts, float lr, float beta1, float beta2,
+                            float eps, uint32_t* steps, uint8_t* image_f, uint8_t* image_b, float* loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t step = steps[0] + 1u;
+    if (i < kWeights) {
+        float g = 0.0f;
+        for (uint32_t c = 0; c < parts; ++c) g += partials[(size_t)c * kPartial + i];
+        const float mi = beta1 * m[i] + (1.0f - beta1) * g;
+        const float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
+        m[i] = mi;
+        v[i] = vi;
+        const float mh = mi / (1.0f - powf(beta1, (float)step)), vh = vi / (1.0f - powf(beta2, (float)step));
+        const float w = master[i] - lr * mh / (sqrtf(vh) + eps);
+        master[i] = w;
+        uint32_t fwd, bwd;
+        image_positions(i, fwd, bwd);
+        const __nv_bfloat16 b = __float2bfloat16_rn(w);
+        *reinterpret_cast<__nv_bfloat16*>(image_f + fwd) = b;
+        *reinterpret_cast<__nv_bfloat16*>(image_b + bwd) = b;
+    } else if (i == kWeights) {
+        float l = 0.0f;
+        for (uint32_t c = 0; c < parts; ++c) l += partials[(size_t)c * kPartial + kWeights];
+        *loss = l;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(steps + 1, 1u) == gridDim.x - 1) {  // steps[1]: blocks done
+            steps[1] = 0u;
+            steps[0] = step;
+        }
+    }
 }
 
 }  // namespace mlp
@@ -637,21 +747,31 @@ void launch_mlp_pack_backward(const float* master, uint8_t* image, cudaStream_t 
     mlp::pack_backward_kernel<<<(mlp::kWeights + 255) / 256, 256, 0, s>>>(master, image);
 }
 
-cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
-                             float* grads, float* loss, uint32_t* error, uint32_t ctas, cudaStream_t s) {
-    if (batch == 0) return cudaSuccess;
+uint32_t mlp_train_parts(uint32_t batch, uint32_t ctas) {
     const uint32_t tiles = (batch + mlp::kRows - 1) / mlp::kRows;
-    mlp::train_kernel<<<tiles < ctas ? tiles : ctas, mlp::kThreads, mlp::kTrainSmem, s>>>(features, targets, batch, image_f, image_b, grads,
-                                                                                           loss, error);
+    return tiles < ctas ? tiles : ctas;
+}
+
+uint32_t mlp_partial_floats() { return (uint32_t)mlp::kPartial; }
+
+cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
+                             float* partials, uint32_t* error, uint32_t ctas, cudaStream_t s) {
+    if (batch == 0) return cudaSuccess;
+    mlp::train_kernel<<<mlp_train_parts(batch, ctas), mlp::kThreads, mlp::kTrainSmem, s>>>(features, targets, batch, image_f, image_b,
+                                                                                           partials, error);
     return cudaGetLastError();
 }
 
-void launch_mlp_adam(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps,
-                     const uint32_t* step, cudaStream_t s) {
-    mlp::adam_kernel<<<(mlp::kWeights + 255) / 256, 256, 0, s>>>(master, m, v, grads, lr, beta1, beta2, eps, step);
+void launch_mlp_reduce(const float* partials, uint32_t parts, float* grads, float* loss, cudaStream_t s) {
+    mlp::reduce_kernel<<<(mlp::kWeights + 256) / 256, 256, 0, s>>>(partials, parts, grads, loss);
 }
 
-void launch_mlp_step(uint32_t* step, cudaStream_t s) { mlp::step_kernel<<<1, 1, 0, s>>>(step); }
+void launch_mlp_adam(float* master, float* m, float* v, const float* partials, uint32_t parts, float lr, float beta1, float beta2, float eps,
+                     uint32_t* steps, uint8_t* image_f, uint8_t* image_b, float* loss, cudaStream_t s) {
+    mlp::adam_kernel<<<(mlp::kWeights + 256) / 256, 256, 0, s>>>(master, m, v, partials, parts, lr, beta1, beta2, eps, steps, image_f,
+                                                                  image_b, loss);
+}
+
 
 void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,
                         float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s) {

@@ -120,7 +120,6 @@ const void* prepare_kernel_address();
 const void* accumulate_kernel_address();
 // MLP radiance cache (vgi_mlp.cu).
 cudaError_t mlp_set_attributes();
-void launch_mlp_step(uint32_t* step, cudaStream_t s);
 void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,
                         float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s);
 void launch_mlp_encode_training(const uint4* slot_meta, const uint4* results, const float4* materials, uint32_t n_slots,
@@ -135,10 +134,16 @@ void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s);
 cudaError_t launch_mlp_forward(const float* features, const uint8_t* image, float4* outputs, uint32_t n, uint32_t* error, uint32_t ctas,
                                cudaStream_t s);
 void launch_mlp_pack_backward(const float* master, uint8_t* image, cudaStream_t s);
+// Training: train writes one partial row (gradient sums, loss) per CTA,
+// mlp_train_parts(batch, ctas) rows; reduce sums them into grads and the
+// loss; adam sums them, steps the FP32 masters and repacks both images.
+uint32_t mlp_train_parts(uint32_t batch, uint32_t ctas);
+uint32_t mlp_partial_floats();
 cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
-                             float* grads, float* loss, uint32_t* error, uint32_t ctas, cudaStream_t s);
-void launch_mlp_adam(float* master, float* m, float* v, const float* grads, float lr, float beta1, float beta2, float eps,
-                     const uint32_t* step, cudaStream_t s);
+                             float* partials, uint32_t* error, uint32_t ctas, cudaStream_t s);
+void launch_mlp_reduce(const float* partials, uint32_t parts, float* grads, float* loss, cudaStream_t s);
+void launch_mlp_adam(float* master, float* m, float* v, const float* partials, uint32_t parts, float lr, float beta1, float beta2, float eps,
+                     uint32_t* steps, uint8_t* image_f, uint8_t* image_b, float* loss, cudaStream_t s);
 uint32_t mlp_weight_count();
 uint32_t mlp_image_bytes();
 void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s);
