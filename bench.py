@@ -366,6 +366,46 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_mlp(frames=3):
+    """A small MLP cache workload for ncu captures of the network kernels:
+    the same generator at 256x256x256 voxels (64 emissive voxels), faces
+    facing an eye at (128, 200, 128), 2 paths a face, the network ending
+    uncached first hits from the first frame, 65,536 training samples in 16
+    Adam steps a frame. About 1 GB on the device."""
+    import vgi
+
+    coords, vox = vgi.terrain(16, 16, 16, seed=2, octaves=4, period=64.0, base_height=128.0, falloff=400.0, emitters=64)
+    rng = np.random.default_rng(2)
+    m = vgi.VoxelGiMaterials()
+    for k in range(8):
+        m.set(k, vgi.MaterialTransport(diffuse=tuple(rng.uniform(0.2, 0.8, 3))))
+    for k in range(248):
+        m.set(8 + k, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5), emission=(5.0, 5.0, 5.0)))
+    sun = vgi.DirectionalTransportLight((0.4, 0.8, 0.3), (3.0, 3.0, 3.0))
+    faces = vgi.exposed_faces(coords, vox, facing=(128.0, 200.0, 128.0))
+    g = vgi.GpuTracer(0)
+    g.upload_regions(coords, vox)
+    g.set_materials(m.words())
+    g.set_lights(sun.words(), 1)
+    g.set_environment((0.0, 0.0, 0.0))
+    g.build_emitters()
+    g.set_transport(vgi.TransportSettings(bounces=BOUNCES, path_steps=2048))
+    g.set_faces(faces)
+    init = np.concatenate([(rng.normal(0.0, 1.0 / np.sqrt(i), size=(i, o)) * 0.5).astype(np.float32).reshape(-1)
+                           for i, o in vgi.GpuTracer.MLP_LAYERS])
+    g.mlp_set_weights(init)
+    g.set_mlp_cache(True, warm_frames=0, samples=MLP_SAMPLES, steps_per_frame=MLP_STEPS, lr=MLP_LR)
+    for f in range(frames):
+        g.frame(MLP_SPP, 16 * f)
+    g.sync()
+    st = g.mlp_stats()
+    print(json.dumps({"profile_mlp": {"faces": int(faces.shape[0]), "frames": frames, "queries_last_frame": st["queries"],
+                                      "adam_steps": st["steps"], "error": st["error"]}}), flush=True)
+    g.close()
+    if st["error"]:
+        sys.exit(1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -375,7 +415,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default layout (for profiling runs)")
     ap.add_argument("--no-mlp", action="store_true", help="skip the MLP cache comparison")
+    ap.add_argument("--profile-mlp", action="store_true", help="only a small MLP cache workload, for ncu captures")
     args = ap.parse_args()
+    if args.profile_mlp:
+        profile_mlp()
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -347,7 +347,10 @@ MlpEncoding mlp_encoding(const vgi_ctx* c) {
 }
 
 // Samples per training face in an MLP-terminated frame's training trace.
-constexpr uint32_t kMlpTrainSamples = 4;
+#ifndef VGI_MLP_TRAIN_SAMPLES
+#define VGI_MLP_TRAIN_SAMPLES 4
+#endif
+constexpr uint32_t kMlpTrainSamples = VGI_MLP_TRAIN_SAMPLES;
 
 // `marks`: record the frame's timing events (off for the training trace).
 int run_trace(vgi_ctx* c, const TraceArgs& a, bool count, bool marks = true) {
