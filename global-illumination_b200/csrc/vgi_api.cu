@@ -353,13 +353,9 @@ MlpEncoding mlp_encoding(const vgi_ctx* c) {
 constexpr uint32_t kMlpTrainSamples = VGI_MLP_TRAIN_SAMPLES;
 
 // `marks`: record the frame's timing events (off for the training trace).
-int run_trace(vgi_ctx* c, const TraceArgs& a, bool count, bool marks = true) {
-    if (c->layout == VGI_LAYOUT_SINGLE_KERNEL) {
-        if (c->timing && !count) c->traverse_launches = 0;
-        launch_trace(a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
-        VGI_CUDA(c, cudaGetLastError());
-        return VGI_OK;
-    }
+// Sizes the context's wavefront buffers for a trace of `a` and describes
+// them; drops the frame graph when a buffer moved.
+int wave_buffers(vgi_ctx* c, const TraceArgs& a, bool count, bool marks, WaveBuffers& b) {
     const size_t paths = (size_t)a.n_tasks * a.samples;
     const size_t slots = paths * (2 + a.light_count) + (size_t)a.n_tasks * a.light_count;
     if (paths >= (1ull << 30) || slots > 0xffffffffull) return fail(c, VGI_ERR_CAPACITY, "too many paths for the wavefront layout");
@@ -386,7 +382,7 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count, bool marks = true) {
     // A captured frame holds the old buffers' addresses.
     if (before[0] != c->w_state.ptr || before[1] != c->w_ray.ptr || before[2] != c->w_status.ptr || queue_before != c->w_mlp_queue.ptr)
         drop_graph(c);
-    WaveBuffers b{};
+    b = WaveBuffers{};
     b.state = c->w_state.ptr;
     b.ray = c->w_ray.ptr;
     b.hit = c->w_hit.ptr;
@@ -408,6 +404,18 @@ int run_trace(vgi_ctx* c, const TraceArgs& a, bool count, bool marks = true) {
         if (marks) c->mlp_queue_capacity = (uint32_t)paths;
     }
     if (b.traverse_marks) c->traverse_launches = std::min<uint32_t>((mlp ? 1u : c->transport.bounces) + 1u, 4u);
+    return VGI_OK;
+}
+
+int run_trace(vgi_ctx* c, const TraceArgs& a, bool count, bool marks = true) {
+    if (c->layout == VGI_LAYOUT_SINGLE_KERNEL) {
+        if (c->timing && !count) c->traverse_launches = 0;
+        launch_trace(a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
+        VGI_CUDA(c, cudaGetLastError());
+        return VGI_OK;
+    }
+    WaveBuffers b;
+    if (int e = wave_buffers(c, a, count, marks, b)) return e;
     launch_wave(b, a, c->transport.bounces, transport_limited(c), c->transport.budgeted != 0, count, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     return VGI_OK;
@@ -1679,6 +1687,312 @@ void vgi_directional_light_record(const float* d, const float* radiance3, const 
         out12[4 + k] = radiance3[k];
         out12[9 + k] = custom3 ? custom3[k] : 0.0f;
     }
+}
+
+// ---- batched frames ---------------------------------------------------------
+}  // extern "C"
+
+struct vgi_batch {
+    std::vector<vgi_ctx*> ctxs;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<cudaEvent_t> ready;
+    DevBuf<uint8_t> args;                    // the traversal's argument table on the device
+    std::vector<uint8_t> table;              // ... and the host copy it was made from
+    DevBuf<uint32_t> head;                   // the batched traversal's shared queue head
+    uint32_t blocks = 0, refill_min = 8;
+    bool use_graph = false, graph_dirty = true;
+    uint32_t graph_samples = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaGraphNode_t> prepare_nodes, accumulate_nodes;
+    std::string error;
+};
+
+namespace {
+int batch_fail(vgi_batch* b, int code, const std::string& what) {
+    b->error = what;
+    return code;
+}
+#define VGI_BCUDA(b, expr)                                                                               \
+    do {                                                                                                 \
+        cudaError_t err_ = (expr);                                                                       \
+        if (err_ != cudaSuccess) return batch_fail(b, VGI_ERR_CUDA, std::string(#expr ": ") + cudaGetErrorString(err_)); \
+    } while (0)
+
+void batch_drop_graph(vgi_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->prepare_nodes.clear();
+    b->accumulate_nodes.clear();
+    b->graph_dirty = true;
+}
+
+// Every context of a batch traces like vgi_frame in the wavefront layout
+// with one transport for all.
+int batch_check(vgi_batch* b) {
+    const vgi_ctx* c0 = b->ctxs[0];
+    for (vgi_ctx* c : b->ctxs) {
+        if (int e = check_ready(c, true)) return batch_fail(b, e, std::string("scene not ready: ") + c->error);
+        if (c->device != b->device) return batch_fail(b, VGI_ERR_INVALID, "batched scenes must share one device");
+        if (c->layout != VGI_LAYOUT_WAVEFRONT) return batch_fail(b, VGI_ERR_STATE, "batched scenes trace in the wavefront layout");
+        if (c->mlp_cache) return batch_fail(b, VGI_ERR_STATE, "the MLP cache mode is per scene, not batched");
+        if (c->transport.bounces != c0->transport.bounces || transport_limited(c) != transport_limited(c0) ||
+            (c->transport.budgeted != 0) != (c0->transport.budgeted != 0))
+            return batch_fail(b, VGI_ERR_STATE, "batched scenes must share bounces, reach limit and step budget");
+    }
+    return VGI_OK;
+}
+
+// The scenes' buffers and trace arguments for `samples` paths a face, over
+// the given tasks and results (null: each scene's own). Rebuilds and uploads
+// the traversal's argument table when anything in it changed.
+int batch_scenes(vgi_batch* b, uint32_t samples, bool scratch, std::vector<WaveScene>& scenes) {
+    const uint32_t n = (uint32_t)b->ctxs.size();
+    scenes.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        vgi_ctx* c = b->ctxs[i];
+        const uint4* tasks = c->tasks.ptr;
+        uint4* results = c->results.ptr;
+        if (scratch) {
+            VGI_BCUDA(b, c->scratch_tasks.reserve((size_t)c->n_slots * 2));
+            VGI_BCUDA(b, c->scratch_results.reserve((size_t)c->n_slots * 6));
+            tasks = c->scratch_tasks.ptr;
+            results = c->scratch_results.ptr;
+        }
+        scenes[i].a = trace_args(c, tasks, results, c->n_slots, samples, true);
+        if (wave_buffers(c, scenes[i].a, false, false, scenes[i].b) != VGI_OK) return batch_fail(b, VGI_ERR_CUDA, c->error);
+        const size_t paths = (size_t)c->n_slots * samples;
+        if (paths >= (1ull << 30)) return batch_fail(b, VGI_ERR_CAPACITY, "too many paths in a batched scene");
+    }
+    std::vector<uint8_t> table((size_t)wave_batch_stages(b->ctxs[0]->transport.bounces) * n * wave_args_bytes());
+    wave_batch_args(scenes.data(), n, b->ctxs[0]->transport.bounces, table.data());
+    if (table != b->table) {
+        batch_drop_graph(b);
+        VGI_BCUDA(b, b->args.reserve(table.size()));
+        VGI_BCUDA(b, cudaMemcpyAsync(b->args.ptr, table.data(), table.size(), cudaMemcpyHostToDevice, b->stream));
+        VGI_BCUDA(b, cudaStreamSynchronize(b->stream));
+        b->table.swap(table);
+    }
+    return VGI_OK;
+}
+
+void batch_trace(vgi_batch* b, const std::vector<WaveScene>& scenes) {
+    const vgi_ctx* c0 = b->ctxs[0];
+    launch_wave_batch(scenes.data(), (uint32_t)scenes.size(), b->args.ptr, b->head.ptr, c0->transport.bounces, transport_limited(c0),
+                      c0->transport.budgeted != 0, b->blocks, b->refill_min, b->stream);
+}
+
+// Orders the batch stream after every scene's stream.
+int batch_enter(vgi_batch* b) {
+    for (size_t i = 0; i < b->ctxs.size(); ++i) {
+        VGI_BCUDA(b, cudaEventRecord(b->ready[i], b->ctxs[i]->stream));
+        VGI_BCUDA(b, cudaStreamWaitEvent(b->stream, b->ready[i], 0));
+    }
+    return VGI_OK;
+}
+// ... and every scene's stream after the batch's work.
+int batch_leave(vgi_batch* b) {
+    VGI_BCUDA(b, cudaEventRecord(b->done, b->stream));
+    for (vgi_ctx* c : b->ctxs) VGI_BCUDA(b, cudaStreamWaitEvent(c->stream, b->done, 0));
+    return VGI_OK;
+}
+
+// The node that the last launch on a capturing stream added.
+cudaGraphNode_t last_captured(cudaStream_t s) {
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t n = 0;
+    if (cudaStreamGetCaptureInfo(s, &status, nullptr, nullptr, &deps, &n) != cudaSuccess || n != 1) return nullptr;
+    return deps[0];
+}
+
+cudaError_t set_node_args(cudaGraphExec_t exec, cudaGraphNode_t node, const AccumArgs& acc) {
+    cudaKernelNodeParams p{};
+    cudaError_t e = cudaGraphKernelNodeGetParams(node, &p);
+    if (e != cudaSuccess) return e;
+    AccumArgs copy = acc;
+    void* args[] = {&copy};
+    p.kernelParams = args;
+    p.extra = nullptr;
+    return cudaGraphExecKernelNodeSetParams(exec, node, &p);
+}
+}  // namespace
+
+extern "C" {
+
+int vgi_batch_create(vgi_ctx* const* ctxs, uint32_t n, vgi_batch** out) {
+    if (!ctxs || !out || n == 0) return VGI_ERR_INVALID;
+    if (n > kMaxBatchScenes) return VGI_ERR_CAPACITY;
+    *out = nullptr;
+    for (uint32_t i = 0; i < n; ++i)
+        if (!ctxs[i]) return VGI_ERR_INVALID;
+    auto* b = new vgi_batch();
+    b->ctxs.assign(ctxs, ctxs + n);
+    b->device = ctxs[0]->device;
+    b->blocks = ctxs[0]->traverse_blocks;
+    b->refill_min = ctxs[0]->refill_min;
+    b->ready.resize(n, nullptr);
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+    for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&b->ready[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = b->head.reserve(1);
+    if (e != cudaSuccess) {
+        vgi_batch_destroy(b);
+        return VGI_ERR_CUDA;
+    }
+    *out = b;
+    return VGI_OK;
+}
+
+int vgi_batch_destroy(vgi_batch* b) {
+    if (!b) return VGI_ERR_INVALID;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    b->args.release();
+    b->head.release();
+    for (cudaEvent_t e : b->ready)
+        if (e) cudaEventDestroy(e);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return VGI_OK;
+}
+
+const char* vgi_batch_last_error(const vgi_batch* b) { return b ? b->error.c_str() : "null batch"; }
+
+int vgi_batch_set_graph(vgi_batch* b, int enable) {
+    if (!b) return VGI_ERR_INVALID;
+    batch_drop_graph(b);
+    b->use_graph = enable != 0;
+    return VGI_OK;
+}
+
+int vgi_batch_frame(vgi_batch* b, uint32_t samples, uint32_t clock_ms) {
+    if (!b) return VGI_ERR_INVALID;
+    if (samples == 0) return batch_fail(b, VGI_ERR_INVALID, "samples must be positive");
+    VGI_BCUDA(b, cudaSetDevice(b->device));
+    if (int e = batch_check(b)) return e;
+    if (int e = batch_enter(b)) return e;
+    std::vector<WaveScene> scenes;
+    if (int e = batch_scenes(b, samples, false, scenes)) return e;
+    const uint32_t n = (uint32_t)b->ctxs.size();
+    std::vector<AccumArgs> acc(n);
+    for (uint32_t i = 0; i < n; ++i) acc[i] = accum_args(b->ctxs[i], samples, clock_ms);
+    if (b->use_graph && b->exec && !b->graph_dirty && b->graph_samples == samples) {
+        for (uint32_t i = 0; i < n; ++i) {
+            VGI_BCUDA(b, set_node_args(b->exec, b->prepare_nodes[i], acc[i]));
+            VGI_BCUDA(b, set_node_args(b->exec, b->accumulate_nodes[i], acc[i]));
+        }
+        VGI_BCUDA(b, cudaGraphLaunch(b->exec, b->stream));
+    } else {
+        // Captured on the second frame with unchanged buffers; run directly
+        // otherwise.
+        const bool capture = b->use_graph && !b->graph_dirty && b->graph_samples == samples;
+        if (capture) {
+            batch_drop_graph(b);
+            VGI_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            launch_prepare(acc[i], b->stream);
+            if (capture) b->prepare_nodes.push_back(last_captured(b->stream));
+        }
+        batch_trace(b, scenes);
+        for (uint32_t i = 0; i < n; ++i) {
+            launch_accumulate(acc[i], b->stream);
+            if (capture) b->accumulate_nodes.push_back(last_captured(b->stream));
+        }
+        if (capture) {
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            bool found = e == cudaSuccess;
+            for (uint32_t i = 0; i < n && found; ++i) found = b->prepare_nodes[i] && b->accumulate_nodes[i];
+            if (!found) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                b->prepare_nodes.clear();
+                b->accumulate_nodes.clear();
+                return batch_fail(b, VGI_ERR_CUDA, "batched frame capture failed");
+            }
+            b->graph = g;
+            VGI_BCUDA(b, cudaGraphInstantiate(&b->exec, g, 0));
+            VGI_BCUDA(b, cudaGraphLaunch(b->exec, b->stream));
+            b->graph_dirty = false;
+        } else if (b->use_graph) {
+            b->graph_dirty = false;  // the next frame is captured
+        }
+        b->graph_samples = samples;
+    }
+    VGI_BCUDA(b, cudaGetLastError());
+    for (vgi_ctx* c : b->ctxs) {
+        c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
+        if (c->batch_id == 0) c->batch_id = 1;
+    }
+    return batch_leave(b);
+}
+
+int vgi_batch_sync(vgi_batch* b) {
+    if (!b) return VGI_ERR_INVALID;
+    VGI_BCUDA(b, cudaStreamSynchronize(b->stream));
+    return VGI_OK;
+}
+
+int vgi_batch_autotune(vgi_batch* b, uint32_t samples, uint32_t* refill_out, uint32_t* blocks_out, float* ms_out) {
+    if (!b) return VGI_ERR_INVALID;
+    if (samples == 0) return batch_fail(b, VGI_ERR_INVALID, "samples must be positive");
+    VGI_BCUDA(b, cudaSetDevice(b->device));
+    if (int e = batch_check(b)) return e;
+    if (int e = batch_enter(b)) return e;
+    // State-free traces of each scene's current tasks into scratch results.
+    for (vgi_ctx* c : b->ctxs) {
+        VGI_BCUDA(b, c->scratch_tasks.reserve((size_t)c->n_slots * 2));
+        VGI_BCUDA(b, cudaMemcpyAsync(c->scratch_tasks.ptr, c->tasks.ptr, (size_t)c->n_slots * 32, cudaMemcpyDeviceToDevice, b->stream));
+    }
+    std::vector<WaveScene> scenes;
+    if (int e = batch_scenes(b, samples, true, scenes)) return e;
+    const uint32_t sms = b->ctxs[0]->traverse_blocks / wave_traverse_blocks_per_sm();
+    const uint32_t refills[] = {4, 8, 12, 16};
+    const uint32_t per_sm[] = {wave_traverse_blocks_per_sm(), wave_traverse_blocks_per_sm() > 2 ? 2u : 1u};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    VGI_BCUDA(b, cudaEventCreate(&e0));
+    VGI_BCUDA(b, cudaEventCreate(&e1));
+    float best = 1e30f;
+    uint32_t best_refill = b->refill_min, best_blocks = b->blocks;
+    for (uint32_t ps : per_sm) {
+        for (uint32_t r : refills) {
+            b->refill_min = r;
+            b->blocks = sms * ps;
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2; ++rep) {  // the first run warms caches
+                cudaEventRecord(e0, b->stream);
+                batch_trace(b, scenes);
+                cudaEventRecord(e1, b->stream);
+                cudaEventSynchronize(e1);
+                cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (ms < best) {
+                best = ms;
+                best_refill = r;
+                best_blocks = b->blocks;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->refill_min = best_refill;
+    b->blocks = best_blocks;
+    batch_drop_graph(b);
+    b->table.clear();  // the frame's table differs from the scratch one
+    VGI_BCUDA(b, cudaGetLastError());
+    if (refill_out) *refill_out = best_refill;
+    if (blocks_out) *blocks_out = best_blocks;
+    if (ms_out) *ms_out = best;
+    return batch_leave(b);
 }
 
 }  // extern "C"

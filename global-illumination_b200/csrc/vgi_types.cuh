@@ -86,6 +86,22 @@ struct WaveBuffers {
     cudaEvent_t* mlp_marks;   // optional: start/end events of the query launch
 };
 
+// One scene of a batched frame: its wavefront buffers and trace arguments.
+struct WaveScene {
+    WaveBuffers b;
+    TraceArgs a;
+};
+// Batched frames (vgi_wave.cuh): the traversal of every stage runs once over
+// the rays of all scenes. The argument table holds wave_batch_stages(hits)
+// x n records of wave_args_bytes() each, built on the host by
+// wave_batch_args and copied to the device once for a set of buffers.
+constexpr uint32_t kMaxBatchScenes = 256;
+uint32_t wave_batch_stages(uint32_t hits);
+size_t wave_args_bytes();
+void wave_batch_args(const WaveScene* scenes, uint32_t n, uint32_t hits, void* out);
+void launch_wave_batch(const WaveScene* scenes, uint32_t n, const void* device_args, uint32_t* head, uint32_t hits, bool limited,
+                       bool budgeted, uint32_t blocks, uint32_t refill_min, cudaStream_t s);
+
 // The view tier's buffers and controls (vgi_view.cuh) for n receivers.
 struct ViewArgs {
     TraceArgs t;

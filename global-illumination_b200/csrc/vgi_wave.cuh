@@ -714,6 +714,73 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_TRAVERSE_MIN_BLOCKS) wave_trav
     flush_counters<C>(A, cnt);
 }
 
+// The same traversal over the rays of several scenes at once: scene i's
+// WaveArgs (this stage's queue, ray and hit arrays, geometry) is scenes[i],
+// and the rays are pulled from the concatenation of the scenes' queues by
+// one shared head, so one resident grid keeps busy however uneven the
+// scenes are. Each lane keeps the scene of its ray; a step reads that
+// scene's arrays, so every ray takes exactly the steps it takes alone.
+constexpr uint32_t kMaxBatch = 256;
+
+template <bool BUDGETED>
+__global__ void __launch_bounds__(kWaveBlock, VGI_TRAVERSE_MIN_BLOCKS)
+    wave_traverse_batch_kernel(const WaveArgs* scenes, uint32_t n_scenes, uint32_t* head, uint32_t refill_min) {
+    __shared__ uint32_t first_ray[kMaxBatch + 1];  // prefix sums of the scenes' queue counts
+    if (threadIdx.x == 0) {
+        uint32_t sum = 0;
+        for (uint32_t i = 0; i < n_scenes; ++i) {
+            first_ray[i] = sum;
+            sum += *scenes[i].count_in;
+        }
+        first_ray[n_scenes] = sum;
+    }
+    __syncthreads();
+    const uint32_t total = first_ray[n_scenes];
+    Cnt<false> cnt;
+    const int lane = threadIdx.x & 31;
+    RayRun s;
+    s.slot = kNoIndex;
+    uint32_t scene = 0;
+    bool exhausted = false;
+    for (;;) {
+        const bool need = s.slot == kNoIndex;
+        const unsigned want = __ballot_sync(0xffffffffu, need);
+        if (!exhausted && (uint32_t)__popc(want) >= (want == 0xffffffffu ? 1u : refill_min)) {
+            const int leader = __ffs(want) - 1;
+            uint32_t first = 0;
+            if (lane == leader) first = atomicAdd(head, (uint32_t)__popc(want));
+            first = __shfl_sync(0xffffffffu, first, leader);
+            const uint32_t mine = first + __popc(want & ((1u << lane) - 1u));
+            if (first + __popc(want) >= total) exhausted = true;
+            if (need && mine < total) {
+                // The last scene whose first ray is at or before `mine`.
+                uint32_t lo = 0, hi = n_scenes - 1;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1) >> 1;
+                    if (first_ray[mid] <= mine) lo = mid;
+                    else hi = mid - 1;
+                }
+                scene = lo;
+                const WaveArgs& W = scenes[scene];
+                start_ray<BUDGETED, false>(W, s, W.queue_in[mine - first_ray[scene]], cnt);
+            }
+        }
+        const bool idle = s.slot == kNoIndex;
+        const unsigned busy = __ballot_sync(0xffffffffu, !idle);
+        if (!busy) {
+            if (exhausted) break;
+            continue;
+        }
+        uint32_t status = kGo, material = 0u;
+        I3 voxel{0, 0, 0};
+        const uint32_t creep_limit = exhausted ? 0xffffffffu : s.step + 64u;
+        const WaveArgs& W = scenes[scene];
+        if (!idle) classify_step<BUDGETED, false>(W, s, cnt, status, material, voxel);
+        __syncwarp();
+        if (!idle) finish_step<BUDGETED, false>(W, s, cnt, status, material, voxel, creep_limit);
+    }
+}
+
 // Stage s >= 1: complete the pending hit, then the continuation's new hit
 // (one iteration of advance_path, voxel_path.wgsl:432-490).
 template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
@@ -1115,7 +1182,92 @@ void wave_hits(const WaveBuffers& b, const TraceArgs& a, bool limited, bool budg
 #undef VGI_WAVE
 }
 
+// One scene's WaveArgs for stage k (1-based) of a frame: the queues
+// alternate between the two buffers stage after stage, as in wave_run.
+WaveArgs stage_args(const WaveBuffers& b, const TraceArgs& a, uint32_t k) {
+    WaveArgs W{};
+    W.t = a;
+    W.n_paths = a.n_tasks * a.samples;
+    W.slots = 2u + a.light_count;
+    W.state = b.state;
+    W.ray = b.ray;
+    W.status = b.status;
+    W.hit = b.hit;
+    W.queue_head = b.counters + 2;
+    W.scatter_queue = b.scatter;
+    W.scatter_count = b.counters + 3;
+    W.mlp_queue = nullptr;
+    W.mlp_count = b.counters + 4;
+    const bool odd = (k & 1u) != 0u;  // k = 0: begin writes the first stage's queue
+    W.queue_in = odd ? b.queue[0] : b.queue[1];
+    W.count_in = odd ? b.counters + 0 : b.counters + 1;
+    W.queue_out = odd ? b.queue[1] : b.queue[0];
+    W.count_out = odd ? b.counters + 1 : b.counters + 0;
+    if (k == 0) {
+        W.queue_out = b.queue[0];
+        W.count_out = b.counters + 0;
+    }
+    return W;
+}
+
+template <uint32_t H, bool L, bool B>
+void wave_batch_run(const WaveScene* sc, uint32_t n, const WaveArgs* device_args, uint32_t* head, uint32_t blocks, uint32_t refill_min,
+                    cudaStream_t s) {
+    for (uint32_t i = 0; i < n; ++i) {
+        const WaveArgs W = stage_args(sc[i].b, sc[i].a, 0);
+        cudaMemsetAsync(W.count_out, 0, sizeof(uint32_t), s);
+        wave_begin_kernel<H, L, B, false><<<(W.n_paths + kWaveBlock - 1) / kWaveBlock, kWaveBlock, 0, s>>>(W);
+    }
+    for (uint32_t stage = 1; stage <= H + 1u; ++stage) {
+        cudaMemsetAsync(head, 0, sizeof(uint32_t), s);
+        wave_traverse_batch_kernel<B><<<blocks, kWaveBlock, 0, s>>>(device_args + (size_t)(stage - 1u) * n, n, head, refill_min);
+        if (stage == H + 1u) break;
+        for (uint32_t i = 0; i < n; ++i) {
+            const WaveArgs W = stage_args(sc[i].b, sc[i].a, stage);
+            cudaMemsetAsync(W.count_out, 0, sizeof(uint32_t), s);
+            cudaMemsetAsync(W.scatter_count, 0, sizeof(uint32_t), s);
+            wave_shade_kernel<H, L, B, false><<<(W.n_paths + kWaveBlock - 1) / kWaveBlock, kWaveBlock, 0, s>>>(W, stage);
+            wave_scatter_kernel<H, L, B, false><<<sc[i].b.traverse_blocks, kWaveBlock, 0, s>>>(W);
+        }
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const WaveArgs W = stage_args(sc[i].b, sc[i].a, H + 1u);
+        const uint32_t face_blocks = (uint32_t)((((uint64_t)sc[i].a.n_tasks << sc[i].a.lanes_log2) + kWaveBlock - 1) / kWaveBlock);
+        wave_finalize_kernel<H, L, B, false><<<face_blocks, kWaveBlock, 0, s>>>(W);
+    }
+}
+
 }  // namespace
+
+uint32_t wave_batch_stages(uint32_t hits) { return (hits <= 1 ? 1u : hits > 3 ? 3u : hits) + 1u; }
+
+size_t wave_args_bytes() { return sizeof(WaveArgs); }
+
+void wave_batch_args(const WaveScene* sc, uint32_t n, uint32_t hits, void* out) {
+    WaveArgs* dst = static_cast<WaveArgs*>(out);
+    const uint32_t stages = wave_batch_stages(hits);
+    for (uint32_t k = 1; k <= stages; ++k)
+        for (uint32_t i = 0; i < n; ++i) dst[(size_t)(k - 1u) * n + i] = stage_args(sc[i].b, sc[i].a, k);
+}
+
+void launch_wave_batch(const WaveScene* sc, uint32_t n, const void* args, uint32_t* head, uint32_t hits, bool limited, bool budgeted,
+                       uint32_t blocks, uint32_t refill_min, cudaStream_t s) {
+    if (n == 0 || n > kMaxBatch) return;
+    const WaveArgs* device_args = static_cast<const WaveArgs*>(args);
+    const uint32_t h = hits <= 1 ? 1u : hits > 3 ? 3u : hits;
+#define VGI_BATCH(HH, LL, BB) wave_batch_run<HH, LL, BB>(sc, n, device_args, head, blocks, refill_min, s)
+    if (h == 1) {
+        if (limited) { if (budgeted) VGI_BATCH(1, true, true); else VGI_BATCH(1, true, false); }
+        else { if (budgeted) VGI_BATCH(1, false, true); else VGI_BATCH(1, false, false); }
+    } else if (h == 2) {
+        if (limited) { if (budgeted) VGI_BATCH(2, true, true); else VGI_BATCH(2, true, false); }
+        else { if (budgeted) VGI_BATCH(2, false, true); else VGI_BATCH(2, false, false); }
+    } else {
+        if (limited) { if (budgeted) VGI_BATCH(3, true, true); else VGI_BATCH(3, true, false); }
+        else { if (budgeted) VGI_BATCH(3, false, true); else VGI_BATCH(3, false, false); }
+    }
+#undef VGI_BATCH
+}
 
 void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t s) {
     if (a.n_tasks == 0 || a.samples == 0) return;

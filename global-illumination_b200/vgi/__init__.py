@@ -183,6 +183,13 @@ _SIGNATURES = {
     "vgi_mlp_encode": (_INT, [_P, _P, _U32, _P]),
     "vgi_set_mlp_cache": (_INT, [_P, ctypes.c_int, _U32, _U32, _U32, ctypes.c_float]),
     "vgi_mlp_stats": (_INT, [_P, _P]),
+    "vgi_batch_create": (_INT, [_P, _U32, _P]),
+    "vgi_batch_destroy": (_INT, [_P]),
+    "vgi_batch_last_error": (ctypes.c_char_p, [_P]),
+    "vgi_batch_frame": (_INT, [_P, _U32, _U32]),
+    "vgi_batch_set_graph": (_INT, [_P, ctypes.c_int]),
+    "vgi_batch_sync": (_INT, [_P]),
+    "vgi_batch_autotune": (_INT, [_P, _U32, _P, _P, _P]),
     "vgi_read_results": (_INT, [_P, _U32, _U32, _P]),
     "vgi_read_state": (_INT, [_P, _U32, _U32, _P]),
     "vgi_write_state": (_INT, [_P, _U32, _U32, _P]),
@@ -687,6 +694,51 @@ def host_top_level(coords, solid) -> Optional[np.ndarray]:
     out = np.zeros(cells * 6, np.uint8)
     rc = library().vgi_host_top_level(_ptr(coords), _ptr(s), coords.shape[0], _ptr(out), out.size)
     return None if rc == 1 else out.reshape(-1, 6)
+
+
+class GpuBatch:
+    """Several GpuTracer scenes traced together (vgi_batch_*): one frame of
+    every scene, with each stage's traversal one launch over all their rays.
+    The tracers must outlive the batch."""
+
+    def __init__(self, tracers):
+        self._lib = library()
+        self.tracers = list(tracers)
+        handles = (ctypes.c_void_p * len(self.tracers))(*[t._h.value for t in self.tracers])
+        h = ctypes.c_void_p()
+        rc = self._lib.vgi_batch_create(handles, len(self.tracers), ctypes.byref(h))
+        if rc != OK:
+            raise VgiError(rc, "vgi_batch_create failed")
+        self._h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != OK:
+            raise VgiError(rc, self._lib.vgi_batch_last_error(self._h).decode())
+
+    def frame(self, samples: int, clock_ms: int = 0) -> None:
+        self._check(self._lib.vgi_batch_frame(self._h, samples, clock_ms))
+
+    def set_graph(self, enable: bool) -> None:
+        self._check(self._lib.vgi_batch_set_graph(self._h, 1 if enable else 0))
+
+    def sync(self) -> None:
+        self._check(self._lib.vgi_batch_sync(self._h))
+
+    def autotune(self, samples: int) -> dict:
+        refill, blocks, ms = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_float()
+        self._check(self._lib.vgi_batch_autotune(self._h, samples, ctypes.byref(refill), ctypes.byref(blocks), ctypes.byref(ms)))
+        return {"refill_min": refill.value, "blocks": blocks.value, "trace_ms": ms.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.vgi_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def tasks_for(faces: np.ndarray, sequence: int = 0) -> np.ndarray:

@@ -300,6 +300,31 @@ typedef struct vgi_mlp_status {
 /* Synchronous. */
 int vgi_mlp_stats(vgi_ctx* ctx, vgi_mlp_status* out);
 
+/* ---- batched scenes ----------------------------------------------------------
+ * No counterpart in the reference (its scenes are traced one at a time):
+ * several contexts, one per scene, traced together. vgi_batch_frame runs
+ * for every scene what vgi_frame runs (prepare, the wavefront trace with
+ * cache gather, accumulate), but the traversal of each stage is ONE
+ * persistent launch over the rays of all scenes, so scenes of very uneven
+ * size share the GPU. Every scene's results and state are those its own
+ * vgi_frame would give. The scenes must be ready (geometry, model, faces),
+ * on one device, in the wavefront layout, with the same bounces, reach limit
+ * and step budget, and with the MLP cache mode off; at most 256 of them.
+ * The batch enqueues on its own stream, ordered after and before each
+ * scene's stream. vgi_batch_set_graph captures the whole batched frame into
+ * one CUDA graph on the second frame after any change, as vgi_set_graph
+ * does for one scene. vgi_batch_autotune times state-free batched traces of
+ * the scenes' current tasks over the traversal's refill threshold and grid
+ * size, keeps the fastest, and reports it. */
+typedef struct vgi_batch vgi_batch;
+int vgi_batch_create(vgi_ctx* const* ctxs, uint32_t n, vgi_batch** out);
+int vgi_batch_destroy(vgi_batch* batch);
+const char* vgi_batch_last_error(const vgi_batch* batch);
+int vgi_batch_frame(vgi_batch* batch, uint32_t samples, uint32_t clock_ms);
+int vgi_batch_set_graph(vgi_batch* batch, int enable);
+int vgi_batch_sync(vgi_batch* batch);
+int vgi_batch_autotune(vgi_batch* batch, uint32_t samples, uint32_t* refill_min, uint32_t* blocks, float* trace_ms);
+
 /* ---- read-back: bounded snapshots (complete_readback, src/gpu.rs:1024-1170) --- */
 int vgi_read_results(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words24);
 int vgi_read_state(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words36);
