@@ -19,6 +19,9 @@ empty cache and an untrained network until its relMSE against the FP64
 reference reaches the plain trace's (after the plain run's frames), and
 reports both forms' ms/frame, rays/s and time to that relMSE, with the
 query kernel's tensor-core throughput.
+``batched_scenes`` traces 32 seeded scenes of uneven size (32..256 voxels a
+side) both as separate per-scene frames and as batched frames (one
+traversal launch per stage over all scenes), from the same empty caches.
 ``--impl reference`` times the CPU oracle (the restatement of the
 reference's algorithm; the reference itself is Rust/WGSL and has no CPU
 path) on the box's host cores.
@@ -366,6 +369,133 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def make_batch_scenes(n, seed0=100):
+    """Seeded scenes of uneven size for the batched form: the terrain
+    generator with 2..16 regions (32..256 voxels) per axis drawn uniformly,
+    base height half the height, one emissive voxel per 1024 columns (at
+    least 4), the same materials and sun as the terrain workload, faces
+    facing an eye above the scene's centre (0.8 of its height)."""
+    import vgi
+
+    rng = np.random.default_rng(seed0)
+    out = []
+    for k in range(n):
+        nx, ny, nz = (int(v) for v in rng.integers(2, 17, size=3))
+        X, Y, Z = 16 * nx, 16 * ny, 16 * nz
+        coords, vox = vgi.terrain(nx, ny, nz, seed=seed0 + k, octaves=4, period=64.0, base_height=0.5 * Y, falloff=1.5 * Y,
+                                  emitters=max(4, X * Z // 1024))
+        faces = vgi.exposed_faces(coords, vox, facing=(0.5 * X, 0.8 * Y, 0.5 * Z))
+        out.append((coords, vox, faces, (X, Y, Z)))
+    return out
+
+
+def batch_comparison(local, stream, flush, n_scenes, steps, warmup):
+    """Batched scenes: the same frames of every scene three ways, each scene
+    graph-replayed: one scene after another (serial, as the reference's
+    trace worker runs them), every scene's vgi_frame on its own stream (the
+    streams overlap on the GPU), and vgi_batch_frame (one traversal launch
+    per stage over all scenes). All start from empty caches, so the ray work
+    is identical; frames are CUDA-event timed from a common start to the
+    last scene's end, L2 flushed in between."""
+    import torch
+
+    import vgi
+
+    scenes = make_batch_scenes(n_scenes)
+    rng = np.random.default_rng(2)
+    m = vgi.VoxelGiMaterials()
+    for k in range(8):
+        m.set(k, vgi.MaterialTransport(diffuse=tuple(rng.uniform(0.2, 0.8, 3))))
+    for k in range(248):
+        m.set(8 + k, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5), emission=(float(rng.uniform(1.0, 10.0)),) * 3))
+    words = m.words()
+    sun = vgi.DirectionalTransportLight((0.4, 0.8, 0.3), (3.0, 3.0, 3.0)).words()
+    tracers = []
+    for coords, vox, faces, _ in scenes:
+        t = vgi.GpuTracer(local)
+        t.upload_regions(coords, vox)
+        t.set_materials(words)
+        t.set_lights(sun, 1)
+        t.set_environment((0.0, 0.0, 0.0))
+        t.build_emitters()
+        t.set_transport(vgi.TransportSettings(bounces=BOUNCES, path_steps=2048))
+        t.set_faces(faces)
+        tracers.append(t)
+    streams = [torch.cuda.ExternalStream(t.stream, device=torch.device("cuda", local)) for t in tracers]
+
+    def timed(run_frame, n_frames, clock0):
+        ms = []
+        for f in range(n_frames):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(f))
+                start = torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+            for st in streams:
+                st.wait_event(start)
+            run_frame(clock0 + 16 * f)
+            ends = []
+            for st in streams:
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(st)
+                ends.append(e)
+            for e in ends:
+                e.synchronize()
+            ms.append(max(start.elapsed_time(e) for e in ends))
+        return ms
+
+    for t in tracers:
+        t.set_graph(True)
+
+    def separate(clock):
+        for t in tracers:
+            t.frame(SPP, clock)
+
+    def serial(clock):
+        # One scene after another, as the reference's trace worker runs them.
+        for k, t in enumerate(tracers):
+            if k:
+                e = torch.cuda.Event()
+                e.record(streams[k - 1])
+                streams[k].wait_event(e)
+            t.frame(SPP, clock)
+
+    def reset():
+        for t, (_, _, faces, _) in zip(tracers, scenes):
+            t.set_faces(faces)  # empty caches again: every run traces the same frames
+
+    warm_ser = timed(serial, warmup, 0)
+    census = sum(t.census(SPP)["rays"] for t in tracers)
+    ser = timed(serial, steps, 16 * warmup)
+    reset()
+    warm_sep = timed(separate, warmup, 0)
+    sep = timed(separate, steps, 16 * warmup)
+    for t in tracers:
+        t.set_graph(False)
+    reset()
+    batch = vgi.GpuBatch(tracers)
+    tune = batch.autotune(SPP)
+    batch.set_graph(True)
+    warm_bat = timed(lambda clock: batch.frame(SPP, clock), warmup, 0)
+    bat = timed(lambda clock: batch.frame(SPP, clock), steps, 16 * warmup)
+    batch.close()
+    for t in tracers:
+        t.close()
+    sep_ms, bat_ms, ser_ms = float(np.mean(sep)), float(np.mean(bat)), float(np.mean(ser))
+    faces_total = int(sum(f.shape[0] for _, _, f, _ in scenes))
+    extents = [e for _, _, _, e in scenes]
+    return {
+        "scenes": n_scenes, "faces": faces_total,
+        "faces_min_max": [int(min(f.shape[0] for _, _, f, _ in scenes)), int(max(f.shape[0] for _, _, f, _ in scenes))],
+        "extent_voxels_min_max": [int(min(min(e) for e in extents)), int(max(max(e) for e in extents))],
+        "spp": SPP, "bounces": BOUNCES, "rays_per_frame": int(census),
+        "serial_ms_per_frame": ser_ms, "separate_ms_per_frame": sep_ms, "batched_ms_per_frame": bat_ms,
+        "serial_rays_per_s": census / (ser_ms * 1e-3), "separate_rays_per_s": census / (sep_ms * 1e-3),
+        "batched_rays_per_s": census / (bat_ms * 1e-3),
+        "speedup_vs_serial": ser_ms / bat_ms, "speedup_vs_separate_streams": sep_ms / bat_ms, "autotune": tune,
+        "note": "rays per frame from a census after the warm-up frames; both runs trace identical frames from empty caches",
+    }
+
+
 def profile_mlp(frames=3):
     """A small MLP cache workload for ncu captures of the network kernels:
     the same generator at 256x256x256 voxels (64 emissive voxels), faces
@@ -416,6 +546,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default layout (for profiling runs)")
     ap.add_argument("--no-mlp", action="store_true", help="skip the MLP cache comparison")
     ap.add_argument("--profile-mlp", action="store_true", help="only a small MLP cache workload, for ncu captures")
+    ap.add_argument("--batch-scenes", type=int, default=32, help="scenes in the batched-scene comparison (0: skip it)")
     args = ap.parse_args()
     if args.profile_mlp:
         profile_mlp()
@@ -554,6 +685,9 @@ def main():
             # After the CPU baseline, which reads the plain trace's warm state.
             plain = {"frames": plain_frames, "ms_per_frame": graph_ms, "relmse": quality["value"]}
             mlp, clock = mlp_comparison(g, faces, reference, stream, flush, plain, clock, max_frames=max(4 * plain_frames, 64))
+        batched = None
+        if args.batch_scenes > 0:
+            batched = batch_comparison(local, stream, flush, args.batch_scenes, args.steps, args.warmup)
         line = {
             "metric": METRIC,
             "value": total_rays / (total_ms * 1e-3),
@@ -592,6 +726,7 @@ def main():
             "clocks": clocks,
             "relmse": quality,
             "mlp_cache": mlp,
+            "batched_scenes": batched,
         }
         if base:
             line["cpu_baseline"] = base

@@ -1695,9 +1695,10 @@ void vgi_directional_light_record(const float* d, const float* radiance3, const 
 struct vgi_batch {
     std::vector<vgi_ctx*> ctxs;
     int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t done = nullptr;
-    std::vector<cudaEvent_t> ready;
+    cudaStream_t stream = nullptr;           // batched traversals; the frame's start and end
+    cudaEvent_t done = nullptr, fork = nullptr;
+    std::vector<cudaEvent_t> ready, join;
+    std::vector<cudaStream_t> side;          // one per scene: its own kernels
     DevBuf<uint8_t> args;                    // the traversal's argument table on the device
     std::vector<uint8_t> table;              // ... and the host copy it was made from
     DevBuf<uint32_t> head;                   // the batched traversal's shared queue head
@@ -1780,10 +1781,16 @@ int batch_scenes(vgi_batch* b, uint32_t samples, bool scratch, std::vector<WaveS
     return VGI_OK;
 }
 
-void batch_trace(vgi_batch* b, const std::vector<WaveScene>& scenes) {
+void batch_trace(vgi_batch* b, const std::vector<WaveScene>& scenes, const AccumArgs* acc = nullptr, bool capture = false) {
     const vgi_ctx* c0 = b->ctxs[0];
-    launch_wave_batch(scenes.data(), (uint32_t)scenes.size(), b->args.ptr, b->head.ptr, c0->transport.bounces, transport_limited(c0),
-                      c0->transport.budgeted != 0, b->blocks, b->refill_min, b->stream);
+    BatchStreams st{b->stream, b->side.data(), b->fork, b->join.data(), b->head.ptr, b->blocks, b->refill_min};
+    if (capture) {
+        b->prepare_nodes.assign(scenes.size(), nullptr);
+        b->accumulate_nodes.assign(scenes.size(), nullptr);
+    }
+    launch_wave_batch(scenes.data(), (uint32_t)scenes.size(), b->args.ptr, c0->transport.bounces, transport_limited(c0),
+                      c0->transport.budgeted != 0, st, acc, capture ? b->prepare_nodes.data() : nullptr,
+                      capture ? b->accumulate_nodes.data() : nullptr);
 }
 
 // Orders the batch stream after every scene's stream.
@@ -1799,15 +1806,6 @@ int batch_leave(vgi_batch* b) {
     VGI_BCUDA(b, cudaEventRecord(b->done, b->stream));
     for (vgi_ctx* c : b->ctxs) VGI_BCUDA(b, cudaStreamWaitEvent(c->stream, b->done, 0));
     return VGI_OK;
-}
-
-// The node that the last launch on a capturing stream added.
-cudaGraphNode_t last_captured(cudaStream_t s) {
-    cudaStreamCaptureStatus status;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t n = 0;
-    if (cudaStreamGetCaptureInfo(s, &status, nullptr, nullptr, &deps, &n) != cudaSuccess || n != 1) return nullptr;
-    return deps[0];
 }
 
 cudaError_t set_node_args(cudaGraphExec_t exec, cudaGraphNode_t node, const AccumArgs& acc) {
@@ -1836,10 +1834,15 @@ int vgi_batch_create(vgi_ctx* const* ctxs, uint32_t n, vgi_batch** out) {
     b->blocks = ctxs[0]->traverse_blocks;
     b->refill_min = ctxs[0]->refill_min;
     b->ready.resize(n, nullptr);
+    b->join.resize(n, nullptr);
+    b->side.resize(n, nullptr);
     cudaError_t e = cudaSetDevice(b->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&b->ready[i], cudaEventDisableTiming);
+    for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+    for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = b->head.reserve(1);
     if (e != cudaSuccess) {
         vgi_batch_destroy(b);
@@ -1858,6 +1861,11 @@ int vgi_batch_destroy(vgi_batch* b) {
     b->head.release();
     for (cudaEvent_t e : b->ready)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : b->join)
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t s : b->side)
+        if (s) cudaStreamDestroy(s);
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->done) cudaEventDestroy(b->done);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -1898,15 +1906,7 @@ int vgi_batch_frame(vgi_batch* b, uint32_t samples, uint32_t clock_ms) {
             batch_drop_graph(b);
             VGI_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         }
-        for (uint32_t i = 0; i < n; ++i) {
-            launch_prepare(acc[i], b->stream);
-            if (capture) b->prepare_nodes.push_back(last_captured(b->stream));
-        }
-        batch_trace(b, scenes);
-        for (uint32_t i = 0; i < n; ++i) {
-            launch_accumulate(acc[i], b->stream);
-            if (capture) b->accumulate_nodes.push_back(last_captured(b->stream));
-        }
+        batch_trace(b, scenes, acc.data(), capture);
         if (capture) {
             cudaGraph_t g = nullptr;
             const cudaError_t e = cudaStreamEndCapture(b->stream, &g);

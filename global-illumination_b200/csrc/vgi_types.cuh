@@ -99,8 +99,20 @@ constexpr uint32_t kMaxBatchScenes = 256;
 uint32_t wave_batch_stages(uint32_t hits);
 size_t wave_args_bytes();
 void wave_batch_args(const WaveScene* scenes, uint32_t n, uint32_t hits, void* out);
-void launch_wave_batch(const WaveScene* scenes, uint32_t n, const void* device_args, uint32_t* head, uint32_t hits, bool limited,
-                       bool budgeted, uint32_t blocks, uint32_t refill_min, cudaStream_t s);
+// The streams of a batched frame: the batched traversals run on `main`,
+// each scene's own kernels on side[i]; fork and join[i] order them.
+struct BatchStreams {
+    cudaStream_t main;
+    const cudaStream_t* side;
+    cudaEvent_t fork;
+    const cudaEvent_t* join;
+    uint32_t* head;            // the batched traversal's shared queue head
+    uint32_t blocks, refill_min;
+};
+// acc (null: trace only) gives each scene's prepare and accumulate; when
+// capturing, their graph nodes are stored in prepare_nodes / accumulate_nodes.
+void launch_wave_batch(const WaveScene* scenes, uint32_t n, const void* device_args, uint32_t hits, bool limited, bool budgeted,
+                       const BatchStreams& st, const AccumArgs* acc, cudaGraphNode_t* prepare_nodes, cudaGraphNode_t* accumulate_nodes);
 
 // The view tier's buffers and controls (vgi_view.cuh) for n receivers.
 struct ViewArgs {

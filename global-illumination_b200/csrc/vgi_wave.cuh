@@ -1210,31 +1210,69 @@ WaveArgs stage_args(const WaveBuffers& b, const TraceArgs& a, uint32_t k) {
     return W;
 }
 
+// The node the last launch on a capturing stream added (null when the
+// stream is not capturing).
+cudaGraphNode_t last_node(cudaStream_t s) {
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t n = 0;
+    if (cudaStreamGetCaptureInfo(s, &status, nullptr, nullptr, &deps, &n) != cudaSuccess || status != cudaStreamCaptureStatusActive ||
+        n != 1)
+        return nullptr;
+    return deps[0];
+}
+
+// Each scene's own kernels run on its side stream, so the scenes' small
+// kernels overlap; the side streams join the main stream for each stage's
+// batched traversal and fork from it afterwards.
 template <uint32_t H, bool L, bool B>
-void wave_batch_run(const WaveScene* sc, uint32_t n, const WaveArgs* device_args, uint32_t* head, uint32_t blocks, uint32_t refill_min,
-                    cudaStream_t s) {
+void wave_batch_run(const WaveScene* sc, uint32_t n, const WaveArgs* device_args, const BatchStreams& st, const AccumArgs* acc,
+                    cudaGraphNode_t* prepare_nodes, cudaGraphNode_t* accumulate_nodes) {
+    auto fork = [&]() {
+        cudaEventRecord(st.fork, st.main);
+        for (uint32_t i = 0; i < n; ++i) cudaStreamWaitEvent(st.side[i], st.fork, 0);
+    };
+    auto join = [&]() {
+        for (uint32_t i = 0; i < n; ++i) {
+            cudaEventRecord(st.join[i], st.side[i]);
+            cudaStreamWaitEvent(st.main, st.join[i], 0);
+        }
+    };
+    fork();
     for (uint32_t i = 0; i < n; ++i) {
+        const cudaStream_t s = st.side[i];
+        if (acc) {
+            launch_prepare(acc[i], s);
+            if (prepare_nodes) prepare_nodes[i] = last_node(s);
+        }
         const WaveArgs W = stage_args(sc[i].b, sc[i].a, 0);
         cudaMemsetAsync(W.count_out, 0, sizeof(uint32_t), s);
         wave_begin_kernel<H, L, B, false><<<(W.n_paths + kWaveBlock - 1) / kWaveBlock, kWaveBlock, 0, s>>>(W);
     }
     for (uint32_t stage = 1; stage <= H + 1u; ++stage) {
-        cudaMemsetAsync(head, 0, sizeof(uint32_t), s);
-        wave_traverse_batch_kernel<B><<<blocks, kWaveBlock, 0, s>>>(device_args + (size_t)(stage - 1u) * n, n, head, refill_min);
-        if (stage == H + 1u) break;
+        join();
+        cudaMemsetAsync(st.head, 0, sizeof(uint32_t), st.main);
+        wave_traverse_batch_kernel<B><<<st.blocks, kWaveBlock, 0, st.main>>>(device_args + (size_t)(stage - 1u) * n, n, st.head, st.refill_min);
+        fork();
         for (uint32_t i = 0; i < n; ++i) {
+            const cudaStream_t s = st.side[i];
             const WaveArgs W = stage_args(sc[i].b, sc[i].a, stage);
-            cudaMemsetAsync(W.count_out, 0, sizeof(uint32_t), s);
-            cudaMemsetAsync(W.scatter_count, 0, sizeof(uint32_t), s);
-            wave_shade_kernel<H, L, B, false><<<(W.n_paths + kWaveBlock - 1) / kWaveBlock, kWaveBlock, 0, s>>>(W, stage);
-            wave_scatter_kernel<H, L, B, false><<<sc[i].b.traverse_blocks, kWaveBlock, 0, s>>>(W);
+            if (stage <= H) {
+                cudaMemsetAsync(W.count_out, 0, sizeof(uint32_t), s);
+                cudaMemsetAsync(W.scatter_count, 0, sizeof(uint32_t), s);
+                wave_shade_kernel<H, L, B, false><<<(W.n_paths + kWaveBlock - 1) / kWaveBlock, kWaveBlock, 0, s>>>(W, stage);
+                wave_scatter_kernel<H, L, B, false><<<sc[i].b.traverse_blocks, kWaveBlock, 0, s>>>(W);
+            } else {
+                const uint32_t face_blocks = (uint32_t)((((uint64_t)sc[i].a.n_tasks << sc[i].a.lanes_log2) + kWaveBlock - 1) / kWaveBlock);
+                wave_finalize_kernel<H, L, B, false><<<face_blocks, kWaveBlock, 0, s>>>(W);
+                if (acc) {
+                    launch_accumulate(acc[i], s);
+                    if (accumulate_nodes) accumulate_nodes[i] = last_node(s);
+                }
+            }
         }
     }
-    for (uint32_t i = 0; i < n; ++i) {
-        const WaveArgs W = stage_args(sc[i].b, sc[i].a, H + 1u);
-        const uint32_t face_blocks = (uint32_t)((((uint64_t)sc[i].a.n_tasks << sc[i].a.lanes_log2) + kWaveBlock - 1) / kWaveBlock);
-        wave_finalize_kernel<H, L, B, false><<<face_blocks, kWaveBlock, 0, s>>>(W);
-    }
+    join();
 }
 
 }  // namespace
@@ -1250,12 +1288,12 @@ void wave_batch_args(const WaveScene* sc, uint32_t n, uint32_t hits, void* out) 
         for (uint32_t i = 0; i < n; ++i) dst[(size_t)(k - 1u) * n + i] = stage_args(sc[i].b, sc[i].a, k);
 }
 
-void launch_wave_batch(const WaveScene* sc, uint32_t n, const void* args, uint32_t* head, uint32_t hits, bool limited, bool budgeted,
-                       uint32_t blocks, uint32_t refill_min, cudaStream_t s) {
+void launch_wave_batch(const WaveScene* sc, uint32_t n, const void* args, uint32_t hits, bool limited, bool budgeted,
+                       const BatchStreams& st, const AccumArgs* acc, cudaGraphNode_t* prepare_nodes, cudaGraphNode_t* accumulate_nodes) {
     if (n == 0 || n > kMaxBatch) return;
     const WaveArgs* device_args = static_cast<const WaveArgs*>(args);
     const uint32_t h = hits <= 1 ? 1u : hits > 3 ? 3u : hits;
-#define VGI_BATCH(HH, LL, BB) wave_batch_run<HH, LL, BB>(sc, n, device_args, head, blocks, refill_min, s)
+#define VGI_BATCH(HH, LL, BB) wave_batch_run<HH, LL, BB>(sc, n, device_args, st, acc, prepare_nodes, accumulate_nodes)
     if (h == 1) {
         if (limited) { if (budgeted) VGI_BATCH(1, true, true); else VGI_BATCH(1, true, false); }
         else { if (budgeted) VGI_BATCH(1, false, true); else VGI_BATCH(1, false, false); }
