@@ -1018,6 +1018,56 @@ int vgi_frame(vgi_ctx* c, uint32_t samples, uint32_t clock_ms) {
     return VGI_OK;
 }
 
+int vgi_frame_shard(vgi_ctx* c, uint32_t samples, uint32_t clock_ms, uint32_t first, uint32_t n) {
+    int rc = check_ready(c, true);
+    if (rc != VGI_OK) return rc;
+    if (samples == 0 || n == 0) return fail(c, VGI_ERR_INVALID, "samples and the shard's slots must be positive");
+    if (first > c->n_slots || n > c->n_slots - first) return fail(c, VGI_ERR_INVALID, "shard outside the slots");
+    if (c->mlp_cache) return fail(c, VGI_ERR_STATE, "the MLP cache mode traces whole frames");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    // The shard's slots are a contiguous range: every per-slot array starts
+    // at `first`, and the traced count is n. The gather still reads every
+    // slot's record (the face index covers all faces).
+    AccumArgs acc = accum_args(c, samples, clock_ms);
+    acc.state += (size_t)first * 9;
+    acc.slot_meta += (size_t)first * 3;
+    acc.checkpoint += (size_t)first * 3;
+    acc.outputs += (size_t)first * 6;
+    acc.tasks += (size_t)first * 2;
+    acc.cache += first;
+    acc.n = n;
+    acc.controls[0] = acc.controls[5] = acc.controls[14] = acc.controls[24] = n;
+    launch_prepare(acc, c->stream);
+    TraceArgs tr = trace_args(c, c->tasks.ptr + (size_t)first * 2, c->results.ptr + (size_t)first * 6, n, samples, true);
+    rc = run_trace(c, tr, false, false);
+    if (rc != VGI_OK) return rc;
+    launch_accumulate(acc, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
+    if (c->batch_id == 0) c->batch_id = 1;
+    return VGI_OK;
+}
+
+int vgi_read_cache(vgi_ctx* c, uint32_t first, uint32_t n, float* dst4, int on_device) {
+    if (!c || (n && !dst4) || first > c->n_slots || n > c->n_slots - first) return VGI_ERR_INVALID;
+    if (n == 0) return VGI_OK;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, cudaMemcpyAsync(dst4, c->cache.ptr + first, (size_t)n * 16, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                c->stream));
+    if (!on_device) VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_write_cache(vgi_ctx* c, uint32_t first, uint32_t n, const float* src4, int on_device) {
+    if (!c || (n && !src4) || first > c->n_slots || n > c->n_slots - first) return VGI_ERR_INVALID;
+    if (n == 0) return VGI_OK;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, cudaMemcpyAsync(c->cache.ptr + first, src4, (size_t)n * 16, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                c->stream));
+    if (!on_device) VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
 int vgi_set_layout(vgi_ctx* c, uint32_t layout, uint32_t refill_min) {
     if (c) drop_graph(c);  // what a frame launches may change
     if (!c) return VGI_ERR_INVALID;

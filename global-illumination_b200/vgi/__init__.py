@@ -183,6 +183,9 @@ _SIGNATURES = {
     "vgi_mlp_encode": (_INT, [_P, _P, _U32, _P]),
     "vgi_set_mlp_cache": (_INT, [_P, ctypes.c_int, _U32, _U32, _U32, ctypes.c_float]),
     "vgi_mlp_stats": (_INT, [_P, _P]),
+    "vgi_frame_shard": (_INT, [_P, _U32, _U32, _U32, _U32]),
+    "vgi_read_cache": (_INT, [_P, _U32, _U32, _P, ctypes.c_int]),
+    "vgi_write_cache": (_INT, [_P, _U32, _U32, _P, ctypes.c_int]),
     "vgi_batch_create": (_INT, [_P, _U32, _P]),
     "vgi_batch_destroy": (_INT, [_P]),
     "vgi_batch_last_error": (ctypes.c_char_p, [_P]),
@@ -562,6 +565,28 @@ class GpuTracer:
         out = np.zeros((f.shape[0], 96), np.float32)
         self._check(self._lib.vgi_mlp_encode(self._h, _ptr(f), f.shape[0], _ptr(out)))
         return out
+
+    # face-sharded frames
+    def frame_shard(self, samples: int, clock_ms: int, first: int, n: int) -> None:
+        """prepare, trace and accumulate of slots [first, first + n) only."""
+        self._check(self._lib.vgi_frame_shard(self._h, samples, clock_ms, first, n))
+
+    def read_cache(self, first: int, n: int) -> np.ndarray:
+        """Gather records of slots [first, first + n): (n, 4) u32 words."""
+        out = np.zeros((n, 4), np.uint32)
+        self._check(self._lib.vgi_read_cache(self._h, first, n, _ptr(out), 0))
+        return out
+
+    def write_cache(self, first: int, n: int, records: np.ndarray) -> None:
+        r = _c(records, np.uint32).reshape(n, 4)
+        self._check(self._lib.vgi_write_cache(self._h, first, n, _ptr(r), 0))
+
+    def read_cache_device(self, first: int, n: int, device_ptr: int) -> None:
+        """Enqueues a copy of the records into device memory (context stream)."""
+        self._check(self._lib.vgi_read_cache(self._h, first, n, ctypes.c_void_p(device_ptr), 1))
+
+    def write_cache_device(self, first: int, n: int, device_ptr: int) -> None:
+        self._check(self._lib.vgi_write_cache(self._h, first, n, ctypes.c_void_p(device_ptr), 1))
 
     def set_mlp_cache(self, enable: bool = True, warm_frames: int = 8, samples: int = 65536, steps_per_frame: int = 16,
                       lr: float = 1e-2) -> None:

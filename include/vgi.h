@@ -300,6 +300,24 @@ typedef struct vgi_mlp_status {
 /* Synchronous. */
 int vgi_mlp_stats(vgi_ctx* ctx, vgi_mlp_status* out);
 
+/* ---- face-sharded frames -------------------------------------------------------
+ * No counterpart in the reference. Faces are independent given the frame's
+ * geometry and the world cache's snapshot, so a frame can be split across
+ * GPUs by slot range. Every rank's context holds all faces (vgi_set_faces
+ * with the full list: the face index and one 16-byte gather record per
+ * slot), but vgi_frame_shard prepares, traces and accumulates only slots
+ * [first, first + n). Between frames every rank publishes its range's
+ * gather records (vgi_read_cache) and takes the others' (vgi_write_cache),
+ * for example with one all-gather; the next frame then gathers from the
+ * same snapshot a single GPU would, so every slot's results and state are
+ * those of vgi_frame. Records are 4 words: mean rgb, the count word (bits).
+ * With on_device set the pointer is device memory of the context's device
+ * and the copy is enqueued on the context's stream; otherwise it is host
+ * memory and the call is synchronous. */
+int vgi_frame_shard(vgi_ctx* ctx, uint32_t samples, uint32_t clock_ms, uint32_t first, uint32_t n);
+int vgi_read_cache(vgi_ctx* ctx, uint32_t first, uint32_t n, float* dst4, int on_device);
+int vgi_write_cache(vgi_ctx* ctx, uint32_t first, uint32_t n, const float* src4, int on_device);
+
 /* ---- batched scenes ----------------------------------------------------------
  * No counterpart in the reference (its scenes are traced one at a time):
  * several contexts, one per scene, traced together. vgi_batch_frame runs

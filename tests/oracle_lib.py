@@ -266,6 +266,27 @@ def _trace_faces_predicted(geometry, params, materials, lights, emitter_words, t
     return out, d
 
 
+class OracleShardTracer:
+    """The oracle as a face-sharding tracer (the CPU stand-in for a GPU rank
+    in the sharding tests). Its gather reads the slots' state rows, so its
+    records are whole 36-word state rows."""
+
+    record_words = 36
+
+    def __init__(self, frames: "Frames"):
+        self.frames = frames
+        self.cache_hits = 0
+
+    def frame_shard(self, samples, clock_ms, first, n):
+        self.cache_hits += self.frames.frame_shard(samples, clock_ms, first, n)["cache_hits"]
+
+    def read_cache(self, first, n):
+        return self.frames.state[first:first + n].copy()
+
+    def write_cache(self, first, n, records):
+        self.frames.state[first:first + n] = np.asarray(records, np.uint32).reshape(n, 36)
+
+
 def controls_words(n, samples, clock_ms, transport, batch_id=1, n_events=0):
     """The Controls words the product's frame uses (src/gpu/resident.rs:708-760)."""
     w = np.zeros(36, np.uint32)
@@ -334,6 +355,23 @@ class Frames:
                                self.state, self.index, self.threads, predicted)
         L.orc_accumulate(ptr(self.state), ptr(self.meta), ptr(self.checkpoint), ptr(out), ptr(self.slots), self.n, ptr(ctl))
         self.results = out
+        self.batch_id = (self.batch_id + 1) & 0x0FFFFFFF or 1
+        return cnt
+
+    def frame_shard(self, samples, clock_ms, first, n):
+        """frame() over slots [first, first + n) only (vgi_frame_shard)."""
+        ctl = controls_words(n, samples, clock_ms, self.transport, self.batch_id)
+        L = lib()
+        slots = np.arange(first, first + n, dtype=np.uint32)
+        tasks = np.ascontiguousarray(self.tasks[first:first + n])
+        L.orc_begin_trace(ptr(self.state), ptr(self.meta), ptr(tasks), ptr(slots), n, ptr(ctl))
+        L.orc_mark_changed(ptr(self.state), ptr(self.meta), ptr(slots), n, ptr(ctl))
+        params = self.params_fn(n, samples)
+        out, cnt = trace_faces(self.geometry, params, self.materials, self.lights, self.emitter_words, tasks, self.pipe, self.state,
+                               self.index, self.threads)
+        L.orc_accumulate(ptr(self.state), ptr(self.meta), ptr(self.checkpoint), ptr(out), ptr(slots), n, ptr(ctl))
+        self.tasks[first:first + n] = tasks
+        self.results[first:first + n] = out
         self.batch_id = (self.batch_id + 1) & 0x0FFFFFFF or 1
         return cnt
 
