@@ -106,6 +106,13 @@ struct vgi_ctx {
     DevBuf<uint4> tasks, results, state, slot_meta, checkpoint, face_index;
     DevBuf<float4> cache;
     DevBuf<uint4> scratch_tasks, scratch_results;
+    // Pipelined batches (vgi_submit_batch): host copies on their own streams
+    // through two device staging buffers each way, so a batch's copies
+    // overlap the frames around it.
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    DevBuf<uint4> stage_tasks[2], stage_results[2];
+    cudaEvent_t tasks_ready[2] = {}, tasks_free[2] = {}, results_ready[2] = {}, results_done[2] = {};
+    uint64_t submitted = 0;
     // view tier: receivers, paths, continuations, estimates, owner queue, events
     DevBuf<uint4> v_receivers, v_paths, v_conts, v_estimates, v_events, v_scratch;
     DevBuf<uint32_t> v_queue;
@@ -558,6 +565,14 @@ int vgi_destroy(vgi_ctx* c) {
         if (e) cudaEventDestroy(e);
     for (auto& e : c->mlp_marks)
         if (e) cudaEventDestroy(e);
+    for (int k = 0; k < 2; ++k) {
+        c->stage_tasks[k].release();
+        c->stage_results[k].release();
+        for (cudaEvent_t e : {c->tasks_ready[k], c->tasks_free[k], c->results_ready[k], c->results_done[k]})
+            if (e) cudaEventDestroy(e);
+    }
+    if (c->copy_in) cudaStreamDestroy(c->copy_in);
+    if (c->copy_out) cudaStreamDestroy(c->copy_out);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return VGI_OK;
@@ -1114,6 +1129,54 @@ int vgi_trace_batch(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samp
     if (rc != VGI_OK) return rc;
     VGI_CUDA(c, cudaMemcpyAsync(results, c->results.ptr, (size_t)n * 96, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_submit_batch(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samples, uint32_t clock_ms, uint32_t* results,
+                     uint64_t* ticket) {
+    int rc = check_ready(c, true);
+    if (rc != VGI_OK) return rc;
+    if (!tasks || !results || n != c->n_slots) return fail(c, VGI_ERR_INVALID, "one task per slot expected");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    if (!c->copy_in) {
+        VGI_CUDA(c, cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
+        VGI_CUDA(c, cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k)
+            for (cudaEvent_t* e : {&c->tasks_ready[k], &c->tasks_free[k], &c->results_ready[k], &c->results_done[k]})
+                VGI_CUDA(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    const uint64_t k = c->submitted;
+    const int b = (int)(k & 1u);
+    const bool reused = k >= 2;  // this staging pair served batch k - 2
+    VGI_CUDA(c, c->stage_tasks[b].reserve((size_t)n * 2));
+    VGI_CUDA(c, c->stage_results[b].reserve((size_t)n * 6));
+    // Tasks in: after the frame of batch k - 2 has taken its staged tasks.
+    if (reused) VGI_CUDA(c, cudaStreamWaitEvent(c->copy_in, c->tasks_free[b], 0));
+    VGI_CUDA(c, cudaMemcpyAsync(c->stage_tasks[b].ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->copy_in));
+    VGI_CUDA(c, cudaEventRecord(c->tasks_ready[b], c->copy_in));
+    // The frame, between the staged tasks and the staged results.
+    VGI_CUDA(c, cudaStreamWaitEvent(c->stream, c->tasks_ready[b], 0));
+    VGI_CUDA(c, cudaMemcpyAsync(c->tasks.ptr, c->stage_tasks[b].ptr, (size_t)n * 32, cudaMemcpyDeviceToDevice, c->stream));
+    VGI_CUDA(c, cudaEventRecord(c->tasks_free[b], c->stream));
+    rc = vgi_frame(c, samples, clock_ms);
+    if (rc != VGI_OK) return rc;
+    if (reused) VGI_CUDA(c, cudaStreamWaitEvent(c->stream, c->results_done[b], 0));
+    VGI_CUDA(c, cudaMemcpyAsync(c->stage_results[b].ptr, c->results.ptr, (size_t)n * 96, cudaMemcpyDeviceToDevice, c->stream));
+    VGI_CUDA(c, cudaEventRecord(c->results_ready[b], c->stream));
+    // Results out, while the next frames run.
+    VGI_CUDA(c, cudaStreamWaitEvent(c->copy_out, c->results_ready[b], 0));
+    VGI_CUDA(c, cudaMemcpyAsync(results, c->stage_results[b].ptr, (size_t)n * 96, cudaMemcpyDeviceToHost, c->copy_out));
+    VGI_CUDA(c, cudaEventRecord(c->results_done[b], c->copy_out));
+    c->submitted = k + 1;
+    if (ticket) *ticket = k;
+    return VGI_OK;
+}
+
+int vgi_complete_batch(vgi_ctx* c, uint64_t ticket) {
+    if (!c) return VGI_ERR_INVALID;
+    if (ticket >= c->submitted) return fail(c, VGI_ERR_INVALID, "no such batch submitted");
+    if (c->submitted - ticket > 2) return VGI_OK;  // its staging pair has been reused since: it completed before that
+    VGI_CUDA(c, cudaEventSynchronize(c->results_done[ticket & 1u]));
     return VGI_OK;
 }
 

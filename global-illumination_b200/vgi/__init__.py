@@ -184,6 +184,8 @@ _SIGNATURES = {
     "vgi_set_mlp_cache": (_INT, [_P, ctypes.c_int, _U32, _U32, _U32, ctypes.c_float]),
     "vgi_mlp_stats": (_INT, [_P, _P]),
     "vgi_frame_shard": (_INT, [_P, _U32, _U32, _U32, _U32]),
+    "vgi_submit_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P, _P]),
+    "vgi_complete_batch": (_INT, [_P, _U64]),
     "vgi_read_cache": (_INT, [_P, _U32, _U32, _P, ctypes.c_int]),
     "vgi_write_cache": (_INT, [_P, _U32, _U32, _P, ctypes.c_int]),
     "vgi_batch_create": (_INT, [_P, _U32, _P]),
@@ -565,6 +567,17 @@ class GpuTracer:
         out = np.zeros((f.shape[0], 96), np.float32)
         self._check(self._lib.vgi_mlp_encode(self._h, _ptr(f), f.shape[0], _ptr(out)))
         return out
+
+    def submit_batch(self, tasks: np.ndarray, samples: int, clock_ms: int, out: np.ndarray) -> int:
+        """vgi_submit_batch: returns a ticket; `tasks` and `out` (ideally
+        pinned) must stay alive and unchanged until complete_batch(ticket)."""
+        assert tasks.dtype == np.uint32 and tasks.flags.c_contiguous and out.dtype == np.uint32 and out.flags.c_contiguous
+        ticket = ctypes.c_uint64()
+        self._check(self._lib.vgi_submit_batch(self._h, _ptr(tasks), tasks.shape[0], samples, clock_ms, _ptr(out), ctypes.byref(ticket)))
+        return ticket.value
+
+    def complete_batch(self, ticket: int) -> None:
+        self._check(self._lib.vgi_complete_batch(self._h, ticket))
 
     # face-sharded frames
     def frame_shard(self, samples: int, clock_ms: int, first: int, n: int) -> None:

@@ -175,6 +175,19 @@ int vgi_frame_times(vgi_ctx* ctx, float* ms4);
  * 8-word tasks in (one per slot, in slot order; their sequence words are
  * replaced by the slot's), 24-word results out. Synchronous. */
 int vgi_trace_batch(vgi_ctx* ctx, const uint32_t* tasks, uint32_t n, uint32_t samples, uint32_t clock_ms, uint32_t* results);
+/* vgi_trace_batch without the wait: the tasks are copied in and the results
+ * out on the context's copy streams through device staging buffers, so a
+ * batch's copies overlap the frames before and after it, like the crate's
+ * submit_compact / complete_readback with batches in flight (gpu.rs:647-1170).
+ * Returns at once with a ticket; vgi_complete_batch(ticket) waits until
+ * `results` holds the batch's FaceResults. The host buffers (pinned memory,
+ * for copies that overlap) must stay valid and unchanged until then. Two
+ * batches may be in flight: submitting a third waits, on the device, for
+ * the first's copies. Frames run in submission order on the context's
+ * stream; other calls on the context order after the submitted frames. */
+int vgi_submit_batch(vgi_ctx* ctx, const uint32_t* tasks, uint32_t n, uint32_t samples, uint32_t clock_ms, uint32_t* results,
+                     uint64_t* ticket);
+int vgi_complete_batch(vgi_ctx* ctx, uint64_t ticket);
 /* A counting trace of the next frame's work (no state change): rays, paths,
  * steps and algorithmic bytes. Synchronous. */
 int vgi_census(vgi_ctx* ctx, uint32_t samples, vgi_counters* counters);
