@@ -1256,6 +1256,7 @@ int vgi_trace_tasks(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samp
     int rc = check_ready(c, false);
     if (rc != VGI_OK) return rc;
     if (!tasks || !results) return VGI_ERR_INVALID;
+    if (samples == 0) return fail(c, VGI_ERR_INVALID, "samples must be positive");
     if (n == 0) return VGI_OK;
     VGI_CUDA(c, c->scratch_tasks.reserve((size_t)n * 2));
     VGI_CUDA(c, c->scratch_results.reserve((size_t)n * 6));
