@@ -225,7 +225,8 @@ def mlp_comparison(g, faces, ref, stream, flush, plain, clock, max_frames):
         e.synchronize()
         frame_ms.append(s.elapsed_time(e))
         total += frame_ms[-1]
-        value = relmse_now(g, ref) if (f + 1) % 2 == 0 or f + 1 == plain["frames"] else None
+        every = 2 if f < 64 else 4
+        value = relmse_now(g, ref) if (f + 1) % every == 0 or f + 1 == plain["frames"] else None
         if value is not None:
             curve.append([f + 1, round(total, 2), round(value, 6)])
             if f + 1 == plain["frames"]:
@@ -699,7 +700,7 @@ def main():
         if not args.no_mlp:
             # After the CPU baseline, which reads the plain trace's warm state.
             plain = {"frames": plain_frames, "ms_per_frame": graph_ms, "relmse": quality["value"]}
-            mlp, clock = mlp_comparison(g, faces, reference, stream, flush, plain, clock, max_frames=max(4 * plain_frames, 64))
+            mlp, clock = mlp_comparison(g, faces, reference, stream, flush, plain, clock, max_frames=max(8 * plain_frames, 64))
         batched = None
         if args.batch_scenes > 0:
             batched = batch_comparison(local, stream, flush, args.batch_scenes, args.steps, args.warmup)
