@@ -177,7 +177,10 @@ __global__ void __launch_bounds__(kBlock) accumulate_kernel(AccumArgs a) {
     st[6] = disp;
     st[7] = s7;
     write_record(a.cache, slot, nm, count);
-    // record_stability (picked = false)
+    // record_stability; tasks from batch.x on are GPU picks, whose record
+    // reports the merged count and whose CPU mirror becomes stale.
+    const bool picked = i >= ctl[24];
+    if (picked && a.picks) a.picks[i].z = count;
     uint4* rank_p = a.slot_meta + slot * 3u + 2u;
     bool same_revision = (sched.y & 8u) != 0u && sched.w == ctl[16];
     uint32_t scount = count & 0x7fffffffu;
@@ -198,7 +201,8 @@ __global__ void __launch_bounds__(kBlock) accumulate_kernel(AccumArgs a) {
     sched.w = ctl[16];
     *sched_p = sched;
     uint4 rank = *rank_p;
-    *rank_p = make_uint4(f2b(sample_noise(nm, ns)), ctl[2], f2b(max3(rr, rg, rb)), 0x80000000u | scount | (rank.w & kMirrorStale));
+    *rank_p = make_uint4(f2b(sample_noise(nm, ns)), ctl[2], f2b(max3(rr, rg, rb)),
+                         0x80000000u | scount | (picked ? kMirrorStale : (rank.w & kMirrorStale)));
     uint4 w1 = s1;
     if ((sched.y & 15u) == 12u) w1.y |= 0x80000000u;
     out[0] = nm;
@@ -330,6 +334,203 @@ __global__ void __launch_bounds__(kBlock) seed_incarnations_kernel(uint4* state,
     if (slot < n) state[slot * 9u + 7u].x = slot + 1u;
 }
 
+// ---- GPU selection (voxel_accumulate.wgsl:448-695) ----------------------------
+// Controls words as the reference's Controls: counts.z = [2] clock ms;
+// limits.z = [14] slots; schedule = [16..19] (revision, stable error bits,
+// stable samples, audit interval ms); focus = [20..23] (voxel xyz, pick
+// budget); batch = [24..27] (CPU traced faces, batch id, classify range);
+// mirror.x = [32] mirror records per batch.
+constexpr uint32_t kBootstrap = 8u, kClasses = 4u;
+constexpr uint32_t kSelThreshold = 1024u, kSelRemainder = 1028u, kSelTies = 1032u, kSelTotal = 1036u, kSelMirrors = 1037u;
+
+__device__ __forceinline__ int page_axis(int p) { return (p - (p < 0 ? 31 : 0)) / 32; }
+
+// candidate (voxel_accumulate.wgsl:474-511): class (0 coverage, 1 refinement,
+// 2 sweep, 3 urgent) << 8 | key bucket, or kNoIndex.
+__device__ uint32_t candidate_key(const AccumArgs& a, uint32_t slot) {
+    const uint32_t* ctl = a.controls;
+    const uint4 identity = a.slot_meta[slot * 3u];
+    if ((identity.w & 8u) == 0u) return kNoIndex;
+    const uint4 schedule = a.slot_meta[slot * 3u + 1u];
+    const uint32_t last_cpu = schedule.y >> 4u;
+    if (last_cpu != 0u && ((ctl[25] - last_cpu) & 0x0fffffffu) < 4u) return kNoIndex;
+    const uint4 rank = a.slot_meta[slot * 3u + 2u];
+    const uint32_t count = rank.w & 0x1fffffffu;
+    const bool fresh = (schedule.y & 8u) != 0u && schedule.w == ctl[16];
+    const uint32_t since = ctl[2] - rank.y;
+    const uint32_t age_ms = rank.w < 0x80000000u ? 0x7fffffffu : (since > 0x7fffffffu ? 0u : since);
+    const uint32_t required = u2f(rank.z) < 0.02f ? (ctl[18] > 256u ? ctl[18] : 256u) : ctl[18];
+    const bool due = !fresh || count < required || (schedule.y & 7u) < 4u || age_ms >= ctl[19] || (rank.w & kUrgent) != 0u;
+    if (!due) return kNoIndex;
+    const int px = (int)identity.x, py = (int)identity.y, pz = (int)identity.z;
+    const int fx = (int)ctl[20], fy = (int)ctl[21], fz = (int)ctl[22];
+    if ((rank.w & kUrgent) != 0u || count < kBootstrap) {
+        const float dx = (float)(px - fx), dy = (float)(py - fy), dz = (float)(pz - fz);
+        const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+        const uint32_t b = f2u(__fmul_rn(own_log2(__fadd_rn(d2, 1.0f)), 8.0f));
+        return (((rank.w & kUrgent) != 0u ? 3u : 0u) << 8u) | (b < 255u ? b : 255u);
+    }
+    const int ax = abs(page_axis(px) - page_axis(fx)), ay = abs(page_axis(py) - page_axis(fy)), az = abs(page_axis(pz) - page_axis(fz));
+    const int page_distance = ax > ay ? (ax > az ? ax : az) : (ay > az ? ay : az);
+    if (page_distance <= 2) {
+        const float age = wmin(__fmul_rn((float)age_ms, 0.001f), 10.0f);
+        const float error = count < 2u ? 1.0f : wmin(__fdiv_rn(u2f(rank.x), __fsqrt_rn((float)count)), 8.0f);
+        const float priority = __fadd_rn(__fadd_rn(error, __fmul_rn(age, 0.1f)), page_distance <= 1 ? 0.25f : 0.0f);
+        const uint32_t b = f2u(__fmul_rn(wmax(__fadd_rn(own_log2(priority), 8.0f), 0.0f), 16.0f));
+        return (1u << 8u) | (255u - (b < 255u ? b : 255u));
+    }
+    const uint32_t b = f2u(__fmul_rn(own_log2(__fadd_rn((float)age_ms, 1.0f)), 8.0f));
+    return (2u << 8u) | (255u - (b < 255u ? b : 255u));
+}
+
+// select_classify: keys of the slots [batch.z, batch.w); faces whose
+// statistics mirror is stale are counted, and emitted up to mirror.x.
+__global__ void __launch_bounds__(kBlock) select_classify_kernel(AccumArgs a, uint32_t* keys, uint32_t* selection) {
+    __shared__ uint32_t group_mirrors, group_base;
+    const uint32_t* ctl = a.controls;
+    if (threadIdx.x == 0) group_mirrors = 0u;
+    __syncthreads();
+    const uint32_t slot = ctl[26] + blockIdx.x * kBlock + threadIdx.x;
+    bool stale = false;
+    uint32_t mirror_index = 0u;
+    if (slot < ctl[27]) {
+        keys[slot] = candidate_key(a, slot);
+        stale = (a.slot_meta[slot * 3u + 2u].w & kMirrorStale) != 0u && (a.slot_meta[slot * 3u].w & 8u) != 0u;
+        if (stale) mirror_index = atomicAdd(&group_mirrors, 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) group_base = group_mirrors > 0u ? atomicAdd(selection + kSelMirrors, group_mirrors) : 0u;
+    __syncthreads();
+    // No statistics mirror here beyond mirror.x records (the CPU mirror is
+    // the crate's): a face counted past it keeps its stale flag.
+    if (!stale || group_base + mirror_index >= ctl[32]) return;
+    a.slot_meta[slot * 3u + 2u].w &= ~kMirrorStale;
+}
+
+// select_histogram: per-class 256-bucket histograms of the keys.
+__global__ void __launch_bounds__(kBlock) select_histogram_kernel(const uint32_t* keys, uint32_t n_slots, uint32_t* selection) {
+    __shared__ uint32_t local[1024];
+    for (uint32_t b = threadIdx.x; b < 1024u; b += kBlock) local[b] = 0u;
+    __syncthreads();
+    const uint32_t id = blockIdx.x * kBlock + threadIdx.x;
+    if (id < n_slots) {
+        const uint32_t key = keys[id];
+        if (key != kNoIndex) atomicAdd(local + ((key >> 8u) < 3u ? (key >> 8u) : 3u) * 256u + (key & 255u), 1u);
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < 1024u; b += kBlock)
+        if (local[b] != 0u) atomicAdd(selection + b, local[b]);
+}
+
+// select_threshold: one block; inclusive scans of the histograms, the
+// per-class quotas (urgent first, then 1/4, 1/2, 1/4 with unused share lent
+// to refinement, coverage, sweep, urgent), the threshold bucket and the
+// ties it takes.
+__global__ void __launch_bounds__(kBlock) select_threshold_kernel(const uint32_t* controls_budget, uint32_t budget, uint32_t* selection) {
+    __shared__ uint32_t scan[1024];
+    __shared__ uint32_t taken[4];
+    const uint32_t t = threadIdx.x;
+    for (uint32_t c = 0; c < kClasses; ++c) scan[c * 256u + t] = selection[c * 256u + t];
+    __syncthreads();
+    for (uint32_t step = 1u; step < 256u; step <<= 1u) {
+        uint32_t add[4] = {0u, 0u, 0u, 0u};
+        for (uint32_t c = 0; c < kClasses; ++c)
+            if (t >= step) add[c] = scan[c * 256u + t - step];
+        __syncthreads();
+        for (uint32_t c = 0; c < kClasses; ++c) scan[c * 256u + t] += add[c];
+        __syncthreads();
+    }
+    if (t == 0u) {
+        uint32_t take[4] = {0u, 0u, 0u, 0u};
+        const uint32_t u = scan[3u * 256u + 255u], q = budget - budget / 4u;
+        take[3] = u < q ? u : q;
+        const uint32_t rest = budget - take[3];
+        take[0] = rest / 4u < scan[255u] ? rest / 4u : scan[255u];
+        take[1] = rest / 2u < scan[256u + 255u] ? rest / 2u : scan[256u + 255u];
+        const uint32_t r2 = rest - rest / 4u - rest / 2u;
+        take[2] = r2 < scan[512u + 255u] ? r2 : scan[512u + 255u];
+        uint32_t spare = budget - take[0] - take[1] - take[2] - take[3];
+        const uint32_t lend[4] = {1u, 0u, 2u, 3u};
+        for (uint32_t o = 0; o < kClasses; ++o) {
+            const uint32_t c = lend[o];
+            const uint32_t room = scan[c * 256u + 255u] - take[c];
+            const uint32_t extra = spare < room ? spare : room;
+            take[c] += extra;
+            spare -= extra;
+        }
+        for (uint32_t c = 0; c < kClasses; ++c) {
+            taken[c] = take[c];
+            selection[kSelThreshold + c] = 256u;
+            selection[kSelRemainder + c] = 0u;
+        }
+    }
+    __syncthreads();
+    for (uint32_t c = 0; c < kClasses; ++c) {
+        const uint32_t below = t > 0u ? scan[c * 256u + t - 1u] : 0u;
+        if (taken[c] > 0u && below < taken[c] && scan[c * 256u + t] >= taken[c]) {
+            selection[kSelThreshold + c] = t;
+            selection[kSelRemainder + c] = taken[c] - below;
+        }
+    }
+    (void)controls_budget;
+}
+
+// select_emit: the picks, appended after the CPU's traced faces: a task
+// (voxel, face, current sequence), the pick record and the task's slot.
+// Ties at a threshold bucket and picks are reserved per block.
+__global__ void __launch_bounds__(kBlock) select_emit_kernel(AccumArgs a, uint32_t n_slots, uint32_t* keys, uint32_t* selection,
+                                                             uint32_t* pick_slots) {
+    __shared__ uint32_t group_ties[4], group_tie_base[4], group_picks, group_pick_base;
+    const uint32_t* ctl = a.controls;
+    if (threadIdx.x < kClasses) group_ties[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) group_picks = 0u;
+    __syncthreads();
+    const uint32_t slot = blockIdx.x * kBlock + threadIdx.x;
+    const uint32_t key = slot < n_slots ? keys[slot] : kNoIndex;
+    const uint32_t group = (key >> 8u) < 3u ? (key >> 8u) : 3u, bucket = key & 255u;
+    const uint32_t threshold = atomicAdd(selection + kSelThreshold + group, 0u);
+    const bool candidate = key != kNoIndex && bucket <= threshold;
+    const bool tie = candidate && bucket == threshold;
+    uint32_t tie_index = 0u;
+    if (tie) tie_index = atomicAdd(group_ties + group, 1u);
+    __syncthreads();
+    if (threadIdx.x < kClasses) {
+        const uint32_t n = group_ties[threadIdx.x];
+        group_tie_base[threadIdx.x] = n > 0u ? atomicAdd(selection + kSelTies + threadIdx.x, n) : 0u;
+    }
+    __syncthreads();
+    const bool accept = candidate && (!tie || group_tie_base[group] + tie_index < atomicAdd(selection + kSelRemainder + group, 0u));
+    uint32_t pick_index = 0u;
+    if (accept) pick_index = atomicAdd(&group_picks, 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) group_pick_base = group_picks > 0u ? atomicAdd(selection + kSelTotal, group_picks) : 0u;
+    __syncthreads();
+    const uint32_t pick = group_pick_base + pick_index;
+    if (!accept || pick >= ctl[23]) return;
+    keys[slot] = kNoIndex;  // re-ranked when its range comes round
+    const uint4 identity = a.slot_meta[slot * 3u];
+    if ((identity.w & 8u) == 0u) return;  // a stale key of a retired slot: a hole
+    const uint32_t task = ctl[24] + pick;
+    const uint4* st = a.state + slot * 9u;
+    a.tasks[task * 2u] = make_uint4(identity.x, identity.y, identity.z, identity.w & 7u);
+    a.tasks[task * 2u + 1u].x = st[1].z;  // begin_trace
+    pick_slots[task] = slot;
+    a.picks[task] = make_uint4(slot, a.slot_meta[slot * 3u + 1u].z, st[1].y & 0x3fffffffu, st[7].x);
+}
+
+// mark_changed (voxel_accumulate.wgsl:432-446) for the traced tasks.
+__global__ void __launch_bounds__(kBlock) mark_changed_kernel(AccumArgs a) {
+    const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= a.n || i >= a.controls[0]) return;
+    const uint32_t slot = a.slots ? a.slots[i] : i;
+    if (slot == kNoIndex) return;
+    uint4* sm = a.slot_meta + slot * 3u + 1u;
+    const float pending = u2f(sm->x);
+    if (pending <= 0.0f) return;
+    if (binds(a.state, slot, pending, u2f(a.controls[11]))) a.state[slot * 9u + 1u].y |= 0x80000000u;
+    else sm->x = 0u;
+}
+
 }  // namespace
 
 void launch_seed_incarnations(uint4* state, uint32_t n, cudaStream_t s) {
@@ -358,6 +559,19 @@ void launch_accumulate(const AccumArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
     accumulate_kernel<<<(a.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(a);
 }
+void launch_select(const AccumArgs& a, uint32_t n_slots, uint32_t* keys, uint32_t* selection, uint32_t* pick_slots, cudaStream_t s) {
+    const uint32_t first = a.controls[26], end = a.controls[27];
+    if (end > first) select_classify_kernel<<<(end - first + kBlock - 1) / kBlock, kBlock, 0, s>>>(a, keys, selection);
+    const uint32_t blocks = (n_slots + kBlock - 1) / kBlock;
+    if (blocks) select_histogram_kernel<<<blocks, kBlock, 0, s>>>(keys, n_slots, selection);
+    select_threshold_kernel<<<1, kBlock, 0, s>>>(nullptr, a.controls[23], selection);
+    if (blocks) select_emit_kernel<<<blocks, kBlock, 0, s>>>(a, n_slots, keys, selection, pick_slots);
+}
+
+void launch_mark_changed(const AccumArgs& a, cudaStream_t s) {
+    if (a.n) mark_changed_kernel<<<(a.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(a);
+}
+
 void launch_apply_events(const AccumArgs& a, const uint4* events, uint32_t n_slots, cudaStream_t s) {
     if (n_slots == 0) return;
     apply_events_kernel<<<(n_slots + kBlock - 1) / kBlock, kBlock, 0, s>>>(a, events, n_slots);

@@ -113,6 +113,12 @@ struct vgi_ctx {
     DevBuf<uint4> stage_tasks[2], stage_results[2];
     cudaEvent_t tasks_ready[2] = {}, tasks_free[2] = {}, results_ready[2] = {}, results_done[2] = {};
     uint64_t submitted = 0;
+    // Scheduled frames (vgi_frame_scheduled): selection keys (kept between
+    // frames), selection scratch, and the picks' tasks, slots, records and results.
+    DevBuf<uint32_t> sel_keys, selection, pick_slots;
+    DevBuf<uint4> pick_tasks, pick_records, pick_results;
+    uint32_t pick_budget = 0;
+    bool keys_reset = true;  // the face set changed: every key starts as "not a candidate"
     // view tier: receivers, paths, continuations, estimates, owner queue, events
     DevBuf<uint4> v_receivers, v_paths, v_conts, v_estimates, v_events, v_scratch;
     DevBuf<uint32_t> v_queue;
@@ -555,6 +561,8 @@ int vgi_destroy(vgi_ctx* c) {
     c->mlp_master.release(); c->mlp_image.release(); c->mlp_error.release();
     c->mlp_image_b.release(); c->mlp_adam.release(); c->mlp_grads.release(); c->mlp_steps.release(); c->mlp_partials.release();
     c->w_mlp_queue.release(); c->mlp_features.release(); c->mlp_targets.release();
+    c->sel_keys.release(); c->selection.release(); c->pick_slots.release();
+    c->pick_tasks.release(); c->pick_records.release(); c->pick_results.release();
     c->mlp_train_tasks.release(); c->mlp_train_results.release(); c->mlp_query_count.release();
     c->counters.release();
     c->w_state.release(); c->w_ray.release(); c->w_hit.release(); c->w_status.release();
@@ -915,6 +923,7 @@ int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->n_slots = n;
     c->batch_id = 1;  // a new face set starts a new batch sequence
+    c->keys_reset = true;
     return VGI_OK;
 }
 
@@ -1060,6 +1069,72 @@ int vgi_frame_shard(vgi_ctx* c, uint32_t samples, uint32_t clock_ms, uint32_t fi
     VGI_CUDA(c, cudaGetLastError());
     c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
     if (c->batch_id == 0) c->batch_id = 1;
+    return VGI_OK;
+}
+
+int vgi_frame_scheduled(vgi_ctx* c, uint32_t samples, uint32_t clock_ms, const vgi_schedule* sched) {
+    int rc = check_ready(c, true);
+    if (rc != VGI_OK) return rc;
+    if (!sched || samples == 0) return fail(c, VGI_ERR_INVALID, "a schedule and positive samples are required");
+    if (sched->budget == 0 || sched->budget > c->n_slots) return fail(c, VGI_ERR_INVALID, "pick budget outside 1..slots");
+    if (sched->classify_first > sched->classify_end || sched->classify_end > c->n_slots)
+        return fail(c, VGI_ERR_INVALID, "classification range outside the slots");
+    if (c->mlp_cache) return fail(c, VGI_ERR_STATE, "the MLP cache mode traces whole frames");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    const uint32_t n = c->n_slots, budget = sched->budget;
+    VGI_CUDA(c, c->sel_keys.reserve(n));
+    // Keys of a new face set start as "not a candidate" until their range is classified.
+    if (c->keys_reset) VGI_CUDA(c, cudaMemsetAsync(c->sel_keys.ptr, 0xff, (size_t)n * 4, c->stream));
+    c->keys_reset = false;
+    VGI_CUDA(c, c->selection.reserve(kSelectionWords));
+    VGI_CUDA(c, c->pick_slots.reserve(budget));
+    VGI_CUDA(c, c->pick_tasks.reserve((size_t)budget * 2));
+    VGI_CUDA(c, c->pick_records.reserve(budget));
+    VGI_CUDA(c, c->pick_results.reserve((size_t)budget * 6));
+    c->pick_budget = budget;
+    AccumArgs acc = accum_args(c, samples, clock_ms);
+    acc.tasks = c->pick_tasks.ptr;
+    acc.outputs = c->pick_results.ptr;
+    acc.slots = c->pick_slots.ptr;
+    acc.picks = c->pick_records.ptr;
+    acc.n = budget;
+    acc.controls[0] = budget;
+    acc.controls[19] = sched->audit_ms;
+    acc.controls[20] = (uint32_t)sched->focus[0];
+    acc.controls[21] = (uint32_t)sched->focus[1];
+    acc.controls[22] = (uint32_t)sched->focus[2];
+    acc.controls[23] = budget;
+    acc.controls[24] = 0;  // no CPU-traced faces: every task is a pick
+    acc.controls[26] = sched->classify_first;
+    acc.controls[27] = sched->classify_end;
+    acc.controls[32] = 0;  // no statistics-mirror records
+    VGI_CUDA(c, cudaMemsetAsync(c->selection.ptr, 0, kSelectionWords * 4, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->pick_slots.ptr, 0xff, (size_t)budget * 4, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->pick_tasks.ptr, 0xff, (size_t)budget * 32, c->stream));  // face 0xffffffff: no task
+    VGI_CUDA(c, cudaMemsetAsync(c->pick_records.ptr, 0xff, (size_t)budget * 16, c->stream));
+    launch_select(acc, n, c->sel_keys.ptr, c->selection.ptr, c->pick_slots.ptr, c->stream);
+    launch_mark_changed(acc, c->stream);
+    const TraceArgs tr = trace_args(c, c->pick_tasks.ptr, c->pick_results.ptr, budget, samples, true);
+    rc = run_trace(c, tr, false, false);
+    if (rc != VGI_OK) return rc;
+    launch_accumulate(acc, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
+    if (c->batch_id == 0) c->batch_id = 1;
+    return VGI_OK;
+}
+
+int vgi_read_selection(vgi_ctx* c, uint32_t* keys, uint32_t* selection, uint32_t* picks4, uint32_t* tasks8, uint32_t* results24) {
+    if (!c) return VGI_ERR_INVALID;
+    if (!c->selection.ptr) return fail(c, VGI_ERR_STATE, "no scheduled frame has run");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    const uint32_t b = c->pick_budget;
+    if (keys) VGI_CUDA(c, cudaMemcpyAsync(keys, c->sel_keys.ptr, (size_t)c->n_slots * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (selection) VGI_CUDA(c, cudaMemcpyAsync(selection, c->selection.ptr, kSelectionWords * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (picks4) VGI_CUDA(c, cudaMemcpyAsync(picks4, c->pick_records.ptr, (size_t)b * 16, cudaMemcpyDeviceToHost, c->stream));
+    if (tasks8) VGI_CUDA(c, cudaMemcpyAsync(tasks8, c->pick_tasks.ptr, (size_t)b * 32, cudaMemcpyDeviceToHost, c->stream));
+    if (results24) VGI_CUDA(c, cudaMemcpyAsync(results24, c->pick_results.ptr, (size_t)b * 96, cudaMemcpyDeviceToHost, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }
 

@@ -104,6 +104,31 @@ __device__ __forceinline__ void own_sincos(float x, float* s, float* c) {
     }
 }
 
+// log2 for the selection's key buckets, the same operations as the oracle's
+// own_log2: x = m 2^e with m reduced to [sqrt(1/2), sqrt(2)), and
+// ln m = 2 atanh(t), t = (m - 1) / (m + 1), by its series t + t^3/3 + ...
+// + t^9/9 (|t| < 0.172, so the next term is below 2^-24 of the result).
+// Zero and subnormal inputs give e = -127 plus the series of their raw
+// significand, which the callers' clamps treat like -infinity.
+__device__ __forceinline__ float own_log2(float x) {
+    const uint32_t b = __float_as_uint(x);
+    int e = (int)((b >> 23) & 255u) - 127;
+    float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
+    if (m > 1.41421354f) {
+        m = __fmul_rn(m, 0.5f);
+        e += 1;
+    }
+    const float t = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
+    const float t2 = __fmul_rn(t, t);
+    float p = 0.222222224f;                     // 2/9
+    p = __fadd_rn(__fmul_rn(p, t2), 0.285714298f);  // 2/7
+    p = __fadd_rn(__fmul_rn(p, t2), 0.4f);          // 2/5
+    p = __fadd_rn(__fmul_rn(p, t2), 0.666666687f);  // 2/3
+    p = __fadd_rn(__fmul_rn(p, t2), 2.0f);
+    const float ln_m = __fmul_rn(p, t);
+    return __fadd_rn((float)e, __fmul_rn(ln_m, 1.44269502f));  // 1 / ln 2
+}
+
 __device__ __forceinline__ float own_exp(float x) {
     if (x != x) return x;
     if (x > 88.5f) return __int_as_float(0x7f800000);

@@ -53,7 +53,14 @@ struct AccumArgs {
     const uint32_t* slots;  // task -> slot (null: identity)
     uint32_t n;
     uint32_t controls[36];
+    uint4* picks;         // GPU picks' records (slot, revision, count, incarnation) per task, or null
 };
+
+// The GPU selection of a scheduled frame (vgi_accumulate.cu): selection
+// scratch words and the per-slot keys.
+constexpr uint32_t kSelectionWords = 1038;
+void launch_select(const AccumArgs& a, uint32_t n_slots, uint32_t* keys, uint32_t* selection, uint32_t* pick_slots, cudaStream_t s);
+void launch_mark_changed(const AccumArgs& a, cudaStream_t s);
 
 // Device buffers of the wavefront layout (vgi_wave.cuh) for P = tasks x
 // samples paths and S = P * (2 + lights) + tasks * lights ray slots.

@@ -44,6 +44,12 @@ class TransportUnavailable(VgiError):
     (src/lib.rs:355-357); it never falls back to the CPU."""
 
 
+class Schedule(ctypes.Structure):
+    """vgi_schedule."""
+    _fields_ = [("focus", ctypes.c_int32 * 3), ("budget", ctypes.c_uint32), ("classify_first", ctypes.c_uint32),
+                ("classify_end", ctypes.c_uint32), ("audit_ms", ctypes.c_uint32)]
+
+
 class MlpStatus(ctypes.Structure):
     """vgi_mlp_status."""
     _fields_ = [("frames", ctypes.c_uint32), ("steps", ctypes.c_uint32), ("terminating", ctypes.c_uint32),
@@ -185,6 +191,8 @@ _SIGNATURES = {
     "vgi_mlp_stats": (_INT, [_P, _P]),
     "vgi_frame_shard": (_INT, [_P, _U32, _U32, _U32, _U32]),
     "vgi_submit_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P, _P]),
+    "vgi_frame_scheduled": (_INT, [_P, _U32, _U32, _P]),
+    "vgi_read_selection": (_INT, [_P, _P, _P, _P, _P, _P]),
     "vgi_complete_batch": (_INT, [_P, _U64]),
     "vgi_read_cache": (_INT, [_P, _U32, _U32, _P, ctypes.c_int]),
     "vgi_write_cache": (_INT, [_P, _U32, _U32, _P, ctypes.c_int]),
@@ -578,6 +586,24 @@ class GpuTracer:
 
     def complete_batch(self, ticket: int) -> None:
         self._check(self._lib.vgi_complete_batch(self._h, ticket))
+
+    # scheduled frames
+    def frame_scheduled(self, samples: int, clock_ms: int, budget: int, focus=(0, 0, 0), classify=None, audit_ms: int = 1000) -> None:
+        """A frame that traces `budget` faces the GPU selection picks."""
+        first, end = classify if classify is not None else (0, self.n_slots)
+        sched = Schedule((ctypes.c_int32 * 3)(*[int(v) for v in focus]), budget, first, end, audit_ms)
+        self._check(self._lib.vgi_frame_scheduled(self._h, samples, clock_ms, ctypes.byref(sched)))
+        self._budget = budget
+
+    def read_selection(self) -> dict:
+        n, b = self.n_slots, getattr(self, "_budget", 0)
+        keys = np.zeros(n, np.uint32)
+        sel = np.zeros(1038, np.uint32)
+        picks = np.zeros((b, 4), np.uint32)
+        tasks = np.zeros((b, 8), np.uint32)
+        results = np.zeros((b, 24), np.uint32)
+        self._check(self._lib.vgi_read_selection(self._h, _ptr(keys), _ptr(sel), _ptr(picks), _ptr(tasks), _ptr(results)))
+        return {"keys": keys, "selection": sel, "picks": picks, "tasks": tasks, "results": results}
 
     # face-sharded frames
     def frame_shard(self, samples: int, clock_ms: int, first: int, n: int) -> None:

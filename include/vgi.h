@@ -313,6 +313,40 @@ typedef struct vgi_mlp_status {
 /* Synchronous. */
 int vgi_mlp_stats(vgi_ctx* ctx, vgi_mlp_status* out);
 
+/* ---- scheduled frames: the GPU world-cache scheduler --------------------------
+ * The reference's GPU selection of bulk work (shaders/voxel_accumulate.wgsl:
+ * 448-695: candidate, select_classify, select_histogram, select_threshold,
+ * select_emit; scheduling.rs states the rules): instead of every slot, a
+ * frame traces `budget` faces it picks itself. Each live, due face competes
+ * in one class: urgent (an edit's change binds it), coverage (fewer than 8
+ * samples; nearest the focus first), refinement (within two 32-voxel pages
+ * of the focus; highest error + age first) or sweep (elsewhere; oldest
+ * first). Urgent faces take up to 3/4 of the budget, the rest goes 1/4,
+ * 1/2, 1/4 with unused share lent on; per-class histograms of 256 key
+ * buckets give the exact thresholds. Keys persist per slot; each frame
+ * re-classifies slots [classify_first, classify_end) (the reference rotates
+ * a quarter per batch), and a picked face's key is cleared until its range
+ * comes round. A face is due unless fresh in this transport revision, with
+ * its required samples, stable for 4 batches and younger than audit_ms.
+ * The picks are traced and accumulated as GPU picks: each pick record is
+ * (slot, revision tag, merged count, incarnation), and the face's
+ * statistics mirror is marked stale (this library keeps no CPU mirror).
+ * Ties at a threshold bucket are taken in block order, so which of them are
+ * picked can differ from run to run (as on the reference's GPU); the keys,
+ * histograms, thresholds and counts do not. */
+typedef struct vgi_schedule {
+    int32_t focus[3];          /* the camera's voxel */
+    uint32_t budget;           /* faces to pick and trace, 1..slots */
+    uint32_t classify_first, classify_end;
+    uint32_t audit_ms;         /* a fresh, stable face is due again after this long */
+} vgi_schedule;
+int vgi_frame_scheduled(vgi_ctx* ctx, uint32_t samples, uint32_t clock_ms, const vgi_schedule* schedule);
+/* After a scheduled frame: keys (one word per slot), the 1038 selection words
+ * (4 x 256 histogram buckets, thresholds, remainders, ties, total, mirror
+ * count), and per pick task its record (4 words), FaceTask (8) and
+ * FaceResult as accumulate left it (24). Any pointer may be null. */
+int vgi_read_selection(vgi_ctx* ctx, uint32_t* keys, uint32_t* selection, uint32_t* picks4, uint32_t* tasks8, uint32_t* results24);
+
 /* ---- face-sharded frames -------------------------------------------------------
  * No counterpart in the reference. Faces are independent given the frame's
  * geometry and the world cache's snapshot, so a frame can be split across

@@ -80,6 +80,30 @@ static inline uint32_t reverse_bits(uint32_t v) {
 // Own sine/cosine: k = nearest multiple of pi/2 (x * 2/pi rounded), three-part
 // Cody-Waite reduction (each part has 12 trailing zero bits so k * part is
 // exact), then Taylor polynomials on |r| <= pi/4 (sin to r^11, cos to r^12).
+// log2 by exponent split and the atanh series (the device's own_log2, same
+// operations): m in [sqrt(1/2), sqrt(2)), ln m = 2 (t + t^3/3 + ... + t^9/9).
+static inline float own_log2(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    int e = (int)((b >> 23) & 255u) - 127;
+    uint32_t mb = (b & 0x7fffffu) | 0x3f800000u;
+    float m;
+    std::memcpy(&m, &mb, 4);
+    if (m > 1.41421354f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    const float t = (m - 1.0f) / (m + 1.0f);
+    const float t2 = t * t;
+    float p = 0.222222224f;
+    p = p * t2 + 0.285714298f;
+    p = p * t2 + 0.4f;
+    p = p * t2 + 0.666666687f;
+    p = p * t2 + 2.0f;
+    const float ln_m = p * t;
+    return (float)e + ln_m * 1.44269502f;
+}
+
 static inline void own_sincos(float x, float* s, float* c) {
     const float two_over_pi = 0x1.45f306p-1f;
     const float p1 = 0x1.92p+0f, p2 = 0x1.fb4p-12f, p3 = 0x1.4442d2p-24f;

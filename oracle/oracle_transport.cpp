@@ -1040,11 +1040,13 @@ static float sample_noise(const uint32_t* base) {
     return max3(e[0], e[1], e[2]);
 }
 
-// accumulate (voxel_accumulate.wgsl:135-227) with record_stability (:237-262)
-// for batches of CPU-owned faces only (no GPU picks: batch.x = n).
-// outputs: 24 words per task (FaceResult in, state words 0..5 out).
-int orc_accumulate(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint, uint32_t* outputs, const uint32_t* slots,
-                   uint32_t n, const uint32_t* controls) {
+// accumulate (voxel_accumulate.wgsl:135-227) with record_stability (:237-262).
+// Tasks from batch.x (controls[24]) on are GPU picks: their pick record
+// (4 words per task, may be null) takes the merged count and the slot's
+// statistics mirror becomes stale. outputs: 24 words per task (FaceResult
+// in, state words 0..5 out).
+static int accumulate_impl(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint, uint32_t* outputs, const uint32_t* slots,
+                           uint32_t n, const uint32_t* controls, uint32_t* picks) {
     const uint32_t MIRROR_STALE = 0x20000000u;
     for (uint32_t i = 0; i < n; ++i) {
         uint32_t slot = slots[i];
@@ -1111,7 +1113,9 @@ int orc_accumulate(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint, u
         base[7] = base[24];
         base[13] = base[25]; base[14] = base[26]; base[15] = base[27];
         for (int k = 0; k < 24; ++k) out[k] = base[k];
-        // record_stability (picked = false: batch.x == n)
+        const bool picked = i >= controls[24];
+        if (picked && picks) picks[(size_t)i * 4 + 2] = base[5] & 0x7fffffffu;
+        // record_stability
         uint32_t* sched = slot_meta + ((size_t)slot * 3 + 1) * 4;
         uint32_t* rank = slot_meta + ((size_t)slot * 3 + 2) * 4;
         uint32_t sy = sched[1], sw = sched[3];
@@ -1135,9 +1139,142 @@ int orc_accumulate(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint, u
         rank[0] = fbits(sample_noise(base));
         rank[1] = controls[2];
         rank[2] = fbits(max3(after.x, after.y, after.z));
-        rank[3] = 0x80000000u | scount | (old_rank_w & MIRROR_STALE);
+        rank[3] = 0x80000000u | scount | (picked ? MIRROR_STALE : (old_rank_w & MIRROR_STALE));
         // settled_flag
         if ((sched[1] & 15u) == 12u) out[5] |= 0x80000000u;
+    }
+    return 0;
+}
+
+int orc_accumulate(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint, uint32_t* outputs, const uint32_t* slots,
+                   uint32_t n, const uint32_t* controls) {
+    return accumulate_impl(state, slot_meta, checkpoint, outputs, slots, n, controls, nullptr);
+}
+
+int orc_accumulate_picks(uint32_t* state, uint32_t* slot_meta, uint32_t* checkpoint, uint32_t* outputs, const uint32_t* slots,
+                         uint32_t n, const uint32_t* controls, uint32_t* picks) {
+    return accumulate_impl(state, slot_meta, checkpoint, outputs, slots, n, controls, picks);
+}
+
+// ---- GPU selection (voxel_accumulate.wgsl:448-695), restated serially ----------
+static int page_axis(int p) { return (p - (p < 0 ? 31 : 0)) / 32; }
+
+// candidate (voxel_accumulate.wgsl:474-511): class << 8 | bucket, or none.
+static uint32_t candidate_key(const uint32_t* slot_meta, uint32_t slot, const uint32_t* ctl) {
+    const uint32_t URGENT = 0x40000000u;
+    const uint32_t* identity = slot_meta + (size_t)slot * 12;
+    if ((identity[3] & 8u) == 0u) return 0xffffffffu;
+    const uint32_t* schedule = identity + 4;
+    const uint32_t last_cpu = schedule[1] >> 4u;
+    if (last_cpu != 0u && ((ctl[25] - last_cpu) & 0x0fffffffu) < 4u) return 0xffffffffu;
+    const uint32_t* rank = identity + 8;
+    const uint32_t count = rank[3] & 0x1fffffffu;
+    const bool fresh = (schedule[1] & 8u) != 0u && schedule[3] == ctl[16];
+    const uint32_t since = ctl[2] - rank[1];
+    const uint32_t age_ms = rank[3] < 0x80000000u ? 0x7fffffffu : (since > 0x7fffffffu ? 0u : since);
+    const uint32_t required = bitsf(rank[2]) < 0.02f ? umax(ctl[18], 256u) : ctl[18];
+    const bool due = !fresh || count < required || (schedule[1] & 7u) < 4u || age_ms >= ctl[19] || (rank[3] & URGENT) != 0u;
+    if (!due) return 0xffffffffu;
+    const int px = (int)identity[0], py = (int)identity[1], pz = (int)identity[2];
+    const int fx = (int)ctl[20], fy = (int)ctl[21], fz = (int)ctl[22];
+    if ((rank[3] & URGENT) != 0u || count < 8u) {
+        const float dx = (float)(px - fx), dy = (float)(py - fy), dz = (float)(pz - fz);
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        const uint32_t b = f2u(own_log2(d2 + 1.0f) * 8.0f);
+        return (((rank[3] & URGENT) != 0u ? 3u : 0u) << 8u) | umin(b, 255u);
+    }
+    const int ax = std::abs(page_axis(px) - page_axis(fx)), ay = std::abs(page_axis(py) - page_axis(fy)),
+              az = std::abs(page_axis(pz) - page_axis(fz));
+    const int page_distance = imax(ax, imax(ay, az));
+    if (page_distance <= 2) {
+        const float age = wmin((float)age_ms * 0.001f, 10.0f);
+        const float error = count < 2u ? 1.0f : wmin(bitsf(rank[0]) / std::sqrt((float)count), 8.0f);
+        const float priority = (error + age * 0.1f) + (page_distance <= 1 ? 0.25f : 0.0f);
+        const uint32_t b = f2u(wmax(own_log2(priority) + 8.0f, 0.0f) * 16.0f);
+        return (1u << 8u) | (255u - umin(b, 255u));
+    }
+    const uint32_t b = f2u(own_log2((float)age_ms + 1.0f) * 8.0f);
+    return (2u << 8u) | (255u - umin(b, 255u));
+}
+
+// candidate keys only, for slots [controls[26], controls[27]).
+int orc_classify(const uint32_t* slot_meta, uint32_t* keys, uint32_t n_slots, const uint32_t* ctl) {
+    for (uint32_t slot = ctl[26]; slot < ctl[27] && slot < n_slots; ++slot) keys[slot] = candidate_key(slot_meta, slot, ctl);
+    return 0;
+}
+
+// select_classify, select_histogram, select_threshold and select_emit over
+// n_slots slots. keys: one word per slot (kept between calls, as the GPU's);
+// selection: 1038 words, zeroed by the caller; emit takes ties and picks in
+// slot order. tasks (8 words), pick_slots and picks (4 words) per task from
+// batch.x (controls[24]) up to the budget (controls[23]).
+int orc_select(const uint32_t* state, uint32_t* slot_meta, uint32_t* keys, uint32_t n_slots, const uint32_t* ctl, uint32_t* selection,
+               uint32_t* tasks, uint32_t* pick_slots, uint32_t* picks) {
+    const uint32_t MIRROR_STALE = 0x20000000u;
+    for (uint32_t slot = ctl[26]; slot < ctl[27] && slot < n_slots; ++slot) {
+        keys[slot] = candidate_key(slot_meta, slot, ctl);
+        uint32_t* rank = slot_meta + ((size_t)slot * 3 + 2) * 4;
+        const bool stale = (rank[3] & MIRROR_STALE) != 0u && (slot_meta[(size_t)slot * 12 + 3] & 8u) != 0u;
+        if (stale) {
+            if (selection[1037] < ctl[32]) rank[3] &= ~MIRROR_STALE;
+            selection[1037] += 1u;
+        }
+    }
+    for (uint32_t slot = 0; slot < n_slots; ++slot)
+        if (keys[slot] != 0xffffffffu) selection[umin(keys[slot] >> 8u, 3u) * 256u + (keys[slot] & 255u)] += 1u;
+    uint32_t scan[4][256];
+    for (uint32_t c = 0; c < 4; ++c) {
+        uint32_t sum = 0;
+        for (uint32_t t = 0; t < 256; ++t) scan[c][t] = (sum += selection[c * 256u + t]);
+    }
+    const uint32_t budget = ctl[23];
+    uint32_t take[4] = {0, 0, 0, 0};
+    take[3] = umin(scan[3][255], budget - budget / 4u);
+    const uint32_t rest = budget - take[3];
+    take[0] = umin(rest / 4u, scan[0][255]);
+    take[1] = umin(rest / 2u, scan[1][255]);
+    take[2] = umin(rest - rest / 4u - rest / 2u, scan[2][255]);
+    uint32_t spare = budget - take[0] - take[1] - take[2] - take[3];
+    const uint32_t lend[4] = {1u, 0u, 2u, 3u};
+    for (uint32_t o = 0; o < 4; ++o) {
+        const uint32_t c = lend[o];
+        const uint32_t extra = umin(spare, scan[c][255] - take[c]);
+        take[c] += extra;
+        spare -= extra;
+    }
+    for (uint32_t c = 0; c < 4; ++c) {
+        selection[1024 + c] = 256u;
+        selection[1028 + c] = 0u;
+        for (uint32_t t = 0; t < 256; ++t) {
+            const uint32_t below = t > 0 ? scan[c][t - 1] : 0u;
+            if (take[c] > 0u && below < take[c] && scan[c][t] >= take[c]) {
+                selection[1024 + c] = t;
+                selection[1028 + c] = take[c] - below;
+            }
+        }
+    }
+    for (uint32_t slot = 0; slot < n_slots; ++slot) {
+        const uint32_t key = keys[slot];
+        if (key == 0xffffffffu) continue;
+        const uint32_t group = umin(key >> 8u, 3u), bucket = key & 255u;
+        const uint32_t threshold = selection[1024 + group];
+        if (bucket > threshold) continue;
+        bool accept = true;
+        if (bucket == threshold) accept = selection[1032 + group]++ < selection[1028 + group];
+        if (!accept) continue;
+        const uint32_t pick = selection[1036]++;
+        if (pick >= budget) continue;
+        keys[slot] = 0xffffffffu;
+        const uint32_t* identity = slot_meta + (size_t)slot * 12;
+        if ((identity[3] & 8u) == 0u) continue;
+        const uint32_t task = ctl[24] + pick;
+        const uint32_t* st = state + (size_t)slot * 36;
+        uint32_t* tk = tasks + (size_t)task * 8;
+        tk[0] = identity[0]; tk[1] = identity[1]; tk[2] = identity[2]; tk[3] = identity[3] & 7u;
+        tk[4] = st[6];
+        pick_slots[task] = slot;
+        uint32_t* pr = picks + (size_t)task * 4;
+        pr[0] = slot; pr[1] = slot_meta[(size_t)slot * 12 + 6]; pr[2] = st[5] & 0x3fffffffu; pr[3] = st[28];
     }
     return 0;
 }
