@@ -149,6 +149,8 @@ struct vgi_ctx {
     bool mlp_queried = false;                 // a frame has queried the network (counters[4] holds its count)
     uint32_t n_view = 0;
     DevBuf<uint4> events;
+    DevBuf<int4> footprints;                 // change-footprint tasks of the last event list
+    DevBuf<uint32_t> footprint_sums;
     uint32_t n_events = 0;
     uint64_t n_events_read = 0;  // uint4 words of the last measured event list, readable back
     DevBuf<unsigned long long> counters;
@@ -561,6 +563,7 @@ int vgi_destroy(vgi_ctx* c) {
     c->mlp_master.release(); c->mlp_image.release(); c->mlp_error.release();
     c->mlp_image_b.release(); c->mlp_adam.release(); c->mlp_grads.release(); c->mlp_steps.release(); c->mlp_partials.release();
     c->w_mlp_queue.release(); c->mlp_features.release(); c->mlp_targets.release();
+    c->footprints.release(); c->footprint_sums.release();
     c->sel_keys.release(); c->selection.release(); c->pick_slots.release();
     c->pick_tasks.release(); c->pick_records.release(); c->pick_results.release();
     c->mlp_train_tasks.release(); c->mlp_train_results.release(); c->mlp_query_count.release();
@@ -1362,10 +1365,40 @@ int vgi_apply_events(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint6
     return VGI_OK;
 }
 
+static int apply_events_impl(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint64_t n_words, const uint32_t* measures,
+                             uint32_t n_entries, const int32_t* footprints, uint32_t n_footprints);
+
 int vgi_apply_events_measured(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint64_t n_words, const uint32_t* measures,
                               uint32_t n_entries) {
-    if (!c || (n_words && !words) || (n_words & 3) || (uint64_t)n_events * 12 > n_words || (n_entries && !measures))
+    return apply_events_impl(c, words, n_events, n_words, measures, n_entries, nullptr, 0);
+}
+
+int vgi_apply_events_footprints(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint64_t n_words, const uint32_t* measures,
+                                uint32_t n_entries, const int32_t* footprints, uint32_t n_footprints) {
+    return apply_events_impl(c, words, n_events, n_words, measures, n_entries, footprints, n_footprints);
+}
+
+static int apply_events_impl(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint64_t n_words, const uint32_t* measures,
+                             uint32_t n_entries, const int32_t* footprints, uint32_t n_footprints) {
+    if (!c || (n_words && !words) || (n_words & 3) || (uint64_t)n_events * 12 > n_words || (n_entries && !measures) ||
+        (n_footprints && !footprints))
         return VGI_ERR_INVALID;
+    // Footprint tasks: a count record, then (box min, header record) (box
+    // max, bound record) (first thread, grid, 0, 0); the first threads tile
+    // grid^2 threads per task in order, and both records name event words.
+    uint64_t threads = 0;
+    if (n_footprints) {
+        if (footprints[0] != (int32_t)n_footprints || n_footprints > 4096) return fail(c, VGI_ERR_INVALID, "footprint count record");
+        for (uint32_t e = 0; e < n_footprints; ++e) {
+            const int32_t* t = footprints + 4 + (size_t)e * 12;
+            const int64_t grid = t[9], header = t[3], bound = t[7];
+            if (t[8] != (int32_t)threads || grid < 1 || grid > 1024 || header < 0 || bound < 0 || (uint64_t)header + 2 > n_words / 4 ||
+                (uint64_t)bound + 2 > n_words / 4 || t[0] > t[4] || t[1] > t[5] || t[2] > t[6])
+                return fail(c, VGI_ERR_INVALID, "footprint tasks must tile their threads, span a box and name event records");
+            threads += (uint64_t)grid * (uint64_t)grid;
+            if (threads > 0x7fffffffull) return fail(c, VGI_ERR_CAPACITY, "too many footprint threads");
+        }
+    }
     // Entries must tile their positions in order and name a bound record.
     uint64_t positions = 0;
     for (uint32_t e = 0; e < n_entries; ++e) {
@@ -1384,6 +1417,22 @@ int vgi_apply_events_measured(vgi_ctx* c, const uint32_t* words, uint32_t n_even
     VGI_CUDA(c, cudaSetDevice(c->device));
     VGI_CUDA(c, c->events.reserve(std::max<uint64_t>(n_words / 4, 1)));
     if (n_words) VGI_CUDA(c, cudaMemcpyAsync(c->events.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    if (n_footprints) {
+        // Where each changed box's shadow lands, into its reserved Light
+        // event, before the measured edits and retention read the events.
+        if (!c->geometry || !c->materials.ptr || !c->lights.ptr) return fail(c, VGI_ERR_STATE, "footprints need geometry and the model");
+        std::vector<uint32_t> sums((size_t)n_footprints * 8, 0u);
+        for (uint32_t e = 0; e < n_footprints; ++e) sums[(size_t)e * 8] = sums[(size_t)e * 8 + 1] = sums[(size_t)e * 8 + 2] = 0xffffffffu;
+        VGI_CUDA(c, c->footprints.reserve((size_t)n_footprints * 3 + 1));
+        VGI_CUDA(c, c->footprint_sums.reserve(sums.size()));
+        VGI_CUDA(c, cudaMemcpyAsync(c->footprints.ptr, footprints, ((size_t)n_footprints * 3 + 1) * 16, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, cudaMemcpyAsync(c->footprint_sums.ptr, sums.data(), sums.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        const TraceArgs tr = trace_args(c, nullptr, nullptr, 0, 1, false);
+        launch_footprints(tr, c->footprints.ptr, n_footprints, (uint32_t)threads, c->n_directional, c->footprint_sums.ptr, c->events.ptr,
+                          c->stream);
+        VGI_CUDA(c, cudaGetLastError());
+        VGI_CUDA(c, cudaStreamSynchronize(c->stream));  // the host vector above is the copy's source
+    }
     if (n_entries) {
         VGI_CUDA(c, c->measures.reserve((size_t)n_entries * 3));
         VGI_CUDA(c, c->measure_max.reserve(n_entries));

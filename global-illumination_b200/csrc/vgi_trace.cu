@@ -894,6 +894,109 @@ __global__ void node_aux_kernel(const uint4* __restrict__ emitters, uint32_t fir
 
 }  // namespace
 
+// ---- change footprints (voxel_trace.wgsl:94-202) ------------------------------
+namespace {
+constexpr int32_t kFootprintBias = 1073741824;
+
+// The last task whose first thread is at most t (first threads ascend).
+__device__ uint32_t footprint_task(const int4* fp, uint32_t t) {
+    uint32_t lo = 0u, hi = (uint32_t)fp[0].x;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) / 2u;
+        if ((uint32_t)fp[1u + mid * 3u + 2u].x <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// trace_footprints: one thread per tube of a square grid across a changed
+// box's diagonal, per directional light. A tube clear on the sun side that
+// lands on a surface below adds the reflected power through it to the task's
+// flux (x 64) and its voxel to the landing box (biased by 2^30).
+__global__ void __launch_bounds__(64) trace_footprints_kernel(const TraceArgs A, const int4* fp, uint32_t threads, uint32_t n_directional,
+                                                              uint32_t* sums) {
+    const uint32_t id = blockIdx.x * 64u + threadIdx.x;
+    if ((uint32_t)fp[0].x == 0u || id >= threads) return;
+    Cnt<false> cnt;
+    const uint32_t e = footprint_task(fp, id);
+    const int4 a = fp[1u + e * 3u], b = fp[1u + e * 3u + 1u], c = fp[1u + e * 3u + 2u];
+    const uint32_t grid = (uint32_t)c.y;
+    const uint32_t local = id - (uint32_t)c.x;
+    if (local >= grid * grid) return;
+    const V3 lo{(float)a.x, (float)a.y, (float)a.z};
+    const V3 hi = add_s(V3{(float)b.x, (float)b.y, (float)b.z}, 1.0f);
+    const V3 center = (lo + hi) * 0.5f;
+    const float diagonal = len3(hi - lo);
+    const float spacing = __fdiv_rn(diagonal, (float)grid);
+    const float half = __fmul_rn(0.5f, diagonal);
+    const float ox = __fsub_rn(__fmul_rn(__fadd_rn((float)(local % grid), 0.5f), spacing), half);
+    const float oy = __fsub_rn(__fmul_rn(__fadd_rn((float)(local / grid), 0.5f), spacing), half);
+    const V3 w{0.2126f, 0.7152f, 0.0722f};
+    const uint32_t base = e * 8u;
+    float flux = 0.0f;
+#pragma unroll 1
+    for (uint32_t i = 0; i < n_directional; ++i) {
+        const float4 Lp = __ldg(A.lights + i * 3u), Le = __ldg(A.lights + i * 3u + 1u), Lx = __ldg(A.lights + i * 3u + 2u);
+        const V3 color{wmax(__fsub_rn(Le.x, Lx.y), 0.0f), wmax(__fsub_rn(Le.y, Lx.z), 0.0f), wmax(__fsub_rn(Le.z, Lx.w), 0.0f)};
+        if (color.x == 0.0f && color.y == 0.0f && color.z == 0.0f) continue;
+        const V3 direction = normalize3(V3{Lp.x, Lp.y, Lp.z});
+        const V3 pick = fabsf(direction.y) > 0.9f ? V3{1.0f, 0.0f, 0.0f} : V3{0.0f, 1.0f, 0.0f};
+        const V3 u = normalize3(cross3(direction, pick));
+        const V3 v = cross3(direction, u);
+        const V3 point = (center + u * ox) + v * oy;
+        const V3 inverse{__fdiv_rn(1.0f, fabsf(direction.x) < 1e-8f ? 1e-8f : direction.x),
+                         __fdiv_rn(1.0f, fabsf(direction.y) < 1e-8f ? 1e-8f : direction.y),
+                         __fdiv_rn(1.0f, fabsf(direction.z) < 1e-8f ? 1e-8f : direction.z)};
+        const V3 nearv = (lo - point) * inverse, farv = (hi - point) * inverse;
+        const float enter = wmax(wmax(wmin(nearv.x, farv.x), wmin(nearv.y, farv.y)), wmin(nearv.z, farv.z));
+        const float exit = wmin(wmin(wmax(nearv.x, farv.x), wmax(nearv.y, farv.y)), wmax(nearv.z, farv.z));
+        if (enter > exit) continue;
+        // Shadowed beyond the box either way: the change cannot matter.
+        if (trace_domain(A, point + direction * __fadd_rn(exit, 0.01f), direction, A.max_distance, true, 2048u, cnt).status != 0u) continue;
+        const V3 start = point + direction * __fsub_rn(enter, 0.01f);
+        const Ray hit = trace_domain(A, start, -direction, A.max_distance, true, 2048u, cnt);
+        if (hit.status != 1u || dot3(hit.normal, direction) <= 0.0f || len3(hit.position - start) < 0.02f) continue;
+        const float4 d = __ldg(A.materials + hit.material * 4u);
+        flux = __fadd_rn(flux, __fmul_rn(__fmul_rn(__fmul_rn(dot3(color, w), dot3(V3{d.x, d.y, d.z}, w)), spacing), spacing));
+        const uint32_t px = (uint32_t)(hit.voxel.x + kFootprintBias), py = (uint32_t)(hit.voxel.y + kFootprintBias),
+                       pz = (uint32_t)(hit.voxel.z + kFootprintBias);
+        atomicMin(sums + base, px);
+        atomicMin(sums + base + 1u, py);
+        atomicMin(sums + base + 2u, pz);
+        atomicMax(sums + base + 3u, px);
+        atomicMax(sums + base + 4u, py);
+        atomicMax(sums + base + 5u, pz);
+    }
+    if (flux > 0.0f) atomicAdd(sums + base + 6u, f2u(__fadd_rn(__fmul_rn(flux, 64.0f), 0.5f)));
+}
+
+// finish_footprints: each task's landing box becomes its reserved Light
+// event (header union and its one bound); nothing landed: the empty bound stays.
+__global__ void __launch_bounds__(64) finish_footprints_kernel(const int4* fp, const uint32_t* sums, uint4* events) {
+    const uint32_t e = blockIdx.x * 64u + threadIdx.x;
+    if (e >= (uint32_t)fp[0].x) return;
+    const uint32_t base = e * 8u;
+    const uint32_t x = sums[base];
+    if (x == 0xffffffffu) return;
+    const int mnx = (int)x - kFootprintBias, mny = (int)sums[base + 1u] - kFootprintBias, mnz = (int)sums[base + 2u] - kFootprintBias;
+    const int mxx = (int)sums[base + 3u] - kFootprintBias, mxy = (int)sums[base + 4u] - kFootprintBias,
+              mxz = (int)sums[base + 5u] - kFootprintBias;
+    const float flux = __fdiv_rn((float)sums[base + 6u], 64.0f);
+    const uint32_t header = (uint32_t)fp[1u + e * 3u].w, bound = (uint32_t)fp[1u + e * 3u + 1u].w;
+    events[header] = make_uint4((uint32_t)mnx, (uint32_t)mny, (uint32_t)mnz, events[header].w);
+    events[header + 1u] = make_uint4((uint32_t)mxx, (uint32_t)mxy, (uint32_t)mxz, events[header + 1u].w);
+    events[bound] = make_uint4((uint32_t)mnx, (uint32_t)mny, (uint32_t)mnz, __float_as_uint(flux));
+    events[bound + 1u] = make_uint4((uint32_t)mxx, (uint32_t)mxy, (uint32_t)mxz, 4u);
+}
+}  // namespace
+
+void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uint32_t threads, uint32_t n_directional, uint32_t* sums,
+                       uint4* events, cudaStream_t s) {
+    if (n_tasks == 0) return;
+    if (threads) trace_footprints_kernel<<<(threads + 63) / 64, 64, 0, s>>>(a, fp, threads, n_directional, sums);
+    finish_footprints_kernel<<<(n_tasks + 63) / 64, 64, 0, s>>>(fp, sums, events);
+}
+
 void launch_node_aux(const uint4* emitters, uint32_t first_node, uint32_t nodes, float4* aux, cudaStream_t s) {
     if (nodes == 0) return;
     node_aux_kernel<<<(nodes + 255) / 256, 256, 0, s>>>(emitters, first_node, nodes, aux);

@@ -153,6 +153,10 @@ void launch_reference64(const TraceArgs& a, const double* cdf, const int4* emitt
 // The per-frame kernels whose arguments a captured frame graph updates.
 const void* prepare_kernel_address();
 const void* accumulate_kernel_address();
+// Change footprints (vgi_trace.cu): fp = a count record, then 3 records per
+// task; sums = 8 words per task (min xyz, max xyz, flux x 64, unused).
+void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uint32_t threads, uint32_t n_directional, uint32_t* sums,
+                       uint4* events, cudaStream_t s);
 // MLP radiance cache (vgi_mlp.cu).
 cudaError_t mlp_set_attributes();
 void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,

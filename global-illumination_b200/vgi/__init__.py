@@ -192,6 +192,7 @@ _SIGNATURES = {
     "vgi_frame_shard": (_INT, [_P, _U32, _U32, _U32, _U32]),
     "vgi_submit_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P, _P]),
     "vgi_frame_scheduled": (_INT, [_P, _U32, _U32, _P]),
+    "vgi_apply_events_footprints": (_INT, [_P, _P, _U32, _U64, _P, _U32, _P, _U32]),
     "vgi_read_selection": (_INT, [_P, _P, _P, _P, _P, _P]),
     "vgi_complete_batch": (_INT, [_P, _U64]),
     "vgi_read_cache": (_INT, [_P, _U32, _U32, _P, ctypes.c_int]),
@@ -502,6 +503,19 @@ class GpuTracer:
         return out
 
     # ---- view tier -----------------------------------------------------------
+    def apply_events_footprints(self, words: np.ndarray, n_events: int, footprints: np.ndarray, measures=None) -> np.ndarray:
+        """Retention events whose reserved Light events take the changed boxes'
+        shadow footprints first; returns the event words as retention read them."""
+        w = _c(words, np.uint32).reshape(-1)
+        fp = _c(footprints, np.int32).reshape(-1, 4)
+        m = _c(measures if measures is not None else np.zeros((0, 12), np.uint32), np.uint32).reshape(-1, 12)
+        n_fp = (fp.shape[0] - 1) // 3
+        self._check(self._lib.vgi_apply_events_footprints(self._h, _ptr(w), n_events, w.size, _ptr(m) if m.size else None, m.shape[0],
+                                                          _ptr(fp), n_fp))
+        out = np.zeros_like(w)
+        self._check(self._lib.vgi_read_events(self._h, _ptr(out), out.size))
+        return out
+
     def view_set_receivers(self, faces: np.ndarray) -> None:
         """Visible unit faces (voxel xyz, face, material rows) as view receivers."""
         f = _c(faces, np.int32).reshape(-1, 5)

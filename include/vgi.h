@@ -212,6 +212,20 @@ int vgi_apply_events(vgi_ctx* ctx, const uint32_t* words, uint32_t n_events, uin
  * vgi_read_events until the next call. */
 int vgi_apply_events_measured(vgi_ctx* ctx, const uint32_t* words, uint32_t n_events, uint64_t n_words, const uint32_t* measures,
                               uint32_t n_entries);
+/* Change footprints (trace_footprints, finish_footprints, shaders/voxel_trace.wgsl:
+ * 94-202; planned by plan_footprints / encode_footprints, src/gpu/resident.rs:
+ * 1218-1325): before the measured edits and retention read the event list,
+ * sunlight tubes through each changed box, along each directional light whose
+ * sun side is clear, find where the box's shadow lands; that landing box
+ * and its reflected power (x 64, rounded) become the task's reserved Light
+ * event (its header union and its one bound, kind 4). A task whose tubes
+ * land nowhere keeps its empty bound. footprints: (1 + 3 n) records of 4
+ * int32 words, encode_footprints' layout: the count, then per task (box min,
+ * header record) (box max, bound record) (first thread, grid, 0, 0), with
+ * grid^2 threads per task tiling the threads in order. Otherwise as
+ * vgi_apply_events_measured; vgi_read_events returns the filled events. */
+int vgi_apply_events_footprints(vgi_ctx* ctx, const uint32_t* words, uint32_t n_events, uint64_t n_words, const uint32_t* measures,
+                                uint32_t n_entries, const int32_t* footprints, uint32_t n_footprints);
 int vgi_read_events(vgi_ctx* ctx, uint32_t* words, uint64_t n_words);
 
 /* ---- view tier: the visible-face path history of the view renderer -----------

@@ -1197,6 +1197,103 @@ static uint32_t candidate_key(const uint32_t* slot_meta, uint32_t slot, const ui
     return (2u << 8u) | (255u - umin(b, 255u));
 }
 
+// trace_footprints + finish_footprints (voxel_trace.wgsl:94-202), thread by
+// thread: fp = (1 + 3 n) records of 4 int32 words, sums = 8 words per task
+// (the caller's initial min 0xffffffff, max 0, flux 0), events = event words.
+int orc_footprints(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
+                   const float* materials, const float* lights, const int32_t* fp, uint32_t threads, uint32_t* sums, uint32_t* events) {
+    const int32_t BIAS = 1073741824;
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, materials, lights, nullptr, nullptr, nullptr, orc_pipeline{1, 0, 2048, 0, 1}};
+    Ctx x{g, m, Counters{}};
+    const uint32_t n = (uint32_t)fp[0];
+    const uint32_t n_directional = ((const uint32_t*)params)[11];
+    const float reach = params[17];
+    for (uint32_t id = 0; id < threads && n > 0; ++id) {
+        uint32_t lo_t = 0, hi_t = n;
+        while (hi_t - lo_t > 1u) {
+            const uint32_t mid = (lo_t + hi_t) / 2u;
+            if ((uint32_t)fp[(1 + mid * 3 + 2) * 4] <= id) lo_t = mid;
+            else hi_t = mid;
+        }
+        const uint32_t e = lo_t;
+        const int32_t* a = fp + (1 + e * 3) * 4;
+        const int32_t* b = a + 4;
+        const int32_t* c = a + 8;
+        const uint32_t grid = (uint32_t)c[1];
+        const uint32_t local = id - (uint32_t)c[0];
+        if (local >= grid * grid) continue;
+        const f3 lo{(float)a[0], (float)a[1], (float)a[2]};
+        const f3 hi{(float)b[0] + 1.0f, (float)b[1] + 1.0f, (float)b[2] + 1.0f};
+        const f3 center = muls(add(lo, hi), 0.5f);
+        const f3 span = sub(hi, lo);
+        const float diagonal = std::sqrt(dot(span, span));
+        const float spacing = diagonal / (float)grid;
+        const float half = 0.5f * diagonal;
+        const float ox = ((float)(local % grid) + 0.5f) * spacing - half;
+        const float oy = ((float)(local / grid) + 0.5f) * spacing - half;
+        const f3 w{0.2126f, 0.7152f, 0.0722f};
+        const uint32_t base = e * 8;
+        float flux = 0.0f;
+        for (uint32_t i = 0; i < n_directional; ++i) {
+            const float* L = lights + (size_t)i * 12;
+            const f3 color{wmax(L[4] - L[9], 0.0f), wmax(L[5] - L[10], 0.0f), wmax(L[6] - L[11], 0.0f)};
+            if (color.x == 0.0f && color.y == 0.0f && color.z == 0.0f) continue;
+            const f3 raw{L[0], L[1], L[2]};
+            const float len = std::sqrt(dot(raw, raw));
+            const f3 direction{raw.x / len, raw.y / len, raw.z / len};
+            const f3 pick = std::fabs(direction.y) > 0.9f ? f3{1.0f, 0.0f, 0.0f} : f3{0.0f, 1.0f, 0.0f};
+            const f3 uc = cross(direction, pick);
+            const float ul = std::sqrt(dot(uc, uc));
+            const f3 u{uc.x / ul, uc.y / ul, uc.z / ul};
+            const f3 v = cross(direction, u);
+            const f3 point = add(add(center, muls(u, ox)), muls(v, oy));
+            const f3 inverse{1.0f / (std::fabs(direction.x) < 1e-8f ? 1e-8f : direction.x),
+                             1.0f / (std::fabs(direction.y) < 1e-8f ? 1e-8f : direction.y),
+                             1.0f / (std::fabs(direction.z) < 1e-8f ? 1e-8f : direction.z)};
+            const f3 nearv = mul(sub(lo, point), inverse), farv = mul(sub(hi, point), inverse);
+            const float enter = wmax(wmax(wmin(nearv.x, farv.x), wmin(nearv.y, farv.y)), wmin(nearv.z, farv.z));
+            const float exit = wmin(wmin(wmax(nearv.x, farv.x), wmax(nearv.y, farv.y)), wmax(nearv.z, farv.z));
+            if (enter > exit) continue;
+            if (trace_domain_limited(x, add(point, muls(direction, exit + 0.01f)), direction, reach, true, 2048u).status != 0u) continue;
+            const f3 start = add(point, muls(direction, enter - 0.01f));
+            const RayResult hit = trace_domain_limited(x, start, neg(direction), reach, true, 2048u);
+            const f3 gap = sub(hit.position, start);
+            if (hit.status != 1u || dot(hit.normal, direction) <= 0.0f || std::sqrt(dot(gap, gap)) < 0.02f) continue;
+            const float* mat = materials + (size_t)hit.material * 16;
+            flux = flux + ((dot(color, w) * dot(f3{mat[0], mat[1], mat[2]}, w)) * spacing) * spacing;
+            const uint32_t p[3] = {(uint32_t)(hit.voxel.x + BIAS), (uint32_t)(hit.voxel.y + BIAS), (uint32_t)(hit.voxel.z + BIAS)};
+            for (int k = 0; k < 3; ++k) {
+                sums[base + k] = umin(sums[base + k], p[k]);
+                sums[base + 3 + k] = umax(sums[base + 3 + k], p[k]);
+            }
+        }
+        if (flux > 0.0f) sums[base + 6] += f2u(flux * 64.0f + 0.5f);
+    }
+    for (uint32_t e = 0; e < n; ++e) {
+        const uint32_t base = e * 8;
+        if (sums[base] == 0xffffffffu) continue;
+        int32_t mn[3], mx[3];
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = (int32_t)sums[base + k] - BIAS;
+            mx[k] = (int32_t)sums[base + 3 + k] - BIAS;
+        }
+        const float flux = (float)sums[base + 6] / 64.0f;
+        const uint32_t header = (uint32_t)fp[(1 + e * 3) * 4 + 3], bound = (uint32_t)fp[(1 + e * 3 + 1) * 4 + 3];
+        uint32_t* h = events + (size_t)header * 4;
+        uint32_t* bd = events + (size_t)bound * 4;
+        for (int k = 0; k < 3; ++k) {
+            h[k] = (uint32_t)mn[k];
+            h[4 + k] = (uint32_t)mx[k];
+            bd[k] = (uint32_t)mn[k];
+            bd[4 + k] = (uint32_t)mx[k];
+        }
+        bd[3] = fbits(flux);
+        bd[7] = 4u;
+    }
+    return 0;
+}
+
 // candidate keys only, for slots [controls[26], controls[27]).
 int orc_classify(const uint32_t* slot_meta, uint32_t* keys, uint32_t n_slots, const uint32_t* ctl) {
     for (uint32_t slot = ctl[26]; slot < ctl[27] && slot < n_slots; ++slot) keys[slot] = candidate_key(slot_meta, slot, ctl);

@@ -51,6 +51,7 @@ _SIG = {
     "orc_trace_faces_predicted": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _U32, _P, _P, _INT]),
     "orc_predicted_misses": (_U64, [_P]),
     "orc_accumulate_picks": (_INT, [_P, _P, _P, _P, _P, _U32, _P, _P]),
+    "orc_footprints": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _U32, _P, _P]),
     "orc_classify": (_INT, [_P, _P, _U32, _P]),
     "orc_select": (_INT, [_P, _P, _P, _U32, _P, _P, _P, _P, _P]),
     "orc_trace_ray": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P]),
