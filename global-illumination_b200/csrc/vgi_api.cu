@@ -1141,6 +1141,55 @@ int vgi_read_selection(vgi_ctx* c, uint32_t* keys, uint32_t* selection, uint32_t
     return VGI_OK;
 }
 
+int vgi_discover_faces(vgi_ctx* c, const vgi_camera* cam, uint32_t* pixels8, vgi_face* faces, uint32_t capacity, uint32_t* n_faces) {
+    if (!c || !cam || (capacity && !faces)) return VGI_ERR_INVALID;
+    if (!c->geometry) return fail(c, VGI_ERR_STATE, "no geometry uploaded");
+    const uint64_t n = (uint64_t)cam->width * cam->height;
+    if (n == 0 || n > (1ull << 26)) return fail(c, VGI_ERR_INVALID, "camera size outside 1..2^26 pixels");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    uint32_t mask = 1;
+    while (mask < 2 * n) mask <<= 1;
+    DevBuf<float> dcam;
+    DevBuf<uint4> pixels;
+    DevBuf<unsigned long long> set;
+    DevBuf<int4> list;
+    DevBuf<uint32_t> counters;
+    VGI_CUDA(c, dcam.reserve(10));
+    VGI_CUDA(c, pixels.reserve(n * 2));
+    VGI_CUDA(c, set.reserve(mask));
+    VGI_CUDA(c, list.reserve(std::max<uint32_t>(capacity, 1)));
+    VGI_CUDA(c, counters.reserve(2));
+    float host_cam[10] = {cam->eye[0], cam->eye[1], cam->eye[2], cam->forward[0], cam->forward[1], cam->forward[2],
+                          cam->up[0], cam->up[1], cam->up[2], cam->tan_half_fov};
+    VGI_CUDA(c, cudaMemcpyAsync(dcam.ptr, host_cam, sizeof(host_cam), cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(set.ptr, 0xff, (size_t)mask * 8, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(counters.ptr, 0, 8, c->stream));
+    const TraceArgs tr = trace_args(c, nullptr, nullptr, 0, 1, false);
+    launch_discover(tr, dcam.ptr, cam->width, cam->height, pixels.ptr, set.ptr, mask - 1, list.ptr, counters.ptr, capacity, counters.ptr + 1,
+                    c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    uint32_t counts[2] = {0, 0};
+    VGI_CUDA(c, cudaMemcpyAsync(counts, counters.ptr, 8, cudaMemcpyDeviceToHost, c->stream));
+    if (pixels8) VGI_CUDA(c, cudaMemcpyAsync(pixels8, pixels.ptr, n * 32, cudaMemcpyDeviceToHost, c->stream));
+    std::vector<int4> found(std::min(counts[0], capacity));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (n_faces) *n_faces = counts[0];
+    if (counts[0] > capacity) return fail(c, VGI_ERR_CAPACITY, "more faces than the list holds: n_faces says how many");
+    if (counts[1]) return fail(c, VGI_ERR_CAPACITY, "the face set overflowed");
+    if (!found.empty()) VGI_CUDA(c, cudaMemcpy(found.data(), list.ptr, found.size() * 16, cudaMemcpyDeviceToHost));
+    // The list order follows the GPU's insertions; sort it by voxel z, y, x
+    // and face, the order of the scene's exposed faces.
+    std::sort(found.begin(), found.end(), [](const int4& a, const int4& b) {
+        if (a.z != b.z) return a.z < b.z;
+        if (a.y != b.y) return a.y < b.y;
+        if (a.x != b.x) return a.x < b.x;
+        return (a.w & 7) < (b.w & 7);
+    });
+    for (size_t k = 0; k < found.size(); ++k)
+        faces[k] = vgi_face{{found[k].x, found[k].y, found[k].z}, (uint32_t)found[k].w & 7u, (uint32_t)found[k].w >> 8};
+    return VGI_OK;
+}
+
 int vgi_read_cache(vgi_ctx* c, uint32_t first, uint32_t n, float* dst4, int on_device) {
     if (!c || (n && !dst4) || first > c->n_slots || n > c->n_slots - first) return VGI_ERR_INVALID;
     if (n == 0) return VGI_OK;

@@ -990,6 +990,72 @@ __global__ void __launch_bounds__(64) finish_footprints_kernel(const int4* fp, c
 }
 }  // namespace
 
+// ---- headless discovery: primary rays into the NAADF geometry -----------------
+namespace {
+// A pixel's primary ray (the camera of vgi_camera): right = normalize(
+// forward x up), up' = right x forward; sx = ((2 (x + 0.5)) / W - 1) *
+// tan_half * (W / H), sy = (1 - (2 (y + 0.5)) / H) * tan_half; direction =
+// normalize((forward + right sx) + up' sy). Host callers normalise forward.
+__device__ V3 pixel_ray(const float* cam, uint32_t x, uint32_t y, uint32_t w, uint32_t h) {
+    const V3 forward{cam[3], cam[4], cam[5]}, up{cam[6], cam[7], cam[8]};
+    const V3 right = normalize3(cross3(forward, up));
+    const V3 up2 = cross3(right, forward);
+    const float fw = (float)w, fh = (float)h;
+    const float sx = __fmul_rn(__fmul_rn(__fsub_rn(__fdiv_rn(__fmul_rn(2.0f, __fadd_rn((float)x, 0.5f)), fw), 1.0f), cam[9]), __fdiv_rn(fw, fh));
+    const float sy = __fmul_rn(__fsub_rn(1.0f, __fdiv_rn(__fmul_rn(2.0f, __fadd_rn((float)y, 0.5f)), fh)), cam[9]);
+    return normalize3((forward + right * sx) + up2 * sy);
+}
+
+__device__ __forceinline__ unsigned long long face_key64(I3 v, uint32_t face) {
+    const unsigned long long m = (1ull << 20) - 1ull;
+    return ((unsigned long long)((uint32_t)v.x & m)) | ((unsigned long long)((uint32_t)v.y & m) << 20) |
+           ((unsigned long long)((uint32_t)v.z & m) << 40) | ((unsigned long long)face << 60);
+}
+
+// One thread per pixel: the first hit of the pixel's ray (visible geometry,
+// 2048 steps) as (voxel xyz, face (6: none), material, status, distance
+// bits, 0); each hit face enters the set once and the thread that inserted
+// it appends the face (voxel xyz, face, material) to the list.
+__global__ void __launch_bounds__(128) discover_kernel(const TraceArgs A, const float* cam, uint32_t w, uint32_t h, uint4* pixels,
+                                                       unsigned long long* set, uint32_t set_mask, int4* faces, uint32_t* count,
+                                                       uint32_t capacity, uint32_t* overflow) {
+    const uint32_t id = blockIdx.x * 128u + threadIdx.x;
+    if (id >= w * h) return;
+    Cnt<false> cnt;
+    const uint32_t x = id % w, y = id / w;
+    const V3 eye{cam[0], cam[1], cam[2]};
+    const V3 dir = pixel_ray(cam, x, y, w, h);
+    const Ray r = trace_domain(A, eye, dir, A.max_distance, true, 2048u, cnt);
+    const uint32_t face = r.status == 1u ? face_index_of(r.normal) : 6u;
+    const float distance = r.status == 1u ? len3(r.position - eye) : 0.0f;
+    pixels[(size_t)id * 2u] = make_uint4((uint32_t)r.voxel.x, (uint32_t)r.voxel.y, (uint32_t)r.voxel.z, face);
+    pixels[(size_t)id * 2u + 1u] = make_uint4(r.material, r.status, __float_as_uint(distance), 0u);
+    if (face > 5u) return;
+    const unsigned long long key = face_key64(r.voxel, face);
+    uint32_t s = (hash_voxel(r.voxel.x, r.voxel.y, r.voxel.z) ^ pcg(face + 1u)) & set_mask;
+    // Bounded probing: the set holds at least twice the pixels.
+#pragma unroll 1
+    for (uint32_t probe = 0; probe <= set_mask; ++probe) {
+        const unsigned long long old = atomicCAS(set + s, ~0ull, key);
+        if (old == key) return;  // already listed
+        if (old == ~0ull) {
+            const uint32_t k = atomicAdd(count, 1u);
+            // Past the capacity only the count grows: the host reports it.
+            if (k < capacity) faces[k] = make_int4(r.voxel.x, r.voxel.y, r.voxel.z, (int)(face | (r.material << 8)));
+            return;
+        }
+        s = (s + 1u) & set_mask;
+    }
+    atomicOr(overflow, 1u);
+}
+}  // namespace
+
+void launch_discover(const TraceArgs& a, const float* cam, uint32_t w, uint32_t h, uint4* pixels, unsigned long long* set, uint32_t set_mask,
+                     int4* faces, uint32_t* count, uint32_t capacity, uint32_t* overflow, cudaStream_t s) {
+    const uint32_t n = w * h;
+    if (n) discover_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, cam, w, h, pixels, set, set_mask, faces, count, capacity, overflow);
+}
+
 void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uint32_t threads, uint32_t n_directional, uint32_t* sums,
                        uint4* events, cudaStream_t s) {
     if (n_tasks == 0) return;

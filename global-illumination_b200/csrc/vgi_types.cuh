@@ -157,6 +157,10 @@ const void* accumulate_kernel_address();
 // task; sums = 8 words per task (min xyz, max xyz, flux x 64, unused).
 void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uint32_t threads, uint32_t n_directional, uint32_t* sums,
                        uint4* events, cudaStream_t s);
+// Headless discovery (vgi_trace.cu): cam = eye xyz, forward xyz, up xyz,
+// tan(half vertical fov); set = 64-bit keys, all ones when empty.
+void launch_discover(const TraceArgs& a, const float* cam, uint32_t w, uint32_t h, uint4* pixels, unsigned long long* set, uint32_t set_mask,
+                     int4* faces, uint32_t* count, uint32_t capacity, uint32_t* overflow, cudaStream_t s);
 // MLP radiance cache (vgi_mlp.cu).
 cudaError_t mlp_set_attributes();
 void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,

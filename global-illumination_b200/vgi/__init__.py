@@ -44,6 +44,12 @@ class TransportUnavailable(VgiError):
     (src/lib.rs:355-357); it never falls back to the CPU."""
 
 
+class Camera(ctypes.Structure):
+    """vgi_camera."""
+    _fields_ = [("eye", ctypes.c_float * 3), ("forward", ctypes.c_float * 3), ("up", ctypes.c_float * 3), ("tan_half_fov", ctypes.c_float),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
+
+
 class Schedule(ctypes.Structure):
     """vgi_schedule."""
     _fields_ = [("focus", ctypes.c_int32 * 3), ("budget", ctypes.c_uint32), ("classify_first", ctypes.c_uint32),
@@ -192,6 +198,7 @@ _SIGNATURES = {
     "vgi_frame_shard": (_INT, [_P, _U32, _U32, _U32, _U32]),
     "vgi_submit_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P, _P]),
     "vgi_frame_scheduled": (_INT, [_P, _U32, _U32, _P]),
+    "vgi_discover_faces": (_INT, [_P, _P, _P, _P, _U32, _P]),
     "vgi_apply_events_footprints": (_INT, [_P, _P, _U32, _U64, _P, _U32, _P, _U32]),
     "vgi_read_selection": (_INT, [_P, _P, _P, _P, _P, _P]),
     "vgi_complete_batch": (_INT, [_P, _U64]),
@@ -600,6 +607,22 @@ class GpuTracer:
 
     def complete_batch(self, ticket: int) -> None:
         self._check(self._lib.vgi_complete_batch(self._h, ticket))
+
+    # headless discovery
+    def discover_faces(self, eye, forward, up, tan_half_fov: float, width: int, height: int, capacity: Optional[int] = None):
+        """Primary rays per pixel: (pixels (h, w, 8) u32 records, faces (n, 5)
+        rows voxel xyz, face, material). The default capacity, one face per
+        pixel, always suffices."""
+        capacity = width * height if capacity is None else capacity
+        f = np.asarray(forward, np.float64)
+        f = (f / np.linalg.norm(f)).astype(np.float32)
+        cam = Camera((ctypes.c_float * 3)(*map(float, eye)), (ctypes.c_float * 3)(*map(float, f)),
+                     (ctypes.c_float * 3)(*map(float, up)), float(tan_half_fov), width, height)
+        pixels = np.zeros((height, width, 8), np.uint32)
+        faces = np.zeros((capacity, 5), np.int32)
+        n = ctypes.c_uint32()
+        self._check(self._lib.vgi_discover_faces(self._h, ctypes.byref(cam), _ptr(pixels), _ptr(faces), capacity, ctypes.byref(n)))
+        return pixels, faces[: n.value].copy()
 
     # scheduled frames
     def frame_scheduled(self, samples: int, clock_ms: int, budget: int, focus=(0, 0, 0), classify=None, audit_ms: int = 1000) -> None:

@@ -327,6 +327,28 @@ typedef struct vgi_mlp_status {
 /* Synchronous. */
 int vgi_mlp_stats(vgi_ctx* ctx, vgi_mlp_status* out);
 
+/* ---- headless discovery ---------------------------------------------------------
+ * The face list from the GPU instead of a raster prepass (as NAADF's
+ * renderFirstHit): one primary ray per pixel of a pinhole camera through
+ * the NAADF geometry (trace_domain_limited with visible geometry, 2048
+ * steps). Pixel (x, y): right = normalize(forward x up), up' = right x
+ * forward, sx = ((2 (x + 0.5)) / width - 1) tan_half_fov (width / height),
+ * sy = (1 - (2 (y + 0.5)) / height) tan_half_fov, direction =
+ * normalize((forward + right sx) + up' sy); forward must be unit length.
+ * pixels8 (may be null) receives per pixel (voxel xyz, face (6: no hit),
+ * material, status, distance (f32 bits), 0); faces receives each hit face
+ * once (its voxel, face and the hit's material), sorted by voxel z, y, x and
+ * face. *n_faces is the number of distinct faces even when it exceeds
+ * `capacity` (then VGI_ERR_CAPACITY). At most 2^26 pixels. Synchronous. */
+typedef struct vgi_camera {
+    float eye[3];
+    float forward[3];
+    float up[3];
+    float tan_half_fov;
+    uint32_t width, height;
+} vgi_camera;
+int vgi_discover_faces(vgi_ctx* ctx, const vgi_camera* camera, uint32_t* pixels8, vgi_face* faces, uint32_t capacity, uint32_t* n_faces);
+
 /* ---- scheduled frames: the GPU world-cache scheduler --------------------------
  * The reference's GPU selection of bulk work (shaders/voxel_accumulate.wgsl:
  * 448-695: candidate, select_classify, select_histogram, select_threshold,

@@ -1294,6 +1294,49 @@ int orc_footprints(const int32_t* directory, uint64_t slots, const uint32_t* hea
     return 0;
 }
 
+// Headless discovery's per-pixel first hits (the GPU's discover kernel):
+// cam = eye xyz, forward xyz (unit), up xyz, tan(half vertical fov);
+// pixels = 8 words per pixel (voxel xyz, face or 6, material, status,
+// distance bits, 0).
+int orc_discover(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
+                 const float* cam, uint32_t w, uint32_t h, uint32_t* pixels, int threads) {
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, nullptr, nullptr, nullptr, nullptr, nullptr, orc_pipeline{1, 0, 2048, 0, 1}};
+    const f3 eye{cam[0], cam[1], cam[2]}, forward{cam[3], cam[4], cam[5]}, up{cam[6], cam[7], cam[8]};
+    const f3 rc = cross(forward, up);
+    const float rl = std::sqrt(dot(rc, rc));
+    const f3 right{rc.x / rl, rc.y / rl, rc.z / rl};
+    const f3 up2 = cross(right, forward);
+    const float fw = (float)w, fh = (float)h;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<uint32_t> next{0};
+    auto worker = [&]() {
+        Ctx x{g, m, Counters{}};
+        for (;;) {
+            const uint32_t id = next.fetch_add(1);
+            if (id >= w * h) break;
+            const uint32_t px = id % w, py = id / w;
+            const float sx = ((2.0f * ((float)px + 0.5f)) / fw - 1.0f) * cam[9] * (fw / fh);
+            const float sy = (1.0f - (2.0f * ((float)py + 0.5f)) / fh) * cam[9];
+            const f3 raw = add(add(forward, muls(right, sx)), muls(up2, sy));
+            const float len = std::sqrt(dot(raw, raw));
+            const f3 dir{raw.x / len, raw.y / len, raw.z / len};
+            const RayResult r = trace_domain_limited(x, eye, dir, params[17], true, 2048u);
+            const uint32_t face = r.status == 1u ? face_index_of(r.normal) : 6u;
+            const f3 gap = sub(r.position, eye);
+            const float distance = r.status == 1u ? std::sqrt(dot(gap, gap)) : 0.0f;
+            uint32_t* o = pixels + (size_t)id * 8;
+            o[0] = (uint32_t)r.voxel.x; o[1] = (uint32_t)r.voxel.y; o[2] = (uint32_t)r.voxel.z; o[3] = face;
+            o[4] = r.material; o[5] = r.status; o[6] = fbits(distance); o[7] = 0;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    return 0;
+}
+
 // candidate keys only, for slots [controls[26], controls[27]).
 int orc_classify(const uint32_t* slot_meta, uint32_t* keys, uint32_t n_slots, const uint32_t* ctl) {
     for (uint32_t slot = ctl[26]; slot < ctl[27] && slot < n_slots; ++slot) keys[slot] = candidate_key(slot_meta, slot, ctl);

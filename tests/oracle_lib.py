@@ -52,6 +52,7 @@ _SIG = {
     "orc_predicted_misses": (_U64, [_P]),
     "orc_accumulate_picks": (_INT, [_P, _P, _P, _P, _P, _U32, _P, _P]),
     "orc_footprints": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _U32, _P, _P]),
+    "orc_discover": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P, _INT]),
     "orc_classify": (_INT, [_P, _P, _U32, _P]),
     "orc_select": (_INT, [_P, _P, _P, _U32, _P, _P, _P, _P, _P]),
     "orc_trace_ray": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P]),
@@ -171,6 +172,31 @@ def canonical(directory, headers, cells, coords):
     rc = lib().orc_canonical(ptr(d), d.size // 4, ptr(h), ptr(cl), cells.size, ptr(co), co.shape[0], ptr(out))
     assert rc == 0, rc
     return out
+
+
+def discover(geometry, params, eye, forward, up, tan_half_fov, width, height, threads=0):
+    """orc_discover: (height, width, 8) per-pixel first-hit records, as the
+    GPU's vgi_discover_faces writes them."""
+    d, h, cl, _ = geometry
+    d = c(d, np.int32)
+    cl = c(cl, np.uint32) if len(cl) else np.zeros(1, np.uint32)
+    cam = np.array([*eye, *forward, *up, tan_half_fov], np.float32)
+    out = np.zeros((height, width, 8), np.uint32)
+    rc = lib().orc_discover(ptr(d), d.size // 4, ptr(c(h, np.uint32)), ptr(cl), ptr(c(params, np.float32)), ptr(cam), width, height,
+                            ptr(out), threads)
+    assert rc == 0
+    return out
+
+
+def discovered_faces(pixels):
+    """The distinct hit faces of per-pixel records as (n, 5) rows voxel xyz,
+    face, material, sorted by voxel z, y, x and face."""
+    p = np.asarray(pixels, np.uint32).reshape(-1, 8)
+    p = p[p[:, 3] < 6]
+    rows = np.stack([p[:, 0].view(np.int32), p[:, 1].view(np.int32), p[:, 2].view(np.int32), p[:, 3].astype(np.int32),
+                     p[:, 4].astype(np.int32)], 1)
+    rows = np.unique(rows, axis=0)
+    return rows[np.lexsort((rows[:, 3], rows[:, 0], rows[:, 1], rows[:, 2]))]
 
 
 # ---- model words ------------------------------------------------------------
