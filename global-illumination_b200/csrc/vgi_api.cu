@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -148,6 +149,23 @@ struct vgi_ctx {
     bool mlp_timed = false;                   // the last timed frame recorded mlp_marks
     bool mlp_queried = false;                 // a frame has queried the network (counters[4] holds its count)
     uint32_t n_view = 0;
+    // The view receivers' owner hash for the far tier's handoff (stale after
+    // vgi_view_set_receivers).
+    DevBuf<uint32_t> v_hash;
+    uint32_t v_hash_mask = 0;
+    bool v_hash_valid = false;
+    bool custom_lights = false;               // some light has custom visible RGB
+    // far tier: cell histories (this frame's and the previous one's), the
+    // output cells, the trace queue and the statistics
+    DevBuf<uint4> far_cells[2];
+    DevBuf<uint4> far_output;
+    DevBuf<uint32_t> far_queue, far_stats;
+    uint32_t far_current = 0;
+    uint32_t far_shape[4] = {0, 0, 0, 0};     // cells x, y, pixels per side, enabled | measure << 1
+    uint32_t far_size[2] = {0, 0};            // viewport
+    float far_prev[10] = {};
+    uint32_t far_last_frame = 0;
+    bool far_has_prev = false;
     DevBuf<uint4> events;
     DevBuf<int4> footprints;                 // change-footprint tasks of the last event list
     DevBuf<uint32_t> footprint_sums;
@@ -815,6 +833,10 @@ int vgi_set_lights(vgi_ctx* c, const float* lights, uint32_t n, uint32_t n_direc
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->n_lights = n;
     c->n_directional = n_directional;
+    // transport.y of the view's parameters (src/gpu/view.rs:104-116).
+    c->custom_lights = false;
+    for (uint32_t i = 0; i < n; ++i)
+        for (int k = 9; k < 12; ++k) c->custom_lights |= lights[(size_t)i * 12 + k] != 0.0f;
     return VGI_OK;
 }
 
@@ -1555,6 +1577,135 @@ int vgi_view_set_receivers(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     }
     VGI_CUDA(c, cudaMemsetAsync(c->v_queue.ptr, 0, (12 + 2 * m) * 4, c->stream));
     c->n_view = n;
+    c->v_hash_valid = false;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+// ---- far tier (voxel_view_pixels.wgsl) -------------------------------------------
+int vgi_far_frame(vgi_ctx* c, const vgi_camera* cam, const vgi_far_settings* settings, uint32_t frame) {
+    if (!c || !cam || !settings) return VGI_ERR_INVALID;
+    if (!view_ready(c)) return fail(c, VGI_ERR_STATE, "the far tier needs geometry, materials, lights and emitters");
+    if (cam->width == 0 || cam->height == 0 || (uint64_t)cam->width * cam->height > (1ull << 26))
+        return fail(c, VGI_ERR_INVALID, "camera size outside 1..2^26 pixels");
+    if (settings->measure > 2) return fail(c, VGI_ERR_INVALID, "far measure is 0, 1 or 2");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    // FarTierSettings::normalized and cell_for (src/settings.rs:140-167).
+    const float voxel_pixels = std::isfinite(settings->voxel_pixels) ? std::min(std::max(settings->voxel_pixels, 0.0f), 4096.0f) : 0.0f;
+    const float history = std::isfinite(settings->history) ? std::min(std::max(settings->history, 1.0f), 1024.0f) : 32.0f;
+    const uint32_t rate = std::min<uint32_t>(std::max<uint32_t>(settings->rate, 1u), 8u);
+    const uint32_t steps = std::min<uint32_t>(std::max<uint32_t>(settings->steps, 16u), 2048u);
+    uint32_t size = std::min<uint32_t>(settings->cell, 4u);
+    if (size == 0) size = (uint32_t)std::min(std::max(std::round((float)cam->height / 480.0f), 1.0f), 4.0f);
+    const uint32_t cx = (cam->width + size - 1) / size, cy = (cam->height + size - 1) / size;
+    const uint32_t cells = cx * cy;
+    const uint32_t flags = (voxel_pixels > 0.0f ? 1u : 0u) | (settings->measure << 1);
+    if (cx != c->far_shape[0] || cy != c->far_shape[1] || cam->width != c->far_size[0] || cam->height != c->far_size[1]) {
+        for (auto& b : c->far_cells) {
+            VGI_CUDA(c, b.reserve((size_t)cells * 3));
+            VGI_CUDA(c, cudaMemsetAsync(b.ptr, 0, (size_t)cells * 48, c->stream));
+        }
+        VGI_CUDA(c, c->far_output.reserve(4 + (size_t)cells));
+        VGI_CUDA(c, cudaMemsetAsync(c->far_output.ptr, 0, (4 + (size_t)cells) * 16, c->stream));
+        VGI_CUDA(c, c->far_queue.reserve(1 + (size_t)cells));
+        VGI_CUDA(c, c->far_stats.reserve(8));
+        c->far_has_prev = false;
+        c->far_size[0] = cam->width;
+        c->far_size[1] = cam->height;
+    }
+    c->far_shape[0] = cx;
+    c->far_shape[1] = cy;
+    c->far_shape[2] = size;
+    c->far_shape[3] = flags;
+    // A camera not drawn last frame loses its history (src/gpu/view/runtime.rs:870-871).
+    const bool previous = c->far_has_prev && frame - c->far_last_frame <= 1u;
+    FarView f{};
+    const float cam_words[10] = {cam->eye[0], cam->eye[1], cam->eye[2], cam->forward[0], cam->forward[1], cam->forward[2],
+                                 cam->up[0], cam->up[1], cam->up[2], cam->tan_half_fov};
+    std::copy(cam_words, cam_words + 10, f.cam);
+    std::copy(previous ? c->far_prev : cam_words, (previous ? c->far_prev : cam_words) + 10, f.prev);
+    f.width = cam->width;
+    f.height = cam->height;
+    f.grid[0] = cx;
+    f.grid[1] = cy;
+    f.grid[2] = size;
+    f.grid[3] = flags;
+    const uint32_t prev_bits = previous ? c->far_last_frame : 0xffffffffu;
+    f.tune[0] = voxel_pixels;
+    f.tune[1] = history;
+    f.tune[2] = (float)rate;
+    std::memcpy(&f.tune[3], &prev_bits, 4);
+    // pixel_axis: the view forward and clip_from_view[1][1] * height / 2.
+    f.axis[0] = cam->forward[0];
+    f.axis[1] = cam->forward[1];
+    f.axis[2] = cam->forward[2];
+    f.axis[3] = (1.0f / cam->tan_half_fov) * (float)cam->height * 0.5f;
+    for (int k = 0; k < 3; ++k) {
+        f.interest_min[k] = settings->interest_min[k];
+        f.interest_max[k] = settings->interest_max[k];
+    }
+    f.interest_min[3] = f.interest_max[3] = settings->bounded ? 1 : 0;
+    f.frame = frame;
+    f.custom = c->custom_lights ? 1u : 0u;
+    if (c->n_view) {
+        if (!c->v_hash_valid) {
+            uint32_t mask = 63;
+            while (mask + 1 < 2 * c->n_view) mask = mask * 2 + 1;
+            VGI_CUDA(c, c->v_hash.reserve((size_t)mask + 1));
+            VGI_CUDA(c, cudaMemsetAsync(c->v_hash.ptr, 0, ((size_t)mask + 1) * 4, c->stream));
+            launch_receiver_hash(c->v_receivers.ptr, c->n_view, c->v_hash.ptr, mask, c->stream);
+            c->v_hash_mask = mask;
+            c->v_hash_valid = true;
+        }
+        f.receivers = c->v_receivers.ptr;
+        f.estimates = c->v_estimates.ptr;
+        f.receiver_hash = c->v_hash.ptr;
+        f.hash_mask = c->v_hash_mask;
+        f.n_receivers = c->n_view;
+    }
+    TraceArgs a = trace_args(c, nullptr, nullptr, 0, 1, c->n_slots > 0);
+    a.path_steps = steps;
+    VGI_CUDA(c, cudaMemsetAsync(c->far_queue.ptr, 0, 4, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->far_stats.ptr, 0, 32, c->stream));
+    const uint32_t prev_index = c->far_current;
+    c->far_current ^= 1u;
+    launch_far(a, f, c->far_cells[prev_index].ptr, c->far_cells[c->far_current].ptr, c->far_output.ptr, c->far_queue.ptr, c->far_stats.ptr,
+               transport_limited(c), c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    std::copy(cam_words, cam_words + 10, c->far_prev);
+    c->far_last_frame = frame;
+    c->far_has_prev = true;
+    return VGI_OK;
+}
+
+int vgi_far_reset(vgi_ctx* c) {
+    if (!c) return VGI_ERR_INVALID;
+    // A new camera's state: zeroed histories and output (the stale cells a
+    // reader skips by their stamp start empty).
+    const size_t cells = (size_t)c->far_shape[0] * c->far_shape[1];
+    if (cells) {
+        VGI_CUDA(c, cudaSetDevice(c->device));
+        for (auto& b : c->far_cells) VGI_CUDA(c, cudaMemsetAsync(b.ptr, 0, cells * 48, c->stream));
+        VGI_CUDA(c, cudaMemsetAsync(c->far_output.ptr, 0, (4 + cells) * 16, c->stream));
+        VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    c->far_current = 0;
+    c->far_has_prev = false;
+    return VGI_OK;
+}
+
+int vgi_far_read(vgi_ctx* c, uint32_t* shape4, uint32_t* output, uint32_t* cells12, uint32_t* stats8) {
+    if (!c) return VGI_ERR_INVALID;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    const size_t cells = (size_t)c->far_shape[0] * c->far_shape[1];
+    if (shape4) std::copy(c->far_shape, c->far_shape + 4, shape4);
+    if (cells) {
+        if (output) VGI_CUDA(c, cudaMemcpyAsync(output, c->far_output.ptr, (4 + cells) * 16, cudaMemcpyDeviceToHost, c->stream));
+        if (cells12) VGI_CUDA(c, cudaMemcpyAsync(cells12, c->far_cells[c->far_current].ptr, cells * 48, cudaMemcpyDeviceToHost, c->stream));
+        if (stats8) VGI_CUDA(c, cudaMemcpyAsync(stats8, c->far_stats.ptr, 32, cudaMemcpyDeviceToHost, c->stream));
+    } else if (stats8) {
+        std::fill(stats8, stats8 + 8, 0u);
+    }
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }

@@ -20,6 +20,10 @@
 // is staged in shared memory; geometry, face index, cache records and emitter
 // words are read through the read-only path (they stay resident in the 126 MB
 // L2 for the configurations this targets).
+#include <cuda_fp16.h>
+
+#include <algorithm>
+
 #include "vgi_device.cuh"
 #include "vgi_types.cuh"
 
@@ -1054,6 +1058,333 @@ void launch_discover(const TraceArgs& a, const float* cam, uint32_t w, uint32_t 
                      int4* faces, uint32_t* count, uint32_t capacity, uint32_t* overflow, cudaStream_t s) {
     const uint32_t n = w * h;
     if (n) discover_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, cam, w, h, pixels, set, set_mask, faces, count, capacity, overflow);
+}
+
+// ---- far tier (voxel_view_pixels.wgsl:53-216) ------------------------------------
+// Per-pixel lighting for faces small on screen, without face identity: each
+// cell samples one of its pixels per frame, keeps a history reprojected by
+// world position and traces a path when that history is short or one frame
+// in `rate`. The raster depth and normal the shader reads become one primary
+// ray per cell through the NAADF geometry (as in discovery).
+namespace {
+
+__device__ __forceinline__ float comp(V3 v, uint32_t a) { return a == 0u ? v.x : (a == 1u ? v.y : v.z); }
+__device__ __forceinline__ void set_comp(V3& v, uint32_t a, float x) {
+    if (a == 0u) v.x = x;
+    else if (a == 1u) v.y = x;
+    else v.z = x;
+}
+
+// voxel_traversal.wgsl:74-80: a coarse page's block stride (header w bits 28-30).
+template <bool C>
+__device__ int voxel_stride(const TraceArgs& A, I3 voxel, Cnt<C>& cnt) {
+    const int rx = (int)floorf(__fdiv_rn((float)voxel.x, 16.0f)), ry = (int)floorf(__fdiv_rn((float)voxel.y, 16.0f)),
+              rz = (int)floorf(__fdiv_rn((float)voxel.z, 16.0f));
+    if (!in_bounds(A, rx, ry, rz)) return 1;
+    const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
+    if (index == kNoIndex) return 1;
+    return 1 << ((__ldg(A.headers + index).w >> 28u) & 7u);
+}
+
+// voxel_view_runtime.wgsl:26-30
+__device__ __forceinline__ bool in_interest(const FarView& F, I3 voxel) {
+    if (F.interest_min[3] == 0) return true;
+    const int rx = (int)floorf(__fdiv_rn((float)voxel.x, 16.0f)), ry = (int)floorf(__fdiv_rn((float)voxel.y, 16.0f)),
+              rz = (int)floorf(__fdiv_rn((float)voxel.z, 16.0f));
+    return rx >= F.interest_min[0] && ry >= F.interest_min[1] && rz >= F.interest_min[2] && rx <= F.interest_max[0] &&
+           ry <= F.interest_max[1] && rz <= F.interest_max[2];
+}
+
+// pixel_owned (voxel_view_pixels.wgsl:53-65), by distance from the camera.
+template <bool C>
+__device__ bool pixel_owned(const TraceArgs& A, const FarView& F, I3 voxel, uint32_t face, Cnt<C>& cnt) {
+    const uint32_t grid = F.grid[3];
+    if ((grid & 1u) == 0u || face >= 6u) return false;
+    const uint32_t mode = (grid >> 1u) & 3u;
+    const int s = mode == 2u ? voxel_stride(A, voxel, cnt) : 1;
+    const I3 block{voxel.x & -s, voxel.y & -s, voxel.z & -s};
+    const V3 ray = add_s(itof(block), __fmul_rn(0.5f, (float)s)) - V3{F.cam[0], F.cam[1], F.cam[2]};
+    if (dot3(ray, V3{F.axis[0], F.axis[1], F.axis[2]}) <= 0.0f) return false;
+    const float side = __fdiv_rn(__fmul_rn((float)s, F.axis[3]), len3(ray));
+    if (mode == 0u) return side < F.tune[0];
+    return __fmul_rn(__fmul_rn(side, side), fabsf(dot3(face_normal(face), normalize3(ray)))) < F.tune[0];
+}
+
+// f32 -> f16 bits, round to nearest even (pack2x16float's conversion).
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    return (uint32_t)__half_as_ushort(__float2half_rn(a)) | ((uint32_t)__half_as_ushort(__float2half_rn(b)) << 16u);
+}
+
+struct FarCell {
+    V3 mean;
+    float count;
+    V3 surface;
+    uint32_t face;
+    uint32_t sequence;
+};
+__device__ __forceinline__ FarCell load_cell(const uint4* cells, uint32_t i) {
+    const uint4 a = cells[i * 3u], b = cells[i * 3u + 1u], c = cells[i * 3u + 2u];
+    return FarCell{V3{__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z)}, __uint_as_float(a.w),
+                   V3{__uint_as_float(b.x), __uint_as_float(b.y), __uint_as_float(b.z)}, b.w, c.x};
+}
+__device__ __forceinline__ void store_cell(uint4* cells, uint32_t i, const FarCell& v) {
+    cells[i * 3u] = make_uint4(__float_as_uint(v.mean.x), __float_as_uint(v.mean.y), __float_as_uint(v.mean.z), __float_as_uint(v.count));
+    cells[i * 3u + 1u] = make_uint4(__float_as_uint(v.surface.x), __float_as_uint(v.surface.y), __float_as_uint(v.surface.z), v.face);
+    cells[i * 3u + 2u] = make_uint4(v.sequence, 0u, 0u, 0u);
+}
+
+// write_output (voxel_view_pixels.wgsl:76-81) with custom_direct (67-74).
+template <class T>
+__device__ void far_write(const FarView& F, T& tracer, uint4* output, uint32_t index, const FarCell& v) {
+    const uint32_t axis = (v.face & 7u) / 2u;
+    V3 shown = v.mean;
+    if (F.custom) {
+        V3 value, custom;
+        tracer.template direct_at<true>(v.surface, face_normal(v.face & 7u), value, custom);
+        shown = shown + custom;
+    }
+    output[4u + index] = make_uint4(pack2(shown.x, shown.y), pack2(shown.z, v.count), v.face, __float_as_uint(comp(v.surface, axis)));
+}
+
+// The camera's screen position of a world point: NDC x, y (the previous
+// clip matrix's projection), false behind the camera.
+__device__ bool project(const float* cam, uint32_t w, uint32_t h, V3 point, float& nx, float& ny) {
+    const V3 forward{cam[3], cam[4], cam[5]}, up{cam[6], cam[7], cam[8]};
+    const V3 right = normalize3(cross3(forward, up));
+    const V3 up2 = cross3(right, forward);
+    const V3 v = point - V3{cam[0], cam[1], cam[2]};
+    const float depth = dot3(v, forward);
+    if (depth <= 0.0f) return false;
+    const float scale = __fmul_rn(depth, cam[9]);
+    nx = __fdiv_rn(dot3(v, right), __fmul_rn(scale, __fdiv_rn((float)w, (float)h)));
+    ny = __fdiv_rn(dot3(v, up2), scale);
+    return true;
+}
+
+// previous_cell (voxel_view_pixels.wgsl:83-127).
+template <bool C>
+__device__ void previous_cell(const TraceArgs& A, const FarView& F, const uint4* previous, V3 surface, uint32_t face, I3 voxel, V3& mean,
+                              float& count, uint32_t& sequence, Cnt<C>& cnt) {
+    mean = V3{0.0f, 0.0f, 0.0f};
+    count = 0.0f;
+    sequence = 0u;
+    const uint32_t prev_stamp = __float_as_uint(F.tune[3]);
+    if (prev_stamp == 0xffffffffu) return;
+    float nx, ny;
+    if (!project(F.prev, F.width, F.height, surface, nx, ny)) return;
+    const uint32_t size = F.grid[2];
+    const V3 normal = face_normal(face);
+    const float ux = __fadd_rn(__fmul_rn(nx, 0.5f), 0.5f), uy = __fadd_rn(__fmul_rn(ny, -0.5f), 0.5f);
+    const float px = __fsub_rn(__fdiv_rn(__fmul_rn(ux, (float)F.width), (float)size), 0.5f);
+    const float py = __fsub_rn(__fdiv_rn(__fmul_rn(uy, (float)F.height), (float)size), 0.5f);
+    // Far off-screen points stay far off the grid (and convert safely).
+    const float flx = fminf(fmaxf(floorf(px), -1048576.0f), 1048576.0f), fly = fminf(fmaxf(floorf(py), -1048576.0f), 1048576.0f);
+    const int bx = (int)flx, by = (int)fly;
+    const float fx = __fsub_rn(px, flx), fy = __fsub_rn(py, fly);
+    const float reach = __fdiv_rn(__fmul_rn(__fmul_rn(2.0f, (float)size), len3(surface - V3{F.cam[0], F.cam[1], F.cam[2]})), F.axis[3]);
+    const float tolerance = __fadd_rn(__fmul_rn(4.0f, (float)voxel_stride(A, voxel, cnt)), 0.01f);
+    const uint32_t expected = face | ((prev_stamp & 0x1fffffffu) << 3u);
+    float weight = 0.0f, samples = 0.0f, best = 0.0f;
+    V3 sum{0.0f, 0.0f, 0.0f};
+    for (int y = 0; y <= 1; ++y) {
+        for (int x = 0; x <= 1; ++x) {
+            const int qx = bx + x, qy = by + y;
+            if (qx < 0 || qy < 0 || qx >= (int)F.grid[0] || qy >= (int)F.grid[1]) continue;
+            const FarCell old = load_cell(previous, (uint32_t)qy * F.grid[0] + (uint32_t)qx);
+            if (old.face != expected || old.count == 0.0f) continue;
+            const V3 delta = old.surface - surface;
+            if (fabsf(dot3(delta, normal)) > tolerance || dot3(delta, delta) > __fmul_rn(reach, reach)) continue;
+            const float w = __fadd_rn(__fmul_rn(x == 1 ? fx : __fsub_rn(1.0f, fx), y == 1 ? fy : __fsub_rn(1.0f, fy)), 1e-4f);
+            sum = sum + old.mean * w;
+            samples = __fadd_rn(samples, __fmul_rn(old.count, w));
+            weight = __fadd_rn(weight, w);
+            if (w > best) {
+                best = w;
+                sequence = old.sequence;
+            }
+        }
+    }
+    if (weight > 0.0f) {
+        mean = sum / weight;
+        count = __fdiv_rn(samples, weight);
+    }
+}
+
+// The handoff's receiver lookup: block_receiver (voxel_view_discovery.wgsl:
+// 26-35) then previous_owner (voxel_view_runtime.wgsl:110-120).
+template <bool C>
+__device__ uint32_t far_owner(const TraceArgs& A, const FarView& F, I3 voxel, uint32_t face, Cnt<C>& cnt) {
+    if (F.n_receivers == 0u || F.receiver_hash == nullptr) return kNoIndex;
+    const V3 normal = face_normal(face);
+    I3 key = voxel;
+    V3 surface = add_s(itof(voxel), 0.5f) + normal * 0.5f;
+    const int s = voxel_stride(A, voxel, cnt);
+    if (s != 1) {
+        key = I3{voxel.x & -s, voxel.y & -s, voxel.z & -s};
+        surface = itof(key) + add_s(normal * 0.5f, 0.5f) * (float)s;
+    }
+    uint32_t slot = (hash_voxel(key.x, key.y, key.z) ^ pcg(face + 1u)) & F.hash_mask;
+#pragma unroll 1
+    for (uint32_t step = 0; step < 64u; ++step) {
+        const uint32_t value = F.receiver_hash[slot];
+        if (value == 0u) return kNoIndex;
+        if (value <= F.n_receivers) {
+            const uint4 r0 = F.receivers[(value - 1u) * 2u], r1 = F.receivers[(value - 1u) * 2u + 1u];
+            if (r0.w == face && (int)r1.x == key.x && (int)r1.y == key.y && (int)r1.z == key.z && __uint_as_float(r0.x) == surface.x &&
+                __uint_as_float(r0.y) == surface.y && __uint_as_float(r0.z) == surface.z)
+                return value - 1u;
+        }
+        slot = (slot + 1u) & F.hash_mask;
+    }
+    return kNoIndex;
+}
+
+__device__ __forceinline__ void load_smat(const TraceArgs& A, float4* smat) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        float4 d = __ldg(A.materials + i * 4), e = __ldg(A.materials + i * 4 + 2), x = __ldg(A.materials + i * 4 + 3);
+        smat[i * 2] = make_float4(d.x, d.y, d.z, x.y);
+        smat[i * 2 + 1] = make_float4(e.x, e.y, e.z, 0.0f);
+    }
+    __syncthreads();
+}
+
+constexpr uint32_t kFarHits = 3u;  // DIFFUSE_HITS's default: the far pipelines do not override it
+
+// classify_pixels (voxel_view_pixels.wgsl:129-192).
+template <bool LIMITED>
+__global__ void __launch_bounds__(128) far_classify_kernel(const TraceArgs A, const FarView F, const uint4* __restrict__ previous,
+                                                           uint4* __restrict__ current, uint4* __restrict__ output, uint32_t* __restrict__ queue,
+                                                           uint32_t* __restrict__ stats) {
+    __shared__ float4 smat[512];
+    load_smat(A, smat);
+    Cnt<false> cnt;
+    Tracer<kFarHits, LIMITED, true, false> T{A, smat, cnt};
+    const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stamp = F.frame & 0x1fffffffu;
+    if (id == 0u) {
+        output[0] = make_uint4(__float_as_uint(F.cam[0]), __float_as_uint(F.cam[1]), __float_as_uint(F.cam[2]), 0u);
+        output[1] = make_uint4(__float_as_uint(F.axis[0]), __float_as_uint(F.axis[1]), __float_as_uint(F.axis[2]), __float_as_uint(F.axis[3]));
+        output[2] = make_uint4(F.grid[0], F.grid[1], F.grid[2], F.grid[3]);
+        output[3] = make_uint4(0u, 0u, __float_as_uint(F.tune[0]), stamp);
+    }
+    if (id >= F.grid[0] * F.grid[1]) return;
+    const uint32_t size = F.grid[2];
+    const uint32_t cx = id % F.grid[0], cy = id / F.grid[0];
+    // One pixel of the cell per frame, cycling through all of them.
+    const uint32_t k = (F.frame * 5u + (cx ^ cy)) % (size * size);
+    const uint32_t px = cx * size + k % size, py = cy * size + k / size;
+    if (px >= F.width || py >= F.height) return;
+    const V3 eye{F.cam[0], F.cam[1], F.cam[2]};
+    const V3 dir = pixel_ray(F.cam, px, py, F.width, F.height);
+    const Ray hit = trace_domain(A, eye, dir, A.max_distance, true, 2048u, cnt);
+    if (hit.status != 1u) return;  // nothing drawn at this pixel
+    V3 surface = hit.position;
+    if (((F.grid[3] >> 1u) & 3u) == 0u && F.axis[3] > __fmul_rn(__fmul_rn(1.05f, F.tune[0]), len3(surface - eye))) return;
+    const uint32_t face = face_index_of(hit.normal);
+    if (face >= 6u) return;
+    const V3 normal = face_normal(face);
+    set_comp(surface, face / 2u, rintf(comp(surface, face / 2u)));
+    const V3 inner = surface - normal * 0.01f;
+    const I3 voxel{(int)floorf(inner.x), (int)floorf(inner.y), (int)floorf(inner.z)};
+    if (!in_interest(F, voxel) || !pixel_owned(A, F, voxel, face, cnt)) return;
+    atomicAdd(stats + kFarOwned, 1u);
+    V3 mean;
+    float count;
+    uint32_t sequence;
+    previous_cell(A, F, previous, surface, face, voxel, mean, count, sequence, cnt);
+    if (count > 0.0f) {
+        atomicAdd(stats + kFarReprojected, 1u);
+    } else {
+        // Handoff: a face entering the far band starts from its view receiver's history.
+        const uint32_t owner = far_owner(A, F, voxel, face, cnt);
+        if (owner != kNoIndex && __uint_as_float(F.estimates[owner * 4u].w) > 0.0f) {
+            const uint4 e = F.estimates[owner * 4u];
+            mean = V3{__uint_as_float(e.x), __uint_as_float(e.y), __uint_as_float(e.z)};
+            count = __uint_as_float(e.w);
+            sequence = F.estimates[owner * 4u + 3u].x;
+            atomicAdd(stats + kFarSeeded, 1u);
+        }
+    }
+    const float capped = wmin(count, F.tune[1]);
+    atomicAdd(stats + kFarHistory, (uint32_t)capped);
+    const FarCell value{mean, capped, surface, face | (stamp << 3u), sequence};
+    store_cell(current, id, value);
+    const uint32_t rate = max((uint32_t)F.tune[2], 1u);
+    if (capped < 4.0f || (id + F.frame) % rate == 0u) {
+        const uint32_t slot = atomicAdd(queue, 1u);
+        queue[1u + slot] = id;
+    } else {
+        far_write(F, T, output, id, value);
+    }
+}
+
+// trace_pixel_queue (voxel_view_pixels.wgsl:199-216), grid-stride over the
+// dense queue.
+template <bool LIMITED>
+__global__ void __launch_bounds__(128) far_trace_kernel(const TraceArgs A, const FarView F, const uint32_t* __restrict__ queue,
+                                                        uint4* __restrict__ current, uint4* __restrict__ output, uint32_t* __restrict__ stats) {
+    __shared__ float4 smat[512];
+    load_smat(A, smat);
+    Cnt<false> cnt;
+    Tracer<kFarHits, LIMITED, true, false> T{A, smat, cnt};
+    const uint32_t n = queue[0];
+#pragma unroll 1
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t index = queue[1u + i];
+        FarCell cell = load_cell(current, index);
+        atomicAdd(stats + kFarTraced, 1u);
+        const uint32_t stream = pcg(index * 9781u + 0x9e3779b9u);
+        const V3 normal = face_normal(cell.face & 7u);
+        // trace_receiver (voxel_path.wgsl:504-520)
+        const V3 direction = hemisphere(normal, sample_1d(stream, cell.sequence, 0u), sample_1d(stream, cell.sequence, 1u));
+        V3 value = T.sample_emitter(cell.surface, normal, stream, cell.sequence, 0u);
+        bool unknown = false;
+        if (dot3(normal, direction) > 0.0f) value = value + T.trace_path(cell.surface + normal * 0.001f, direction, normal, stream, cell.sequence, unknown);
+        cell.sequence += 1u;
+        if (!unknown) {
+            cell.count = wmin(__fadd_rn(cell.count, 1.0f), F.tune[1]);
+            const float t = __fdiv_rn(1.0f, cell.count);
+            cell.mean = cell.mean * __fsub_rn(1.0f, t) + value * t;
+        }
+        store_cell(current, index, cell);
+        far_write(F, T, output, index, cell);
+    }
+}
+
+// The view receivers' owner hash (receiver_hash, voxel_view_runtime.wgsl:
+// 96-98): receiver + 1 per slot, linear probing.
+__global__ void receiver_hash_kernel(const uint4* receivers, uint32_t n, uint32_t* hash, uint32_t mask) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4 r0 = receivers[i * 2u], r1 = receivers[i * 2u + 1u];
+    uint32_t slot = (hash_voxel((int)r1.x, (int)r1.y, (int)r1.z) ^ pcg(r0.w + 1u)) & mask;
+#pragma unroll 1
+    for (uint32_t step = 0; step <= mask; ++step) {
+        if (atomicCAS(hash + slot, 0u, i + 1u) == 0u) return;
+        slot = (slot + 1u) & mask;
+    }
+}
+
+}  // namespace
+
+void launch_far(const TraceArgs& a, const FarView& f, const uint4* previous, uint4* current, uint4* output, uint32_t* queue, uint32_t* stats,
+                bool limited, cudaStream_t s) {
+    const uint32_t cells = f.grid[0] * f.grid[1];
+    if (cells == 0) return;
+    const uint32_t blocks = (cells + 127) / 128;
+    // The trace pass strides over at most `cells` queued cells.
+    const uint32_t trace_blocks = std::min<uint32_t>(blocks, 148u * 8u);
+    if (limited) {
+        far_classify_kernel<true><<<blocks, 128, 0, s>>>(a, f, previous, current, output, queue, stats);
+        far_trace_kernel<true><<<trace_blocks, 128, 0, s>>>(a, f, queue, current, output, stats);
+    } else {
+        far_classify_kernel<false><<<blocks, 128, 0, s>>>(a, f, previous, current, output, queue, stats);
+        far_trace_kernel<false><<<trace_blocks, 128, 0, s>>>(a, f, queue, current, output, stats);
+    }
+}
+
+void launch_receiver_hash(const uint4* receivers, uint32_t n, uint32_t* hash, uint32_t mask, cudaStream_t s) {
+    if (n) receiver_hash_kernel<<<(n + 127) / 128, 128, 0, s>>>(receivers, n, hash, mask);
 }
 
 void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uint32_t threads, uint32_t n_directional, uint32_t* sums,

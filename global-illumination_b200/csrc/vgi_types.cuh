@@ -161,6 +161,32 @@ void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uin
 // tan(half vertical fov); set = 64-bit keys, all ones when empty.
 void launch_discover(const TraceArgs& a, const float* cam, uint32_t w, uint32_t h, uint4* pixels, unsigned long long* set, uint32_t set_mask,
                      int4* faces, uint32_t* count, uint32_t capacity, uint32_t* overflow, cudaStream_t s);
+// Far tier (vgi_trace.cu, voxel_view_pixels.wgsl): the view uniforms the
+// classify and trace passes read, with the camera in place of the clip
+// matrices. Cells are 3 uint4 (PixelHistory: mean rgb + count, surface xyz +
+// face word, sequence); the output is a 4-uint4 header then one uint4 per
+// cell; the queue is a count then cell indices; 8 statistics words.
+struct FarView {
+    float cam[10];            // eye xyz, forward xyz (unit), up xyz, tan(half vertical fov)
+    float prev[10];           // the previous frame's camera
+    uint32_t width, height;   // viewport (origin 0, 0)
+    uint32_t grid[4];         // cells x, y, pixels per cell side, enabled | measure << 1
+    float tune[4];            // threshold px, max history, trace rate, previous stamp (bits; all ones: none)
+    float axis[4];            // forward xyz, pixels per unit at depth 1
+    int32_t interest_min[4];  // regions, inclusive; w: bounded
+    int32_t interest_max[4];
+    uint32_t frame;           // this frame's number (history.z)
+    uint32_t custom;          // some light has custom visible RGB (transport.y)
+    const uint4* receivers;   // view receivers for the handoff (2 uint4 each), may be null
+    const uint4* estimates;   // their estimates (4 uint4 each)
+    const uint32_t* receiver_hash;  // receiver + 1 per slot, 0 empty
+    uint32_t hash_mask;
+    uint32_t n_receivers;
+};
+constexpr uint32_t kFarOwned = 0, kFarTraced = 1, kFarHistory = 2, kFarReprojected = 3, kFarSeeded = 4;
+void launch_far(const TraceArgs& a, const FarView& f, const uint4* previous, uint4* current, uint4* output, uint32_t* queue, uint32_t* stats,
+                bool limited, cudaStream_t s);
+void launch_receiver_hash(const uint4* receivers, uint32_t n, uint32_t* hash, uint32_t mask, cudaStream_t s);
 // MLP radiance cache (vgi_mlp.cu).
 cudaError_t mlp_set_attributes();
 void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,

@@ -50,6 +50,33 @@ class Camera(ctypes.Structure):
                 ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
 
 
+class FarSettingsStruct(ctypes.Structure):
+    """vgi_far_settings."""
+    _fields_ = [("voxel_pixels", ctypes.c_float), ("measure", ctypes.c_uint32), ("cell", ctypes.c_uint32), ("history", ctypes.c_float),
+                ("rate", ctypes.c_uint32), ("steps", ctypes.c_uint32), ("interest_min", ctypes.c_int32 * 3),
+                ("interest_max", ctypes.c_int32 * 3), ("bounded", ctypes.c_uint32)]
+
+
+@dataclasses.dataclass
+class FarTierSettings:
+    """FarTierSettings (src/settings.rs:95-137) with its defaults; measure
+    0 = voxel side, 1 = voxel area, 2 = block area; interest = (min, max)
+    region coordinates or None."""
+
+    voxel_pixels: float = 8.0
+    measure: int = 0
+    cell: int = 0
+    history: float = 32.0
+    rate: int = 4
+    steps: int = 128
+    interest: Optional[tuple] = None
+
+    def struct(self) -> FarSettingsStruct:
+        lo, hi = self.interest if self.interest is not None else ((0, 0, 0), (0, 0, 0))
+        return FarSettingsStruct(self.voxel_pixels, self.measure, self.cell, self.history, self.rate, self.steps,
+                                 (ctypes.c_int32 * 3)(*lo), (ctypes.c_int32 * 3)(*hi), 1 if self.interest is not None else 0)
+
+
 class Schedule(ctypes.Structure):
     """vgi_schedule."""
     _fields_ = [("focus", ctypes.c_int32 * 3), ("budget", ctypes.c_uint32), ("classify_first", ctypes.c_uint32),
@@ -199,6 +226,9 @@ _SIGNATURES = {
     "vgi_submit_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P, _P]),
     "vgi_frame_scheduled": (_INT, [_P, _U32, _U32, _P]),
     "vgi_discover_faces": (_INT, [_P, _P, _P, _P, _U32, _P]),
+    "vgi_far_frame": (_INT, [_P, _P, _P, _U32]),
+    "vgi_far_read": (_INT, [_P, _P, _P, _P, _P]),
+    "vgi_far_reset": (_INT, [_P]),
     "vgi_apply_events_footprints": (_INT, [_P, _P, _U32, _U64, _P, _U32, _P, _U32]),
     "vgi_read_selection": (_INT, [_P, _P, _P, _P, _P, _P]),
     "vgi_complete_batch": (_INT, [_P, _U64]),
@@ -313,6 +343,25 @@ class DirectionalTransportLight:
         out = np.zeros(12, np.float32)
         library().vgi_directional_light_record(_ptr(_c(self.direction, np.float32)), _ptr(_c(self.radiance, np.float32)),
                                                _ptr(_c(self.custom_visible, np.float32)), _ptr(out))
+        return out
+
+
+@dataclasses.dataclass
+class PointTransportLight:
+    """A point source (src/gpu.rs:745-753): position and range, intensity,
+    custom visible RGB in extra.yzw."""
+
+    position: Sequence[float]
+    intensity: Sequence[float]
+    range: float
+    custom_visible: Sequence[float] = (0.0, 0.0, 0.0)
+
+    def words(self) -> np.ndarray:
+        out = np.zeros(12, np.float32)
+        out[0:3] = self.position
+        out[3] = self.range
+        out[4:7] = self.intensity
+        out[9:12] = self.custom_visible
         return out
 
 
@@ -623,6 +672,30 @@ class GpuTracer:
         n = ctypes.c_uint32()
         self._check(self._lib.vgi_discover_faces(self._h, ctypes.byref(cam), _ptr(pixels), _ptr(faces), capacity, ctypes.byref(n)))
         return pixels, faces[: n.value].copy()
+
+    # far tier
+    def far_frame(self, eye, forward, up, tan_half_fov: float, width: int, height: int, settings: Optional["FarTierSettings"] = None,
+                  frame: int = 0) -> None:
+        """One far-tier frame (classify, then trace the queue) for a camera;
+        `forward` must be unit length."""
+        cam = Camera((ctypes.c_float * 3)(*map(float, eye)), (ctypes.c_float * 3)(*map(float, forward)),
+                     (ctypes.c_float * 3)(*map(float, up)), float(tan_half_fov), width, height)
+        st = (settings or FarTierSettings()).struct()
+        self._check(self._lib.vgi_far_frame(self._h, ctypes.byref(cam), ctypes.byref(st), frame & 0xFFFFFFFF))
+
+    def far_reset(self) -> None:
+        self._check(self._lib.vgi_far_reset(self._h))
+
+    def far_read(self):
+        """(shape (4,), output (16 + 4 cells,), cells (n, 12), stats (8,)) u32 words."""
+        shape = np.zeros(4, np.uint32)
+        self._check(self._lib.vgi_far_read(self._h, _ptr(shape), None, None, None))
+        n = int(shape[0]) * int(shape[1])
+        output = np.zeros(16 + 4 * n, np.uint32)
+        cells = np.zeros((n, 12), np.uint32)
+        stats = np.zeros(8, np.uint32)
+        self._check(self._lib.vgi_far_read(self._h, None, _ptr(output), _ptr(cells), _ptr(stats)))
+        return shape, output, cells, stats
 
     # scheduled frames
     def frame_scheduled(self, samples: int, clock_ms: int, budget: int, focus=(0, 0, 0), classify=None, audit_ms: int = 1000) -> None:

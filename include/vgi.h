@@ -349,6 +349,47 @@ typedef struct vgi_camera {
 } vgi_camera;
 int vgi_discover_faces(vgi_ctx* ctx, const vgi_camera* camera, uint32_t* pixels8, vgi_face* faces, uint32_t capacity, uint32_t* n_faces);
 
+/* ---- far tier ---------------------------------------------------------------------
+ * Per-pixel lighting for faces small on screen (FarTierSettings,
+ * shaders/voxel_view_pixels.wgsl), headless: each cell of `cell` x `cell`
+ * pixels traces one primary ray per frame through the NAADF geometry at one
+ * of its pixels (a different one each frame) in place of the raster depth
+ * and normal. A hit face far enough to be "small" (measure 0: a voxel's side
+ * in pixels under voxel_pixels; 1: its covered area; 2: the same for its LoD
+ * block) owns the cell: its history is reprojected from the previous
+ * frame's cells through the previous camera, or handed over from the view
+ * receiver of the same face, and a path is traced (trace_receiver with 3
+ * hits, `steps` traversal steps, budgeted rays) while the history is under 4
+ * samples or one frame in `rate`. Frames numbered more than one apart, or a
+ * changed viewport, start without history. Settings are normalized as the
+ * reference does (voxel_pixels 0..4096, 0 disables; history 1..1024; rate
+ * 1..8; steps 16..2048; cell 0..4, 0: round(height / 480) in 1..4).
+ * Asynchronous on the context's stream; vgi_far_read waits. */
+typedef struct vgi_far_settings {
+    float voxel_pixels;
+    uint32_t measure;
+    uint32_t cell;
+    float history;
+    uint32_t rate;
+    uint32_t steps;
+    int32_t interest_min[3]; /* regions, inclusive, when `bounded` */
+    int32_t interest_max[3];
+    uint32_t bounded;
+} vgi_far_settings;
+int vgi_far_frame(vgi_ctx* ctx, const vgi_camera* camera, const vgi_far_settings* settings, uint32_t frame);
+/* Drop the far tier's history (a camera cut): cell histories and output
+ * cells are zeroed and the next frame reprojects nothing. */
+int vgi_far_reset(vgi_ctx* ctx);
+/* shape4 = (cells x, cells y, pixels per cell side, enabled | measure << 1);
+ * output = PixelOutput: 16 header words (camera xyz 0, view forward + pixels
+ * per unit at depth 1, shape, 0 0 threshold-bits stamp), then per cell
+ * pack2x16float(rg), pack2x16float(b, count), face | stamp << 3, surface
+ * coordinate on the face's axis (bits); only owned cells are written each
+ * frame. cells12 = PixelHistory per cell (mean rgb, count, surface xyz, face
+ * word, sequence, 0, 0, 0). stats8 = owned, traced, history, reprojected,
+ * seeded, 0, 0, 0. Any pointer may be null. */
+int vgi_far_read(vgi_ctx* ctx, uint32_t* shape4, uint32_t* output, uint32_t* cells12, uint32_t* stats8);
+
 /* ---- scheduled frames: the GPU world-cache scheduler --------------------------
  * The reference's GPU selection of bulk work (shaders/voxel_accumulate.wgsl:
  * 448-695: candidate, select_classify, select_histogram, select_threshold,

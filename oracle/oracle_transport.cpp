@@ -1294,6 +1294,22 @@ int orc_footprints(const int32_t* directory, uint64_t slots, const uint32_t* hea
     return 0;
 }
 
+// A pinhole camera's ray through pixel (px, py): cam = eye xyz, forward xyz
+// (unit), up xyz, tan(half vertical fov).
+static f3 camera_ray(const float* cam, uint32_t px, uint32_t py, uint32_t w, uint32_t h) {
+    const f3 forward{cam[3], cam[4], cam[5]}, up{cam[6], cam[7], cam[8]};
+    const f3 rc = cross(forward, up);
+    const float rl = std::sqrt(dot(rc, rc));
+    const f3 right{rc.x / rl, rc.y / rl, rc.z / rl};
+    const f3 up2 = cross(right, forward);
+    const float fw = (float)w, fh = (float)h;
+    const float sx = ((2.0f * ((float)px + 0.5f)) / fw - 1.0f) * cam[9] * (fw / fh);
+    const float sy = (1.0f - (2.0f * ((float)py + 0.5f)) / fh) * cam[9];
+    const f3 raw = add(add(forward, muls(right, sx)), muls(up2, sy));
+    const float len = std::sqrt(dot(raw, raw));
+    return f3{raw.x / len, raw.y / len, raw.z / len};
+}
+
 // Headless discovery's per-pixel first hits (the GPU's discover kernel):
 // cam = eye xyz, forward xyz (unit), up xyz, tan(half vertical fov);
 // pixels = 8 words per pixel (voxel xyz, face or 6, material, status,
@@ -1302,12 +1318,7 @@ int orc_discover(const int32_t* directory, uint64_t slots, const uint32_t* heade
                  const float* cam, uint32_t w, uint32_t h, uint32_t* pixels, int threads) {
     Geometry g = make_geometry(directory, slots, headers, cells, params);
     Model m{params, nullptr, nullptr, nullptr, nullptr, nullptr, orc_pipeline{1, 0, 2048, 0, 1}};
-    const f3 eye{cam[0], cam[1], cam[2]}, forward{cam[3], cam[4], cam[5]}, up{cam[6], cam[7], cam[8]};
-    const f3 rc = cross(forward, up);
-    const float rl = std::sqrt(dot(rc, rc));
-    const f3 right{rc.x / rl, rc.y / rl, rc.z / rl};
-    const f3 up2 = cross(right, forward);
-    const float fw = (float)w, fh = (float)h;
+    const f3 eye{cam[0], cam[1], cam[2]};
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     std::atomic<uint32_t> next{0};
     auto worker = [&]() {
@@ -1315,12 +1326,7 @@ int orc_discover(const int32_t* directory, uint64_t slots, const uint32_t* heade
         for (;;) {
             const uint32_t id = next.fetch_add(1);
             if (id >= w * h) break;
-            const uint32_t px = id % w, py = id / w;
-            const float sx = ((2.0f * ((float)px + 0.5f)) / fw - 1.0f) * cam[9] * (fw / fh);
-            const float sy = (1.0f - (2.0f * ((float)py + 0.5f)) / fh) * cam[9];
-            const f3 raw = add(add(forward, muls(right, sx)), muls(up2, sy));
-            const float len = std::sqrt(dot(raw, raw));
-            const f3 dir{raw.x / len, raw.y / len, raw.z / len};
+            const f3 dir = camera_ray(cam, id % w, id / w, w, h);
             const RayResult r = trace_domain_limited(x, eye, dir, params[17], true, 2048u);
             const uint32_t face = r.status == 1u ? face_index_of(r.normal) : 6u;
             const f3 gap = sub(r.position, eye);
@@ -1334,6 +1340,288 @@ int orc_discover(const int32_t* directory, uint64_t slots, const uint32_t* heade
     for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
     worker();
     for (auto& t : pool) t.join();
+    return 0;
+}
+
+// ---- far tier (voxel_view_pixels.wgsl:53-216), headless ---------------------------
+// view = 44 words: camera (10), previous camera (10), width, height, grid
+// (cells x, y, pixels per side, enabled | measure << 1), tune (threshold px,
+// max history, rate, previous stamp bits), axis (forward xyz, pixels per unit
+// at depth 1), interest min (4, w bounded), interest max (4), frame, custom.
+namespace far {
+struct View {
+    const uint32_t* w;
+    const float* cam() const { return reinterpret_cast<const float*>(w); }
+    const float* prev() const { return reinterpret_cast<const float*>(w + 10); }
+    uint32_t width() const { return w[20]; }
+    uint32_t height() const { return w[21]; }
+    uint32_t grid(int i) const { return w[22 + i]; }
+    float tune(int i) const { return bitsf(w[26 + i]); }
+    float axis(int i) const { return bitsf(w[30 + i]); }
+    int32_t imin(int i) const { return (int32_t)w[34 + i]; }
+    int32_t imax(int i) const { return (int32_t)w[38 + i]; }
+    uint32_t frame() const { return w[42]; }
+    bool custom() const { return w[43] != 0u; }
+    f3 eye() const { return f3{cam()[0], cam()[1], cam()[2]}; }
+};
+
+static float comp(f3 v, uint32_t a) { return a == 0u ? v.x : (a == 1u ? v.y : v.z); }
+static void set_comp(f3& v, uint32_t a, float x) { (a == 0u ? v.x : (a == 1u ? v.y : v.z)) = x; }
+static i3 region_of(i3 v) {
+    return i3{(int32_t)std::floor((float)v.x / 16.0f), (int32_t)std::floor((float)v.y / 16.0f), (int32_t)std::floor((float)v.z / 16.0f)};
+}
+
+// voxel_traversal.wgsl:74-80
+static int32_t voxel_stride(Ctx& x, i3 voxel) {
+    const i3 r = region_of(voxel);
+    if (!in_bounds(x, r)) return 1;
+    const uint32_t index = lookup_region(x, r);
+    if (index == 0xffffffffu) return 1;
+    return 1 << ((x.g.headers[(size_t)index * 4 + 3] >> 28u) & 7u);
+}
+
+// voxel_view_runtime.wgsl:26-30
+static bool in_interest(const View& v, i3 voxel) {
+    if (v.imin(3) == 0) return true;
+    const i3 r = region_of(voxel);
+    return r.x >= v.imin(0) && r.y >= v.imin(1) && r.z >= v.imin(2) && r.x <= v.imax(0) && r.y <= v.imax(1) && r.z <= v.imax(2);
+}
+
+// voxel_view_pixels.wgsl:53-65
+static bool pixel_owned(Ctx& x, const View& v, i3 voxel, uint32_t face) {
+    const uint32_t grid = v.grid(3);
+    if ((grid & 1u) == 0u || face >= 6u) return false;
+    const uint32_t mode = (grid >> 1u) & 3u;
+    const int32_t s = mode == 2u ? voxel_stride(x, voxel) : 1;
+    const f3 block{(float)(voxel.x & -s), (float)(voxel.y & -s), (float)(voxel.z & -s)};
+    const f3 ray = sub(adds(block, 0.5f * (float)s), v.eye());
+    if (dot(ray, f3{v.axis(0), v.axis(1), v.axis(2)}) <= 0.0f) return false;
+    const float side = ((float)s * v.axis(3)) / length(ray);
+    if (mode == 0u) return side < v.tune(0);
+    return (side * side) * std::fabs(dot(face_normal(face), normalize(ray))) < v.tune(0);
+}
+
+// f32 -> f16 bits, IEEE round to nearest even (pack2x16float's conversion).
+static uint32_t half_bits(float f) {
+    const uint32_t u = fbits(f);
+    const uint32_t sign = (u >> 16) & 0x8000u;
+    const uint32_t a = u & 0x7fffffffu;
+    if (a >= 0x7f800000u) return sign | (a > 0x7f800000u ? 0x7fffu : 0x7c00u);
+    if (a >= 0x477ff000u) return sign | 0x7c00u;  // at or past 65520: rounds to infinity
+    if (a < 0x38800000u) {                         // under 2^-14: a subnormal half, exact scaling by 2^24
+        return sign | (uint32_t)std::nearbyint(bitsf(a) * 16777216.0f);
+    }
+    uint32_t h = (((a >> 23) - 112u) << 10) | ((a & 0x7fffffu) >> 13);
+    const uint32_t rest = a & 0x1fffu;
+    if (rest > 0x1000u || (rest == 0x1000u && (h & 1u))) h += 1u;
+    return sign | h;
+}
+static uint32_t pack2(float a, float b) { return half_bits(a) | (half_bits(b) << 16); }
+
+struct Cell { f3 mean; float count; f3 surface; uint32_t face; uint32_t sequence; };
+static Cell load(const uint32_t* cells, uint32_t i) {
+    const uint32_t* c = cells + (size_t)i * 12;
+    return Cell{f3{bitsf(c[0]), bitsf(c[1]), bitsf(c[2])}, bitsf(c[3]), f3{bitsf(c[4]), bitsf(c[5]), bitsf(c[6])}, c[7], c[8]};
+}
+static void store(uint32_t* cells, uint32_t i, const Cell& v) {
+    uint32_t* c = cells + (size_t)i * 12;
+    c[0] = fbits(v.mean.x); c[1] = fbits(v.mean.y); c[2] = fbits(v.mean.z); c[3] = fbits(v.count);
+    c[4] = fbits(v.surface.x); c[5] = fbits(v.surface.y); c[6] = fbits(v.surface.z); c[7] = v.face;
+    c[8] = v.sequence; c[9] = 0; c[10] = 0; c[11] = 0;
+}
+
+// write_output + custom_direct (voxel_view_pixels.wgsl:67-81)
+static void write_output(Ctx& x, const View& v, uint32_t* output, uint32_t index, const Cell& cell) {
+    const uint32_t axis = (cell.face & 7u) / 2u;
+    f3 shown = cell.mean;
+    if (v.custom()) shown = add(shown, direct_at(x, cell.surface, face_normal(cell.face & 7u)).custom);
+    uint32_t* o = output + 16 + (size_t)index * 4;
+    o[0] = pack2(shown.x, shown.y);
+    o[1] = pack2(shown.z, cell.count);
+    o[2] = cell.face;
+    o[3] = fbits(comp(cell.surface, axis));
+}
+
+// The previous camera's NDC of a world point; false behind it.
+static bool project(const float* cam, uint32_t w, uint32_t h, f3 point, float& nx, float& ny) {
+    const f3 forward{cam[3], cam[4], cam[5]}, up{cam[6], cam[7], cam[8]};
+    const f3 right = normalize(cross(forward, up));
+    const f3 up2 = cross(right, forward);
+    const f3 d = sub(point, f3{cam[0], cam[1], cam[2]});
+    const float depth = dot(d, forward);
+    if (depth <= 0.0f) return false;
+    const float scale = depth * cam[9];
+    nx = dot(d, right) / (scale * ((float)w / (float)h));
+    ny = dot(d, up2) / scale;
+    return true;
+}
+
+// previous_cell (voxel_view_pixels.wgsl:83-127)
+static void previous_cell(Ctx& x, const View& v, const uint32_t* previous, f3 surface, uint32_t face, i3 voxel, f3& mean, float& count,
+                          uint32_t& sequence) {
+    mean = f3{0, 0, 0};
+    count = 0.0f;
+    sequence = 0;
+    const uint32_t prev_stamp = fbits(v.tune(3));
+    if (prev_stamp == 0xffffffffu) return;
+    float nx, ny;
+    if (!project(v.prev(), v.width(), v.height(), surface, nx, ny)) return;
+    const uint32_t size = v.grid(2);
+    const f3 normal = face_normal(face);
+    const float ux = nx * 0.5f + 0.5f, uy = ny * -0.5f + 0.5f;
+    const float px = (ux * (float)v.width()) / (float)size - 0.5f;
+    const float py = (uy * (float)v.height()) / (float)size - 0.5f;
+    const float flx = std::fmin(std::fmax(std::floor(px), -1048576.0f), 1048576.0f);
+    const float fly = std::fmin(std::fmax(std::floor(py), -1048576.0f), 1048576.0f);
+    const int32_t bx = (int32_t)flx, by = (int32_t)fly;
+    const float fx = px - flx, fy = py - fly;
+    const float reach = ((2.0f * (float)size) * length(sub(surface, v.eye()))) / v.axis(3);
+    const float tolerance = 4.0f * (float)voxel_stride(x, voxel) + 0.01f;
+    const uint32_t expected = face | ((prev_stamp & 0x1fffffffu) << 3u);
+    float weight = 0.0f, samples = 0.0f, best = 0.0f;
+    f3 sum{0, 0, 0};
+    for (int32_t yy = 0; yy <= 1; ++yy) {
+        for (int32_t xx = 0; xx <= 1; ++xx) {
+            const int32_t qx = bx + xx, qy = by + yy;
+            if (qx < 0 || qy < 0 || qx >= (int32_t)v.grid(0) || qy >= (int32_t)v.grid(1)) continue;
+            const Cell old = load(previous, (uint32_t)qy * v.grid(0) + (uint32_t)qx);
+            if (old.face != expected || old.count == 0.0f) continue;
+            const f3 delta = sub(old.surface, surface);
+            if (std::fabs(dot(delta, normal)) > tolerance || dot(delta, delta) > reach * reach) continue;
+            const float wgt = (xx == 1 ? fx : 1.0f - fx) * (yy == 1 ? fy : 1.0f - fy) + 1e-4f;
+            sum = add(sum, muls(old.mean, wgt));
+            samples = samples + old.count * wgt;
+            weight = weight + wgt;
+            if (wgt > best) {
+                best = wgt;
+                sequence = old.sequence;
+            }
+        }
+    }
+    if (weight > 0.0f) {
+        mean = divs(sum, weight);
+        count = samples / weight;
+    }
+}
+
+// block_receiver then the receiver of the same key (the view receivers are
+// unique faces, so a scan finds what the owner hash finds).
+static uint32_t owner(Ctx& x, i3 voxel, uint32_t face, const uint32_t* receivers, uint32_t n) {
+    const f3 normal = face_normal(face);
+    i3 key = voxel;
+    f3 surface = add(adds(f3{(float)voxel.x, (float)voxel.y, (float)voxel.z}, 0.5f), muls(normal, 0.5f));
+    const int32_t s = n ? voxel_stride(x, voxel) : 1;
+    if (s != 1) {
+        key = i3{voxel.x & -s, voxel.y & -s, voxel.z & -s};
+        surface = add(f3{(float)key.x, (float)key.y, (float)key.z}, muls(adds(muls(normal, 0.5f), 0.5f), (float)s));
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t* r = receivers + (size_t)i * 8;
+        if (r[3] == face && (int32_t)r[4] == key.x && (int32_t)r[5] == key.y && (int32_t)r[6] == key.z && bitsf(r[0]) == surface.x &&
+            bitsf(r[1]) == surface.y && bitsf(r[2]) == surface.z)
+            return i;
+    }
+    return 0xffffffffu;
+}
+}  // namespace far
+
+int orc_far_frame(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
+                  const float* materials, const float* lights, const uint32_t* emitters, const uint32_t* state, const uint32_t* index,
+                  const orc_pipeline* pipe, const uint32_t* view_words, const uint32_t* receivers, const uint32_t* estimates,
+                  uint32_t n_receivers, const uint32_t* previous, uint32_t* current, uint32_t* output, uint32_t* stats, int threads) {
+    using namespace far;
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, materials, lights, emitters, state, index, *pipe};
+    const View v{view_words};
+    const uint32_t stamp = v.frame() & 0x1fffffffu;
+    const float* cam = v.cam();
+    output[0] = fbits(cam[0]); output[1] = fbits(cam[1]); output[2] = fbits(cam[2]); output[3] = 0;
+    for (int i = 0; i < 4; ++i) {
+        output[4 + i] = fbits(v.axis(i));
+        output[8 + i] = v.grid(i);
+    }
+    output[12] = 0; output[13] = 0; output[14] = fbits(v.tune(0)); output[15] = stamp;
+    const uint32_t n_cells = v.grid(0) * v.grid(1);
+    std::vector<uint8_t> queued(n_cells, 0);
+    std::atomic<uint32_t> st[8];
+    for (auto& a : st) a = 0;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    auto run = [&](auto&& body) {
+        std::atomic<uint32_t> next{0};
+        auto worker = [&]() {
+            Ctx x{g, m, Counters{}};
+            for (;;) {
+                const uint32_t id = next.fetch_add(1);
+                if (id >= n_cells) break;
+                body(x, id);
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+        worker();
+        for (auto& t : pool) t.join();
+    };
+    // classify_pixels (voxel_view_pixels.wgsl:129-192)
+    run([&](Ctx& x, uint32_t id) {
+        const uint32_t size = v.grid(2);
+        const uint32_t cx = id % v.grid(0), cy = id / v.grid(0);
+        const uint32_t k = (v.frame() * 5u + (cx ^ cy)) % (size * size);
+        const uint32_t px = cx * size + k % size, py = cy * size + k / size;
+        if (px >= v.width() || py >= v.height()) return;
+        const f3 eye = v.eye();
+        const RayResult hit = trace_domain_limited(x, eye, camera_ray(cam, px, py, v.width(), v.height()), x.extra(1), true, 2048u);
+        if (hit.status != 1u) return;
+        f3 surface = hit.position;
+        if (((v.grid(3) >> 1u) & 3u) == 0u && v.axis(3) > (1.05f * v.tune(0)) * length(sub(surface, eye))) return;
+        const uint32_t face = face_index_of(hit.normal);
+        if (face >= 6u) return;
+        const f3 normal = face_normal(face);
+        set_comp(surface, face / 2u, std::nearbyint(comp(surface, face / 2u)));
+        const f3 inner = sub(surface, muls(normal, 0.01f));
+        const i3 voxel{(int32_t)std::floor(inner.x), (int32_t)std::floor(inner.y), (int32_t)std::floor(inner.z)};
+        if (!in_interest(v, voxel) || !pixel_owned(x, v, voxel, face)) return;
+        st[0] += 1;
+        f3 mean;
+        float count;
+        uint32_t sequence;
+        previous_cell(x, v, previous, surface, face, voxel, mean, count, sequence);
+        if (count > 0.0f) {
+            st[3] += 1;
+        } else {
+            const uint32_t o = owner(x, voxel, face, receivers, n_receivers);
+            if (o != 0xffffffffu && bitsf(estimates[(size_t)o * 16 + 3]) > 0.0f) {
+                const uint32_t* e = estimates + (size_t)o * 16;
+                mean = f3{bitsf(e[0]), bitsf(e[1]), bitsf(e[2])};
+                count = bitsf(e[3]);
+                sequence = e[12];
+                st[4] += 1;
+            }
+        }
+        const float capped = wmin(count, v.tune(1));
+        st[2] += (uint32_t)capped;
+        const Cell value{mean, capped, surface, face | (stamp << 3u), sequence};
+        store(current, id, value);
+        const uint32_t rate = std::max((uint32_t)v.tune(2), 1u);
+        if (capped < 4.0f || (id + v.frame()) % rate == 0u) queued[id] = 1;
+        else write_output(x, v, output, id, value);
+    });
+    // trace_pixel_queue (voxel_view_pixels.wgsl:199-216)
+    run([&](Ctx& x, uint32_t id) {
+        if (!queued[id]) return;
+        Cell cell = load(current, id);
+        st[1] += 1;
+        const uint32_t stream = pcg(id * 9781u + 0x9e3779b9u);
+        const ReceiverSample sample = trace_receiver(x, cell.surface, face_normal(cell.face & 7u), stream, cell.sequence);
+        cell.sequence += 1u;
+        if (sample.known) {
+            cell.count = wmin(cell.count + 1.0f, v.tune(1));
+            const float t = 1.0f / cell.count;
+            cell.mean = add(muls(cell.mean, 1.0f - t), muls(f3{sample.energy.x, sample.energy.y, sample.energy.z}, t));
+        }
+        store(current, id, cell);
+        write_output(x, v, output, id, cell);
+    });
+    for (int i = 0; i < 8; ++i) stats[i] = st[i];
     return 0;
 }
 

@@ -53,6 +53,7 @@ _SIG = {
     "orc_accumulate_picks": (_INT, [_P, _P, _P, _P, _P, _U32, _P, _P]),
     "orc_footprints": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _U32, _P, _P]),
     "orc_discover": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P, _INT]),
+    "orc_far_frame": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _P, _INT]),
     "orc_classify": (_INT, [_P, _P, _U32, _P]),
     "orc_select": (_INT, [_P, _P, _P, _U32, _P, _P, _P, _P, _P]),
     "orc_trace_ray": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P]),
@@ -197,6 +198,79 @@ def discovered_faces(pixels):
                      p[:, 4].astype(np.int32)], 1)
     rows = np.unique(rows, axis=0)
     return rows[np.lexsort((rows[:, 3], rows[:, 0], rows[:, 1], rows[:, 2]))]
+
+
+class FarTier:
+    """The far tier's host side restated (vgi_far_frame): settings
+    normalisation, cell size, the view words, the previous camera and the
+    ping-pong of cell histories, with the frame itself run by orc_far_frame."""
+
+    def __init__(self):
+        self.cells = [None, None]
+        self.output = None
+        self.current = 0
+        self.shape = None
+        self.size = None
+        self.previous = None  # (camera words, frame)
+
+    def view_words(self, camera, settings, frame, custom):
+        eye, forward, up, tan_half, w, h = camera
+        s = settings
+        vp = float(np.clip(s.voxel_pixels, 0.0, 4096.0)) if np.isfinite(s.voxel_pixels) else 0.0
+        history = float(np.clip(s.history, 1.0, 1024.0)) if np.isfinite(s.history) else 32.0
+        rate = min(max(s.rate, 1), 8)
+        ratio = np.float32(h) / np.float32(480.0)
+        size = min(s.cell, 4) or min(max(int(np.floor(ratio)) + (1 if ratio - np.floor(ratio) >= 0.5 else 0), 1), 4)
+        cx, cy = -(-w // size), -(-h // size)
+        flags = (1 if vp > 0 else 0) | (s.measure << 1)
+        cam = np.array([*eye, *forward, *up, tan_half], np.float32)
+        if self.shape != (cx, cy) or self.size != (w, h):
+            self.cells = [np.zeros((cx * cy, 12), np.uint32), np.zeros((cx * cy, 12), np.uint32)]
+            self.output = np.zeros(16 + 4 * cx * cy, np.uint32)
+            self.previous = None
+            self.shape, self.size = (cx, cy), (w, h)
+        prev_ok = self.previous is not None and ((frame - self.previous[1]) & 0xFFFFFFFF) <= 1
+        words = np.zeros(44, np.uint32)
+        f = words.view(np.float32)
+        f[0:10] = cam
+        f[10:20] = self.previous[0] if prev_ok else cam
+        words[20:22] = (w, h)
+        words[22:26] = (cx, cy, size, flags)
+        f[26:29] = (vp, history, float(rate))
+        words[29] = self.previous[1] if prev_ok else 0xFFFFFFFF
+        f[30:33] = forward
+        f[33] = np.float32(np.float32(np.float32(1.0) / np.float32(tan_half)) * np.float32(h)) * np.float32(0.5)
+        if s.interest is not None:
+            words[34:37] = np.asarray(s.interest[0], np.int32).view(np.uint32)
+            words[38:41] = np.asarray(s.interest[1], np.int32).view(np.uint32)
+            words[37] = words[41] = 1
+        words[42] = frame & 0xFFFFFFFF
+        words[43] = 1 if custom else 0
+        return words, cam
+
+    def frame(self, geometry, params, materials, lights, emitter_words, pipe, camera, settings, frame, custom=False,
+              receivers=None, estimates=None, state=None, index=None, threads=0):
+        words, cam = self.view_words(camera, settings, frame, custom)
+        d, h, cl, _ = geometry
+        d = c(d, np.int32)
+        cl = c(cl, np.uint32) if len(cl) else np.zeros(1, np.uint32)
+        lights = c(lights, np.float32).reshape(-1)
+        if lights.size == 0:
+            lights = np.zeros(12, np.float32)
+        previous = self.cells[self.current]
+        self.current ^= 1
+        current = self.cells[self.current]
+        stats = np.zeros(8, np.uint32)
+        n_recv = 0 if receivers is None else len(receivers)
+        rc = lib().orc_far_frame(ptr(d), d.size // 4, ptr(c(h, np.uint32)), ptr(cl), ptr(c(params, np.float32)), ptr(c(materials, np.float32)),
+                                 ptr(lights), ptr(c(emitter_words, np.uint32)), ptr(None if state is None else c(state, np.uint32)),
+                                 ptr(None if index is None else c(index, np.uint32)), ctypes.byref(pipe), ptr(words),
+                                 ptr(None if receivers is None else c(receivers, np.uint32)),
+                                 ptr(None if estimates is None else c(estimates, np.uint32)), n_recv, ptr(previous), ptr(current),
+                                 ptr(self.output), ptr(stats), threads)
+        assert rc == 0
+        self.previous = (cam, frame & 0xFFFFFFFF)
+        return current, self.output, stats
 
 
 # ---- model words ------------------------------------------------------------
