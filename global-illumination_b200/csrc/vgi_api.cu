@@ -155,6 +155,14 @@ struct vgi_ctx {
     uint32_t v_hash_mask = 0;
     bool v_hash_valid = false;
     bool custom_lights = false;               // some light has custom visible RGB
+    // reconstruction: screen tile per view receiver (CSR lists per tile),
+    // the published FarPixels and the publish counters
+    DevBuf<uint32_t> v_tile_of, v_tile_start, v_tile_items;
+    uint32_t v_tiles[2] = {0, 0};
+    uint32_t v_tiles_n = 0;                   // receivers the tiles were given for
+    DevBuf<uint4> v_published;
+    DevBuf<uint32_t> v_publish_stats;
+    bool v_published_valid = false;
     // far tier: cell histories (this frame's and the previous one's), the
     // output cells, the trace queue and the statistics
     DevBuf<uint4> far_cells[2];
@@ -1578,9 +1586,27 @@ int vgi_view_set_receivers(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, cudaMemsetAsync(c->v_queue.ptr, 0, (12 + 2 * m) * 4, c->stream));
     c->n_view = n;
     c->v_hash_valid = false;
+    c->v_tiles_n = 0;
+    c->v_published_valid = false;
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }
+
+namespace {
+// The view receivers' owner hash (built once per receiver list).
+int ensure_receiver_hash(vgi_ctx* c) {
+    if (c->n_view == 0 || c->v_hash_valid) return VGI_OK;
+    uint32_t mask = 63;
+    while (mask + 1 < 2 * c->n_view) mask = mask * 2 + 1;
+    VGI_CUDA(c, c->v_hash.reserve((size_t)mask + 1));
+    VGI_CUDA(c, cudaMemsetAsync(c->v_hash.ptr, 0, ((size_t)mask + 1) * 4, c->stream));
+    launch_receiver_hash(c->v_receivers.ptr, c->n_view, c->v_hash.ptr, mask, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    c->v_hash_mask = mask;
+    c->v_hash_valid = true;
+    return VGI_OK;
+}
+}  // namespace
 
 // ---- far tier (voxel_view_pixels.wgsl) -------------------------------------------
 int vgi_far_frame(vgi_ctx* c, const vgi_camera* cam, const vgi_far_settings* settings, uint32_t frame) {
@@ -1648,15 +1674,8 @@ int vgi_far_frame(vgi_ctx* c, const vgi_camera* cam, const vgi_far_settings* set
     f.frame = frame;
     f.custom = c->custom_lights ? 1u : 0u;
     if (c->n_view) {
-        if (!c->v_hash_valid) {
-            uint32_t mask = 63;
-            while (mask + 1 < 2 * c->n_view) mask = mask * 2 + 1;
-            VGI_CUDA(c, c->v_hash.reserve((size_t)mask + 1));
-            VGI_CUDA(c, cudaMemsetAsync(c->v_hash.ptr, 0, ((size_t)mask + 1) * 4, c->stream));
-            launch_receiver_hash(c->v_receivers.ptr, c->n_view, c->v_hash.ptr, mask, c->stream);
-            c->v_hash_mask = mask;
-            c->v_hash_valid = true;
-        }
+        const int rc = ensure_receiver_hash(c);
+        if (rc != VGI_OK) return rc;
         f.receivers = c->v_receivers.ptr;
         f.estimates = c->v_estimates.ptr;
         f.receiver_hash = c->v_hash.ptr;
@@ -1706,6 +1725,126 @@ int vgi_far_read(vgi_ctx* c, uint32_t* shape4, uint32_t* output, uint32_t* cells
     } else if (stats8) {
         std::fill(stats8, stats8 + 8, 0u);
     }
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+// ---- reconstruction and presentation (voxel_view_runtime.wgsl:380-521,
+// voxel_gi_presentation.wesl:350-412) ------------------------------------------------
+int vgi_view_set_tiles(vgi_ctx* c, const uint32_t* tiles, uint32_t n, uint32_t tiles_x, uint32_t tiles_y) {
+    if (!c || (n && !tiles)) return VGI_ERR_INVALID;
+    if (n != c->n_view) return fail(c, VGI_ERR_INVALID, "one tile per view receiver");
+    if ((uint64_t)tiles_x * tiles_y > (1u << 24)) return fail(c, VGI_ERR_INVALID, "at most 2^24 tiles");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    const uint32_t n_tiles = tiles_x * tiles_y;
+    // Lists per tile in receiver order (a counting sort): the donor order of
+    // the reconstruction does not depend on the GPU's scheduling.
+    std::vector<uint32_t> start((size_t)n_tiles + 1, 0), items(std::max<uint32_t>(n, 1)), tile_of(std::max<uint32_t>(n, 1), 0xffffffffu);
+    for (uint32_t i = 0; i < n; ++i)
+        if (tiles[i] < n_tiles) ++start[tiles[i] + 1];
+    for (uint32_t t = 0; t < n_tiles; ++t) start[t + 1] += start[t];
+    std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (tiles[i] >= n_tiles) continue;
+        tile_of[i] = tiles[i];
+        items[fill[tiles[i]]++] = i;
+    }
+    VGI_CUDA(c, c->v_tile_of.reserve(tile_of.size()));
+    VGI_CUDA(c, c->v_tile_start.reserve(start.size()));
+    VGI_CUDA(c, c->v_tile_items.reserve(items.size()));
+    VGI_CUDA(c, cudaMemcpyAsync(c->v_tile_of.ptr, tile_of.data(), tile_of.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(c->v_tile_start.ptr, start.data(), start.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(c->v_tile_items.ptr, items.data(), items.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->v_tiles[0] = tiles_x;
+    c->v_tiles[1] = tiles_y;
+    c->v_tiles_n = n;
+    return VGI_OK;
+}
+
+namespace {
+ViewDisplay view_display(vgi_ctx* c) {
+    ViewDisplay d{};
+    d.receivers = c->v_receivers.ptr;
+    d.estimates = c->v_estimates.ptr;
+    d.conts = c->v_conts.ptr;
+    d.tile_of = c->v_tile_of.ptr;
+    d.tile_start = c->v_tile_start.ptr;
+    d.tile_items = c->v_tile_items.ptr;
+    d.tiles_x = c->v_tiles[0];
+    d.tiles_y = c->v_tiles[1];
+    d.receiver_hash = c->v_hash.ptr;
+    d.hash_mask = c->v_hash_mask;
+    d.n = c->n_view;
+    d.custom = c->custom_lights ? 1u : 0u;
+    d.published = c->v_published.ptr;
+    d.stats = c->v_publish_stats.ptr;
+    return d;
+}
+}  // namespace
+
+int vgi_view_reconstruct(vgi_ctx* c, const vgi_view_display* display) {
+    if (!c || !display) return VGI_ERR_INVALID;
+    if (!view_ready(c)) return fail(c, VGI_ERR_STATE, "the view tier needs geometry, materials, lights and emitters");
+    if (c->n_view == 0) return VGI_OK;
+    if (c->v_tiles_n != c->n_view) return fail(c, VGI_ERR_STATE, "vgi_view_set_tiles first");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    int rc = ensure_receiver_hash(c);
+    if (rc != VGI_OK) return rc;
+    VGI_CUDA(c, c->v_published.reserve((size_t)c->n_view * 3));
+    VGI_CUDA(c, c->v_publish_stats.reserve(5));
+    VGI_CUDA(c, cudaMemsetAsync(c->v_publish_stats.ptr, 0, 20, c->stream));
+    ViewDisplay d = view_display(c);
+    d.display[0] = display->evidence_goal;
+    d.display[1] = display->spatial;
+    d.display[2] = display->temporal;
+    launch_reconstruct(trace_args(c, nullptr, nullptr, 0, 1, c->n_slots > 0), d, transport_limited(c), c->transport.budgeted != 0, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    c->v_published_valid = true;
+    return VGI_OK;
+}
+
+int vgi_view_read_published(vgi_ctx* c, uint32_t* pixels12, uint32_t* stats5) {
+    if (!c) return VGI_ERR_INVALID;
+    if (c->n_view && !c->v_published_valid) return fail(c, VGI_ERR_STATE, "nothing published since the receivers changed");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    if (c->n_view) {
+        if (pixels12) VGI_CUDA(c, cudaMemcpyAsync(pixels12, c->v_published.ptr, (size_t)c->n_view * 48, cudaMemcpyDeviceToHost, c->stream));
+        if (stats5) VGI_CUDA(c, cudaMemcpyAsync(stats5, c->v_publish_stats.ptr, 20, cudaMemcpyDeviceToHost, c->stream));
+    } else if (stats5) {
+        std::fill(stats5, stats5 + 5, 0u);
+    }
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_view_present(vgi_ctx* c, const vgi_camera* cam, int corners, float* rgba) {
+    if (!c || !cam || !rgba) return VGI_ERR_INVALID;
+    if (!c->geometry) return fail(c, VGI_ERR_STATE, "no geometry uploaded");
+    if (c->n_view && !c->v_published_valid) return fail(c, VGI_ERR_STATE, "vgi_view_reconstruct first");
+    const uint64_t n = (uint64_t)cam->width * cam->height;
+    if (n == 0 || n > (1ull << 26)) return fail(c, VGI_ERR_INVALID, "camera size outside 1..2^26 pixels");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    DevBuf<float> dcam;
+    DevBuf<float4> image;
+    VGI_CUDA(c, dcam.reserve(10));
+    VGI_CUDA(c, image.reserve(n));
+    const float host_cam[10] = {cam->eye[0], cam->eye[1], cam->eye[2], cam->forward[0], cam->forward[1], cam->forward[2],
+                                cam->up[0], cam->up[1], cam->up[2], cam->tan_half_fov};
+    VGI_CUDA(c, cudaMemcpyAsync(dcam.ptr, host_cam, sizeof(host_cam), cudaMemcpyHostToDevice, c->stream));
+    ViewDisplay d = view_display(c);
+    uint32_t empty = 0;
+    DevBuf<uint32_t> no_hash;
+    if (c->n_view == 0) {
+        // No receivers: every face displays zero.
+        VGI_CUDA(c, no_hash.reserve(1));
+        VGI_CUDA(c, cudaMemcpyAsync(no_hash.ptr, &empty, 4, cudaMemcpyHostToDevice, c->stream));
+        d.receiver_hash = no_hash.ptr;
+        d.hash_mask = 0;
+    }
+    launch_present(trace_args(c, nullptr, nullptr, 0, 1, false), d, dcam.ptr, cam->width, cam->height, corners != 0, image.ptr, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    VGI_CUDA(c, cudaMemcpyAsync(rgba, image.ptr, n * 16, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }

@@ -1387,6 +1387,265 @@ void launch_receiver_hash(const uint4* receivers, uint32_t n, uint32_t* hash, ui
     if (n) receiver_hash_kernel<<<(n + 127) / 128, 128, 0, s>>>(receivers, n, hash, mask);
 }
 
+// ---- reconstruction and presentation --------------------------------------------
+namespace {
+
+__device__ __forceinline__ float luminance(V3 c) { return dot3(c, V3{0.2126f, 0.7152f, 0.0722f}); }
+__device__ __forceinline__ V3 v3w(uint4 w) { return V3{__uint_as_float(w.x), __uint_as_float(w.y), __uint_as_float(w.z)}; }
+
+// mean_variance (voxel_view_runtime.wgsl:383-394): the mean's variance with
+// a 64-sample prior and the unseen-light floor `reference / n`.
+__device__ float mean_variance(uint4 mean_w, uint4 moment_w, float reference) {
+    const V3 mean = v3w(mean_w), moment = v3w(moment_w);
+    const float n = wmax(__uint_as_float(mean_w.w), 1.0f);
+    const float m = luminance(mean);
+    const V3 channel{wmax(__fsub_rn(moment.x, __fmul_rn(mean.x, mean.x)), 0.0f), wmax(__fsub_rn(moment.y, __fmul_rn(mean.y, mean.y)), 0.0f),
+                     wmax(__fsub_rn(moment.z, __fmul_rn(mean.z, mean.z)), 0.0f)};
+    const float deviation = luminance(V3{__fsqrt_rn(channel.x), __fsqrt_rn(channel.y), __fsqrt_rn(channel.z)});
+    const float prior = __fmul_rn(m, m);
+    const float rest = wmax(__fsub_rn(n, 1.0f), 0.0f);
+    const float shrunk = __fdiv_rn(__fadd_rn(__fmul_rn(__fmul_rn(deviation, deviation), rest), __fmul_rn(prior, 64.0f)), __fadd_rn(rest, 64.0f));
+    const float unseen = __fdiv_rn(reference, n);
+    return __fadd_rn(__fdiv_rn(shrunk, n), __fmul_rn(unseen, unseen));
+}
+
+// coplanar_donor (voxel_view_runtime.wgsl:396-404); every caller-given
+// receiver is its own owner.
+__device__ bool coplanar_donor(const ViewDisplay& D, uint4 r0, uint4 r1, V3 normal, uint32_t candidate) {
+    const uint4 d0 = D.receivers[candidate * 2u];
+    if (d0.w != r0.w) return false;
+    const V3 delta = v3w(d0) - v3w(r0);
+    // receiver_stride: twice the surface's offset from the voxel along the face's next axis.
+    const uint32_t u = (r0.w / 2u + 1u) % 3u;
+    const float su = u == 0u ? __uint_as_float(r0.x) : (u == 1u ? __uint_as_float(r0.y) : __uint_as_float(r0.z));
+    const int vu = u == 0u ? (int)r1.x : (u == 1u ? (int)r1.y : (int)r1.z);
+    const float reach = __fmul_rn(16.0f, __fmul_rn(2.0f, __fsub_rn(su, (float)vu)));
+    return fabsf(dot3(delta, normal)) <= 0.05f && dot3(delta, delta) <= __fmul_rn(reach, reach);
+}
+
+// reconstruct_view (voxel_view_runtime.wgsl:406-474): inverse-variance
+// weighting of coplanar donors in the screen tiles around the receiver's,
+// with the centre's bias bound, then a temporal blend of the shown value.
+// Tile lists are visited in receiver order.
+__global__ void __launch_bounds__(128) reconstruct_kernel(const ViewDisplay D) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const uint4 r0 = D.receivers[i * 2u], r1 = D.receivers[i * 2u + 1u];
+    const uint32_t tile = D.tile_of[i];
+    if (r0.w >= 6u || tile >= D.tiles_x * D.tiles_y) return;
+    const uint4 c_mean = D.estimates[i * 4u], c_moment = D.estimates[i * 4u + 1u], c_shown = D.estimates[i * 4u + 2u];
+    const V3 normal = face_normal(r0.w);
+    const int tx = (int)(tile % D.tiles_x), ty = (int)(tile / D.tiles_x);
+    const float center_luminance = luminance(v3w(c_mean));
+    float reference = center_luminance;
+    for (int y = -1; y <= 1; ++y)
+        for (int x = -1; x <= 1; ++x) {
+            const int qx = tx + x, qy = ty + y;
+            if (qx < 0 || qy < 0 || qx >= (int)D.tiles_x || qy >= (int)D.tiles_y) continue;
+            const uint32_t t = (uint32_t)qy * D.tiles_x + (uint32_t)qx;
+            for (uint32_t k = D.tile_start[t]; k < D.tile_start[t + 1u]; ++k) {
+                const uint32_t candidate = D.tile_items[k];
+                if (candidate == i || !coplanar_donor(D, r0, r1, normal, candidate)) continue;
+                const uint4 value = D.estimates[candidate * 4u];
+                if (__uint_as_float(value.w) > 0.0f) reference = wmax(reference, luminance(v3w(value)));
+            }
+        }
+    const float center_variance = mean_variance(c_mean, c_moment, reference);
+    const float tolerance = __fmul_rn(D.display[0], center_luminance);
+    const float tol2 = __fmul_rn(tolerance, tolerance);
+    const float deficit = __fdiv_rn(center_variance, wmax(tol2, 1e-12f));
+    const int radius = (int)wclamp(ceilf(__fmul_rn(__fsqrt_rn(__fdiv_rn(deficit, 3.14159f)), 0.5f)), 1.0f, 4.0f);
+    const bool unsampled = __uint_as_float(c_mean.w) <= 0.0f;
+    V3 sum{0.0f, 0.0f, 0.0f};
+    float weight = 0.0f;
+    if (!unsampled) {
+        const float w = __fdiv_rn(1.0f, wmax(center_variance, 1e-12f));
+        sum = v3w(c_mean) * w;
+        weight = w;
+    }
+    if ((unsampled || center_variance > tol2) && D.display[1] > 0.0f) {
+        for (int y = -radius; y <= radius; ++y)
+            for (int x = -radius; x <= radius; ++x) {
+                const int qx = tx + x, qy = ty + y;
+                if (qx < 0 || qy < 0 || qx >= (int)D.tiles_x || qy >= (int)D.tiles_y) continue;
+                const uint32_t t = (uint32_t)qy * D.tiles_x + (uint32_t)qx;
+                for (uint32_t k = D.tile_start[t]; k < D.tile_start[t + 1u]; ++k) {
+                    const uint32_t candidate = D.tile_items[k];
+                    if (candidate == i || !coplanar_donor(D, r0, r1, normal, candidate)) continue;
+                    const uint4 value = D.estimates[candidate * 4u];
+                    if (__uint_as_float(value.w) <= 0.0f) continue;
+                    const float variance = mean_variance(value, D.estimates[candidate * 4u + 1u], reference);
+                    float bias2 = 0.0f;
+                    if (!unsampled) {
+                        const float difference = __fsub_rn(luminance(v3w(value)), center_luminance);
+                        bias2 = wmax(__fsub_rn(__fsub_rn(__fmul_rn(difference, difference), variance), center_variance), 0.0f);
+                    }
+                    const float w = __fdiv_rn(1.0f, wmax(__fadd_rn(variance, bias2), 1e-12f));
+                    sum = sum + v3w(value) * w;
+                    weight = __fadd_rn(weight, w);
+                }
+            }
+    }
+    if (weight <= 0.0f) return;
+    const float keep = unsampled ? 0.0f : __fsub_rn(1.0f, D.display[1]);
+    const V3 desired = (sum / weight) * __fsub_rn(1.0f, keep) + v3w(c_mean) * keep;
+    const float blend = __uint_as_float(c_shown.w) > 0.0f ? D.display[2] : 1.0f;
+    const V3 shown = v3w(c_shown) * __fsub_rn(1.0f, blend) + desired * blend;
+    D.estimates[i * 4u + 2u] = make_uint4(__float_as_uint(shown.x), __float_as_uint(shown.y), __float_as_uint(shown.z), __float_as_uint(1.0f));
+}
+
+// publish_view (voxel_view_runtime.wgsl:476-521): a FarPixel per receiver
+// (surface, face, irradiance, evidence, sky corner words) and the counters.
+template <bool LIMITED, bool BUDGETED>
+__global__ void __launch_bounds__(128) publish_kernel(const TraceArgs A, const ViewDisplay D) {
+    __shared__ float4 smat[512];
+    load_smat(A, smat);
+    Cnt<false> cnt;
+    Tracer<1u, LIMITED, BUDGETED, false> T{A, smat, cnt};
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const uint4 r0 = D.receivers[i * 2u];
+    uint4 out0 = make_uint4(0u, 0u, 0u, 0xffffffffu), out1 = make_uint4(0u, 0u, 0u, 0u), out2 = make_uint4(0u, 0u, 0u, 0u);
+    if (r0.w < 6u) {
+        const uint4 mean = D.estimates[i * 4u], shown = D.estimates[i * 4u + 2u], identity = D.estimates[i * 4u + 3u];
+        V3 irradiance = v3w(shown);
+        if (D.custom) {
+            V3 value, custom;
+            T.template direct_at<true>(v3w(r0), face_normal(r0.w), value, custom);
+            irradiance = irradiance + custom;
+        }
+        const float count = __uint_as_float(mean.w);
+        const bool lit = __uint_as_float(shown.w) > 0.0f || irradiance.x > 0.0f || irradiance.y > 0.0f || irradiance.z > 0.0f;
+        const float evidence = lit ? wmax(count, 0.001f) : 0.0f;
+        uint32_t sky[4];
+        for (uint32_t corner = 0; corner < 4u; ++corner) {
+            const uint32_t byte = (identity.z >> (corner * 8u)) & 255u;
+            sky[corner] = (byte & 15u) | ((byte & 128u) << 24u);
+        }
+        out0 = r0;
+        out1 = make_uint4(__float_as_uint(irradiance.x), __float_as_uint(irradiance.y), __float_as_uint(irradiance.z), __float_as_uint(evidence));
+        out2 = make_uint4(sky[0], sky[1], sky[2], sky[3]);
+        atomicAdd(D.stats + 0, (uint32_t)count);
+        atomicMax(D.stats + 1, (uint32_t)count);
+        if (count == 0.0f) atomicAdd(D.stats + 2, 1u);
+        if (evidence > 0.0f) atomicAdd(D.stats + 3, 1u);
+        if (D.conts[i * 8u + 4u].w == 1u) atomicAdd(D.stats + 4, 1u);
+    }
+    D.published[i * 3u] = out0;
+    D.published[i * 3u + 1u] = out1;
+    D.published[i * 3u + 2u] = out2;
+}
+
+// display_face (voxel_gi_presentation.wesl:363-371): a published face's
+// irradiance and evidence (at most 1), zero where none is published.
+__device__ float4 display_face(const ViewDisplay& D, I3 voxel, uint32_t face, int s) {
+    const V3 n = face_normal(face);
+    const V3 surface = itof(voxel) + add_s(n * 0.5f, 0.5f) * (float)s;
+    uint32_t slot = (hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(face + 1u)) & D.hash_mask;
+#pragma unroll 1
+    for (uint32_t step = 0; step < 64u; ++step) {
+        const uint32_t entry = D.receiver_hash[slot];
+        if (entry == 0u) break;
+        if (entry <= D.n) {
+            const uint4 p0 = D.published[(entry - 1u) * 3u];
+            if (p0.w == face && __uint_as_float(p0.x) == surface.x && __uint_as_float(p0.y) == surface.y && __uint_as_float(p0.z) == surface.z) {
+                const uint4 p1 = D.published[(entry - 1u) * 3u + 1u];
+                return make_float4(__uint_as_float(p1.x), __uint_as_float(p1.y), __uint_as_float(p1.z), wmin(__uint_as_float(p1.w), 1.0f));
+            }
+        }
+        slot = (slot + 1u) & D.hash_mask;
+    }
+    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// corner_value (voxel_gi_presentation.wesl:353-361): the connected
+// coplanar faces' evidence-weighted mean at a shared corner.
+__device__ V3 corner_value(float4 c, float4 eu, float4 ev, float4 diag) {
+    float sx = __fadd_rn(__fadd_rn(__fmul_rn(c.x, c.w), __fmul_rn(eu.x, eu.w)), __fmul_rn(ev.x, ev.w));
+    float sy = __fadd_rn(__fadd_rn(__fmul_rn(c.y, c.w), __fmul_rn(eu.y, eu.w)), __fmul_rn(ev.y, ev.w));
+    float sz = __fadd_rn(__fadd_rn(__fmul_rn(c.z, c.w), __fmul_rn(eu.z, eu.w)), __fmul_rn(ev.z, ev.w));
+    float sw = __fadd_rn(__fadd_rn(c.w, eu.w), ev.w);
+    if (eu.w > 0.0f || ev.w > 0.0f) {
+        sx = __fadd_rn(sx, __fmul_rn(diag.x, diag.w));
+        sy = __fadd_rn(sy, __fmul_rn(diag.y, diag.w));
+        sz = __fadd_rn(sz, __fmul_rn(diag.z, diag.w));
+        sw = __fadd_rn(sw, diag.w);
+    }
+    const float d = wmax(sw, 0.000001f);
+    return V3{__fdiv_rn(sx, d), __fdiv_rn(sy, d), __fdiv_rn(sz, d)};
+}
+__device__ __forceinline__ V3 mix3(V3 a, V3 b, float t) { return a * __fsub_rn(1.0f, t) + b * t; }
+
+// corner_irradiance (voxel_gi_presentation.wesl:377-412) at each pixel's
+// first hit: rgb and the centre face's evidence.
+__global__ void __launch_bounds__(128) present_kernel(const TraceArgs A, const ViewDisplay D, const float* cam, uint32_t w, uint32_t h,
+                                                      bool corners, float4* image) {
+    const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= w * h) return;
+    Cnt<false> cnt;
+    const V3 eye{cam[0], cam[1], cam[2]};
+    const Ray hit = trace_domain(A, eye, pixel_ray(cam, id % w, id / w, w, h), A.max_distance, true, 2048u, cnt);
+    if (hit.status != 1u) {
+        image[id] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    const V3 position = hit.position, normal = hit.normal;
+    const V3 inner = position - normal * 0.01f;
+    const I3 cell{(int)floorf(inner.x), (int)floorf(inner.y), (int)floorf(inner.z)};
+    const int s = voxel_stride(A, cell, cnt);
+    const I3 voxel{cell.x & -s, cell.y & -s, cell.z & -s};
+    uint32_t face = 0u;
+    I3 u{0, s, 0}, v{0, 0, s};
+    if (fabsf(normal.y) > 0.5f) {
+        face = 2u;
+        u = I3{s, 0, 0};
+    } else if (fabsf(normal.z) > 0.5f) {
+        face = 4u;
+        u = I3{s, 0, 0};
+        v = I3{0, s, 0};
+    }
+    const uint32_t axis = face / 2u;
+    face += (axis == 0u ? normal.x : (axis == 1u ? normal.y : normal.z)) < 0.0f ? 1u : 0u;
+    const float4 center = display_face(D, voxel, face, s);
+    if (!corners) {
+        image[id] = center;
+        return;
+    }
+    auto at = [&](int du, int dv) {
+        return display_face(D, I3{voxel.x + du * u.x + dv * v.x, voxel.y + du * u.y + dv * v.y, voxel.z + du * u.z + dv * v.z}, face, s);
+    };
+    const float4 left = at(-1, 0), right = at(1, 0), bottom = at(0, -1), top = at(0, 1);
+    const V3 c00 = corner_value(center, left, bottom, at(-1, -1));
+    const V3 c10 = corner_value(center, right, bottom, at(1, -1));
+    const V3 c01 = corner_value(center, left, top, at(-1, 1));
+    const V3 c11 = corner_value(center, right, top, at(1, 1));
+    const V3 local = (position - itof(voxel)) / (float)(s * s);
+    const float ux = wclamp(dot3(local, itof(u)), 0.0f, 1.0f), uy = wclamp(dot3(local, itof(v)), 0.0f, 1.0f);
+    const V3 rgb = mix3(mix3(c00, c10, ux), mix3(c01, c11, ux), uy);
+    image[id] = make_float4(rgb.x, rgb.y, rgb.z, center.w);
+}
+
+}  // namespace
+
+void launch_reconstruct(const TraceArgs& a, const ViewDisplay& d, bool limited, bool budgeted, cudaStream_t s) {
+    if (d.n == 0) return;
+    const uint32_t blocks = (d.n + 127) / 128;
+    reconstruct_kernel<<<blocks, 128, 0, s>>>(d);
+    if (limited) {
+        if (budgeted) publish_kernel<true, true><<<blocks, 128, 0, s>>>(a, d);
+        else publish_kernel<true, false><<<blocks, 128, 0, s>>>(a, d);
+    } else {
+        if (budgeted) publish_kernel<false, true><<<blocks, 128, 0, s>>>(a, d);
+        else publish_kernel<false, false><<<blocks, 128, 0, s>>>(a, d);
+    }
+}
+
+void launch_present(const TraceArgs& a, const ViewDisplay& d, const float* cam, uint32_t w, uint32_t h, bool corners, float4* image,
+                    cudaStream_t s) {
+    const uint32_t n = w * h;
+    if (n) present_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, d, cam, w, h, corners, image);
+}
+
 void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uint32_t threads, uint32_t n_directional, uint32_t* sums,
                        uint4* events, cudaStream_t s) {
     if (n_tasks == 0) return;

@@ -187,6 +187,27 @@ constexpr uint32_t kFarOwned = 0, kFarTraced = 1, kFarHistory = 2, kFarReproject
 void launch_far(const TraceArgs& a, const FarView& f, const uint4* previous, uint4* current, uint4* output, uint32_t* queue, uint32_t* stats,
                 bool limited, cudaStream_t s);
 void launch_receiver_hash(const uint4* receivers, uint32_t n, uint32_t* hash, uint32_t mask, cudaStream_t s);
+// Reconstruction and presentation of the view receivers (vgi_trace.cu,
+// voxel_view_runtime.wgsl:380-521 and voxel_gi_presentation.wesl:350-412).
+struct ViewDisplay {
+    const uint4* receivers;       // 2 uint4 each
+    uint4* estimates;             // 4 uint4 each (shown is written)
+    const uint4* conts;           // 8 uint4 each
+    const uint32_t* tile_of;      // per receiver: screen tile, all ones: none
+    const uint32_t* tile_start;   // CSR over tiles: receivers of tile t are items[start[t] .. start[t + 1])
+    const uint32_t* tile_items;
+    uint32_t tiles_x, tiles_y;
+    const uint32_t* receiver_hash;  // receiver + 1 per slot
+    uint32_t hash_mask;
+    uint32_t n;
+    float display[3];             // evidence goal, spatial strength, temporal blend
+    uint32_t custom;              // add custom direct RGB when publishing
+    uint4* published;             // FarPixel per receiver: 3 uint4
+    uint32_t* stats;              // history, max history, uncovered, displayed, paused
+};
+void launch_reconstruct(const TraceArgs& a, const ViewDisplay& d, bool limited, bool budgeted, cudaStream_t s);
+void launch_present(const TraceArgs& a, const ViewDisplay& d, const float* cam, uint32_t w, uint32_t h, bool corners, float4* image,
+                    cudaStream_t s);
 // MLP radiance cache (vgi_mlp.cu).
 cudaError_t mlp_set_attributes();
 void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,

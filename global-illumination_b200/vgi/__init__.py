@@ -50,6 +50,35 @@ class Camera(ctypes.Structure):
                 ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
 
 
+class ViewDisplay(ctypes.Structure):
+    """vgi_view_display."""
+    _fields_ = [("evidence_goal", ctypes.c_float), ("spatial", ctypes.c_float), ("temporal", ctypes.c_float)]
+
+
+def witness_tiles(pixels: np.ndarray, faces: np.ndarray, grid_x: int, grid_y: int) -> np.ndarray:
+    """Each receiver's screen tile from discovery's per-pixel records (h, w,
+    8): the first pixel in raster order that saw its face is its witness;
+    its cell is pixel * grid / viewport and its tile the 2 x 2-cell tile
+    (tile_of_pixel, voxel_view_discovery.wgsl:160-165). All ones: never
+    seen. Tiles are ((grid_x + 1) // 2) x ((grid_y + 1) // 2)."""
+    h, w = pixels.shape[:2]
+    p = np.asarray(pixels, np.uint32).reshape(-1, 8)
+    hit = np.nonzero(p[:, 3] < 6)[0]
+    seen = {}
+    for i in hit[::-1]:  # later pixels first, so the first pixel wins
+        seen[(int(p[i, 0]), int(p[i, 1]), int(p[i, 2]), int(p[i, 3]))] = int(i)
+    tiles_x = (grid_x + 1) // 2
+    out = np.full(len(faces), 0xFFFFFFFF, np.uint32)
+    for k, f in enumerate(np.asarray(faces, np.int32).reshape(-1, 5)):
+        i = seen.get((int(f[0]) & 0xFFFFFFFF, int(f[1]) & 0xFFFFFFFF, int(f[2]) & 0xFFFFFFFF, int(f[3])))
+        if i is None:
+            continue
+        cx = min((i % w) * grid_x // w, grid_x - 1)
+        cy = min((i // w) * grid_y // h, grid_y - 1)
+        out[k] = (cy // 2) * tiles_x + cx // 2
+    return out
+
+
 class FarSettingsStruct(ctypes.Structure):
     """vgi_far_settings."""
     _fields_ = [("voxel_pixels", ctypes.c_float), ("measure", ctypes.c_uint32), ("cell", ctypes.c_uint32), ("history", ctypes.c_float),
@@ -229,6 +258,10 @@ _SIGNATURES = {
     "vgi_far_frame": (_INT, [_P, _P, _P, _U32]),
     "vgi_far_read": (_INT, [_P, _P, _P, _P, _P]),
     "vgi_far_reset": (_INT, [_P]),
+    "vgi_view_set_tiles": (_INT, [_P, _P, _U32, _U32, _U32]),
+    "vgi_view_reconstruct": (_INT, [_P, _P]),
+    "vgi_view_read_published": (_INT, [_P, _P, _P]),
+    "vgi_view_present": (_INT, [_P, _P, _INT, _P]),
     "vgi_apply_events_footprints": (_INT, [_P, _P, _U32, _U64, _P, _U32, _P, _U32]),
     "vgi_read_selection": (_INT, [_P, _P, _P, _P, _P, _P]),
     "vgi_complete_batch": (_INT, [_P, _U64]),
@@ -672,6 +705,31 @@ class GpuTracer:
         n = ctypes.c_uint32()
         self._check(self._lib.vgi_discover_faces(self._h, ctypes.byref(cam), _ptr(pixels), _ptr(faces), capacity, ctypes.byref(n)))
         return pixels, faces[: n.value].copy()
+
+    # reconstruction and presentation of the view receivers
+    def view_set_tiles(self, tiles: np.ndarray, tiles_x: int, tiles_y: int) -> None:
+        t = _c(tiles, np.uint32).reshape(-1)
+        self._check(self._lib.vgi_view_set_tiles(self._h, _ptr(t), t.size, tiles_x, tiles_y))
+
+    def view_reconstruct(self, evidence_goal: float = 0.031, spatial: float = 1.0, temporal: float = 1.0) -> None:
+        d = ViewDisplay(evidence_goal, spatial, temporal)
+        self._check(self._lib.vgi_view_reconstruct(self._h, ctypes.byref(d)))
+
+    def view_read_published(self):
+        """(FarPixel words (n, 12), counters (5,))."""
+        n = getattr(self, "n_view", 0)
+        pixels = np.zeros((n, 12), np.uint32)
+        stats = np.zeros(5, np.uint32)
+        self._check(self._lib.vgi_view_read_published(self._h, _ptr(pixels), _ptr(stats)))
+        return pixels, stats
+
+    def view_present(self, eye, forward, up, tan_half_fov: float, width: int, height: int, corners: bool = True) -> np.ndarray:
+        """corner_irradiance at each pixel's first hit: (height, width, 4) f32."""
+        cam = Camera((ctypes.c_float * 3)(*map(float, eye)), (ctypes.c_float * 3)(*map(float, forward)),
+                     (ctypes.c_float * 3)(*map(float, up)), float(tan_half_fov), width, height)
+        out = np.zeros((height, width, 4), np.float32)
+        self._check(self._lib.vgi_view_present(self._h, ctypes.byref(cam), 1 if corners else 0, _ptr(out)))
+        return out
 
     # far tier
     def far_frame(self, eye, forward, up, tan_half_fov: float, width: int, height: int, settings: Optional["FarTierSettings"] = None,

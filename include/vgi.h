@@ -349,6 +349,33 @@ typedef struct vgi_camera {
 } vgi_camera;
 int vgi_discover_faces(vgi_ctx* ctx, const vgi_camera* camera, uint32_t* pixels8, vgi_face* faces, uint32_t capacity, uint32_t* n_faces);
 
+/* ---- reconstruction and presentation of the view receivers ------------------------
+ * vgi_view_set_tiles gives each view receiver its screen tile (tiles_x x
+ * tiles_y, all ones: none; e.g. the 2 x 2-cell tile of the pixel where
+ * discovery first saw its face, as the receiver pool's witness). Then
+ * vgi_view_reconstruct runs reconstruct_view (inverse-variance weighting of
+ * coplanar donors in the tiles around, radius 1..4 tiles from the evidence
+ * deficit, a bias bound against the centre, a temporal blend of the shown
+ * value; voxel_view_runtime.wgsl:380-474; donors in receiver order per
+ * tile) and publish_view (a FarPixel per receiver: surface xyz, face (all
+ * ones: none), irradiance rgb = shown plus custom direct light, evidence,
+ * four sky corner words; voxel_view_runtime.wgsl:476-521). Counters: summed
+ * history, max history, uncovered, displayed, paused. vgi_view_present
+ * evaluates the presentation's corner_irradiance at each pixel's first hit
+ * (voxel_gi_presentation.wesl:350-412): the face's published irradiance,
+ * or with `corners` the evidence-weighted virtual-corner interpolation over
+ * coplanar neighbours; rgba = rgb and the face's evidence (at most 1),
+ * zeros where the ray hits nothing. */
+typedef struct vgi_view_display {
+    float evidence_goal; /* display.x: relative noise threshold (the reference's default 0.031) */
+    float spatial;       /* display.y: spatial reconstruction strength (default 1) */
+    float temporal;      /* display.z: blend of the shown value per frame */
+} vgi_view_display;
+int vgi_view_set_tiles(vgi_ctx* ctx, const uint32_t* tiles, uint32_t n, uint32_t tiles_x, uint32_t tiles_y);
+int vgi_view_reconstruct(vgi_ctx* ctx, const vgi_view_display* display);
+int vgi_view_read_published(vgi_ctx* ctx, uint32_t* pixels12, uint32_t* stats5);
+int vgi_view_present(vgi_ctx* ctx, const vgi_camera* camera, int corners, float* rgba);
+
 /* ---- far tier ---------------------------------------------------------------------
  * Per-pixel lighting for faces small on screen (FarTierSettings,
  * shaders/voxel_view_pixels.wgsl), headless: each cell of `cell` x `cell`

@@ -1625,6 +1625,247 @@ int orc_far_frame(const int32_t* directory, uint64_t slots, const uint32_t* head
     return 0;
 }
 
+// ---- reconstruction and presentation of the view receivers -------------------------
+// receivers: 8 words each (surface xyz, face, voxel xyz, sequence);
+// estimates: 16 (mean, moment, shown, identity); conts: 32; tile_of: a tile
+// per receiver (all ones: none); published: 12 words each (FarPixel).
+namespace recon {
+static const f3 LUM{0.2126f, 0.7152f, 0.0722f};
+static f3 w3(const uint32_t* w) { return f3{bitsf(w[0]), bitsf(w[1]), bitsf(w[2])}; }
+
+// voxel_view_runtime.wgsl:383-394
+static float mean_variance(const uint32_t* e, float reference) {
+    const f3 mean = w3(e), moment = w3(e + 4);
+    const float n = wmax(bitsf(e[3]), 1.0f);
+    const float m = dot(mean, LUM);
+    const f3 channel{wmax(moment.x - mean.x * mean.x, 0.0f), wmax(moment.y - mean.y * mean.y, 0.0f), wmax(moment.z - mean.z * mean.z, 0.0f)};
+    const float deviation = dot(f3{std::sqrt(channel.x), std::sqrt(channel.y), std::sqrt(channel.z)}, LUM);
+    const float prior = m * m;
+    const float rest = wmax(n - 1.0f, 0.0f);
+    const float shrunk = (deviation * deviation * rest + prior * 64.0f) / (rest + 64.0f);
+    const float unseen = reference / n;
+    return shrunk / n + unseen * unseen;
+}
+
+// voxel_view_runtime.wgsl:396-404 (each caller-given receiver owns itself)
+static bool coplanar_donor(const uint32_t* receivers, const uint32_t* r, f3 normal, uint32_t candidate) {
+    const uint32_t* d = receivers + (size_t)candidate * 8;
+    if (d[3] != r[3]) return false;
+    const f3 delta = sub(w3(d), w3(r));
+    const uint32_t u = (r[3] / 2u + 1u) % 3u;
+    const float reach = 16.0f * (2.0f * (bitsf(r[u]) - (float)(int32_t)r[4 + u]));
+    return std::fabs(dot(delta, normal)) <= 0.05f && dot(delta, delta) <= reach * reach;
+}
+
+static f3 mix3(f3 a, f3 b, float t) { return add(muls(a, 1.0f - t), muls(b, t)); }
+}  // namespace recon
+
+int orc_reconstruct(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
+                    const float* materials, const float* lights, const uint32_t* emitters, const orc_pipeline* pipe, const uint32_t* receivers,
+                    uint32_t* estimates, const uint32_t* conts, const uint32_t* tile_of, uint32_t tiles_x, uint32_t tiles_y, uint32_t n,
+                    const float* display, uint32_t custom, uint32_t* published, uint32_t* stats) {
+    using namespace recon;
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, materials, lights, emitters, nullptr, nullptr, *pipe};
+    Ctx x{g, m, Counters{}};
+    const uint32_t n_tiles = tiles_x * tiles_y;
+    std::vector<std::vector<uint32_t>> lists(n_tiles);
+    for (uint32_t i = 0; i < n; ++i)
+        if (tile_of[i] < n_tiles) lists[tile_of[i]].push_back(i);
+    // Every receiver reads the estimates as they were before this pass.
+    const std::vector<uint32_t> before(estimates, estimates + (size_t)n * 16);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t* r = receivers + (size_t)i * 8;
+        const uint32_t tile = tile_of[i];
+        if (r[3] >= 6u || tile >= n_tiles) continue;
+        const uint32_t* center = before.data() + (size_t)i * 16;
+        const f3 normal = face_normal(r[3]);
+        const int32_t tx = (int32_t)(tile % tiles_x), ty = (int32_t)(tile / tiles_x);
+        const float center_luminance = dot(w3(center), LUM);
+        float reference = center_luminance;
+        auto visit = [&](int32_t radius, auto&& body) {
+            for (int32_t y = -radius; y <= radius; ++y)
+                for (int32_t xx = -radius; xx <= radius; ++xx) {
+                    const int32_t qx = tx + xx, qy = ty + y;
+                    if (qx < 0 || qy < 0 || qx >= (int32_t)tiles_x || qy >= (int32_t)tiles_y) continue;
+                    for (uint32_t candidate : lists[(uint32_t)qy * tiles_x + (uint32_t)qx]) {
+                        if (candidate == i || !coplanar_donor(receivers, r, normal, candidate)) continue;
+                        body(before.data() + (size_t)candidate * 16);
+                    }
+                }
+        };
+        visit(1, [&](const uint32_t* value) {
+            if (bitsf(value[3]) > 0.0f) reference = wmax(reference, dot(w3(value), LUM));
+        });
+        const float center_variance = mean_variance(center, reference);
+        const float tolerance = display[0] * center_luminance;
+        const float tol2 = tolerance * tolerance;
+        const float deficit = center_variance / wmax(tol2, 1e-12f);
+        const int32_t radius = (int32_t)wclamp(std::ceil(std::sqrt(deficit / 3.14159f) * 0.5f), 1.0f, 4.0f);
+        const bool unsampled = bitsf(center[3]) <= 0.0f;
+        f3 sum{0, 0, 0};
+        float weight = 0.0f;
+        if (!unsampled) {
+            const float w = 1.0f / wmax(center_variance, 1e-12f);
+            sum = muls(w3(center), w);
+            weight = w;
+        }
+        if ((unsampled || center_variance > tol2) && display[1] > 0.0f) {
+            visit(radius, [&](const uint32_t* value) {
+                if (bitsf(value[3]) <= 0.0f) return;
+                const float variance = mean_variance(value, reference);
+                float bias2 = 0.0f;
+                if (!unsampled) {
+                    const float difference = dot(w3(value), LUM) - center_luminance;
+                    bias2 = wmax(difference * difference - variance - center_variance, 0.0f);
+                }
+                const float w = 1.0f / wmax(variance + bias2, 1e-12f);
+                sum = add(sum, muls(w3(value), w));
+                weight = weight + w;
+            });
+        }
+        if (weight <= 0.0f) continue;
+        const float keep = unsampled ? 0.0f : 1.0f - display[1];
+        const f3 desired = mix3(divs(sum, weight), w3(center), keep);
+        const float blend = bitsf(center[11]) > 0.0f ? display[2] : 1.0f;
+        const f3 shown = mix3(w3(center + 8), desired, blend);
+        uint32_t* out = estimates + (size_t)i * 16 + 8;
+        out[0] = fbits(shown.x); out[1] = fbits(shown.y); out[2] = fbits(shown.z); out[3] = fbits(1.0f);
+    }
+    // publish_view (voxel_view_runtime.wgsl:476-521)
+    for (int k = 0; k < 5; ++k) stats[k] = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t* r = receivers + (size_t)i * 8;
+        uint32_t* o = published + (size_t)i * 12;
+        std::fill(o, o + 12, 0u);
+        o[3] = 0xffffffffu;
+        if (r[3] >= 6u) continue;
+        const uint32_t* e = estimates + (size_t)i * 16;
+        f3 irradiance = w3(e + 8);
+        if (custom) irradiance = add(irradiance, direct_at(x, w3(r), face_normal(r[3])).custom);
+        const float count = bitsf(e[3]);
+        const bool lit = bitsf(e[11]) > 0.0f || irradiance.x > 0.0f || irradiance.y > 0.0f || irradiance.z > 0.0f;
+        const float evidence = lit ? wmax(count, 0.001f) : 0.0f;
+        o[0] = r[0]; o[1] = r[1]; o[2] = r[2]; o[3] = r[3];
+        o[4] = fbits(irradiance.x); o[5] = fbits(irradiance.y); o[6] = fbits(irradiance.z); o[7] = fbits(evidence);
+        for (uint32_t corner = 0; corner < 4u; ++corner) {
+            const uint32_t byte = (e[14] >> (corner * 8u)) & 255u;
+            o[8 + corner] = (byte & 15u) | ((byte & 128u) << 24u);
+        }
+        stats[0] += (uint32_t)count;
+        stats[1] = std::max(stats[1], (uint32_t)count);
+        if (count == 0.0f) stats[2] += 1;
+        if (evidence > 0.0f) stats[3] += 1;
+        if (conts[(size_t)i * 32 + 19] == 1u) stats[4] += 1;
+    }
+    return 0;
+}
+
+// corner_value (voxel_gi_presentation.wesl:353-361); value = rgb, w = weight.
+static f3 corner_value(F4 c, F4 eu, F4 ev, F4 diag) {
+    float sx = c.x * c.w + eu.x * eu.w + ev.x * ev.w;
+    float sy = c.y * c.w + eu.y * eu.w + ev.y * ev.w;
+    float sz = c.z * c.w + eu.z * eu.w + ev.z * ev.w;
+    float sw = c.w + eu.w + ev.w;
+    if (eu.w > 0.0f || ev.w > 0.0f) {
+        sx = sx + diag.x * diag.w;
+        sy = sy + diag.y * diag.w;
+        sz = sz + diag.z * diag.w;
+        sw = sw + diag.w;
+    }
+    const float d = wmax(sw, 0.000001f);
+    return f3{sx / d, sy / d, sz / d};
+}
+
+int orc_corner_value(const float* center, const float* edge_u, const float* edge_v, const float* diagonal, float* out3) {
+    const f3 v = corner_value(ld4(center), ld4(edge_u), ld4(edge_v), ld4(diagonal));
+    out3[0] = v.x; out3[1] = v.y; out3[2] = v.z;
+    return 0;
+}
+
+// corner_irradiance (voxel_gi_presentation.wesl:377-412) at each pixel's first hit.
+int orc_present(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
+                const uint32_t* published, uint32_t n, const float* cam, uint32_t w, uint32_t h, int corners, float* image, int threads) {
+    Geometry g = make_geometry(directory, slots, headers, cells, params);
+    Model m{params, nullptr, nullptr, nullptr, nullptr, nullptr, orc_pipeline{1, 0, 2048, 0, 1}};
+    std::unordered_map<uint64_t, uint32_t> index;  // (face, surface) -> published entry
+    auto key = [](uint32_t face, uint32_t a, uint32_t b, uint32_t c) {
+        uint64_t k = face;
+        k = k * 0x9e3779b97f4a7c15ull ^ a;
+        k = k * 0x9e3779b97f4a7c15ull ^ b;
+        return k * 0x9e3779b97f4a7c15ull ^ c;
+    };
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t* p = published + (size_t)i * 12;
+        if (p[3] < 6u) index.emplace(key(p[3], p[0], p[1], p[2]), i);
+    }
+    auto display_face = [&](i3 voxel, uint32_t face, int32_t s) -> F4 {
+        const f3 nrm = face_normal(face);
+        const f3 surface = add(f3{(float)voxel.x, (float)voxel.y, (float)voxel.z}, muls(adds(muls(nrm, 0.5f), 0.5f), (float)s));
+        auto it = index.find(key(face, fbits(surface.x), fbits(surface.y), fbits(surface.z)));
+        if (it == index.end()) return F4{0, 0, 0, 0};
+        const uint32_t* p = published + (size_t)it->second * 12;
+        if (p[3] != face || p[0] != fbits(surface.x) || p[1] != fbits(surface.y) || p[2] != fbits(surface.z)) return F4{0, 0, 0, 0};
+        return F4{bitsf(p[4]), bitsf(p[5]), bitsf(p[6]), wmin(bitsf(p[7]), 1.0f)};
+    };
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<uint32_t> next{0};
+    auto worker = [&]() {
+        Ctx x{g, m, Counters{}};
+        for (;;) {
+            const uint32_t id = next.fetch_add(1);
+            if (id >= w * h) break;
+            float* o = image + (size_t)id * 4;
+            const f3 eye{cam[0], cam[1], cam[2]};
+            const RayResult hit = trace_domain_limited(x, eye, camera_ray(cam, id % w, id / w, w, h), x.extra(1), true, 2048u);
+            if (hit.status != 1u) {
+                o[0] = o[1] = o[2] = o[3] = 0.0f;
+                continue;
+            }
+            const f3 position = hit.position, normal = hit.normal;
+            const f3 inner = sub(position, muls(normal, 0.01f));
+            const i3 cell{(int32_t)std::floor(inner.x), (int32_t)std::floor(inner.y), (int32_t)std::floor(inner.z)};
+            const int32_t s = far::voxel_stride(x, cell);
+            const i3 voxel{cell.x & -s, cell.y & -s, cell.z & -s};
+            uint32_t face = 0u;
+            i3 u{0, s, 0}, v{0, 0, s};
+            if (std::fabs(normal.y) > 0.5f) {
+                face = 2u;
+                u = i3{s, 0, 0};
+            } else if (std::fabs(normal.z) > 0.5f) {
+                face = 4u;
+                u = i3{s, 0, 0};
+                v = i3{0, s, 0};
+            }
+            const uint32_t axis = face / 2u;
+            face += (axis == 0u ? normal.x : (axis == 1u ? normal.y : normal.z)) < 0.0f ? 1u : 0u;
+            const F4 center = display_face(voxel, face, s);
+            if (!corners) {
+                o[0] = center.x; o[1] = center.y; o[2] = center.z; o[3] = center.w;
+                continue;
+            }
+            auto at = [&](int32_t du, int32_t dv) {
+                return display_face(i3{voxel.x + du * u.x + dv * v.x, voxel.y + du * u.y + dv * v.y, voxel.z + du * u.z + dv * v.z}, face, s);
+            };
+            const F4 left = at(-1, 0), right = at(1, 0), bottom = at(0, -1), top = at(0, 1);
+            const f3 c00 = corner_value(center, left, bottom, at(-1, -1));
+            const f3 c10 = corner_value(center, right, bottom, at(1, -1));
+            const f3 c01 = corner_value(center, left, top, at(-1, 1));
+            const f3 c11 = corner_value(center, right, top, at(1, 1));
+            const f3 local = divs(sub(position, f3{(float)voxel.x, (float)voxel.y, (float)voxel.z}), (float)(s * s));
+            const float ux = wclamp(dot(local, f3{(float)u.x, (float)u.y, (float)u.z}), 0.0f, 1.0f);
+            const float uy = wclamp(dot(local, f3{(float)v.x, (float)v.y, (float)v.z}), 0.0f, 1.0f);
+            const f3 rgb = recon::mix3(recon::mix3(c00, c10, ux), recon::mix3(c01, c11, ux), uy);
+            o[0] = rgb.x; o[1] = rgb.y; o[2] = rgb.z; o[3] = center.w;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    return 0;
+}
+
 // candidate keys only, for slots [controls[26], controls[27]).
 int orc_classify(const uint32_t* slot_meta, uint32_t* keys, uint32_t n_slots, const uint32_t* ctl) {
     for (uint32_t slot = ctl[26]; slot < ctl[27] && slot < n_slots; ++slot) keys[slot] = candidate_key(slot_meta, slot, ctl);

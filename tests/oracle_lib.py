@@ -54,6 +54,9 @@ _SIG = {
     "orc_footprints": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _U32, _P, _P]),
     "orc_discover": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P, _INT]),
     "orc_far_frame": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _P, _INT]),
+    "orc_reconstruct": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _U32, _U32, _P, _U32, _P, _P]),
+    "orc_corner_value": (_INT, [_P, _P, _P, _P, _P]),
+    "orc_present": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _P, _U32, _U32, _INT, _P, _INT]),
     "orc_classify": (_INT, [_P, _P, _U32, _P]),
     "orc_select": (_INT, [_P, _P, _P, _U32, _P, _P, _P, _P, _P]),
     "orc_trace_ray": (_INT, [_P, _U64, _P, _P, _P, _P, _U32, _U32, _P]),
@@ -271,6 +274,57 @@ class FarTier:
         assert rc == 0
         self.previous = (cam, frame & 0xFFFFFFFF)
         return current, self.output, stats
+
+
+def _geometry_args(geometry):
+    d, h, cl, _ = geometry
+    d = c(d, np.int32)
+    cl = c(cl, np.uint32) if len(cl) else np.zeros(1, np.uint32)
+    return d, c(h, np.uint32), cl
+
+
+def reconstruct(geometry, params, materials, lights, emitter_words, pipe, receivers, estimates, conts, tile_of, tiles_x, tiles_y,
+                display=(0.031, 1.0, 1.0), custom=False):
+    """orc_reconstruct: (estimates after, published (n, 12), counters (5,))."""
+    d, h, cl = _geometry_args(geometry)
+    lights = c(lights, np.float32).reshape(-1)
+    if lights.size == 0:
+        lights = np.zeros(12, np.float32)
+    est = np.array(estimates, np.uint32).reshape(-1, 16).copy()
+    n = est.shape[0]
+    published = np.zeros((n, 12), np.uint32)
+    stats = np.zeros(5, np.uint32)
+    rc = lib().orc_reconstruct(ptr(d), d.size // 4, ptr(h), ptr(cl), ptr(c(params, np.float32)), ptr(c(materials, np.float32)), ptr(lights),
+                               ptr(c(emitter_words, np.uint32)), ctypes.byref(pipe), ptr(c(receivers, np.uint32)), ptr(est),
+                               ptr(c(conts, np.uint32)), ptr(c(tile_of, np.uint32)), tiles_x, tiles_y, n,
+                               ptr(np.asarray(display, np.float32)), 1 if custom else 0, ptr(published), ptr(stats))
+    assert rc == 0
+    return est, published, stats
+
+
+def corner_value(center, edge_u=None, edge_v=None, diagonal=None):
+    """orc_corner_value on (rgb, weight) pairs; None = no face (weight 0)."""
+    def w(x):
+        if x is None:
+            return np.zeros(4, np.float32)
+        value, weight = x
+        rgb = np.broadcast_to(np.float32(value), 3) if np.ndim(value) == 0 else np.asarray(value, np.float32)
+        return np.array([*rgb, weight], np.float32)
+
+    out = np.zeros(3, np.float32)
+    lib().orc_corner_value(ptr(w(center)), ptr(w(edge_u)), ptr(w(edge_v)), ptr(w(diagonal)), ptr(out))
+    return out
+
+
+def present(geometry, params, published, eye, forward, up, tan_half_fov, width, height, corners=True, threads=0):
+    d, h, cl = _geometry_args(geometry)
+    p = c(published, np.uint32).reshape(-1, 12)
+    cam = np.array([*eye, *forward, *up, tan_half_fov], np.float32)
+    out = np.zeros((height, width, 4), np.float32)
+    rc = lib().orc_present(ptr(d), d.size // 4, ptr(h), ptr(cl), ptr(c(params, np.float32)), ptr(p if p.size else np.zeros(12, np.uint32)),
+                           p.shape[0], ptr(cam), width, height, 1 if corners else 0, ptr(out), threads)
+    assert rc == 0
+    return out
 
 
 # ---- model words ------------------------------------------------------------
