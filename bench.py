@@ -22,6 +22,8 @@ query kernel's tensor-core throughput.
 ``batched_scenes`` traces 32 seeded scenes of uneven size (32..256 voxels a
 side) both as separate per-scene frames and as batched frames (one
 traversal launch per stage over all scenes), from the same empty caches.
+``next_rows`` times headless discovery, a far-tier frame and the view
+receivers' frame, reconstruction and presentation at 1920x1080.
 ``--impl reference`` times the CPU oracle (the restatement of the
 reference's algorithm; the reference itself is Rust/WGSL and has no CPU
 path) on the box's host cores.
@@ -497,6 +499,80 @@ def batch_comparison(local, stream, flush, n_scenes, steps, warmup):
     }
 
 
+def next_rows(g, stream, steps=5):
+    """The rows either side of the frame, on the bench terrain at 1920x1080
+    from the cube-map camera's position: headless discovery (one primary ray
+    per pixel and the distinct faces), a far-tier frame at the reference's
+    default settings (8-pixel voxels, 2-pixel cells at 1080p, history 32,
+    rate 4, 128 steps), and the view receivers' frame, reconstruction and
+    presentation over the discovered faces. Discovery, view frames and
+    presentation are synchronous calls (host wall time, host sort and copies
+    included); far frames and reconstruction are timed with CUDA events."""
+    import torch
+    import vgi
+
+    w, h = 1920, 1080
+    fwd = np.asarray((0.5, -0.45, 0.6), np.float64)
+    cam = (EYE, (fwd / np.linalg.norm(fwd)).astype(np.float32), (0.0, 1.0, 0.0), 0.5774, w, h)
+
+    def wall(fn):
+        fn()
+        times = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            out = fn()
+            times.append(1000.0 * (time.perf_counter() - t0))
+        return float(statistics.median(times)), out
+
+    def events(fn):
+        fn()
+        torch.cuda.synchronize()
+        pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in pairs:
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        return float(statistics.median([a.elapsed_time(b) for a, b in pairs]))
+
+    out = {"camera": {"eye": list(EYE), "forward": [float(x) for x in cam[1]], "tan_half_fov": cam[3], "width": w, "height": h}}
+    ms, (pixels, faces) = wall(lambda: g.discover_faces(*cam))
+    out["discovery"] = {"ms": ms, "pixels": w * h, "faces": int(len(faces)), "rays_per_s": w * h / (ms * 1e-3)}
+
+    settings = vgi.FarTierSettings()
+    g.far_reset()
+    frame = [0]
+
+    def far():
+        g.far_frame(*cam, settings=settings, frame=frame[0])
+        frame[0] += 1
+
+    for _ in range(6):  # past the four warm-up traces: one trace in `rate` frames
+        far()
+    ms = events(far)
+    shape, _, _, stats = g.far_read()
+    cells = int(shape[0] * shape[1])
+    out["far_tier"] = {"ms": ms, "cells": cells, "owned": int(stats[0]), "traced": int(stats[1]), "cells_per_s": cells / (ms * 1e-3),
+                       "traced_paths_per_s": int(stats[1]) / (ms * 1e-3)}
+
+    g.view_set_receivers(faces)
+    gx, gy = w // 4, h // 4
+    g.view_set_tiles(vgi.witness_tiles(pixels, faces, gx, gy), (gx + 1) // 2, (gy + 1) // 2)
+    clock = [0]
+
+    def view():
+        g.view_frame(clock_ms=clock[0])
+        clock[0] += 16
+
+    ms_view, _ = wall(view)
+    ms_recon = events(lambda: g.view_reconstruct())
+    ms_present, _ = wall(lambda: g.view_present(*cam))
+    out["view"] = {"receivers": int(len(faces)), "frame_ms": ms_view, "reconstruct_ms": ms_recon, "present_ms": ms_present,
+                   "receivers_per_s": len(faces) / (ms_view * 1e-3)}
+    g.view_set_receivers(np.zeros((0, 5), np.int32))
+    return out
+
+
 def profile_mlp(frames=3):
     """A small MLP cache workload for ncu captures of the network kernels:
     the same generator at 256x256x256 voxels (64 emissive voxels), faces
@@ -548,6 +624,7 @@ def main():
     ap.add_argument("--no-mlp", action="store_true", help="skip the MLP cache comparison")
     ap.add_argument("--profile-mlp", action="store_true", help="only a small MLP cache workload, for ncu captures")
     ap.add_argument("--batch-scenes", type=int, default=32, help="scenes in the batched-scene comparison (0: skip it)")
+    ap.add_argument("--no-next-rows", action="store_true", help="skip discovery, far tier and reconstruction timings")
     args = ap.parse_args()
     if args.profile_mlp:
         profile_mlp()
@@ -704,6 +781,7 @@ def main():
         batched = None
         if args.batch_scenes > 0:
             batched = batch_comparison(local, stream, flush, args.batch_scenes, args.steps, args.warmup)
+        beside = None if args.no_next_rows else next_rows(g, stream)
         line = {
             "metric": METRIC,
             "value": total_rays / (total_ms * 1e-3),
@@ -743,6 +821,7 @@ def main():
             "relmse": quality,
             "mlp_cache": mlp,
             "batched_scenes": batched,
+            "next_rows": beside,
         }
         if base:
             line["cpu_baseline"] = base

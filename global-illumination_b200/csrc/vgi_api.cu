@@ -155,6 +155,13 @@ struct vgi_ctx {
     uint32_t v_hash_mask = 0;
     bool v_hash_valid = false;
     bool custom_lights = false;               // some light has custom visible RGB
+    // discovery and presentation scratch, kept between calls
+    DevBuf<float> disc_cam;
+    DevBuf<uint4> disc_pixels;
+    DevBuf<unsigned long long> disc_set;
+    DevBuf<int4> disc_list;
+    DevBuf<uint32_t> disc_counters;
+    DevBuf<float4> present_image;
     // reconstruction: screen tile per view receiver (CSR lists per tile),
     // the published FarPixels and the publish counters
     DevBuf<uint32_t> v_tile_of, v_tile_start, v_tile_items;
@@ -1179,11 +1186,11 @@ int vgi_discover_faces(vgi_ctx* c, const vgi_camera* cam, uint32_t* pixels8, vgi
     VGI_CUDA(c, cudaSetDevice(c->device));
     uint32_t mask = 1;
     while (mask < 2 * n) mask <<= 1;
-    DevBuf<float> dcam;
-    DevBuf<uint4> pixels;
-    DevBuf<unsigned long long> set;
-    DevBuf<int4> list;
-    DevBuf<uint32_t> counters;
+    DevBuf<float>& dcam = c->disc_cam;
+    DevBuf<uint4>& pixels = c->disc_pixels;
+    DevBuf<unsigned long long>& set = c->disc_set;
+    DevBuf<int4>& list = c->disc_list;
+    DevBuf<uint32_t>& counters = c->disc_counters;
     VGI_CUDA(c, dcam.reserve(10));
     VGI_CUDA(c, pixels.reserve(n * 2));
     VGI_CUDA(c, set.reserve(mask));
@@ -1825,8 +1832,8 @@ int vgi_view_present(vgi_ctx* c, const vgi_camera* cam, int corners, float* rgba
     const uint64_t n = (uint64_t)cam->width * cam->height;
     if (n == 0 || n > (1ull << 26)) return fail(c, VGI_ERR_INVALID, "camera size outside 1..2^26 pixels");
     VGI_CUDA(c, cudaSetDevice(c->device));
-    DevBuf<float> dcam;
-    DevBuf<float4> image;
+    DevBuf<float>& dcam = c->disc_cam;
+    DevBuf<float4>& image = c->present_image;
     VGI_CUDA(c, dcam.reserve(10));
     VGI_CUDA(c, image.reserve(n));
     const float host_cam[10] = {cam->eye[0], cam->eye[1], cam->eye[2], cam->forward[0], cam->forward[1], cam->forward[2],

@@ -63,19 +63,24 @@ def witness_tiles(pixels: np.ndarray, faces: np.ndarray, grid_x: int, grid_y: in
     seen. Tiles are ((grid_x + 1) // 2) x ((grid_y + 1) // 2)."""
     h, w = pixels.shape[:2]
     p = np.asarray(pixels, np.uint32).reshape(-1, 8)
+
+    def key(x, y, z, f):
+        m = np.uint64(0xFFFFF)
+        return ((x.astype(np.uint64) & m) | ((y.astype(np.uint64) & m) << np.uint64(20)) | ((z.astype(np.uint64) & m) << np.uint64(40))
+                | (f.astype(np.uint64) << np.uint64(60)))
+
     hit = np.nonzero(p[:, 3] < 6)[0]
-    seen = {}
-    for i in hit[::-1]:  # later pixels first, so the first pixel wins
-        seen[(int(p[i, 0]), int(p[i, 1]), int(p[i, 2]), int(p[i, 3]))] = int(i)
-    tiles_x = (grid_x + 1) // 2
-    out = np.full(len(faces), 0xFFFFFFFF, np.uint32)
-    for k, f in enumerate(np.asarray(faces, np.int32).reshape(-1, 5)):
-        i = seen.get((int(f[0]) & 0xFFFFFFFF, int(f[1]) & 0xFFFFFFFF, int(f[2]) & 0xFFFFFFFF, int(f[3])))
-        if i is None:
-            continue
-        cx = min((i % w) * grid_x // w, grid_x - 1)
-        cy = min((i // w) * grid_y // h, grid_y - 1)
-        out[k] = (cy // 2) * tiles_x + cx // 2
+    seen, first = np.unique(key(p[hit, 0], p[hit, 1], p[hit, 2], p[hit, 3]), return_index=True)
+    first = hit[first]  # np.unique keeps each key's first occurrence: the first pixel in raster order
+    f = np.asarray(faces, np.int32).reshape(-1, 5).view(np.uint32)
+    k = key(f[:, 0], f[:, 1], f[:, 2], f[:, 3])
+    at = np.minimum(np.searchsorted(seen, k), max(len(seen) - 1, 0))
+    found = (len(seen) > 0) & (seen[at] == k) if len(seen) else np.zeros(len(k), bool)
+    out = np.full(len(k), 0xFFFFFFFF, np.uint32)
+    i = first[at[found]]
+    cx = np.minimum((i % w) * grid_x // w, grid_x - 1)
+    cy = np.minimum((i // w) * grid_y // h, grid_y - 1)
+    out[found] = ((cy // 2) * ((grid_x + 1) // 2) + cx // 2).astype(np.uint32)
     return out
 
 
