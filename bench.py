@@ -53,10 +53,11 @@ METRIC = "rays/s and ms/frame at equal relMSE vs FP64 ref: MLP cache vs plain, 1
 WORKLOAD = "terrain 512x256x512 fBm, sun + 256 emissive voxels, faces facing a cube-map camera at (256,200,256), 8 spp, 2 bounces via world cache, FP32"
 
 
-def make_scene(seed):
+def make_scene(seed, regions=(32, 16, 32), eye=EYE):
     import vgi
 
-    coords, vox = vgi.terrain(32, 16, 32, seed=seed, octaves=4, period=64.0, base_height=128.0, falloff=400.0, emitters=256)
+    coords, vox = vgi.terrain(*regions, seed=seed, octaves=4, period=64.0, base_height=8.0 * regions[1], falloff=25.0 * regions[1],
+                              emitters=256)
     rng = np.random.default_rng(seed)
     m = vgi.VoxelGiMaterials()
     for k in range(8):
@@ -65,7 +66,7 @@ def make_scene(seed):
         r = float(rng.uniform(1.0, 10.0))
         m.set(8 + k, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5), emission=(r, r, r)))
     sun = vgi.DirectionalTransportLight((0.4, 0.8, 0.3), (3.0, 3.0, 3.0))
-    faces = vgi.exposed_faces(coords, vox, facing=EYE)
+    faces = vgi.exposed_faces(coords, vox, facing=eye)
     transport = vgi.TransportSettings(bounces=BOUNCES, path_steps=2048)
     return coords, vox, m.words(), sun.words(), faces, transport
 
@@ -499,7 +500,7 @@ def batch_comparison(local, stream, flush, n_scenes, steps, warmup):
     }
 
 
-def next_rows(g, stream, steps=5):
+def next_rows(g, stream, steps=5, eye=EYE):
     """The rows either side of the frame, on the bench terrain at 1920x1080
     from the cube-map camera's position: headless discovery (one primary ray
     per pixel and the distinct faces), a far-tier frame at the reference's
@@ -513,7 +514,7 @@ def next_rows(g, stream, steps=5):
 
     w, h = 1920, 1080
     fwd = np.asarray((0.5, -0.45, 0.6), np.float64)
-    cam = (EYE, (fwd / np.linalg.norm(fwd)).astype(np.float32), (0.0, 1.0, 0.0), 0.5774, w, h)
+    cam = (eye, (fwd / np.linalg.norm(fwd)).astype(np.float32), (0.0, 1.0, 0.0), 0.5774, w, h)
 
     def wall(fn):
         fn()
@@ -535,9 +536,11 @@ def next_rows(g, stream, steps=5):
         torch.cuda.synchronize()
         return float(statistics.median([a.elapsed_time(b) for a, b in pairs]))
 
-    out = {"camera": {"eye": list(EYE), "forward": [float(x) for x in cam[1]], "tan_half_fov": cam[3], "width": w, "height": h}}
+    out = {"camera": {"eye": list(eye), "forward": [float(x) for x in cam[1]], "tan_half_fov": cam[3], "width": w, "height": h}}
     ms, (pixels, faces) = wall(lambda: g.discover_faces(*cam))
-    out["discovery"] = {"ms": ms, "pixels": w * h, "faces": int(len(faces)), "rays_per_s": w * h / (ms * 1e-3)}
+    ms_faces, _ = wall(lambda: g.discover_faces(*cam, pixels=False))
+    out["discovery"] = {"ms": ms, "ms_faces_only": ms_faces, "pixels": w * h, "faces": int(len(faces)),
+                        "rays_per_s": w * h / (ms_faces * 1e-3)}
 
     settings = vgi.FarTierSettings()
     g.far_reset()
@@ -571,6 +574,30 @@ def next_rows(g, stream, steps=5):
                    "receivers_per_s": len(faces) / (ms_view * 1e-3)}
     g.view_set_receivers(np.zeros((0, 5), np.int32))
     return out
+
+
+def profile_next(small=False):
+    """Only the bench terrain (or, small, the same terrain at 256x128x256,
+    with the camera above it at (64, 160, 64) looking the same way) and one
+    pass of the next-row workload, for ncu captures of the discovery,
+    far-tier and reconstruction kernels."""
+    import torch
+    import vgi
+
+    eye = (64.0, 160.0, 64.0) if small else EYE
+    coords, vox, words, lights, faces, transport = make_scene(2, (16, 8, 16) if small else (32, 16, 32), eye)
+    g = vgi.GpuTracer(0)
+    g.upload_regions(coords, vox)
+    g.set_materials(words)
+    g.set_lights(lights, 1)
+    g.set_environment((0.0, 0.0, 0.0))
+    g.build_emitters()
+    g.set_transport(transport)
+    g.set_faces(faces)
+    g.frame(SPP, 0)
+    stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", 0))
+    print(json.dumps(next_rows(g, stream, steps=1, eye=eye)), flush=True)
+    g.close()
 
 
 def profile_mlp(frames=3):
@@ -625,9 +652,14 @@ def main():
     ap.add_argument("--profile-mlp", action="store_true", help="only a small MLP cache workload, for ncu captures")
     ap.add_argument("--batch-scenes", type=int, default=32, help="scenes in the batched-scene comparison (0: skip it)")
     ap.add_argument("--no-next-rows", action="store_true", help="skip discovery, far tier and reconstruction timings")
+    ap.add_argument("--profile-next", action="store_true", help="only the next-row workload once, for ncu captures")
+    ap.add_argument("--small", action="store_true", help="with --profile-next: the 256x128x256 terrain")
     args = ap.parse_args()
     if args.profile_mlp:
         profile_mlp()
+        return
+    if args.profile_next:
+        profile_next(args.small)
         return
     if args.warmup < 3:
         args.warmup = 3

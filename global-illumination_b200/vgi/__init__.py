@@ -696,20 +696,22 @@ class GpuTracer:
         self._check(self._lib.vgi_complete_batch(self._h, ticket))
 
     # headless discovery
-    def discover_faces(self, eye, forward, up, tan_half_fov: float, width: int, height: int, capacity: Optional[int] = None):
-        """Primary rays per pixel: (pixels (h, w, 8) u32 records, faces (n, 5)
-        rows voxel xyz, face, material). The default capacity, one face per
-        pixel, always suffices."""
+    def discover_faces(self, eye, forward, up, tan_half_fov: float, width: int, height: int, capacity: Optional[int] = None,
+                       pixels: bool = True):
+        """Primary rays per pixel: (pixels (h, w, 8) u32 records or None,
+        faces (n, 5) rows voxel xyz, face, material). The default capacity,
+        one face per pixel, always suffices."""
         capacity = width * height if capacity is None else capacity
         f = np.asarray(forward, np.float64)
         f = (f / np.linalg.norm(f)).astype(np.float32)
         cam = Camera((ctypes.c_float * 3)(*map(float, eye)), (ctypes.c_float * 3)(*map(float, f)),
                      (ctypes.c_float * 3)(*map(float, up)), float(tan_half_fov), width, height)
-        pixels = np.zeros((height, width, 8), np.uint32)
+        records = np.zeros((height, width, 8), np.uint32) if pixels else None
         faces = np.zeros((capacity, 5), np.int32)
         n = ctypes.c_uint32()
-        self._check(self._lib.vgi_discover_faces(self._h, ctypes.byref(cam), _ptr(pixels), _ptr(faces), capacity, ctypes.byref(n)))
-        return pixels, faces[: n.value].copy()
+        self._check(self._lib.vgi_discover_faces(self._h, ctypes.byref(cam), _ptr(records) if pixels else None, _ptr(faces), capacity,
+                                                 ctypes.byref(n)))
+        return records, faces[: n.value].copy()
 
     # reconstruction and presentation of the view receivers
     def view_set_tiles(self, tiles: np.ndarray, tiles_x: int, tiles_y: int) -> None:
