@@ -1426,36 +1426,72 @@ __device__ bool coplanar_donor(const ViewDisplay& D, uint4 r0, uint4 r1, V3 norm
 // reconstruct_view (voxel_view_runtime.wgsl:406-474): inverse-variance
 // weighting of coplanar donors in the screen tiles around the receiver's,
 // with the centre's bias bound, then a temporal blend of the shown value.
-// Tile lists are visited in receiver order.
+// One warp per receiver: lane l takes the window's tiles l, l + 32, ... in
+// row-major order (donors of a tile in receiver order) and keeps its own
+// partial sums; lane 0 adds the centre's term and then the lanes' partials
+// in lane order, so the sums have one fixed order.
+__device__ __forceinline__ float shfl_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = wmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
 __global__ void __launch_bounds__(128) reconstruct_kernel(const ViewDisplay D) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.n) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= D.n) return;  // whole warps
     const uint4 r0 = D.receivers[i * 2u], r1 = D.receivers[i * 2u + 1u];
     const uint32_t tile = D.tile_of[i];
     if (r0.w >= 6u || tile >= D.tiles_x * D.tiles_y) return;
-    const uint4 c_mean = D.estimates[i * 4u], c_moment = D.estimates[i * 4u + 1u], c_shown = D.estimates[i * 4u + 2u];
+    const uint4 c_mean = D.estimates[i * 4u], c_moment = D.estimates[i * 4u + 1u];
     const V3 normal = face_normal(r0.w);
     const int tx = (int)(tile % D.tiles_x), ty = (int)(tile / D.tiles_x);
     const float center_luminance = luminance(v3w(c_mean));
+    // The brightest sampled coplanar donor in the 3 x 3 tiles (a maximum: any order).
     float reference = center_luminance;
-    for (int y = -1; y <= 1; ++y)
-        for (int x = -1; x <= 1; ++x) {
-            const int qx = tx + x, qy = ty + y;
-            if (qx < 0 || qy < 0 || qx >= (int)D.tiles_x || qy >= (int)D.tiles_y) continue;
-            const uint32_t t = (uint32_t)qy * D.tiles_x + (uint32_t)qx;
-            for (uint32_t k = D.tile_start[t]; k < D.tile_start[t + 1u]; ++k) {
-                const uint32_t candidate = D.tile_items[k];
-                if (candidate == i || !coplanar_donor(D, r0, r1, normal, candidate)) continue;
-                const uint4 value = D.estimates[candidate * 4u];
-                if (__uint_as_float(value.w) > 0.0f) reference = wmax(reference, luminance(v3w(value)));
-            }
+    for (uint32_t k = lane; k < 9u; k += 32u) {
+        const int qx = tx + (int)(k % 3u) - 1, qy = ty + (int)(k / 3u) - 1;
+        if (qx < 0 || qy < 0 || qx >= (int)D.tiles_x || qy >= (int)D.tiles_y) continue;
+        const uint32_t t = (uint32_t)qy * D.tiles_x + (uint32_t)qx;
+        for (uint32_t j = D.tile_start[t]; j < D.tile_start[t + 1u]; ++j) {
+            const uint32_t candidate = D.tile_items[j];
+            if (candidate == i || !coplanar_donor(D, r0, r1, normal, candidate)) continue;
+            const uint4 value = D.estimates[candidate * 4u];
+            if (__uint_as_float(value.w) > 0.0f) reference = wmax(reference, luminance(v3w(value)));
         }
+    }
+    reference = shfl_max(reference);
     const float center_variance = mean_variance(c_mean, c_moment, reference);
     const float tolerance = __fmul_rn(D.display[0], center_luminance);
     const float tol2 = __fmul_rn(tolerance, tolerance);
     const float deficit = __fdiv_rn(center_variance, wmax(tol2, 1e-12f));
     const int radius = (int)wclamp(ceilf(__fmul_rn(__fsqrt_rn(__fdiv_rn(deficit, 3.14159f)), 0.5f)), 1.0f, 4.0f);
     const bool unsampled = __uint_as_float(c_mean.w) <= 0.0f;
+    V3 part{0.0f, 0.0f, 0.0f};
+    float part_w = 0.0f;
+    const bool gather = (unsampled || center_variance > tol2) && D.display[1] > 0.0f;
+    if (gather) {
+        const uint32_t side = 2u * (uint32_t)radius + 1u;
+        for (uint32_t k = lane; k < side * side; k += 32u) {
+            const int qx = tx + (int)(k % side) - radius, qy = ty + (int)(k / side) - radius;
+            if (qx < 0 || qy < 0 || qx >= (int)D.tiles_x || qy >= (int)D.tiles_y) continue;
+            const uint32_t t = (uint32_t)qy * D.tiles_x + (uint32_t)qx;
+            for (uint32_t j = D.tile_start[t]; j < D.tile_start[t + 1u]; ++j) {
+                const uint32_t candidate = D.tile_items[j];
+                if (candidate == i || !coplanar_donor(D, r0, r1, normal, candidate)) continue;
+                const uint4 value = D.estimates[candidate * 4u];
+                if (__uint_as_float(value.w) <= 0.0f) continue;
+                const float variance = mean_variance(value, D.estimates[candidate * 4u + 1u], reference);
+                float bias2 = 0.0f;
+                if (!unsampled) {
+                    const float difference = __fsub_rn(luminance(v3w(value)), center_luminance);
+                    bias2 = wmax(__fsub_rn(__fsub_rn(__fmul_rn(difference, difference), variance), center_variance), 0.0f);
+                }
+                const float w = __fdiv_rn(1.0f, wmax(__fadd_rn(variance, bias2), 1e-12f));
+                part = part + v3w(value) * w;
+                part_w = __fadd_rn(part_w, w);
+            }
+        }
+    }
     V3 sum{0.0f, 0.0f, 0.0f};
     float weight = 0.0f;
     if (!unsampled) {
@@ -1463,30 +1499,16 @@ __global__ void __launch_bounds__(128) reconstruct_kernel(const ViewDisplay D) {
         sum = v3w(c_mean) * w;
         weight = w;
     }
-    if ((unsampled || center_variance > tol2) && D.display[1] > 0.0f) {
-        for (int y = -radius; y <= radius; ++y)
-            for (int x = -radius; x <= radius; ++x) {
-                const int qx = tx + x, qy = ty + y;
-                if (qx < 0 || qy < 0 || qx >= (int)D.tiles_x || qy >= (int)D.tiles_y) continue;
-                const uint32_t t = (uint32_t)qy * D.tiles_x + (uint32_t)qx;
-                for (uint32_t k = D.tile_start[t]; k < D.tile_start[t + 1u]; ++k) {
-                    const uint32_t candidate = D.tile_items[k];
-                    if (candidate == i || !coplanar_donor(D, r0, r1, normal, candidate)) continue;
-                    const uint4 value = D.estimates[candidate * 4u];
-                    if (__uint_as_float(value.w) <= 0.0f) continue;
-                    const float variance = mean_variance(value, D.estimates[candidate * 4u + 1u], reference);
-                    float bias2 = 0.0f;
-                    if (!unsampled) {
-                        const float difference = __fsub_rn(luminance(v3w(value)), center_luminance);
-                        bias2 = wmax(__fsub_rn(__fsub_rn(__fmul_rn(difference, difference), variance), center_variance), 0.0f);
-                    }
-                    const float w = __fdiv_rn(1.0f, wmax(__fadd_rn(variance, bias2), 1e-12f));
-                    sum = sum + v3w(value) * w;
-                    weight = __fadd_rn(weight, w);
-                }
-            }
+    if (gather) {
+        for (uint32_t l = 0; l < 32u; ++l) {
+            const V3 p{__shfl_sync(0xffffffffu, part.x, l), __shfl_sync(0xffffffffu, part.y, l), __shfl_sync(0xffffffffu, part.z, l)};
+            const float pw = __shfl_sync(0xffffffffu, part_w, l);
+            sum = sum + p;
+            weight = __fadd_rn(weight, pw);
+        }
     }
-    if (weight <= 0.0f) return;
+    if (lane != 0u || weight <= 0.0f) return;
+    const uint4 c_shown = D.estimates[i * 4u + 2u];
     const float keep = unsampled ? 0.0f : __fsub_rn(1.0f, D.display[1]);
     const V3 desired = (sum / weight) * __fsub_rn(1.0f, keep) + v3w(c_mean) * keep;
     const float blend = __uint_as_float(c_shown.w) > 0.0f ? D.display[2] : 1.0f;
@@ -1630,7 +1652,7 @@ __global__ void __launch_bounds__(128) present_kernel(const TraceArgs A, const V
 void launch_reconstruct(const TraceArgs& a, const ViewDisplay& d, bool limited, bool budgeted, cudaStream_t s) {
     if (d.n == 0) return;
     const uint32_t blocks = (d.n + 127) / 128;
-    reconstruct_kernel<<<blocks, 128, 0, s>>>(d);
+    reconstruct_kernel<<<(d.n + 3) / 4, 128, 0, s>>>(d);  // a warp per receiver
     if (limited) {
         if (budgeted) publish_kernel<true, true><<<blocks, 128, 0, s>>>(a, d);
         else publish_kernel<true, false><<<blocks, 128, 0, s>>>(a, d);

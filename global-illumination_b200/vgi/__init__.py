@@ -706,8 +706,8 @@ class GpuTracer:
         f = (f / np.linalg.norm(f)).astype(np.float32)
         cam = Camera((ctypes.c_float * 3)(*map(float, eye)), (ctypes.c_float * 3)(*map(float, f)),
                      (ctypes.c_float * 3)(*map(float, up)), float(tan_half_fov), width, height)
-        records = np.zeros((height, width, 8), np.uint32) if pixels else None
-        faces = np.zeros((capacity, 5), np.int32)
+        records = np.empty((height, width, 8), np.uint32) if pixels else None
+        faces = np.empty((capacity, 5), np.int32)  # the library writes the first n rows
         n = ctypes.c_uint32()
         self._check(self._lib.vgi_discover_faces(self._h, ctypes.byref(cam), _ptr(records) if pixels else None, _ptr(faces), capacity,
                                                  ctypes.byref(n)))

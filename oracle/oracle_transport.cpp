@@ -1683,18 +1683,20 @@ int orc_reconstruct(const int32_t* directory, uint64_t slots, const uint32_t* he
         const int32_t tx = (int32_t)(tile % tiles_x), ty = (int32_t)(tile / tiles_x);
         const float center_luminance = dot(w3(center), LUM);
         float reference = center_luminance;
+        // body(lane, donor): the window's tiles in row-major order, tile k
+        // belonging to lane k mod 32 (the GPU's warp split).
         auto visit = [&](int32_t radius, auto&& body) {
-            for (int32_t y = -radius; y <= radius; ++y)
-                for (int32_t xx = -radius; xx <= radius; ++xx) {
-                    const int32_t qx = tx + xx, qy = ty + y;
-                    if (qx < 0 || qy < 0 || qx >= (int32_t)tiles_x || qy >= (int32_t)tiles_y) continue;
-                    for (uint32_t candidate : lists[(uint32_t)qy * tiles_x + (uint32_t)qx]) {
-                        if (candidate == i || !coplanar_donor(receivers, r, normal, candidate)) continue;
-                        body(before.data() + (size_t)candidate * 16);
-                    }
+            const int32_t side = 2 * radius + 1;
+            for (int32_t k = 0; k < side * side; ++k) {
+                const int32_t qx = tx + k % side - radius, qy = ty + k / side - radius;
+                if (qx < 0 || qy < 0 || qx >= (int32_t)tiles_x || qy >= (int32_t)tiles_y) continue;
+                for (uint32_t candidate : lists[(uint32_t)qy * tiles_x + (uint32_t)qx]) {
+                    if (candidate == i || !coplanar_donor(receivers, r, normal, candidate)) continue;
+                    body(k % 32, before.data() + (size_t)candidate * 16);
                 }
+            }
         };
-        visit(1, [&](const uint32_t* value) {
+        visit(1, [&](int32_t, const uint32_t* value) {
             if (bitsf(value[3]) > 0.0f) reference = wmax(reference, dot(w3(value), LUM));
         });
         const float center_variance = mean_variance(center, reference);
@@ -1711,7 +1713,13 @@ int orc_reconstruct(const int32_t* directory, uint64_t slots, const uint32_t* he
             weight = w;
         }
         if ((unsampled || center_variance > tol2) && display[1] > 0.0f) {
-            visit(radius, [&](const uint32_t* value) {
+            f3 part[32];
+            float part_w[32];
+            for (int l = 0; l < 32; ++l) {
+                part[l] = f3{0, 0, 0};
+                part_w[l] = 0.0f;
+            }
+            visit(radius, [&](int32_t lane, const uint32_t* value) {
                 if (bitsf(value[3]) <= 0.0f) return;
                 const float variance = mean_variance(value, reference);
                 float bias2 = 0.0f;
@@ -1720,9 +1728,13 @@ int orc_reconstruct(const int32_t* directory, uint64_t slots, const uint32_t* he
                     bias2 = wmax(difference * difference - variance - center_variance, 0.0f);
                 }
                 const float w = 1.0f / wmax(variance + bias2, 1e-12f);
-                sum = add(sum, muls(w3(value), w));
-                weight = weight + w;
+                part[lane] = add(part[lane], muls(w3(value), w));
+                part_w[lane] = part_w[lane] + w;
             });
+            for (int l = 0; l < 32; ++l) {
+                sum = add(sum, part[l]);
+                weight = weight + part_w[l];
+            }
         }
         if (weight <= 0.0f) continue;
         const float keep = unsampled ? 0.0f : 1.0f - display[1];
