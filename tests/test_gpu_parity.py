@@ -25,10 +25,11 @@ class Case:
         self.transport = transport or vgi.TransportSettings()
         self.faces = vgi.exposed_faces(self.coords, self.vox) if faces is None else faces
         self.emitters, self.n_emit, self.total = vgi.host_emitters(self.coords, self.vox, self.materials)
+        self.strides = None  # per-region stride log2 (coarse pages), or None
 
     def load(self, g: vgi.GpuTracer, with_faces=True, layout=vgi.GpuTracer.WAVEFRONT):
         g.set_layout(layout)
-        g.upload_regions(self.coords, self.vox)
+        g.upload_regions(self.coords, self.vox, self.strides)
         g.set_materials(self.materials)
         g.set_lights(self.lights, self.n_directional)
         g.set_environment(self.env)
