@@ -743,26 +743,36 @@ int vgi_edit_voxels(vgi_ctx* c, const int32_t* edits, uint32_t n) {
     if (!c || (n && !edits)) return VGI_ERR_INVALID;
     if (!c->geometry || c->keys.empty()) return fail(c, VGI_ERR_STATE, "edits need geometry uploaded as regions");
     VGI_CUDA(c, cudaSetDevice(c->device));
-    std::vector<uint2> packed;
-    packed.reserve(n);
+    for (uint32_t e = 0; e < n; ++e)
+        if (edits[e * 4 + 3] < 0 || edits[e * 4 + 3] > 256) return fail(c, VGI_ERR_INVALID, "voxel value outside 0..256");
+    std::vector<uint64_t> touched;  // region << 16 | voxel within it
+    touched.reserve(n);
     std::vector<uint32_t> dirty;
     std::vector<uint8_t> was_blocked(c->keys.size(), 2);
+    // Edits apply in order, so a voxel edited twice keeps its last value
+    // (the host copy); the device scatter then writes each voxel once.
     for (uint32_t e = 0; e < n; ++e) {
         int32_t x = edits[e * 4], y = edits[e * 4 + 1], z = edits[e * 4 + 2];
-        int32_t value = edits[e * 4 + 3];
-        if (value < 0 || value > 256) return fail(c, VGI_ERR_INVALID, "voxel value outside 0..256");
         auto it = c->where.find(RegionKey{x >> 4, y >> 4, z >> 4});
         if (it == c->where.end()) continue;
         uint32_t r = it->second;
         uint32_t local = (uint32_t)((x & 15) + 16 * ((y & 15) + 16 * (z & 15)));
-        c->host_voxels[(size_t)r * 4096 + local] = (uint16_t)value;
-        packed.push_back(make_uint2(r, (local << 16) | (uint32_t)value));
+        c->host_voxels[(size_t)r * 4096 + local] = (uint16_t)edits[e * 4 + 3];
+        touched.push_back(((uint64_t)r << 16) | local);
         if (was_blocked[r] == 2) {
             was_blocked[r] = c->host_headers[r].x != 1u ? 1 : 0;
             dirty.push_back(r);
         }
     }
-    if (packed.empty()) return VGI_OK;
+    if (touched.empty()) return VGI_OK;
+    std::sort(touched.begin(), touched.end());
+    touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+    std::vector<uint2> packed;
+    packed.reserve(touched.size());
+    for (uint64_t k : touched) {
+        const uint32_t r = (uint32_t)(k >> 16), local = (uint32_t)(k & 0xffffu);
+        packed.push_back(make_uint2(r, (local << 16) | (uint32_t)c->host_voxels[(size_t)r * 4096 + local]));
+    }
     VGI_CUDA(c, c->edit_buf.reserve(packed.size()));
     VGI_CUDA(c, cudaMemcpyAsync(c->edit_buf.ptr, packed.data(), packed.size() * sizeof(uint2), cudaMemcpyHostToDevice, c->stream));
     launch_scatter_edits(c->edit_buf.ptr, (uint32_t)packed.size(), c->voxels.ptr, c->stream);

@@ -4,6 +4,7 @@ results and state must be bit-identical to its own frames."""
 import numpy as np
 import pytest
 
+import oracle_lib as O
 import vgi
 from test_gpu_parity import assert_words_equal, terrain_case
 
@@ -87,3 +88,66 @@ def test_batch_rejects_mixed_transport(tracers):
     finally:
         batch.close()
         tracers[1].set_transport(cases[1].transport)
+
+
+def edit_stream(case, rng, mean=4.0):
+    """One frame's edits for a scene, as the batched workload makes them:
+    a Poisson(mean) number (1..512) of spheres of radius 1-5 at random
+    surface voxels, carving air or placing an albedo material, inside the
+    scene; one retention event per sphere over its box."""
+    from test_gpu_parity import encode_events
+
+    size = (case.coords.max(0) + 1) * 16
+    k = int(np.clip(rng.poisson(mean), 1, 512))
+    edits, events = [], []
+    for row in case.faces[rng.integers(0, len(case.faces), k)]:
+        c = row[:3].astype(np.int64)
+        r = int(rng.integers(1, 6))
+        value = 256 if rng.random() < 0.5 else int(rng.integers(0, 8))
+        for dz in range(-r, r + 1):
+            for dy in range(-r, r + 1):
+                for dx in range(-r, r + 1):
+                    p = c + (dx, dy, dz)
+                    if dx * dx + dy * dy + dz * dz <= r * r and np.all(p >= 0) and np.all(p < size):
+                        edits.append((*p, value))
+        lo, hi = np.maximum(c - r, 0), np.minimum(c + r, size - 1)
+        events.append((lo, hi, [(lo, hi, 40.0, 3)]))
+    words, n = encode_events(events)
+    return np.array(edits, np.int32), words, n
+
+
+def test_batched_frames_with_edit_streams_equal_own_frames(tracers):
+    cases = scenes(measured_retention=1.0)
+    rng = np.random.default_rng(21)
+    streams = [[edit_stream(case, rng) for _ in range(5)] for case in cases]
+    want = []
+    for t, case, stream in zip(tracers, cases, streams):
+        case.load(t)
+        for f, (edits, words, n) in enumerate(stream):
+            t.edit_voxels(edits)
+            t.apply_events(words, n)
+            t.frame(8, clock_ms=16 * f)
+        want.append((t.read_results(), t.read_state(), t.geometry()))
+    for t, case in zip(tracers, cases):
+        case.load(t)
+    batch = vgi.GpuBatch(tracers)
+    try:
+        batch.set_graph(True)  # edits between frames must drop or keep the captured graph correctly
+        for f in range(5):
+            for t, stream in zip(tracers, streams):
+                edits, words, n = stream[f]
+                t.edit_voxels(edits)
+                t.apply_events(words, n)
+            batch.frame(8, clock_ms=16 * f)
+        batch.sync()
+        for k, (t, (results, state, geometry)) in enumerate(zip(tracers, want)):
+            # The packing's cell offsets depend on the context's history; the
+            # canonical form (per region, independent of layout) must agree.
+            d, h, cl, _ = t.geometry()
+            wd, wh, wcl, _ = geometry
+            coords = cases[k].coords
+            assert_words_equal(O.canonical(d, h, cl, coords), O.canonical(wd, wh, wcl, coords), f"scene {k} geometry")
+            assert_words_equal(t.read_results(), results, f"scene {k} results")
+            assert_words_equal(t.read_state(), state, f"scene {k} state")
+    finally:
+        batch.close()

@@ -91,3 +91,22 @@ def test_invalid_inputs_are_refused(gpu):
     gpu.frame(8)
     ref.frame(8)
     assert_words_equal(gpu.read_results(), ref.results, "frame after refused calls")
+
+
+def test_repeated_voxel_edits_keep_the_last_value(gpu):
+    """Edits apply in order (VoxelGiInput::edit_voxel): a voxel edited twice
+    in one list keeps its last value, as the oracle's in-order edits do."""
+    case = terrain_case()
+    case.load(gpu, with_faces=False)
+    ref = O.Scene(case.coords, case.vox, top_mode=0)
+    rng = np.random.default_rng(8)
+    block = [(x, y, z) for x in range(30, 38) for y in range(20, 36) for z in range(40, 48)]
+    edits = [(x, y, z, 256) for x, y, z in block] + [(x, y, z, int(rng.integers(0, 8))) for x, y, z in block]
+    edits += [(x, y, z, 256) for x, y, z in block[::3]]
+    # Shuffled, so a voxel's edits are far apart in the list; both sides apply the list in order.
+    edits = np.array(edits, np.int32)[rng.permutation(len(edits))]
+    gpu.edit_voxels(edits)
+    ref.edit(edits)
+    d, h, cl, _ = gpu.geometry()
+    rd, rh, rcl, _ = ref.arrays()
+    assert_words_equal(O.canonical(d, h, cl, case.coords), O.canonical(rd, rh, rcl, case.coords), "geometry after repeated edits")
