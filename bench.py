@@ -19,7 +19,7 @@ empty cache and an untrained network until its relMSE against the FP64
 reference reaches the plain trace's (after the plain run's frames), and
 reports both forms' ms/frame, rays/s and time to that relMSE, with the
 query kernel's tensor-core throughput.
-``batched_scenes`` traces 32 seeded scenes of uneven size (32..256 voxels a
+``batched_scenes`` traces 64 seeded scenes of uneven size (32..256 voxels a
 side) both as separate per-scene frames and as batched frames (one
 traversal launch per stage over all scenes), from the same empty caches.
 ``next_rows`` times headless discovery, a far-tier frame and the view
@@ -650,7 +650,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default layout (for profiling runs)")
     ap.add_argument("--no-mlp", action="store_true", help="skip the MLP cache comparison")
     ap.add_argument("--profile-mlp", action="store_true", help="only a small MLP cache workload, for ncu captures")
-    ap.add_argument("--batch-scenes", type=int, default=32, help="scenes in the batched-scene comparison (0: skip it)")
+    ap.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-scene comparison (0: skip it)")
     ap.add_argument("--no-next-rows", action="store_true", help="skip discovery, far tier and reconstruction timings")
     ap.add_argument("--profile-next", action="store_true", help="only the next-row workload once, for ncu captures")
     ap.add_argument("--small", action="store_true", help="with --profile-next: the 256x128x256 terrain")

@@ -3,6 +3,7 @@
 #include "../../include/vgi_scenes.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -146,6 +147,97 @@ void vgi_scene_terrain(const vgi_terrain_params* p, uint32_t nx, uint32_t ny, ui
         if (cell != 256) continue;
         cell = (uint16_t)(8 + placed % 248);
         ++placed;
+    }
+}
+
+void vgi_scene_cave(const vgi_cave_params* p, uint32_t nx, uint32_t ny, uint32_t nz, uint16_t* voxels) {
+    const int32_t X = (int32_t)nx * 16, Y = (int32_t)ny * 16, Z = (int32_t)nz * 16;
+    const uint32_t seed = p->seed;
+    auto at = [&](int32_t x, int32_t y, int32_t z) -> uint16_t& {
+        const uint32_t region = (uint32_t)(x >> 4) + nx * ((uint32_t)(y >> 4) + ny * (uint32_t)(z >> 4));
+        return voxels[region_voxel(region, x & 15, y & 15, z & 15)];
+    };
+    // Rock with materials from a coarse field.
+    parallel_for((uint32_t)Z, [&](uint32_t z) {
+        for (int32_t y = 0; y < Y; ++y)
+            for (int32_t x = 0; x < X; ++x) {
+                const float v = value_noise(seed ^ 0x5bd1e995u, (float)x * (1.0f / 48.0f), (float)y * (1.0f / 24.0f), (float)z * (1.0f / 48.0f));
+                at(x, y, (int32_t)z) = (uint16_t)std::min(7, std::max(0, (int32_t)std::floor((v + 1.0f) * 4.0f)));
+            }
+    });
+    const int32_t ceiling = Y - (int32_t)p->roof;  // tunnels stay below it
+    auto carve = [&](float cx, float cy, float cz, float r, int32_t y_max) {
+        const int32_t x0 = std::max(0, (int32_t)std::floor(cx - r)), x1 = std::min(X - 1, (int32_t)std::ceil(cx + r));
+        const int32_t y0 = std::max(1, (int32_t)std::floor(cy - r)), y1 = std::min(y_max - 1, (int32_t)std::ceil(cy + r));
+        const int32_t z0 = std::max(0, (int32_t)std::floor(cz - r)), z1 = std::min(Z - 1, (int32_t)std::ceil(cz + r));
+        for (int32_t z = z0; z <= z1; ++z)
+            for (int32_t y = y0; y <= y1; ++y)
+                for (int32_t x = x0; x <= x1; ++x) {
+                    const float dx = (float)x + 0.5f - cx, dy = (float)y + 0.5f - cy, dz = (float)z + 0.5f - cz;
+                    if (dx * dx + dy * dy + dz * dz <= r * r) at(x, y, z) = 256;
+                }
+    };
+    uint32_t state = host_pcg(seed ^ 0x68e31da4u);
+    auto uniform = [&]() {
+        state = host_pcg(state + 0x9e3779b9u);
+        return (float)(state >> 8) * (1.0f / 16777216.0f);
+    };
+    // Skylight shafts through the roof.
+    std::vector<std::array<float, 2>> shafts;
+    for (uint32_t k = 0; k < p->skylights; ++k) {
+        const float sx = p->skylight_radius + uniform() * ((float)X - 2.0f * p->skylight_radius);
+        const float sz = p->skylight_radius + uniform() * ((float)Z - 2.0f * p->skylight_radius);
+        shafts.push_back({sx, sz});
+        for (int32_t y = ceiling - (int32_t)p->radius_max; y < Y; ++y) carve(sx, (float)y + 0.5f, sz, p->skylight_radius, Y + 1);
+    }
+    // Worm tunnels.
+    const float span = p->radius_max - p->radius_min;
+    for (uint32_t w = 0; w < p->worms; ++w) {
+        const uint32_t ws = host_pcg(seed + 0x1000u * (w + 1u));
+        float px, py, pz;
+        if (w < shafts.size()) {
+            px = shafts[w][0];
+            pz = shafts[w][1];
+            py = (float)ceiling - p->radius_max;
+        } else {
+            px = uniform() * (float)X;
+            pz = uniform() * (float)Z;
+            py = p->radius_max + 1.0f + uniform() * std::max(1.0f, (float)ceiling - 2.0f * p->radius_max - 2.0f);
+        }
+        float yaw = uniform() * 6.2831853f, pitch = 0.0f;
+        for (uint32_t t = 0; t < p->steps; ++t) {
+            const float r = p->radius_min + span * (0.5f + 0.5f * value_noise(ws, (float)t * 0.05f, 0.5f, 0.5f));
+            carve(px, py, pz, r, ceiling);
+            yaw += 0.35f * value_noise(ws ^ 0x27d4eb2du, (float)t * 0.1f, 1.5f, 0.5f);
+            pitch = 0.3f * value_noise(ws ^ 0x165667b1u, (float)t * 0.07f, 2.5f, 0.5f);
+            const float step = std::max(1.0f, 0.5f * r);
+            px += step * std::cos(pitch) * std::cos(yaw);
+            pz += step * std::cos(pitch) * std::sin(yaw);
+            py += step * std::sin(pitch);
+            // Reflect at the sides; stay between the floor and the roof.
+            if (px < 0.0f || px >= (float)X) {
+                yaw = 3.14159265f - yaw;
+                px = std::min(std::max(px, 0.0f), (float)X - 1.0f);
+            }
+            if (pz < 0.0f || pz >= (float)Z) {
+                yaw = -yaw;
+                pz = std::min(std::max(pz, 0.0f), (float)Z - 1.0f);
+            }
+            py = std::min(std::max(py, r + 1.0f), std::max(r + 1.0f, (float)ceiling - r - 1.0f));
+        }
+    }
+    // Emitters on tunnel floors: the lowest air voxel above rock in a random column.
+    uint32_t placed = 0;
+    for (uint32_t attempt = 0; attempt < p->emitters * 64 && placed < p->emitters; ++attempt) {
+        const int32_t x = (int32_t)(uniform() * (float)X), z = (int32_t)(uniform() * (float)Z);
+        if (x >= X || z >= Z) continue;
+        for (int32_t y = 1; y < ceiling; ++y) {
+            if (at(x, y, z) == 256 && at(x, y - 1, z) != 256) {
+                at(x, y, z) = (uint16_t)(8 + (placed & 1u));
+                ++placed;
+                break;
+            }
+        }
     }
 }
 

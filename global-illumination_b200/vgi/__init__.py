@@ -260,6 +260,7 @@ _SIGNATURES = {
     "vgi_submit_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P, _P]),
     "vgi_frame_scheduled": (_INT, [_P, _U32, _U32, _P]),
     "vgi_discover_faces": (_INT, [_P, _P, _P, _P, _U32, _P]),
+    "vgi_scene_cave": (None, [_P, _U32, _U32, _U32, _P]),
     "vgi_far_frame": (_INT, [_P, _P, _P, _U32]),
     "vgi_far_read": (_INT, [_P, _P, _P, _P, _P]),
     "vgi_far_reset": (_INT, [_P]),
@@ -872,6 +873,21 @@ def terrain(nx: int, ny: int, nz: int, seed: int = 2, octaves: int = 4, period: 
     p = TerrainParams(seed, octaves, period, base_height, falloff, emitters)
     vox = np.zeros(nx * ny * nz * 4096, np.uint16)
     library().vgi_scene_terrain(ctypes.byref(p), nx, ny, nz, _ptr(vox))
+    return grid_coords(nx, ny, nz), vox
+
+
+class CaveParams(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint32), ("worms", ctypes.c_uint32), ("steps", ctypes.c_uint32), ("radius_min", ctypes.c_float),
+                ("radius_max", ctypes.c_float), ("roof", ctypes.c_uint32), ("skylights", ctypes.c_uint32),
+                ("skylight_radius", ctypes.c_float), ("emitters", ctypes.c_uint32)]
+
+
+def cave(nx: int, ny: int, nz: int, seed: int = 1, worms: int = 40, steps: int = 600, radius_min: float = 3.0, radius_max: float = 12.0,
+         roof: int = 16, skylights: int = 16, skylight_radius: float = 6.0, emitters: int = 2000):
+    """The worm-tunnel cave (vgi_scene_cave): (coords, voxels)."""
+    p = CaveParams(seed, worms, steps, radius_min, radius_max, roof, skylights, skylight_radius, emitters)
+    vox = np.zeros(nx * ny * nz * 4096, np.uint16)
+    library().vgi_scene_cave(ctypes.byref(p), nx, ny, nz, _ptr(vox))
     return grid_coords(nx, ny, nz), vox
 
 

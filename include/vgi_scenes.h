@@ -41,6 +41,27 @@ typedef struct {
 } vgi_terrain_params;
 void vgi_scene_terrain(const vgi_terrain_params* p, uint32_t nx, uint32_t ny, uint32_t nz, uint16_t* voxels);
 
+/* Cave: solid rock (materials 0..7 by a coarse noise field) carved by
+ * `worms` seeded worm tunnels, random walks steered by value noise whose
+ * radius varies along the walk in [radius_min, radius_max], under a solid
+ * roof `roof` voxels thick. `skylights` vertical shafts of radius
+ * `skylight_radius` cut through the roof, and the first tunnels start under
+ * them. `emitters` emissive voxels sit on tunnel floors, alternately
+ * material 8 (green) and 9 (orange). Region grid nx x ny x nz in (z, y, x)
+ * order. */
+typedef struct {
+    uint32_t seed;
+    uint32_t worms;
+    uint32_t steps;
+    float radius_min;
+    float radius_max;
+    uint32_t roof;
+    uint32_t skylights;
+    float skylight_radius;
+    uint32_t emitters;
+} vgi_cave_params;
+void vgi_scene_cave(const vgi_cave_params* p, uint32_t nx, uint32_t ny, uint32_t nz, uint16_t* voxels);
+
 /* Exposed faces: a face of a solid voxel whose neighbour is loaded air.
  * Optional filters: a square frustum (eye xyz, forward xyz, half-angle
  * tangent) on the face centre with the face turned towards the eye; or, with
