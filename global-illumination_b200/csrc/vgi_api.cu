@@ -181,6 +181,7 @@ struct vgi_ctx {
     float far_prev[10] = {};
     uint32_t far_last_frame = 0;
     bool far_has_prev = false;
+    bool far_handoff = false;                 // view frames seed new receivers from far cells
     DevBuf<uint4> events;
     DevBuf<int4> footprints;                 // change-footprint tasks of the last event list
     DevBuf<uint32_t> footprint_sums;
@@ -1714,6 +1715,12 @@ int vgi_far_frame(vgi_ctx* c, const vgi_camera* cam, const vgi_far_settings* set
     return VGI_OK;
 }
 
+int vgi_set_far_handoff(vgi_ctx* c, int enable) {
+    if (!c) return VGI_ERR_INVALID;
+    c->far_handoff = enable != 0;
+    return VGI_OK;
+}
+
 int vgi_far_reset(vgi_ctx* c) {
     if (!c) return VGI_ERR_INVALID;
     // A new camera's state: zeroed histories and output (the stale cells a
@@ -1886,6 +1893,22 @@ int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events
     }
     v.events = c->v_events.ptr;
     v.n_events = n_events;
+    if (c->far_handoff && c->far_has_prev && (c->far_shape[3] & 1u)) {
+        // The last far frame's cells, seen from its camera.
+        FarView& f = v.far;
+        std::copy(c->far_prev, c->far_prev + 10, f.cam);
+        std::copy(c->far_prev, c->far_prev + 10, f.prev);
+        f.width = c->far_size[0];
+        f.height = c->far_size[1];
+        std::copy(c->far_shape, c->far_shape + 4, f.grid);
+        std::memcpy(&f.tune[3], &c->far_last_frame, 4);
+        f.axis[0] = c->far_prev[3];
+        f.axis[1] = c->far_prev[4];
+        f.axis[2] = c->far_prev[5];
+        f.axis[3] = (1.0f / c->far_prev[9]) * (float)c->far_size[1] * 0.5f;
+        v.far_cells = c->far_cells[c->far_current].ptr;
+        v.far_stats = c->far_stats.ptr;
+    }
     launch_view_frame(v, transport_limited(c), c->transport.budgeted != 0, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));

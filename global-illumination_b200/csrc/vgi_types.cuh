@@ -122,45 +122,6 @@ void launch_wave_batch(const WaveScene* scenes, uint32_t n, const void* device_a
                        const BatchStreams& st, const AccumArgs* acc, cudaGraphNode_t* prepare_nodes, cudaGraphNode_t* accumulate_nodes);
 
 // The view tier's buffers and controls (vgi_view.cuh) for n receivers.
-struct ViewArgs {
-    TraceArgs t;
-    uint4* receivers;      // 2 per receiver: surface xyz, face | voxel xyz, sequence
-    uint4* paths;          // 8 per receiver (ViewPath)
-    uint4* conts;          // 8 per receiver (ViewContinuation)
-    uint4* estimates;      // 4 per receiver (ViewEstimate)
-    uint32_t* queue;       // 12 counters, owners (n), cursor words (n)
-    uint4* shared_state;   // the world cache's slots (9 uint4 each)
-    uint4* shared_meta;    // 3 uint4 per slot
-    float4* shared_cache;  // the slots' gather records
-    const uint4* events;
-    uint32_t n_events, reach;
-    uint32_t n;
-    uint32_t range[4];     // ViewWave.range: first owner, invocations, hits per visit, finite depth
-    uint32_t ticket[4];
-    uint32_t view_first, shared, clock;
-    float physical;        // measured retention c
-    uint32_t hits;         // DIFFUSE_HITS for trace_view_paths
-};
-
-void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
-void launch_view_frame(const ViewArgs& v, bool limited, bool budgeted, cudaStream_t stream);
-void launch_view_trace_paths(const ViewArgs& v, uint32_t samples, uint4* out, bool limited, bool budgeted, cudaStream_t stream);
-void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
-uint32_t wave_traverse_blocks_per_sm();
-void launch_reference64(const TraceArgs& a, const double* cdf, const int4* emitters, uint32_t n_emitters, double total,
-                        const uint4* tasks, uint32_t n_tasks, uint32_t samples, uint64_t seed, double* sum, double* second,
-                        uint32_t* known, cudaStream_t s);
-// The per-frame kernels whose arguments a captured frame graph updates.
-const void* prepare_kernel_address();
-const void* accumulate_kernel_address();
-// Change footprints (vgi_trace.cu): fp = a count record, then 3 records per
-// task; sums = 8 words per task (min xyz, max xyz, flux x 64, unused).
-void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uint32_t threads, uint32_t n_directional, uint32_t* sums,
-                       uint4* events, cudaStream_t s);
-// Headless discovery (vgi_trace.cu): cam = eye xyz, forward xyz, up xyz,
-// tan(half vertical fov); set = 64-bit keys, all ones when empty.
-void launch_discover(const TraceArgs& a, const float* cam, uint32_t w, uint32_t h, uint4* pixels, unsigned long long* set, uint32_t set_mask,
-                     int4* faces, uint32_t* count, uint32_t capacity, uint32_t* overflow, cudaStream_t s);
 // Far tier (vgi_trace.cu, voxel_view_pixels.wgsl): the view uniforms the
 // classify and trace passes read, with the camera in place of the clip
 // matrices. Cells are 3 uint4 (PixelHistory: mean rgb + count, surface xyz +
@@ -183,6 +144,50 @@ struct FarView {
     uint32_t hash_mask;
     uint32_t n_receivers;
 };
+struct ViewArgs {
+    TraceArgs t;
+    uint4* receivers;      // 2 per receiver: surface xyz, face | voxel xyz, sequence
+    uint4* paths;          // 8 per receiver (ViewPath)
+    uint4* conts;          // 8 per receiver (ViewContinuation)
+    uint4* estimates;      // 4 per receiver (ViewEstimate)
+    uint32_t* queue;       // 12 counters, owners (n), cursor words (n)
+    uint4* shared_state;   // the world cache's slots (9 uint4 each)
+    uint4* shared_meta;    // 3 uint4 per slot
+    float4* shared_cache;  // the slots' gather records
+    const uint4* events;
+    uint32_t n_events, reach;
+    uint32_t n;
+    uint32_t range[4];     // ViewWave.range: first owner, invocations, hits per visit, finite depth
+    uint32_t ticket[4];
+    uint32_t view_first, shared, clock;
+    float physical;        // measured retention c
+    uint32_t hits;         // DIFFUSE_HITS for trace_view_paths
+    // The far tier's handoff (null: off): a new, unmeasured receiver starts
+    // from the far cell at its centre; far_stats[5] counts them.
+    const uint4* far_cells;
+    uint32_t* far_stats;
+    FarView far;
+};
+
+void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
+void launch_view_frame(const ViewArgs& v, bool limited, bool budgeted, cudaStream_t stream);
+void launch_view_trace_paths(const ViewArgs& v, uint32_t samples, uint4* out, bool limited, bool budgeted, cudaStream_t stream);
+void launch_wave(const WaveBuffers& b, const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);
+uint32_t wave_traverse_blocks_per_sm();
+void launch_reference64(const TraceArgs& a, const double* cdf, const int4* emitters, uint32_t n_emitters, double total,
+                        const uint4* tasks, uint32_t n_tasks, uint32_t samples, uint64_t seed, double* sum, double* second,
+                        uint32_t* known, cudaStream_t s);
+// The per-frame kernels whose arguments a captured frame graph updates.
+const void* prepare_kernel_address();
+const void* accumulate_kernel_address();
+// Change footprints (vgi_trace.cu): fp = a count record, then 3 records per
+// task; sums = 8 words per task (min xyz, max xyz, flux x 64, unused).
+void launch_footprints(const TraceArgs& a, const int4* fp, uint32_t n_tasks, uint32_t threads, uint32_t n_directional, uint32_t* sums,
+                       uint4* events, cudaStream_t s);
+// Headless discovery (vgi_trace.cu): cam = eye xyz, forward xyz, up xyz,
+// tan(half vertical fov); set = 64-bit keys, all ones when empty.
+void launch_discover(const TraceArgs& a, const float* cam, uint32_t w, uint32_t h, uint4* pixels, unsigned long long* set, uint32_t set_mask,
+                     int4* faces, uint32_t* count, uint32_t capacity, uint32_t* overflow, cudaStream_t s);
 constexpr uint32_t kFarOwned = 0, kFarTraced = 1, kFarHistory = 2, kFarReprojected = 3, kFarSeeded = 4;
 void launch_far(const TraceArgs& a, const FarView& f, const uint4* previous, uint4* current, uint4* output, uint32_t* queue, uint32_t* stats,
                 bool limited, cudaStream_t s);

@@ -370,6 +370,31 @@ __global__ void __launch_bounds__(kBlock) view_load_kernel(const ViewArgs V) {
     V.receivers[i * 2u + 1u].w = identity.x;
 }
 
+// The far tier's handoff in load_shared_faces (voxel_view_cache.wgsl:
+// 196-212): a new, unmeasured receiver (no samples, no sequence, nothing
+// from the world cache) starts from the far cell at its centre
+// (previous_cell over the last far frame's cells), with one unit of weight:
+// mean and shown = the cell's rgb, moment = its square.
+__global__ void __launch_bounds__(kBlock) view_far_seed_kernel(const ViewArgs V) {
+    const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= V.n) return;
+    const uint4 r0 = V.receivers[i * 2u], r1 = V.receivers[i * 2u + 1u];
+    if (r0.w >= 6u) return;
+    uint4* e = V.estimates + i * 4u;
+    if (__uint_as_float(e[0].w) != 0.0f || e[3].x != 0u) return;
+    Cnt<false> cnt;
+    V3 mean;
+    float count;
+    uint32_t sequence;
+    previous_cell(V.t, V.far, V.far_cells, f3w(r0), r0.w, I3{(int)r1.x, (int)r1.y, (int)r1.z}, mean, count, sequence, cnt);
+    if (count <= 0.0f) return;
+    const uint32_t one = __float_as_uint(1.0f);
+    e[0] = w3(mean, one);
+    e[1] = w3(V3{__fmul_rn(mean.x, mean.x), __fmul_rn(mean.y, mean.y), __fmul_rn(mean.z, mean.z)}, 0u);
+    e[2] = w3(mean, one);
+    atomicAdd(V.far_stats + 5, 1u);
+}
+
 // trace_visible_paths (voxel_view_runtime.wgsl:272-325): one thread per
 // owner invocation; completed paths update the estimate's discounted running
 // mean and second moment.
@@ -479,6 +504,7 @@ void view_frame_impl(const ViewArgs& V, cudaStream_t s) {
     view_reproject_kernel<<<grid, kBlock, 0, s>>>(V);
     if (V.n_events) view_retain_kernel<<<grid, kBlock, 0, s>>>(V);
     if (V.shared) view_load_kernel<<<grid, kBlock, 0, s>>>(V);
+    if (V.far_cells) view_far_seed_kernel<<<grid, kBlock, 0, s>>>(V);
     const uint32_t work = V.n < V.range[1] ? V.n : V.range[1];
     if (work && V.range[2]) view_trace_kernel<LIMITED, BUDGETED><<<(work + kBlock - 1) / kBlock, kBlock, 0, s>>>(V);
     if (V.shared) view_store_kernel<<<grid, kBlock, 0, s>>>(V);

@@ -404,6 +404,12 @@ typedef struct vgi_far_settings {
     uint32_t bounded;
 } vgi_far_settings;
 int vgi_far_frame(vgi_ctx* ctx, const vgi_camera* camera, const vgi_far_settings* settings, uint32_t frame);
+/* With `enable`, a view frame starts each new, unmeasured view receiver
+ * (no samples, no sequence, nothing from the world cache) from the far cell
+ * at its centre in the last far frame, seen from that frame's camera, with
+ * one unit of weight (load_shared_faces's far handoff); stats8[5] of
+ * vgi_far_read counts them. Off by default. */
+int vgi_set_far_handoff(vgi_ctx* ctx, int enable);
 /* Drop the far tier's history (a camera cut): cell histories and output
  * cells are zeroed and the next frame reprojects nothing. */
 int vgi_far_reset(vgi_ctx* ctx);
@@ -414,7 +420,8 @@ int vgi_far_reset(vgi_ctx* ctx);
  * coordinate on the face's axis (bits); only owned cells are written each
  * frame. cells12 = PixelHistory per cell (mean rgb, count, surface xyz, face
  * word, sequence, 0, 0, 0). stats8 = owned, traced, history, reprojected,
- * seeded, 0, 0, 0. Any pointer may be null. */
+ * seeded from view receivers, view receivers seeded from far cells (by view
+ * frames since this far frame), 0, 0. Any pointer may be null. */
 int vgi_far_read(vgi_ctx* ctx, uint32_t* shape4, uint32_t* output, uint32_t* cells12, uint32_t* stats8);
 
 /* ---- scheduled frames: the GPU world-cache scheduler --------------------------

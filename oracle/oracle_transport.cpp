@@ -2334,7 +2334,8 @@ int orc_trace_view_paths(const int32_t* directory, uint64_t slots, const uint32_
 int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
                    const float* materials, const float* lights, const uint32_t* emitters, uint32_t* state, uint32_t* meta,
                    const uint32_t* index, const orc_pipeline* pipe, uint32_t* receivers, uint32_t n, uint32_t* paths, uint32_t* conts,
-                   uint32_t* estimates, uint32_t* queue, const uint32_t* wave_words, const uint32_t* view_words, const uint32_t* events) {
+                   uint32_t* estimates, uint32_t* queue, const uint32_t* wave_words, const uint32_t* view_words, const uint32_t* events,
+                   const uint32_t* far_words, const uint32_t* far_cells, uint32_t* far_stats) {
     using namespace view;
     Geometry g = make_geometry(directory, slots, headers, cells, params);
     Model m{params, materials, lights, emitters, state, index, *pipe};
@@ -2414,6 +2415,28 @@ int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* hea
             cursor[i] = first;
             e[12] = pending ? paths[(size_t)i * 32 + 3] : first;
             r[7] = e[12];
+        }
+    }
+    // load_shared_faces's far handoff (voxel_view_cache.wgsl:196-212): a new,
+    // unmeasured receiver starts from the far cell at its centre.
+    if (far_words) {
+        Ctx fx{g, m, Counters{}};
+        const far::View fv{far_words};
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint32_t* r = receivers + (size_t)i * 8;
+            if (r[3] >= 6u) continue;
+            uint32_t* e = estimates + (size_t)i * 16;
+            if (bitsf(e[3]) != 0.0f || e[12] != 0u) continue;
+            f3 mean;
+            float count;
+            uint32_t sequence;
+            far::previous_cell(fx, fv, far_cells, f3{bitsf(r[0]), bitsf(r[1]), bitsf(r[2])}, r[3],
+                               i3{(int32_t)r[4], (int32_t)r[5], (int32_t)r[6]}, mean, count, sequence);
+            if (count <= 0.0f) continue;
+            e[0] = fbits(mean.x); e[1] = fbits(mean.y); e[2] = fbits(mean.z); e[3] = fbits(1.0f);
+            e[4] = fbits(mean.x * mean.x); e[5] = fbits(mean.y * mean.y); e[6] = fbits(mean.z * mean.z); e[7] = 0u;
+            e[8] = e[0]; e[9] = e[1]; e[10] = e[2]; e[11] = fbits(1.0f);
+            far_stats[5] += 1;
         }
     }
     // trace_visible_paths

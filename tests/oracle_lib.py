@@ -73,7 +73,7 @@ _SIG = {
     "orc_apply_events": (_INT, [_P, _P, _P, _P, _U32, _P]),
     "orc_measure_edits": (_INT, [_P, _P, _P, _P, _P, _U32, _P]),
     "orc_trace_view_paths": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _U32, _P]),
-    "orc_view_frame": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _P, _P, _P, _P]),
+    "orc_view_frame": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "orc_face_index": (_I64, [_P, _U32, _P, _U64]),
     "orc_emitters": (_I64, [_P, _U32, _P, _P, _P, _U64, _P]),
 }
@@ -500,6 +500,7 @@ class Frames:
         self.slots = np.arange(n, dtype=np.uint32)
         self.batch_id = 1
         self.results = np.zeros((n, 24), np.uint32)
+        self.far_stats = np.zeros(8, np.uint32)
 
     def frame(self, samples, clock_ms=0, predicted=None, pipe=None):
         """One frame; `predicted` and `pipe` as trace_faces takes them (the
@@ -554,7 +555,9 @@ class Frames:
         self.view["estimates"][:, 13] = materials
 
     def view_frame(self, first=0, invocations=0, max_hits=8, depth=0, ticket=(0, 0, 0, 0), view_first=False, shared=True,
-                   clock_ms=0, events=None, n_events=0, measured_retention=1.0):
+                   clock_ms=0, events=None, n_events=0, measured_retention=1.0, far=None):
+        """far = (44 far-tier view words, cells (n, 12)) turns on the far
+        handoff; self.far_stats[5] counts the receivers it seeds."""
         v = self.view
         n = v["receivers"].shape[0]
         wave = np.array([first, invocations or n, max_hits, depth, *ticket], np.uint32)
@@ -566,7 +569,8 @@ class Frames:
         lib().orc_view_frame(ptr(d), d.size // 4, ptr(h), ptr(cl), ptr(params), ptr(self.materials), ptr(self.lights),
                              ptr(self.emitter_words), ptr(self.state), ptr(self.meta), ptr(self.index), ctypes.byref(self.pipe),
                              ptr(v["receivers"]), n, ptr(v["paths"]), ptr(v["continuations"]), ptr(v["estimates"]), ptr(v["queue"]),
-                             ptr(wave), ptr(view), ptr(ev))
+                             ptr(wave), ptr(view), ptr(ev), ptr(None if far is None else c(far[0], np.uint32)),
+                             ptr(None if far is None else c(far[1], np.uint32)), ptr(self.far_stats))
 
     def measure_edits(self, words, measures, n_entries, material_light):
         """measure_edits + finish_edits on a copy of the event words."""

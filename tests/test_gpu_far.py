@@ -100,3 +100,40 @@ def test_far_cells_take_over_view_receiver_history(gpu):
     stats = far_pair(gpu, case, [cam], settings, frames=[100])
     assert stats[4] > 100, stats  # seeded from the receivers' estimates
     clear_view(gpu)
+
+
+def test_view_receivers_take_over_far_cells(gpu):
+    """The far handoff in load_shared_faces: new view receivers start from
+    the far cell at their centre; the view frame then matches the oracle's
+    given the same far cells."""
+    case = terrain_case(bounces=2)
+    case.load(gpu, with_faces=False)
+    clear_view(gpu)
+    f = unit((0.2, -1.0, 0.3))
+    cam = ((48.5, 80.25, 47.75), f, (0.0, 0.0, 1.0), 0.45, 80, 64)
+    settings = vgi.FarTierSettings(voxel_pixels=64.0, cell=2, rate=1, steps=96)
+    gpu.far_reset()
+    for frame in range(3):
+        gpu.far_frame(*cam, settings=settings, frame=frame)
+    _, _, far_cells, _ = gpu.far_read()
+    _, faces = gpu.discover_faces(*cam)
+    gpu.view_set_receivers(faces)
+    receivers = gpu.view_read()["receivers"]
+    gpu.set_far_handoff(True)
+    try:
+        gpu.view_frame(clock_ms=5)
+    finally:
+        gpu.set_far_handoff(False)
+    got = gpu.view_read()
+    _, _, _, stats = gpu.far_read()
+    geometry = gpu.geometry()
+    ref = O.Frames(geometry, case.params_fn(geometry), case.materials, case.lights, case.emitters, np.zeros((0, 5), np.int32),
+                   case.transport, case.pipe(1))
+    ref.view_start(receivers, faces[:, 4])
+    words, _ = O.FarTier().view_words(cam, settings, 2, False)
+    words[29] = 2  # the cells' stamp: the last far frame
+    ref.view_frame(clock_ms=5, far=(words, far_cells))
+    for key in ("estimates", "paths", "continuations"):
+        assert_words_equal(got[key], ref.view[key], f"view {key} after the far handoff")
+    assert stats[5] == ref.far_stats[5] and stats[5] > 100, (stats, ref.far_stats)
+    clear_view(gpu)
