@@ -182,6 +182,8 @@ struct vgi_ctx {
     uint32_t far_last_frame = 0;
     bool far_has_prev = false;
     bool far_handoff = false;                 // view frames seed new receivers from far cells
+    bool topology_prior = false;              // view frames seed new receivers from their neighbours
+    DevBuf<uint4> v_prev_estimates;           // the estimates before a frame's seeding
     DevBuf<uint4> events;
     DevBuf<int4> footprints;                 // change-footprint tasks of the last event list
     DevBuf<uint32_t> footprint_sums;
@@ -1715,6 +1717,12 @@ int vgi_far_frame(vgi_ctx* c, const vgi_camera* cam, const vgi_far_settings* set
     return VGI_OK;
 }
 
+int vgi_set_topology_prior(vgi_ctx* c, int enable) {
+    if (!c) return VGI_ERR_INVALID;
+    c->topology_prior = enable != 0;
+    return VGI_OK;
+}
+
 int vgi_set_far_handoff(vgi_ctx* c, int enable) {
     if (!c) return VGI_ERR_INVALID;
     c->far_handoff = enable != 0;
@@ -1908,6 +1916,16 @@ int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events
         f.axis[3] = (1.0f / c->far_prev[9]) * (float)c->far_size[1] * 0.5f;
         v.far_cells = c->far_cells[c->far_current].ptr;
         v.far_stats = c->far_stats.ptr;
+    }
+    if (c->topology_prior) {
+        const int rc = ensure_receiver_hash(c);
+        if (rc != VGI_OK) return rc;
+        VGI_CUDA(c, c->v_prev_estimates.reserve((size_t)c->n_view * 4));
+        VGI_CUDA(c, cudaMemcpyAsync(c->v_prev_estimates.ptr, c->v_estimates.ptr, (size_t)c->n_view * 64, cudaMemcpyDeviceToDevice, c->stream));
+        v.topology = 1u;
+        v.receiver_hash = c->v_hash.ptr;
+        v.hash_mask = c->v_hash_mask;
+        v.prev_estimates = c->v_prev_estimates.ptr;
     }
     launch_view_frame(v, transport_limited(c), c->transport.budgeted != 0, c->stream);
     VGI_CUDA(c, cudaGetLastError());

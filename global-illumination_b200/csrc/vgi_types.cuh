@@ -167,6 +167,13 @@ struct ViewArgs {
     const uint4* far_cells;
     uint32_t* far_stats;
     FarView far;
+    // The topology prior (bootstrap_face; 0: off): donors are the receivers
+    // of the owner hash, read from the estimates as they were before this
+    // frame's seeding, and the world cache's slots.
+    uint32_t topology;
+    const uint32_t* receiver_hash;
+    uint32_t hash_mask;
+    const uint4* prev_estimates;
 };
 
 void launch_trace(const TraceArgs& a, uint32_t hits, bool limited, bool budgeted, bool count, cudaStream_t stream);

@@ -11,8 +11,8 @@
 //
 // The caller gives the receivers (one per visible unit face), so every
 // receiver owns itself and the owner queue is receiver order; raster
-// discovery, reprojection across views, the topology prior of new faces and
-// sun-corner records are not part of this path. Records keep the shaders'
+// discovery, reprojection across views and sun-corner records are not part
+// of this path. Records keep the shaders'
 // layouts (uint4 words): ViewReceiver 2, ViewPath 8, ViewContinuation 8,
 // ViewEstimate 4. One thread runs one owner's visits, as the shader does.
 
@@ -263,17 +263,16 @@ __device__ void advance_view_path(Tracer<1, LIMITED, BUDGETED, false>& T, const 
     stored[7] = make_uint4(V.ticket[0], V.ticket[1], V.ticket[2], V.ticket[3]);
 }
 
-// shared_slot (voxel_view_cache.wgsl:6-26) for a unit face of `material`.
-__device__ uint32_t view_shared_slot(const ViewArgs& V, uint32_t index, uint32_t material) {
+// shared_slot (voxel_view_cache.wgsl:6-26) for the unit face (voxel, face) of `material`.
+__device__ uint32_t view_shared_slot_key(const ViewArgs& V, I3 voxel, uint32_t face, uint32_t material) {
     if (!V.shared || V.t.face_index == nullptr) return kNoIndex;
-    const uint4 r0 = V.receivers[index * 2u], r1 = V.receivers[index * 2u + 1u];
     const uint4 header = V.t.face_index[0];
-    uint32_t bucket = (hash_voxel((int)r1.x, (int)r1.y, (int)r1.z) ^ pcg(r0.w + 1u)) & header.x;
+    uint32_t bucket = (hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(face + 1u)) & header.x;
 #pragma unroll 1
     for (uint32_t attempt = 0; attempt < header.y; ++attempt) {
         const uint4 e = V.t.face_index[bucket + 1u];
         if (e.w == 0xffffffffu) return kNoIndex;
-        if (e.x == r1.x && e.y == r1.y && e.z == r1.z && (e.w >> 29u) == r0.w) {
+        if ((int)e.x == voxel.x && (int)e.y == voxel.y && (int)e.z == voxel.z && (e.w >> 29u) == face) {
             const uint32_t slot = e.w & 0x1fffffffu;
             const uint32_t key = V.shared_meta[slot * 3u].w;
             if ((key & 8u) == 0u || (key >> 16u) != material) return kNoIndex;
@@ -282,6 +281,11 @@ __device__ uint32_t view_shared_slot(const ViewArgs& V, uint32_t index, uint32_t
         bucket = (bucket + 1u) & header.x;
     }
     return kNoIndex;
+}
+
+__device__ __forceinline__ uint32_t view_shared_slot(const ViewArgs& V, uint32_t index, uint32_t material) {
+    const uint4 r0 = V.receivers[index * 2u], r1 = V.receivers[index * 2u + 1u];
+    return view_shared_slot_key(V, I3{(int)r1.x, (int)r1.y, (int)r1.z}, r0.w, material);
 }
 
 // reproject_paths' share for caller-given receivers: the receiver takes its
@@ -313,9 +317,10 @@ __global__ void __launch_bounds__(kBlock) view_retain_kernel(const ViewArgs V) {
     if (c.woken && V.conts[i * 8u + 4u].w == 1u) V.conts[i * 8u + 4u].w = 0u;
 }
 
-// load_shared_faces (voxel_view_cache.wgsl:28-98, 188-223) without the
-// topology prior: hand the world cache's authority to the view estimate
-// and reserve this frame's sequence range on the slot.
+// load_shared_faces (voxel_view_cache.wgsl:28-98, 188-223), its world-cache
+// part: hand the world cache's authority to the view estimate and reserve
+// this frame's sequence range on the slot (the priors for new receivers are
+// view_seed_kernel's).
 __global__ void __launch_bounds__(kBlock) view_load_kernel(const ViewArgs V) {
     const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= V.n) return;
@@ -370,29 +375,153 @@ __global__ void __launch_bounds__(kBlock) view_load_kernel(const ViewArgs V) {
     V.receivers[i * 2u + 1u].w = identity.x;
 }
 
-// The far tier's handoff in load_shared_faces (voxel_view_cache.wgsl:
-// 196-212): a new, unmeasured receiver (no samples, no sequence, nothing
-// from the world cache) starts from the far cell at its centre
-// (previous_cell over the last far frame's cells), with one unit of weight:
-// mean and shown = the cell's rgb, moment = its square.
-__global__ void __launch_bounds__(kBlock) view_far_seed_kernel(const ViewArgs V) {
+// voxel_material (voxel_traversal.wgsl:48-70): the material of one voxel, 256 for air.
+__device__ uint32_t voxel_material(const TraceArgs& A, I3 v) {
+    const int rx = (int)floorf(__fdiv_rn((float)v.x, 16.0f)), ry = (int)floorf(__fdiv_rn((float)v.y, 16.0f)),
+              rz = (int)floorf(__fdiv_rn((float)v.z, 16.0f));
+    if (!in_bounds(A, rx, ry, rz)) return 256u;
+    Cnt<false> cnt;
+    const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
+    if (index == kNoIndex) return 256u;
+    const uint4 meta = __ldg(A.headers + index);
+    if (meta.x == 1u) return 256u;
+    if (meta.x != 3u) return meta.y;
+    const uint32_t lx = (uint32_t)(v.x & 15), ly = (uint32_t)(v.y & 15), lz = (uint32_t)(v.z & 15);
+    const uint32_t word = __ldg(A.cells + meta.y + ((lz >> 2) * 4u + (ly >> 2)) * 4u + (lx >> 2));
+    if ((word & 3u) == 0u) return 256u;
+    if ((word & 3u) == 1u) return word >> 2u;
+    const uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
+    const uint32_t cell = (__ldg(A.cells + (word >> 2u) + idx / 2u) >> ((idx & 1u) * 16u)) & 65535u;
+    return (cell & 1u) != 0u ? cell >> 1u : 256u;
+}
+
+// prior_air (voxel_view_cache.wgsl:141-144): known air in a loaded region.
+__device__ bool prior_air(const TraceArgs& A, I3 v) {
+    const int rx = (int)floorf(__fdiv_rn((float)v.x, 16.0f)), ry = (int)floorf(__fdiv_rn((float)v.y, 16.0f)),
+              rz = (int)floorf(__fdiv_rn((float)v.z, 16.0f));
+    if (!in_bounds(A, rx, ry, rz)) return false;
+    Cnt<false> cnt;
+    return lookup_region(A, rx, ry, rz, cnt) != kNoIndex && voxel_material(A, v) == 256u;
+}
+
+struct FacePrior {
+    V3 mean, moment;
+    float weight;
+};
+
+// prior_donor (voxel_view_cache.wgsl:108-131): the last frame's estimate of
+// the receiver on this unit face, or the world cache's slot if it holds more
+// samples; at least 16 samples either way.
+__device__ FacePrior prior_donor(const ViewArgs& V, I3 voxel, uint32_t face) {
+    FacePrior donor{V3{0.0f, 0.0f, 0.0f}, V3{0.0f, 0.0f, 0.0f}, 0.0f};
+    const V3 surface = add_s(itof(voxel), 0.5f) + face_normal(face) * 0.5f;
+    uint32_t slot = (hash_voxel(voxel.x, voxel.y, voxel.z) ^ pcg(face + 1u)) & V.hash_mask;
+#pragma unroll 1
+    for (uint32_t step = 0; step < 64u; ++step) {
+        const uint32_t value = V.receiver_hash[slot];
+        if (value == 0u) break;
+        if (value <= V.n) {
+            const uint4 r0 = V.receivers[(value - 1u) * 2u], r1 = V.receivers[(value - 1u) * 2u + 1u];
+            if (r0.w == face && (int)r1.x == voxel.x && (int)r1.y == voxel.y && (int)r1.z == voxel.z && __uint_as_float(r0.x) == surface.x &&
+                __uint_as_float(r0.y) == surface.y && __uint_as_float(r0.z) == surface.z) {
+                const uint4 m = V.prev_estimates[(value - 1u) * 4u], mo = V.prev_estimates[(value - 1u) * 4u + 1u];
+                if (__uint_as_float(m.w) >= 16.0f) donor = FacePrior{f3w(m), f3w(mo), __uint_as_float(m.w)};
+                break;
+            }
+        }
+        slot = (slot + 1u) & V.hash_mask;
+    }
+    const uint32_t cache = view_shared_slot_key(V, voxel, face, voxel_material(V.t, voxel));
+    if (cache != kNoIndex) {
+        const uint4* base = V.shared_state + cache * 9u;
+        const uint32_t count = base[1].y & 0x7fffffffu;
+        if (count >= 16u && (float)count > donor.weight) donor = FacePrior{f3w(base[0]), f3w(base[2]), (float)count};
+    }
+    return donor;
+}
+
+__device__ __forceinline__ void add_prior(FacePrior& sum, const FacePrior& donor, float weight) {
+    if (donor.weight == 0.0f) return;
+    sum.mean = sum.mean + donor.mean * weight;
+    sum.moment = sum.moment + donor.moment * weight;
+    sum.weight = __fadd_rn(sum.weight, weight);
+}
+
+// bootstrap_face (voxel_view_cache.wgsl:146-186) for a receiver whose
+// geometry is not pending: a newly exposed face takes the incident light of
+// the coplanar faces it connects to, or of the faces around its air cell.
+__device__ FacePrior bootstrap_face(const ViewArgs& V, uint4 r0, uint4 r1) {
+    FacePrior prior{V3{0.0f, 0.0f, 0.0f}, V3{0.0f, 0.0f, 0.0f}, 0.0f};
+    const uint32_t rf = r0.w;
+    const I3 origin{(int)r1.x, (int)r1.y, (int)r1.z};
+    const V3 nf = face_normal(rf);
+    const I3 normal{(int)nf.x, (int)nf.y, (int)nf.z};
+    const I3 air{origin.x + normal.x, origin.y + normal.y, origin.z + normal.z};
+    // receiver_stride: unit faces only.
+    const uint32_t u = (rf / 2u + 1u) % 3u;
+    const float su = u == 0u ? __uint_as_float(r0.x) : (u == 1u ? __uint_as_float(r0.y) : __uint_as_float(r0.z));
+    const int vu = u == 0u ? origin.x : (u == 1u ? origin.y : origin.z);
+    if (__fmul_rn(2.0f, __fsub_rn(su, (float)vu)) != 1.0f) return prior;
+    if (voxel_material(V.t, origin) == 256u || !prior_air(V.t, air)) return prior;
+    for (uint32_t f = 0; f < 6u; ++f) {
+        const V3 o = face_normal(f);
+        const I3 off{(int)o.x, (int)o.y, (int)o.z};
+        const I3 v{origin.x + off.x, origin.y + off.y, origin.z + off.z};
+        const bool covered = off.x == -normal.x && off.y == -normal.y && off.z == -normal.z;
+        if (covered || prior_air(V.t, I3{v.x + normal.x, v.y + normal.y, v.z + normal.z})) add_prior(prior, prior_donor(V, v, rf), 1.0f);
+    }
+    if (prior.weight == 0.0f) {
+        for (uint32_t f = 0; f < 6u; ++f) {
+            const V3 o = face_normal(f);
+            const I3 off{(int)o.x, (int)o.y, (int)o.z};
+            const float alignment = dot3(itof(normal), o);
+            const float w = alignment > 0.0f ? 1.0f : 0.25f;
+            add_prior(prior, prior_donor(V, air, f), w);
+            const I3 covered{origin.x - off.x, origin.y - off.y, origin.z - off.z};
+            if (covered.x != air.x || covered.y != air.y || covered.z != air.z) add_prior(prior, prior_donor(V, covered, f), w);
+            add_prior(prior, prior_donor(V, I3{air.x - off.x, air.y - off.y, air.z - off.z}, f), w);
+        }
+    }
+    if (prior.weight > 0.0f) {
+        prior.mean = prior.mean / prior.weight;
+        const V3 m2 = prior.moment / prior.weight;
+        prior.moment = V3{wmax(m2.x, __fmul_rn(prior.mean.x, prior.mean.x)), wmax(m2.y, __fmul_rn(prior.mean.y, prior.mean.y)),
+                          wmax(m2.z, __fmul_rn(prior.mean.z, prior.mean.z))};
+        prior.weight = 1.0f;
+    }
+    return prior;
+}
+
+// The priors of load_shared_faces (voxel_view_cache.wgsl:192-212): a new,
+// unmeasured receiver (no samples, no sequence, nothing from the world
+// cache) starts from its topology prior, or else, with the far tier's
+// handoff, from the far cell at its centre (previous_cell over the last far
+// frame's cells): one unit of weight, mean and shown = the prior's rgb.
+__global__ void __launch_bounds__(kBlock) view_seed_kernel(const ViewArgs V) {
     const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= V.n) return;
     const uint4 r0 = V.receivers[i * 2u], r1 = V.receivers[i * 2u + 1u];
     if (r0.w >= 6u) return;
     uint4* e = V.estimates + i * 4u;
     if (__uint_as_float(e[0].w) != 0.0f || e[3].x != 0u) return;
-    Cnt<false> cnt;
-    V3 mean;
-    float count;
-    uint32_t sequence;
-    previous_cell(V.t, V.far, V.far_cells, f3w(r0), r0.w, I3{(int)r1.x, (int)r1.y, (int)r1.z}, mean, count, sequence, cnt);
-    if (count <= 0.0f) return;
-    const uint32_t one = __float_as_uint(1.0f);
-    e[0] = w3(mean, one);
-    e[1] = w3(V3{__fmul_rn(mean.x, mean.x), __fmul_rn(mean.y, mean.y), __fmul_rn(mean.z, mean.z)}, 0u);
-    e[2] = w3(mean, one);
-    atomicAdd(V.far_stats + 5, 1u);
+    FacePrior prior{V3{0.0f, 0.0f, 0.0f}, V3{0.0f, 0.0f, 0.0f}, 0.0f};
+    if (V.topology) prior = bootstrap_face(V, r0, r1);
+    if (prior.weight == 0.0f && V.far_cells) {
+        Cnt<false> cnt;
+        V3 mean;
+        float count;
+        uint32_t sequence;
+        previous_cell(V.t, V.far, V.far_cells, f3w(r0), r0.w, I3{(int)r1.x, (int)r1.y, (int)r1.z}, mean, count, sequence, cnt);
+        if (count > 0.0f) {
+            prior = FacePrior{mean, V3{__fmul_rn(mean.x, mean.x), __fmul_rn(mean.y, mean.y), __fmul_rn(mean.z, mean.z)}, 1.0f};
+            atomicAdd(V.far_stats + 5, 1u);
+        }
+    }
+    if (prior.weight <= 0.0f) return;
+    const uint32_t one = __float_as_uint(prior.weight);
+    e[0] = w3(prior.mean, one);
+    e[1] = w3(prior.moment, 0u);
+    e[2] = w3(prior.mean, __float_as_uint(1.0f));
 }
 
 // trace_visible_paths (voxel_view_runtime.wgsl:272-325): one thread per
@@ -504,7 +633,7 @@ void view_frame_impl(const ViewArgs& V, cudaStream_t s) {
     view_reproject_kernel<<<grid, kBlock, 0, s>>>(V);
     if (V.n_events) view_retain_kernel<<<grid, kBlock, 0, s>>>(V);
     if (V.shared) view_load_kernel<<<grid, kBlock, 0, s>>>(V);
-    if (V.far_cells) view_far_seed_kernel<<<grid, kBlock, 0, s>>>(V);
+    if (V.far_cells || V.topology) view_seed_kernel<<<grid, kBlock, 0, s>>>(V);
     const uint32_t work = V.n < V.range[1] ? V.n : V.range[1];
     if (work && V.range[2]) view_trace_kernel<LIMITED, BUDGETED><<<(work + kBlock - 1) / kBlock, kBlock, 0, s>>>(V);
     if (V.shared) view_store_kernel<<<grid, kBlock, 0, s>>>(V);

@@ -265,6 +265,7 @@ _SIGNATURES = {
     "vgi_far_read": (_INT, [_P, _P, _P, _P, _P]),
     "vgi_far_reset": (_INT, [_P]),
     "vgi_set_far_handoff": (_INT, [_P, _INT]),
+    "vgi_set_topology_prior": (_INT, [_P, _INT]),
     "vgi_view_set_tiles": (_INT, [_P, _P, _U32, _U32, _U32]),
     "vgi_view_reconstruct": (_INT, [_P, _P]),
     "vgi_view_read_published": (_INT, [_P, _P, _P]),
@@ -749,6 +750,9 @@ class GpuTracer:
                      (ctypes.c_float * 3)(*map(float, up)), float(tan_half_fov), width, height)
         st = (settings or FarTierSettings()).struct()
         self._check(self._lib.vgi_far_frame(self._h, ctypes.byref(cam), ctypes.byref(st), frame & 0xFFFFFFFF))
+
+    def set_topology_prior(self, enable: bool) -> None:
+        self._check(self._lib.vgi_set_topology_prior(self._h, 1 if enable else 0))
 
     def set_far_handoff(self, enable: bool) -> None:
         self._check(self._lib.vgi_set_far_handoff(self._h, 1 if enable else 0))

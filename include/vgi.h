@@ -410,6 +410,14 @@ int vgi_far_frame(vgi_ctx* ctx, const vgi_camera* camera, const vgi_far_settings
  * one unit of weight (load_shared_faces's far handoff); stats8[5] of
  * vgi_far_read counts them. Off by default. */
 int vgi_set_far_handoff(vgi_ctx* ctx, int enable);
+/* With `enable`, a view frame first gives each new, unmeasured unit-face
+ * receiver whose voxel is solid and whose air cell is known its topology
+ * prior (bootstrap_face, voxel_view_cache.wgsl:100-186): the mean of the
+ * connected coplanar faces' incident light, else a weighted mean over the
+ * faces around its air cell; donors are the other receivers as they were
+ * before the frame, and world-cache slots, with at least 16 samples. The
+ * far handoff applies only where this prior finds nothing. Off by default. */
+int vgi_set_topology_prior(vgi_ctx* ctx, int enable);
 /* Drop the far tier's history (a camera cut): cell histories and output
  * cells are zeroed and the next frame reprojects nothing. */
 int vgi_far_reset(vgi_ctx* ctx);

@@ -2307,6 +2307,104 @@ static uint32_t shared_slot(const Shared& sh, const uint32_t* receiver, uint32_t
 }
 
 }  // namespace view
+
+// The topology prior of load_shared_faces (voxel_view_cache.wgsl:100-186).
+namespace prior {
+// voxel_material (voxel_traversal.wgsl:48-70)
+static uint32_t voxel_material(Ctx& x, i3 v) {
+    const i3 r = far::region_of(v);
+    if (!in_bounds(x, r)) return 256u;
+    const uint32_t index = lookup_region(x, r);
+    if (index == 0xffffffffu) return 256u;
+    const uint32_t* meta = x.g.headers + (size_t)index * 4;
+    if (meta[0] == 1u) return 256u;
+    if (meta[0] != 3u) return meta[1];
+    const uint32_t lx = (uint32_t)(v.x & 15), ly = (uint32_t)(v.y & 15), lz = (uint32_t)(v.z & 15);
+    const uint32_t word = x.g.cells[meta[1] + ((lz >> 2) * 4u + (ly >> 2)) * 4u + (lx >> 2)];
+    if ((word & 3u) == 0u) return 256u;
+    if ((word & 3u) == 1u) return word >> 2u;
+    const uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
+    const uint32_t cell = (x.g.cells[(word >> 2u) + idx / 2u] >> ((idx & 1u) * 16u)) & 65535u;
+    return (cell & 1u) != 0u ? cell >> 1u : 256u;
+}
+static bool prior_air(Ctx& x, i3 v) {
+    const i3 r = far::region_of(v);
+    return in_bounds(x, r) && lookup_region(x, r) != 0xffffffffu && voxel_material(x, v) == 256u;
+}
+struct FacePrior { f3 mean{0, 0, 0}, moment{0, 0, 0}; float weight = 0.0f; };
+struct Donors {
+    const uint32_t* receivers;
+    uint32_t n;
+    const uint32_t* before;  // estimates before the seeding, 16 words each
+    const view::Shared* sh;
+};
+static FacePrior prior_donor(Ctx& x, const Donors& d, i3 voxel, uint32_t face) {
+    FacePrior donor;
+    const f3 surface = add(adds(f3{(float)voxel.x, (float)voxel.y, (float)voxel.z}, 0.5f), muls(face_normal(face), 0.5f));
+    for (uint32_t i = 0; i < d.n; ++i) {
+        const uint32_t* r = d.receivers + (size_t)i * 8;
+        if (r[3] == face && (int32_t)r[4] == voxel.x && (int32_t)r[5] == voxel.y && (int32_t)r[6] == voxel.z && bitsf(r[0]) == surface.x &&
+            bitsf(r[1]) == surface.y && bitsf(r[2]) == surface.z) {
+            const uint32_t* e = d.before + (size_t)i * 16;
+            if (bitsf(e[3]) >= 16.0f) donor = FacePrior{f3{bitsf(e[0]), bitsf(e[1]), bitsf(e[2])}, f3{bitsf(e[4]), bitsf(e[5]), bitsf(e[6])}, bitsf(e[3])};
+            break;
+        }
+    }
+    const uint32_t key[8] = {fbits(surface.x), fbits(surface.y), fbits(surface.z), face, (uint32_t)voxel.x, (uint32_t)voxel.y, (uint32_t)voxel.z, 0u};
+    const uint32_t slot = view::shared_slot(*d.sh, key, voxel_material(x, voxel));
+    if (slot != 0xffffffffu) {
+        const uint32_t* base = d.sh->state + (size_t)slot * 36;
+        const uint32_t count = base[5] & 0x7fffffffu;
+        if (count >= 16u && (float)count > donor.weight)
+            donor = FacePrior{f3{bitsf(base[0]), bitsf(base[1]), bitsf(base[2])}, f3{bitsf(base[8]), bitsf(base[9]), bitsf(base[10])}, (float)count};
+    }
+    return donor;
+}
+static void add_prior(FacePrior& sum, const FacePrior& donor, float weight) {
+    if (donor.weight == 0.0f) return;
+    sum.mean = add(sum.mean, muls(donor.mean, weight));
+    sum.moment = add(sum.moment, muls(donor.moment, weight));
+    sum.weight = sum.weight + weight;
+}
+static FacePrior bootstrap_face(Ctx& x, const Donors& d, const uint32_t* r) {
+    FacePrior prior;
+    const uint32_t rf = r[3];
+    const i3 origin{(int32_t)r[4], (int32_t)r[5], (int32_t)r[6]};
+    const f3 nf = face_normal(rf);
+    const i3 normal{(int32_t)nf.x, (int32_t)nf.y, (int32_t)nf.z};
+    const i3 air{origin.x + normal.x, origin.y + normal.y, origin.z + normal.z};
+    const uint32_t u = (rf / 2u + 1u) % 3u;
+    const int32_t vu = u == 0u ? origin.x : (u == 1u ? origin.y : origin.z);
+    if (2.0f * (bitsf(r[u]) - (float)vu) != 1.0f) return prior;
+    if (voxel_material(x, origin) == 256u || !prior_air(x, air)) return prior;
+    for (uint32_t f = 0; f < 6u; ++f) {
+        const f3 o = face_normal(f);
+        const i3 off{(int32_t)o.x, (int32_t)o.y, (int32_t)o.z};
+        const i3 v{origin.x + off.x, origin.y + off.y, origin.z + off.z};
+        const bool covered = off.x == -normal.x && off.y == -normal.y && off.z == -normal.z;
+        if (covered || prior_air(x, i3{v.x + normal.x, v.y + normal.y, v.z + normal.z})) add_prior(prior, prior_donor(x, d, v, rf), 1.0f);
+    }
+    if (prior.weight == 0.0f) {
+        for (uint32_t f = 0; f < 6u; ++f) {
+            const f3 o = face_normal(f);
+            const i3 off{(int32_t)o.x, (int32_t)o.y, (int32_t)o.z};
+            const float alignment = dot(f3{(float)normal.x, (float)normal.y, (float)normal.z}, o);
+            const float w = alignment > 0.0f ? 1.0f : 0.25f;
+            add_prior(prior, prior_donor(x, d, air, f), w);
+            const i3 covered{origin.x - off.x, origin.y - off.y, origin.z - off.z};
+            if (covered.x != air.x || covered.y != air.y || covered.z != air.z) add_prior(prior, prior_donor(x, d, covered, f), w);
+            add_prior(prior, prior_donor(x, d, i3{air.x - off.x, air.y - off.y, air.z - off.z}, f), w);
+        }
+    }
+    if (prior.weight > 0.0f) {
+        prior.mean = divs(prior.mean, prior.weight);
+        const f3 m2 = divs(prior.moment, prior.weight);
+        prior.moment = f3{wmax(m2.x, prior.mean.x * prior.mean.x), wmax(m2.y, prior.mean.y * prior.mean.y), wmax(m2.z, prior.mean.z * prior.mean.z)};
+        prior.weight = 1.0f;
+    }
+    return prior;
+}
+}  // namespace prior
 }  // namespace orc
 
 extern "C" {
@@ -2417,26 +2515,36 @@ int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* hea
             r[7] = e[12];
         }
     }
-    // load_shared_faces's far handoff (voxel_view_cache.wgsl:196-212): a new,
-    // unmeasured receiver starts from the far cell at its centre.
-    if (far_words) {
+    // The priors of load_shared_faces (voxel_view_cache.wgsl:192-212): a new,
+    // unmeasured receiver starts from its topology prior, or else from the
+    // far cell at its centre.
+    const bool topology = view_words[6] != 0u;
+    if (far_words || topology) {
         Ctx fx{g, m, Counters{}};
-        const far::View fv{far_words};
+        const std::vector<uint32_t> before(estimates, estimates + (size_t)n * 16);
+        const prior::Donors donors{receivers, n, before.data(), &sh};
         for (uint32_t i = 0; i < n; ++i) {
             const uint32_t* r = receivers + (size_t)i * 8;
             if (r[3] >= 6u) continue;
             uint32_t* e = estimates + (size_t)i * 16;
             if (bitsf(e[3]) != 0.0f || e[12] != 0u) continue;
-            f3 mean;
-            float count;
-            uint32_t sequence;
-            far::previous_cell(fx, fv, far_cells, f3{bitsf(r[0]), bitsf(r[1]), bitsf(r[2])}, r[3],
-                               i3{(int32_t)r[4], (int32_t)r[5], (int32_t)r[6]}, mean, count, sequence);
-            if (count <= 0.0f) continue;
-            e[0] = fbits(mean.x); e[1] = fbits(mean.y); e[2] = fbits(mean.z); e[3] = fbits(1.0f);
-            e[4] = fbits(mean.x * mean.x); e[5] = fbits(mean.y * mean.y); e[6] = fbits(mean.z * mean.z); e[7] = 0u;
+            prior::FacePrior p;
+            if (topology) p = prior::bootstrap_face(fx, donors, r);
+            if (p.weight == 0.0f && far_words) {
+                f3 mean;
+                float count;
+                uint32_t sequence;
+                far::previous_cell(fx, far::View{far_words}, far_cells, f3{bitsf(r[0]), bitsf(r[1]), bitsf(r[2])}, r[3],
+                                   i3{(int32_t)r[4], (int32_t)r[5], (int32_t)r[6]}, mean, count, sequence);
+                if (count > 0.0f) {
+                    p = prior::FacePrior{mean, f3{mean.x * mean.x, mean.y * mean.y, mean.z * mean.z}, 1.0f};
+                    far_stats[5] += 1;
+                }
+            }
+            if (p.weight <= 0.0f) continue;
+            e[0] = fbits(p.mean.x); e[1] = fbits(p.mean.y); e[2] = fbits(p.mean.z); e[3] = fbits(p.weight);
+            e[4] = fbits(p.moment.x); e[5] = fbits(p.moment.y); e[6] = fbits(p.moment.z); e[7] = 0u;
             e[8] = e[0]; e[9] = e[1]; e[10] = e[2]; e[11] = fbits(1.0f);
-            far_stats[5] += 1;
         }
     }
     // trace_visible_paths

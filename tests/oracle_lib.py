@@ -555,13 +555,13 @@ class Frames:
         self.view["estimates"][:, 13] = materials
 
     def view_frame(self, first=0, invocations=0, max_hits=8, depth=0, ticket=(0, 0, 0, 0), view_first=False, shared=True,
-                   clock_ms=0, events=None, n_events=0, measured_retention=1.0, far=None):
+                   clock_ms=0, events=None, n_events=0, measured_retention=1.0, far=None, topology=False):
         """far = (44 far-tier view words, cells (n, 12)) turns on the far
         handoff; self.far_stats[5] counts the receivers it seeds."""
         v = self.view
         n = v["receivers"].shape[0]
         wave = np.array([first, invocations or n, max_hits, depth, *ticket], np.uint32)
-        view = np.array([int(view_first), int(shared and self.n > 0), clock_ms, n_events, 192 * 192, 0], np.uint32)
+        view = np.array([int(view_first), int(shared and self.n > 0), clock_ms, n_events, 192 * 192, 0, int(topology)], np.uint32)
         view[5] = np.float32(max(measured_retention, 0.0)).view(np.uint32)
         ev = np.zeros(4, np.uint32) if events is None else c(events, np.uint32)
         d, h, cl, _ = self.geometry

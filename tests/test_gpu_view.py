@@ -99,3 +99,30 @@ def test_view_without_shared_cache_keeps_its_own_history(gpu):
         compare_view(gpu, ref, f"unshared view frame {k}")
     est = ref.view["estimates"]
     assert (est[:, 3].view(np.float32) > 0).any() and (est[:, 15] == 0).all()
+
+
+def test_topology_prior_seeds_new_receivers_like_the_oracle(gpu):
+    """bootstrap_face: new view receivers next to world-cache faces with at
+    least 16 samples start from those faces' light; a view frame without
+    tracing shows the priors, a traced one follows, both equal to the
+    oracle's."""
+    case = terrain_case(bounces=2)
+    ref = world(gpu, case, 3)  # 24 samples a world face
+    exposed = vgi.exposed_faces(case.coords, case.vox)
+    world_keys = {tuple(r[:4]) for r in case.faces}
+    fresh = np.array([r for r in exposed[1::3] if tuple(r[:4]) not in world_keys][:4000], np.int32)
+    gpu.view_set_receivers(fresh)
+    ref.view_start(gpu.view_read()["receivers"], fresh[:, 4])
+    gpu.set_topology_prior(True)
+    try:
+        gpu.view_frame(max_hits=0, clock_ms=200)
+        ref.view_frame(max_hits=0, clock_ms=200, topology=True)
+        compare_view(gpu, ref, "priors")
+        weights = gpu.view_read()["estimates"].view(np.float32)[:, 3]
+        assert (weights == 1.0).sum() > len(fresh) // 2, (weights == 1.0).sum()
+        gpu.view_frame(max_hits=4, clock_ms=216)
+        ref.view_frame(max_hits=4, clock_ms=216, topology=True)
+        compare_view(gpu, ref, "frame after the priors")
+    finally:
+        gpu.set_topology_prior(False)
+    gpu.view_set_receivers(np.zeros((0, 5), np.int32))
