@@ -183,6 +183,7 @@ struct vgi_ctx {
     bool far_has_prev = false;
     bool far_handoff = false;                 // view frames seed new receivers from far cells
     bool topology_prior = false;              // view frames seed new receivers from their neighbours
+    uint32_t view_frames = 0;                 // view frames since the receivers were set
     DevBuf<uint4> v_prev_estimates;           // the estimates before a frame's seeding
     DevBuf<uint4> events;
     DevBuf<int4> footprints;                 // change-footprint tasks of the last event list
@@ -1605,6 +1606,7 @@ int vgi_view_set_receivers(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     }
     VGI_CUDA(c, cudaMemsetAsync(c->v_queue.ptr, 0, (12 + 2 * m) * 4, c->stream));
     c->n_view = n;
+    c->view_frames = 0;
     c->v_hash_valid = false;
     c->v_tiles_n = 0;
     c->v_published_valid = false;
@@ -1917,6 +1919,9 @@ int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events
         v.far_cells = c->far_cells[c->far_current].ptr;
         v.far_stats = c->far_stats.ptr;
     }
+    v.frame = c->view_frames;
+    v.has_previous = c->view_frames > 0 ? 1u : 0u;
+    v.n_directional = c->n_directional;
     if (c->topology_prior) {
         const int rc = ensure_receiver_hash(c);
         if (rc != VGI_OK) return rc;
@@ -1929,6 +1934,7 @@ int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events
     }
     launch_view_frame(v, transport_limited(c), c->transport.budgeted != 0, c->stream);
     VGI_CUDA(c, cudaGetLastError());
+    c->view_frames += 1;
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }

@@ -171,6 +171,9 @@ struct ViewArgs {
     // of the owner hash, read from the estimates as they were before this
     // frame's seeding, and the world cache's slots.
     uint32_t topology;
+    // Sun corners (reproject_paths): this view frame's number, whether the
+    // receivers were in the last view frame, and the directional lights.
+    uint32_t frame, has_previous, n_directional;
     const uint32_t* receiver_hash;
     uint32_t hash_mask;
     const uint4* prev_estimates;

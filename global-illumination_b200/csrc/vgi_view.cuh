@@ -290,6 +290,33 @@ __device__ __forceinline__ uint32_t view_shared_slot(const ViewArgs& V, uint32_t
 
 // reproject_paths' share for caller-given receivers: the receiver takes its
 // estimate's sequence, and every receiver is its own owner (queue rank = index).
+// sky_corner_visibility (voxel_path.wgsl:246-266): per directional light
+// with visible colour (at most 4) whether the corner sees it; all zero when a
+// ray runs out of steps, bit 31 set otherwise.
+__device__ uint32_t sky_corner_visibility(const TraceArgs& A, uint32_t n_directional, V3 position) {
+    uint32_t word = 0x80000000u, bit = 0u;
+    Cnt<false> cnt;
+    for (uint32_t i = 0; i < n_directional && bit < 4u; ++i) {
+        const float4 p = __ldg(A.lights + i * 3u), e = __ldg(A.lights + i * 3u + 1u), x = __ldg(A.lights + i * 3u + 2u);
+        if (wmax(__fsub_rn(e.x, x.y), 0.0f) == 0.0f && wmax(__fsub_rn(e.y, x.z), 0.0f) == 0.0f && wmax(__fsub_rn(e.z, x.w), 0.0f) == 0.0f)
+            continue;
+        const V3 direction = normalize3(V3{p.x, p.y, p.z});
+        const uint32_t status = trace_domain(A, position + direction * 0.002f, direction, A.max_distance, true, 2048u, cnt).status;
+        if (status == 2u) {
+            word = 0u;
+            break;
+        }
+        if (status == 0u) word |= 1u << bit;
+        bit += 1u;
+    }
+    return word;
+}
+
+// reproject_paths (voxel_view_runtime.wgsl:148-215) for caller-given
+// receivers: the receiver takes its estimate's sequence, every receiver is
+// its own owner (queue rank = index), and a face lit by a directional light
+// refreshes its four corner sun words one frame in 4 (staggered by index),
+// at once when it is new to the view.
 __global__ void __launch_bounds__(kBlock) view_reproject_kernel(const ViewArgs V) {
     const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
     if (i == 0) {
@@ -297,6 +324,41 @@ __global__ void __launch_bounds__(kBlock) view_reproject_kernel(const ViewArgs V
         V.queue[kViewOwners] = V.n;
     }
     if (i >= V.n) return;
+    const uint4 r0 = V.receivers[i * 2u], r1 = V.receivers[i * 2u + 1u];
+    if (r0.w < 6u) {
+        const V3 normal = face_normal(r0.w);
+        bool lit = false;
+        for (uint32_t l = 0; l < V.n_directional; ++l) {
+            const float4 p = __ldg(V.t.lights + l * 3u);
+            lit = lit || dot3(normal, V3{p.x, p.y, p.z}) > 0.0f;
+        }
+        const uint32_t old = V.estimates[i * 4u + 3u].z;
+        const bool carried = V.has_previous && old != 0u && (V.frame + i) % 4u != 0u;
+        uint32_t corners = carried ? old : 0x80808080u;
+        if (lit && !carried) {
+            V3 u{0.0f, 1.0f, 0.0f}, v{0.0f, 0.0f, 1.0f};
+            if (r0.w / 2u == 1u) u = V3{1.0f, 0.0f, 0.0f};
+            else if (r0.w / 2u == 2u) {
+                u = V3{1.0f, 0.0f, 0.0f};
+                v = V3{0.0f, 1.0f, 0.0f};
+            }
+            const uint32_t a = (r0.w / 2u + 1u) % 3u;
+            const float sa = a == 0u ? __uint_as_float(r0.x) : (a == 1u ? __uint_as_float(r0.y) : __uint_as_float(r0.z));
+            const int va = a == 0u ? (int)r1.x : (a == 1u ? (int)r1.y : (int)r1.z);
+            const float s = __fmul_rn(2.0f, __fsub_rn(sa, (float)va));  // receiver_stride
+            u = u * s;
+            v = v * s;
+            const V3 base = V3{(float)(int)r1.x, (float)(int)r1.y, (float)(int)r1.z} +
+                            V3{wmax(normal.x, 0.0f), wmax(normal.y, 0.0f), wmax(normal.z, 0.0f)} * s;
+            corners = 0u;
+            for (uint32_t corner = 0; corner < 4u; ++corner) {
+                const V3 position = (base + u * (float)(corner & 1u)) + v * (float)(corner >> 1u);
+                const uint32_t word = sky_corner_visibility(V.t, V.n_directional, position);
+                corners |= ((word & 15u) | ((word >> 24u) & 128u)) << (corner * 8u);
+            }
+        }
+        V.estimates[i * 4u + 3u].z = corners;
+    }
     V.receivers[i * 2u + 1u].w = V.estimates[i * 4u + 3u].x;
     V.queue[kViewPrefix + i] = i;
     V.queue[kViewPrefix + V.n + i] = i;

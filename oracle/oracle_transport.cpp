@@ -2448,10 +2448,55 @@ int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* hea
     uint32_t* cursor = queue + PREFIX + n;
     // reproject_paths: the receiver's sequence is its estimate's, and every
     // receiver is its own owner.
+    // and the sun corners: a face lit by a directional light refreshes its
+    // four corner words one frame in 4 (staggered by index), at once when
+    // new to the view (voxel_view_runtime.wgsl:168-200).
+    const uint32_t frame = view_words[7];
+    const bool has_previous = view_words[8] != 0u;
+    Ctx cx{g, m, Counters{}};
+    const uint32_t n_directional = cx.pcount(11);
+    auto sky_corner_visibility = [&](f3 position) {
+        uint32_t word = 0x80000000u, bit = 0u;
+        for (uint32_t l = 0; l < n_directional && bit < 4u; ++l) {
+            const float* L = lights + (size_t)l * 12;
+            if (wmax(L[4] - L[9], 0.0f) == 0.0f && wmax(L[5] - L[10], 0.0f) == 0.0f && wmax(L[6] - L[11], 0.0f) == 0.0f) continue;
+            const f3 direction = normalize(f3{L[0], L[1], L[2]});
+            const uint32_t status = trace_domain_limited(cx, add(position, muls(direction, 0.002f)), direction, cx.extra(1), true, 2048u).status;
+            if (status == 2u) { word = 0u; break; }
+            if (status == 0u) word |= 1u << bit;
+            bit += 1u;
+        }
+        return word;
+    };
     for (uint32_t i = 0; i < n; ++i) {
         uint32_t* r = receivers + (size_t)i * 8;
         if (r[3] >= 6u) continue;
-        r[7] = estimates[(size_t)i * 16 + 12];
+        uint32_t* e = estimates + (size_t)i * 16;
+        const f3 normal = face_normal(r[3]);
+        bool lit = false;
+        for (uint32_t l = 0; l < n_directional; ++l) lit = lit || dot(normal, f3{lights[l * 12], lights[l * 12 + 1], lights[l * 12 + 2]}) > 0.0f;
+        const uint32_t old = e[14];
+        const bool carried = has_previous && old != 0u && (frame + i) % 4u != 0u;
+        uint32_t corners = carried ? old : 0x80808080u;
+        if (lit && !carried) {
+            f3 u{0, 1, 0}, v{0, 0, 1};
+            if (r[3] / 2u == 1u) u = f3{1, 0, 0};
+            else if (r[3] / 2u == 2u) { u = f3{1, 0, 0}; v = f3{0, 1, 0}; }
+            const uint32_t a = (r[3] / 2u + 1u) % 3u;
+            const float s = 2.0f * (bitsf(r[a]) - (float)(int32_t)r[4 + a]);
+            u = muls(u, s);
+            v = muls(v, s);
+            const f3 base = add(f3{(float)(int32_t)r[4], (float)(int32_t)r[5], (float)(int32_t)r[6]},
+                                muls(f3{wmax(normal.x, 0.0f), wmax(normal.y, 0.0f), wmax(normal.z, 0.0f)}, s));
+            corners = 0u;
+            for (uint32_t corner = 0; corner < 4u; ++corner) {
+                const f3 position = add(add(base, muls(u, (float)(corner & 1u))), muls(v, (float)(corner >> 1u)));
+                const uint32_t word = sky_corner_visibility(position);
+                corners |= ((word & 15u) | ((word >> 24u) & 128u)) << (corner * 8u);
+            }
+        }
+        e[14] = corners;
+        r[7] = e[12];
         const uint32_t entry = queue[OWNERS]++;
         owners[entry] = i;
         cursor[i] = entry;

@@ -553,6 +553,7 @@ class Frames:
                      "continuations": np.zeros((n, 32), np.uint32), "estimates": np.zeros((n, 16), np.uint32),
                      "queue": np.zeros(12 + 2 * n, np.uint32)}
         self.view["estimates"][:, 13] = materials
+        self.view_frames = 0
 
     def view_frame(self, first=0, invocations=0, max_hits=8, depth=0, ticket=(0, 0, 0, 0), view_first=False, shared=True,
                    clock_ms=0, events=None, n_events=0, measured_retention=1.0, far=None, topology=False):
@@ -561,7 +562,10 @@ class Frames:
         v = self.view
         n = v["receivers"].shape[0]
         wave = np.array([first, invocations or n, max_hits, depth, *ticket], np.uint32)
-        view = np.array([int(view_first), int(shared and self.n > 0), clock_ms, n_events, 192 * 192, 0, int(topology)], np.uint32)
+        frames = getattr(self, "view_frames", 0)
+        view = np.array([int(view_first), int(shared and self.n > 0), clock_ms, n_events, 192 * 192, 0, int(topology), frames,
+                         int(frames > 0)], np.uint32)
+        self.view_frames = frames + 1
         view[5] = np.float32(max(measured_retention, 0.0)).view(np.uint32)
         ev = np.zeros(4, np.uint32) if events is None else c(events, np.uint32)
         d, h, cl, _ = self.geometry

@@ -126,3 +126,25 @@ def test_topology_prior_seeds_new_receivers_like_the_oracle(gpu):
     finally:
         gpu.set_topology_prior(False)
     gpu.view_set_receivers(np.zeros((0, 5), np.int32))
+
+
+def test_sun_corners_are_traced_like_the_oracle(gpu):
+    """reproject_paths' corner sun words: faces lit by the sun trace their
+    four corners (some lit, some in shadow) and refresh one frame in 4."""
+    case = terrain_case(bounces=2)
+    ref = world(gpu, case, 1)
+    faces = case.faces[::4].copy()
+    gpu.view_set_receivers(faces)
+    ref.view_start(gpu.view_read()["receivers"], faces[:, 4])
+    for k in range(5):
+        gpu.view_frame(max_hits=1, clock_ms=300 + k)
+        ref.view_frame(max_hits=1, clock_ms=300 + k)
+        compare_view(gpu, ref, f"sun corners, view frame {k}")
+    corners = gpu.view_read()["estimates"][:, 14]
+    traced = corners != 0x80808080
+    assert traced.mean() > 0.3
+    corner_bytes = np.stack([(corners[traced] >> (8 * k)) & 255 for k in range(4)]).ravel()
+    valid = (corner_bytes & 128) != 0
+    sees_sun = (corner_bytes & 1) != 0
+    assert (valid & sees_sun).any() and (valid & ~sees_sun).any(), "corners in sun and in shadow"
+    gpu.view_set_receivers(np.zeros((0, 5), np.int32))
