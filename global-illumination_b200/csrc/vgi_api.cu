@@ -1597,14 +1597,14 @@ int vgi_view_set_receivers(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, c->v_paths.reserve(m * 8));
     VGI_CUDA(c, c->v_conts.reserve(m * 8));
     VGI_CUDA(c, c->v_estimates.reserve(m * 4));
-    VGI_CUDA(c, c->v_queue.reserve(12 + 2 * m));
+    VGI_CUDA(c, c->v_queue.reserve(12 + 2 * m + kSunFlipWords));
     if (n) {
         VGI_CUDA(c, cudaMemcpyAsync(c->v_receivers.ptr, receivers.data(), (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
         VGI_CUDA(c, cudaMemcpyAsync(c->v_estimates.ptr, estimates.data(), (size_t)n * 64, cudaMemcpyHostToDevice, c->stream));
         VGI_CUDA(c, cudaMemsetAsync(c->v_paths.ptr, 0, (size_t)n * 128, c->stream));
         VGI_CUDA(c, cudaMemsetAsync(c->v_conts.ptr, 0, (size_t)n * 128, c->stream));
     }
-    VGI_CUDA(c, cudaMemsetAsync(c->v_queue.ptr, 0, (12 + 2 * m) * 4, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->v_queue.ptr, 0, (12 + 2 * m + kSunFlipWords) * 4, c->stream));
     c->n_view = n;
     c->view_frames = 0;
     c->v_hash_valid = false;
@@ -1919,6 +1919,8 @@ int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events
         v.far_cells = c->far_cells[c->far_current].ptr;
         v.far_stats = c->far_stats.ptr;
     }
+    // This frame's sun-flip reports start empty.
+    VGI_CUDA(c, cudaMemsetAsync(c->v_queue.ptr + 12 + 2 * (size_t)c->n_view, 0, kSunFlipWords * 4, c->stream));
     v.frame = c->view_frames;
     v.has_previous = c->view_frames > 0 ? 1u : 0u;
     v.n_directional = c->n_directional;
@@ -1935,6 +1937,18 @@ int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events
     launch_view_frame(v, transport_limited(c), c->transport.budgeted != 0, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     c->view_frames += 1;
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
+int vgi_view_read_sun_flips(vgi_ctx* c, uint32_t* words) {
+    if (!c || !words) return VGI_ERR_INVALID;
+    if (c->n_view == 0) {
+        std::fill(words, words + kSunFlipWords, 0u);
+        return VGI_OK;
+    }
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    VGI_CUDA(c, cudaMemcpyAsync(words, c->v_queue.ptr + 12 + 2 * (size_t)c->n_view, kSunFlipWords * 4, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }

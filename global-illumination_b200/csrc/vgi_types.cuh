@@ -144,6 +144,10 @@ struct FarView {
     uint32_t hash_mask;
     uint32_t n_receivers;
 };
+// Sun-flip reports after a view queue of 12 + 2n words: a count and 3
+// zero words, kMaxSunFlips records (voxel xyz, flux bits), then the overflow
+// (biased min xyz as max of bias - v, max xyz biased, flux x 64 summed).
+constexpr uint32_t kMaxSunFlips = 2048u, kSunFlipWords = 4u + kMaxSunFlips * 4u + 7u;
 struct ViewArgs {
     TraceArgs t;
     uint4* receivers;      // 2 per receiver: surface xyz, face | voxel xyz, sequence

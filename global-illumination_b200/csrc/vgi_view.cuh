@@ -290,6 +290,50 @@ __device__ __forceinline__ uint32_t view_shared_slot(const ViewArgs& V, uint32_t
 
 // reproject_paths' share for caller-given receivers: the receiver takes its
 // estimate's sequence, and every receiver is its own owner (queue rank = index).
+// report_sun_flips (voxel_view_runtime.wgsl:231-270): the flux a face's
+// corners gained or lost from the sun between two corner words, queued as
+// (voxel, flux) for the scheduler; past kMaxSunFlips records the flips widen
+// one overflow box and add to its summed flux.
+__device__ void report_sun_flips(const ViewArgs& V, I3 voxel, V3 normal, uint32_t material, uint32_t before, uint32_t after) {
+    const V3 w{0.2126f, 0.7152f, 0.0722f};
+    float flux = 0.0f;
+    uint32_t bit = 0u;
+    for (uint32_t i = 0; i < V.n_directional && bit < 4u; ++i) {
+        const float4 p = __ldg(V.t.lights + i * 3u), e = __ldg(V.t.lights + i * 3u + 1u), x = __ldg(V.t.lights + i * 3u + 2u);
+        const V3 color{wmax(__fsub_rn(e.x, x.y), 0.0f), wmax(__fsub_rn(e.y, x.z), 0.0f), wmax(__fsub_rn(e.z, x.w), 0.0f)};
+        if (color.x == 0.0f && color.y == 0.0f && color.z == 0.0f) continue;
+        const float cosine = wmax(dot3(normal, normalize3(V3{p.x, p.y, p.z})), 0.0f);
+        for (uint32_t corner = 0; corner < 4u; ++corner) {
+            const uint32_t a = (before >> (corner * 8u)) & 255u, b = (after >> (corner * 8u)) & 255u;
+            if ((a & b & 128u) != 0u && ((a ^ b) & (1u << bit)) != 0u)
+                flux = __fadd_rn(flux, __fmul_rn(__fmul_rn(0.25f, dot3(color, w)), cosine));
+        }
+        bit += 1u;
+    }
+    if (flux <= 0.0f) return;
+    const float4 d = __ldg(V.t.materials + (material & 255u) * 4u);
+    flux = __fmul_rn(flux, dot3(V3{d.x, d.y, d.z}, w));
+    uint32_t* flips = V.queue + kViewPrefix + 2u * V.n;
+    const uint32_t slot = atomicAdd(flips, 1u);
+    if (slot >= kMaxSunFlips) {
+        uint32_t* overflow = flips + 4u + kMaxSunFlips * 4u;
+        const int bias = 1073741824;
+        atomicMax(overflow + 0, (uint32_t)(bias - voxel.x));
+        atomicMax(overflow + 1, (uint32_t)(bias - voxel.y));
+        atomicMax(overflow + 2, (uint32_t)(bias - voxel.z));
+        atomicMax(overflow + 3, (uint32_t)(voxel.x + bias));
+        atomicMax(overflow + 4, (uint32_t)(voxel.y + bias));
+        atomicMax(overflow + 5, (uint32_t)(voxel.z + bias));
+        atomicAdd(overflow + 6, (uint32_t)__fadd_rn(__fmul_rn(flux, 64.0f), 0.5f));
+        return;
+    }
+    uint32_t* record = flips + 4u + slot * 4u;
+    record[0] = (uint32_t)voxel.x;
+    record[1] = (uint32_t)voxel.y;
+    record[2] = (uint32_t)voxel.z;
+    record[3] = __float_as_uint(flux);
+}
+
 // sky_corner_visibility (voxel_path.wgsl:246-266): per directional light
 // with visible colour (at most 4) whether the corner sees it; all zero when a
 // ray runs out of steps, bit 31 set otherwise.
@@ -356,6 +400,8 @@ __global__ void __launch_bounds__(kBlock) view_reproject_kernel(const ViewArgs V
                 const uint32_t word = sky_corner_visibility(V.t, V.n_directional, position);
                 corners |= ((word & 15u) | ((word >> 24u) & 128u)) << (corner * 8u);
             }
+            if (V.has_previous && old != 0u)
+                report_sun_flips(V, I3{(int)r1.x, (int)r1.y, (int)r1.z}, normal, V.estimates[i * 4u + 3u].y, old, corners);
         }
         V.estimates[i * 4u + 3u].z = corners;
     }
@@ -411,6 +457,12 @@ __global__ void __launch_bounds__(kBlock) view_load_kernel(const ViewArgs V) {
     if (__uint_as_float(shown.w) == 0.0f && count > 0u) {
         const uint4 sh = base[6];
         shown = __uint_as_float(sh.w) > 0.0f ? sh : make_uint4(mean.x, mean.y, mean.z, __float_as_uint(1.0f));
+    }
+    // A face entering view again compares its fresh corners with those the
+    // world slot kept from when it was last seen.
+    if (identity.w != incarnation) {
+        const uint4 r0 = V.receivers[i * 2u], r1 = V.receivers[i * 2u + 1u];
+        report_sun_flips(V, I3{(int)r1.x, (int)r1.y, (int)r1.z}, face_normal(r0.w), identity.y, base[8].x, identity.z);
     }
     identity.w = incarnation;
     const bool pending = V.conts[i * 8u + 4u].w == 1u;

@@ -266,6 +266,7 @@ _SIGNATURES = {
     "vgi_far_reset": (_INT, [_P]),
     "vgi_set_far_handoff": (_INT, [_P, _INT]),
     "vgi_set_topology_prior": (_INT, [_P, _INT]),
+    "vgi_view_read_sun_flips": (_INT, [_P, _P]),
     "vgi_view_set_tiles": (_INT, [_P, _P, _U32, _U32, _U32]),
     "vgi_view_reconstruct": (_INT, [_P, _P]),
     "vgi_view_read_published": (_INT, [_P, _P, _P]),
@@ -750,6 +751,13 @@ class GpuTracer:
                      (ctypes.c_float * 3)(*map(float, up)), float(tan_half_fov), width, height)
         st = (settings or FarTierSettings()).struct()
         self._check(self._lib.vgi_far_frame(self._h, ctypes.byref(cam), ctypes.byref(st), frame & 0xFFFFFFFF))
+
+    def view_read_sun_flips(self):
+        """(records (count, 4): voxel xyz, flux bits, up to 2048; overflow (7,))."""
+        words = np.zeros(4 + 2048 * 4 + 7, np.uint32)
+        self._check(self._lib.vgi_view_read_sun_flips(self._h, _ptr(words)))
+        count = int(words[0])
+        return words[4:4 + 4 * min(count, 2048)].reshape(-1, 4), words[4 + 2048 * 4:]
 
     def set_topology_prior(self, enable: bool) -> None:
         self._check(self._lib.vgi_set_topology_prior(self._h, 1 if enable else 0))

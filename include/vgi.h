@@ -255,6 +255,14 @@ int vgi_view_set_receivers(vgi_ctx* ctx, const vgi_face* faces, uint32_t n);
  * Synchronous. */
 int vgi_view_frame(vgi_ctx* ctx, const vgi_view_wave* wave, const uint32_t* events, uint32_t n_events, uint64_t n_words);
 /* Snapshots of the view records; each pointer may be null. */
+/* The last view frame's sun-flip reports (report_sun_flips,
+ * voxel_view_runtime.wgsl:229-270): faces whose refreshed corner words, or
+ * whose corners on re-entering view against those their world slot kept,
+ * changed a lit bit. 8,203 words: the count and 3 zeros; 2,048 records
+ * (voxel xyz, flux as f32 bits) in an arbitrary order; then the overflow of
+ * flips past 2,048: max of 2^30 - voxel xyz, max of voxel xyz + 2^30, and
+ * the sum of round(flux * 64). */
+int vgi_view_read_sun_flips(vgi_ctx* ctx, uint32_t* words);
 int vgi_view_read(vgi_ctx* ctx, uint32_t* receivers8, uint32_t* paths32, uint32_t* continuations32, uint32_t* estimates16,
                   uint32_t* queue);
 /* trace_view_paths: `samples` complete receiver samples per receiver

@@ -2443,7 +2443,43 @@ int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* hea
     Shared sh{state, meta, index, view_words[1] != 0u};
     const uint32_t clock = view_words[2], n_events = view_words[3], reach = view_words[4];
     const float physical = bitsf(view_words[5]);
-    for (uint32_t i = 0; i < PREFIX + 2 * n; ++i) queue[i] = 0u;
+    const uint32_t FLIP_WORDS = 4u + 2048u * 4u + 7u;
+    for (uint32_t i = 0; i < PREFIX + 2 * n + FLIP_WORDS; ++i) queue[i] = 0u;
+    // report_sun_flips (voxel_view_runtime.wgsl:231-270)
+    auto report_sun_flips = [&](const uint32_t* r, f3 normal, uint32_t material, uint32_t before, uint32_t after) {
+        const f3 w{0.2126f, 0.7152f, 0.0722f};
+        const uint32_t nd = fbits(params[11]);
+        float flux = 0.0f;
+        uint32_t bit = 0u;
+        for (uint32_t l = 0; l < nd && bit < 4u; ++l) {
+            const float* L = lights + (size_t)l * 12;
+            const f3 color{wmax(L[4] - L[9], 0.0f), wmax(L[5] - L[10], 0.0f), wmax(L[6] - L[11], 0.0f)};
+            if (color.x == 0.0f && color.y == 0.0f && color.z == 0.0f) continue;
+            const float cosine = wmax(dot(normal, normalize(f3{L[0], L[1], L[2]})), 0.0f);
+            for (uint32_t corner = 0; corner < 4u; ++corner) {
+                const uint32_t a = (before >> (corner * 8u)) & 255u, b = (after >> (corner * 8u)) & 255u;
+                if ((a & b & 128u) != 0u && ((a ^ b) & (1u << bit)) != 0u) flux = flux + 0.25f * dot(color, w) * cosine;
+            }
+            bit += 1u;
+        }
+        if (flux <= 0.0f) return;
+        const float* d = materials + (size_t)(material & 255u) * 16;
+        flux = flux * dot(f3{d[0], d[1], d[2]}, w);
+        uint32_t* flips = queue + PREFIX + 2 * n;
+        const uint32_t slot = flips[0]++;
+        if (slot >= 2048u) {
+            uint32_t* overflow = flips + 4 + 2048 * 4;
+            const int32_t bias = 1073741824;
+            for (int k = 0; k < 3; ++k) {
+                overflow[k] = umax(overflow[k], (uint32_t)(bias - (int32_t)r[4 + k]));
+                overflow[3 + k] = umax(overflow[3 + k], (uint32_t)((int32_t)r[4 + k] + bias));
+            }
+            overflow[6] += (uint32_t)(flux * 64.0f + 0.5f);
+            return;
+        }
+        uint32_t* record = flips + 4 + (size_t)slot * 4;
+        record[0] = r[4]; record[1] = r[5]; record[2] = r[6]; record[3] = fbits(flux);
+    };
     uint32_t* owners = queue + PREFIX;
     uint32_t* cursor = queue + PREFIX + n;
     // reproject_paths: the receiver's sequence is its estimate's, and every
@@ -2494,6 +2530,7 @@ int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* hea
                 const uint32_t word = sky_corner_visibility(position);
                 corners |= ((word & 15u) | ((word >> 24u) & 128u)) << (corner * 8u);
             }
+            if (has_previous && old != 0u) report_sun_flips(r, normal, e[13], old, corners);
         }
         e[14] = corners;
         r[7] = e[12];
@@ -2544,6 +2581,7 @@ int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* hea
                 if (shown.w > 0.0f) wF4(e + 8, shown);
                 else { e[8] = e[0]; e[9] = e[1]; e[10] = e[2]; e[11] = fbits(1.0f); }
             }
+            if (e[15] != incarnation) report_sun_flips(r, face_normal(r[3]), e[13], base[32], e[14]);
             e[15] = incarnation;
             const bool pending = conts[(size_t)i * 32 + 19] == 1u;
             const uint32_t rank = cursor[i];

@@ -203,6 +203,9 @@ def discovered_faces(pixels):
     return rows[np.lexsort((rows[:, 3], rows[:, 0], rows[:, 1], rows[:, 2]))]
 
 
+SUN_FLIP_WORDS = 4 + 2048 * 4 + 7  # the view queue's sun-flip reports
+
+
 class FarTier:
     """The far tier's host side restated (vgi_far_frame): settings
     normalisation, cell size, the view words, the previous camera and the
@@ -551,7 +554,7 @@ class Frames:
         n = receivers.shape[0]
         self.view = {"receivers": c(receivers, np.uint32).copy(), "paths": np.zeros((n, 32), np.uint32),
                      "continuations": np.zeros((n, 32), np.uint32), "estimates": np.zeros((n, 16), np.uint32),
-                     "queue": np.zeros(12 + 2 * n, np.uint32)}
+                     "queue": np.zeros(12 + 2 * n + SUN_FLIP_WORDS, np.uint32)}
         self.view["estimates"][:, 13] = materials
         self.view_frames = 0
 

@@ -36,7 +36,16 @@ def receivers_for(faces):
 def compare_view(gpu, ref, what):
     got = gpu.view_read()
     for key in ("receivers", "paths", "continuations", "estimates", "queue"):
-        assert_words_equal(got[key], ref.view[key], f"{what}: view {key}")
+        want = ref.view[key][: got[key].size] if key == "queue" else ref.view[key]
+        assert_words_equal(got[key], want, f"{what}: view {key}")
+    # Sun-flip reports: the GPU queues them in arbitrary order.
+    records, overflow = gpu.view_read_sun_flips()
+    flips = ref.view["queue"][got["queue"].size:]
+    count = int(flips[0])
+    want = flips[4:4 + 4 * min(count, 2048)].reshape(-1, 4)
+    order = lambda a: a[np.lexsort(a.T[::-1])] if len(a) else a
+    assert_words_equal(order(records), order(want), f"{what}: sun flips")
+    assert_words_equal(overflow, flips[4 + 2048 * 4:], f"{what}: sun-flip overflow")
     assert_words_equal(gpu.read_state(), ref.state, f"{what}: world state")
     assert_words_equal(gpu.read_slot_meta(), ref.meta, f"{what}: world slot metadata")
 
@@ -147,4 +156,15 @@ def test_sun_corners_are_traced_like_the_oracle(gpu):
     valid = (corner_bytes & 128) != 0
     sees_sun = (corner_bytes & 1) != 0
     assert (valid & sees_sun).any() and (valid & ~sees_sun).any(), "corners in sun and in shadow"
+    # The sun turns: as each face refreshes, corners that changed are reported as flips.
+    sun = vgi.DirectionalTransportLight((-0.6, 0.5, -0.2), (3.0, 3.0, 3.0)).words()
+    gpu.set_lights(sun, 1)
+    ref.lights = sun
+    flips = 0
+    for k in range(4):
+        gpu.view_frame(max_hits=1, clock_ms=310 + k)
+        ref.view_frame(max_hits=1, clock_ms=310 + k)
+        compare_view(gpu, ref, f"sun corners after the sun turned, view frame {k}")
+        flips += len(gpu.view_read_sun_flips()[0])
+    assert flips > 0
     gpu.view_set_receivers(np.zeros((0, 5), np.int32))
