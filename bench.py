@@ -280,16 +280,54 @@ def mlp_comparison(g, faces, ref, stream, flush, plain, clock, max_frames):
     return out, clock
 
 
-def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total, budget_s=15.0):
-    """The oracle on a bounded face sample with the GPU's warm cache state."""
+def bench_config(n_faces, warmup):
+    """The workload both arms report, word for word the same: the GPU arm
+    traces whole frames of it, the CPU arm bounded face samples of the same
+    frames from the same warm state."""
+    return {"workload": WORKLOAD, "scene_seed": 2, "faces": int(n_faces), "spp": SPP, "bounces": BOUNCES, "path_steps": 2048,
+            "warm_state": f"world cache after {warmup} frames from empty, then one frame per step",
+            "l2": "device arm: a 256 MB buffer written between timed frames, outside the event pair; the host arm has no device L2"}
+
+
+def oracle_scene(seed=2, regions=(32, 16, 32), eye=EYE):
+    """The bench scene made with the oracle library alone (no libvgi): the
+    same seeded generator as make_scene, the materials and sun restated as
+    their GPU records."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    coords, vox = O.terrain(*regions, seed=seed, octaves=4, period=64.0, base_height=8.0 * regions[1], falloff=25.0 * regions[1],
+                            emitters=256)
+    rng = np.random.default_rng(seed)
+    entries = [((0.45, 0.45, 0.45), (0.0, 0.0, 0.0))] * 256
+    for k in range(8):
+        entries[k] = (tuple(rng.uniform(0.2, 0.8, 3)), (0.0, 0.0, 0.0))
+    for k in range(248):
+        r = float(rng.uniform(1.0, 10.0))
+        entries[8 + k] = ((0.5, 0.5, 0.5), (r, r, r))
+    words = O.material_words(entries)
+    sun = O.directional_light_words((0.4, 0.8, 0.3), (3.0, 3.0, 3.0))
+    faces = O.exposed_faces(coords, vox, facing=eye)
+    return coords, vox, words, sun, faces
+
+
+def cpu_baseline(g, coords, vox, words, lights, faces, budget_s=15.0, parity_faces=2048):
+    """The oracle on a bounded face sample with the GPU's warm state, on all
+    host threads, and the parity leg: the GPU re-traces the sample's first
+    chunk (trace_tasks: the same tasks, sequences, cache state and face
+    index) and its results are compared with the oracle's word for word. The
+    oracle builds its own geometry and emitters from the voxels."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
 
     n = faces.shape[0]
+    scene = O.Scene(coords, vox, top_mode=0)
+    geometry = scene.arrays()
+    emitters, n_emit, total = O.emitters(coords, vox, words)
     state = g.read_state()
     index = O.face_index(faces[:, :4])
     rng = np.random.default_rng(7)
-    sample = np.sort(rng.choice(n, size=min(n, 2048), replace=False))
+    sample = np.sort(rng.choice(n, size=min(n, parity_faces), replace=False))
     tasks = np.zeros((sample.size, 8), np.uint32)
     tasks[:, 0:3] = faces[sample, 0:3].view(np.uint32)
     tasks[:, 3] = faces[sample, 3]
@@ -298,76 +336,83 @@ def cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit,
     params = O.params_words(sample.size, SPP, d.size // 4, 1, geometry[3], 1, (0, 0, 0), total, n_emit)
     threads = os.cpu_count() or 1
     pipe = O.Pipeline(BOUNCES, 0, 2048, 0, SPP)
+    gpu_first = g.trace_tasks(tasks, SPP)
     rays = 0
     start = time.perf_counter()
     chunks = 0
+    ref_first = None
     while True:
         # Successive chunks trace the sample's next frames (sequence + spp).
-        _, cnt = O.trace_faces(geometry, params, words, lights, emitters, tasks, pipe, state, index, threads)
+        out, cnt = O.trace_faces(geometry, params, words, lights, emitters, tasks, pipe, state, index, threads)
+        if ref_first is None:
+            ref_first = out
         tasks[:, 4] += SPP
         rays += cnt["rays"]
         chunks += 1
         if time.perf_counter() - start > budget_s or chunks >= 100000:
             break
     elapsed = time.perf_counter() - start
-    return {"value": rays / elapsed, "unit": "rays/s", "cores": threads, "kind": "port",
+    base = {"value": rays / elapsed, "unit": "rays/s", "cores": threads, "kind": "port",
             "sample": f"{chunks} x {sample.size} of {n} faces (seeded), {SPP} spp, the GPU's warm cache state, {threads} threads, {elapsed:.1f} s"}
+    differ = gpu_first != ref_first
+    parity = {"faces": int(sample.size), "words": int(differ.size), "words_differ": int(differ.sum()),
+              "faces_differ": int(differ.any(axis=1).sum()),
+              "how": "GPU trace_tasks vs the oracle on the same seeded faces, tasks, warm state and face index; "
+                     "the oracle's geometry and emitters built from the voxels"}
+    return base, parity
 
 
 def run_reference(args):
-    """--impl reference: the CPU oracle (restatement of the reference's
-    algorithm) on bounded samples of the same workload, all host threads."""
+    """--impl reference: the CPU oracle (the restatement of the reference's
+    algorithm; the reference itself is Rust/WGSL with no CPU path) on the
+    same workload, all host threads, without loading libvgi. Its warm-up
+    runs the GPU arm's warm-up frames in full (so the state is the one the
+    GPU arm's timed frames start from: the two are bit-identical); each
+    timed step is one frame over a seeded sample of the faces."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
-    import vgi
 
-    coords, vox, words, lights, faces, transport = make_scene(2)
+    coords, vox, words, lights, faces = oracle_scene(2)
     scene = O.Scene(coords, vox, top_mode=0)
     geometry = scene.arrays()
     emitters, n_emit, total = O.emitters(coords, vox, words)
     n = faces.shape[0]
-    # Warm-cache equivalent of the GPU's steady state: every slot holds 16+
-    # samples (the ray work depends only on which faces are cached, not on
-    # their values), sequences advanced as after the warm-up frames.
-    state = np.zeros((n, 36), np.uint32)
-    state[:, 5] = 16
-    state[:, 6] = SPP * 2
-    index = O.face_index(faces[:, :4])
     threads = os.cpu_count() or 1
-    pipe = O.Pipeline(BOUNCES, 0, 2048, 0, SPP)
+    d = geometry[0]
+
+    def params(count, samples):
+        return O.params_words(count, samples, d.size // 4, 1, geometry[3], 1, (0, 0, 0), total, n_emit)
+
+    frames = O.Frames(geometry, params, words, lights, emitters, faces, O.transport_settings(bounces=BOUNCES, path_steps=2048),
+                      O.Pipeline(BOUNCES, 0, 2048, 0, SPP), threads=threads)
+    clock = 0
+    t0 = time.perf_counter()
+    for _ in range(args.warmup):
+        frames.frame(SPP, clock)
+        clock += 16
+    warm_s = time.perf_counter() - t0
     rng = np.random.default_rng(11)
-    per_step = 2048
-
-    def step(k):
-        sample = np.sort(rng.choice(n, size=per_step, replace=False))
-        tasks = np.zeros((per_step, 8), np.uint32)
-        tasks[:, 0:3] = faces[sample, 0:3].view(np.uint32)
-        tasks[:, 3] = faces[sample, 3]
-        tasks[:, 4] = SPP * (2 + k)
-        params = O.params_words(per_step, SPP, geometry[0].size // 4, 1, geometry[3], 1, (0, 0, 0), total, n_emit)
-        t0 = time.perf_counter()
-        _, cnt = O.trace_faces(geometry, params, words, lights, emitters, tasks, pipe, state, index, threads)
-        return cnt["rays"], time.perf_counter() - t0
-
-    for k in range(args.warmup):
-        step(k)
+    per_step = min(n, 8192)
     rays, secs = 0, 0.0
-    for k in range(args.steps):
-        r, s = step(args.warmup + k)
-        rays += r
-        secs += s
+    for _ in range(args.steps):
+        sample = np.sort(rng.choice(n, size=per_step, replace=False)).astype(np.uint32)
+        t0 = time.perf_counter()
+        cnt, _ = frames.frame_slots(SPP, clock, sample)
+        secs += time.perf_counter() - t0
+        clock += 16
+        rays += cnt["rays"]
     value = rays / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "faces": int(n), "spp": SPP, "bounces": BOUNCES,
-                   "step": f"oracle trace of {per_step} seeded faces of {n} per step (bounded CPU sample)"},
+        "config": bench_config(n, args.warmup),
         "cpu_baseline": {"value": value, "unit": "rays/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} steps x {per_step} of {n} faces, warm-cache counts, {threads} threads"},
+                         "sample": f"{args.warmup} full warm-up frames ({warm_s:.1f} s), then {args.steps} frames over "
+                                   f"{per_step} seeded faces of {n} each (begin, trace with gather, accumulate), {threads} threads"},
         "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -803,11 +848,9 @@ def main():
     if rank == 0:
         plain_frames = 2 * args.warmup + 3 * args.steps + 1  # warm-up, timed, graph, e2e warm-up and e2e frames
         quality = relmse(g, reference, plain_frames)
-        base = None
+        base = parity = None
         if world == 1 and not args.no_cpu_baseline:
-            geometry = g.geometry()
-            emitters, n_emit, total = vgi.host_emitters(coords, vox, words)
-            base = cpu_baseline(g, geometry, words, lights, faces, transport, emitters, n_emit, total)
+            base, parity = cpu_baseline(g, coords, vox, words, lights, faces)
         mlp = None
         if not args.no_mlp:
             # After the CPU baseline, which reads the plain trace's warm state.
@@ -830,13 +873,14 @@ def main():
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "faces": int(n), "spp": SPP, "bounces": BOUNCES, "parallelism": f"independent scene per GPU x{world}",
-                       "paths_per_frame": int(paths_per_frame), "rays_per_frame": rays_per_frame,
+            "config": bench_config(n, args.warmup),
+            "parallelism": f"independent scene per GPU x{world}",
+            "parity": parity,
+            "detail": {"paths_per_frame": int(paths_per_frame), "rays_per_frame": rays_per_frame,
                        "census": {"steps": before["steps"], "bytes": before["bytes"], "traverse_bytes": before["traverse_bytes"],
                                   "cache_hits": before["cache_hits"],
                                   "unknown": before["unknown"], "status": before["status"]},
                        "traverse_lanes": lane_use(before),
-                       "l2": "256 MB buffer written between timed frames (outside the event pair)",
                        "kernel_ms": {"prepare": float(np.mean([t[0] for t in kernel_ms])), "trace": trace_ms,
                                      "traverse": traverse_ms, "accumulate": float(np.mean([t[2] for t in kernel_ms]))},
                        "trace_algorithmic_gbs": bytes_per_frame / (trace_ms * 1e-3) / 1e9,

@@ -28,6 +28,20 @@ namespace {
 
 using namespace vgi;
 
+// Failures injected by vgi_inject_failure for the calling thread (a context
+// has one owner thread): the next `alloc` device allocations and `upload`
+// host-to-device copies fail without reaching the device.
+thread_local uint32_t t_fail_allocs = 0, t_fail_uploads = 0;
+
+// A host-to-device copy on `s`, or the injected failure.
+cudaError_t h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (t_fail_uploads) {
+        --t_fail_uploads;
+        return cudaErrorInvalidValue;
+    }
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+}
+
 template <class T>
 struct DevBuf {
     T* ptr = nullptr;
@@ -38,6 +52,10 @@ struct DevBuf {
         ptr = nullptr;
         count = 0;
         if (n == 0) return cudaSuccess;
+        if (t_fail_allocs) {
+            --t_fail_allocs;
+            return cudaErrorMemoryAllocation;
+        }
         cudaError_t e = cudaMalloc(&ptr, n * sizeof(T));
         if (e == cudaSuccess) count = n;
         return e;
@@ -140,6 +158,7 @@ struct vgi_ctx {
     DevBuf<uint32_t> mlp_query_count;         // queries of the last terminating frame
     uint32_t mlp_queue_capacity = 0;          // paths of the last terminating frame's trace
     uint32_t mlp_ctas = 0, mlp_sms = 0;
+    uint32_t mlp_wait = kMlpWaitPolls;  // polls per tensor-core wait (vgi_mlp_set_wait_limit)
     // MLP termination in vgi_frame: off, or on after `mlp_warm` plain frames
     // that train the network; `mlp_batch` rows x `mlp_train_steps` steps a frame.
     bool mlp_cache = false;
@@ -451,6 +470,7 @@ int wave_buffers(vgi_ctx* c, const TraceArgs& a, bool count, bool marks, WaveBuf
         b.mlp_queue = c->w_mlp_queue.ptr;
         b.mlp_error = c->mlp_error.ptr + 1;
         b.mlp_ctas = c->mlp_ctas;
+        b.mlp_wait = c->mlp_wait;
         b.mlp_enc = mlp_encoding(c);
         if (c->timing && !count && marks) b.mlp_marks = c->mlp_marks;
         if (marks) c->mlp_queue_capacity = (uint32_t)paths;
@@ -508,7 +528,7 @@ int finish_headers(vgi_ctx* c) {
         c->host_headers[r].w = pos;
     }
     VGI_CUDA(c, c->zw.reserve(std::max<size_t>(n, 1)));
-    VGI_CUDA(c, cudaMemcpyAsync(c->zw.ptr, zw.data(), n * sizeof(uint2), cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->zw.ptr, zw.data(), n * sizeof(uint2), c->stream));
     launch_set_header_extents(c->headers.ptr, c->zw.ptr, n, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     return VGI_OK;
@@ -529,10 +549,10 @@ int pack_regions(vgi_ctx* c, const std::vector<uint32_t>* list) {
     if (list) {
         grid = (uint32_t)list->size();
         VGI_CUDA(c, c->region_list.reserve(std::max<size_t>(grid, 1)));
-        VGI_CUDA(c, cudaMemcpyAsync(c->region_list.ptr, list->data(), grid * 4, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, h2d(c->region_list.ptr, list->data(), grid * 4, c->stream));
         dlist = c->region_list.ptr;
     }
-    VGI_CUDA(c, cudaMemcpyAsync(c->alloc.ptr, &c->cells_used, 8, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->alloc.ptr, &c->cells_used, 8, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->pack_error.ptr, 0, 4, c->stream));
     launch_classify_pack(c->voxels.ptr, dlist, grid, n, c->headers.ptr, c->cells.ptr, c->alloc.ptr, c->cells.count, c->pack_error.ptr,
                          c->stream);
@@ -567,8 +587,11 @@ int vgi_create(const vgi_config* config, vgi_ctx** out) {
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return VGI_UNAVAILABLE;
     int device = config ? config->device : 0;
     if (device < 0 || device >= count) return VGI_ERR_INVALID;
+    // A device that cannot set up a context idles the caller like a missing
+    // one (the reference's transport_unavailable after a failed pipeline
+    // build, src/tests.rs:38-80): no context, VGI_UNAVAILABLE.
     if (cudaSetDevice(device) != cudaSuccess) return VGI_UNAVAILABLE;
-    if (init_trace_constants() != cudaSuccess) return VGI_ERR_CUDA;
+    if (init_trace_constants() != cudaSuccess) return VGI_UNAVAILABLE;
     auto* c = new vgi_ctx();
     c->device = device;
     c->transport = default_transport();
@@ -577,8 +600,8 @@ int vgi_create(const vgi_config* config, vgi_ctx** out) {
     c->traverse_blocks = (uint32_t)sms * wave_traverse_blocks_per_sm();
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         c->counters.reserve(16) != cudaSuccess || c->alloc.reserve(1) != cudaSuccess || c->pack_error.reserve(1) != cudaSuccess) {
-        delete c;
-        return VGI_ERR_CUDA;
+        vgi_destroy(c);
+        return VGI_UNAVAILABLE;
     }
     *out = c;
     return VGI_OK;
@@ -644,14 +667,21 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
     if (c) drop_graph(c);  // what a frame launches may change
     if (!c || (n && (!coords || !voxels))) return VGI_ERR_INVALID;
     VGI_CUDA(c, cudaSetDevice(c->device));
-    c->keys.assign(n, RegionKey{0, 0, 0});
-    c->where.clear();
+    // Refused inputs leave the context as it was.
+    std::vector<RegionKey> keys(n, RegionKey{0, 0, 0});
+    std::unordered_map<RegionKey, uint32_t, RegionKeyHash> where;
     for (uint32_t r = 0; r < n; ++r) {
-        c->keys[r] = RegionKey{coords[r * 3], coords[r * 3 + 1], coords[r * 3 + 2]};
-        if (!c->where.emplace(c->keys[r], r).second) return fail(c, VGI_ERR_INVALID, "duplicate region coordinate");
+        keys[r] = RegionKey{coords[r * 3], coords[r * 3 + 1], coords[r * 3 + 2]};
+        if (!where.emplace(keys[r], r).second) return fail(c, VGI_ERR_INVALID, "duplicate region coordinate");
     }
     for (size_t i = 0; i < (size_t)n * 4096; ++i)
         if (voxels[i] > 256) return fail(c, VGI_ERR_INVALID, "voxel value above 256 (materials are 0..255, 256 is air)");
+    // From here a failure (allocation, copy) leaves no geometry: frames and
+    // edits are refused with VGI_ERR_STATE until an upload succeeds, and
+    // never read half-replaced buffers.
+    c->geometry = false;
+    c->keys = std::move(keys);
+    c->where = std::move(where);
     c->host_voxels.assign(voxels, voxels + (size_t)n * 4096);
     c->strides.assign(n, 0);
     if (strides) std::copy(strides, strides + n, c->strides.begin());
@@ -663,7 +693,7 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
     VGI_CUDA(c, c->headers.reserve(std::max<uint32_t>(n, 1)));
     VGI_CUDA(c, c->cells.reserve(capacity));
     c->cells.count = capacity;
-    if (n) VGI_CUDA(c, cudaMemcpyAsync(c->voxels.ptr, voxels, (size_t)n * 8192, cudaMemcpyHostToDevice, c->stream));
+    if (n) VGI_CUDA(c, h2d(c->voxels.ptr, voxels, (size_t)n * 8192, c->stream));
     c->cells_used = 0;
     int rc = pack_regions(c, nullptr);
     if (rc != VGI_OK) return rc;
@@ -684,7 +714,7 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
     std::vector<int32_t> dir = build_directory(c->keys);
     c->dir_slots = dir.size() / 4;
     VGI_CUDA(c, c->directory.reserve(c->dir_slots));
-    VGI_CUDA(c, cudaMemcpyAsync(c->directory.ptr, dir.data(), dir.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->directory.ptr, dir.data(), dir.size() * 4, c->stream));
     VGI_CUDA(c, upload_grid(c, dir.data(), c->dir_slots));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->geometry = true;
@@ -725,9 +755,9 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
     VGI_CUDA(c, c->directory.reserve(slots));
     VGI_CUDA(c, c->headers.reserve(std::max<uint32_t>(n_headers, 1)));
     VGI_CUDA(c, c->cells.reserve(std::max<uint64_t>(n_cells, 1)));
-    VGI_CUDA(c, cudaMemcpyAsync(c->directory.ptr, directory, slots * 16, cudaMemcpyHostToDevice, c->stream));
-    if (n_headers) VGI_CUDA(c, cudaMemcpyAsync(c->headers.ptr, headers, (size_t)n_headers * 16, cudaMemcpyHostToDevice, c->stream));
-    if (n_cells) VGI_CUDA(c, cudaMemcpyAsync(c->cells.ptr, cells, n_cells * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->directory.ptr, directory, slots * 16, c->stream));
+    if (n_headers) VGI_CUDA(c, h2d(c->headers.ptr, headers, (size_t)n_headers * 16, c->stream));
+    if (n_cells) VGI_CUDA(c, h2d(c->cells.ptr, cells, n_cells * 4, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->dir_slots = slots;
     c->cells_used = n_cells;
@@ -778,7 +808,7 @@ int vgi_edit_voxels(vgi_ctx* c, const int32_t* edits, uint32_t n) {
         packed.push_back(make_uint2(r, (local << 16) | (uint32_t)c->host_voxels[(size_t)r * 4096 + local]));
     }
     VGI_CUDA(c, c->edit_buf.reserve(packed.size()));
-    VGI_CUDA(c, cudaMemcpyAsync(c->edit_buf.ptr, packed.data(), packed.size() * sizeof(uint2), cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->edit_buf.ptr, packed.data(), packed.size() * sizeof(uint2), c->stream));
     launch_scatter_edits(c->edit_buf.ptr, (uint32_t)packed.size(), c->voxels.ptr, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     // Repack only the edited regions into fresh cell space; a full repack
@@ -835,7 +865,7 @@ int vgi_set_materials(vgi_ctx* c, const float* m) {
     VGI_CUDA(c, cudaSetDevice(c->device));
     c->host_materials.assign(m, m + 256 * 16);
     VGI_CUDA(c, c->materials.reserve(256 * 4));
-    VGI_CUDA(c, cudaMemcpyAsync(c->materials.ptr, m, 256 * 64, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->materials.ptr, m, 256 * 64, c->stream));
     // The luminance of each material's albedo and emission, for measuring
     // edits (ResidentCache::set_materials, src/gpu/resident.rs:816-838).
     std::vector<float2> light(256);
@@ -845,7 +875,7 @@ int vgi_set_materials(vgi_ctx* c, const float* m) {
         light[i] = make_float2(0.2126f * d[0] + 0.7152f * d[1] + 0.0722f * d[2], 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2]);
     }
     VGI_CUDA(c, c->material_light.reserve(256));
-    VGI_CUDA(c, cudaMemcpyAsync(c->material_light.ptr, light.data(), 256 * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->material_light.ptr, light.data(), 256 * sizeof(float2), c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }
@@ -858,7 +888,7 @@ int vgi_set_lights(vgi_ctx* c, const float* lights, uint32_t n, uint32_t n_direc
     std::vector<float> words(std::max<uint32_t>(n, 1) * 12, 0.0f);
     if (n) std::copy(lights, lights + n * 12, words.begin());
     VGI_CUDA(c, c->lights.reserve(words.size() / 4));
-    VGI_CUDA(c, cudaMemcpyAsync(c->lights.ptr, words.data(), words.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->lights.ptr, words.data(), words.size() * 4, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->n_lights = n;
     c->n_directional = n_directional;
@@ -909,7 +939,7 @@ int vgi_set_emitters(vgi_ctx* c, const uint32_t* words, uint64_t n_words, uint32
     }
     VGI_CUDA(c, cudaSetDevice(c->device));
     VGI_CUDA(c, c->emitters.reserve(n_words / 4));
-    VGI_CUDA(c, cudaMemcpyAsync(c->emitters.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->emitters.ptr, words, n_words * 4, c->stream));
     c->host_emitter_records.assign(words, words + (size_t)n_faces * 8);
     const uint32_t nodes = (uint32_t)((n_words - records * 8) / 16);
     VGI_CUDA(c, c->node_aux.reserve(2 * (size_t)std::max<uint32_t>(nodes, 1)));
@@ -959,6 +989,10 @@ int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     }
     std::vector<uint32_t> index = build_face_index(keys);
     size_t m = std::max<uint32_t>(n, 1);
+    // Until this call succeeds the context has no faces: a failed allocation
+    // or copy below leaves frames refused (VGI_ERR_STATE), never reading
+    // released buffers with the old slot count.
+    c->n_slots = 0;
     VGI_CUDA(c, c->tasks.reserve(m * 2));
     VGI_CUDA(c, c->results.reserve(m * 6));
     VGI_CUDA(c, c->state.reserve(m * 9));
@@ -966,14 +1000,14 @@ int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, c->checkpoint.reserve(m * 3));
     VGI_CUDA(c, c->cache.reserve(m));
     VGI_CUDA(c, c->face_index.reserve(index.size() / 4));
-    VGI_CUDA(c, cudaMemcpyAsync(c->tasks.ptr, tasks.data(), (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->tasks.ptr, tasks.data(), (size_t)n * 32, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->results.ptr, 0, m * 96, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->state.ptr, 0, m * 144, c->stream));
     launch_seed_incarnations(c->state.ptr, n, c->stream);
-    VGI_CUDA(c, cudaMemcpyAsync(c->slot_meta.ptr, meta.data(), (size_t)n * 48, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->slot_meta.ptr, meta.data(), (size_t)n * 48, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->checkpoint.ptr, 0, m * 48, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->cache.ptr, 0, m * 16, c->stream));
-    VGI_CUDA(c, cudaMemcpyAsync(c->face_index.ptr, index.data(), index.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->face_index.ptr, index.data(), index.size() * 4, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->n_slots = n;
     c->batch_id = 1;  // a new face set starts a new batch sequence
@@ -1212,7 +1246,7 @@ int vgi_discover_faces(vgi_ctx* c, const vgi_camera* cam, uint32_t* pixels8, vgi
     VGI_CUDA(c, counters.reserve(2));
     float host_cam[10] = {cam->eye[0], cam->eye[1], cam->eye[2], cam->forward[0], cam->forward[1], cam->forward[2],
                           cam->up[0], cam->up[1], cam->up[2], cam->tan_half_fov};
-    VGI_CUDA(c, cudaMemcpyAsync(dcam.ptr, host_cam, sizeof(host_cam), cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(dcam.ptr, host_cam, sizeof(host_cam), c->stream));
     VGI_CUDA(c, cudaMemsetAsync(set.ptr, 0xff, (size_t)mask * 8, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(counters.ptr, 0, 8, c->stream));
     const TraceArgs tr = trace_args(c, nullptr, nullptr, 0, 1, false);
@@ -1302,7 +1336,7 @@ int vgi_trace_batch(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samp
     int rc = check_ready(c, true);
     if (rc != VGI_OK) return rc;
     if (!tasks || !results || n != c->n_slots) return fail(c, VGI_ERR_INVALID, "one task per slot expected");
-    VGI_CUDA(c, cudaMemcpyAsync(c->tasks.ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->tasks.ptr, tasks, (size_t)n * 32, c->stream));
     rc = vgi_frame(c, samples, clock_ms);
     if (rc != VGI_OK) return rc;
     VGI_CUDA(c, cudaMemcpyAsync(results, c->results.ptr, (size_t)n * 96, cudaMemcpyDeviceToHost, c->stream));
@@ -1330,7 +1364,7 @@ int vgi_submit_batch(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t sam
     VGI_CUDA(c, c->stage_results[b].reserve((size_t)n * 6));
     // Tasks in: after the frame of batch k - 2 has taken its staged tasks.
     if (reused) VGI_CUDA(c, cudaStreamWaitEvent(c->copy_in, c->tasks_free[b], 0));
-    VGI_CUDA(c, cudaMemcpyAsync(c->stage_tasks[b].ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->copy_in));
+    VGI_CUDA(c, h2d(c->stage_tasks[b].ptr, tasks, (size_t)n * 32, c->copy_in));
     VGI_CUDA(c, cudaEventRecord(c->tasks_ready[b], c->copy_in));
     // The frame, between the staged tasks and the staged results.
     VGI_CUDA(c, cudaStreamWaitEvent(c->stream, c->tasks_ready[b], 0));
@@ -1438,7 +1472,7 @@ int vgi_trace_tasks(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t samp
     if (n == 0) return VGI_OK;
     VGI_CUDA(c, c->scratch_tasks.reserve((size_t)n * 2));
     VGI_CUDA(c, c->scratch_results.reserve((size_t)n * 6));
-    VGI_CUDA(c, cudaMemcpyAsync(c->scratch_tasks.ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->scratch_tasks.ptr, tasks, (size_t)n * 32, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->counters.ptr, 0, kCounterWords * 8, c->stream));
     bool with_cache = c->n_slots > 0;
     TraceArgs tr = trace_args(c, c->scratch_tasks.ptr, c->scratch_results.ptr, n, samples, with_cache);
@@ -1455,7 +1489,7 @@ int vgi_apply_events(vgi_ctx* c, const uint32_t* words, uint32_t n_events, uint6
     if (c->n_slots == 0) return VGI_OK;
     VGI_CUDA(c, cudaSetDevice(c->device));
     VGI_CUDA(c, c->events.reserve(std::max<uint64_t>(n_words / 4, 1)));
-    if (n_words) VGI_CUDA(c, cudaMemcpyAsync(c->events.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    if (n_words) VGI_CUDA(c, h2d(c->events.ptr, words, n_words * 4, c->stream));
     c->n_events = n_events;
     AccumArgs acc = accum_args(c, 0, 0);
     launch_apply_events(acc, c->events.ptr, c->n_slots, c->stream);
@@ -1516,7 +1550,7 @@ static int apply_events_impl(vgi_ctx* c, const uint32_t* words, uint32_t n_event
     if (n_entries && !c->material_light.ptr) return fail(c, VGI_ERR_STATE, "measured edits need the material table");
     VGI_CUDA(c, cudaSetDevice(c->device));
     VGI_CUDA(c, c->events.reserve(std::max<uint64_t>(n_words / 4, 1)));
-    if (n_words) VGI_CUDA(c, cudaMemcpyAsync(c->events.ptr, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    if (n_words) VGI_CUDA(c, h2d(c->events.ptr, words, n_words * 4, c->stream));
     if (n_footprints) {
         // Where each changed box's shadow lands, into its reserved Light
         // event, before the measured edits and retention read the events.
@@ -1525,8 +1559,8 @@ static int apply_events_impl(vgi_ctx* c, const uint32_t* words, uint32_t n_event
         for (uint32_t e = 0; e < n_footprints; ++e) sums[(size_t)e * 8] = sums[(size_t)e * 8 + 1] = sums[(size_t)e * 8 + 2] = 0xffffffffu;
         VGI_CUDA(c, c->footprints.reserve((size_t)n_footprints * 3 + 1));
         VGI_CUDA(c, c->footprint_sums.reserve(sums.size()));
-        VGI_CUDA(c, cudaMemcpyAsync(c->footprints.ptr, footprints, ((size_t)n_footprints * 3 + 1) * 16, cudaMemcpyHostToDevice, c->stream));
-        VGI_CUDA(c, cudaMemcpyAsync(c->footprint_sums.ptr, sums.data(), sums.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, h2d(c->footprints.ptr, footprints, ((size_t)n_footprints * 3 + 1) * 16, c->stream));
+        VGI_CUDA(c, h2d(c->footprint_sums.ptr, sums.data(), sums.size() * 4, c->stream));
         const TraceArgs tr = trace_args(c, nullptr, nullptr, 0, 1, false);
         launch_footprints(tr, c->footprints.ptr, n_footprints, (uint32_t)threads, c->n_directional, c->footprint_sums.ptr, c->events.ptr,
                           c->stream);
@@ -1536,7 +1570,7 @@ static int apply_events_impl(vgi_ctx* c, const uint32_t* words, uint32_t n_event
     if (n_entries) {
         VGI_CUDA(c, c->measures.reserve((size_t)n_entries * 3));
         VGI_CUDA(c, c->measure_max.reserve(n_entries));
-        VGI_CUDA(c, cudaMemcpyAsync(c->measures.ptr, measures, (size_t)n_entries * 48, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, h2d(c->measures.ptr, measures, (size_t)n_entries * 48, c->stream));
         launch_measure_edits(c->state.ptr, c->slot_meta.ptr, c->face_index.ptr, c->material_light.ptr, c->measures.ptr, n_entries,
                              (uint32_t)positions, c->measure_max.ptr, c->events.ptr, c->stream);
         VGI_CUDA(c, cudaGetLastError());
@@ -1599,8 +1633,8 @@ int vgi_view_set_receivers(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, c->v_estimates.reserve(m * 4));
     VGI_CUDA(c, c->v_queue.reserve(12 + 2 * m + kSunFlipWords));
     if (n) {
-        VGI_CUDA(c, cudaMemcpyAsync(c->v_receivers.ptr, receivers.data(), (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
-        VGI_CUDA(c, cudaMemcpyAsync(c->v_estimates.ptr, estimates.data(), (size_t)n * 64, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, h2d(c->v_receivers.ptr, receivers.data(), (size_t)n * 32, c->stream));
+        VGI_CUDA(c, h2d(c->v_estimates.ptr, estimates.data(), (size_t)n * 64, c->stream));
         VGI_CUDA(c, cudaMemsetAsync(c->v_paths.ptr, 0, (size_t)n * 128, c->stream));
         VGI_CUDA(c, cudaMemsetAsync(c->v_conts.ptr, 0, (size_t)n * 128, c->stream));
     }
@@ -1786,9 +1820,9 @@ int vgi_view_set_tiles(vgi_ctx* c, const uint32_t* tiles, uint32_t n, uint32_t t
     VGI_CUDA(c, c->v_tile_of.reserve(tile_of.size()));
     VGI_CUDA(c, c->v_tile_start.reserve(start.size()));
     VGI_CUDA(c, c->v_tile_items.reserve(items.size()));
-    VGI_CUDA(c, cudaMemcpyAsync(c->v_tile_of.ptr, tile_of.data(), tile_of.size() * 4, cudaMemcpyHostToDevice, c->stream));
-    VGI_CUDA(c, cudaMemcpyAsync(c->v_tile_start.ptr, start.data(), start.size() * 4, cudaMemcpyHostToDevice, c->stream));
-    VGI_CUDA(c, cudaMemcpyAsync(c->v_tile_items.ptr, items.data(), items.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->v_tile_of.ptr, tile_of.data(), tile_of.size() * 4, c->stream));
+    VGI_CUDA(c, h2d(c->v_tile_start.ptr, start.data(), start.size() * 4, c->stream));
+    VGI_CUDA(c, h2d(c->v_tile_items.ptr, items.data(), items.size() * 4, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->v_tiles[0] = tiles_x;
     c->v_tiles[1] = tiles_y;
@@ -1865,14 +1899,14 @@ int vgi_view_present(vgi_ctx* c, const vgi_camera* cam, int corners, float* rgba
     VGI_CUDA(c, image.reserve(n));
     const float host_cam[10] = {cam->eye[0], cam->eye[1], cam->eye[2], cam->forward[0], cam->forward[1], cam->forward[2],
                                 cam->up[0], cam->up[1], cam->up[2], cam->tan_half_fov};
-    VGI_CUDA(c, cudaMemcpyAsync(dcam.ptr, host_cam, sizeof(host_cam), cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(dcam.ptr, host_cam, sizeof(host_cam), c->stream));
     ViewDisplay d = view_display(c);
     uint32_t empty = 0;
     DevBuf<uint32_t> no_hash;
     if (c->n_view == 0) {
         // No receivers: every face displays zero.
         VGI_CUDA(c, no_hash.reserve(1));
-        VGI_CUDA(c, cudaMemcpyAsync(no_hash.ptr, &empty, 4, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, h2d(no_hash.ptr, &empty, 4, c->stream));
         d.receiver_hash = no_hash.ptr;
         d.hash_mask = 0;
     }
@@ -1899,7 +1933,7 @@ int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events
     v.clock = wave->clock_ms;
     if (n_events) {
         VGI_CUDA(c, c->v_events.reserve(n_words / 4));
-        VGI_CUDA(c, cudaMemcpyAsync(c->v_events.ptr, events, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+        VGI_CUDA(c, h2d(c->v_events.ptr, events, n_words * 4, c->stream));
     }
     v.events = c->v_events.ptr;
     v.n_events = n_events;
@@ -1919,8 +1953,9 @@ int vgi_view_frame(vgi_ctx* c, const vgi_view_wave* wave, const uint32_t* events
         v.far_cells = c->far_cells[c->far_current].ptr;
         v.far_stats = c->far_stats.ptr;
     }
-    // This frame's sun-flip reports start empty.
-    VGI_CUDA(c, cudaMemsetAsync(c->v_queue.ptr + 12 + 2 * (size_t)c->n_view, 0, kSunFlipWords * 4, c->stream));
+    // Sun-flip reports build up over frames until vgi_view_read_sun_flips
+    // delivers them (the reference clears its region only after a timing
+    // receipt copied it, src/gpu/view/timing.rs:386-387).
     v.frame = c->view_frames;
     v.has_previous = c->view_frames > 0 ? 1u : 0u;
     v.n_directional = c->n_directional;
@@ -1948,7 +1983,10 @@ int vgi_view_read_sun_flips(vgi_ctx* c, uint32_t* words) {
         return VGI_OK;
     }
     VGI_CUDA(c, cudaSetDevice(c->device));
-    VGI_CUDA(c, cudaMemcpyAsync(words, c->v_queue.ptr + 12 + 2 * (size_t)c->n_view, kSunFlipWords * 4, cudaMemcpyDeviceToHost, c->stream));
+    uint32_t* region = c->v_queue.ptr + 12 + 2 * (size_t)c->n_view;
+    VGI_CUDA(c, cudaMemcpyAsync(words, region, kSunFlipWords * 4, cudaMemcpyDeviceToHost, c->stream));
+    // Delivered: the region starts over.
+    VGI_CUDA(c, cudaMemsetAsync(region, 0, kSunFlipWords * 4, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }
@@ -2012,9 +2050,9 @@ int vgi_reference_fp64(vgi_ctx* c, const uint32_t* tasks, uint32_t n, uint32_t s
     VGI_CUDA(c, d_sum.reserve((size_t)n * 3));
     VGI_CUDA(c, d_second.reserve((size_t)n * 3));
     VGI_CUDA(c, d_known.reserve(n));
-    VGI_CUDA(c, cudaMemcpyAsync(d_cdf.ptr, cdf.data(), cdf.size() * 8, cudaMemcpyHostToDevice, c->stream));
-    VGI_CUDA(c, cudaMemcpyAsync(d_recs.ptr, recs.data(), recs.size() * 16, cudaMemcpyHostToDevice, c->stream));
-    VGI_CUDA(c, cudaMemcpyAsync(d_tasks.ptr, tasks, (size_t)n * 32, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(d_cdf.ptr, cdf.data(), cdf.size() * 8, c->stream));
+    VGI_CUDA(c, h2d(d_recs.ptr, recs.data(), recs.size() * 16, c->stream));
+    VGI_CUDA(c, h2d(d_tasks.ptr, tasks, (size_t)n * 32, c->stream));
     TraceArgs a = trace_args(c, nullptr, nullptr, 0, 1, false);
     launch_reference64(a, d_cdf.ptr, d_recs.ptr, (uint32_t)ne, cdf[ne], d_tasks.ptr, n, samples, seed, d_sum.ptr, d_second.ptr, d_known.ptr,
                        c->stream);
@@ -2054,7 +2092,7 @@ int vgi_mlp_set_weights(vgi_ctx* c, const float* master, uint32_t count) {
     VGI_CUDA(c, c->mlp_partials.reserve((size_t)sms * mlp_partial_floats()));
     VGI_CUDA(c, c->mlp_adam.reserve((size_t)count * 2));
     VGI_CUDA(c, c->mlp_grads.reserve((size_t)count + 1));
-    VGI_CUDA(c, cudaMemcpyAsync(c->mlp_master.ptr, master, (size_t)count * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->mlp_master.ptr, master, (size_t)count * 4, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_adam.ptr, 0, (size_t)count * 8, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_steps.ptr, 0, 8, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_grads.ptr, 0, (size_t)(count + 1) * 4, c->stream));
@@ -2082,9 +2120,9 @@ int vgi_mlp_forward(vgi_ctx* c, const float* features, uint32_t n, float* out4) 
     DevBuf<float4> out;
     VGI_CUDA(c, in.reserve((size_t)n * 96));
     VGI_CUDA(c, out.reserve(n));
-    VGI_CUDA(c, cudaMemcpyAsync(in.ptr, features, (size_t)n * 96 * 4, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(in.ptr, features, (size_t)n * 96 * 4, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->mlp_error.ptr, 0, 4, c->stream));
-    VGI_CUDA(c, launch_mlp_forward(in.ptr, c->mlp_image.ptr, out.ptr, n, c->mlp_error.ptr, c->mlp_ctas, c->stream));
+    VGI_CUDA(c, launch_mlp_forward(in.ptr, c->mlp_image.ptr, out.ptr, n, c->mlp_error.ptr, c->mlp_ctas, c->stream, c->mlp_wait));
     uint32_t err = 0;
     VGI_CUDA(c, cudaMemcpyAsync(&err, c->mlp_error.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
     VGI_CUDA(c, cudaMemcpyAsync(out4, out.ptr, (size_t)n * 16, cudaMemcpyDeviceToHost, c->stream));
@@ -2100,7 +2138,7 @@ int vgi_mlp_forward(vgi_ctx* c, const float* features, uint32_t n, float* out4) 
 static uint32_t mlp_batch_partials(vgi_ctx* c, const float* features, const float4* targets, uint32_t n, int* rc) {
     *rc = VGI_OK;
     const cudaError_t e = launch_mlp_train(features, targets, n, c->mlp_image.ptr, c->mlp_image_b.ptr, c->mlp_partials.ptr,
-                                           c->mlp_error.ptr, c->mlp_sms, c->stream);
+                                           c->mlp_error.ptr, c->mlp_sms, c->stream, c->mlp_wait);
     if (e != cudaSuccess) *rc = fail(c, VGI_ERR_CUDA, std::string("MLP training launch: ") + cudaGetErrorString(e));
     return mlp_train_parts(n, c->mlp_sms);
 }
@@ -2108,8 +2146,8 @@ static uint32_t mlp_batch_partials(vgi_ctx* c, const float* features, const floa
 static int mlp_upload_batch(vgi_ctx* c, const float* features, const float* targets4, uint32_t n, DevBuf<float>& in, DevBuf<float4>& y) {
     VGI_CUDA(c, in.reserve((size_t)n * 96));
     VGI_CUDA(c, y.reserve(n));
-    VGI_CUDA(c, cudaMemcpyAsync(in.ptr, features, (size_t)n * 96 * 4, cudaMemcpyHostToDevice, c->stream));
-    VGI_CUDA(c, cudaMemcpyAsync(y.ptr, targets4, (size_t)n * 16, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(in.ptr, features, (size_t)n * 96 * 4, c->stream));
+    VGI_CUDA(c, h2d(y.ptr, targets4, (size_t)n * 16, c->stream));
     return VGI_OK;
 }
 
@@ -2203,7 +2241,7 @@ int vgi_mlp_encode(vgi_ctx* c, const vgi_face* faces, uint32_t n, float* feature
     DevBuf<float> out;
     VGI_CUDA(c, m.reserve(n));
     VGI_CUDA(c, out.reserve((size_t)n * 96));
-    VGI_CUDA(c, cudaMemcpyAsync(m.ptr, meta.data(), (size_t)n * 16, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(m.ptr, meta.data(), (size_t)n * 16, c->stream));
     launch_mlp_encode_faces(m.ptr, n, c->materials.ptr, mlp_encoding(c), out.ptr, c->stream);
     VGI_CUDA(c, cudaGetLastError());
     VGI_CUDA(c, cudaMemcpyAsync(features, out.ptr, (size_t)n * 96 * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -2231,6 +2269,21 @@ int vgi_set_mlp_cache(vgi_ctx* c, int enable, uint32_t warm_frames, uint32_t bat
     c->mlp_train_steps = steps_per_frame;
     c->mlp_lr = lr;
     c->mlp_frames = 0;
+    return VGI_OK;
+}
+
+int vgi_mlp_set_wait_limit(vgi_ctx* c, uint32_t polls) {
+    if (!c) return VGI_ERR_INVALID;
+    drop_graph(c);  // captured query launches carry the old limit
+    c->mlp_wait = polls == VGI_MLP_WAIT_DEFAULT ? kMlpWaitPolls : polls;
+    return VGI_OK;
+}
+
+int vgi_inject_failure(vgi_ctx* c, uint32_t what, uint32_t count) {
+    (void)c;
+    if (what == VGI_INJECT_ALLOC) t_fail_allocs = count;
+    else if (what == VGI_INJECT_UPLOAD) t_fail_uploads = count;
+    else return VGI_ERR_INVALID;
     return VGI_OK;
 }
 
@@ -2299,8 +2352,8 @@ int vgi_write_state(vgi_ctx* c, uint32_t first, uint32_t n, const uint32_t* word
         std::memcpy(&w, s + 5, 4);
         rec[i] = make_float4(r, g, b, w);
     }
-    VGI_CUDA(c, cudaMemcpyAsync(c->state.ptr + (size_t)first * 9, words36, (size_t)n * 144, cudaMemcpyHostToDevice, c->stream));
-    VGI_CUDA(c, cudaMemcpyAsync(c->cache.ptr + first, rec.data(), (size_t)n * 16, cudaMemcpyHostToDevice, c->stream));
+    VGI_CUDA(c, h2d(c->state.ptr + (size_t)first * 9, words36, (size_t)n * 144, c->stream));
+    VGI_CUDA(c, h2d(c->cache.ptr + first, rec.data(), (size_t)n * 16, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }
@@ -2429,7 +2482,7 @@ int batch_scenes(vgi_batch* b, uint32_t samples, bool scratch, std::vector<WaveS
     if (table != b->table) {
         batch_drop_graph(b);
         VGI_BCUDA(b, b->args.reserve(table.size()));
-        VGI_BCUDA(b, cudaMemcpyAsync(b->args.ptr, table.data(), table.size(), cudaMemcpyHostToDevice, b->stream));
+        VGI_BCUDA(b, h2d(b->args.ptr, table.data(), table.size(), b->stream));
         VGI_BCUDA(b, cudaStreamSynchronize(b->stream));
         b->table.swap(table);
     }

@@ -91,12 +91,23 @@ __device__ __forceinline__ bool bar_try(uint32_t bar, uint32_t phase) {
         : "memory");
     return done != 0;
 }
-// Waits for the mbarrier phase, at most `kWaitLimit` polls.
-constexpr uint32_t kWaitLimit = 1u << 22;
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t phase) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
+// Waits for the mbarrier phase, at most `limit` polls (the kernels take the
+// limit as an argument: kMlpWaitPolls unless a caller lowers it to make a
+// wait run out on purpose).
+constexpr uint32_t kWaitLimit = kMlpWaitPolls;
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t phase, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (bar_try(bar, phase)) return true;
     return false;
+}
+// A wait that ran out: the error word is set and the CTA leaves its loop, but
+// only after the copy or MMAs that were to arrive on the barrier have landed
+// (a second wait, at the full limit), so no async write into this CTA's
+// shared memory or TMEM is still in flight when it frees its TMEM and exits.
+__device__ __forceinline__ void give_up(uint32_t bar, uint32_t phase, uint32_t* abort_flag, uint32_t* error) {
+    atomicOr(abort_flag, 1u);
+    atomicOr(error, 1u);
+    bar_wait(bar, phase, kWaitLimit);
 }
 
 // One-dimensional bulk copy global -> this CTA's shared memory on the TMA
@@ -274,7 +285,7 @@ struct PathQueries {
 };
 
 template <class Rows>
-__global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, const uint8_t* image, uint32_t* error) {
+__global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, const uint8_t* image, uint32_t* error, uint32_t wait_polls) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* weights = smem;
     uint8_t* tile = smem + kImageBytes;
@@ -304,10 +315,7 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, cons
     const uint32_t tmem = *tmem_slot;
     const uint32_t lane_base = tmem + ((warp * 32u) << 16);
     // The weight image (phase 0 of the mbarrier), then one phase per layer.
-    if (!bar_wait(bar_addr, 0u)) {
-        atomicOr(abort_flag, 1u);
-        atomicOr(error, 1u);
-    }
+    if (!bar_wait(bar_addr, 0u, wait_polls)) give_up(bar_addr, 0u, abort_flag, error);
     uint32_t phase = 1;
     __syncthreads();
     const uint32_t first_tile = *abort_flag ? tiles : blockIdx.x;
@@ -330,10 +338,7 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, cons
                              idesc, kk > 0 ? 1u : 0u);
                 mma_commit(bar_addr);
             }
-            if (!bar_wait(bar_addr, phase)) {
-                atomicOr(abort_flag, 1u);
-                atomicOr(error, 1u);
-            }
+            if (!bar_wait(bar_addr, phase, wait_polls)) give_up(bar_addr, phase, abort_flag, error);
             phase ^= 1u;
             __syncthreads();
             if (*abort_flag) {
@@ -496,7 +501,7 @@ __device__ __forceinline__ void store_t(uint8_t* smem, uint32_t base, uint32_t r
 
 __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, const float4* targets, uint32_t batch,
                                                          const uint8_t* image_f, const uint8_t* image_b, float* partials,
-                                                         uint32_t* error) {
+                                                         uint32_t* error, uint32_t wait_polls) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kBarT);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kBarT + 8);
@@ -532,10 +537,7 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
     // the copies). Returns false when the wait ran out.
     uint32_t phase = 0;
     auto finish = [&]() -> bool {
-        if (!bar_wait(bar_addr, phase)) {
-            atomicOr(abort_flag, 1u);
-            atomicOr(error, 1u);
-        }
+        if (!bar_wait(bar_addr, phase, wait_polls)) give_up(bar_addr, phase, abort_flag, error);
         phase ^= 1u;
         __syncthreads();
         if (*abort_flag) return false;
@@ -755,10 +757,10 @@ uint32_t mlp_train_parts(uint32_t batch, uint32_t ctas) {
 uint32_t mlp_partial_floats() { return (uint32_t)mlp::kPartial; }
 
 cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
-                             float* partials, uint32_t* error, uint32_t ctas, cudaStream_t s) {
+                             float* partials, uint32_t* error, uint32_t ctas, cudaStream_t s, uint32_t wait_polls) {
     if (batch == 0) return cudaSuccess;
     mlp::train_kernel<<<mlp_train_parts(batch, ctas), mlp::kThreads, mlp::kTrainSmem, s>>>(features, targets, batch, image_f, image_b,
-                                                                                           partials, error);
+                                                                                           partials, error, wait_polls);
     return cudaGetLastError();
 }
 
@@ -774,10 +776,10 @@ void launch_mlp_adam(float* master, float* m, float* v, const float* partials, u
 
 
 void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,
-                        float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s) {
+                        float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s, uint32_t wait_polls) {
     if (capacity == 0) return;
     const mlp::PathQueries rows{queue, count, capacity, enc, out};
-    mlp::forward_kernel<mlp::PathQueries><<<ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error);
+    mlp::forward_kernel<mlp::PathQueries><<<ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error, wait_polls);
 }
 
 void launch_mlp_encode_training(const uint4* slot_meta, const uint4* results, const float4* materials, uint32_t n_slots,
@@ -817,11 +819,12 @@ void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s) {
 }
 
 cudaError_t launch_mlp_forward(const float* features, const uint8_t* image, float4* outputs, uint32_t n, uint32_t* error, uint32_t ctas,
-                               cudaStream_t s) {
+                               cudaStream_t s, uint32_t wait_polls) {
     if (n == 0) return cudaSuccess;
     const uint32_t tiles = (n + mlp::kRows - 1) / mlp::kRows;
     const mlp::FeatureRows rows{features, outputs, n};
-    mlp::forward_kernel<mlp::FeatureRows><<<tiles < ctas ? tiles : ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error);
+    mlp::forward_kernel<mlp::FeatureRows><<<tiles < ctas ? tiles : ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error,
+                                                                                                              wait_polls);
     return cudaGetLastError();
 }
 

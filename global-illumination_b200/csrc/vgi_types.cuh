@@ -71,6 +71,11 @@ struct MlpEncoding {
     float inv[3];
 };
 
+// The MLP cache's tensor-core kernels bound every mbarrier wait to
+// `wait_polls` polls: kMlpWaitPolls unless a caller lowers it
+// (vgi_mlp_set_wait_limit); a wait that runs out sets the error word.
+constexpr uint32_t kMlpWaitPolls = 1u << 22;
+
 struct WaveBuffers {
     float4* state;            // 9 * P path-state words
     float4* ray;              // 2 * S
@@ -89,6 +94,7 @@ struct WaveBuffers {
     float4* mlp_queue;        // 2 * P
     uint32_t* mlp_error;
     uint32_t mlp_ctas;
+    uint32_t mlp_wait = kMlpWaitPolls;
     MlpEncoding mlp_enc;
     cudaEvent_t* mlp_marks;   // optional: start/end events of the query launch
 };
@@ -230,7 +236,7 @@ void launch_present(const TraceArgs& a, const ViewDisplay& d, const float* cam, 
 // MLP radiance cache (vgi_mlp.cu).
 cudaError_t mlp_set_attributes();
 void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t capacity, const uint8_t* image, const MlpEncoding& enc,
-                        float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s);
+                        float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s, uint32_t wait_polls = kMlpWaitPolls);
 void launch_mlp_encode_training(const uint4* slot_meta, const uint4* results, const float4* materials, uint32_t n_slots,
                                 const uint32_t* step, uint32_t batch, const MlpEncoding& enc, float* features, float4* targets,
                                 cudaStream_t s);
@@ -241,7 +247,7 @@ void launch_mlp_encode_faces(const uint4* meta, uint32_t n, const float4* materi
                              cudaStream_t s);
 void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s);
 cudaError_t launch_mlp_forward(const float* features, const uint8_t* image, float4* outputs, uint32_t n, uint32_t* error, uint32_t ctas,
-                               cudaStream_t s);
+                               cudaStream_t s, uint32_t wait_polls = kMlpWaitPolls);
 void launch_mlp_pack_backward(const float* master, uint8_t* image, cudaStream_t s);
 // Training: train writes one partial row (gradient sums, loss) per CTA,
 // mlp_train_parts(batch, ctas) rows; reduce sums them into grads and the
@@ -249,7 +255,7 @@ void launch_mlp_pack_backward(const float* master, uint8_t* image, cudaStream_t 
 uint32_t mlp_train_parts(uint32_t batch, uint32_t ctas);
 uint32_t mlp_partial_floats();
 cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
-                             float* partials, uint32_t* error, uint32_t ctas, cudaStream_t s);
+                             float* partials, uint32_t* error, uint32_t ctas, cudaStream_t s, uint32_t wait_polls = kMlpWaitPolls);
 void launch_mlp_reduce(const float* partials, uint32_t parts, float* grads, float* loss, cudaStream_t s);
 void launch_mlp_adam(float* master, float* m, float* v, const float* partials, uint32_t parts, float lr, float beta1, float beta2, float eps,
                      uint32_t* steps, uint8_t* image_f, uint8_t* image_b, float* loss, cudaStream_t s);

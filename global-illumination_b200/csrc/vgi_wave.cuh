@@ -1158,7 +1158,7 @@ void wave_run(const WaveBuffers& b, const TraceArgs& a, cudaStream_t s) {
             // One diffuse hit: the queued hits take the network's value.
             if (b.mlp_marks) cudaEventRecord(b.mlp_marks[0], s);
             launch_mlp_queries(W.mlp_queue, W.mlp_count, W.n_paths, b.mlp_image, b.mlp_enc, W.state + (size_t)kX * W.n_paths, b.mlp_error,
-                               b.mlp_ctas, s);
+                               b.mlp_ctas, s, b.mlp_wait);
             if (b.mlp_marks) cudaEventRecord(b.mlp_marks[1], s);
         } else {
             wave_scatter_kernel<H, L, B, C><<<b.traverse_blocks, kWaveBlock, 0, s>>>(W);

@@ -27,6 +27,10 @@ ERR_CUDA = -2
 ERR_STATE = -3
 ERR_CAPACITY = -4
 
+INJECT_ALLOC = 1
+INJECT_UPLOAD = 2
+MLP_WAIT_DEFAULT = 0xFFFFFFFF
+
 AIR = 256
 FACE_OFFSETS = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
 
@@ -267,6 +271,8 @@ _SIGNATURES = {
     "vgi_set_far_handoff": (_INT, [_P, _INT]),
     "vgi_set_topology_prior": (_INT, [_P, _INT]),
     "vgi_view_read_sun_flips": (_INT, [_P, _P]),
+    "vgi_mlp_set_wait_limit": (_INT, [_P, _U32]),
+    "vgi_inject_failure": (_INT, [_P, _U32, _U32]),
     "vgi_view_set_tiles": (_INT, [_P, _P, _U32, _U32, _U32]),
     "vgi_view_reconstruct": (_INT, [_P, _P]),
     "vgi_view_read_published": (_INT, [_P, _P, _P]),
@@ -752,12 +758,23 @@ class GpuTracer:
         st = (settings or FarTierSettings()).struct()
         self._check(self._lib.vgi_far_frame(self._h, ctypes.byref(cam), ctypes.byref(st), frame & 0xFFFFFFFF))
 
+    def mlp_set_wait_limit(self, polls: Optional[int] = None) -> None:
+        """Polls per tensor-core wait of the MLP kernels (None: the default;
+        0: every wait gives up at once, to exercise the run-out path)."""
+        self._check(self._lib.vgi_mlp_set_wait_limit(self._h, MLP_WAIT_DEFAULT if polls is None else int(polls)))
+
+    def inject_failure(self, what: int, count: int = 1) -> None:
+        """vgi_inject_failure for this thread: INJECT_ALLOC or INJECT_UPLOAD."""
+        inject_failure(what, count)
+
     def view_read_sun_flips(self):
-        """(records (count, 4): voxel xyz, flux bits, up to 2048; overflow (7,))."""
+        """The sun-flip reports since the last read, which this read clears:
+        (records (up to 2048, 4): voxel xyz, flux bits; overflow (7,); count
+        of all flips, records and overflow together)."""
         words = np.zeros(4 + 2048 * 4 + 7, np.uint32)
         self._check(self._lib.vgi_view_read_sun_flips(self._h, _ptr(words)))
         count = int(words[0])
-        return words[4:4 + 4 * min(count, 2048)].reshape(-1, 4), words[4 + 2048 * 4:]
+        return words[4:4 + 4 * min(count, 2048)].reshape(-1, 4), words[4 + 2048 * 4:], count
 
     def set_topology_prior(self, enable: bool) -> None:
         self._check(self._lib.vgi_set_topology_prior(self._h, 1 if enable else 0))
@@ -865,6 +882,15 @@ class GpuTracer:
 
 
 # ---- synthetic workloads and host-runtime helpers ----------------------------
+
+def inject_failure(what: int, count: int = 1) -> None:
+    """Makes the calling thread's next `count` device allocations
+    (INJECT_ALLOC) or host-to-device copies (INJECT_UPLOAD) in libvgi fail
+    without reaching the device (vgi_inject_failure); 0 cancels."""
+    rc = library().vgi_inject_failure(None, what, count)
+    if rc != OK:
+        raise VgiError(rc, "vgi_inject_failure refused its arguments")
+
 
 def grid_coords(nx: int, ny: int, nz: int) -> np.ndarray:
     out = np.zeros((nx * ny * nz, 3), np.int32)

@@ -255,10 +255,14 @@ int vgi_view_set_receivers(vgi_ctx* ctx, const vgi_face* faces, uint32_t n);
  * Synchronous. */
 int vgi_view_frame(vgi_ctx* ctx, const vgi_view_wave* wave, const uint32_t* events, uint32_t n_events, uint64_t n_words);
 /* Snapshots of the view records; each pointer may be null. */
-/* The last view frame's sun-flip reports (report_sun_flips,
- * voxel_view_runtime.wgsl:229-270): faces whose refreshed corner words, or
- * whose corners on re-entering view against those their world slot kept,
- * changed a lit bit. 8,203 words: the count and 3 zeros; 2,048 records
+/* The sun-flip reports (report_sun_flips, voxel_view_runtime.wgsl:229-270)
+ * of the view frames since the last call (or since vgi_view_set_receivers):
+ * faces whose refreshed corner words, or whose corners on re-entering view
+ * against those their world slot kept, changed a lit bit. Reports build up
+ * across frames and this call clears them after copying, as the reference's
+ * timing receipt does (src/gpu/view/timing.rs:386-387), so a caller that
+ * reads less often than once a frame loses no change. 8,203 words: the
+ * count and 3 zeros; 2,048 records
  * (voxel xyz, flux as f32 bits) in an arbitrary order; then the overflow of
  * flips past 2,048: max of 2^30 - voxel xyz, max of voxel xyz + 2^30, and
  * the sum of round(flux * 64). */
@@ -334,6 +338,16 @@ typedef struct vgi_mlp_status {
 } vgi_mlp_status;
 /* Synchronous. */
 int vgi_mlp_stats(vgi_ctx* ctx, vgi_mlp_status* out);
+/* No counterpart in the reference (its wgpu waits are the driver's). Every
+ * mbarrier wait of the MLP cache's tensor-core kernels gives up after
+ * `polls` polls (VGI_MLP_WAIT_DEFAULT restores the default, about 4 M): the
+ * kernel sets the error word, lets the copy or MMAs it waited for land,
+ * frees its TMEM and returns, and the call reports VGI_ERR_CUDA (frames:
+ * vgi_mlp_stats' error). 0 makes every wait give up at once, so a caller
+ * can check that path and that the context still works afterwards. Applies
+ * to launches and frame graphs made after the call. */
+#define VGI_MLP_WAIT_DEFAULT 0xffffffffu
+int vgi_mlp_set_wait_limit(vgi_ctx* ctx, uint32_t polls);
 
 /* ---- headless discovery ---------------------------------------------------------
  * The face list from the GPU instead of a raster prepass (as NAADF's
@@ -523,6 +537,22 @@ int vgi_read_state(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words36);
 int vgi_write_state(vgi_ctx* ctx, uint32_t first, uint32_t n, const uint32_t* words36);
 int vgi_read_slot_meta(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words12);
 
+/* ---- failure injection ---------------------------------------------------------
+ * No counterpart in the reference's interface; it plays the part of the
+ * reference's injected failures (src/tests.rs:38-80). For the calling
+ * thread, the next `count` device allocations (what = VGI_INJECT_ALLOC) or
+ * host-to-device copies (what = VGI_INJECT_UPLOAD) made by this library fail
+ * without reaching the device, as out of memory or as a failed copy. The
+ * call that meets one returns VGI_ERR_CUDA with the reason in
+ * vgi_last_error; the context stays usable: an upload or vgi_set_faces that
+ * failed leaves no geometry or no faces (frames return VGI_ERR_STATE) until
+ * the next successful one. A failure met inside vgi_create gives
+ * VGI_UNAVAILABLE and no context, as a device that cannot run the path.
+ * count = 0 cancels. ctx may be null. */
+#define VGI_INJECT_ALLOC 1u
+#define VGI_INJECT_UPLOAD 2u
+int vgi_inject_failure(vgi_ctx* ctx, uint32_t what, uint32_t count);
+
 /* ---- region packing without allocation -------------------------------------
  * No counterpart in the reference. This is for callers that must not allocate
  * device memory. One example is an engine that has reserved all of its GPU
@@ -534,18 +564,24 @@ int vgi_read_slot_meta(vgi_ctx* ctx, uint32_t first, uint32_t n, uint32_t* words
  * (a cudaStream_t, 0 for the legacy default stream). The regions are n x 4096
  * u16 voxels in the caller's device memory, 16-byte aligned, values 0..256.
  * Outputs, also in the caller's device memory:
- *   headers: n x 4 u32, 16-byte aligned, (kind, material or cell offset, 0, 0)
- *            as vgi_upload_regions' packer writes them;
+ *   headers: n x 4 u32, 16-byte aligned, (kind, material or cell offset, 0, 0):
+ *            the kinds and materials vgi_upload_regions' packer writes;
  *   cells:   `cells_capacity` u32 words.
  * On success, *cells_used is the number of cell words written. Cells are laid
- * out in region order, so the layout depends only on the input.
+ * out in region order, so the layout depends only on the input. Bricks are
+ * not deduplicated: every mixed brick gets its own 32 words, where
+ * vgi_upload_regions stores identical bricks once, so the cells take more
+ * room (about twice as much on the 512x256x512 terrain: 51 MB against
+ * 25 MB). The brick words decode to the same voxels and extents.
  *
  * The call allocates nothing. Its scratch is a static device array sized for
  * VGI_STATIC_PACK_MAX_REGIONS regions (about 256 KiB per GPU, held until the
  * process exits). The first call on each device looks up that array's device
- * address; make it before any stream capture. The call synchronises `stream`.
- * Every call shares the array, so two calls whose work overlaps on the GPU
- * race; serialise them on one stream.
+ * address and keeps it for the process; make it before any stream capture.
+ * A cudaDeviceReset of that device afterwards leaves the kept address stale
+ * and is not supported. The call synchronises `stream`. Every call shares
+ * the array, so two calls whose work overlaps on the GPU race; serialise
+ * them on one stream.
  *
  * Returns VGI_ERR_CAPACITY for n above the maximum or when cells_capacity is
  * too small, and VGI_ERR_INVALID for null or misaligned pointers or voxel

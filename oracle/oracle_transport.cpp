@@ -2407,7 +2407,25 @@ static FacePrior bootstrap_face(Ctx& x, const Donors& d, const uint32_t* r) {
 }  // namespace prior
 }  // namespace orc
 
+// Every sun flip reported since the log was last cleared, as (voxel xyz, flux
+// bits): the full list behind the 2,048 records and the overflow box, so a
+// test can check the GPU's records and overflow whatever order its atomics
+// took.
+static std::vector<uint32_t>& sun_flip_log() {
+    static std::vector<uint32_t> log;
+    return log;
+}
+
 extern "C" {
+
+uint64_t orc_sun_flip_log(uint32_t* out, uint64_t capacity) {
+    const std::vector<uint32_t>& log = sun_flip_log();
+    const uint64_t n = log.size() / 4;
+    if (out) std::copy(log.begin(), log.begin() + (size_t)std::min(n, capacity) * 4, out);
+    return n;
+}
+
+void orc_sun_flip_log_clear() { sun_flip_log().clear(); }
 
 // trace_view_paths: `paths` gets 32 words per (receiver, sample).
 int orc_trace_view_paths(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
@@ -2429,6 +2447,7 @@ int orc_trace_view_paths(const int32_t* directory, uint64_t slots, const uint32_
 // load_shared_faces, trace_visible_paths, store_shared_faces.
 // `wave` = range (first, count, max hits, depth), ticket[4];
 // `view` = (view_first, shared, clock_ms, n_events, reach, measured_retention bits).
+
 int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* headers, const uint32_t* cells, const float* params,
                    const float* materials, const float* lights, const uint32_t* emitters, uint32_t* state, uint32_t* meta,
                    const uint32_t* index, const orc_pipeline* pipe, uint32_t* receivers, uint32_t n, uint32_t* paths, uint32_t* conts,
@@ -2443,8 +2462,10 @@ int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* hea
     Shared sh{state, meta, index, view_words[1] != 0u};
     const uint32_t clock = view_words[2], n_events = view_words[3], reach = view_words[4];
     const float physical = bitsf(view_words[5]);
-    const uint32_t FLIP_WORDS = 4u + 2048u * 4u + 7u;
-    for (uint32_t i = 0; i < PREFIX + 2 * n + FLIP_WORDS; ++i) queue[i] = 0u;
+    // The owner queue starts over each frame; the sun-flip region after it
+    // keeps building up until the caller reads and clears it (the
+    // reference's timing receipt, src/gpu/view/timing.rs:386-387).
+    for (uint32_t i = 0; i < PREFIX + 2 * n; ++i) queue[i] = 0u;
     // report_sun_flips (voxel_view_runtime.wgsl:231-270)
     auto report_sun_flips = [&](const uint32_t* r, f3 normal, uint32_t material, uint32_t before, uint32_t after) {
         const f3 w{0.2126f, 0.7152f, 0.0722f};
@@ -2465,6 +2486,7 @@ int orc_view_frame(const int32_t* directory, uint64_t slots, const uint32_t* hea
         if (flux <= 0.0f) return;
         const float* d = materials + (size_t)(material & 255u) * 16;
         flux = flux * dot(f3{d[0], d[1], d[2]}, w);
+        sun_flip_log().insert(sun_flip_log().end(), {r[4], r[5], r[6], fbits(flux)});
         uint32_t* flips = queue + PREFIX + 2 * n;
         const uint32_t slot = flips[0]++;
         if (slot >= 2048u) {

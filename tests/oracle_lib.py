@@ -9,6 +9,7 @@ import ctypes
 import os
 import struct
 import subprocess
+import types
 
 import numpy as np
 
@@ -76,6 +77,15 @@ _SIG = {
     "orc_view_frame": (_INT, [_P, _U64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "orc_face_index": (_I64, [_P, _U32, _P, _U64]),
     "orc_emitters": (_I64, [_P, _U32, _P, _P, _P, _U64, _P]),
+    "orc_sun_flip_log": (_U64, [_P, _U64]),
+    "orc_sun_flip_log_clear": (None, []),
+    # Seeded scene generators (input synthesis, compiled into liboracle from
+    # the package's vgi_scenes.cpp), so CPU-only callers need no libvgi.
+    "vgi_scene_grid_coords": (_U32, [_U32, _U32, _U32, _P]),
+    "vgi_scene_stone_room": (None, [_P]),
+    "vgi_scene_terrain": (None, [_P, _U32, _U32, _U32, _P]),
+    "vgi_scene_cave": (None, [_P, _U32, _U32, _U32, _P]),
+    "vgi_scene_faces": (_U64, [_P, _U32, _P, _P, _P, _U64]),
 }
 
 _lib = None
@@ -362,6 +372,85 @@ def emitters(coords, voxels, materials):
     return out, int(info[0]), float(info[2:3].view(np.float32)[0])
 
 
+class _TerrainParams(ctypes.Structure):
+    _fields_ = [("seed", _U32), ("octaves", _U32), ("period", _F), ("base_height", _F), ("falloff", _F), ("emitters", _U32)]
+
+
+class _FaceFilter(ctypes.Structure):
+    _fields_ = [("use_frustum", _U32), ("eye", _F * 3), ("forward", _F * 3), ("tan_half", _F), ("use_box", _U32),
+                ("box_min", ctypes.c_int32 * 3), ("box_max", ctypes.c_int32 * 3), ("use_facing", _U32)]
+
+
+def grid_coords(nx, ny, nz):
+    out = np.zeros((nx * ny * nz, 3), np.int32)
+    lib().vgi_scene_grid_coords(nx, ny, nz, ptr(out))
+    return out
+
+
+def stone_room():
+    vox = np.zeros(8 * 4096, np.uint16)
+    lib().vgi_scene_stone_room(ptr(vox))
+    return grid_coords(2, 2, 2), vox
+
+
+def terrain(nx, ny, nz, seed=2, octaves=4, period=64.0, base_height=96.0, falloff=48.0, emitters=256):
+    """The seeded fBm terrain (vgi_scene_terrain), made without libvgi."""
+    p = _TerrainParams(seed, octaves, period, base_height, falloff, emitters)
+    vox = np.zeros(nx * ny * nz * 4096, np.uint16)
+    lib().vgi_scene_terrain(ctypes.byref(p), nx, ny, nz, ptr(vox))
+    return grid_coords(nx, ny, nz), vox
+
+
+def exposed_faces(coords, voxels, facing=None):
+    """Exposed faces (voxel xyz, face, material), optionally only those turned
+    towards the eye `facing` (vgi_scene_faces), made without libvgi."""
+    co = c(coords, np.int32).reshape(-1, 3)
+    vx = c(voxels, np.uint16).reshape(-1)
+    flt = _FaceFilter()
+    if facing is not None:
+        flt.use_facing = 1
+        flt.eye[:] = list(map(float, facing))
+    n = lib().vgi_scene_faces(ptr(co), co.shape[0], ptr(vx), ctypes.byref(flt), None, 0)
+    out = np.zeros((max(n, 1), 5), np.int32)
+    lib().vgi_scene_faces(ptr(co), co.shape[0], ptr(vx), ctypes.byref(flt), ptr(out), n)
+    return out[:n]
+
+
+def material_words(entries):
+    """GpuMaterial words for 256 (diffuse, emission) pairs: the reference's
+    VoxelGiMaterials::bounded (src/world.rs:166-173) clamps diffuse to [0, 1]
+    and emission to [0, 1e12] (non-finite -> 0); GpuMaterial
+    (src/gpu.rs:713-723) puts diffuse in words 0-2, emission in 8-10 and the
+    largest emission channel in word 13."""
+    out = np.zeros((256, 16), np.float32)
+    for m, (diffuse, emission) in enumerate(entries):
+        d = np.asarray(diffuse, np.float32)
+        e = np.asarray(emission, np.float32)
+        d = np.where(np.isfinite(d), np.minimum(np.maximum(d, np.float32(0)), np.float32(1)), np.float32(0))
+        e = np.where(np.isfinite(e), np.minimum(np.maximum(e, np.float32(0)), np.float32(1e12)), np.float32(0))
+        out[m, 0:3] = d
+        out[m, 8:11] = e
+        out[m, 13] = max(e[0], max(e[1], e[2]))
+    return out.reshape(-1)
+
+
+def directional_light_words(direction, radiance, custom=(0.0, 0.0, 0.0)):
+    """GpuLight words of a directional source (src/gpu.rs:733-744): the
+    direction times 1 / length in float32 (glam's normalize_or_zero), range
+    -1, radiance, custom visible RGB in words 9-11."""
+    d = np.asarray(direction, np.float32)
+    length = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]), dtype=np.float32)
+    with np.errstate(divide="ignore"):
+        rcp = np.float32(1.0) / np.float32(length)
+    out = np.zeros(12, np.float32)
+    if np.isfinite(rcp) and rcp > 0:
+        out[0:3] = d * rcp
+    out[3] = -1.0
+    out[4:7] = np.asarray(radiance, np.float32)
+    out[9:12] = np.asarray(custom, np.float32)
+    return out
+
+
 def face_index(faces):
     f = c(faces, np.int32).reshape(-1, 4)
     cap = 1024
@@ -448,6 +537,20 @@ class OracleShardTracer:
         self.frames.state[first:first + n] = np.asarray(records, np.uint32).reshape(n, 36)
 
 
+def transport_settings(**overrides):
+    """The transport fields controls_words reads, with the defaults of
+    TransportSettings and TraceWork (src/settings.rs:393-428,
+    src/work.rs:11-47), for callers that do not load libvgi."""
+    t = types.SimpleNamespace(reach=768.0, bounces=3, path_steps=2048, budgeted=False, history_limit=0, recency=1.0,
+                              measured_retention=1.0, response_seconds=0.075, lanes=0, transport_revision=0, stable_error=0.12,
+                              stable_samples=32)
+    for k, v in overrides.items():
+        if not hasattr(t, k):
+            raise KeyError(k)
+        setattr(t, k, v)
+    return t
+
+
 def controls_words(n, samples, clock_ms, transport, batch_id=1, n_events=0):
     """The Controls words the product's frame uses (src/gpu/resident.rs:708-760)."""
     w = np.zeros(36, np.uint32)
@@ -520,6 +623,27 @@ class Frames:
         self.batch_id = (self.batch_id + 1) & 0x0FFFFFFF or 1
         return cnt
 
+    def frame_slots(self, samples, clock_ms, slots):
+        """frame() over the listed slots only (begin_trace, mark_changed,
+        trace with the gather over every slot's state, accumulate); the
+        other slots keep their state. Returns the counters and the results
+        of the listed slots."""
+        slots = c(slots, np.uint32)
+        n = slots.size
+        ctl = controls_words(n, samples, clock_ms, self.transport, self.batch_id)
+        L = lib()
+        tasks = np.ascontiguousarray(self.tasks[slots])
+        L.orc_begin_trace(ptr(self.state), ptr(self.meta), ptr(tasks), ptr(slots), n, ptr(ctl))
+        L.orc_mark_changed(ptr(self.state), ptr(self.meta), ptr(slots), n, ptr(ctl))
+        params = self.params_fn(n, samples)
+        out, cnt = trace_faces(self.geometry, params, self.materials, self.lights, self.emitter_words, tasks, self.pipe, self.state,
+                               self.index, self.threads)
+        L.orc_accumulate(ptr(self.state), ptr(self.meta), ptr(self.checkpoint), ptr(out), ptr(slots), n, ptr(ctl))
+        self.tasks[slots] = tasks
+        self.results[slots] = out
+        self.batch_id = (self.batch_id + 1) & 0x0FFFFFFF or 1
+        return cnt, out
+
     def frame_shard(self, samples, clock_ms, first, n):
         """frame() over slots [first, first + n) only (vgi_frame_shard)."""
         ctl = controls_words(n, samples, clock_ms, self.transport, self.batch_id)
@@ -557,6 +681,24 @@ class Frames:
                      "queue": np.zeros(12 + 2 * n + SUN_FLIP_WORDS, np.uint32)}
         self.view["estimates"][:, 13] = materials
         self.view_frames = 0
+        lib().orc_sun_flip_log_clear()
+
+    def view_read_sun_flips(self):
+        """vgi_view_read_sun_flips on the oracle: (records (up to 2048, 4),
+        overflow (7,), every flip since the last read (n, 4)), clearing the
+        region and the log as the library's read does."""
+        n = self.view["receivers"].shape[0]
+        region = self.view["queue"][12 + 2 * n:]
+        count = int(region[0])
+        records = region[4:4 + 4 * min(count, 2048)].reshape(-1, 4).copy()
+        overflow = region[4 + 2048 * 4:].copy()
+        total = int(lib().orc_sun_flip_log(None, 0))
+        log = np.zeros((total, 4), np.uint32)
+        lib().orc_sun_flip_log(ptr(log), total)
+        assert total == count, (total, count)
+        region[:] = 0
+        lib().orc_sun_flip_log_clear()
+        return records, overflow, log
 
     def view_frame(self, first=0, invocations=0, max_hits=8, depth=0, ticket=(0, 0, 0, 0), view_first=False, shared=True,
                    clock_ms=0, events=None, n_events=0, measured_retention=1.0, far=None, topology=False):

@@ -164,9 +164,10 @@ def run_frames(gpu, case, frames, samples, layout=vgi.GpuTracer.WAVEFRONT):
 
 @pytest.mark.parametrize("layout", LAYOUTS)
 def test_stone_room_frames_match_oracle(gpu, layout):
-    # Config 1 shape: 4 spp, 1 bounce via the cache, 64 DDA steps, history 64.
+    # Config 1 in full: 64 frames of 4 spp, 1 bounce via the cache, 64 DDA
+    # steps, history 64 (alpha 1/16 once 64 samples are in).
     case = stone_room_case()
-    ref = run_frames(gpu, case, 24, 4, layout)
+    ref = run_frames(gpu, case, 64, 4, layout)
     assert_words_equal(gpu.read_results(), ref.results, "frame results")
     assert_words_equal(gpu.read_state(), ref.state, "resident state")
     assert_words_equal(gpu.read_slot_meta(), ref.meta, "slot metadata")

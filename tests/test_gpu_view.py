@@ -38,16 +38,49 @@ def compare_view(gpu, ref, what):
     for key in ("receivers", "paths", "continuations", "estimates", "queue"):
         want = ref.view[key][: got[key].size] if key == "queue" else ref.view[key]
         assert_words_equal(got[key], want, f"{what}: view {key}")
-    # Sun-flip reports: the GPU queues them in arbitrary order.
-    records, overflow = gpu.view_read_sun_flips()
-    flips = ref.view["queue"][got["queue"].size:]
-    count = int(flips[0])
-    want = flips[4:4 + 4 * min(count, 2048)].reshape(-1, 4)
-    order = lambda a: a[np.lexsort(a.T[::-1])] if len(a) else a
-    assert_words_equal(order(records), order(want), f"{what}: sun flips")
-    assert_words_equal(overflow, flips[4 + 2048 * 4:], f"{what}: sun-flip overflow")
     assert_words_equal(gpu.read_state(), ref.state, f"{what}: world state")
     assert_words_equal(gpu.read_slot_meta(), ref.meta, f"{what}: world slot metadata")
+    return compare_flips(gpu, ref, what)
+
+
+def ordered(a):
+    return a[np.lexsort(a.T[::-1])] if len(a) else a
+
+
+def compare_flips(gpu, ref, what):
+    """Reads, and so clears, both sides' sun-flip reports and compares them.
+    The GPU takes its record slots by atomics, so which flips get the 2,048
+    records is arbitrary: up to 2,048 flips the records compare as a set;
+    past that, the GPU's records must be drawn from the oracle's full list
+    and the rest must make up the overflow exactly (the biased min/max box
+    and the summed round(flux * 64)). Returns the number of flips."""
+    records, overflow, count = gpu.view_read_sun_flips()
+    want_records, want_overflow, log = ref.view_read_sun_flips()
+    assert count == log.shape[0], f"{what}: {count} sun flips, the oracle has {log.shape[0]}"
+    if count <= 2048:
+        assert_words_equal(ordered(records), ordered(log), f"{what}: sun flips")
+        assert_words_equal(overflow, want_overflow, f"{what}: sun-flip overflow")
+        return count
+    # Multiset difference: the oracle's flips that are not among the GPU's records.
+    keys = lambda a: [tuple(r) for r in a]
+    pool = {}
+    for k in keys(log):
+        pool[k] = pool.get(k, 0) + 1
+    for k in keys(records):
+        assert pool.get(k, 0) > 0, f"{what}: GPU flip record {k} is not one of the oracle's flips"
+        pool[k] -= 1
+    rest = np.array([k for k, m in pool.items() for _ in range(m)], np.uint32).reshape(-1, 4)
+    assert rest.shape[0] == count - 2048
+    bias = np.int64(1 << 30)
+    v = rest[:, 0:3].view(np.int32).astype(np.int64)
+    flux = rest[:, 3].view(np.float32)
+    rounded = ((flux * np.float32(64.0)) + np.float32(0.5)).astype(np.uint32)
+    expect = np.zeros(7, np.uint32)
+    expect[0:3] = (bias - v).max(axis=0).astype(np.uint32)
+    expect[3:6] = (v + bias).max(axis=0).astype(np.uint32)
+    expect[6] = np.uint32(rounded.astype(np.uint64).sum() & 0xFFFFFFFF)
+    assert_words_equal(overflow, expect, f"{what}: sun-flip overflow")
+    return count
 
 
 def test_view_paths_match_oracle(gpu):
@@ -164,7 +197,67 @@ def test_sun_corners_are_traced_like_the_oracle(gpu):
     for k in range(4):
         gpu.view_frame(max_hits=1, clock_ms=310 + k)
         ref.view_frame(max_hits=1, clock_ms=310 + k)
-        compare_view(gpu, ref, f"sun corners after the sun turned, view frame {k}")
-        flips += len(gpu.view_read_sun_flips()[0])
+        flips += compare_view(gpu, ref, f"sun corners after the sun turned, view frame {k}")
     assert flips > 0
+    gpu.view_set_receivers(np.zeros((0, 5), np.int32))
+
+
+def test_sun_flips_build_up_until_read(gpu):
+    """Sun-flip reports are kept across view frames until
+    vgi_view_read_sun_flips delivers them (the reference clears its region
+    only after a timing receipt copied it): two frames of a turning sun
+    without a read in between deliver both frames' flips, past the 2,048
+    records into the overflow box."""
+    case = terrain_case(bounces=2)
+    ref = world(gpu, case, 1)
+    faces = case.faces.copy()
+    gpu.view_set_receivers(faces)
+    ref.view_start(gpu.view_read()["receivers"], faces[:, 4])
+    for k in range(4):  # every receiver traces its corners at least once
+        gpu.view_frame(max_hits=1, clock_ms=400 + k)
+        ref.view_frame(max_hits=1, clock_ms=400 + k)
+    compare_view(gpu, ref, "corners before the sun turns")
+    counts = []
+    for k, direction in enumerate([(-0.6, 0.5, -0.2), (0.1, 0.6, 0.8)]):
+        sun = vgi.DirectionalTransportLight(direction, (3.0, 3.0, 3.0)).words()
+        gpu.set_lights(sun, 1)
+        ref.lights = sun
+        for j in range(4):  # one frame in four refreshes each receiver
+            gpu.view_frame(max_hits=1, clock_ms=410 + 4 * k + j)
+            ref.view_frame(max_hits=1, clock_ms=410 + 4 * k + j)
+        counts.append(int(ref.view["queue"][12 + 2 * faces.shape[0]]))
+    assert counts[0] > 0 and counts[1] > counts[0], counts
+    total = compare_view(gpu, ref, "flips of eight frames read at once")
+    assert total == counts[1] > 2048, counts
+    # Read: the region starts over.
+    records, overflow, count = gpu.view_read_sun_flips()
+    assert count == 0 and len(records) == 0 and not overflow.any()
+    gpu.view_set_receivers(np.zeros((0, 5), np.int32))
+
+
+def test_sun_flips_of_faces_that_reenter_view(gpu):
+    """A receiver that leaves the view keeps its corner words in its world
+    slot; when it re-enters after the sun turned, its fresh corners are
+    compared with the kept ones and the change is reported (the re-entry
+    branch of report_sun_flips), in the first view frame after re-entry, when
+    no refresh can report yet."""
+    case = terrain_case(bounces=2)
+    ref = world(gpu, case, 1)
+    faces = case.faces.copy()
+    gpu.view_set_receivers(faces)
+    ref.view_start(gpu.view_read()["receivers"], faces[:, 4])
+    for k in range(4):
+        gpu.view_frame(max_hits=1, clock_ms=500 + k)
+        ref.view_frame(max_hits=1, clock_ms=500 + k)
+    compare_view(gpu, ref, "corners kept by the world slots")
+    gpu.view_set_receivers(np.zeros((0, 5), np.int32))
+    sun = vgi.DirectionalTransportLight((-0.6, 0.5, -0.2), (3.0, 3.0, 3.0)).words()
+    gpu.set_lights(sun, 1)
+    ref.lights = sun
+    gpu.view_set_receivers(faces)
+    ref.view_start(gpu.view_read()["receivers"], faces[:, 4])
+    gpu.view_frame(max_hits=1, clock_ms=520)
+    ref.view_frame(max_hits=1, clock_ms=520)
+    count = compare_view(gpu, ref, "first view frame after re-entry")
+    assert count > 0
     gpu.view_set_receivers(np.zeros((0, 5), np.int32))

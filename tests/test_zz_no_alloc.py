@@ -23,7 +23,7 @@ import vgi
 pytestmark = pytest.mark.gpu
 
 
-def _pack_static(coords, vox, capacity_words):
+def _pack_static(coords, vox, capacity_words, with_used=False):
     import torch
 
     lib = vgi.library()
@@ -37,7 +37,8 @@ def _pack_static(coords, vox, capacity_words):
     used = ctypes.c_uint64(0)
     stream = torch.cuda.current_stream()
     rc = fn(voxels.data_ptr(), n, headers.data_ptr(), cells.data_ptr(), capacity_words, ctypes.byref(used), stream.cuda_stream)
-    return rc, headers.cpu().numpy().view(np.uint32), cells.cpu().numpy().view(np.uint32)[: used.value]
+    out = (rc, headers.cpu().numpy().view(np.uint32), cells.cpu().numpy().view(np.uint32)[: used.value])
+    return out + (used.value,) if with_used else out
 
 
 def _reference_geometry(coords, vox):
@@ -84,3 +85,23 @@ def test_static_pack_rejects_more_regions_than_its_scratch_holds():
     fake = ctypes.c_void_p(256)  # never dereferenced: the size check comes first
     rc = fn(fake, 65537, fake, fake, 1 << 20, ctypes.byref(used), None)
     assert rc == vgi.ERR_CAPACITY and used.value == 0
+
+
+def test_static_pack_reports_a_cell_buffer_too_small_and_recovers():
+    # A cell buffer smaller than the scene needs: VGI_ERR_CAPACITY, nothing
+    # counted as used. The next call with room packs the same scene exactly,
+    # since each call clears the shared array's total and error words.
+    coords, vox = vgi.terrain(6, 4, 6, seed=21, base_height=30.0, falloff=18.0, emitters=16)
+    rc, _, _, used = _pack_static(coords, vox, capacity_words=100, with_used=True)
+    assert rc == vgi.ERR_CAPACITY and used == 0
+    assert _check_scene(coords, vox) > 100
+
+
+def test_static_pack_rejects_voxel_values_above_air():
+    # 256 is air; 257 is no voxel value: VGI_ERR_INVALID, then a good call works.
+    coords, vox = vgi.stone_room()
+    bad = vox.copy()
+    bad[4096 * 3 + 100] = 257
+    rc, _, _, used = _pack_static(coords, bad, capacity_words=coords.shape[0] * (64 + 64 * 32), with_used=True)
+    assert rc == vgi.ERR_INVALID and used == 0
+    assert _check_scene(coords, vox) > 0
