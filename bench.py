@@ -645,6 +645,34 @@ def profile_next(small=False):
     g.close()
 
 
+def profile_frame(small=False, frames=4):
+    """The plain frame for ncu captures of the wavefront kernels: the bench
+    terrain (or, small, the same generator at 256x128x256 voxels with the
+    eye at (128, 100, 128), 222k faces, about 0.8 GB on the device) and
+    `frames` frames in the default layout, so a capture can skip the
+    warm-up frames' launches (3 traversal launches a frame)."""
+    import vgi
+
+    regions = (16, 8, 16) if small else (32, 16, 32)
+    eye = (128.0, 100.0, 128.0) if small else EYE
+    coords, vox, words, lights, faces, transport = make_scene(2, regions, eye)
+    g = vgi.GpuTracer(0)
+    g.upload_regions(coords, vox)
+    g.set_materials(words)
+    g.set_lights(lights, 1)
+    g.set_environment((0.0, 0.0, 0.0))
+    g.build_emitters()
+    g.set_transport(transport)
+    g.set_faces(faces)
+    for f in range(frames):
+        g.frame(SPP, 16 * f)
+    g.sync()
+    census = g.census(SPP)
+    print(json.dumps({"profile_frame": {"faces": int(faces.shape[0]), "frames": frames, "rays": census["rays"], "steps": census["steps"],
+                                        "traverse_bytes": census["traverse_bytes"]}}), flush=True)
+    g.close()
+
+
 def profile_mlp(frames=3):
     """A small MLP cache workload for ncu captures of the network kernels:
     the same generator at 256x256x256 voxels (64 emissive voxels), faces
@@ -698,8 +726,12 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-scene comparison (0: skip it)")
     ap.add_argument("--no-next-rows", action="store_true", help="skip discovery, far tier and reconstruction timings")
     ap.add_argument("--profile-next", action="store_true", help="only the next-row workload once, for ncu captures")
-    ap.add_argument("--small", action="store_true", help="with --profile-next: the 256x128x256 terrain")
+    ap.add_argument("--profile-frame", action="store_true", help="only plain frames of the terrain, for ncu captures")
+    ap.add_argument("--small", action="store_true", help="with --profile-next or --profile-frame: the 256x128x256 terrain")
     args = ap.parse_args()
+    if args.profile_frame:
+        profile_frame(args.small)
+        return
     if args.profile_mlp:
         profile_mlp()
         return

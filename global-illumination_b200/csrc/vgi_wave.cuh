@@ -536,6 +536,8 @@ __device__ __forceinline__ void creep(const TraceArgs& A, RayRun& s, Cnt<C>& cnt
 
 constexpr uint32_t kGo = 0xffffffffu;
 
+#ifdef VGI_BRANCHED_STEP
+
 // The first half of a step: everything up to the box step. It leaves `status`
 // at kGo when the ray skips the box in s.plane, or sets the ray's outcome.
 template <bool BUDGETED, bool C>
@@ -640,6 +642,120 @@ __device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<
         }
     }
 }
+
+#else
+// The first half of a step: everything up to the box step. It leaves `status`
+// at kGo when the ray skips the box in s.plane, or sets the ray's outcome.
+//
+// Written as one straight pass for every lane rather than as nested branches
+// per level: each lookup (region grid and header, brick word, cell word) is a
+// load that the lanes needing it make together, and the decode of whatever
+// level a lane stopped at is a set of selects. A warp therefore issues the
+// lookup once per step, not once per branch some lane takes; the words read,
+// the boxes chosen and every float operation are those of the branched form
+// (trace_domain_limited, voxel_traversal.wgsl:152-213).
+template <bool BUDGETED, bool C>
+__device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<C>& cnt, uint32_t& status, uint32_t& material, I3& voxel) {
+    const TraceArgs& A = W.t;
+    const bool out_of_steps = s.step >= A.path_steps;
+    voxel = I3{f2i(floorf(s.pos.x)), f2i(floorf(s.pos.y)), f2i(floorf(s.pos.z))};
+    const int rx = voxel.x >> 4, ry = voxel.y >> 4, rz = voxel.z >> 4;
+    const bool same = s.shift != kNoIndex && (voxel.x >> s.shift) == s.kx && (voxel.y >> s.shift) == s.ky &&
+                      (voxel.z >> s.shift) == s.kz;
+    const bool beyond = s.dist > s.maxd;
+    const bool lookup = !out_of_steps && !same && !beyond && in_bounds(A, rx, ry, rz);
+    if constexpr (C) {
+        if (!out_of_steps) cnt.step();
+        if (!out_of_steps && same && !beyond) cnt.tbytes(s.shift == 4u ? 0u : (s.shift == 2u ? 4u : 8u));
+    }
+    // Region: the header of a region entered this step (the timed pass reads
+    // the dense grid, the counting pass probes the directory to count its
+    // words; both give lookup_region's answer).
+    const bool new_region = lookup && (s.lrx != rx || s.lry != ry || s.lrz != rz);
+    uint32_t index = kNoIndex;
+    if (new_region) {
+        if (!C && A.region_grid)
+            index = (uint32_t)__ldg(A.region_grid + ((size_t)(rz - A.mn[2]) * (uint32_t)(A.mx[1] - A.mn[1] + 1) + (uint32_t)(ry - A.mn[1])) *
+                                                        (uint32_t)(A.mx[0] - A.mn[0] + 1) +
+                                    (uint32_t)(rx - A.mn[0]));
+        else
+            index = lookup_region(A, rx, ry, rz, cnt);
+    }
+    const bool missing = new_region && index == kNoIndex;
+    if (new_region && !missing) {
+        cnt.tbytes(16);
+        s.meta = __ldg(A.headers + index);
+        s.lrx = rx;
+        s.lry = ry;
+        s.lrz = rz;
+    }
+    const bool present = lookup && !missing;
+    const bool air_region = present && s.meta.x == 1u;
+    const bool mixed = present && s.meta.x == 3u;
+    const bool solid_region = present && s.meta.x != 1u && s.meta.x != 3u;
+    // Brick word of a mixed region, then the cell word of a mixed brick.
+    const uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
+    const uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
+    uint32_t brick = 0u;
+    if (mixed) {
+        brick = __ldg(A.cells + s.meta.y + (bz * 4u + by) * 4u + bx);
+        cnt.tbytes(4);
+    }
+    const bool empty_brick = mixed && (brick & 3u) == 0u;
+    const bool solid_brick = mixed && (brick & 3u) == 1u;
+    const bool mixed_brick = mixed && (brick & 3u) >= 2u;
+    const uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
+    uint32_t word = 0u;
+    if (mixed_brick) {
+        word = __ldg(A.cells + (brick >> 2u) + (idx >> 1));
+        cnt.tbytes(4);
+    }
+    const uint32_t c = (word >> ((idx & 1u) * 16u)) & 65535u;
+    const bool solid_cell = mixed_brick && (c & 1u) != 0u;
+    // The outcome.
+    status = kGo;
+    if (out_of_steps) {
+        status = 2u;
+        material = 0xffffffffu;
+    } else if (same) {
+        if (beyond) status = 0u;
+    } else if (!lookup) {
+        status = 0u;
+    } else if (solid_region || solid_brick || solid_cell) {
+        status = 1u;
+        material = solid_region ? s.meta.y : (solid_brick ? brick >> 2u : c >> 1u);
+    }
+    if (!BUDGETED && missing) {
+        // visible_geometry crosses a missing region; otherwise the ray ends
+        // as unknown or escaped by geometry_ahead.
+        status = geometry_ahead(A, s.pos, s.dir, s.inv, __fsub_rn(s.maxd, s.dist), cnt) ? 2u : 0u;
+    }
+    if (lookup && status == kGo) {
+        // The box the ray skips: the region's top-level box (an air region;
+        // a missing region crossed under the budget rule, without extents and
+        // not kept, since it is looked up again every step), the brick's box
+        // (an empty brick) or the voxel's box (an air cell).
+        const bool region_box = air_region || missing;
+        const uint32_t e = empty_brick ? (brick >> 2u) : (c >> 1u);
+        I3 ng = neg_ext(e), ps = pos_ext(e);
+        if (air_region) {
+            ng = unpack_bytes(s.meta.z);
+            ps = unpack_bytes(s.meta.w);
+        }
+        if (missing) ng = ps = I3{0, 0, 0};
+        const I3 cell = region_box ? I3{rx, ry, rz} : (empty_brick ? I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz} : voxel);
+        const float size = region_box ? 16.0f : (empty_brick ? 4.0f : 1.0f);
+        const uint32_t shift = missing ? kNoIndex : (air_region ? 4u : (empty_brick ? 2u : 0u));
+        s.plane = box_planes(s.dir, cell, ng, ps, size);
+        s.shift = shift;
+        if (shift != kNoIndex) {
+            s.kx = voxel.x >> shift;
+            s.ky = voxel.y >> shift;
+            s.kz = voxel.z >> shift;
+        }
+    }
+}
+#endif
 
 // The second half: the ray ends with its outcome, or takes the box step.
 template <bool BUDGETED, bool C>
