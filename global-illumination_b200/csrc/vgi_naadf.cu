@@ -210,7 +210,23 @@ __global__ void set_header_extents_kernel(uint4* __restrict__ headers, const uin
     headers[i].w = v.y;
 }
 
+// The region header per cell of the dense region grid (kind 0 where the
+// grid holds -1, a region the directory does not find), so a ray entering a
+// region reads its header with one load instead of an index, then a header.
+__global__ void grid_headers_kernel(const int32_t* __restrict__ grid, uint32_t n, const uint4* __restrict__ headers,
+                                    uint4* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t h = grid[i];
+    out[i] = h < 0 ? make_uint4(0u, 0u, 0u, 0u) : headers[h];
+}
+
 }  // namespace
+
+void launch_grid_headers(const int32_t* grid, uint32_t n, const uint4* headers, uint4* out, cudaStream_t s) {
+    if (n == 0) return;
+    grid_headers_kernel<<<(n + 255) / 256, 256, 0, s>>>(grid, n, headers, out);
+}
 
 void launch_classify_pack(const uint16_t* voxels, const uint32_t* regions, uint32_t grid, uint32_t n, uint4* headers, uint32_t* cells,
                           unsigned long long* alloc, unsigned long long capacity, uint32_t* error, cudaStream_t s) {

@@ -31,6 +31,7 @@ struct TraceArgs {
     const float4* lights;      // 3 float4 per light (GpuLight)
     // world cache
     const int32_t* region_grid;  // lookup_region's answer per region of [mn, mx], x fastest (null: probe the directory)
+    const uint4* region_headers; // with region_grid: the header it names per region (kind 0: not found)
     const uint4* face_index;   // [0] = (mask, probes, 0, 0), entries from 1
     const float4* cache;       // per slot: mean rgb, count word (bits)
     // faces

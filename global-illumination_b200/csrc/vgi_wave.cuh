@@ -101,10 +101,14 @@ __device__ __forceinline__ void enqueue(const WaveArgs& W, bool want, uint32_t s
     if (want) W.queue_out[base + __popc(mask & ((1u << lane) - 1u))] = slot;
 }
 
-__device__ __forceinline__ void put_ray(const WaveArgs& W, uint32_t slot, V3 o, V3 d, float maxd, bool full) {
+// `hit`: 0 for a ray whose status alone is read (shadow rays), else 1 + the
+// index of its full hit record (path p's slot k in {0, 1}: 2p + k), which
+// the traversal writes when the ray ends.
+__device__ __forceinline__ void put_ray(const WaveArgs& W, uint32_t slot, V3 o, V3 d, float maxd, uint32_t hit) {
     W.ray[2u * slot] = make_float4(o.x, o.y, o.z, maxd);
-    W.ray[2u * slot + 1u] = make_float4(d.x, d.y, d.z, fl(full ? 1u : 0u));
+    W.ray[2u * slot + 1u] = make_float4(d.x, d.y, d.z, fl(hit));
 }
+__device__ __forceinline__ uint32_t hit_of(uint32_t p, uint32_t k) { return 2u * p + k + 1u; }
 
 template <uint32_t HITS, bool LIMITED, bool BUDGETED, bool C>
 struct WaveTracer {
@@ -200,7 +204,7 @@ struct WaveTracer {
                     direction = normalize3(pos);
                 }
                 emit = !skip && wmax(dot3(normal, direction), 0.0f) > 0.0f;
-                if (emit) put_ray(W, first_slot + i, origin, direction, distance, false);
+                if (emit) put_ray(W, first_slot + i, origin, direction, distance, 0u);
             }
             enqueue(W, emit, first_slot + i);
         }
@@ -361,7 +365,7 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_BEGIN_MIN_BLOCKS) wave_begin_k
         float sdist;
         s0 = T.prepare_nee(surface, normal, stream, sequence, 0u, so, sd, sdist, pending);
         if (s0) {
-            put_ray(W, base + 1u, so, sd, sdist, false);
+            put_ray(W, base + 1u, so, sd, sdist, 0u);
             flags |= kFlagS0;
             field(W, kN0, p) = make_float4(pending.x, pending.y, pending.z, 0.0f);
         } else {
@@ -378,7 +382,7 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_BEGIN_MIN_BLOCKS) wave_begin_k
             if (previous_pdf > 0.0f) {
                 c0 = true;
                 flags |= kFlagContinue;
-                put_ray(W, base, start, direction, T.reach(), true);
+                put_ray(W, base, start, direction, T.reach(), hit_of(p, 0u));
             }
             field(W, kPP, p) = make_float4(previous_position.x, previous_position.y, previous_position.z, fl(flags));
         } else {
@@ -413,16 +417,15 @@ struct RayRun {
     V3 plane;
     int kx, ky, kz;
     uint32_t shift;  // kNoIndex: no box cached
-    bool full;
+    uint32_t hit;    // 0, or 1 + the index of the ray's full hit record
 };
 
 template <bool BUDGETED>
 __device__ __forceinline__ void finish_ray(const WaveArgs& W, RayRun& s, uint32_t status, uint32_t material, I3 voxel, V3 position, V3 normal) {
     if (BUDGETED && status == 2u && material == 0xffffffffu) status = 0u;  // trace()'s budget rule
     W.status[s.slot] = status;
-    if (s.full) {
-        const uint32_t p = s.slot / W.slots, k = s.slot - p * W.slots;
-        uint4* h = W.hit + ((size_t)p * 2u + k) * 3u;
+    if (s.hit) {
+        uint4* h = W.hit + (size_t)(s.hit - 1u) * 3u;
         h[0] = make_uint4(status, material, (uint32_t)voxel.x, (uint32_t)voxel.y);
         h[1] = make_uint4((uint32_t)voxel.z, bits(position.x), bits(position.y), bits(position.z));
         h[2] = make_uint4(bits(normal.x), bits(normal.y), bits(normal.z), 0u);
@@ -437,7 +440,7 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
     const TraceArgs& A = W.t;
     const float4 ro = W.ray[2u * slot], rd = W.ray[2u * slot + 1u];
     s.slot = slot;
-    s.full = (bits(rd.w) & 1u) != 0u;
+    s.hit = bits(rd.w);
     s.dir = V3{rd.x, rd.y, rd.z};
     s.inv = direction_recip(s.dir);
     s.maxd = ro.w;
@@ -671,23 +674,31 @@ __device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<
     // Region: the header of a region entered this step (the timed pass reads
     // the dense grid, the counting pass probes the directory to count its
     // words; both give lookup_region's answer).
+    // The timed pass reads the region's header straight from the dense
+    // header grid (kind 0 where the directory finds no region), one load.
     const bool new_region = lookup && (s.lrx != rx || s.lry != ry || s.lrz != rz);
-    uint32_t index = kNoIndex;
+    bool missing = false;
     if (new_region) {
-        if (!C && A.region_grid)
-            index = (uint32_t)__ldg(A.region_grid + ((size_t)(rz - A.mn[2]) * (uint32_t)(A.mx[1] - A.mn[1] + 1) + (uint32_t)(ry - A.mn[1])) *
-                                                        (uint32_t)(A.mx[0] - A.mn[0] + 1) +
-                                    (uint32_t)(rx - A.mn[0]));
-        else
-            index = lookup_region(A, rx, ry, rz, cnt);
-    }
-    const bool missing = new_region && index == kNoIndex;
-    if (new_region && !missing) {
-        cnt.tbytes(16);
-        s.meta = __ldg(A.headers + index);
-        s.lrx = rx;
-        s.lry = ry;
-        s.lrz = rz;
+        uint4 h;
+        if (!C && A.region_headers) {
+            h = __ldg(A.region_headers + ((size_t)(rz - A.mn[2]) * (uint32_t)(A.mx[1] - A.mn[1] + 1) + (uint32_t)(ry - A.mn[1])) *
+                                             (uint32_t)(A.mx[0] - A.mn[0] + 1) +
+                          (uint32_t)(rx - A.mn[0]));
+            missing = h.x == 0u;
+        } else {
+            const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
+            missing = index == kNoIndex;
+            if (!missing) {
+                cnt.tbytes(16);
+                h = __ldg(A.headers + index);
+            }
+        }
+        if (!missing) {
+            s.meta = h;
+            s.lrx = rx;
+            s.lry = ry;
+            s.lrz = rz;
+        }
     }
     const bool present = lookup && !missing;
     const bool air_region = present && s.meta.x == 1u;
@@ -1108,20 +1119,20 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SCATTER_MIN_BLOCKS) wave_scatt
                     if (continuation_sample(pstream, sequence, bounce, 2u) < 0.5f) {
                         kind = kKindTermEmitter;
                         emit_n = T.prepare_nee(hp, hn, pstream, sequence, bounce + 1u, so, sd, sdist, pend);
-                        if (emit_n) put_ray(W, base + 1u, so, sd, sdist, false);
+                        if (emit_n) put_ray(W, base + 1u, so, sd, sdist, 0u);
                     } else {
                         kind = kKindTermCosine;
                         const V3 tdir =
                             hemisphere(hn, continuation_sample(pstream, sequence, bounce, 0u), continuation_sample(pstream, sequence, bounce, 1u));
                         if (dot3(hn, tdir) > 0.0f) {
                             emit_n = true;
-                            put_ray(W, base + 1u, hp + hn * 0.002f, tdir, T.reach(), true);
+                            put_ray(W, base + 1u, hp + hn * 0.002f, tdir, T.reach(), hit_of(p, 1u));
                         }
                     }
                 }
             } else {
                 emit_n = T.prepare_nee(hp, hn, pstream, sequence, bounce + 1u, so, sd, sdist, pend);
-                if (emit_n) put_ray(W, base + 1u, so, sd, sdist, false);
+                if (emit_n) put_ray(W, base + 1u, so, sd, sdist, 0u);
                 // The continuation (voxel_path.wgsl:472-489).
                 V3 tn = tp * diffuse;
                 const float maximum = wmax(tn.x, wmax(tn.y, tn.z));
@@ -1140,7 +1151,7 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SCATTER_MIN_BLOCKS) wave_scatt
                     if (npdf > 0.0f) {
                         emit_c = true;
                         flags |= kFlagContinue;
-                        put_ray(W, base, hp + hn * 0.002f, ndir, T.reach(), true);
+                        put_ray(W, base, hp + hn * 0.002f, ndir, T.reach(), hit_of(p, 0u));
                         field(W, kTP, p) = make_float4(tn.x, tn.y, tn.z, fl(bounce + 1u));
                     }
                 }
