@@ -20,6 +20,7 @@ void launch_classify_pack(const uint16_t* voxels, const uint32_t* regions, uint3
                           unsigned long long* alloc, unsigned long long capacity, uint32_t* error, cudaStream_t s);
 void launch_scatter_edits(const uint2* edits, uint32_t n, uint16_t* voxels, cudaStream_t s);
 void launch_set_header_extents(uint4* headers, const uint2* zw, uint32_t n, cudaStream_t s);
+void launch_grid_headers(const int32_t* grid, uint32_t n, const uint4* headers, uint4* out, cudaStream_t s);
 void launch_dedup_bricks(const uint4* headers, uint32_t n, uint32_t* cells, uint32_t* table, uint32_t mask, uint32_t* error,
                          cudaStream_t s);
 }  // namespace vgi
@@ -94,6 +95,8 @@ struct vgi_ctx {
     bool geometry = false;
     DevBuf<int4> directory;
     DevBuf<int32_t> grid;  // region_grid: header index per region of the bounding box
+    DevBuf<uint4> grid_headers;  // the header each grid cell names (kind 0: none)
+    uint64_t grid_cells = 0;
     bool has_grid = false;
     DevBuf<uint4> headers;
     DevBuf<uint32_t> cells;
@@ -339,6 +342,7 @@ TraceArgs trace_args(vgi_ctx* c, const uint4* tasks, uint4* results, uint32_t n,
     a.light_count = c->n_lights;
     a.lights = c->lights.ptr;
     a.region_grid = c->has_grid ? c->grid.ptr : nullptr;
+    a.region_headers = c->has_grid ? c->grid_headers.ptr : nullptr;
     a.face_index = with_cache ? c->face_index.ptr : nullptr;
     a.cache = with_cache ? c->cache.ptr : nullptr;
     a.tasks = tasks;
@@ -391,13 +395,26 @@ void drop_graph(vgi_ctx* c) {
 cudaError_t upload_grid(vgi_ctx* c, const int32_t* directory, uint64_t slots) {
     const std::vector<int32_t> grid = region_grid(directory, slots, c->bounds, c->bounds + 3, 1ull << 24);
     c->has_grid = !grid.empty();
+    c->grid_cells = grid.size();
     if (!c->has_grid) return cudaSuccess;
     cudaError_t e = c->grid.reserve(grid.size());
-    if (e != cudaSuccess) return e;
+    if (e == cudaSuccess) e = c->grid_headers.reserve(grid.size());
+    if (e != cudaSuccess) {
+        c->has_grid = false;
+        return e;
+    }
     e = cudaMemcpyAsync(c->grid.ptr, grid.data(), grid.size() * 4, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return e;
     // The staging vector dies here, so the copy completes first.
     return cudaStreamSynchronize(c->stream);
+}
+
+// Copies the current headers into the grid's header cells; every call that
+// changes the headers or the grid ends with it.
+cudaError_t refresh_grid_headers(vgi_ctx* c) {
+    if (!c->has_grid) return cudaSuccess;
+    launch_grid_headers(c->grid.ptr, (uint32_t)c->grid_cells, c->headers.ptr, c->grid_headers.ptr, c->stream);
+    return cudaGetLastError();
 }
 
 // Enqueues the face trace for `a` in the context's layout.
@@ -716,6 +733,7 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
     VGI_CUDA(c, c->directory.reserve(c->dir_slots));
     VGI_CUDA(c, h2d(c->directory.ptr, dir.data(), dir.size() * 4, c->stream));
     VGI_CUDA(c, upload_grid(c, dir.data(), c->dir_slots));
+    VGI_CUDA(c, refresh_grid_headers(c));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->geometry = true;
     return VGI_OK;
@@ -752,6 +770,7 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
         }
     }
     VGI_CUDA(c, cudaSetDevice(c->device));
+    c->geometry = false;  // until the arrays below are all in place
     VGI_CUDA(c, c->directory.reserve(slots));
     VGI_CUDA(c, c->headers.reserve(std::max<uint32_t>(n_headers, 1)));
     VGI_CUDA(c, c->cells.reserve(std::max<uint64_t>(n_cells, 1)));
@@ -763,6 +782,7 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
     c->cells_used = n_cells;
     for (int k = 0; k < 6; ++k) c->bounds[k] = bounds6[k];
     VGI_CUDA(c, upload_grid(c, directory, slots));
+    VGI_CUDA(c, refresh_grid_headers(c));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->keys.clear();
     c->where.clear();
@@ -833,6 +853,7 @@ int vgi_edit_voxels(vgi_ctx* c, const int32_t* edits, uint32_t n) {
     }
     rc = finish_headers(c);
     if (rc != VGI_OK) return rc;
+    VGI_CUDA(c, refresh_grid_headers(c));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
 }

@@ -313,6 +313,66 @@ std::vector<int32_t> build_directory(const std::vector<RegionKey>& keys) {
     }
 }
 
+std::vector<int32_t> build_directory(const std::vector<std::pair<RegionKey, uint32_t>>& entries) {
+    size_t capacity = 1;
+    while (capacity < entries.size() * 2) capacity <<= 1;
+    for (;;) {
+        std::vector<int32_t> dir(capacity * 4, 0);
+        for (size_t i = 0; i < capacity; ++i) dir[i * 4 + 3] = -1;
+        bool fits = true;
+        for (const auto& e : entries)
+            if (!directory_insert(dir, e.first, e.second)) {
+                fits = false;
+                break;
+            }
+        if (fits) return dir;
+        capacity *= 2;
+    }
+}
+
+bool directory_insert(std::vector<int32_t>& dir, const RegionKey& key, uint32_t header) {
+    const size_t mask = dir.size() / 4 - 1;
+    size_t slot = host_hash_voxel(key.x, key.y, key.z) & mask;
+    size_t distance = 0;
+    while (dir[slot * 4 + 3] != -1) {
+        slot = (slot + 1) & mask;
+        if (++distance >= 32) return false;
+    }
+    dir[slot * 4] = key.x;
+    dir[slot * 4 + 1] = key.y;
+    dir[slot * 4 + 2] = key.z;
+    dir[slot * 4 + 3] = (int32_t)header;
+    return true;
+}
+
+bool directory_remove(std::vector<int32_t>& dir, const RegionKey& key) {
+    const size_t mask = dir.size() / 4 - 1;
+    auto at = [&](size_t s) { return RegionKey{dir[s * 4], dir[s * 4 + 1], dir[s * 4 + 2]}; };
+    size_t slot = host_hash_voxel(key.x, key.y, key.z) & mask;
+    for (size_t probe = 0;; ++probe) {
+        if (dir[slot * 4 + 3] == -1 || probe > mask) return false;
+        if (at(slot) == key) break;
+        slot = (slot + 1) & mask;
+    }
+    dir[slot * 4 + 3] = -1;
+    dir[slot * 4] = dir[slot * 4 + 1] = dir[slot * 4 + 2] = 0;
+    size_t hole = slot, next = slot;
+    for (;;) {
+        next = (next + 1) & mask;
+        if (dir[next * 4 + 3] == -1) return true;
+        const RegionKey k = at(next);
+        const size_t home = host_hash_voxel(k.x, k.y, k.z) & mask;
+        // The entry stays when its home lies cyclically in (hole, next].
+        const bool stays = hole <= next ? (hole < home && home <= next) : (hole < home || home <= next);
+        if (!stays) {
+            std::copy(dir.begin() + next * 4, dir.begin() + next * 4 + 4, dir.begin() + hole * 4);
+            dir[next * 4 + 3] = -1;
+            dir[next * 4] = dir[next * 4 + 1] = dir[next * 4 + 2] = 0;
+            hole = next;
+        }
+    }
+}
+
 namespace {
 struct FaceHash {
     std::vector<std::array<uint32_t, 4>> slots;
@@ -431,7 +491,8 @@ uint32_t tree_split(std::vector<TreeNode>& nodes, std::vector<uint32_t>& order, 
 }
 }  // namespace
 
-EmitterWords build_emitters(const std::vector<RegionKey>& keys, const uint16_t* voxels, const float* materials) {
+EmitterWords build_emitters(const std::vector<RegionKey>& keys, const uint16_t* voxels, const float* materials,
+                            const std::vector<uint8_t>* live) {
     EmitterWords out;
     float weight[256];
     bool any = false;
@@ -439,13 +500,16 @@ EmitterWords build_emitters(const std::vector<RegionKey>& keys, const uint16_t* 
         weight[m] = materials[m * 16 + 13];
         any = any || weight[m] > 0.0f;
     }
+    auto held = [&](uint32_t r) { return !live || (*live)[r] != 0; };
     std::unordered_map<RegionKey, uint32_t, RegionKeyHash> where;
-    for (uint32_t r = 0; r < keys.size(); ++r) where[keys[r]] = r;
+    for (uint32_t r = 0; r < keys.size(); ++r)
+        if (held(r)) where[keys[r]] = r;
     std::vector<Emitter> em;
     double total = 0.0;
     if (any) {
         std::vector<uint32_t> order;
         for (uint32_t r = 0; r < keys.size(); ++r) {
+            if (!held(r)) continue;
             const uint16_t* m = voxels + (size_t)r * 4096;
             bool emits = false;
             for (int i = 0; i < 4096 && !emits; ++i) emits = m[i] != 256 && weight[m[i]] > 0.0f;

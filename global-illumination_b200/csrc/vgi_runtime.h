@@ -45,6 +45,15 @@ public:
 // hash_voxel(region), capacity nextpow2(2n) doubled until every entry sits
 // fewer than 32 probes from its home slot.
 std::vector<int32_t> build_directory(const std::vector<RegionKey>& keys);
+// The same build over (key, header) pairs, for a header array with free slots.
+std::vector<int32_t> build_directory(const std::vector<std::pair<RegionKey, uint32_t>>& entries);
+// In-place maintenance between builds (src/gpu_scene.rs:337-409): a linear-
+// probing insert that refuses a probe chain of 32 or more (the caller then
+// rebuilds), and backward-shift deletion, which leaves no tombstones and
+// never lengthens a probe chain. Both keep `dir` (4 words a slot) valid for
+// lookup_region.
+bool directory_insert(std::vector<int32_t>& dir, const RegionKey& key, uint32_t header);
+bool directory_remove(std::vector<int32_t>& dir, const RegionKey& key);
 
 // Face index (src/gpu/face_index.rs): (voxel, face) -> slot, capacity 1024
 // doubled before half load, rehashing in table order as the worker does.
@@ -58,7 +67,10 @@ struct EmitterWords {
     uint32_t faces = 0;
     float total_weight = 0.0f;
 };
-EmitterWords build_emitters(const std::vector<RegionKey>& keys, const uint16_t* voxels, const float* materials);
+// `live` (optional) marks the header slots that hold a region; the others
+// are skipped.
+EmitterWords build_emitters(const std::vector<RegionKey>& keys, const uint16_t* voxels, const float* materials,
+                            const std::vector<uint8_t>* live = nullptr);
 
 uint32_t host_pcg(uint32_t v);
 uint32_t host_hash_voxel(int32_t x, int32_t y, int32_t z);
