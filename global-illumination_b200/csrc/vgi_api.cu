@@ -21,6 +21,8 @@ void launch_classify_pack(const uint16_t* voxels, const uint32_t* regions, uint3
 void launch_scatter_edits(const uint2* edits, uint32_t n, uint16_t* voxels, cudaStream_t s);
 void launch_set_header_extents(uint4* headers, const uint2* zw, uint32_t n, cudaStream_t s);
 void launch_grid_headers(const int32_t* grid, uint32_t n, const uint4* headers, uint4* out, cudaStream_t s);
+void launch_scatter_regions(const uint16_t* staged, const uint32_t* slots, uint32_t n, uint16_t* voxels, cudaStream_t s);
+void launch_clear_headers(uint4* headers, const uint32_t* slots, uint32_t n, cudaStream_t s);
 void launch_dedup_bricks(const uint4* headers, uint32_t n, uint32_t* cells, uint32_t* table, uint32_t mask, uint32_t* error,
                          cudaStream_t s);
 }  // namespace vgi
@@ -61,6 +63,29 @@ struct DevBuf {
         if (e == cudaSuccess) count = n;
         return e;
     }
+    // Grows to at least n elements (half as much again as before, at least),
+    // keeping the first `keep` elements; stream-ordered, then synchronised.
+    cudaError_t grow(size_t n, size_t keep, cudaStream_t s) {
+        if (n <= count && ptr) return cudaSuccess;
+        const size_t cap = std::max(n, count + count / 2);
+        if (t_fail_allocs) {
+            --t_fail_allocs;
+            return cudaErrorMemoryAllocation;
+        }
+        T* fresh = nullptr;
+        cudaError_t e = cudaMalloc(&fresh, cap * sizeof(T));
+        if (e != cudaSuccess) return e;
+        if (ptr && keep) e = cudaMemcpyAsync(fresh, ptr, std::min(keep, count) * sizeof(T), cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            cudaFree(fresh);
+            return e;
+        }
+        if (ptr) cudaFree(ptr);
+        ptr = fresh;
+        count = cap;
+        return cudaSuccess;
+    }
     void release() {
         if (ptr) cudaFree(ptr);
         ptr = nullptr;
@@ -93,6 +118,16 @@ struct vgi_ctx {
     uint64_t dir_slots = 0;
     uint64_t cells_used = 0;
     bool geometry = false;
+    // Region residency (vgi_load_regions / vgi_unload_regions): keys, voxels,
+    // strides and headers are per header slot; `live` marks the slots that
+    // hold a region, freed slots are reused last freed first, and the
+    // directory is kept on the host and changed in place.
+    std::vector<uint8_t> live;
+    std::vector<uint32_t> free_slots;
+    std::vector<int32_t> host_dir;
+    bool packed_geometry = false;  // from vgi_upload_packed: no voxels to repack
+    DevBuf<uint16_t> staged_voxels;
+    DevBuf<uint32_t> slot_list;
     DevBuf<int4> directory;
     DevBuf<int32_t> grid;  // region_grid: header index per region of the bounding box
     DevBuf<uint4> grid_headers;  // the header each grid cell names (kind 0: none)
@@ -534,8 +569,9 @@ int read_counters(vgi_ctx* c, vgi_counters* out) {
 // Headers z/w from the top-level field and strides; uploads them.
 int finish_headers(vgi_ctx* c) {
     const uint32_t n = (uint32_t)c->keys.size();
-    std::vector<uint2> zw(n);
+    std::vector<uint2> zw(n, make_uint2(0u, 0u));
     for (uint32_t r = 0; r < n; ++r) {
+        if (!c->live.empty() && !c->live[r]) continue;  // a freed slot (kind 0)
         Extents e = c->top.at(c->keys[r].x, c->keys[r].y, c->keys[r].z);
         uint32_t neg = (uint32_t)e[0] | ((uint32_t)e[2] << 8) | ((uint32_t)e[4] << 16);
         uint32_t pos = (uint32_t)e[1] | ((uint32_t)e[3] << 8) | ((uint32_t)e[5] << 16);
@@ -561,6 +597,13 @@ bool region_blocked(const vgi_ctx* c, int32_t x, int32_t y, int32_t z) {
 // the headers' kind/payload words.
 int pack_regions(vgi_ctx* c, const std::vector<uint32_t>* list) {
     const uint32_t n = (uint32_t)c->keys.size();
+    // With freed slots a full repack covers the live ones only.
+    std::vector<uint32_t> live_list;
+    if (!list && !c->free_slots.empty()) {
+        for (uint32_t r = 0; r < n; ++r)
+            if (c->live[r]) live_list.push_back(r);
+        list = &live_list;
+    }
     uint32_t grid = n;
     const uint32_t* dlist = nullptr;
     if (list) {
@@ -735,6 +778,10 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
     VGI_CUDA(c, upload_grid(c, dir.data(), c->dir_slots));
     VGI_CUDA(c, refresh_grid_headers(c));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->host_dir = std::move(dir);
+    c->live.assign(n, 1);
+    c->free_slots.clear();
+    c->packed_geometry = false;
     c->geometry = true;
     return VGI_OK;
 }
@@ -788,6 +835,10 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
     c->where.clear();
     c->host_voxels.clear();
     c->host_headers.clear();
+    c->live.clear();
+    c->free_slots.clear();
+    c->host_dir.clear();
+    c->packed_geometry = true;
     c->geometry = true;
     return VGI_OK;
 }
@@ -856,6 +907,208 @@ int vgi_edit_voxels(vgi_ctx* c, const int32_t* edits, uint32_t n) {
     VGI_CUDA(c, refresh_grid_headers(c));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     return VGI_OK;
+}
+
+// Region residency changes, the GPU side of page streaming
+// (VoxelGiInput::page_loaded / page_changed / page_unloaded, src/input.rs:54-70):
+// TransportScene::with_page_contents (src/world.rs:982-1046) for the scene,
+// with region-sized pages, and PackedScene::update (src/gpu_scene.rs:72-309)
+// for the packed arrays. Removals come first, then loads (a region both
+// removed and loaded ends up loaded). Only the loaded regions are classified
+// and packed, into fresh cell space; once the arena would pass three
+// quarters, every resident region is repacked from offset 0, which reclaims
+// the space of replaced and removed regions and of bricks no region holds
+// any longer (the reference's release_bricks, here one compaction instead of
+// per-brick reference counts). Header slots of removed regions are freed and
+// reused last freed first; the directory changes in place (linear-probing
+// insert, backward-shift delete) and is rebuilt only when its capacity
+// changes or an insert would probe 32 slots. The top-level field is updated
+// incrementally over the touched regions unless every touched region keeps
+// its residency and emptiness. World-cache slots are not touched.
+static int apply_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides,
+                         const int32_t* removed, uint32_t n_removed) {
+    if (c) drop_graph(c);  // what a frame launches may change
+    if (!c || (n && (!coords || !voxels)) || (n_removed && !removed)) return VGI_ERR_INVALID;
+    if (c->geometry && c->packed_geometry) return fail(c, VGI_ERR_STATE, "host-packed geometry has no regions to load into");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    {
+        // Refused inputs leave the context as it was.
+        std::unordered_map<RegionKey, uint32_t, RegionKeyHash> seen;
+        for (uint32_t i = 0; i < n; ++i)
+            if (!seen.emplace(RegionKey{coords[i * 3], coords[i * 3 + 1], coords[i * 3 + 2]}, i).second)
+                return fail(c, VGI_ERR_INVALID, "duplicate region coordinate");
+        for (size_t i = 0; i < (size_t)n * 4096; ++i)
+            if (voxels[i] > 256) return fail(c, VGI_ERR_INVALID, "voxel value above 256 (materials are 0..255, 256 is air)");
+    }
+    if (!c->geometry) {
+        // No geometry yet: the loads start from an empty scene.
+        c->keys.clear();
+        c->where.clear();
+        c->host_voxels.clear();
+        c->strides.clear();
+        c->host_headers.clear();
+        c->live.clear();
+        c->free_slots.clear();
+        c->host_dir.clear();
+        c->top = TopLevelField{};
+        c->cells_used = 0;
+        c->packed_geometry = false;
+    }
+    // From here a failure leaves no geometry (frames refused) until an
+    // upload or a load succeeds.
+    c->geometry = false;
+    // Residency and emptiness of every touched region before the change:
+    // -1 not loaded, 0 loaded air, 1 loaded with a solid voxel.
+    auto status_of = [c](const RegionKey& k) -> int {
+        auto it = c->where.find(k);
+        if (it == c->where.end()) return -1;
+        return c->host_headers[it->second].x != 1u ? 1 : 0;
+    };
+    std::unordered_map<RegionKey, int, RegionKeyHash> before;
+    std::vector<RegionKey> touched;
+    std::vector<uint32_t> freed;
+    for (uint32_t i = 0; i < n_removed; ++i) {
+        const RegionKey k{removed[i * 3], removed[i * 3 + 1], removed[i * 3 + 2]};
+        auto it = c->where.find(k);
+        if (it == c->where.end()) continue;
+        if (!before.count(k)) before[k] = status_of(k);
+        const uint32_t slot = it->second;
+        c->where.erase(it);
+        c->live[slot] = 0;
+        c->free_slots.push_back(slot);
+        c->host_headers[slot] = make_uint4(0u, 0u, 0u, 0u);
+        if (!c->host_dir.empty()) directory_remove(c->host_dir, k);
+        freed.push_back(slot);
+        touched.push_back(k);
+    }
+    const uint32_t old_slots = (uint32_t)c->keys.size();
+    std::vector<uint32_t> slots(n);
+    std::vector<RegionKey> inserted;
+    for (uint32_t i = 0; i < n; ++i) {
+        const RegionKey k{coords[i * 3], coords[i * 3 + 1], coords[i * 3 + 2]};
+        if (!before.count(k)) before[k] = status_of(k);
+        auto it = c->where.find(k);
+        uint32_t slot;
+        if (it != c->where.end()) {
+            slot = it->second;
+        } else {
+            if (!c->free_slots.empty()) {
+                slot = c->free_slots.back();
+                c->free_slots.pop_back();
+            } else {
+                slot = (uint32_t)c->keys.size();
+                c->keys.push_back(k);
+                c->live.push_back(0);
+                c->strides.push_back(0);
+                c->host_headers.push_back(make_uint4(0u, 0u, 0u, 0u));
+                c->host_voxels.resize(c->host_voxels.size() + 4096);
+            }
+            c->keys[slot] = k;
+            c->live[slot] = 1;
+            c->where[k] = slot;
+            inserted.push_back(k);
+        }
+        std::copy(voxels + (size_t)i * 4096, voxels + (size_t)(i + 1) * 4096, c->host_voxels.begin() + (size_t)slot * 4096);
+        c->strides[slot] = strides ? strides[i] : 0;
+        slots[i] = slot;
+        touched.push_back(k);
+    }
+    // A freed slot that a load took again is live.
+    freed.erase(std::remove_if(freed.begin(), freed.end(), [c](uint32_t s) { return c->live[s] != 0; }), freed.end());
+    const uint32_t total = (uint32_t)c->keys.size();
+    uint32_t n_live = 0;
+    for (uint8_t l : c->live) n_live += l;
+    // Device storage: voxels and headers per slot, the cell arena sized for
+    // every live region mixed (brick pointers are 30-bit word offsets).
+    VGI_CUDA(c, c->voxels.grow((size_t)std::max<uint32_t>(total, 1) * 4096, (size_t)old_slots * 4096, c->stream));
+    VGI_CUDA(c, c->headers.grow(std::max<uint32_t>(total, 1), old_slots, c->stream));
+    const unsigned long long capacity = std::min<unsigned long long>((unsigned long long)n_live * (64 + 64 * 32) + 64, 1ull << 30);
+    VGI_CUDA(c, c->cells.grow(capacity, c->cells_used, c->stream));
+    if (n) {
+        VGI_CUDA(c, c->staged_voxels.reserve((size_t)n * 4096));
+        VGI_CUDA(c, h2d(c->staged_voxels.ptr, voxels, (size_t)n * 8192, c->stream));
+    }
+    std::vector<uint32_t> lists(slots);
+    lists.insert(lists.end(), freed.begin(), freed.end());
+    VGI_CUDA(c, c->slot_list.reserve(std::max<size_t>(lists.size(), 1)));
+    if (!lists.empty()) VGI_CUDA(c, h2d(c->slot_list.ptr, lists.data(), lists.size() * 4, c->stream));
+    launch_scatter_regions(c->staged_voxels.ptr, c->slot_list.ptr, n, c->voxels.ptr, c->stream);
+    launch_clear_headers(c->headers.ptr, c->slot_list.ptr + n, (uint32_t)freed.size(), c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    // Pack the loaded regions, or every live one when the arena is short.
+    const bool compact = c->cells_used + (unsigned long long)n * (64 + 64 * 32) > c->cells.count * 3 / 4;
+    if (compact) c->cells_used = 0;
+    std::vector<uint32_t> pack = slots;
+    std::sort(pack.begin(), pack.end());
+    int rc = pack_regions(c, compact ? nullptr : &pack);
+    if (rc != VGI_OK) return rc;
+    // Directory: in place, or rebuilt at a new capacity.
+    size_t capacity_slots = 1;
+    while (capacity_slots < (size_t)n_live * 2) capacity_slots <<= 1;
+    bool rebuild = c->host_dir.empty() || capacity_slots * 4 > c->host_dir.size() || capacity_slots * 8 * 4 < c->host_dir.size();
+    if (!rebuild)
+        for (const RegionKey& k : inserted)
+            if (!directory_insert(c->host_dir, k, c->where[k])) {
+                rebuild = true;
+                break;
+            }
+    if (rebuild) {
+        std::vector<std::pair<RegionKey, uint32_t>> entries;
+        entries.reserve(n_live);
+        for (uint32_t r = 0; r < total; ++r)
+            if (c->live[r]) entries.emplace_back(c->keys[r], r);
+        c->host_dir = build_directory(entries);
+    }
+    c->dir_slots = c->host_dir.size() / 4;
+    VGI_CUDA(c, c->directory.reserve(c->dir_slots));
+    VGI_CUDA(c, h2d(c->directory.ptr, c->host_dir.data(), c->host_dir.size() * 4, c->stream));
+    // Bounds and the top-level field.
+    int32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool first = true;
+    for (uint32_t r = 0; r < total; ++r) {
+        if (!c->live[r]) continue;
+        const RegionKey& k = c->keys[r];
+        const int32_t v[3] = {k.x, k.y, k.z};
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = first ? v[a] : std::min(lo[a], v[a]);
+            hi[a] = first ? v[a] : std::max(hi[a], v[a]);
+        }
+        first = false;
+    }
+    for (int a = 0; a < 3; ++a) {
+        c->bounds[a] = lo[a];
+        c->bounds[3 + a] = hi[a];
+    }
+    bool topology_unchanged = true;
+    for (const auto& kv : before) {
+        const int now = status_of(kv.first);
+        if (kv.second < 0 || now < 0 || kv.second != now) topology_unchanged = false;
+    }
+    if (!topology_unchanged) {
+        std::sort(touched.begin(), touched.end(), [](const RegionKey& a, const RegionKey& b) {
+            if (a.z != b.z) return a.z < b.z;
+            if (a.y != b.y) return a.y < b.y;
+            return a.x < b.x;
+        });
+        touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+        c->top = c->top.updated(lo, hi, n_live > 0, [c](int32_t x, int32_t y, int32_t z) { return region_blocked(c, x, y, z); },
+                                touched);
+    }
+    rc = finish_headers(c);
+    if (rc != VGI_OK) return rc;
+    VGI_CUDA(c, upload_grid(c, c->host_dir.data(), c->dir_slots));
+    VGI_CUDA(c, refresh_grid_headers(c));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->geometry = true;
+    return VGI_OK;
+}
+
+int vgi_load_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides) {
+    return apply_regions(c, coords, n, voxels, strides, nullptr, 0);
+}
+
+int vgi_unload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n) {
+    return apply_regions(c, nullptr, 0, nullptr, nullptr, coords, n);
 }
 
 int vgi_geometry_info(vgi_ctx* c, uint64_t* sizes3, int32_t* bounds6) {
@@ -975,7 +1228,7 @@ int vgi_set_emitters(vgi_ctx* c, const uint32_t* words, uint64_t n_words, uint32
 int vgi_build_emitters(vgi_ctx* c) {
     if (!c) return VGI_ERR_INVALID;
     if (c->keys.empty() && c->geometry) return fail(c, VGI_ERR_STATE, "emitters need geometry uploaded as regions");
-    EmitterWords e = build_emitters(c->keys, c->host_voxels.data(), c->host_materials.data());
+    EmitterWords e = build_emitters(c->keys, c->host_voxels.data(), c->host_materials.data(), c->live.empty() ? nullptr : &c->live);
     return vgi_set_emitters(c, e.words.data(), e.words.size(), e.faces, e.total_weight);
 }
 

@@ -221,7 +221,35 @@ __global__ void grid_headers_kernel(const int32_t* __restrict__ grid, uint32_t n
     out[i] = h < 0 ? make_uint4(0u, 0u, 0u, 0u) : headers[h];
 }
 
+// Loaded regions into their header slots: region i of the staged upload
+// (4096 voxels, 512 x 16 bytes) to slot slots[i] of the voxel store.
+__global__ void scatter_regions_kernel(const uint4* __restrict__ staged, const uint32_t* __restrict__ slots, uint32_t n,
+                                       uint4* __restrict__ voxels) {
+    const uint32_t i = blockIdx.x;
+    if (i >= n) return;
+    const uint4* src = staged + (size_t)i * 512;
+    uint4* dst = voxels + (size_t)slots[i] * 512;
+    for (uint32_t k = threadIdx.x; k < 512; k += blockDim.x) dst[k] = src[k];
+}
+
+// Unloaded regions' header slots become kind 0 (no region): the packer's
+// deduplication and the header grid skip them until a load reuses the slot.
+__global__ void clear_headers_kernel(uint4* __restrict__ headers, const uint32_t* __restrict__ slots, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) headers[slots[i]] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 }  // namespace
+
+void launch_scatter_regions(const uint16_t* staged, const uint32_t* slots, uint32_t n, uint16_t* voxels, cudaStream_t s) {
+    if (n == 0) return;
+    scatter_regions_kernel<<<n, 128, 0, s>>>(reinterpret_cast<const uint4*>(staged), slots, n, reinterpret_cast<uint4*>(voxels));
+}
+
+void launch_clear_headers(uint4* headers, const uint32_t* slots, uint32_t n, cudaStream_t s) {
+    if (n == 0) return;
+    clear_headers_kernel<<<(n + 255) / 256, 256, 0, s>>>(headers, slots, n);
+}
 
 void launch_grid_headers(const int32_t* grid, uint32_t n, const uint4* headers, uint4* out, cudaStream_t s) {
     if (n == 0) return;

@@ -225,6 +225,8 @@ _SIGNATURES = {
     "vgi_upload_regions": (_INT, [_P, _P, _U32, _P, _P]),
     "vgi_upload_packed": (_INT, [_P, _P, _U64, _P, _U32, _P, _U64, _P]),
     "vgi_edit_voxels": (_INT, [_P, _P, _U32]),
+    "vgi_load_regions": (_INT, [_P, _P, _U32, _P, _P]),
+    "vgi_unload_regions": (_INT, [_P, _P, _U32]),
     "vgi_geometry_info": (_INT, [_P, _P, _P]),
     "vgi_read_geometry": (_INT, [_P, _P, _P, _P]),
     "vgi_set_materials": (_INT, [_P, _P]),
@@ -497,6 +499,20 @@ class GpuTracer:
         c = _c(cells, np.uint32).reshape(-1)
         b = _c(bounds, np.int32).reshape(-1)
         self._check(self._lib.vgi_upload_packed(self._h, _ptr(d), d.size // 4, _ptr(h), h.size // 4, _ptr(c), c.size, _ptr(b)))
+
+    def load_regions(self, coords: np.ndarray, voxels: np.ndarray, strides: Optional[np.ndarray] = None) -> None:
+        """page_loaded / page_changed: regions (coords n x 3, voxels n x 4096)
+        loaded into the GPU geometry, replacing resident ones."""
+        c = _c(coords, np.int32).reshape(-1, 3)
+        v = _c(voxels, np.uint16).reshape(-1)
+        assert v.size == c.shape[0] * 4096
+        st = None if strides is None else _c(strides, np.uint8)
+        self._check(self._lib.vgi_load_regions(self._h, _ptr(c), c.shape[0], _ptr(v), _ptr(st)))
+
+    def unload_regions(self, coords: np.ndarray) -> None:
+        """page_unloaded: regions removed from the GPU geometry."""
+        c = _c(coords, np.int32).reshape(-1, 3)
+        self._check(self._lib.vgi_unload_regions(self._h, _ptr(c), c.shape[0]))
 
     def edit_voxels(self, edits: np.ndarray) -> None:
         e = _c(edits, np.int32).reshape(-1, 4)

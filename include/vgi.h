@@ -108,6 +108,23 @@ int vgi_upload_regions(vgi_ctx* ctx, const int32_t* coords, uint32_t n, const ui
  * slot, headers 4 words per region, cells) and region bounds min xyz, max xyz. */
 int vgi_upload_packed(vgi_ctx* ctx, const int32_t* directory, uint64_t slots, const uint32_t* headers, uint32_t n_headers,
                       const uint32_t* cells, uint64_t n_cells, const int32_t* bounds6);
+/* Page streaming on the GPU geometry: VoxelGiInput::page_loaded and
+ * page_changed (vgi_load_regions) and page_unloaded (vgi_unload_regions),
+ * src/input.rs:54-70, applied as TransportScene::with_page_contents
+ * (src/world.rs:982-1046) with region-sized pages and PackedScene::update
+ * (src/gpu_scene.rs:72-409). Regions keep the vgi_upload_regions layout; a
+ * loaded coordinate already resident is replaced, an unloaded one that is
+ * not resident is ignored. Only the loaded regions are packed on the GPU;
+ * the directory changes in place (linear-probing insert, backward-shift
+ * delete; rebuilt when its capacity changes or a probe chain would reach
+ * 32); the top-level field is updated incrementally over the touched
+ * regions. Every world-cache slot stays as it is. A load on a context
+ * without geometry starts from an empty scene. Refused inputs (duplicate
+ * coordinates, voxels above 256) change nothing; another failure leaves no
+ * geometry until the next successful upload or load. Not for geometry from
+ * vgi_upload_packed (VGI_ERR_STATE). Synchronous. */
+int vgi_load_regions(vgi_ctx* ctx, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides);
+int vgi_unload_regions(vgi_ctx* ctx, const int32_t* coords, uint32_t n);
 /* VoxelGiInput::edit_voxel batch (src/input.rs:90-93): 4 ints per edit
  * (x, y, z, value). Voxels outside uploaded regions are ignored. The edited
  * regions are repacked on the GPU and the top-level field is updated

@@ -529,6 +529,85 @@ int orc_scene_edit(orc_scene* sc, const int32_t* edits, uint32_t n) {
     return 0;
 }
 
+// Loads (or replaces) and unloads regions: TransportScene::with_page_contents
+// (world.rs:982-1046) with region-sized pages. Removals come first, then
+// loads. The touched regions (removed, loaded or replaced) update the
+// top-level field incrementally over the new region map (TopLevelAadf::
+// updated, world.rs:473-583) unless every touched region keeps its residency
+// and emptiness; then the scene is packed again from scratch (the canonical
+// form of PackedScene's incremental update equals a full pack, the property
+// gpu_scene.rs's lineage test pins). Unloading a region that is not loaded
+// does nothing.
+int orc_scene_regions(orc_scene* sc, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides,
+                      const int32_t* removed, uint32_t n_removed) {
+    Scene& s = sc->s;
+    struct Region {
+        std::array<int32_t, 3> c;
+        std::vector<uint16_t> v;
+        uint8_t stride;
+    };
+    std::map<std::array<int32_t, 3>, Region> regions;  // keyed (z, y, x)
+    for (size_t h = 0; h < s.coords.size(); ++h) {
+        const auto& c = s.coords[h];
+        regions[zyx(c[0], c[1], c[2])] =
+            Region{c, std::vector<uint16_t>(s.voxels.begin() + h * 4096, s.voxels.begin() + (h + 1) * 4096), s.strides[h]};
+    }
+    auto status = [&](const std::array<int32_t, 3>& key) -> int {
+        auto it = regions.find(key);
+        if (it == regions.end()) return -1;
+        for (uint16_t m : it->second.v)
+            if (m != AIR) return 1;
+        return 0;
+    };
+    std::map<std::array<int32_t, 3>, int> before;
+    std::vector<std::array<int32_t, 3>> touched;
+    for (uint32_t i = 0; i < n_removed; ++i) {
+        const std::array<int32_t, 3> c{removed[i * 3], removed[i * 3 + 1], removed[i * 3 + 2]};
+        const auto key = zyx(c[0], c[1], c[2]);
+        if (!regions.count(key)) continue;
+        if (!before.count(key)) before[key] = status(key);
+        regions.erase(key);
+        touched.push_back(c);
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const std::array<int32_t, 3> c{coords[i * 3], coords[i * 3 + 1], coords[i * 3 + 2]};
+        const auto key = zyx(c[0], c[1], c[2]);
+        if (!before.count(key)) before[key] = status(key);
+        regions[key] = Region{c, std::vector<uint16_t>(voxels + (size_t)i * 4096, voxels + (size_t)(i + 1) * 4096),
+                              strides ? strides[i] : (uint8_t)0};
+        touched.push_back(c);
+    }
+    bool topology_unchanged = true;
+    for (const auto& kv : before) {
+        const int now = status(kv.first);
+        if (kv.second < 0 || now < 0 || kv.second != now) topology_unchanged = false;
+    }
+    s.coords.clear();
+    s.voxels.clear();
+    s.strides.clear();
+    s.index.clear();
+    for (const auto& kv : regions) {
+        s.index[kv.first] = (uint32_t)s.coords.size();
+        s.coords.push_back(kv.second.c);
+        s.voxels.insert(s.voxels.end(), kv.second.v.begin(), kv.second.v.end());
+        s.strides.push_back(kv.second.stride);
+    }
+    if (!topology_unchanged) {
+        std::sort(touched.begin(), touched.end(), [](const std::array<int32_t, 3>& a, const std::array<int32_t, 3>& b) {
+            return zyx(a[0], a[1], a[2]) < zyx(b[0], b[1], b[2]);
+        });
+        touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+        if (s.top_mode == 0) {
+            TopLevel previous = s.top;
+            build_top(s, previous, touched);
+        } else {
+            build_top(s, TopLevel{}, {});
+        }
+    }
+    pack_scene(s);
+    return 0;
+}
+
 // sizes: [directory slots, headers, cells]; bounds: min xyz, max xyz.
 int orc_scene_info(const orc_scene* sc, uint64_t* sizes, int32_t* bounds) {
     const Scene& s = sc->s;

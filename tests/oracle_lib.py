@@ -44,6 +44,7 @@ _SIG = {
     "orc_scene_create": (_INT, [_P, _U32, _P, _P, _INT, _P]),
     "orc_scene_free": (None, [_P]),
     "orc_scene_edit": (_INT, [_P, _P, _U32]),
+    "orc_scene_regions": (_INT, [_P, _P, _U32, _P, _P, _P, _U32]),
     "orc_scene_info": (_INT, [_P, _P, _P]),
     "orc_scene_copy": (_INT, [_P, _P, _P, _P]),
     "orc_scene_top_level": (_INT, [_P, _P]),
@@ -156,6 +157,16 @@ class Scene:
     def edit(self, edits) -> None:
         e = c(edits, np.int32).reshape(-1, 4)
         assert lib().orc_scene_edit(self._h, ptr(e), e.shape[0]) == 0
+
+    def regions(self, coords=None, voxels=None, removed=None, strides=None) -> None:
+        """Loads (or replaces) regions and unloads others (orc_scene_regions)."""
+        co = c(np.zeros((0, 3)) if coords is None else coords, np.int32).reshape(-1, 3)
+        vx = c(np.zeros(0) if voxels is None else voxels, np.uint16).reshape(-1)
+        assert vx.size == co.shape[0] * 4096
+        rm = c(np.zeros((0, 3)) if removed is None else removed, np.int32).reshape(-1, 3)
+        st = None if strides is None else c(strides, np.uint8)
+        assert lib().orc_scene_regions(self._h, ptr(co) if co.size else None, co.shape[0], ptr(vx) if vx.size else None, ptr(st),
+                                       ptr(rm) if rm.size else None, rm.shape[0]) == 0
 
     def arrays(self):
         sizes = np.zeros(3, np.uint64)

@@ -219,10 +219,17 @@ def test_top_level_field_is_a_valid_fixed_point():
                 coords.append((x, y, z))
                 vox.append(v)
     scene = O.Scene(np.array(coords), np.concatenate(vox), top_mode=0)
+    assert_valid_fixed_point(scene, {tuple(c): v for c, v in zip(coords, vox)})
+
+
+def assert_valid_fixed_point(scene, present):
+    """world.rs:596-684 assert_valid_fixed_point on the oracle scene's
+    top-level field: every box holds only loaded empty regions inside the
+    bounds, and no box can grow by the merging rule. `present` maps region
+    coordinates to their voxels."""
     field = scene.top_level()
     bounds = scene.arrays()[3]
     size = bounds[3:] - bounds[:3] + 1
-    present = {tuple(c): v for c, v in zip(coords, vox)}
     blocked = np.ones(tuple(size[::-1]), bool)
     for (x, y, z), v in present.items():
         blocked[z - bounds[2], y - bounds[1], x - bounds[0]] = (v != 256).any()
