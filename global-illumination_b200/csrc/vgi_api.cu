@@ -10,6 +10,7 @@
 #include <cstring>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "vgi_runtime.h"
@@ -125,6 +126,7 @@ struct vgi_ctx {
     std::vector<uint8_t> live;
     std::vector<uint32_t> free_slots;
     std::vector<int32_t> host_dir;
+    std::vector<uint32_t> host_cells;  // packed geometry only: the cells vgi_patch_packed patches
     bool packed_geometry = false;  // from vgi_upload_packed: no voxels to repack
     DevBuf<uint16_t> staged_voxels;
     DevBuf<uint32_t> slot_list;
@@ -746,6 +748,11 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
     c->strides.assign(n, 0);
     if (strides) std::copy(strides, strides + n, c->strides.begin());
     c->host_headers.assign(n, make_uint4(0, 0, 0, 0));
+    // Every region is live: the packer and the header pass read these.
+    c->live.assign(n, 1);
+    c->free_slots.clear();
+    c->host_cells.clear();
+    c->packed_geometry = false;
     // Worst case: every region mixed with 64 mixed bricks (64 + 64 * 32 words);
     // brick pointers are 30-bit word offsets.
     unsigned long long capacity = std::min<unsigned long long>((unsigned long long)n * (64 + 64 * 32) + 64, 1ull << 30);
@@ -779,19 +786,15 @@ int vgi_upload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint
     VGI_CUDA(c, refresh_grid_headers(c));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->host_dir = std::move(dir);
-    c->live.assign(n, 1);
-    c->free_slots.clear();
-    c->packed_geometry = false;
     c->geometry = true;
     return VGI_OK;
 }
 
-int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, const uint32_t* headers, uint32_t n_headers,
-                      const uint32_t* cells, uint64_t n_cells, const int32_t* bounds6) {
-    if (c) drop_graph(c);  // what a frame launches may change
-    if (!c || !directory || !headers || !bounds6 || slots == 0 || (slots & (slots - 1))) return VGI_ERR_INVALID;
-    if (n_cells && !cells) return VGI_ERR_INVALID;
-    // Every index the traversal follows must stay inside the arrays.
+namespace {
+// Checks host-packed arrays before they reach the device: every index the
+// traversal follows must stay inside the arrays, and every material below 256.
+int validate_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, const uint32_t* headers, uint32_t n_headers,
+                    const uint32_t* cells, uint64_t n_cells) {
     for (uint64_t s = 0; s < slots; ++s) {
         int32_t w = directory[s * 4 + 3];
         if (w < -1 || (w >= 0 && (uint32_t)w >= n_headers)) return fail(c, VGI_ERR_INVALID, "directory entry names no header");
@@ -816,6 +819,17 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
                 }
         }
     }
+    return VGI_OK;
+}
+}  // namespace
+
+int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, const uint32_t* headers, uint32_t n_headers,
+                      const uint32_t* cells, uint64_t n_cells, const int32_t* bounds6) {
+    if (c) drop_graph(c);  // what a frame launches may change
+    if (!c || !directory || !headers || !bounds6 || slots == 0 || (slots & (slots - 1))) return VGI_ERR_INVALID;
+    if (n_cells && !cells) return VGI_ERR_INVALID;
+    int rc = validate_packed(c, directory, slots, headers, n_headers, cells, n_cells);
+    if (rc != VGI_OK) return rc;
     VGI_CUDA(c, cudaSetDevice(c->device));
     c->geometry = false;  // until the arrays below are all in place
     VGI_CUDA(c, c->directory.reserve(slots));
@@ -834,11 +848,99 @@ int vgi_upload_packed(vgi_ctx* c, const int32_t* directory, uint64_t slots, cons
     c->keys.clear();
     c->where.clear();
     c->host_voxels.clear();
-    c->host_headers.clear();
     c->live.clear();
     c->free_slots.clear();
-    c->host_dir.clear();
+    // The host copies of the packed arrays, which vgi_patch_packed patches
+    // and checks before any delta reaches the device.
+    c->host_dir.assign(directory, directory + slots * 4);
+    c->host_headers.resize(n_headers);
+    std::memcpy(c->host_headers.data(), headers, (size_t)n_headers * 16);
+    c->host_cells.assign(cells, cells + n_cells);
     c->packed_geometry = true;
+    c->geometry = true;
+    return VGI_OK;
+}
+
+int vgi_patch_packed(vgi_ctx* c, uint64_t slots, uint32_t n_headers, uint64_t n_cells, const int32_t* bounds6, int directory_rebuilt,
+                     const uint64_t* dir_ranges, uint32_t n_dir_ranges, const int32_t* dir_data, const uint64_t* header_ranges,
+                     uint32_t n_header_ranges, const uint32_t* header_data, const uint64_t* cell_ranges, uint32_t n_cell_ranges,
+                     const uint32_t* cell_data) {
+    if (c) drop_graph(c);  // what a frame launches may change
+    if (!c || !bounds6 || slots == 0 || (slots & (slots - 1))) return VGI_ERR_INVALID;
+    if ((n_dir_ranges && !dir_ranges) || (n_header_ranges && !header_ranges) || (n_cell_ranges && !cell_ranges))
+        return VGI_ERR_INVALID;
+    if (!c->geometry || !c->packed_geometry) return fail(c, VGI_ERR_STATE, "a packed delta needs geometry from vgi_upload_packed");
+    if (!directory_rebuilt && slots != c->dir_slots)
+        return fail(c, VGI_ERR_INVALID, "a directory of another capacity must be sent whole (directory_rebuilt)");
+    if (directory_rebuilt && !dir_data) return VGI_ERR_INVALID;
+    // The ranges' elements, back to back in each data array.
+    auto check_ranges = [](const uint64_t* r, uint32_t n, uint64_t length, const void* data, uint64_t* total) {
+        *total = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (r[2 * i] > length || r[2 * i + 1] > length - r[2 * i]) return false;
+            *total += r[2 * i + 1];
+        }
+        return *total == 0 || data != nullptr;
+    };
+    uint64_t dir_total = 0, header_total = 0, cell_total = 0;
+    if ((!directory_rebuilt && !check_ranges(dir_ranges, n_dir_ranges, slots, dir_data, &dir_total)) ||
+        !check_ranges(header_ranges, n_header_ranges, n_headers, header_data, &header_total) ||
+        !check_ranges(cell_ranges, n_cell_ranges, n_cells, cell_data, &cell_total))
+        return fail(c, VGI_ERR_INVALID, "a delta range lies outside its array");
+    // The patched arrays on the host; grown elements start at zero, as the
+    // device's grown tails do below.
+    std::vector<int32_t> dir;
+    if (directory_rebuilt) {
+        dir.assign(dir_data, dir_data + slots * 4);
+    } else {
+        dir = c->host_dir;
+        for (uint32_t i = 0, at = 0; i < n_dir_ranges; at += (uint32_t)dir_ranges[2 * i + 1] * 4, ++i)
+            std::copy(dir_data + at, dir_data + at + dir_ranges[2 * i + 1] * 4, dir.begin() + dir_ranges[2 * i] * 4);
+    }
+    std::vector<uint4> hdr = c->host_headers;
+    hdr.resize(n_headers, make_uint4(0u, 0u, 0u, 0u));
+    for (uint64_t i = 0, at = 0; i < n_header_ranges; at += header_ranges[2 * i + 1] * 4, ++i)
+        std::memcpy(hdr.data() + header_ranges[2 * i], header_data + at, header_ranges[2 * i + 1] * 16);
+    std::vector<uint32_t> cl = c->host_cells;
+    cl.resize(n_cells, 0u);
+    for (uint64_t i = 0, at = 0; i < n_cell_ranges; at += cell_ranges[2 * i + 1], ++i)
+        std::copy(cell_data + at, cell_data + at + cell_ranges[2 * i + 1], cl.begin() + cell_ranges[2 * i]);
+    int rc = validate_packed(c, dir.data(), slots, reinterpret_cast<const uint32_t*>(hdr.data()), n_headers, cl.data(), n_cells);
+    if (rc != VGI_OK) return rc;
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    // One transaction on the stream. A longer array grows with its contents
+    // copied on the device (the grown tail cleared); only the ranges cross
+    // the bus. A failure from here leaves no geometry until the next upload.
+    c->geometry = false;
+    const size_t old_headers = c->host_headers.size(), old_cells = c->host_cells.size();
+    if (directory_rebuilt) {
+        VGI_CUDA(c, c->directory.reserve(slots));
+        VGI_CUDA(c, h2d(c->directory.ptr, dir.data(), slots * 16, c->stream));
+    } else {
+        for (uint32_t i = 0, at = 0; i < n_dir_ranges; at += (uint32_t)dir_ranges[2 * i + 1] * 4, ++i)
+            if (dir_ranges[2 * i + 1]) VGI_CUDA(c, h2d(c->directory.ptr + dir_ranges[2 * i], dir_data + at, dir_ranges[2 * i + 1] * 16, c->stream));
+    }
+    VGI_CUDA(c, c->headers.grow(std::max<uint32_t>(n_headers, 1), old_headers, c->stream));
+    if (n_headers > old_headers)
+        VGI_CUDA(c, cudaMemsetAsync(c->headers.ptr + old_headers, 0, (n_headers - old_headers) * 16, c->stream));
+    for (uint64_t i = 0, at = 0; i < n_header_ranges; at += header_ranges[2 * i + 1] * 4, ++i)
+        if (header_ranges[2 * i + 1])
+            VGI_CUDA(c, h2d(c->headers.ptr + header_ranges[2 * i], header_data + at, header_ranges[2 * i + 1] * 16, c->stream));
+    VGI_CUDA(c, c->cells.grow(std::max<uint64_t>(n_cells, 1), old_cells, c->stream));
+    if (n_cells > old_cells) VGI_CUDA(c, cudaMemsetAsync(c->cells.ptr + old_cells, 0, (n_cells - old_cells) * 4, c->stream));
+    for (uint64_t i = 0, at = 0; i < n_cell_ranges; at += cell_ranges[2 * i + 1], ++i)
+        if (cell_ranges[2 * i + 1])
+            VGI_CUDA(c, h2d(c->cells.ptr + cell_ranges[2 * i], cell_data + at, cell_ranges[2 * i + 1] * 4, c->stream));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->dir_slots = slots;
+    c->cells_used = n_cells;
+    for (int k = 0; k < 6; ++k) c->bounds[k] = bounds6[k];
+    c->host_dir = std::move(dir);
+    c->host_headers = std::move(hdr);
+    c->host_cells = std::move(cl);
+    VGI_CUDA(c, upload_grid(c, c->host_dir.data(), slots));
+    VGI_CUDA(c, refresh_grid_headers(c));
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->geometry = true;
     return VGI_OK;
 }
@@ -950,6 +1052,7 @@ static int apply_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const ui
         c->live.clear();
         c->free_slots.clear();
         c->host_dir.clear();
+        c->host_cells.clear();
         c->top = TopLevelField{};
         c->cells_used = 0;
         c->packed_geometry = false;
@@ -967,6 +1070,20 @@ static int apply_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const ui
     std::unordered_map<RegionKey, int, RegionKeyHash> before;
     std::vector<RegionKey> touched;
     std::vector<uint32_t> freed;
+    // A loaded region whose voxels and stride equal the resident region's is
+    // the same region (build_page_regions keeps the previous Arc), so it is
+    // not touched, even when the same call also unloads it
+    // (with_page_contents' touched.retain, src/world.rs:1016-1020).
+    std::unordered_set<RegionKey, RegionKeyHash> unchanged;
+    for (uint32_t i = 0; i < n; ++i) {
+        const RegionKey k{coords[i * 3], coords[i * 3 + 1], coords[i * 3 + 2]};
+        auto it = c->where.find(k);
+        if (it == c->where.end()) continue;
+        const uint8_t stride = strides ? strides[i] : 0;
+        if (c->strides[it->second] == stride &&
+            std::equal(voxels + (size_t)i * 4096, voxels + (size_t)(i + 1) * 4096, c->host_voxels.begin() + (size_t)it->second * 4096))
+            unchanged.insert(k);
+    }
     for (uint32_t i = 0; i < n_removed; ++i) {
         const RegionKey k{removed[i * 3], removed[i * 3 + 1], removed[i * 3 + 2]};
         auto it = c->where.find(k);
@@ -979,7 +1096,7 @@ static int apply_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const ui
         c->host_headers[slot] = make_uint4(0u, 0u, 0u, 0u);
         if (!c->host_dir.empty()) directory_remove(c->host_dir, k);
         freed.push_back(slot);
-        touched.push_back(k);
+        if (!unchanged.count(k)) touched.push_back(k);
     }
     const uint32_t old_slots = (uint32_t)c->keys.size();
     std::vector<uint32_t> slots(n);
@@ -1011,7 +1128,7 @@ static int apply_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const ui
         std::copy(voxels + (size_t)i * 4096, voxels + (size_t)(i + 1) * 4096, c->host_voxels.begin() + (size_t)slot * 4096);
         c->strides[slot] = strides ? strides[i] : 0;
         slots[i] = slot;
-        touched.push_back(k);
+        if (!unchanged.count(k)) touched.push_back(k);
     }
     // A freed slot that a load took again is live.
     freed.erase(std::remove_if(freed.begin(), freed.end(), [c](uint32_t s) { return c->live[s] != 0; }), freed.end());
@@ -1111,11 +1228,16 @@ int vgi_unload_regions(vgi_ctx* c, const int32_t* coords, uint32_t n) {
     return apply_regions(c, nullptr, 0, nullptr, nullptr, coords, n);
 }
 
+int vgi_update_regions(vgi_ctx* c, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides,
+                       const int32_t* removed, uint32_t n_removed) {
+    return apply_regions(c, coords, n, voxels, strides, removed, n_removed);
+}
+
 int vgi_geometry_info(vgi_ctx* c, uint64_t* sizes3, int32_t* bounds6) {
     if (!c || !sizes3 || !bounds6) return VGI_ERR_INVALID;
     if (!c->geometry) return fail(c, VGI_ERR_STATE, "no geometry uploaded");
     sizes3[0] = c->dir_slots;
-    sizes3[1] = c->keys.empty() ? c->headers.count : c->keys.size();
+    sizes3[1] = c->packed_geometry ? c->host_headers.size() : (c->keys.empty() ? c->headers.count : c->keys.size());
     sizes3[2] = c->cells_used;
     for (int k = 0; k < 6; ++k) bounds6[k] = c->bounds[k];
     return VGI_OK;

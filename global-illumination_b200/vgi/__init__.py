@@ -224,9 +224,11 @@ _SIGNATURES = {
     "vgi_sync": (_INT, [_P]),
     "vgi_upload_regions": (_INT, [_P, _P, _U32, _P, _P]),
     "vgi_upload_packed": (_INT, [_P, _P, _U64, _P, _U32, _P, _U64, _P]),
+    "vgi_patch_packed": (_INT, [_P, _U64, _U32, _U64, _P, _INT, _P, _U32, _P, _P, _U32, _P, _P, _U32, _P]),
     "vgi_edit_voxels": (_INT, [_P, _P, _U32]),
     "vgi_load_regions": (_INT, [_P, _P, _U32, _P, _P]),
     "vgi_unload_regions": (_INT, [_P, _P, _U32]),
+    "vgi_update_regions": (_INT, [_P, _P, _U32, _P, _P, _P, _U32]),
     "vgi_geometry_info": (_INT, [_P, _P, _P]),
     "vgi_read_geometry": (_INT, [_P, _P, _P, _P]),
     "vgi_set_materials": (_INT, [_P, _P]),
@@ -500,6 +502,33 @@ class GpuTracer:
         b = _c(bounds, np.int32).reshape(-1)
         self._check(self._lib.vgi_upload_packed(self._h, _ptr(d), d.size // 4, _ptr(h), h.size // 4, _ptr(c), c.size, _ptr(b)))
 
+    def patch_packed(self, lengths, bounds, directory_rebuilt: bool, directory, headers, cells) -> None:
+        """A SceneDelta on packed geometry (synchronize_geometry): `lengths`
+        = (directory slots, headers, cells) after the change; `directory`,
+        `headers`, `cells` are lists of (start, elements) with elements
+        shaped (k, 4) int32, (k, 4) uint32 and (k,) uint32; with
+        directory_rebuilt, `directory` is the whole new directory instead."""
+
+        def pack(parts, dtype, width):
+            ranges = np.array([[start, len(np.asarray(e).reshape(-1, width))] for start, e in parts], np.uint64).reshape(-1)
+            data = np.concatenate([_c(e, dtype).reshape(-1) for _, e in parts]) if parts else np.zeros(0, dtype)
+            return ranges, data
+
+        b = _c(bounds, np.int32).reshape(-1)
+        if directory_rebuilt:
+            d_ranges, d_data = np.zeros(0, np.uint64), _c(directory, np.int32).reshape(-1)
+            n_d = 0
+        else:
+            d_ranges, d_data = pack(directory, np.int32, 4)
+            n_d = d_ranges.size // 2
+        h_ranges, h_data = pack(headers, np.uint32, 4)
+        c_ranges, c_data = pack(cells, np.uint32, 1)
+        d_data, h_data, c_data = (np.ascontiguousarray(x) for x in (d_data, h_data, c_data))
+        self._check(self._lib.vgi_patch_packed(
+            self._h, int(lengths[0]), int(lengths[1]), int(lengths[2]), _ptr(b), 1 if directory_rebuilt else 0,
+            _ptr(d_ranges), n_d, _ptr(d_data), _ptr(h_ranges), h_ranges.size // 2, _ptr(h_data),
+            _ptr(c_ranges), c_ranges.size // 2, _ptr(c_data)))
+
     def load_regions(self, coords: np.ndarray, voxels: np.ndarray, strides: Optional[np.ndarray] = None) -> None:
         """page_loaded / page_changed: regions (coords n x 3, voxels n x 4096)
         loaded into the GPU geometry, replacing resident ones."""
@@ -513,6 +542,17 @@ class GpuTracer:
         """page_unloaded: regions removed from the GPU geometry."""
         c = _c(coords, np.int32).reshape(-1, 3)
         self._check(self._lib.vgi_unload_regions(self._h, _ptr(c), c.shape[0]))
+
+    def update_regions(self, coords: np.ndarray, voxels: np.ndarray, removed: np.ndarray,
+                       strides: Optional[np.ndarray] = None) -> None:
+        """One frame's page events as one scene change (with_page_contents):
+        `removed` regions unloaded, then `coords`/`voxels` loaded."""
+        c = _c(coords, np.int32).reshape(-1, 3)
+        v = _c(voxels, np.uint16).reshape(-1)
+        assert v.size == c.shape[0] * 4096
+        r = _c(removed, np.int32).reshape(-1, 3)
+        st = None if strides is None else _c(strides, np.uint8)
+        self._check(self._lib.vgi_update_regions(self._h, _ptr(c), c.shape[0], _ptr(v), _ptr(st), _ptr(r), r.shape[0]))
 
     def edit_voxels(self, edits: np.ndarray) -> None:
         e = _c(edits, np.int32).reshape(-1, 4)

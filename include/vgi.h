@@ -108,6 +108,24 @@ int vgi_upload_regions(vgi_ctx* ctx, const int32_t* coords, uint32_t n, const ui
  * slot, headers 4 words per region, cells) and region bounds min xyz, max xyz. */
 int vgi_upload_packed(vgi_ctx* ctx, const int32_t* directory, uint64_t slots, const uint32_t* headers, uint32_t n_headers,
                       const uint32_t* cells, uint64_t n_cells, const int32_t* bounds6);
+/* One SceneDelta applied to geometry from vgi_upload_packed, as
+ * GpuTracer::synchronize_geometry stages it (src/gpu/geometry.rs:19-124;
+ * SceneDelta, src/gpu_scene.rs:49-60). `slots`, `n_headers` and `n_cells` are
+ * the arrays' new lengths and `bounds6` the new region bounds. Each range is a
+ * (start, count) pair of u64 element indices; each data array holds its
+ * ranges' elements back to back (directory 4 ints per slot, headers 4 words
+ * per region, cells one word). directory_rebuilt != 0: `dir_data` is the whole
+ * new directory (`slots` entries) and dir_ranges is ignored; a directory of
+ * another capacity must come this way. An array that grows keeps its contents
+ * on the device (its new tail starts at zero); only the ranges cross the bus,
+ * all on the context's stream as one transaction, complete when the call
+ * returns. The patched arrays are checked on the host copy first, as
+ * vgi_upload_packed checks whole arrays: a refused delta (VGI_ERR_INVALID)
+ * changes nothing. VGI_ERR_STATE without packed geometry. */
+int vgi_patch_packed(vgi_ctx* ctx, uint64_t slots, uint32_t n_headers, uint64_t n_cells, const int32_t* bounds6, int directory_rebuilt,
+                     const uint64_t* dir_ranges, uint32_t n_dir_ranges, const int32_t* dir_data, const uint64_t* header_ranges,
+                     uint32_t n_header_ranges, const uint32_t* header_data, const uint64_t* cell_ranges, uint32_t n_cell_ranges,
+                     const uint32_t* cell_data);
 /* Page streaming on the GPU geometry: VoxelGiInput::page_loaded and
  * page_changed (vgi_load_regions) and page_unloaded (vgi_unload_regions),
  * src/input.rs:54-70, applied as TransportScene::with_page_contents
@@ -125,6 +143,16 @@ int vgi_upload_packed(vgi_ctx* ctx, const int32_t* directory, uint64_t slots, co
  * vgi_upload_packed (VGI_ERR_STATE). Synchronous. */
 int vgi_load_regions(vgi_ctx* ctx, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides);
 int vgi_unload_regions(vgi_ctx* ctx, const int32_t* coords, uint32_t n);
+/* One frame's page events as one scene change, as with_page_contents takes
+ * its changed and removed pages together (src/world.rs:982-1046): `removed`
+ * (3 ints per region) are unloaded, then `coords`/`voxels` loaded, and the
+ * top-level field is updated once over every touched region. A loaded region
+ * equal to the resident one (same voxels and stride) is not touched, even if
+ * the same call unloads it. The top-level field is an order-dependent fixed
+ * point, so one call here and a vgi_unload_regions then vgi_load_regions pair
+ * can leave different (equally valid) extents. */
+int vgi_update_regions(vgi_ctx* ctx, const int32_t* coords, uint32_t n, const uint16_t* voxels, const uint8_t* strides,
+                       const int32_t* removed, uint32_t n_removed);
 /* VoxelGiInput::edit_voxel batch (src/input.rs:90-93): 4 ints per edit
  * (x, y, z, value). Voxels outside uploaded regions are ignored. The edited
  * regions are repacked on the GPU and the top-level field is updated

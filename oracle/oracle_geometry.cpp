@@ -18,6 +18,7 @@
 #include <array>
 #include <deque>
 #include <map>
+#include <set>
 #include <vector>
 
 namespace orc {
@@ -561,13 +562,26 @@ int orc_scene_regions(orc_scene* sc, const int32_t* coords, uint32_t n, const ui
     };
     std::map<std::array<int32_t, 3>, int> before;
     std::vector<std::array<int32_t, 3>> touched;
+    // build_page_regions keeps the previous region when the page brings the
+    // same materials and stride (src/world.rs:1490-1494), and touched.retain
+    // drops a key whose region is the same before and after (:1016-1020),
+    // even when the same change also removed it.
+    std::set<std::array<int32_t, 3>> unchanged;
+    for (uint32_t i = 0; i < n; ++i) {
+        const auto key = zyx(coords[i * 3], coords[i * 3 + 1], coords[i * 3 + 2]);
+        auto it = regions.find(key);
+        if (it == regions.end()) continue;
+        if (it->second.stride == (strides ? strides[i] : (uint8_t)0) &&
+            std::equal(it->second.v.begin(), it->second.v.end(), voxels + (size_t)i * 4096))
+            unchanged.insert(key);
+    }
     for (uint32_t i = 0; i < n_removed; ++i) {
         const std::array<int32_t, 3> c{removed[i * 3], removed[i * 3 + 1], removed[i * 3 + 2]};
         const auto key = zyx(c[0], c[1], c[2]);
         if (!regions.count(key)) continue;
         if (!before.count(key)) before[key] = status(key);
         regions.erase(key);
-        touched.push_back(c);
+        if (!unchanged.count(key)) touched.push_back(c);
     }
     for (uint32_t i = 0; i < n; ++i) {
         const std::array<int32_t, 3> c{coords[i * 3], coords[i * 3 + 1], coords[i * 3 + 2]};
@@ -575,7 +589,7 @@ int orc_scene_regions(orc_scene* sc, const int32_t* coords, uint32_t n, const ui
         if (!before.count(key)) before[key] = status(key);
         regions[key] = Region{c, std::vector<uint16_t>(voxels + (size_t)i * 4096, voxels + (size_t)(i + 1) * 4096),
                               strides ? strides[i] : (uint8_t)0};
-        touched.push_back(c);
+        if (!unchanged.count(key)) touched.push_back(c);
     }
     bool topology_unchanged = true;
     for (const auto& kv : before) {

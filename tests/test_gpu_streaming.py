@@ -1,10 +1,14 @@
-"""Page streaming on the GPU geometry (vgi_load_regions / vgi_unload_regions:
-page_loaded, page_changed and page_unloaded, src/input.rs:54-70) against the
-oracle's restatement of TransportScene::with_page_contents with the same
-region deltas (orc_scene_regions).
+"""Page streaming on the GPU geometry (vgi_update_regions, vgi_load_regions,
+vgi_unload_regions: page_loaded, page_changed and page_unloaded,
+src/input.rs:54-70) against the oracle's restatement of
+TransportScene::with_page_contents with the same region deltas
+(orc_scene_regions).
 
 A terrain streams in and out across frames: regions load, unload, load
-again, and loaded ones are replaced with carved copies. After every delta:
+again, loaded ones are replaced with carved copies, and some are sent again
+unchanged (also while being unloaded in the same change). Odd deltas are one
+scene change (vgi_update_regions), even ones an unload then a load, and the
+oracle takes the same changes. After every delta:
 - the GPU's packed geometry equals the oracle's in canonical form (every
   region of the terrain, resident or not, with its top-level extents);
 - without the top-level extents, it also equals a fresh pack of the same
@@ -80,7 +84,10 @@ def test_streamed_pages_match_the_oracle():
                 out = [k for k in resident if rng.random() < 0.25]
                 back = [tuple(c) for c in coords if tuple(c) not in resident and rng.random() < 0.5]
                 change = [k for k in resident if k not in out and rng.random() < 0.1]
-                loads = back + change
+                # Pages sent again with the same voxels, some also unloaded in
+                # the same change: the same regions, so not touched.
+                same = [k for k in resident if k not in change and rng.random() < 0.1]
+                loads = back + change + same
                 for k in back:
                     current[k] = vox[key[k]]
                 for i, k in enumerate(change):
@@ -88,14 +95,24 @@ def test_streamed_pages_match_the_oracle():
                 load_coords = np.array(loads, np.int32).reshape(-1, 3)
                 load_vox = np.stack([current[k] for k in loads]) if loads else np.zeros((0, 4096), np.uint16)
                 out_coords = np.array(out, np.int32).reshape(-1, 3)
-                if out:
-                    g.unload_regions(out_coords)
-                if loads:
-                    g.load_regions(load_coords, load_vox)
-                ref.regions(load_coords, load_vox, removed=out_coords)
+                if step % 2:
+                    # One scene change per frame, as with_page_contents takes
+                    # the frame's changed and removed pages together.
+                    g.update_regions(load_coords, load_vox, out_coords)
+                    ref.regions(load_coords, load_vox, removed=out_coords)
+                else:
+                    # Unload, then load: two scene changes on both sides.
+                    if out:
+                        g.unload_regions(out_coords)
+                    if loads:
+                        g.load_regions(load_coords, load_vox)
+                    ref.regions(removed=out_coords)
+                    ref.regions(load_coords, load_vox)
+                resident.update(same)
                 for k in out:
-                    resident.discard(k)
-                    current.pop(k, None)
+                    if k not in same:
+                        resident.discard(k)
+                        current.pop(k, None)
                 resident.update(back)
             # Geometry: canonical form over every region of the terrain.
             d, h, cl, bounds = g.geometry()
