@@ -494,7 +494,7 @@ int wave_buffers(vgi_ctx* c, const TraceArgs& a, bool count, bool marks, WaveBuf
         room_slots = std::max(room_slots, tp * (2 + a.light_count) + rows * a.light_count);
     }
     const void* before[3] = {c->w_state.ptr, c->w_ray.ptr, c->w_status.ptr};
-    VGI_CUDA(c, c->w_state.reserve(std::max<size_t>(room_paths, 1) * 9));
+    VGI_CUDA(c, c->w_state.reserve(std::max<size_t>(room_paths, 1) * kWavePathFields));
     VGI_CUDA(c, c->w_ray.reserve(std::max<size_t>(room_slots, 1) * 2));
     VGI_CUDA(c, c->w_hit.reserve(std::max<size_t>(room_paths, 1) * 6));
     VGI_CUDA(c, c->w_status.reserve(std::max<size_t>(room_slots, 1)));

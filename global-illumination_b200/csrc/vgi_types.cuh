@@ -77,8 +77,11 @@ struct MlpEncoding {
 // (vgi_mlp_set_wait_limit); a wait that runs out sets the error word.
 constexpr uint32_t kMlpWaitPolls = 1u << 22;
 
+// float4 fields of path state per path in the wavefront layout.
+constexpr uint32_t kWavePathFields = 6;
+
 struct WaveBuffers {
-    float4* state;            // 9 * P path-state words
+    float4* state;            // kWavePathFields * P path-state words
     float4* ray;              // 2 * S
     uint32_t* status;         // S
     uint4* hit;               // 6 * P (full results of slots 0 and 1)

@@ -45,17 +45,19 @@ constexpr int kWaveBlock = 256;
 enum : uint32_t {
     kE = 0,    // continuation energy rgb, previous_pdf
     kTP = 1,   // throughput for the next hit rgb, bounce (bits)
-    kPP = 2,   // previous position xyz (the last hit point), flags (bits)
-    kPN = 3,   // previous normal xyz
-    kTH = 4,   // throughput at the pending hit rgb, pending kind (bits)
-    kEM = 5,   // emission * mis of the pending hit rgb
-    kDF = 6,   // diffuse of the pending hit rgb
-    kX = 7,    // cached energy or pending emitter value rgb
-    kN0 = 8,   // receiver NEE (pending, then final) rgb
-    kFields = 9,
+    kPP = 2,   // previous position xyz (the last hit point), the path word (bits)
+    kTH = 3,   // throughput at the pending hit rgb, the hit's emission MIS weight
+    kX = 4,    // cached energy or pending emitter value rgb
+    kN0 = 5,   // receiver NEE (pending, then final) rgb
+    kFields = 6,
 };
+static_assert(kFields == kWavePathFields, "path-state fields");
 
-// Path flags (kPP.w).
+// The path word (kPP.w): flags in bits 0-5, the pending contribution's kind
+// in bits 8-10, the previous normal in bits 12-17 (two bits an axis) and the
+// pending hit's material in bits 24-31. A pending hit's emission * MIS and
+// diffuse are its material's values times kTH.w, formed again where they
+// are used with the same operations, so they need no fields of their own.
 constexpr uint32_t kFlagContinue = 1u;   // slot 0 holds this stage's continuation ray
 constexpr uint32_t kFlagUnknown = 2u;    // reached unloaded space
 constexpr uint32_t kFlagRan = 4u;        // the receiver's continuation was traced
@@ -63,8 +65,21 @@ constexpr uint32_t kFlagS0 = 8u;         // slot 1 holds the receiver's NEE shad
 constexpr uint32_t kFlagN = 16u;         // slot 1 holds the pending hit's NEE or terminal ray
 constexpr uint32_t kFlagValid = 32u;     // a traced sample of a valid task
 
-// Pending-contribution kinds (kTH.w).
+// Pending-contribution kinds (path word bits 8-10).
 constexpr uint32_t kKindNone = 0u, kKindCached = 1u, kKindNee = 2u, kKindTermEmitter = 3u, kKindTermCosine = 4u;
+
+__device__ __forceinline__ uint32_t kind_of(uint32_t w) { return (w >> 8) & 7u; }
+__device__ __forceinline__ uint32_t with_kind(uint32_t w, uint32_t k) { return (w & ~(7u << 8)) | (k << 8); }
+// Normals on the path are face normals or zero: each axis is +0, -0, +1 or
+// -1 (the traversal's normals carry signed zeros), coded 0, 1, 2, 3.
+__device__ __forceinline__ uint32_t axis_code(float v) { return v > 0.0f ? 2u : (v < 0.0f ? 3u : (__float_as_uint(v) >> 31)); }
+__device__ __forceinline__ float axis_value(uint32_t c) { return c == 2u ? 1.0f : (c == 3u ? -1.0f : __uint_as_float(c << 31)); }
+__device__ __forceinline__ uint32_t with_normal(uint32_t w, V3 n) {
+    return (w & ~(63u << 12)) | ((axis_code(n.x) | (axis_code(n.y) << 2) | (axis_code(n.z) << 4)) << 12);
+}
+__device__ __forceinline__ V3 normal_of(uint32_t w) { return V3{axis_value((w >> 12) & 3u), axis_value((w >> 14) & 3u), axis_value((w >> 16) & 3u)}; }
+__device__ __forceinline__ uint32_t with_material(uint32_t w, uint32_t m) { return (w & 0x00ffffffu) | ((m & 255u) << 24); }
+__device__ __forceinline__ uint32_t material_of(uint32_t w) { return w >> 24; }
 
 struct WaveArgs {
     TraceArgs t;
@@ -253,10 +268,15 @@ struct WaveTracer {
     __device__ uint32_t traced_status(uint32_t slot) const { return W.status[slot]; }
 
     // Completes the pending hit of path p: energy += tp * (em*mis + diffuse * (direct + X)).
-    __device__ void combine(uint32_t p, uint32_t kind, uint32_t flags, float4& e) {
-        const float4 th = field(W, kTH, p), em = field(W, kEM, p), df = field(W, kDF, p), xv = field(W, kX, p);
-        const float4 pp = field(W, kPP, p), pn = field(W, kPN, p);
-        const V3 position{pp.x, pp.y, pp.z}, normal{pn.x, pn.y, pn.z};
+    // `word` is the path word and `position` the pending hit point (kPP).
+    __device__ void combine(uint32_t p, uint32_t word, V3 position, float4& e) {
+        const uint32_t kind = kind_of(word), flags = word;
+        const float4 th = field(W, kTH, p), xv = field(W, kX, p);
+        const V3 normal = normal_of(word);
+        const Mat mat = material_nocount(material_of(word));
+        // The hit's emission * mis and diffuse, as the shade stage formed them.
+        const V3 em = V3{mat.emission.x, mat.emission.y, mat.emission.z} * th.w;
+        const V3 df{mat.diffuse.x, mat.diffuse.y, mat.diffuse.z};
         const uint32_t base = p * W.slots;
         V3 unused;
         float unused_w;
@@ -296,7 +316,7 @@ struct WaveTracer {
             }
         }
         const V3 tp{th.x, th.y, th.z};
-        const V3 t = V3{em.x, em.y, em.z} + V3{df.x, df.y, df.z} * (direct + x);
+        const V3 t = em + df * (direct + x);
         const V3 energy = V3{e.x, e.y, e.z} + tp * t;
         e.x = energy.x;
         e.y = energy.y;
@@ -371,6 +391,7 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_BEGIN_MIN_BLOCKS) wave_begin_k
         } else {
             field(W, kN0, p) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
+        // Nothing is pending yet (kind 0 in the path word).
         if (dot3(normal, direction) > 0.0f) {
             flags |= kFlagRan;
             const V3 start = surface + normal * 0.001f;
@@ -378,21 +399,18 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_BEGIN_MIN_BLOCKS) wave_begin_k
             const V3 previous_position = start - normal * 0.001f;
             field(W, kE, p) = make_float4(0.0f, 0.0f, 0.0f, previous_pdf);
             field(W, kTP, p) = make_float4(1.0f, 1.0f, 1.0f, fl(0u));
-            field(W, kPN, p) = make_float4(normal.x, normal.y, normal.z, 0.0f);
             if (previous_pdf > 0.0f) {
                 c0 = true;
                 flags |= kFlagContinue;
                 put_ray(W, base, start, direction, T.reach(), hit_of(p, 0u));
             }
-            field(W, kPP, p) = make_float4(previous_position.x, previous_position.y, previous_position.z, fl(flags));
+            field(W, kPP, p) = make_float4(previous_position.x, previous_position.y, previous_position.z, fl(with_normal(flags, normal)));
         } else {
             field(W, kE, p) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             field(W, kPP, p) = make_float4(0.0f, 0.0f, 0.0f, fl(flags));
         }
-        field(W, kTH, p) = make_float4(0.0f, 0.0f, 0.0f, fl(kKindNone));
     } else if (in) {
         field(W, kPP, p) = make_float4(0.0f, 0.0f, 0.0f, fl(0u));
-        field(W, kTH, p) = make_float4(0.0f, 0.0f, 0.0f, fl(kKindNone));
     }
     enqueue(W, s0, base + 1u);
     enqueue(W, c0, base);
@@ -935,8 +953,7 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SHADE_MIN_BLOCKS) wave_shade_k
             else n0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             field(W, kN0, p) = n0;
         }
-        const uint32_t kind = bits(field(W, kTH, p).w);
-        if (kind != kKindNone) T.combine(p, kind, flags, e);
+        if (kind_of(flags) != kKindNone) T.combine(p, flags, V3{pp.x, pp.y, pp.z}, e);
         flags &= ~(kFlagS0 | kFlagN);
         uint32_t pending_kind = kKindNone;
         if (flags & kFlagContinue) {
@@ -964,8 +981,7 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SHADE_MIN_BLOCKS) wave_shade_k
                 const I3 hv{(int)h0.z, (int)h0.w, (int)h1.x};
                 cnt.bytes(64);
                 const Mat m = T.material_nocount(h0.y);
-                const float4 ppos = pp, pnrm = field(W, kPN, p);
-                const V3 previous_position{ppos.x, ppos.y, ppos.z}, previous_normal{pnrm.x, pnrm.y, pnrm.z};
+                const V3 previous_position{pp.x, pp.y, pp.z}, previous_normal = normal_of(flags);
                 const float previous_pdf = e.w;
                 // direct_at's rays from the hit.
                 emit_d = true;
@@ -977,14 +993,7 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SHADE_MIN_BLOCKS) wave_shade_k
                 const float light_pdf = __fdiv_rn(__fmul_rn(selection_pdf, dot3(delta, delta)), wmax(dot3(hn, -direction), 1e-8f));
                 float mis = 1.0f;
                 if (light_pdf > 0.0f) mis = __fdiv_rn(previous_pdf, __fadd_rn(previous_pdf, light_pdf));
-                const V3 emission{m.emission.x, m.emission.y, m.emission.z};
                 const V3 diffuse{m.diffuse.x, m.diffuse.y, m.diffuse.z};
-                const V3 em_mis = emission * mis;
-                // Task identity for the sampler.
-                const uint32_t face = p / A.samples, sample = p - face * A.samples;
-                const uint4 t0 = __ldg(A.tasks + face * 2u), t1 = __ldg(A.tasks + face * 2u + 1u);
-                const uint32_t pstream = hash_voxel((int)t0.x, (int)t0.y, (int)t0.z) ^ pcg(t0.w + 1u);
-                const uint32_t sequence = t1.x + sample;
                 V3 cached;
                 V3 xval{0.0f, 0.0f, 0.0f};
                 bool have_cache = false;
@@ -1032,19 +1041,17 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SHADE_MIN_BLOCKS) wave_shade_k
                     scatter = true;
                     scatter_entry = p | (bounce << 30);
                 }
-                (void)pstream;
-                (void)sequence;
-                field(W, kTH, p) = make_float4(tp.x, tp.y, tp.z, fl(pending_kind));
-                field(W, kEM, p) = make_float4(em_mis.x, em_mis.y, em_mis.z, 0.0f);
-                field(W, kDF, p) = make_float4(diffuse.x, diffuse.y, diffuse.z, 0.0f);
+                // The hit's emission * mis and diffuse come from its material
+                // and the weight kept here (combine).
+                field(W, kTH, p) = make_float4(tp.x, tp.y, tp.z, mis);
                 field(W, kX, p) = make_float4(xval.x, xval.y, xval.z, 0.0f);
-                field(W, kPN, p) = make_float4(hn.x, hn.y, hn.z, 0.0f);
+                flags = with_material(with_normal(flags, hn), h0.y);
                 pp = make_float4(hp.x, hp.y, hp.z, 0.0f);
                 dpos = hp;
                 dnrm = hn;
             }
         }
-        if (pending_kind == kKindNone) field(W, kTH, p) = make_float4(0.0f, 0.0f, 0.0f, fl(kKindNone));
+        flags = with_kind(flags, pending_kind);
         field(W, kE, p) = e;
         pp.w = fl(flags);
         field(W, kPP, p) = pp;
@@ -1102,9 +1109,11 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SCATTER_MIN_BLOCKS) wave_scatt
         const uint32_t base = p * W.slots;
         bool emit_n = false, emit_c = false;
         if (active) {
-            const float4 pp = field(W, kPP, p), pn = field(W, kPN, p), th = field(W, kTH, p), df = field(W, kDF, p);
-            const V3 hp{pp.x, pp.y, pp.z}, hn{pn.x, pn.y, pn.z}, tp{th.x, th.y, th.z}, diffuse{df.x, df.y, df.z};
+            const float4 pp = field(W, kPP, p), th = field(W, kTH, p);
             uint32_t flags = bits(pp.w);
+            const Mat mat = T.material_nocount(material_of(flags));
+            const V3 hp{pp.x, pp.y, pp.z}, hn = normal_of(flags), tp{th.x, th.y, th.z};
+            const V3 diffuse{mat.diffuse.x, mat.diffuse.y, mat.diffuse.z};
             const uint32_t face = p / A.samples, sample = p - face * A.samples;
             const uint4 t0 = __ldg(A.tasks + face * 2u), t1 = __ldg(A.tasks + face * 2u + 1u);
             const uint32_t pstream = hash_voxel((int)t0.x, (int)t0.y, (int)t0.z) ^ pcg(t0.w + 1u);
@@ -1157,9 +1166,9 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_SCATTER_MIN_BLOCKS) wave_scatt
                 }
             }
             if (emit_n) flags |= kFlagN;
-            field(W, kTH, p) = make_float4(tp.x, tp.y, tp.z, fl(kind));
+            // kTH (the throughput at this hit and its MIS weight) stays.
             field(W, kX, p) = make_float4(pend.x, pend.y, pend.z, 0.0f);
-            field(W, kPP, p) = make_float4(pp.x, pp.y, pp.z, fl(flags));
+            field(W, kPP, p) = make_float4(pp.x, pp.y, pp.z, fl(with_kind(flags, kind)));
         }
         enqueue(W, emit_n, base + 1u);
         enqueue(W, emit_c, base);
@@ -1191,10 +1200,10 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_FINALIZE_MIN_BLOCKS) wave_fina
 #pragma unroll 1
         for (uint32_t i = lane; i < A.samples; i += lanes) {
             const uint32_t p = face * A.samples + i;
-            const uint32_t flags = bits(field(W, kPP, p).w);
+            const float4 pp = field(W, kPP, p);
+            const uint32_t flags = bits(pp.w);
             float4 e = field(W, kE, p);
-            const uint32_t kind = bits(field(W, kTH, p).w);
-            if (kind != kKindNone) T.combine(p, kind, flags, e);
+            if (kind_of(flags) != kKindNone) T.combine(p, flags, V3{pp.x, pp.y, pp.z}, e);
             if (flags & kFlagUnknown) {
                 cnt.unknown();
                 continue;
