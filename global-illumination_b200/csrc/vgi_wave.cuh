@@ -422,11 +422,25 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_BEGIN_MIN_BLOCKS) wave_begin_k
 
 // One lane's ray in flight: trace_domain_limited's loop variables.
 struct RayRun {
-    V3 dir, inv, pos, nrm;
+    V3 dir, pos;
+    // The direction's reciprocals for div_recip on the axes the traversal
+    // treats as moving (|d| > 1e-8), NaN on the others. advance_box gives a
+    // non-moving axis the distance 1e30; a NaN quotient fails its range test
+    // and takes 1e30 the same way, so the step needs no test of its own.
+    V3 inv;
     float dist, maxd;
     int lrx, lry, lrz;
     uint4 meta;
     uint32_t step, slot;
+    // The last step's normal, coded two bits an axis (axis_code), expanded
+    // when the ray ends.
+    uint32_t ncode;
+    // Per axis, from the direction's sign: bits 0-5 the code the axis's
+    // normal component takes when another axis is the exit (advance_box
+    // multiplies 0 by -1 when d > 0: -0), bits 8-13 the code it takes when
+    // it is the exit axis, bit 16 + axis set when d > 0 (the box's exit plane
+    // is its upper face).
+    uint32_t signs;
     // The box of the last step: its exit planes, and the voxel position
     // shifted by the level it was found at (4 region, 2 brick, 0 voxel). A
     // step whose voxel has the same key looks up the same box, so it reuses
@@ -437,6 +451,42 @@ struct RayRun {
     uint32_t shift;  // kNoIndex: no box cached
     uint32_t hit;    // 0, or 1 + the index of the ray's full hit record
 };
+
+__device__ __forceinline__ V3 decode_normal(uint32_t code) {
+    return V3{axis_value(code & 3u), axis_value((code >> 2) & 3u), axis_value((code >> 4) & 3u)};
+}
+
+__device__ __forceinline__ uint32_t direction_signs(V3 d) {
+    const uint32_t px = d.x > 0.0f ? 1u : 0u, py = d.y > 0.0f ? 1u : 0u, pz = d.z > 0.0f ? 1u : 0u;
+    const uint32_t zeros = px | (py << 2) | (pz << 4);
+    const uint32_t exits = (px ? 3u : 2u) | ((py ? 3u : 2u) << 2) | ((pz ? 3u : 2u) << 4);
+    return zeros | (exits << 8) | (px << 16) | (py << 17) | (pz << 18);
+}
+
+__device__ __forceinline__ V3 traversal_recip(V3 d) {
+    const float nan = __uint_as_float(0x7fc00000u);
+    return V3{fabsf(d.x) > 1e-8f ? __frcp_rn(d.x) : nan, fabsf(d.y) > 1e-8f ? __frcp_rn(d.y) : nan,
+              fabsf(d.z) > 1e-8f ? __frcp_rn(d.z) : nan};
+}
+
+// advance_box's step from the box's exit planes (voxel_traversal.wgsl:90-107,
+// as advance_planes): returns the distance to move and sets the normal's
+// code. Every float operation is advance_planes'.
+__device__ __forceinline__ float step_planes(V3 p, V3 d, V3 inv, V3 plane, uint32_t signs, uint32_t& ncode) {
+    const float rx = div_recip(__fsub_rn(plane.x, p.x), d.x, inv.x);
+    const float ry = div_recip(__fsub_rn(plane.y, p.y), d.y, inv.y);
+    const float rz = div_recip(__fsub_rn(plane.z, p.z), d.z, inv.z);
+    const float tx = (rx >= -0.001f && rx < 1e30f) ? rx : 1e30f;
+    const float ty = (ry >= -0.001f && ry < 1e30f) ? ry : 1e30f;
+    const float tz = (rz >= -0.001f && rz < 1e30f) ? rz : 1e30f;
+    const bool choose_y = ty < wmax(tx, 0.0f);
+    const float dxy = wmax(choose_y ? ty : tx, 0.0f);
+    const bool choose_z = tz < dxy;
+    const float dist = wmax(choose_z ? tz : dxy, 0.0f);
+    const uint32_t mask = choose_z ? (3u << 4) : (choose_y ? (3u << 2) : 3u);
+    ncode = dist < 1e30f ? (((signs & ~mask) | ((signs >> 8) & mask)) & 63u) : 0u;
+    return wmax(__fadd_rn(dist, 0.001f), 0.001f);
+}
 
 template <bool BUDGETED>
 __device__ __forceinline__ void finish_ray(const WaveArgs& W, RayRun& s, uint32_t status, uint32_t material, I3 voxel, V3 position, V3 normal) {
@@ -460,17 +510,19 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
     s.slot = slot;
     s.hit = bits(rd.w);
     s.dir = V3{rd.x, rd.y, rd.z};
-    s.inv = direction_recip(s.dir);
+    s.inv = traversal_recip(s.dir);
+    s.signs = direction_signs(s.dir);
     s.maxd = ro.w;
     cnt.ray();
     const V3 origin{ro.x, ro.y, ro.z}, dir = s.dir;
     float nearv = -1e30f, farv = 1e30f;
-    V3 normal{0.0f, 0.0f, 0.0f};
+    uint32_t ncode = 0u;
     const float mnx = __fmul_rn((float)A.mn[0], 16.0f), mny = __fmul_rn((float)A.mn[1], 16.0f), mnz = __fmul_rn((float)A.mn[2], 16.0f);
     const float mxx = __fmul_rn((float)(A.mx[0] + 1), 16.0f), mxy = __fmul_rn((float)(A.mx[1] + 1), 16.0f),
                 mxz = __fmul_rn((float)(A.mx[2] + 1), 16.0f);
     const I3 zi{0, 0, 0};
     const V3 zv{0.0f, 0.0f, 0.0f};
+    // The slab normal: one axis -1 or +1, the others +0.
 #define VGI_SLAB(AX, O, D, Y, MN, MX)                                                   \
     if (fabsf(D) <= 1e-8f) {                                                            \
         if (O < MN || O > MX) { cnt.status(0); finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv); return; } \
@@ -479,8 +531,7 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
         float second = div_recip(__fsub_rn(MX, O), D, Y);                               \
         if (wmin(first, second) > nearv) {                                              \
             nearv = wmin(first, second);                                                \
-            float sg = first < second ? -1.0f : 1.0f;                                   \
-            normal = V3{AX == 0 ? sg : 0.0f, AX == 1 ? sg : 0.0f, AX == 2 ? sg : 0.0f}; \
+            ncode = (first < second ? 3u : 2u) << (2 * AX);                             \
         }                                                                               \
         farv = wmin(farv, wmax(first, second));                                         \
     }
@@ -495,20 +546,13 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
     }
     s.dist = __fadd_rn(wmax(nearv, 0.0f), 0.001f);
     s.pos = origin + dir * s.dist;
-    s.nrm = normal;
+    s.ncode = ncode;
     s.lrx = s.lry = s.lrz = 0x7fffffff;
     s.meta = make_uint4(0, 0, 0, 0);
     s.shift = kNoIndex;
     s.step = 0;
 }
 
-// One iteration of trace_domain_limited's loop (voxel_traversal.wgsl:152-213),
-// including the out-of-steps exit (:214-218). The branches only decide the
-// outcome: either the ray ends (one finish below) or it skips a box, whose
-// cell, extents and size they choose for the single box step. The lanes of a
-// warp take different branches, but none of them runs the box step on its
-// own. A step inside the box of the previous step skips the lookups (see
-// RayRun) and counts the words the lookup would have read.
 // Steps of a ray that grazes a face of its box. If some moving axis's exit
 // distance lies in [-0.001, 0] and adding dir * 0.001 cannot change that
 // coordinate (the move rounds away), then every later step in the same box
@@ -549,122 +593,11 @@ __device__ __forceinline__ void creep(const TraceArgs& A, RayRun& s, Cnt<C>& cnt
         s.pos = s.pos + c;
         s.step += 1u;
     }
-    if (ran) {
-        const float4 a = advance_planes(last, s.dir, s.inv, s.plane);
-        s.nrm = V3{a.x, a.y, a.z};
-    }
+    if (ran) step_planes(last, s.dir, s.inv, s.plane, s.signs, s.ncode);
 }
 
 constexpr uint32_t kGo = 0xffffffffu;
 
-#ifdef VGI_BRANCHED_STEP
-
-// The first half of a step: everything up to the box step. It leaves `status`
-// at kGo when the ray skips the box in s.plane, or sets the ray's outcome.
-template <bool BUDGETED, bool C>
-__device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<C>& cnt, uint32_t& status, uint32_t& material, I3& voxel) {
-    const TraceArgs& A = W.t;
-    if (s.step >= A.path_steps) {
-        status = 2u;
-        material = 0xffffffffu;
-    } else {
-        cnt.step();
-        voxel = I3{f2i(floorf(s.pos.x)), f2i(floorf(s.pos.y)), f2i(floorf(s.pos.z))};
-        const int rx = voxel.x >> 4, ry = voxel.y >> 4, rz = voxel.z >> 4;
-        const bool same = s.shift != kNoIndex && (voxel.x >> s.shift) == s.kx && (voxel.y >> s.shift) == s.ky &&
-                          (voxel.z >> s.shift) == s.kz;
-        if (same) {
-            // Same region (so in bounds), same brick or voxel: the same box.
-            if (s.dist > s.maxd) status = 0u;
-            else cnt.tbytes(s.shift == 4u ? 0u : (s.shift == 2u ? 4u : 8u));
-        } else if (s.dist > s.maxd || !in_bounds(A, rx, ry, rz)) {
-            status = 0u;
-        } else {
-            I3 cell{0, 0, 0}, ng{0, 0, 0}, ps{0, 0, 0};
-            float size = 16.0f;
-            uint32_t shift = 4u;
-            bool missing = false;
-            if (s.lrx != rx || s.lry != ry || s.lrz != rz) {
-                // The timed pass reads the dense grid (the same answer as the
-                // probe); the counting pass probes, to count its words.
-                const uint32_t index =
-                    (!C && A.region_grid)
-                        ? (uint32_t)__ldg(A.region_grid + ((size_t)(rz - A.mn[2]) * (uint32_t)(A.mx[1] - A.mn[1] + 1) + (uint32_t)(ry - A.mn[1])) *
-                                                              (uint32_t)(A.mx[0] - A.mn[0] + 1) +
-                                          (uint32_t)(rx - A.mn[0]))
-                        : lookup_region(A, rx, ry, rz, cnt);
-                if (index == kNoIndex) {
-                    missing = true;
-                } else {
-                    cnt.tbytes(16);
-                    s.meta = __ldg(A.headers + index);
-                    s.lrx = rx;
-                    s.lry = ry;
-                    s.lrz = rz;
-                }
-            }
-            cell = I3{rx, ry, rz};
-            if (missing) {
-                // visible_geometry crosses a missing region; otherwise the ray
-                // ends as unknown or escaped by geometry_ahead.
-                if (!BUDGETED) status = geometry_ahead(A, s.pos, s.dir, s.inv, __fsub_rn(s.maxd, s.dist), cnt) ? 2u : 0u;
-                shift = kNoIndex;
-            } else if (s.meta.x == 1u) {
-                ng = unpack_bytes(s.meta.z);
-                ps = unpack_bytes(s.meta.w);
-            } else if (s.meta.x != 3u) {
-                status = 1u;
-                material = s.meta.y;
-            } else {
-                const uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
-                const uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
-                const uint32_t brick = __ldg(A.cells + s.meta.y + (bz * 4u + by) * 4u + bx);
-                cnt.tbytes(4);
-                const uint32_t state = brick & 3u;
-                if (state == 0u) {
-                    const uint32_t ext = brick >> 2u;
-                    cell = I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz};
-                    ng = neg_ext(ext);
-                    ps = pos_ext(ext);
-                    size = 4.0f;
-                    shift = 2u;
-                } else if (state == 1u) {
-                    status = 1u;
-                    material = brick >> 2u;
-                } else {
-                    const uint32_t idx = ((lz & 3u) * 4u + (ly & 3u)) * 4u + (lx & 3u);
-                    const uint32_t word = __ldg(A.cells + (brick >> 2u) + (idx >> 1));
-                    cnt.tbytes(4);
-                    const uint32_t c = (word >> ((idx & 1u) * 16u)) & 65535u;
-                    if ((c & 1u) != 0u) {
-                        status = 1u;
-                        material = c >> 1u;
-                    } else {
-                        const uint32_t ext = c >> 1u;
-                        cell = voxel;
-                        ng = neg_ext(ext);
-                        ps = pos_ext(ext);
-                        size = 1.0f;
-                        shift = 0u;
-                    }
-                }
-            }
-            if (status == kGo) {
-                // A missing region crossed under the budget rule is looked up
-                // again at every step, so its box is not kept.
-                s.plane = box_planes(s.dir, cell, ng, ps, size);
-                s.shift = shift;
-                if (shift != kNoIndex) {
-                    s.kx = voxel.x >> shift;
-                    s.ky = voxel.y >> shift;
-                    s.kz = voxel.z >> shift;
-                }
-            }
-        }
-    }
-}
-
-#else
 // The first half of a step: everything up to the box step. It leaves `status`
 // at kGo when the ray skips the box in s.plane, or sets the ray's outcome.
 //
@@ -684,24 +617,26 @@ __device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<
     const bool same = s.shift != kNoIndex && (voxel.x >> s.shift) == s.kx && (voxel.y >> s.shift) == s.ky &&
                       (voxel.z >> s.shift) == s.kz;
     const bool beyond = s.dist > s.maxd;
-    const bool lookup = !out_of_steps && !same && !beyond && in_bounds(A, rx, ry, rz);
+    // The region's offset in the bounding box: inside when every axis is
+    // below the box's size (unsigned, so a region below the box wraps high).
+    const uint32_t nx = (uint32_t)(A.mx[0] - A.mn[0] + 1), ny = (uint32_t)(A.mx[1] - A.mn[1] + 1);
+    const uint32_t gx = (uint32_t)rx - (uint32_t)A.mn[0], gy = (uint32_t)ry - (uint32_t)A.mn[1], gz = (uint32_t)rz - (uint32_t)A.mn[2];
+    const bool inside = gx < nx && gy < ny && gz <= (uint32_t)(A.mx[2] - A.mn[2]);
+    const bool lookup = !out_of_steps && !same && !beyond && inside;
     if constexpr (C) {
         if (!out_of_steps) cnt.step();
         if (!out_of_steps && same && !beyond) cnt.tbytes(s.shift == 4u ? 0u : (s.shift == 2u ? 4u : 8u));
     }
-    // Region: the header of a region entered this step (the timed pass reads
-    // the dense grid, the counting pass probes the directory to count its
-    // words; both give lookup_region's answer).
-    // The timed pass reads the region's header straight from the dense
-    // header grid (kind 0 where the directory finds no region), one load.
+    // Region: the header of a region entered this step. The timed pass reads
+    // it straight from the dense header grid (kind 0 where the directory
+    // finds no region), one load; the counting pass probes the directory to
+    // count its words. Both give lookup_region's answer.
     const bool new_region = lookup && (s.lrx != rx || s.lry != ry || s.lrz != rz);
     bool missing = false;
     if (new_region) {
         uint4 h;
         if (!C && A.region_headers) {
-            h = __ldg(A.region_headers + ((size_t)(rz - A.mn[2]) * (uint32_t)(A.mx[1] - A.mn[1] + 1) + (uint32_t)(ry - A.mn[1])) *
-                                             (uint32_t)(A.mx[0] - A.mn[0] + 1) +
-                          (uint32_t)(rx - A.mn[0]));
+            h = __ldg(A.region_headers + (gz * ny + gy) * nx + gx);
             missing = h.x == 0u;
         } else {
             const uint32_t index = lookup_region(A, rx, ry, rz, cnt);
@@ -724,10 +659,9 @@ __device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<
     const bool solid_region = present && s.meta.x != 1u && s.meta.x != 3u;
     // Brick word of a mixed region, then the cell word of a mixed brick.
     const uint32_t lx = (uint32_t)(voxel.x & 15), ly = (uint32_t)(voxel.y & 15), lz = (uint32_t)(voxel.z & 15);
-    const uint32_t bx = lx >> 2, by = ly >> 2, bz = lz >> 2;
     uint32_t brick = 0u;
     if (mixed) {
-        brick = __ldg(A.cells + s.meta.y + (bz * 4u + by) * 4u + bx);
+        brick = __ldg(A.cells + s.meta.y + ((lz >> 2) * 4u + (ly >> 2)) * 4u + (lx >> 2));
         cnt.tbytes(4);
     }
     const bool empty_brick = mixed && (brick & 3u) == 0u;
@@ -763,19 +697,31 @@ __device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<
         // The box the ray skips: the region's top-level box (an air region;
         // a missing region crossed under the budget rule, without extents and
         // not kept, since it is looked up again every step), the brick's box
-        // (an empty brick) or the voxel's box (an air cell).
+        // (an empty brick) or the voxel's box (an air cell). Its cell is the
+        // voxel shifted by the level (voxel >> 4 is the region, voxel >> 2
+        // the brick), and each axis needs one face: the upper one,
+        // (cell + pos + 1) * size, when the ray moves up the axis, else the
+        // lower one, (cell - neg) * size, as box_planes picks them.
         const bool region_box = air_region || missing;
-        const uint32_t e = empty_brick ? (brick >> 2u) : (c >> 1u);
-        I3 ng = neg_ext(e), ps = pos_ext(e);
-        if (air_region) {
-            ng = unpack_bytes(s.meta.z);
-            ps = unpack_bytes(s.meta.w);
-        }
-        if (missing) ng = ps = I3{0, 0, 0};
-        const I3 cell = region_box ? I3{rx, ry, rz} : (empty_brick ? I3{rx * 4 + (int)bx, ry * 4 + (int)by, rz * 4 + (int)bz} : voxel);
+        const uint32_t level = region_box ? 4u : (empty_brick ? 2u : 0u);
         const float size = region_box ? 16.0f : (empty_brick ? 4.0f : 1.0f);
-        const uint32_t shift = missing ? kNoIndex : (air_region ? 4u : (empty_brick ? 2u : 0u));
-        s.plane = box_planes(s.dir, cell, ng, ps, size);
+        const uint32_t e = empty_brick ? (brick >> 2u) : (c >> 1u);
+        int face[3];
+        const int v[3] = {voxel.x, voxel.y, voxel.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const bool up = (s.signs >> (16 + a)) & 1u;
+            // Extents: a byte of the header's neg/pos word (air region), two
+            // bits of the brick or cell word (neg at 4a, pos at 4a + 2), none
+            // (missing region).
+            const uint32_t region_ext = ((up ? s.meta.w : s.meta.z) >> (8 * a)) & 255u;
+            const uint32_t cell_ext = (e >> (4 * a + (up ? 2 : 0))) & 3u;
+            const int ext = missing ? 0 : (int)(air_region ? region_ext : cell_ext);
+            const int cell = v[a] >> level;
+            face[a] = up ? cell + ext + 1 : cell - ext;
+        }
+        s.plane = V3{__fmul_rn((float)face[0], size), __fmul_rn((float)face[1], size), __fmul_rn((float)face[2], size)};
+        const uint32_t shift = missing ? kNoIndex : level;
         s.shift = shift;
         if (shift != kNoIndex) {
             s.kx = voxel.x >> shift;
@@ -784,7 +730,6 @@ __device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<
         }
     }
 }
-#endif
 
 // The second half: the ray ends with its outcome, or takes the box step.
 template <bool BUDGETED, bool C>
@@ -794,15 +739,14 @@ __device__ __forceinline__ void finish_step(const WaveArgs& W, RayRun& s, Cnt<C>
         cnt.status(status);
         const bool hit = status == 1u;
         const V3 zv{0.0f, 0.0f, 0.0f};
-        finish_ray<BUDGETED>(W, s, status, material, hit ? voxel : I3{0, 0, 0}, hit ? s.pos : zv, hit ? s.nrm : zv);
+        finish_ray<BUDGETED>(W, s, status, material, hit ? voxel : I3{0, 0, 0}, hit ? s.pos : zv, hit ? decode_normal(s.ncode) : zv);
         return;
     }
-    const float4 adv = advance_planes(s.pos, s.dir, s.inv, s.plane);
-    s.dist = __fadd_rn(s.dist, adv.w);
-    s.pos = s.pos + s.dir * adv.w;
-    s.nrm = V3{adv.x, adv.y, adv.z};
+    const float w = step_planes(s.pos, s.dir, s.inv, s.plane, s.signs, s.ncode);
+    s.dist = __fadd_rn(s.dist, w);
+    s.pos = s.pos + s.dir * w;
     s.step += 1u;
-    if (adv.w == 0.001f && s.shift != kNoIndex) creep<C>(W.t, s, cnt, creep_limit);
+    if (w == 0.001f && s.shift != kNoIndex) creep<C>(W.t, s, cnt, creep_limit);
 }
 
 // trace() (voxel_path.wgsl:239-243) for every queued ray. Persistent warps
