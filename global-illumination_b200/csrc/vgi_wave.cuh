@@ -501,8 +501,47 @@ __device__ __forceinline__ void finish_ray(const WaveArgs& W, RayRun& s, uint32_
     s.slot = kNoIndex;
 }
 
-// trace_domain_limited's set-up (voxel_traversal.wgsl:127-151): the slab
-// clip against the scene bounds. A ray that misses finishes at once.
+// trace_domain_limited's slab clip (voxel_traversal.wgsl:127-151) of a ray
+// against the scene bounds: the near and far distances, whether an axis that
+// does not move lies outside the bounds, and the nearest slab's normal code
+// (one axis -1, code 3, or +1, code 2; the others +0).
+__device__ __forceinline__ uint32_t slab_clip(const TraceArgs& A, V3 origin, V3 dir, V3 inv, float& nearv, float& farv, bool& miss) {
+    nearv = -1e30f;
+    farv = 1e30f;
+    miss = false;
+    uint32_t ncode = 0u;
+    const float mnx = __fmul_rn((float)A.mn[0], 16.0f), mny = __fmul_rn((float)A.mn[1], 16.0f), mnz = __fmul_rn((float)A.mn[2], 16.0f);
+    const float mxx = __fmul_rn((float)(A.mx[0] + 1), 16.0f), mxy = __fmul_rn((float)(A.mx[1] + 1), 16.0f),
+                mxz = __fmul_rn((float)(A.mx[2] + 1), 16.0f);
+#define VGI_SLAB(AX, O, D, Y, MN, MX)                                  \
+    if (fabsf(D) <= 1e-8f) {                                           \
+        if (O < MN || O > MX) miss = true;                             \
+    } else {                                                           \
+        const float first = div_recip(__fsub_rn(MN, O), D, Y);         \
+        const float second = div_recip(__fsub_rn(MX, O), D, Y);        \
+        if (wmin(first, second) > nearv) {                             \
+            nearv = wmin(first, second);                               \
+            ncode = (first < second ? 3u : 2u) << (2 * AX);            \
+        }                                                              \
+        farv = wmin(farv, wmax(first, second));                        \
+    }
+    VGI_SLAB(0, origin.x, dir.x, inv.x, mnx, mxx)
+    VGI_SLAB(1, origin.y, dir.y, inv.y, mny, mxy)
+    VGI_SLAB(2, origin.z, dir.z, inv.z, mnz, mxz)
+#undef VGI_SLAB
+    return ncode;
+}
+
+// The normal code is the slab clip's and has not been formed yet (below).
+constexpr uint32_t kSlabPending = 1u << 31;
+
+// trace_domain_limited's set-up: the slab clip. A ray that misses finishes
+// at once. For an origin strictly inside the bounds on every axis the clip's
+// outcome needs no division: every moving axis has one negative and one
+// positive slab distance, so the near distance is negative, the far one
+// positive, nothing misses and the start distance is 0 + 0.001. Only the
+// slab normal needs the quotients, and only a ray that hits before its first
+// box step reports it, so that ray forms it when it ends (normal_code).
 template <bool BUDGETED, bool C>
 __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t slot, Cnt<C>& cnt) {
     const TraceArgs& A = W.t;
@@ -514,43 +553,41 @@ __device__ __forceinline__ void start_ray(const WaveArgs& W, RayRun& s, uint32_t
     s.signs = direction_signs(s.dir);
     s.maxd = ro.w;
     cnt.ray();
-    const V3 origin{ro.x, ro.y, ro.z}, dir = s.dir;
-    float nearv = -1e30f, farv = 1e30f;
-    uint32_t ncode = 0u;
-    const float mnx = __fmul_rn((float)A.mn[0], 16.0f), mny = __fmul_rn((float)A.mn[1], 16.0f), mnz = __fmul_rn((float)A.mn[2], 16.0f);
-    const float mxx = __fmul_rn((float)(A.mx[0] + 1), 16.0f), mxy = __fmul_rn((float)(A.mx[1] + 1), 16.0f),
-                mxz = __fmul_rn((float)(A.mx[2] + 1), 16.0f);
-    const I3 zi{0, 0, 0};
-    const V3 zv{0.0f, 0.0f, 0.0f};
-    // The slab normal: one axis -1 or +1, the others +0.
-#define VGI_SLAB(AX, O, D, Y, MN, MX)                                                   \
-    if (fabsf(D) <= 1e-8f) {                                                            \
-        if (O < MN || O > MX) { cnt.status(0); finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv); return; } \
-    } else {                                                                            \
-        float first = div_recip(__fsub_rn(MN, O), D, Y);                                \
-        float second = div_recip(__fsub_rn(MX, O), D, Y);                               \
-        if (wmin(first, second) > nearv) {                                              \
-            nearv = wmin(first, second);                                                \
-            ncode = (first < second ? 3u : 2u) << (2 * AX);                             \
-        }                                                                               \
-        farv = wmin(farv, wmax(first, second));                                         \
+    const V3 origin{ro.x, ro.y, ro.z};
+    const bool inside = origin.x > __fmul_rn((float)A.mn[0], 16.0f) && origin.x < __fmul_rn((float)(A.mx[0] + 1), 16.0f) &&
+                        origin.y > __fmul_rn((float)A.mn[1], 16.0f) && origin.y < __fmul_rn((float)(A.mx[1] + 1), 16.0f) &&
+                        origin.z > __fmul_rn((float)A.mn[2], 16.0f) && origin.z < __fmul_rn((float)(A.mx[2] + 1), 16.0f);
+    if (inside) {
+        s.dist = 0.001f;
+        s.ncode = kSlabPending;
+    } else {
+        float nearv, farv;
+        bool miss;
+        const uint32_t ncode = slab_clip(A, origin, s.dir, s.inv, nearv, farv, miss);
+        if (miss || farv < wmax(nearv, 0.0f)) {
+            cnt.status(0);
+            const I3 zi{0, 0, 0};
+            const V3 zv{0.0f, 0.0f, 0.0f};
+            finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv);
+            return;
+        }
+        s.dist = __fadd_rn(wmax(nearv, 0.0f), 0.001f);
+        s.ncode = ncode;
     }
-    VGI_SLAB(0, origin.x, dir.x, s.inv.x, mnx, mxx)
-    VGI_SLAB(1, origin.y, dir.y, s.inv.y, mny, mxy)
-    VGI_SLAB(2, origin.z, dir.z, s.inv.z, mnz, mxz)
-#undef VGI_SLAB
-    if (farv < wmax(nearv, 0.0f)) {
-        cnt.status(0);
-        finish_ray<BUDGETED>(W, s, 0u, 0u, zi, zv, zv);
-        return;
-    }
-    s.dist = __fadd_rn(wmax(nearv, 0.0f), 0.001f);
-    s.pos = origin + dir * s.dist;
-    s.ncode = ncode;
+    s.pos = origin + s.dir * s.dist;
     s.lrx = s.lry = s.lrz = 0x7fffffff;
     s.meta = make_uint4(0, 0, 0, 0);
     s.shift = kNoIndex;
     s.step = 0;
+}
+
+// The ray's normal code, forming the slab clip's when it is still pending.
+__device__ __forceinline__ uint32_t normal_code(const WaveArgs& W, const RayRun& s) {
+    if (!(s.ncode & kSlabPending)) return s.ncode;
+    const float4 ro = W.ray[2u * s.slot];
+    float nearv, farv;
+    bool miss;
+    return slab_clip(W.t, V3{ro.x, ro.y, ro.z}, s.dir, s.inv, nearv, farv, miss);
 }
 
 // Steps of a ray that grazes a face of its box. If some moving axis's exit
@@ -739,7 +776,7 @@ __device__ __forceinline__ void finish_step(const WaveArgs& W, RayRun& s, Cnt<C>
         cnt.status(status);
         const bool hit = status == 1u;
         const V3 zv{0.0f, 0.0f, 0.0f};
-        finish_ray<BUDGETED>(W, s, status, material, hit ? voxel : I3{0, 0, 0}, hit ? s.pos : zv, hit ? decode_normal(s.ncode) : zv);
+        finish_ray<BUDGETED>(W, s, status, material, hit ? voxel : I3{0, 0, 0}, hit ? s.pos : zv, hit ? decode_normal(normal_code(W, s)) : zv);
         return;
     }
     const float w = step_planes(s.pos, s.dir, s.inv, s.plane, s.signs, s.ncode);
