@@ -24,6 +24,9 @@ side) both as separate per-scene frames and as batched frames (one
 traversal launch per stage over all scenes), from the same empty caches.
 ``next_rows`` times headless discovery, a far-tier frame and the view
 receivers' frame, reconstruction and presentation at 1920x1080.
+``stone_room`` runs the reference's stone-room fixture (32^3, 4 spp, 1 hit,
+64 steps, history 64) for 64 frames on the GPU and on the oracle, timed in
+full, and compares the final results and state word for word.
 ``--impl reference`` times the CPU oracle (the restatement of the
 reference's algorithm; the reference itself is Rust/WGSL and has no CPU
 path) on the box's host cores.
@@ -418,6 +421,96 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+ROOM_SPP, ROOM_FRAMES = 4, 64
+
+
+def stone_room_run(local, stream):
+    """The reference's stone-room fixture, run in full: the 32^3 room
+    (8 regions) with its stone and emissive materials, every exposed face a
+    world-cache slot, 4 paths a face a frame, 1 diffuse hit, 64 traversal
+    steps, history 64, for 64 frames from an empty cache. The GPU runs them
+    graph-replayed (CUDA events around all 64); the oracle runs the same 64
+    frames on all host threads; the two final result and state arrays are
+    compared word for word. Rays and paths per frame come from a counting
+    pass before each frame (the counting pass changes no state)."""
+    import torch
+
+    import vgi
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    coords, vox = vgi.stone_room()
+    m = vgi.VoxelGiMaterials()
+    m.set(0, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5)))
+    m.set(1, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5), emission=(8.0, 4.0, 1.5)))
+    words = m.words()
+    transport = vgi.TransportSettings(bounces=1, path_steps=64, history_limit=64)
+    faces = vgi.exposed_faces(coords, vox)
+    g = vgi.GpuTracer(local)
+    g.upload_regions(coords, vox)
+    g.set_materials(words)
+    g.set_lights(np.zeros(0, np.float32), 0)
+    g.set_environment((0.0, 0.0, 0.0))
+    g.build_emitters()
+    g.set_transport(transport)
+    g.set_faces(faces)
+    geometry = g.geometry()
+    # Work per frame (the counting pass), then the frames themselves.
+    rays = paths = 0
+    shadow = vgi.GpuTracer(local)
+    shadow.upload_regions(coords, vox)
+    shadow.set_materials(words)
+    shadow.set_lights(np.zeros(0, np.float32), 0)
+    shadow.set_environment((0.0, 0.0, 0.0))
+    shadow.build_emitters()
+    shadow.set_transport(transport)
+    shadow.set_faces(faces)
+    for f in range(ROOM_FRAMES):
+        c = shadow.census(ROOM_SPP)
+        rays += c["rays"]
+        paths += c["paths"]
+        shadow.frame(ROOM_SPP, 16 * f)
+    shadow.close()
+    g.set_graph(True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for f in range(ROOM_FRAMES):
+        g.frame(ROOM_SPP, 16 * f)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    gpu_ms = ev[0].elapsed_time(ev[1])
+    g.set_graph(False)
+    got_results, got_state = g.read_results(), g.read_state()
+    g.close()
+
+    emitters, n_emit, total = vgi.host_emitters(coords, vox, words)
+
+    def params(n, samples):
+        return O.params_words(n, samples, geometry[0].size // 4, 0, geometry[3], 0, (0, 0, 0), total, n_emit)
+
+    threads = os.cpu_count() or 1
+    ref = O.Frames(geometry, params, words, np.zeros(0, np.float32), emitters, faces, transport, O.Pipeline(1, 0, 64, 0, ROOM_SPP),
+                   threads=threads)
+    t0 = time.perf_counter()
+    for f in range(ROOM_FRAMES):
+        ref.frame(ROOM_SPP, 16 * f)
+    cpu_s = time.perf_counter() - t0
+    differ = int((got_results != ref.results).sum() + (got_state != ref.state).sum())
+    return {
+        "workload": f"stone room 32^3 (8 regions), {faces.shape[0]} faces, {ROOM_SPP} spp, 1 bounce, 64 steps, history 64, "
+                    f"{ROOM_FRAMES} frames from an empty cache",
+        "frames": ROOM_FRAMES, "rays": int(rays), "paths": int(paths),
+        "gpu": {"ms_per_frame": gpu_ms / ROOM_FRAMES, "rays_per_s": rays / (gpu_ms * 1e-3), "paths_per_s": paths / (gpu_ms * 1e-3),
+                "timing": "CUDA events around all frames, graph-replayed"},
+        "cpu_oracle": {"ms_per_frame": 1000.0 * cpu_s / ROOM_FRAMES, "rays_per_s": rays / cpu_s, "paths_per_s": paths / cpu_s,
+                       "threads": threads},
+        "parity": {"words": int(got_results.size + got_state.size), "words_differ": differ,
+                   "how": "final face results and resident state after all frames, GPU vs oracle"},
+    }
+
+
 def make_batch_scenes(n, seed0=100):
     """Seeded scenes of uneven size for the batched form: the terrain
     generator with 2..16 regions (32..256 voxels) per axis drawn uniformly,
@@ -725,6 +818,7 @@ def main():
     ap.add_argument("--profile-mlp", action="store_true", help="only a small MLP cache workload, for ncu captures")
     ap.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-scene comparison (0: skip it)")
     ap.add_argument("--no-next-rows", action="store_true", help="skip discovery, far tier and reconstruction timings")
+    ap.add_argument("--no-room", action="store_true", help="skip the stone-room run (64 frames on the GPU and the oracle)")
     ap.add_argument("--profile-next", action="store_true", help="only the next-row workload once, for ncu captures")
     ap.add_argument("--profile-frame", action="store_true", help="only plain frames of the terrain, for ncu captures")
     ap.add_argument("--small", action="store_true", help="with --profile-next or --profile-frame: the 256x128x256 terrain")
@@ -892,6 +986,7 @@ def main():
         if args.batch_scenes > 0:
             batched = batch_comparison(local, stream, flush, args.batch_scenes, args.steps, args.warmup)
         beside = None if args.no_next_rows else next_rows(g, stream)
+        room = None if args.no_room else stone_room_run(local, stream)
         line = {
             "metric": METRIC,
             "value": total_rays / (total_ms * 1e-3),
@@ -933,6 +1028,7 @@ def main():
             "mlp_cache": mlp,
             "batched_scenes": batched,
             "next_rows": beside,
+            "stone_room": room,
         }
         if base:
             line["cpu_baseline"] = base

@@ -2715,6 +2715,24 @@ int vgi_mlp_train(vgi_ctx* c, const float* features, const float* targets4, uint
     return mlp_read_status(c, loss);
 }
 
+int vgi_mlp_apply_gradients(vgi_ctx* c, const float* grads, float loss, float lr, int on_device) {
+    if (!c || !grads || !(lr > 0.0f)) return VGI_ERR_INVALID;
+    if (!c->mlp_image.ptr) return fail(c, VGI_ERR_STATE, "MLP weights are not set");
+    VGI_CUDA(c, cudaSetDevice(c->device));
+    // The gradient as one partial row (the loss after it), so the step is the
+    // Adam kernel's own over one row: a gradient from vgi_mlp_gradients gives
+    // the same step as vgi_mlp_train on that batch.
+    const uint32_t count = mlp_weight_count();
+    VGI_CUDA(c, cudaMemcpyAsync(c->mlp_partials.ptr, grads, (size_t)count * 4, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                c->stream));
+    VGI_CUDA(c, cudaMemcpyAsync(c->mlp_partials.ptr + count, &loss, 4, cudaMemcpyHostToDevice, c->stream));
+    launch_mlp_adam(c->mlp_master.ptr, c->mlp_adam.ptr, c->mlp_adam.ptr + count, c->mlp_partials.ptr, 1u, lr, 0.9f, 0.99f, 1e-8f,
+                    c->mlp_steps.ptr, c->mlp_image.ptr, c->mlp_image_b.ptr, c->mlp_grads.ptr + count, c->stream);
+    VGI_CUDA(c, cudaGetLastError());
+    VGI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return VGI_OK;
+}
+
 int vgi_read_events(vgi_ctx* c, uint32_t* words, uint64_t n_words) {
     if (!c || (n_words && !words) || n_words > c->n_events_read * 4) return VGI_ERR_INVALID;
     if (n_words) VGI_CUDA(c, cudaMemcpyAsync(words, c->events.ptr, n_words * 4, cudaMemcpyDeviceToHost, c->stream));

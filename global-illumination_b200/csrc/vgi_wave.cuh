@@ -442,10 +442,10 @@ struct RayRun {
     // is its upper face).
     uint32_t signs;
     // The box of the last step: its exit planes, and the voxel position
-    // shifted by the level it was found at (4 region, 2 brick, 0 voxel). A
-    // step whose voxel has the same key looks up the same box, so it reuses
-    // the planes. Rays that graze a face, where the move across the face is
-    // lost to rounding, take up to the step budget inside one box this way.
+    // shifted by the level it was found at (4 region, 2 brick, 0 voxel).
+    // While the voxel keeps this key the lookup would find the same box:
+    // creep replays the steps of a ray that grazes a face, where the move
+    // across the face is lost to rounding, inside one box this way.
     V3 plane;
     int kx, ky, kz;
     uint32_t shift;  // kNoIndex: no box cached
@@ -651,18 +651,15 @@ __device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<
     const bool out_of_steps = s.step >= A.path_steps;
     voxel = I3{f2i(floorf(s.pos.x)), f2i(floorf(s.pos.y)), f2i(floorf(s.pos.z))};
     const int rx = voxel.x >> 4, ry = voxel.y >> 4, rz = voxel.z >> 4;
-    const bool same = s.shift != kNoIndex && (voxel.x >> s.shift) == s.kx && (voxel.y >> s.shift) == s.ky &&
-                      (voxel.z >> s.shift) == s.kz;
     const bool beyond = s.dist > s.maxd;
     // The region's offset in the bounding box: inside when every axis is
     // below the box's size (unsigned, so a region below the box wraps high).
     const uint32_t nx = (uint32_t)(A.mx[0] - A.mn[0] + 1), ny = (uint32_t)(A.mx[1] - A.mn[1] + 1);
     const uint32_t gx = (uint32_t)rx - (uint32_t)A.mn[0], gy = (uint32_t)ry - (uint32_t)A.mn[1], gz = (uint32_t)rz - (uint32_t)A.mn[2];
     const bool inside = gx < nx && gy < ny && gz <= (uint32_t)(A.mx[2] - A.mn[2]);
-    const bool lookup = !out_of_steps && !same && !beyond && inside;
+    const bool lookup = !out_of_steps && !beyond && inside;
     if constexpr (C) {
         if (!out_of_steps) cnt.step();
-        if (!out_of_steps && same && !beyond) cnt.tbytes(s.shift == 4u ? 0u : (s.shift == 2u ? 4u : 8u));
     }
     // Region: the header of a region entered this step. The timed pass reads
     // it straight from the dense header grid (kind 0 where the directory
@@ -717,8 +714,6 @@ __device__ __forceinline__ void classify_step(const WaveArgs& W, RayRun& s, Cnt<
     if (out_of_steps) {
         status = 2u;
         material = 0xffffffffu;
-    } else if (same) {
-        if (beyond) status = 0u;
     } else if (!lookup) {
         status = 0u;
     } else if (solid_region || solid_brick || solid_cell) {

@@ -261,6 +261,7 @@ _SIGNATURES = {
     "vgi_mlp_forward": (_INT, [_P, _P, _U32, _P]),
     "vgi_mlp_gradients": (_INT, [_P, _P, _P, _U32, _P, _P]),
     "vgi_mlp_train": (_INT, [_P, _P, _P, _U32, ctypes.c_float, _P]),
+    "vgi_mlp_apply_gradients": (_INT, [_P, _P, ctypes.c_float, ctypes.c_float, _INT]),
     "vgi_mlp_encode": (_INT, [_P, _P, _U32, _P]),
     "vgi_set_mlp_cache": (_INT, [_P, ctypes.c_int, _U32, _U32, _U32, ctypes.c_float]),
     "vgi_mlp_stats": (_INT, [_P, _P]),
@@ -742,6 +743,17 @@ class GpuTracer:
         loss = np.zeros(1, np.float32)
         self._check(self._lib.vgi_mlp_train(self._h, _ptr(f), _ptr(y), f.shape[0], float(lr), _ptr(loss)))
         return float(loss[0])
+
+    def mlp_apply_gradients(self, grads, loss: float = 0.0, lr: float = 1e-2) -> None:
+        """One Adam step from a given gradient (a host array, or a CUDA tensor
+        on this context's device)."""
+        if hasattr(grads, "data_ptr"):
+            assert grads.numel() == self.MLP_WEIGHTS and grads.is_contiguous()
+            self._check(self._lib.vgi_mlp_apply_gradients(self._h, ctypes.c_void_p(grads.data_ptr()), float(loss), float(lr), 1))
+        else:
+            g = _c(grads, np.float32).reshape(-1)
+            assert g.size == self.MLP_WEIGHTS
+            self._check(self._lib.vgi_mlp_apply_gradients(self._h, _ptr(g), float(loss), float(lr), 0))
 
     def mlp_encode(self, faces: np.ndarray) -> np.ndarray:
         """The network's inputs (n x 96) for face rows (voxel xyz, face, material)."""

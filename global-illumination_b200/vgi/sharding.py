@@ -85,14 +85,59 @@ class FaceShards:
 
         device = torch.device("cuda", torch.cuda.current_device())
         stream = torch.cuda.ExternalStream(self.tracer.stream, device=device)
+        if getattr(self, "_send", None) is None:
+            # Kept for the life of the shards, so no frame waits on the host
+            # for the copies out of them: every use is ordered on the
+            # tracer's stream (the collective waits for it and it waits for
+            # the collective).
+            self._send = torch.zeros((self.size, 4), dtype=torch.int32, device=device)
+            self._full = torch.empty((self.world * self.size, 4), dtype=torch.int32, device=device)
         with torch.cuda.stream(stream):
-            send = torch.zeros((self.size, 4), dtype=torch.int32, device=device)
             if self.count:
-                self.tracer.read_cache_device(self.first, self.count, send.data_ptr())
-            full = torch.empty((self.world * self.size, 4), dtype=torch.int32, device=device)
-            self.dist.all_gather_into_tensor(full, send, group=self.group)
+                self.tracer.read_cache_device(self.first, self.count, self._send.data_ptr())
+            self.dist.all_gather_into_tensor(self._full, self._send, group=self.group)
             for r, (first, count, size) in enumerate(self.ranges):
                 if r != self.rank and count:
-                    self.tracer.write_cache_device(first, count, full[r * size].data_ptr())
-            # The tensors are released only after the copies have read them.
-            stream.synchronize()
+                    self.tracer.write_cache_device(first, count, self._full[r * size].data_ptr())
+
+
+class MlpDataParallel:
+    """Data-parallel training of the MLP radiance cache: every rank computes
+    the gradient of the loss over its own rows (``mlp_gradients``), one
+    all-reduce averages the 19,456 gradients and the losses, and every rank
+    takes the same Adam step from the average (``mlp_apply_gradients``), so
+    the ranks' weights stay identical. With the NCCL backend the gradient
+    goes through a CUDA tensor; with gloo through a host tensor. Every rank
+    calls ``step`` in the same order with equally many rows."""
+
+    def __init__(self, tracer, group=None):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.tracer = tracer
+        self.group = group
+        self.world = dist.get_world_size(group)
+        self.on_device = dist.get_backend(group) == "nccl"
+
+    def step(self, features, targets, lr: float = 1e-2) -> float:
+        """One data-parallel Adam step over this rank's rows; returns the mean
+        loss over all ranks' rows (before the step)."""
+        import torch
+
+        grads, loss = self.tracer.mlp_gradients(features, targets)
+        buf = torch.from_numpy(np.concatenate([np.asarray(grads, np.float32).reshape(-1), np.float32([loss])]))
+        if not self.on_device:
+            self.dist.all_reduce(buf, group=self.group)
+            buf /= self.world
+            mean_loss = float(buf[-1])
+            self.tracer.mlp_apply_gradients(buf[:-1].numpy(), mean_loss, lr)
+            return mean_loss
+        # On the tracer's stream, so the step reads the reduced gradient.
+        device = torch.device("cuda", torch.cuda.current_device())
+        with torch.cuda.stream(torch.cuda.ExternalStream(self.tracer.stream, device=device)):
+            buf = buf.to(device)
+            self.dist.all_reduce(buf, group=self.group)
+            buf /= self.world
+            mean_loss = float(buf[-1])
+            self.tracer.mlp_apply_gradients(buf[:-1], mean_loss, lr)
+        return mean_loss

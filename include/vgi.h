@@ -352,6 +352,15 @@ int vgi_mlp_forward(vgi_ctx* ctx, const float* features, uint32_t n, float* out4
  * writes the loss before the step. vgi_mlp_set_weights resets Adam. */
 int vgi_mlp_gradients(vgi_ctx* ctx, const float* features, const float* targets4, uint32_t n, float* grads, float* loss);
 int vgi_mlp_train(vgi_ctx* ctx, const float* features, const float* targets4, uint32_t n, float lr, float* loss);
+/* One Adam step from a given gradient (19,456 floats, the master order; host
+ * memory, or device memory on the context's device when on_device != 0) and
+ * its loss, for data-parallel training: every rank takes vgi_mlp_gradients
+ * of its own rows, the ranks average the gradients (an all-reduce), and each
+ * applies the average here, so all ranks keep the same weights. The gradient
+ * of a batch from vgi_mlp_gradients gives the step vgi_mlp_train takes on
+ * that batch. No counterpart in the reference (it has no network).
+ * Synchronous. */
+int vgi_mlp_apply_gradients(vgi_ctx* ctx, const float* grads, float loss, float lr, int on_device);
 /* The network's 96 inputs for n faces (their voxel, face and material), as
  * the frame's queries and training rows compute them: per axis of the face
  * centre x (voxels, normalised to [0, 1] over the loaded regions), sin and

@@ -126,6 +126,28 @@ def test_mlp_adam_steps_match_numpy(gpu):
         w = got
 
 
+def test_mlp_apply_gradients_takes_the_train_step(gpu):
+    """The data-parallel step: the gradient of a batch (mlp_gradients)
+    applied with mlp_apply_gradients is the step mlp_train takes on that
+    batch, within the gradient sums' atomic noise; a CUDA tensor and a host
+    array of the same gradient give the same step exactly."""
+    master = random_weights(9)
+    features, targets = batch(2000, 4)
+    gpu.mlp_set_weights(master)
+    g, loss = gpu.mlp_gradients(features, targets)
+    gpu.mlp_apply_gradients(g, loss, 1e-2)
+    via_apply = gpu.mlp_get_weights()
+    gpu.mlp_set_weights(master)
+    gpu.mlp_train(features, targets, 1e-2)
+    via_train = gpu.mlp_get_weights()
+    diff = np.abs(via_apply - via_train)
+    assert diff[np.abs(g) > 1e-6].max() < 1e-4, diff.max()
+    assert np.mean(diff < 1e-4) > 0.999
+    gpu.mlp_set_weights(master)
+    gpu.mlp_apply_gradients(torch.tensor(g).cuda(), loss, 1e-2)
+    assert np.array_equal(gpu.mlp_get_weights(), via_apply)
+
+
 def test_mlp_training_fits_a_smooth_field(gpu):
     """65,536 rows (one frame's training batch) of a smooth radiance field:
     200 Adam steps at lr 1e-2 bring the loss down by more than 10x."""

@@ -80,3 +80,33 @@ def test_nccl_exchange_of_a_one_rank_group(gpu):
         assert_words_equal(gpu.read_state(), state, "one-rank shard state")
     finally:
         dist.destroy_process_group()
+
+
+def test_mlp_data_parallel_step_of_a_one_rank_group(gpu):
+    """MlpDataParallel through NCCL (device gradient, all-reduce on the
+    tracer's stream): a one-rank group's step is mlp_train's step, within the
+    gradient sums' atomic noise."""
+    import torch
+    import torch.distributed as dist
+
+    from test_gpu_mlp import batch, random_weights
+    from vgi.sharding import MlpDataParallel
+
+    master = random_weights(5)
+    features, targets = batch(3000, 8)
+    gpu.mlp_set_weights(master)
+    gpu.mlp_train(features, targets, 1e-2)
+    want = gpu.mlp_get_weights()
+    gpu.mlp_set_weights(master)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        dp = MlpDataParallel(gpu)
+        assert dp.on_device
+        loss = dp.step(features, targets, lr=1e-2)
+        assert np.isfinite(loss) and loss > 0.0
+        diff = np.abs(gpu.mlp_get_weights() - want)
+        assert np.mean(diff < 1e-4) > 0.999, diff.max()
+    finally:
+        dist.destroy_process_group()
