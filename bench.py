@@ -531,6 +531,37 @@ def make_batch_scenes(n, seed0=100):
     return out
 
 
+SPHERES_PER_FRAME = 32
+
+
+def sphere_edits(coords, faces, rng, mean=SPHERES_PER_FRAME):
+    """One frame of the batched workload's edit stream for a scene: a
+    Poisson(mean) number of spheres of radius 1..5 around surface voxels (the
+    voxels of random faces), each carving air or placing one of the 8
+    materials, half and half, and one measured retention event per sphere
+    box (vgi.encode_edit_events). Returns (edits x, y, z, value; event words;
+    event count; measure records)."""
+    import vgi
+
+    size = (coords.max(0) + 1) * 16
+    k = max(1, int(rng.poisson(mean)))
+    rows = faces[rng.integers(0, len(faces), k)]
+    edits, boxes = [], []
+    for row in rows:
+        c = row[:3].astype(np.int64)
+        r = int(rng.integers(1, 6))
+        value = 256 if rng.random() < 0.5 else int(rng.integers(0, 8))
+        g = np.arange(-r, r + 1)
+        off = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+        off = off[(off * off).sum(1) <= r * r]
+        p = c + off
+        p = p[np.all((p >= 0) & (p < size), axis=1)]
+        edits.append(np.column_stack([p, np.full(len(p), value)]))
+        boxes.append((np.maximum(c - r, 0), np.minimum(c + r, size - 1), len(p), 40.0))
+    words, n, measures = vgi.encode_edit_events(boxes)
+    return np.concatenate(edits).astype(np.int32), words, n, measures
+
+
 def batch_comparison(local, stream, flush, n_scenes, steps, warmup):
     """Batched scenes: the same frames of every scene three ways, each scene
     graph-replayed: one scene after another (serial, as the reference's
@@ -619,6 +650,28 @@ def batch_comparison(local, stream, flush, n_scenes, steps, warmup):
     batch.set_graph(True)
     warm_bat = timed(lambda clock: batch.frame(SPP, clock), warmup, 0)
     bat = timed(lambda clock: batch.frame(SPP, clock), steps, 16 * warmup)
+    # The workload's per-frame edit stream (made beforehand): before every
+    # batched frame each scene applies its sphere edits (vgi_edit_voxels:
+    # repack of the edited regions and the top-level update) and their
+    # measured retention events (vgi_apply_events_measured: the edit measure
+    # and the discount over the scene's slots). Host wall time, since the
+    # edit calls are synchronous.
+    erng = np.random.default_rng(31)
+    edit_stream = [[sphere_edits(coords, faces, erng) for coords, _, faces, _ in scenes] for _ in range(steps)]
+    spheres = int(np.mean([sum(int(n) for _, _, n, _ in frame) for frame in edit_stream]))
+    edit_ms, frame_ms = [], []
+    clock_e = 16 * (warmup + steps)
+    for f in range(steps):
+        t0 = time.perf_counter()
+        for t, (edits, words_e, n_ev, measures) in zip(tracers, edit_stream[f]):
+            t.edit_voxels(edits)
+            t.apply_events_measured(words_e, n_ev, measures)
+        t1 = time.perf_counter()
+        batch.frame(SPP, clock_e + 16 * f)
+        batch.sync()
+        t2 = time.perf_counter()
+        edit_ms.append(1000.0 * (t1 - t0))
+        frame_ms.append(1000.0 * (t2 - t1))
     batch.close()
     for t in tracers:
         t.close()
@@ -634,6 +687,9 @@ def batch_comparison(local, stream, flush, n_scenes, steps, warmup):
         "serial_rays_per_s": census / (ser_ms * 1e-3), "separate_rays_per_s": census / (sep_ms * 1e-3),
         "batched_rays_per_s": census / (bat_ms * 1e-3),
         "speedup_vs_serial": ser_ms / bat_ms, "speedup_vs_separate_streams": sep_ms / bat_ms, "autotune": tune,
+        "with_edits": {"spheres_per_frame": spheres, "radius": "1..5", "edit_ms_per_frame": float(np.mean(edit_ms)),
+                       "frame_ms": float(np.mean(frame_ms)), "total_ms_per_frame": float(np.mean(edit_ms) + np.mean(frame_ms)),
+                       "timing": "host wall time: every scene's edits and measured events, then the batched frame to completion"},
         "note": "rays per frame from a census after the warm-up frames; both runs trace identical frames from empty caches",
     }
 

@@ -2830,6 +2830,12 @@ struct vgi_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<cudaGraphNode_t> prepare_nodes, accumulate_nodes;
+    // Scenes in the MLP cache mode: whether this frame's paths end at the
+    // network, and the query launch's scene table (device and host copies).
+    bool mlp = false, graph_mlp = false;
+    DevBuf<MlpSceneQueries> mlp_table;
+    std::vector<MlpSceneQueries> mlp_host;
+    uint32_t mlp_ctas = 0;
     std::string error;
 };
 
@@ -2862,7 +2868,8 @@ int batch_check(vgi_batch* b) {
         if (int e = check_ready(c, true)) return batch_fail(b, e, std::string("scene not ready: ") + c->error);
         if (c->device != b->device) return batch_fail(b, VGI_ERR_INVALID, "batched scenes must share one device");
         if (c->layout != VGI_LAYOUT_WAVEFRONT) return batch_fail(b, VGI_ERR_STATE, "batched scenes trace in the wavefront layout");
-        if (c->mlp_cache) return batch_fail(b, VGI_ERR_STATE, "the MLP cache mode is per scene, not batched");
+        if (c->mlp_cache != c0->mlp_cache || mlp_terminates(c) != mlp_terminates(c0))
+            return batch_fail(b, VGI_ERR_STATE, "batched scenes must all trace plainly or all end paths at their network, in the same phase");
         if (c->transport.bounces != c0->transport.bounces || transport_limited(c) != transport_limited(c0) ||
             (c->transport.budgeted != 0) != (c0->transport.budgeted != 0))
             return batch_fail(b, VGI_ERR_STATE, "batched scenes must share bounces, reach limit and step budget");
@@ -2891,8 +2898,49 @@ int batch_scenes(vgi_batch* b, uint32_t samples, bool scratch, std::vector<WaveS
         const size_t paths = (size_t)c->n_slots * samples;
         if (paths >= (1ull << 30)) return batch_fail(b, VGI_ERR_CAPACITY, "too many paths in a batched scene");
     }
-    std::vector<uint8_t> table((size_t)wave_batch_stages(b->ctxs[0]->transport.bounces) * n * wave_args_bytes());
-    wave_batch_args(scenes.data(), n, b->ctxs[0]->transport.bounces, table.data());
+    // A frame that ends paths at the network has one diffuse hit.
+    b->mlp = mlp_terminates(b->ctxs[0]);
+    const uint32_t hits = b->mlp ? 1u : b->ctxs[0]->transport.bounces;
+    std::vector<uint8_t> table((size_t)wave_batch_stages(hits) * n * wave_args_bytes());
+    wave_batch_args(scenes.data(), n, hits, table.data());
+    if (b->mlp) {
+        // The query launch's CTAs, shared out in proportion to the scenes'
+        // paths (at least one each).
+        size_t total = 0;
+        for (uint32_t i = 0; i < n; ++i) total += (size_t)scenes[i].a.n_tasks * samples;
+        const uint32_t budget = std::max<uint32_t>(b->ctxs[0]->mlp_ctas, n);
+        std::vector<MlpSceneQueries> q(n);
+        uint32_t first = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            vgi_ctx* c = b->ctxs[i];
+            const size_t paths = (size_t)scenes[i].a.n_tasks * samples;
+            const uint32_t ctas = std::max<uint32_t>(1u, (uint32_t)((double)budget * (double)paths / (double)std::max<size_t>(total, 1)));
+            MlpSceneQueries e;
+            std::memset(&e, 0, sizeof e);  // padding too: the table is compared bytewise
+            e.queue = scenes[i].b.mlp_queue;
+            e.counter = scenes[i].b.counters + 4;
+            e.capacity = (uint32_t)paths;
+            e.first_cta = first;
+            e.ctas = ctas;
+            e.enc = scenes[i].b.mlp_enc;
+            e.out = scenes[i].b.state + (size_t)4 * paths;  // the pending-value field, as wave_run's query launch
+            e.image = scenes[i].b.mlp_image;
+            e.error = scenes[i].b.mlp_error;
+            std::memcpy(&q[i], &e, sizeof e);
+            first += ctas;
+            c->mlp_queue_capacity = (uint32_t)paths;  // what the frame's training draws from
+        }
+        if (q.size() != b->mlp_host.size() || std::memcmp(q.data(), b->mlp_host.data(), q.size() * sizeof(MlpSceneQueries)) != 0) {
+            batch_drop_graph(b);
+            VGI_BCUDA(b, b->mlp_table.reserve(n));
+            VGI_BCUDA(b, h2d(b->mlp_table.ptr, q.data(), n * sizeof(MlpSceneQueries), b->stream));
+            VGI_BCUDA(b, cudaStreamSynchronize(b->stream));
+            b->mlp_host = q;
+        }
+        b->mlp_ctas = first;
+    }
+    if (b->mlp != b->graph_mlp) batch_drop_graph(b);
+    b->graph_mlp = b->mlp;
     if (table != b->table) {
         batch_drop_graph(b);
         VGI_BCUDA(b, b->args.reserve(table.size()));
@@ -2906,11 +2954,17 @@ int batch_scenes(vgi_batch* b, uint32_t samples, bool scratch, std::vector<WaveS
 void batch_trace(vgi_batch* b, const std::vector<WaveScene>& scenes, const AccumArgs* acc = nullptr, bool capture = false) {
     const vgi_ctx* c0 = b->ctxs[0];
     BatchStreams st{b->stream, b->side.data(), b->fork, b->join.data(), b->head.ptr, b->blocks, b->refill_min};
+    if (b->mlp) {
+        st.mlp_scenes = b->mlp_table.ptr;
+        st.mlp_n = (uint32_t)scenes.size();
+        st.mlp_ctas = b->mlp_ctas;
+        st.mlp_wait = c0->mlp_wait;
+    }
     if (capture) {
         b->prepare_nodes.assign(scenes.size(), nullptr);
         b->accumulate_nodes.assign(scenes.size(), nullptr);
     }
-    launch_wave_batch(scenes.data(), (uint32_t)scenes.size(), b->args.ptr, c0->transport.bounces, transport_limited(c0),
+    launch_wave_batch(scenes.data(), (uint32_t)scenes.size(), b->args.ptr, b->mlp ? 1u : c0->transport.bounces, transport_limited(c0),
                       c0->transport.budgeted != 0, st, acc, capture ? b->prepare_nodes.data() : nullptr,
                       capture ? b->accumulate_nodes.data() : nullptr);
 }
@@ -3055,7 +3109,15 @@ int vgi_batch_frame(vgi_batch* b, uint32_t samples, uint32_t clock_ms) {
         c->batch_id = (c->batch_id + 1) & 0x0fffffffu;
         if (c->batch_id == 0) c->batch_id = 1;
     }
-    return batch_leave(b);
+    if (int e = batch_leave(b)) return e;
+    // Each scene's online training, on its own stream after the frame, as
+    // vgi_frame runs it (the scenes' training overlaps on the GPU).
+    for (vgi_ctx* c : b->ctxs) {
+        if (!c->mlp_cache) continue;
+        if (int e = mlp_frame_training(c)) return batch_fail(b, e, std::string("MLP training: ") + c->error);
+        c->mlp_frames += 1;
+    }
+    return VGI_OK;
 }
 
 int vgi_batch_sync(vgi_batch* b) {

@@ -284,8 +284,11 @@ struct PathQueries {
     }
 };
 
+// The forward pass of CTA `cta` of `ctas` over `rows`' 128-row tiles, with
+// the network in `image` (the kernels below give each CTA its rows).
 template <class Rows>
-__global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, const uint8_t* image, uint32_t* error, uint32_t wait_polls) {
+__device__ __forceinline__ void forward_tiles(const Rows& rows, const uint8_t* image, uint32_t cta, uint32_t ctas, uint32_t* error,
+                                              uint32_t wait_polls) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* weights = smem;
     uint8_t* tile = smem + kImageBytes;
@@ -295,7 +298,7 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, cons
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t n = rows.count();
     const uint32_t tiles = (n + kRows - 1) / kRows;
-    if (blockIdx.x >= tiles) return;  // uniform per CTA: nothing allocated yet
+    if (cta >= tiles) return;  // uniform per CTA: nothing allocated yet
 
     const uint32_t bar_addr = smem_u32(bar);
     if (tid == 0) {
@@ -318,9 +321,9 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, cons
     if (!bar_wait(bar_addr, 0u, wait_polls)) give_up(bar_addr, 0u, abort_flag, error);
     uint32_t phase = 1;
     __syncthreads();
-    const uint32_t first_tile = *abort_flag ? tiles : blockIdx.x;
+    const uint32_t first_tile = *abort_flag ? tiles : cta;
 
-    for (uint32_t t = first_tile; t < tiles; t += gridDim.x) {
+    for (uint32_t t = first_tile; t < tiles; t += ctas) {
         const uint32_t row = t * kRows + tid;
         rows.stage(tile, tid, row);
         bool ok = true;
@@ -367,6 +370,31 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, cons
     fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns));
+}
+
+template <class Rows>
+__global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, const uint8_t* image, uint32_t* error, uint32_t wait_polls) {
+    forward_tiles(rows, image, blockIdx.x, gridDim.x, error, wait_polls);
+}
+
+// The queued hits of several scenes (the chunks of a batched frame) in one
+// launch. Each scene keeps its own queue, encoding, output field, network and
+// error word, and owns the CTA range [first_cta, first_cta + ctas) of the
+// grid; a CTA finds its scene by binary search (uniform per CTA) and runs
+// that scene's tiles. Every row's prediction is the one the scene's own
+// query launch gives: a row's outputs depend on its inputs and the weights
+// only, whatever tile it lands in.
+__global__ void __launch_bounds__(kThreads) forward_scenes_kernel(const MlpSceneQueries* scenes, uint32_t n_scenes, uint32_t wait_polls) {
+    uint32_t lo = 0, hi = n_scenes - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (scenes[mid].first_cta <= blockIdx.x) lo = mid;
+        else hi = mid - 1u;
+    }
+    const MlpSceneQueries sc = scenes[lo];
+    if (blockIdx.x - sc.first_cta >= sc.ctas) return;  // uniform per CTA
+    const PathQueries rows{sc.queue, sc.counter, sc.capacity, sc.enc, sc.out};
+    forward_tiles(rows, sc.image, blockIdx.x - sc.first_cta, sc.ctas, sc.error, wait_polls);
 }
 
 __global__ void encode_faces_kernel(const uint4* meta, uint32_t n, const float4* materials, MlpEncoding enc, float* features) {
@@ -782,6 +810,11 @@ void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t cap
     mlp::forward_kernel<mlp::PathQueries><<<ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error, wait_polls);
 }
 
+void launch_mlp_scene_queries(const MlpSceneQueries* scenes, uint32_t n_scenes, uint32_t ctas, cudaStream_t s, uint32_t wait_polls) {
+    if (n_scenes == 0 || ctas == 0) return;
+    mlp::forward_scenes_kernel<<<ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(scenes, n_scenes, wait_polls);
+}
+
 void launch_mlp_encode_training(const uint4* slot_meta, const uint4* results, const float4* materials, uint32_t n_slots,
                                 const uint32_t* step, uint32_t batch, const MlpEncoding& enc, float* features, float4* targets,
                                 cudaStream_t s) {
@@ -810,6 +843,8 @@ cudaError_t mlp_set_attributes() {
     cudaError_t e = cudaFuncSetAttribute(mlp::forward_kernel<mlp::FeatureRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(mlp::forward_kernel<mlp::PathQueries>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mlp::forward_scenes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(mlp::train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
     return e;
 }

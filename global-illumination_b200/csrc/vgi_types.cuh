@@ -72,6 +72,22 @@ struct MlpEncoding {
     float inv[3];
 };
 
+// One scene's network queries in a batched frame's single query launch
+// (launch_mlp_scene_queries): its hit queue (2 float4 a query) and count, the
+// count's bound, the grid's CTAs it owns, its encoding, the path-state field
+// the predictions go to, its network image and its error word.
+struct MlpSceneQueries {
+    const float4* queue;
+    const uint32_t* counter;
+    uint32_t capacity;
+    uint32_t first_cta, ctas;
+    MlpEncoding enc;
+    float4* out;
+    const uint8_t* image;
+    uint32_t* error;
+};
+void launch_mlp_scene_queries(const MlpSceneQueries* scenes, uint32_t n_scenes, uint32_t ctas, cudaStream_t s, uint32_t wait_polls);
+
 // The MLP cache's tensor-core kernels bound every mbarrier wait to
 // `wait_polls` polls: kMlpWaitPolls unless a caller lowers it
 // (vgi_mlp_set_wait_limit); a wait that runs out sets the error word.
@@ -125,6 +141,11 @@ struct BatchStreams {
     const cudaEvent_t* join;
     uint32_t* head;            // the batched traversal's shared queue head
     uint32_t blocks, refill_min;
+    // Scenes that end uncached first hits with their network: the device
+    // table of their queries, its length and the query launch's CTAs (null
+    // table: plain frames).
+    const MlpSceneQueries* mlp_scenes = nullptr;
+    uint32_t mlp_n = 0, mlp_ctas = 0, mlp_wait = kMlpWaitPolls;
 };
 // acc (null: trace only) gives each scene's prepare and accumulate; when
 // capturing, their graph nodes are stored in prepare_nodes / accumulate_nodes.

@@ -1368,12 +1368,18 @@ void wave_batch_run(const WaveScene* sc, uint32_t n, const WaveArgs* device_args
         fork();
         for (uint32_t i = 0; i < n; ++i) {
             const cudaStream_t s = st.side[i];
-            const WaveArgs W = stage_args(sc[i].b, sc[i].a, stage);
+            WaveArgs W = stage_args(sc[i].b, sc[i].a, stage);
             if (stage <= H) {
                 cudaMemsetAsync(W.count_out, 0, sizeof(uint32_t), s);
                 cudaMemsetAsync(W.scatter_count, 0, sizeof(uint32_t), s);
+                if (st.mlp_scenes) {
+                    // Uncached first hits queue for the network (one query
+                    // launch over every scene below), as wave_run's shade.
+                    W.mlp_queue = sc[i].b.mlp_queue;
+                    cudaMemsetAsync(W.mlp_count, 0, sizeof(uint32_t), s);
+                }
                 wave_shade_kernel<H, L, B, false><<<(W.n_paths + kWaveBlock - 1) / kWaveBlock, kWaveBlock, 0, s>>>(W, stage);
-                wave_scatter_kernel<H, L, B, false><<<sc[i].b.traverse_blocks, kWaveBlock, 0, s>>>(W);
+                if (!st.mlp_scenes) wave_scatter_kernel<H, L, B, false><<<sc[i].b.traverse_blocks, kWaveBlock, 0, s>>>(W);
             } else {
                 const uint32_t face_blocks = (uint32_t)((((uint64_t)sc[i].a.n_tasks << sc[i].a.lanes_log2) + kWaveBlock - 1) / kWaveBlock);
                 wave_finalize_kernel<H, L, B, false><<<face_blocks, kWaveBlock, 0, s>>>(W);
@@ -1382,6 +1388,13 @@ void wave_batch_run(const WaveScene* sc, uint32_t n, const WaveArgs* device_args
                     if (accumulate_nodes) accumulate_nodes[i] = last_node(s);
                 }
             }
+        }
+        if (st.mlp_scenes && stage <= H) {
+            // Every scene's queued hits take their network's prediction in
+            // one launch.
+            join();
+            launch_mlp_scene_queries(st.mlp_scenes, st.mlp_n, st.mlp_ctas, st.main, st.mlp_wait);
+            fork();
         }
     }
     join();

@@ -341,6 +341,30 @@ def _c(a, dtype) -> np.ndarray:
 
 # ---- host-side mirror of the reference's model types --------------------------
 
+def encode_edit_events(edits):
+    """Retention events for voxel edits, as encode_events packs them
+    (src/gpu/resident.rs:1320-1414): one event per edited box, `edits` a
+    list of (lo xyz, hi xyz, changed voxels, flux). Each bound is a measured
+    edit (kind 6): its measure record asks measure_edits for the one-voxel
+    margin scan around the box, which sets the flux. Returns (event words,
+    event count, measure records) for GpuTracer.apply_events_measured."""
+    head, bounds, measures = [], [], []
+    n = len(edits)
+    positions = 0
+    for k, (lo, hi, voxels, flux) in enumerate(edits):
+        lo = [int(v) for v in lo]
+        hi = [int(v) for v in hi]
+        head += [[lo[0], lo[1], lo[2], 0], [hi[0], hi[1], hi[2], 0], [0, 0, k, 1]]
+        f = int(np.float32(flux).view(np.uint32))
+        bounds += [[lo[0], lo[1], lo[2], f], [hi[0], hi[1], hi[2], 6]]
+        size = [hi[a] - lo[a] + 3 for a in range(3)]
+        count = size[0] * size[1] * size[2]
+        measures += [[3 * n + 2 * k, positions, count, int(voxels)], [lo[0] - 1, lo[1] - 1, lo[2] - 1, f], [*size, 0]]
+        positions += count
+    words = np.array(head + bounds, np.int64).reshape(-1).astype(np.uint32)
+    return words, n, np.array(measures, np.int64).reshape(-1, 4).astype(np.uint32).reshape(-1, 12) if measures else np.zeros((0, 12), np.uint32)
+
+
 @dataclasses.dataclass
 class MaterialTransport:
     """A transport material's optics (src/world.rs:59-79)."""

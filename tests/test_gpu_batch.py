@@ -151,3 +151,52 @@ def test_batched_frames_with_edit_streams_equal_own_frames(tracers):
             assert_words_equal(t.read_state(), state, f"scene {k} state")
     finally:
         batch.close()
+
+
+def _mlp_frames(tracers, cases, weights, batched, graph, frames=4):
+    for t, case, w in zip(tracers, cases, weights):
+        case.load(t)
+        t.mlp_set_weights(w)
+        t.set_mlp_cache(True, warm_frames=1, samples=4096, steps_per_frame=2, lr=1e-2)
+    batch = vgi.GpuBatch(tracers) if batched else None
+    try:
+        if batch:
+            batch.set_graph(graph)
+        for f in range(frames):
+            # Training's gradient sums vary in their last bits between runs,
+            # so every frame starts from the same weights in both runs.
+            for t, w in zip(tracers, weights):
+                t.mlp_set_weights(w)
+            if batch:
+                batch.frame(8, clock_ms=16 * f)
+            else:
+                for t in tracers:
+                    t.frame(8, clock_ms=16 * f)
+        if batch:
+            batch.sync()
+        out = [(t.read_results(), t.read_state(), t.mlp_stats()) for t in tracers]
+    finally:
+        if batch:
+            batch.close()
+        for t in tracers:
+            t.set_mlp_cache(False)
+    return out
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batched_mlp_frames_equal_each_scenes_own_frames(tracers, graph):
+    """Scenes in the MLP cache mode, batched: after a plain warm-up frame,
+    every scene's uncached first hits take its own network's prediction in
+    one query launch over all scenes, then each scene trains on its own
+    stream. Every frame's results and state equal the scene's own frames."""
+    cases = scenes()
+    rng = np.random.default_rng(12)
+    weights = [np.concatenate([(rng.normal(0.0, 1.0 / np.sqrt(i), size=(i, o)) * 0.5).astype(np.float32).reshape(-1)
+                               for i, o in vgi.GpuTracer.MLP_LAYERS]) for _ in cases]
+    want = _mlp_frames(tracers, cases, weights, batched=False, graph=False)
+    got = _mlp_frames(tracers, cases, weights, batched=True, graph=graph)
+    for k, ((r, st, stats), (wr, wst, wstats)) in enumerate(zip(got, want)):
+        assert wstats["queries"] > 0, "the network ended some paths"
+        assert stats["queries"] == wstats["queries"], (k, stats, wstats)
+        assert_words_equal(r, wr, f"scene {k} results")
+        assert_words_equal(st, wst, f"scene {k} state")

@@ -217,3 +217,24 @@ def test_light_selection_frequencies_match_reported_probabilities():
         df = len(bins) - 1
         chi2 = sum((o - e) ** 2 / e for o, e in bins)
         assert chi2 < df + 10.0 * (2.0 * df) ** 0.5 + 50.0, (chi2, df, position)
+
+
+def test_edit_events_encode_like_the_reference_planner():
+    """vgi.encode_edit_events packs measured edits as encode_events does
+    (src/gpu/resident.rs:1320-1414): event headers (union min, union max,
+    (cap 0, 0, first bound, bounds)), then bounds (min, flux) (max, kind 6),
+    and per bound a measure record (bound record, first position, margin
+    count, changed voxels) (min - 1, flux) (size + margin)."""
+    words, n, measures = vgi.encode_edit_events([((1, 2, 3), (4, 5, 6), 17, 40.0), ((10, 0, 0), (10, 1, 2), 3, 2.5)])
+    assert n == 2
+    w = words.reshape(-1, 4)
+    assert w.shape == (2 * 3 + 2 * 2, 4)
+    assert w[0].tolist() == [1, 2, 3, 0] and w[1].tolist() == [4, 5, 6, 0] and w[2].tolist() == [0, 0, 0, 1]
+    assert w[5].tolist() == [0, 0, 1, 1]
+    f40 = int(np.float32(40.0).view(np.uint32))
+    assert w[6].tolist() == [1, 2, 3, f40] and w[7].tolist() == [4, 5, 6, 6]
+    assert w[8].tolist()[:3] == [10, 0, 0] and w[9].tolist() == [10, 1, 2, 6]
+    m = measures.reshape(-1, 3, 4)
+    assert m[0].tolist() == [[6, 0, 6 * 6 * 6, 17], [0, 1, 2, f40], [6, 6, 6, 0]]
+    assert m[1][0].tolist() == [8, 216, 3 * 4 * 5, 3]
+    assert m[1][1][:3].tolist() == [9, 4294967295, 4294967295]
