@@ -24,6 +24,9 @@ side) both as separate per-scene frames and as batched frames (one
 traversal launch per stage over all scenes), from the same empty caches.
 ``next_rows`` times headless discovery, a far-tier frame and the view
 receivers' frame, reconstruction and presentation at 1920x1080.
+``cave`` traces the 1024x256x1024 cave in 16 uneven chunks as one batch,
+plain and in the MLP cache form with the network's queries batched across
+the chunks, to the plain trace's relMSE against the FP64 reference.
 ``stone_room`` runs the reference's stone-room fixture (32^3, 4 spp, 1 hit,
 64 steps, history 64) for 64 frames on the GPU and on the oracle, timed in
 full, and compares the final results and state word for word.
@@ -419,6 +422,168 @@ def run_reference(args):
         "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# The cave: 1024x256x1024 voxels, cut along x into 16 uneven chunks (widths
+# in regions), traced batched; at most this many faces in all.
+CAVE_REGIONS = (64, 16, 64)
+CAVE_CHUNKS = [2, 2, 3, 3, 3, 4, 4, 4, 4, 4, 5, 5, 5, 5, 5, 6]
+CAVE_FACES = 4_000_000
+
+
+def cave_chunks(local):
+    """The cave workload: seeded worm tunnels (radius 3..12) under a 16-voxel
+    roof with 16 skylight shafts, 2,000 emissive voxels (green (0.5, 4, 1)
+    and orange (6, 2, 0.3)), 8 rock materials, a sun and a sky. Its exposed
+    faces (every k-th, to at most CAVE_FACES) are the world cache. Each chunk
+    is one context holding its own regions and faces; a ray that leaves its
+    chunk ends in unloaded space, as it would at the edge of loaded pages."""
+    import vgi
+
+    coords, vox = vgi.cave(*CAVE_REGIONS, seed=3)
+    vox = vox.reshape(-1, 4096)
+    m = vgi.VoxelGiMaterials()
+    rng = np.random.default_rng(3)
+    for k in range(8):
+        m.set(k, vgi.MaterialTransport(diffuse=tuple(rng.uniform(0.2, 0.8, 3))))
+    m.set(8, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5), emission=(0.5, 4.0, 1.0)))
+    m.set(9, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5), emission=(6.0, 2.0, 0.3)))
+    words = m.words()
+    sun = vgi.DirectionalTransportLight((0.4, 0.8, 0.3), (3.0, 3.0, 3.0)).words()
+    per_chunk = []
+    lo = 0
+    for width in CAVE_CHUNKS:
+        keep = np.nonzero((coords[:, 0] >= lo) & (coords[:, 0] < lo + width))[0]
+        per_chunk.append((coords[keep], np.ascontiguousarray(vox[keep])))
+        lo += width
+    faces = [vgi.exposed_faces(c, v) for c, v in per_chunk]
+    total = sum(len(f) for f in faces)
+    keep = min(1.0, CAVE_FACES / max(total, 1))
+    faces = [f[np.random.default_rng(100 + k).random(len(f)) < keep].copy() for k, f in enumerate(faces)]
+    tracers = []
+    for (c, v), f in zip(per_chunk, faces):
+        t = vgi.GpuTracer(local)
+        t.upload_regions(c, v)
+        t.set_materials(words)
+        t.set_lights(sun, 1)
+        t.set_environment((0.3, 0.4, 0.5))
+        t.build_emitters()
+        t.set_transport(vgi.TransportSettings(bounces=BOUNCES, path_steps=2048))
+        t.set_faces(f)
+        tracers.append(t)
+    return tracers, faces, total, keep
+
+
+def cave_run(local, stream, flush, plain_frames=37):
+    """The cave (configuration 5): 16 uneven chunks traced as one batch
+    (each stage's traversal one launch, graph-replayed, autotuned), plain,
+    then in the MLP cache form with the network's queries batched across
+    the chunks (one query launch a frame, each chunk its own network trained
+    on its own faces, the rows of 65,536 training samples a frame shared out
+    by the chunks' paths). Both start from empty caches; the MLP form runs
+    until its relMSE against the FP64 reference (4,096 faces drawn over the
+    chunks in proportion to their faces) reaches the plain run's after
+    `plain_frames` frames. CUDA events from a common start to the last
+    chunk's end, L2 flushed in between."""
+    import torch
+
+    import vgi
+
+    tracers, faces, total_faces, keep = cave_chunks(local)
+    streams = [torch.cuda.ExternalStream(t.stream, device=torch.device("cuda", local)) for t in tracers]
+    n_faces = [len(f) for f in faces]
+    # FP64 reference per chunk on its share of 4,096 seeded faces.
+    refs = []
+    for t, f in zip(tracers, faces):
+        k = max(1, int(round(4096 * len(f) / sum(n_faces))))
+        refs.append(fp64_reference(t, f, n_faces=k))
+
+    def cave_relmse():
+        num = []
+        for t, ref in zip(tracers, refs):
+            est = t.read_state()[ref["sel"], 0:3].view(np.float32).astype(np.float64)
+            num.append((est @ LUMA - ref["l_ref"]) ** 2 / (ref["l_ref"] ** 2 + 0.01))
+        return float(np.mean(np.concatenate(num)))
+
+    def timed_frame(run, f):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(f))
+            start = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+        for st in streams:
+            st.wait_event(start)
+        run()
+        ends = []
+        for st in streams:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(st)
+            ends.append(e)
+        for e in ends:
+            e.synchronize()
+        return max(start.elapsed_time(e) for e in ends)
+
+    batch = vgi.GpuBatch(tracers)
+    tune = batch.autotune(SPP)
+    batch.set_graph(True)
+    rays = sum(t.census(SPP)["rays"] for t in tracers)
+    clock = 0
+    plain_ms = []
+    for f in range(plain_frames):
+        plain_ms.append(timed_frame(lambda: batch.frame(SPP, clock + 16 * f), f))
+    clock += 16 * plain_frames
+    plain_rel = cave_relmse()
+    rays_late = sum(t.census(SPP)["rays"] for t in tracers)
+    plain_step = float(np.median(plain_ms[3:]))
+    plain_total = float(sum(plain_ms))
+    batch.close()
+
+    # The MLP cache form from empty caches and untrained networks.
+    rng = np.random.default_rng(6)
+    for t, f in zip(tracers, faces):
+        init = np.concatenate([(rng.normal(0.0, 1.0 / np.sqrt(i), size=(i, o)) * 0.5).astype(np.float32).reshape(-1)
+                               for i, o in vgi.GpuTracer.MLP_LAYERS])
+        t.set_faces(f)
+        t.mlp_set_weights(init)
+        share = max(MLP_STEPS * 128, int(MLP_SAMPLES * len(f) / sum(n_faces)))
+        t.set_mlp_cache(True, warm_frames=MLP_WARM, samples=share, steps_per_frame=MLP_STEPS, lr=MLP_LR)
+    batch = vgi.GpuBatch(tracers)
+    batch.set_graph(True)
+    mlp_ms, curve, reached = [], [], None
+    total = 0.0
+    max_frames = 8 * plain_frames
+    for f in range(max_frames):
+        mlp_ms.append(timed_frame(lambda: batch.frame(MLP_SPP, clock + 16 * f), f))
+        total += mlp_ms[-1]
+        if (f + 1) % 4 == 0:
+            value = cave_relmse()
+            curve.append([f + 1, round(total, 2), round(value, 6)])
+            if value <= plain_rel:
+                reached = {"frames": f + 1, "ms": total}
+                break
+    mlp_rays = sum(t.census(MLP_SPP)["rays"] for t in tracers)
+    stats = [t.mlp_stats() for t in tracers]
+    batch.close()
+    for t in tracers:
+        t.set_mlp_cache(False)
+        t.close()
+    mlp_step = float(np.median(mlp_ms[MLP_WARM + 2:])) if len(mlp_ms) > MLP_WARM + 4 else float(np.median(mlp_ms))
+    return {
+        "workload": f"cave {CAVE_REGIONS[0] * 16}x{CAVE_REGIONS[1] * 16}x{CAVE_REGIONS[2] * 16}, 16 uneven chunks "
+                    f"({CAVE_CHUNKS} regions wide), worm tunnels, 16 skylights, 2,000 green and orange emitters, sun and sky; "
+                    f"{sum(n_faces)} faces (a seeded {keep:.3f} of the {total_faces} exposed), {SPP} spp plain / {MLP_SPP} spp MLP, 2 bounces",
+        "chunks": len(tracers), "faces_min_max": [int(min(n_faces)), int(max(n_faces))], "autotune": tune,
+        "plain": {"frames": plain_frames, "ms_per_frame": plain_step, "rays_per_frame": int(rays_late),
+                  "rays_per_s": rays_late / (plain_step * 1e-3), "relmse": plain_rel, "ms_to_relmse": plain_total,
+                  "first_frame_rays": int(rays)},
+        "mlp": {"ms_per_frame": mlp_step, "rays_per_frame": int(mlp_rays), "rays_per_s": mlp_rays / (mlp_step * 1e-3),
+                "frames_per_s_ratio": plain_step / mlp_step, "reached_plain_relmse": reached,
+                "speedup_at_equal_relmse": (plain_total / reached["ms"]) if reached else None,
+                "relmse_curve": curve[::4] + ([curve[-1]] if curve and (len(curve) - 1) % 4 else []),
+                "queries_last_frame": int(sum(s["queries"] for s in stats)), "errors": int(sum(s["error"] for s in stats)),
+                "query_launch": "one launch a frame over every chunk's queued hits (each chunk's network)"},
+        "reference": {"faces": int(sum(r["sel"].size for r in refs)), "spp": refs[0]["spp"],
+                      "seconds": round(sum(r["seconds"] for r in refs), 3)},
+    }
 
 
 ROOM_SPP, ROOM_FRAMES = 4, 64
@@ -875,6 +1040,8 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-scene comparison (0: skip it)")
     ap.add_argument("--no-next-rows", action="store_true", help="skip discovery, far tier and reconstruction timings")
     ap.add_argument("--no-room", action="store_true", help="skip the stone-room run (64 frames on the GPU and the oracle)")
+    ap.add_argument("--no-cave", action="store_true", help="skip the cave run (16 batched chunks, plain and MLP cache)")
+    ap.add_argument("--only-cave", action="store_true", help="only the cave run, printed as its own JSON object")
     ap.add_argument("--profile-next", action="store_true", help="only the next-row workload once, for ncu captures")
     ap.add_argument("--profile-frame", action="store_true", help="only plain frames of the terrain, for ncu captures")
     ap.add_argument("--small", action="store_true", help="with --profile-next or --profile-frame: the 256x128x256 terrain")
@@ -887,6 +1054,14 @@ def main():
         return
     if args.profile_next:
         profile_next(args.small)
+        return
+    if args.only_cave:
+        import torch
+
+        torch.cuda.set_device(0)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+        stream = torch.cuda.current_stream()
+        print(json.dumps({"cave": cave_run(0, stream, flush)}), flush=True)
         return
     if args.warmup < 3:
         args.warmup = 3
@@ -1043,6 +1218,7 @@ def main():
             batched = batch_comparison(local, stream, flush, args.batch_scenes, args.steps, args.warmup)
         beside = None if args.no_next_rows else next_rows(g, stream)
         room = None if args.no_room else stone_room_run(local, stream)
+        cave = None if args.no_cave else cave_run(local, stream, flush)
         line = {
             "metric": METRIC,
             "value": total_rays / (total_ms * 1e-3),
@@ -1085,6 +1261,7 @@ def main():
             "batched_scenes": batched,
             "next_rows": beside,
             "stone_room": room,
+            "cave": cave,
         }
         if base:
             line["cpu_baseline"] = base

@@ -188,7 +188,7 @@ void vgi_scene_cave(const vgi_cave_params* p, uint32_t nx, uint32_t ny, uint32_t
         const float sx = p->skylight_radius + uniform() * ((float)X - 2.0f * p->skylight_radius);
         const float sz = p->skylight_radius + uniform() * ((float)Z - 2.0f * p->skylight_radius);
         shafts.push_back({sx, sz});
-        for (int32_t y = ceiling - (int32_t)p->radius_max; y < Y; ++y) carve(sx, (float)y + 0.5f, sz, p->skylight_radius, Y + 1);
+        for (int32_t y = ceiling - (int32_t)p->radius_max; y < Y; ++y) carve(sx, (float)y + 0.5f, sz, p->skylight_radius, Y);
     }
     // Worm tunnels.
     const float span = p->radius_max - p->radius_min;

@@ -238,3 +238,19 @@ def test_edit_events_encode_like_the_reference_planner():
     assert m[0].tolist() == [[6, 0, 6 * 6 * 6, 17], [0, 1, 2, f40], [6, 6, 6, 0]]
     assert m[1][0].tolist() == [8, 216, 3 * 4 * 5, 3]
     assert m[1][1][:3].tolist() == [9, 4294967295, 4294967295]
+
+
+def test_cave_generator_stays_inside_its_volume():
+    """Skylight shafts reach the top voxel row and no further: the generator
+    writes nothing past the volume it fills (padding after it is untouched),
+    for caves whose shafts land on the last rows of regions."""
+    import ctypes
+
+    nx, ny, nz = 6, 4, 6
+    n = nx * ny * nz * 4096
+    for seed in range(12):
+        p = vgi.CaveParams(seed, 6, 60, 3.0, 8.0, 6, 16, 6.0, 20)
+        buf = np.full(n + 2 * 4096 * nx * ny, 777, np.uint16)
+        vgi.library().vgi_scene_cave(ctypes.byref(p), nx, ny, nz, buf.ctypes.data_as(ctypes.c_void_p))
+        assert (buf[n:] == 777).all(), seed
+        assert (buf[:n] == 256).any() and (buf[:n] != 256).any()
