@@ -676,12 +676,15 @@ class GpuTracer:
         w = _c(words, np.uint32).reshape(-1)
         self._check(self._lib.vgi_apply_events(self._h, _ptr(w), n_events, w.size))
 
-    def apply_events_measured(self, words: np.ndarray, n_events: int, measures: np.ndarray) -> np.ndarray:
+    def apply_events_measured(self, words: np.ndarray, n_events: int, measures: np.ndarray, read: bool = True):
         """Retention events whose measured edits take their flux from the
-        cache first; returns the event words as apply_events read them."""
+        cache first; returns the event words as apply_events read them
+        (None with read=False)."""
         w = _c(words, np.uint32).reshape(-1)
         m = _c(measures, np.uint32).reshape(-1, 12)
         self._check(self._lib.vgi_apply_events_measured(self._h, _ptr(w), n_events, w.size, _ptr(m), m.shape[0]))
+        if not read:
+            return None
         out = np.zeros_like(w)
         if self.n_slots:
             self._check(self._lib.vgi_read_events(self._h, _ptr(out), out.size))
