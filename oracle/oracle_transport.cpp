@@ -989,6 +989,18 @@ void orc_sincos(float x, float* s, float* c) { own_sincos(x, s, c); }
 float orc_exp(float x) { return own_exp(x); }
 uint32_t orc_pcg(uint32_t v) { return pcg(v); }
 uint32_t orc_curve_limit(uint32_t d2) { return curve_limit(d2); }
+// resolve_retention for one receiver voxel over encoded events (the
+// encode_events layout): out_limit = the history cap (NO_LIMIT for none),
+// out_change = the summed predicted change, flags bit 0 measured (every
+// change in range has a known flux, with measured_mode), bit 1 woken.
+int orc_resolve_retention(const uint32_t* events, uint32_t n_events, const int32_t* p3, uint32_t reach, int measured_mode,
+                          uint32_t* out_limit, float* out_change, uint32_t* flags) {
+    const Retention r = resolve_retention(events, p3, n_events, reach, measured_mode != 0, 0u, 0u);
+    *out_limit = r.limit;
+    *out_change = r.change;
+    *flags = (r.measured ? 1u : 0u) | (r.woken ? 2u : 0u);
+    return 0;
+}
 
 // prepare for every traced CPU-owned slot (voxel_accumulate.wgsl:114-133):
 // the task takes the slot's current sequence (begin_trace) and the slot's

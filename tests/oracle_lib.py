@@ -69,6 +69,7 @@ _SIG = {
     "orc_exp": (_F, [_F]),
     "orc_pcg": (_U32, [_U32]),
     "orc_curve_limit": (_U32, [_U32]),
+    "orc_resolve_retention": (_INT, [_P, _U32, _P, _U32, _INT, _P, _P, _P]),
     "orc_begin_trace": (_INT, [_P, _P, _P, _P, _U32, _P]),
     "orc_mark_changed": (_INT, [_P, _P, _P, _U32, _P]),
     "orc_accumulate": (_INT, [_P, _P, _P, _P, _P, _U32, _P]),
@@ -744,3 +745,18 @@ class Frames:
         ctl = controls_words(self.n, 0, 0, self.transport, self.batch_id, n_events)
         w = c(words, np.uint32)
         lib().orc_apply_events(ptr(self.state), ptr(self.meta), ptr(self.checkpoint), ptr(w), self.n, ptr(ctl))
+
+
+def resolve_retention(events, receiver, reach=192 * 192, measured=True):
+    """orc_resolve_retention: (history cap, predicted change or None when some
+    change in range has unknown flux, woken) for one receiver voxel over
+    events in the encode_events layout (words, count)."""
+    words, n = events
+    w = c(words, np.uint32).reshape(-1) if len(words) else np.zeros(4, np.uint32)
+    p = c(receiver, np.int32).reshape(3)
+    lim = ctypes.c_uint32()
+    change = ctypes.c_float()
+    flags = ctypes.c_uint32()
+    assert lib().orc_resolve_retention(ptr(w), n, ptr(p), reach, 1 if measured else 0, ctypes.byref(lim), ctypes.byref(change),
+                                       ctypes.byref(flags)) == 0
+    return lim.value, (change.value if flags.value & 1 else None), bool(flags.value & 2)

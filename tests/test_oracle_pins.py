@@ -343,3 +343,75 @@ def test_measured_edit_flux_is_own_plus_brightest_neighbour_light_twice_per_voxe
     assert out[15] == (np.float32(2.0) + brightest * np.float32(2.0) * np.float32(2.0)).view(np.uint32)
     assert out[19] == 3 | 8
     assert out[23] == words[23] and out[27] == 0
+
+
+def encode_retention_events(events):
+    """encode_events (src/gpu/resident.rs:1320-1414) for the pin cases.
+    An event is ("bounds", [(min, max, flux, kind, high)]) with the union of
+    its bounds, or ("source", cap, [(centre, radius)])."""
+    head, records = [], []
+    first = 0
+    for e in events:
+        if e[0] == "source":
+            _, cap, spheres = e
+            head += [[0, 0, 0, 2], [0, 0, 0, 0], [cap, 0, first, len(spheres)]]
+            first += len(spheres)
+        else:
+            bounds = e[1]
+            lo = np.min([b[0] for b in bounds], axis=0)
+            hi = np.max([b[1] for b in bounds], axis=0)
+            head += [[*lo, 0], [*hi, 0], [0, 0, first, len(bounds)]]
+            first += len(bounds)
+    for e in events:
+        if e[0] == "source":
+            for centre, radius in e[2]:
+                records += [[*np.float32(centre).view(np.uint32), np.float32(radius * radius).view(np.uint32)], [0, 0, 0, 5]]
+        else:
+            for lo, hi, flux, kind, high in e[1]:
+                records += [[*lo, int(np.float32(flux).view(np.uint32))], [*hi, kind | high]]
+    words = np.array(head + records, np.int64).astype(np.uint32).reshape(-1)
+    return words, len(events)
+
+
+def point(p):
+    return (np.array(p), np.array(p))
+
+
+def test_measured_change_follows_flux_height_and_falls_back_when_unknown():
+    # retention.rs:275-319, against the oracle's resolve_retention
+    # (voxel_retention.wgsl:29-96) with the influence radius 192 as reach.
+    def change_at(p, kind, flux, high, receiver):
+        events = encode_retention_events([("bounds", [(*point(p), flux, kind, high)])])
+        return O.resolve_retention(events, receiver)[1]
+
+    edit = change_at((0, 0, 0), 3, 10.0, 0, (10, 0, 0))
+    assert abs(edit - 10.0 / (math.pi * 100.0)) < 1e-6
+    # A load whose top solid voxel (5) is below the receiver replaces no sky it saw.
+    load_high = 5 << 3
+    assert change_at((0, 5, 0), 2, 2.0, load_high, (4, 12, 0)) == 0.0
+    below = change_at((0, 5, 0), 2, 2.0, load_high, (4, 0, 0))
+    assert abs(below - 2.0 * 6.0 / (math.pi * (16 + 25))) < 1e-6
+    # An air-only load (top i32::MIN, saturated to 28 bits).
+    air_high = ((-(1 << 27)) & 0xFFFFFFFF) << 3 & 0xFFFFFFFF
+    assert change_at((0, 0, 0), 2, 2.0, air_high, (1, 1, 1)) == 0.0
+    # Unloads predict nothing; unknown flux falls back to the curve.
+    assert change_at((0, 0, 0), 1, 0.0, 0, (1, 1, 1)) == 0.0
+    unknown = encode_retention_events([("bounds", [(*point((0, 0, 0)), 0.0, 0, 0)])])
+    limit, change, _ = O.resolve_retention(unknown, (64, 0, 0))
+    assert (limit, change) == (809, None)
+
+
+def test_events_reach_and_sources_cap_everywhere():
+    # retention.rs:321-343: an unknown change at 64 caps the origin at H(64);
+    # a source change caps every face at its cap, 4 inside its spheres, and
+    # wakes every face; a change beyond the influence radius does nothing.
+    events = encode_retention_events([("bounds", [(*point((64, 0, 0)), 0.0, 0, 0)]),
+                                      ("source", 64, [((0.0, 0.0, 300.0), 10.0)])])
+    limit, _, woken = O.resolve_retention(events, (0, 0, 0))
+    assert limit == 64 and woken  # min(H(64) = 809, the source cap 64)
+    assert O.resolve_retention(events, (0, 0, 295))[0] == 4
+    assert O.resolve_retention(events, (4000, 0, 0))[2], "source changes wake everyone"
+    only_bounds = encode_retention_events([("bounds", [(*point((64, 0, 0)), 0.0, 0, 0)])])
+    assert O.resolve_retention(only_bounds, (0, 0, 0))[0] == 809
+    far = encode_retention_events([("bounds", [(*point((4000, 0, 0)), 0.0, 0, 0)])])
+    assert O.resolve_retention(far, (0, 0, 0)) == (0xFFFFFFFF, 0.0, False)
