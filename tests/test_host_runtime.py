@@ -254,3 +254,56 @@ def test_cave_generator_stays_inside_its_volume():
         vgi.library().vgi_scene_cave(ctypes.byref(p), nx, ny, nz, buf.ctypes.data_as(ctypes.c_void_p))
         assert (buf[n:] == 777).all(), seed
         assert (buf[:n] == 256).any() and (buf[:n] != 256).any()
+
+
+def _one_region(voxels_materials):
+    vox = np.full(4096, 256, np.uint16)
+    for (x, y, z), m in voxels_materials:
+        vox[x + 16 * (y + 16 * z)] = m
+    return np.zeros((1, 3), np.int32), vox
+
+
+def test_emission_distribution_holds_exposed_faces_with_normalised_power():
+    # emission.rs:400-433: two adjacent emissive voxels have 10 exposed faces
+    # of equal power; the probabilities sum to 1; the CDF's first entry is
+    # 0.1 and its last 1.0, so a choice of 0 takes the first face and 0.999
+    # the last (choose_emitter's search).
+    coords, vox = _one_region([((4, 4, 4), 10), ((5, 4, 4), 10)])
+    entries = [((0.5, 0.5, 0.5), (0.0, 0.0, 0.0))] * 256
+    entries[10] = ((0.5, 0.5, 0.5), (5.0, 5.0, 5.0))
+    words, n_emit, total = O.emitters(coords, vox, O.material_words(entries))
+    assert n_emit == 10
+    records = words[: n_emit * 8].reshape(n_emit, 8)
+    cumulative = records[:, 4].view(np.float32)
+    probability = records[:, 5].view(np.float32)
+    assert abs(float(probability.astype(np.float64).sum()) - 1.0) < 1e-6
+    assert cumulative[0] == np.float32(0.1) and cumulative[-1] == np.float32(1.0)
+    assert (np.diff(cumulative) > 0).all()
+    # The library's host build (vgi_build_emitters) writes the same words.
+    assert (vgi.host_emitters(coords, vox, O.material_words(entries))[0] == words).all()
+
+
+def test_light_tree_keeps_weak_emitters_selectable():
+    # emission/tree.rs:266-293: one emitter a 1e18 times brighter than 63
+    # others in a row; the tree's selection probability of every face, seen
+    # from above the row, stays positive and finite and they sum to 1.
+    O.lib().orc_emitter_probability.restype = ctypes.c_float
+    O.lib().orc_emitter_probability.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_uint32]
+    coords = np.array([[x, 0, 0] for x in range(4)], np.int32)
+    vox = np.full((4, 4096), 256, np.uint16)
+    for x in range(64):
+        vox[x // 16][(x % 16) + 16 * (0 + 16 * 0)] = 4 if x == 0 else 5
+    entries = [((0.5, 0.5, 0.5), (0.0, 0.0, 0.0))] * 256
+    entries[4] = ((0.5, 0.5, 0.5), (1.0, 1.0, 1.0))
+    entries[5] = ((0.5, 0.5, 0.5), (1e-18, 1e-18, 1e-18))
+    words, n_emit, total = O.emitters(coords, vox, O.material_words(entries))
+    assert n_emit >= 32  # the tree, not the CDF
+    records = words[: n_emit * 8].reshape(n_emit, 8).view(np.int32)
+    position = np.array([0.5, 2.0, 0.5], np.float32)
+    normal = np.array([0.0, -1.0, 0.0], np.float32)
+    probabilities = np.array([O.lib().orc_emitter_probability(O.ptr(words), n_emit, total, O.ptr(position), O.ptr(normal),
+                                                              O.ptr(r[:3].copy()), int(r[3])) for r in records], np.float64)
+    assert np.isfinite(probabilities).all() and (probabilities > 0.0).all()
+    assert abs(probabilities.sum() - 1.0) < 1e-5
+    assert (vgi.host_emitters(coords, vox, O.material_words(entries))[0] == words).all()
