@@ -178,3 +178,103 @@ def test_refused_packed_deltas_change_nothing():
         with pytest.raises(vgi.VgiError) as err:
             g.patch_packed((lengths[0] * 2, lengths[1], lengths[2]), packed[3], False, [], [], [])
         assert err.value.status == vgi.ERR_INVALID
+
+
+def page_regions(page, voxels32):
+    """The eight 16^3 regions of a 32^3 page (x fastest) at page coordinate
+    `page` (region coordinates page * 2 + offset)."""
+    v = np.asarray(voxels32, np.uint16).reshape(32, 32, 32)  # z, y, x
+    coords, vox = [], []
+    for oz in range(2):
+        for oy in range(2):
+            for ox in range(2):
+                coords.append([page[0] * 2 + ox, page[1] * 2 + oy, page[2] * 2 + oz])
+                vox.append(v[oz * 16:(oz + 1) * 16, oy * 16:(oy + 1) * 16, ox * 16:(ox + 1) * 16].reshape(4096))
+    return np.array(coords, np.int32), np.stack(vox)
+
+
+def test_sparse_uploads_survive_growth_and_residency_changes():
+    """The reference's sparse-upload scenario (src/gpu/upload_tests.rs:22-80)
+    on both geometry paths: a page with a floor at y = 4; fifteen more pages
+    along x; those unloaded; a page at x = -1; one floor voxel carved; the
+    first page emptied. After every stage the page events
+    (vgi_update_regions) and the sparse packed delta (vgi_patch_packed) give
+    the oracle's geometry, and frames over each give the oracle's results."""
+    floor = np.full((32, 32, 32), 256, np.uint16)
+    floor[:, 4, :] = 1
+    m = vgi.VoxelGiMaterials()
+    m.set(1, vgi.MaterialTransport(diffuse=(0.6, 0.6, 0.6)))
+    m.set(2, vgi.MaterialTransport(diffuse=(0.5, 0.5, 0.5), emission=(4.0, 4.0, 4.0)))
+    words = m.words()
+    sun = vgi.DirectionalTransportLight((0.4, 0.8, 0.3), (3.0, 3.0, 3.0)).words()
+    transport = vgi.TransportSettings(bounces=1, path_steps=128)
+    pipe = O.Pipeline(1, 0, 128, 0, 4)
+    probes = np.array([[x, 4, 8, 2, 1] for x in range(12, 20)], np.int32)  # +Y faces of the floor
+    first_coords, first_vox = page_regions((0, 0, 0), floor)
+    ref = O.Scene(first_coords, first_vox, top_mode=0)
+    streamed, patched = vgi.GpuTracer(0), vgi.GpuTracer(0)
+    try:
+        streamed.update_regions(first_coords, first_vox, np.zeros((0, 3), np.int32))
+        packed = ref.arrays()
+        patched.upload_packed(*packed)
+        for g in (streamed, patched):
+            g.set_materials(words)
+            g.set_lights(sun, 1)
+            g.set_environment((0.1, 0.1, 0.1))
+            g.set_transport(transport)
+        resident = {(0, 0, 0): floor.copy()}
+        for stage in range(6):
+            loads, removed = [], []
+            if stage == 1:
+                loads = [((x, 0, 0), floor) for x in range(1, 16)]
+            elif stage == 2:
+                removed = [(x, 0, 0) for x in range(1, 16)]
+            elif stage == 3:
+                loads = [((-1, 0, 0), floor)]
+            elif stage == 4:
+                carved = resident[(0, 0, 0)].copy()
+                carved[8, 4, 8] = 256
+                loads = [((0, 0, 0), carved)]
+            elif stage == 5:
+                loads = [((0, 0, 0), np.full((32, 32, 32), 256, np.uint16))]
+            if stage:
+                lc = [page_regions(p, v) for p, v in loads]
+                load_coords = np.concatenate([c for c, _ in lc]) if lc else np.zeros((0, 3), np.int32)
+                load_vox = np.concatenate([v for _, v in lc]) if lc else np.zeros((0, 4096), np.uint16)
+                rm = np.concatenate([page_regions(p, floor)[0] for p in removed]) if removed else np.zeros((0, 3), np.int32)
+                streamed.update_regions(load_coords, load_vox, rm)
+                ref.regions(load_coords, load_vox, removed=rm)
+                new = ref.arrays()
+                send_delta(patched, packed, new)
+                packed = new
+                for p in removed:
+                    resident.pop(p, None)
+                for p, v in loads:
+                    resident[p] = v
+            live = [page_regions(p, v) for p, v in resident.items()]
+            live_coords = np.concatenate([c for c, _ in live])
+            live_vox = np.concatenate([v for _, v in live])
+            got_stream = streamed.geometry()
+            got_patch = patched.geometry()
+            for a, b, what in zip(got_patch, packed, ("directory", "headers", "cells", "bounds")):
+                assert_words_equal(np.asarray(a).reshape(-1), np.asarray(b).reshape(-1), f"patched {what}, stage {stage}")
+            assert_words_equal(O.canonical(*got_stream[:3], live_coords), O.canonical(*packed[:3], live_coords),
+                               f"streamed geometry, stage {stage}")
+            emitters, n_emit, total = O.emitters(live_coords, live_vox, words)
+
+            def params(n, samples, geometry=packed, total=total, n_emit=n_emit):
+                return O.params_words(n, samples, geometry[0].size // 4, 1, geometry[3], 1, (0.1, 0.1, 0.1), total, n_emit)
+
+            want = O.Frames(packed, params, words, sun, emitters, probes, transport, pipe)
+            for g in (streamed, patched):
+                g.set_emitters(emitters, n_emit, total)
+                g.set_faces(probes)
+                g.frame(4, clock_ms=0)
+                g.frame(4, clock_ms=16)
+            want.frame(4, clock_ms=0)
+            want.frame(4, clock_ms=16)
+            assert_words_equal(patched.read_results(), want.results, f"patched results, stage {stage}")
+            assert_words_equal(streamed.read_results(), want.results, f"streamed results, stage {stage}")
+    finally:
+        streamed.close()
+        patched.close()
