@@ -1212,6 +1212,9 @@ def main():
     # Dominant kernel: the persistent traversal (BOUNCES + 1 launches per frame).
     achieved = traverse_bytes / (traverse_ms * 1e-3) / 1e9
     traffic = profiled_traffic()
+    # The whole frame's algorithmic bytes per second.
+    frame_bytes = bytes_per_frame + n * (2 * 144 + 48)
+    frame_gbs = frame_bytes / (total_ms / args.steps * 1e-3) / 1e9
     if rank == 0:
         plain_frames = 2 * args.warmup + 3 * args.steps + 1  # warm-up, timed, graph, e2e warm-up and e2e frames
         quality = relmse(g, reference, plain_frames)
@@ -1265,6 +1268,14 @@ def main():
                          "bytes_per_launch": traverse_bytes / traverse_launches,
                          "note": "traversal algorithmic bytes (directory, header, brick, cell words; counting pass) / "
                                  "CUDA-event time of the traversal launches, same frame"},
+            "frame_roofline": {
+                "bound": "hbm", "achieved": frame_gbs, "peak": peak, "unit": "GB/s", "frac": frame_gbs / peak, "peak_source": peak_kind,
+                "bytes_per_frame": frame_bytes,
+                "definition": "the whole plain frame: the trace's algorithmic bytes (counting pass: geometry words, tasks, results, "
+                              "materials, lights, emitter and tree reads, face-index probes, accepted cache states) plus accumulate's "
+                              "state read and write (2 x 144 B) and checkpoint (48 B) per face, over the CUDA-event frame time",
+                "note": "most of these bytes hit L2 (the geometry, face index and gather records stay resident); the DRAM traffic "
+                        "of the frame's kernels is about a third of them (profiles)"},
             "clocks": clocks,
             "relmse": quality,
             "mlp_cache": mlp,

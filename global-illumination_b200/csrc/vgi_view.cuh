@@ -638,19 +638,13 @@ __global__ void __launch_bounds__(kBlock) view_seed_kernel(const ViewArgs V) {
     e[2] = w3(prior.mean, __float_as_uint(1.0f));
 }
 
-// trace_visible_paths (voxel_view_runtime.wgsl:272-325): one thread per
-// owner invocation; completed paths update the estimate's discounted running
-// mean and second moment.
+// One receiver's visits of a view frame (trace_visible_paths,
+// voxel_view_runtime.wgsl:272-325): completed paths update the estimate's
+// discounted running mean and second moment.
 template <bool LIMITED, bool BUDGETED>
-__global__ void __launch_bounds__(kBlock) view_trace_kernel(const ViewArgs V) {
-    __shared__ float4 smat[512];
-    const TraceArgs& A = V.t;
-    view_stage_materials<LIMITED, BUDGETED>(A, smat);
-    Cnt<false> cnt;
-    Tracer<1, LIMITED, BUDGETED, false> T{A, smat, cnt};
-    const uint32_t id = blockIdx.x * kBlock + threadIdx.x;
+__device__ __forceinline__ void view_trace_receiver(Tracer<1, LIMITED, BUDGETED, false>& T, const ViewArgs& V, uint32_t id, uint32_t& attempted,
+                                                    uint32_t& completed, uint32_t& known) {
     const uint32_t count = V.n;
-    if (id >= (count < V.range[1] ? count : V.range[1]) || V.range[2] == 0u) return;
     const uint32_t index = V.queue[kViewPrefix + (V.range[0] + id) % count];
     const uint32_t cap = V.view_first ? 32u : 1u;
     const uint32_t share = (V.range[1] - id + count - 1u) / count;
@@ -660,11 +654,11 @@ __global__ void __launch_bounds__(kBlock) view_trace_kernel(const ViewArgs V) {
     if (V.conts[index * 8u + 4u].w != 1u) next += 1u;
 #pragma unroll 1
     for (uint32_t visit = 0; visit < visits; ++visit) {
-        atomicAdd(V.queue + kViewAttempted, 1u);
+        attempted += 1u;
         advance_view_path<LIMITED, BUDGETED>(T, V, index);
         const uint32_t status = V.conts[index * 8u + 4u].w;
         if (status != 2u && status != 3u) continue;
-        atomicAdd(V.queue + kViewCompleted, 1u);
+        completed += 1u;
         uint4* e = V.estimates + index * 4u;
         uint4 identity = e[3];
         if (reserved) {
@@ -677,7 +671,7 @@ __global__ void __launch_bounds__(kBlock) view_trace_kernel(const ViewArgs V) {
         e[3] = identity;
         const uint4* path = V.paths + index * 8u;
         if (path[5].w != 0u) {
-            atomicAdd(V.queue + kViewKnown, 1u);
+            known += 1u;
             const V3 value = f3w(path[5]) + f3w(path[6]);
             V3 mean = f3w(e[0]), moment = f3w(e[1]);
             float weight = __uint_as_float(e[0].w), change = __uint_as_float(e[1].w);
@@ -705,6 +699,30 @@ __global__ void __launch_bounds__(kBlock) view_trace_kernel(const ViewArgs V) {
         const uint32_t first = V.queue[kViewPrefix + V.n + index];
         const uint32_t used = V.conts[index * 8u + 4u].w == 1u ? V.paths[index * 8u].w + 1u : V.estimates[index * 4u + 3u].x;
         V.queue[kViewPrefix + V.n + index] = first > used ? first : used;
+    }
+}
+
+// trace_visible_paths: one thread per owner invocation.
+template <bool LIMITED, bool BUDGETED>
+__global__ void __launch_bounds__(kBlock) view_trace_kernel(const ViewArgs V) {
+    __shared__ float4 smat[512];
+    const TraceArgs& A = V.t;
+    view_stage_materials<LIMITED, BUDGETED>(A, smat);
+    Cnt<false> cnt;
+    Tracer<1, LIMITED, BUDGETED, false> T{A, smat, cnt};
+    const uint32_t id = blockIdx.x * kBlock + threadIdx.x;
+    const uint32_t count = V.n;
+    // The frame's counters, summed per warp and added once per warp.
+    uint32_t attempted = 0, completed = 0, known = 0;
+    if (id < (count < V.range[1] ? count : V.range[1]) && V.range[2] != 0u)
+        view_trace_receiver<LIMITED, BUDGETED>(T, V, id, attempted, completed, known);
+    attempted = __reduce_add_sync(0xffffffffu, attempted);
+    completed = __reduce_add_sync(0xffffffffu, completed);
+    known = __reduce_add_sync(0xffffffffu, known);
+    if ((threadIdx.x & 31u) == 0u) {
+        if (attempted) atomicAdd(V.queue + kViewAttempted, attempted);
+        if (completed) atomicAdd(V.queue + kViewCompleted, completed);
+        if (known) atomicAdd(V.queue + kViewKnown, known);
     }
 }
 
