@@ -171,3 +171,38 @@ def test_region_loads_refuse_bad_input_and_keep_the_scene():
         g.unload_regions(coords)
         d, h, cl, bounds = g.geometry()
         assert (O.canonical(d, h, cl, coords)[:, 0] == 0).all()
+
+
+def test_one_scene_change_refuses_bad_input_and_handles_reloads():
+    """vgi_update_regions: a refused change (a duplicate loaded coordinate, a
+    voxel above 256) leaves the scene as it was, even with removals in the
+    same call; a region unloaded and loaded again with the same voxels in one
+    change is the same region (geometry and top-level field unchanged), and
+    with other voxels it is replaced."""
+    coords, vox = vgi.stone_room()
+    vox = vox.reshape(-1, 4096)
+    with vgi.GpuTracer(0) as g:
+        g.update_regions(coords, vox, np.zeros((0, 3), np.int32))
+        before = g.geometry()
+        dup = np.concatenate([coords[:2], coords[:1]])
+        with pytest.raises(vgi.VgiError) as err:
+            g.update_regions(dup, np.zeros((3, 4096), np.uint16), coords[3:4])
+        assert err.value.status == vgi.ERR_INVALID
+        bad = np.full((1, 4096), 257, np.uint16)
+        with pytest.raises(vgi.VgiError) as err:
+            g.update_regions(coords[:1], bad, coords[3:4])
+        assert err.value.status == vgi.ERR_INVALID
+        for a, b in zip(before, g.geometry()):
+            assert (np.asarray(a) == np.asarray(b)).all()
+        want = O.canonical(*before[:3], coords)
+        # Unloaded and sent again unchanged in the same change: untouched.
+        g.update_regions(coords[2:4], vox[2:4], coords[2:4])
+        assert (O.canonical(*g.geometry()[:3], coords) == want).all()
+        # Sent again with other voxels: replaced, as the oracle replaces it.
+        changed = vox[2:3].copy()
+        changed[0, :2048] = 256
+        g.update_regions(coords[2:3], changed, coords[2:3])
+        ref = O.Scene(coords, vox, top_mode=0)
+        ref.regions(coords[2:3], changed, removed=coords[2:3])
+        rd, rh, rcl, _ = ref.arrays()
+        assert (O.canonical(*g.geometry()[:3], coords) == O.canonical(rd, rh, rcl, coords)).all()
