@@ -192,7 +192,11 @@ def relmse(g, ref, frames):
 
 
 # MLP cache arm: spp, plain warm-up frames, training samples a frame, Adam steps a frame, learning rate.
-MLP_SPP, MLP_WARM, MLP_SAMPLES, MLP_STEPS, MLP_LR = 2, 8, 65536, 16, 1e-2
+MLP_SPP, MLP_WARM, MLP_SAMPLES, MLP_STEPS, MLP_LR = 2, 16, 65536, 16, 1e-2
+# Rows of one Adam step (16,384: the steps cycle four times through the frame's samples, 128
+# tiles of 128 rows on the 148 SMs) and the share of the samples since the network began ending
+# paths that a face's mean covers (1.0: those samples, not the warm-up frames' before them).
+MLP_STEP_ROWS, MLP_HISTORY = 16384, 1.0
 # Inference FLOPs per query at the network's real widths (81 inputs, 3 outputs):
 # 2 (81*64 + 3*64*64 + 64*3); the kernel computes the padded 96 x 16 shape.
 MLP_QUERY_FLOP = 2 * (81 * 64 + 3 * 64 * 64 + 64 * 3)
@@ -215,6 +219,7 @@ def mlp_comparison(g, faces, ref, stream, flush, plain, clock, max_frames):
     g.set_faces(faces)
     g.mlp_set_weights(init)
     g.set_mlp_cache(True, warm_frames=MLP_WARM, samples=MLP_SAMPLES, steps_per_frame=MLP_STEPS, lr=MLP_LR)
+    g.set_mlp_schedule(MLP_STEP_ROWS, MLP_HISTORY)
     g.set_timing(False)
     g.set_graph(True)
     target = plain["relmse"]
@@ -256,13 +261,14 @@ def mlp_comparison(g, faces, ref, stream, flush, plain, clock, max_frames):
     timed = g.mlp_stats()
     census = g.census(MLP_SPP)
     g.set_mlp_cache(False)
+    g.set_mlp_schedule(0, 0.0)
     steady_ms = float(np.median(frame_ms[MLP_WARM + 2:])) if len(frame_ms) > MLP_WARM + 4 else float(np.median(frame_ms))
     peak, peak_kind = measured_peak("bf16_tflops", 1590.0)
     achieved = timed["queries"] * MLP_QUERY_FLOP / (timed["query_ms"] * 1e-3) / 1e12 if timed["query_ms"] > 0 else None
     plain_total = plain["frames"] * plain["ms_per_frame"]
     out = {
         "config": {"spp": MLP_SPP, "warm_frames": MLP_WARM, "training_samples_per_frame": MLP_SAMPLES, "adam_steps_per_frame": MLP_STEPS,
-                   "lr": MLP_LR, "termination": "uncached first hits take the network's prediction",
+                   "rows_per_adam_step": MLP_STEP_ROWS, "history_share": MLP_HISTORY, "lr": MLP_LR, "termination": "uncached first hits take the network's prediction",
                    "network": "96 (81 used) -> 4 x 64 ReLU -> 16 (3 used, exp), BF16 tcgen05, FP32 accumulate and Adam masters"},
         "plain": {"spp": SPP, "frames": plain["frames"], "ms_per_frame": plain["ms_per_frame"], "relmse": target,
                   "ms_to_relmse": plain_total},
@@ -546,6 +552,7 @@ def cave_run(local, stream, flush, plain_frames=37):
         t.mlp_set_weights(init)
         share = max(MLP_STEPS * 128, int(MLP_SAMPLES * len(f) / sum(n_faces)))
         t.set_mlp_cache(True, warm_frames=MLP_WARM, samples=share, steps_per_frame=MLP_STEPS, lr=MLP_LR)
+        t.set_mlp_schedule(min(share, max(128, MLP_STEP_ROWS * share // MLP_SAMPLES)), MLP_HISTORY)
     batch = vgi.GpuBatch(tracers)
     batch.set_graph(True)
     mlp_ms, curve, reached = [], [], None
@@ -1002,7 +1009,7 @@ def profile_mlp(frames=3):
     the same generator at 256x256x256 voxels (64 emissive voxels), faces
     facing an eye at (128, 200, 128), 2 paths a face, the network ending
     uncached first hits from the first frame, 65,536 training samples in 16
-    Adam steps a frame. About 1 GB on the device."""
+    Adam steps of 16,384 rows a frame. About 1 GB on the device."""
     import vgi
 
     coords, vox = vgi.terrain(16, 16, 16, seed=2, octaves=4, period=64.0, base_height=128.0, falloff=400.0, emitters=64)
@@ -1026,6 +1033,7 @@ def profile_mlp(frames=3):
                            for i, o in vgi.GpuTracer.MLP_LAYERS])
     g.mlp_set_weights(init)
     g.set_mlp_cache(True, warm_frames=0, samples=MLP_SAMPLES, steps_per_frame=MLP_STEPS, lr=MLP_LR)
+    g.set_mlp_schedule(MLP_STEP_ROWS, MLP_HISTORY)
     for f in range(frames):
         g.frame(MLP_SPP, 16 * f)
     g.sync()

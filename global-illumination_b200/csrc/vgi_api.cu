@@ -99,6 +99,7 @@ struct DevBuf {
 };
 
 constexpr uint32_t kHistoryLimit = 65536;
+constexpr uint32_t kMlpHistoryFloor = 32;  // above the cache-binding count of 16
 constexpr float kMaxPathDistance = 768.0f;
 
 }  // namespace
@@ -204,6 +205,11 @@ struct vgi_ctx {
     bool mlp_cache = false;
     uint32_t mlp_warm = 0, mlp_batch = 65536, mlp_train_steps = 1, mlp_frames = 0;
     float mlp_lr = 1e-2f;
+    // vgi_set_mlp_schedule: 0, or the share of the samples taken since the
+    // network began ending paths that a face's mean covers.
+    float mlp_history = 0.0f;
+    // vgi_set_mlp_schedule: rows of one Adam step (0: samples / steps).
+    uint32_t mlp_step_rows = 0;
     bool graph_mlp = false;                   // the captured frame's trace ends paths with the network
     bool mlp_timed = false;                   // the last timed frame recorded mlp_marks
     bool mlp_queried = false;                 // a frame has queried the network (counters[4] holds its count)
@@ -342,6 +348,15 @@ void fill_controls(const vgi_ctx* c, uint32_t samples, uint32_t clock_ms, uint32
     w[1] = samples;
     w[2] = clock_ms;
     w[3] = t.history_limit == 0 ? kHistoryLimit : std::min(t.history_limit, kHistoryLimit);
+    if (c->mlp_history > 0.0f && c->mlp_cache && c->mlp_frames >= c->mlp_warm) {
+        // The MLP cache's growing window: the count cap is the given share of
+        // the samples taken in frames the network answers (this one
+        // included), at least kMlpHistoryFloor, so early frames' answers
+        // from the untrained network fade from the means.
+        const double taken = (double)samples * (double)(c->mlp_frames - c->mlp_warm + 1u);
+        const double window = std::max((double)kMlpHistoryFloor, std::ceil((double)c->mlp_history * taken));
+        w[3] = (uint32_t)std::min((double)w[3], window);
+    }
     w[4] = fbits(std::max(t.response_seconds, 0.001f));
     w[5] = c->n_slots;
     w[10] = fbits(t.recency >= 1.0f ? t.recency : 1.0f);
@@ -2598,7 +2613,10 @@ static int mlp_train_step(vgi_ctx* c, const float* features, const float4* targe
 static int mlp_frame_training(vgi_ctx* c) {
     if (!c->mlp_cache || !c->mlp_image.ptr || c->n_slots == 0) return VGI_OK;
     const MlpEncoding enc = mlp_encoding(c);
-    const uint32_t rows = c->mlp_batch, steps = c->mlp_train_steps, batch = rows / steps;
+    const uint32_t rows = c->mlp_batch, steps = c->mlp_train_steps;
+    // Rows a step: a share of the frame's samples, or (with a schedule) a
+    // batch that may exceed it, the steps then cycling through the samples.
+    const uint32_t batch = c->mlp_step_rows ? std::min(c->mlp_step_rows, rows) : rows / steps;
     if (!mlp_terminates(c)) {
         for (uint32_t k = 0; k < steps; ++k) {
             launch_mlp_encode_training(c->slot_meta.ptr, c->results.ptr, c->materials.ptr, c->n_slots, c->mlp_steps.ptr, batch, enc,
@@ -2614,10 +2632,11 @@ static int mlp_frame_training(vgi_ctx* c) {
     const TraceArgs tr = trace_args(c, c->mlp_train_tasks.ptr, c->mlp_train_results.ptr, rows, kMlpTrainSamples, true);
     if (int e = run_trace(c, tr, false, false)) return e;
     launch_mlp_query_targets(c->mlp_train_results.ptr, rows, c->mlp_targets.ptr, c->stream);
-    for (uint32_t k = 0; k < steps; ++k)
-        if (int e = mlp_train_step(c, c->mlp_features.ptr + (size_t)k * batch * 96, c->mlp_targets.ptr + (size_t)k * batch, batch,
-                                   c->mlp_lr))
-            return e;
+    for (uint32_t k = 0; k < steps; ++k) {
+        uint32_t first = (uint32_t)(((uint64_t)k * batch) % rows);
+        if (first + batch > rows) first = rows - batch;
+        if (int e = mlp_train_step(c, c->mlp_features.ptr + (size_t)first * 96, c->mlp_targets.ptr + first, batch, c->mlp_lr)) return e;
+    }
     c->mlp_queried = true;
     return VGI_OK;
 }
@@ -2665,6 +2684,16 @@ int vgi_set_mlp_cache(vgi_ctx* c, int enable, uint32_t warm_frames, uint32_t bat
     c->mlp_train_steps = steps_per_frame;
     c->mlp_lr = lr;
     c->mlp_frames = 0;
+    return VGI_OK;
+}
+
+int vgi_set_mlp_schedule(vgi_ctx* c, uint32_t rows_per_step, float history_share) {
+    if (!c) return VGI_ERR_INVALID;
+    if (!(history_share >= 0.0f && history_share <= 1.0f)) return fail(c, VGI_ERR_INVALID, "MLP history share must be in [0, 1]");
+    if (rows_per_step > (1u << 22)) return fail(c, VGI_ERR_INVALID, "MLP rows per step: at most 2^22");
+    drop_graph(c);  // the captured training steps change
+    c->mlp_history = history_share;
+    c->mlp_step_rows = rows_per_step;
     return VGI_OK;
 }
 

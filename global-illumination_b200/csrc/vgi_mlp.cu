@@ -190,8 +190,8 @@ __device__ __forceinline__ void stage_face(uint8_t* tile, uint32_t row, const fl
         for (int c = 0; c < 3; ++c) store8(tile, row, (uint32_t)(a * 3 + c), kIn, v + c * 8);
     }
     float v[24];
-    for (int j = 0; j < 24; ++j) v[j] = 0.0f;
-    if (face < 6u) v[face] = 1.0f;
+    // The one-hot by compare, not by a dynamic index, keeps v in registers.
+    for (int j = 0; j < 24; ++j) v[j] = (uint32_t)j == face ? 1.0f : 0.0f;
     v[6] = r;
     v[7] = g;
     v[8] = b;
@@ -350,13 +350,19 @@ __device__ __forceinline__ void forward_tiles(const Rows& rows, const uint8_t* i
             }
             fence_after();
             if (l + 1 < kLayers) {
-                for (uint32_t c0 = 0; c0 < N; c0 += 16u) {
-                    float v[16];
-                    tmem_ld16(lane_base + c0, v);
-                    tmem_wait_ld();
-                    for (int j = 0; j < 16; ++j) v[j] = v[j] > 0.0f ? v[j] : 0.0f;
-                    store8(tile, tid, c0 / 8u, N, v);
-                    store8(tile, tid, c0 / 8u + 1u, N, v + 8);
+                // The row's TMEM loads all in flight, then one wait.
+                float v[64];
+#pragma unroll
+                for (uint32_t c0 = 0; c0 < 64u; c0 += 16u)
+                    if (c0 < N) tmem_ld16(lane_base + c0, v + c0);
+                tmem_wait_ld();
+#pragma unroll
+                for (uint32_t c0 = 0; c0 < 64u; c0 += 16u) {
+                    if (c0 >= N) continue;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[c0 + j] = v[c0 + j] > 0.0f ? v[c0 + j] : 0.0f;
+                    store8(tile, tid, c0 / 8u, N, v + c0);
+                    store8(tile, tid, c0 / 8u + 1u, N, v + c0 + 8);
                 }
             } else {
                 float v[16];
@@ -527,15 +533,23 @@ __device__ __forceinline__ void store_t(uint8_t* smem, uint32_t base, uint32_t r
     *reinterpret_cast<__nv_bfloat16*>(smem + base + t_offset(row, col)) = __float2bfloat16_rn(v);
 }
 
-__global__ void __launch_bounds__(kThreads) train_kernel(const float* features, const float4* targets, uint32_t batch,
-                                                         const uint8_t* image_f, const uint8_t* image_b, float* partials,
-                                                         uint32_t* error, uint32_t wait_polls) {
+// 256 threads: two warps per TMEM lane quadrant. Thread tid serves tile row
+// (sample) tid % 128, the lanes of warp (tid / 32) % 4, and half tid / 128 of
+// each 64-wide row's columns (32 each); the 16-wide output layer is the
+// first half's alone. Two warps per scheduler hide each other's waits.
+constexpr uint32_t kTrainThreads = 256;
+static_assert(kHidden == 64 && kOut == 16 && kIn == 96, "the column split assumes 96 -> 64 ... 64 -> 16");
+
+__global__ void __launch_bounds__(kTrainThreads) train_kernel(const float* features, const float4* targets, uint32_t batch,
+                                                              const uint8_t* image_f, const uint8_t* image_b, float* partials,
+                                                              uint32_t* error, uint32_t wait_polls) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kBarT);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kBarT + 8);
     uint32_t* abort_flag = reinterpret_cast<uint32_t*>(smem + kBarT + 12);
-    float* loss_warps = reinterpret_cast<float*>(smem + kBarT + 16);
+    float* loss_warps = reinterpret_cast<float*>(smem + kBarT + 16);  // 8 floats: kBarT + 16 .. + 48
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t r = tid & (kRows - 1u), half = tid >> 7, col0 = half * 32u;
     const uint32_t bar_addr = smem_u32(bar), s0 = smem_u32(smem);
     if (tid == 0) {
         *abort_flag = 0u;
@@ -547,7 +561,7 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
     }
     // Zero the transposed tiles once: rows past a tile's real features are
     // read by the M = 128 products.
-    for (uint32_t i = tid; i < (kBarT - kH0) / 16; i += kThreads) reinterpret_cast<uint4*>(smem + kH0)[i] = make_uint4(0, 0, 0, 0);
+    for (uint32_t i = tid; i < (kBarT - kH0) / 16; i += kTrainThreads) reinterpret_cast<uint4*>(smem + kH0)[i] = make_uint4(0, 0, 0, 0);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTrainColumns));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -556,7 +570,7 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t lane_base = tmem + ((warp * 32u) << 16);
+    const uint32_t lane_base = tmem + (((warp & 3u) * 32u) << 16);
     const uint32_t tiles = (batch + kRows - 1) / kRows;
     bool first = true, ok = true;
     float loss_sum = 0.0f;
@@ -580,21 +594,23 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
     ok = finish();  // the weight images
 
     for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-        const uint32_t row = t * kRows + tid;
+        const uint32_t row = t * kRows + r;
         const bool valid = row < batch;
-        // Input: A (K = 96) and h_0^T, all 24 loads in flight first.
+        // Input: this half's 48 features of A (K = 96) and h_0^T, the 12
+        // loads in flight first.
         {
-            float4 in[kIn / 4];
-            const float4* src = reinterpret_cast<const float4*>(features + (size_t)row * kIn);
+            float4 in[kIn / 8];
+            const float4* src = reinterpret_cast<const float4*>(features + (size_t)row * kIn) + half * (kIn / 8);
 #pragma unroll
-            for (int q = 0; q < kIn / 4; ++q) in[q] = valid ? src[q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            for (int q = 0; q < kIn / 8; ++q) in[q] = valid ? src[q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
-            for (uint32_t c = 0; c < kIn / 8; ++c) {
+            for (uint32_t c = 0; c < kIn / 16; ++c) {
+                const uint32_t group = half * (kIn / 16) + c;
                 const float v[8] = {in[2 * c].x, in[2 * c].y, in[2 * c].z, in[2 * c].w,
                                     in[2 * c + 1].x, in[2 * c + 1].y, in[2 * c + 1].z, in[2 * c + 1].w};
-                store8(smem + kAT, tid, c, kIn, v);
+                store8(smem + kAT, r, group, kIn, v);
 #pragma unroll
-                for (int j = 0; j < 8; ++j) store_t(smem, kH0, c * 8 + j, tid, v[j]);
+                for (int j = 0; j < 8; ++j) store_t(smem, kH0, group * 8 + j, r, v[j]);
             }
         }
         // Forward.
@@ -612,30 +628,29 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
             }
             if (!(ok = finish())) break;
             if (l + 1 < kLayers) {
+                // This half's 32 columns: both loads in flight, one wait.
+                float v[32];
+                tmem_ld16(lane_base + col0, v);
+                tmem_ld16(lane_base + col0 + 16u, v + 16);
+                tmem_wait_ld();
 #pragma unroll
-                for (uint32_t c0 = 0; c0 < N; c0 += 16u) {
-                    float v[16];
-                    tmem_ld16(lane_base + c0, v);
-                    tmem_wait_ld();
+                for (int j = 0; j < 32; ++j) v[j] = v[j] > 0.0f ? v[j] : 0.0f;
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) v[j] = v[j] > 0.0f ? v[j] : 0.0f;
-                    store8(smem + kAT, tid, c0 / 8u, N, v);
-                    store8(smem + kAT, tid, c0 / 8u + 1u, N, v + 8);
+                for (uint32_t c = 0; c < 4u; ++c) store8(smem + kAT, r, half * 4u + c, N, v + c * 8);
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) store_t(smem, ht_offset(l + 1), c0 + j, tid, v[j]);
-                }
-            } else {
+                for (int j = 0; j < 32; ++j) store_t(smem, ht_offset(l + 1), col0 + j, r, v[j]);
+            } else if (half == 0) {
                 tmem_ld16(lane_base, z);
                 tmem_wait_ld();
             }
         }
         if (!ok) break;
-        // Output gradient.
-        float dz[64];
+        // Output gradient (the first half: the 16-wide layer is its own).
+        float dz[32];
 #pragma unroll
-        for (int j = 0; j < 64; ++j) dz[j] = 0.0f;
-        const float4 y = valid ? targets[row] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (valid && y.x == y.x) {  // a NaN target marks a row without a sample
+        for (int j = 0; j < 32; ++j) dz[j] = 0.0f;
+        const float4 y = valid && half == 0 ? targets[row] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (valid && half == 0 && y.x == y.x) {  // a NaN target marks a row without a sample
             const float p0 = expf(z[0]), p1 = expf(z[1]), p2 = expf(z[2]);
             const float lum = 0.2126f * p0 + 0.7152f * p1 + 0.0722f * p2;
             const float inv = 1.0f / ((lum * lum + 0.01f) * (float)batch);
@@ -649,10 +664,20 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
 #pragma unroll
         for (int l = kLayers - 1; l >= 0; --l) {
             const uint32_t N = out_dim(l), Kin = in_dim(l);
+            // dz_l as the A operand (samples x N) and transposed (N x samples):
+            // this half's 32 columns of a 64-wide layer, or the first half's
+            // 16 of the output layer.
+            if (N == 64u) {
 #pragma unroll
-            for (uint32_t c = 0; c < N / 8u; ++c) store8(smem + kAT, tid, c, N, dz + c * 8);
+                for (uint32_t c = 0; c < 4u; ++c) store8(smem + kAT, r, half * 4u + c, N, dz + c * 8);
 #pragma unroll
-            for (uint32_t o = 0; o < N; ++o) store_t(smem, kDZ, o, tid, dz[o]);
+                for (uint32_t o = 0; o < 32u; ++o) store_t(smem, kDZ, col0 + o, r, dz[o]);
+            } else if (half == 0) {
+#pragma unroll
+                for (uint32_t c = 0; c < 2u; ++c) store8(smem + kAT, r, c, N, dz + c * 8);
+#pragma unroll
+                for (uint32_t o = 0; o < 16u; ++o) store_t(smem, kDZ, o, r, dz[o]);
+            }
             publish();
             if (tid == 0) {
                 fence_after();
@@ -670,26 +695,24 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
             }
             if (!(ok = finish())) break;
             if (l > 0) {
+                // dh (Kin = 64) into this half's dz, then the ReLU mask from
+                // the kept activations.
+                tmem_ld16(lane_base + col0, dz);
+                tmem_ld16(lane_base + col0 + 16u, dz + 16);
+                tmem_wait_ld();
 #pragma unroll
-                for (uint32_t c0 = 0; c0 < Kin; c0 += 16u) {
-                    float v[16];
-                    tmem_ld16(lane_base + c0, v);
-                    tmem_wait_ld();
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const __nv_bfloat16 h = *reinterpret_cast<const __nv_bfloat16*>(smem + ht_offset(l) + t_offset(c0 + j, tid));
-                        dz[c0 + j] = (valid && __bfloat162float(h) > 0.0f) ? v[j] : 0.0f;
-                    }
+                for (int j = 0; j < 32; ++j) {
+                    const __nv_bfloat16 h = *reinterpret_cast<const __nv_bfloat16*>(smem + ht_offset(l) + t_offset(col0 + j, r));
+                    dz[j] = (valid && __bfloat162float(h) > 0.0f) ? dz[j] : 0.0f;
                 }
-#pragma unroll
-                for (uint32_t j = Kin; j < 64; ++j) dz[j] = 0.0f;
             }
         }
         if (!ok) break;
         first = false;
     }
-    // This CTA's gradient sums: row `tid` of each layer's accumulator is
-    // input feature tid.
+    // This CTA's gradient sums: row r of each layer's accumulator is input
+    // feature r; this half writes its 32 columns (the output layer's 16: the
+    // first half).
     float* out = partials + (size_t)blockIdx.x * kPartial;
     if (ok && !first) {
         fence_before();
@@ -698,17 +721,23 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
 #pragma unroll
         for (int l = 0; l < kLayers; ++l) {
             const uint32_t N = out_dim(l);
-#pragma unroll
-            for (uint32_t c0 = 0; c0 < N; c0 += 16u) {
-                float v[16];
-                tmem_ld16(lane_base + grad_column(l) + c0, v);
+            float v[32];
+            if (N == 64u) {
+                tmem_ld16(lane_base + grad_column(l) + col0, v);
+                tmem_ld16(lane_base + grad_column(l) + col0 + 16u, v + 16);
                 tmem_wait_ld();
-                if (tid < (uint32_t)in_dim(l)) {
-                    float4* dst = reinterpret_cast<float4*>(out + weight_offset(l) + tid * N + c0);
-                    dst[0] = make_float4(v[0], v[1], v[2], v[3]);
-                    dst[1] = make_float4(v[4], v[5], v[6], v[7]);
-                    dst[2] = make_float4(v[8], v[9], v[10], v[11]);
-                    dst[3] = make_float4(v[12], v[13], v[14], v[15]);
+                if (r < (uint32_t)in_dim(l)) {
+#pragma unroll
+                    for (uint32_t c = 0; c < 32u; c += 4u)
+                        *reinterpret_cast<float4*>(out + weight_offset(l) + r * N + col0 + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                }
+            } else if (half == 0) {
+                tmem_ld16(lane_base + grad_column(l), v);
+                tmem_wait_ld();
+                if (r < (uint32_t)in_dim(l)) {
+#pragma unroll
+                    for (uint32_t c = 0; c < 16u; c += 4u)
+                        *reinterpret_cast<float4*>(out + weight_offset(l) + r * N + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
                 }
             }
         }
@@ -718,32 +747,59 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const float* features, 
     if ((tid & 31u) == 0) loss_warps[warp] = loss_sum;
     fence_before();
     __syncthreads();
-    if (tid == 0) out[kWeights] = (loss_warps[0] + loss_warps[1]) + (loss_warps[2] + loss_warps[3]);
+    // Warps 4-7 (the second half) carry no loss: their terms are zero.
+    if (tid == 0)
+        out[kWeights] = ((loss_warps[0] + loss_warps[1]) + (loss_warps[2] + loss_warps[3])) +
+                        ((loss_warps[4] + loss_warps[5]) + (loss_warps[6] + loss_warps[7]));
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTrainColumns));
 }
 
-// Sums the CTAs' partial rows in order: grads[i] and the loss.
-__global__ void reduce_kernel(const float* partials, uint32_t parts, float* grads, float* loss) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i <= kWeights) {
-        float g = 0.0f;
-        for (uint32_t c = 0; c < parts; ++c) g += partials[(size_t)c * kPartial + i];
-        if (i < kWeights) grads[i] = g;
-        else *loss = g;
+// The CTAs' partial rows summed, for kSumWeights consecutive entries of a
+// block (weights, then the loss at kWeights): kSumGroups threads share an
+// entry, thread group j summing rows j, j + kSumGroups, ... in order, and the
+// group sums are added in a fixed tree, so the result does not depend on
+// timing. Four groups put four times as many loads in flight as one thread
+// an entry: the partial rows (128 x 78 KB for a 16,384-row step) are read at
+// L2 bandwidth instead of one thread's load latency.
+constexpr int kSumWeights = 64, kSumGroups = 4, kSumThreads = kSumWeights * kSumGroups;
+constexpr int kSumBlocks = (kWeights + 1 + kSumWeights - 1) / kSumWeights;
+
+// Returns the sum for entry `w` in the threads of group 0 (others: 0).
+__device__ __forceinline__ float sum_partials(const float* partials, uint32_t parts, int w, float (*scratch)[kSumWeights]) {
+    const int t = threadIdx.x % kSumWeights, j = threadIdx.x / kSumWeights;
+    float g = 0.0f;
+    if (w <= kWeights) {
+#pragma unroll 8
+        for (uint32_t c = (uint32_t)j; c < parts; c += kSumGroups) g += partials[(size_t)c * kPartial + w];
     }
+    scratch[j][t] = g;
+    __syncthreads();
+    return j == 0 ? (scratch[0][t] + scratch[1][t]) + (scratch[2][t] + scratch[3][t]) : 0.0f;
+}
+static_assert(kSumGroups == 4, "the fixed tree of sum_partials adds four group sums");
+
+// grads[i] and the loss.
+__global__ void __launch_bounds__(kSumThreads) reduce_kernel(const float* partials, uint32_t parts, float* grads, float* loss) {
+    __shared__ float scratch[kSumGroups][kSumWeights];
+    const int w = blockIdx.x * kSumWeights + (int)(threadIdx.x % kSumWeights);
+    const float g = sum_partials(partials, parts, w, scratch);
+    if (threadIdx.x >= (unsigned)kSumWeights || w > kWeights) return;
+    if (w < kWeights) grads[w] = g;
+    else *loss = g;
 }
 
 // One Adam step (Kingma & Ba) on the FP32 masters from the CTAs' partial
 // gradient rows, then both BF16 images. The step count lives on the device
 // (frames replay from a graph): every thread reads it first, and the last
 // block to finish stores it advanced by one.
-__global__ void adam_kernel(float* master, float* m, float* v, const float* partials, uint32_t parts, float lr, float beta1, float beta2,
-                            float eps, uint32_t* steps, uint8_t* image_f, uint8_t* image_b, float* loss) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kSumThreads) adam_kernel(float* master, float* m, float* v, const float* partials, uint32_t parts, float lr,
+                                                          float beta1, float beta2, float eps, uint32_t* steps, uint8_t* image_f,
+                                                          uint8_t* image_b, float* loss) {
+    __shared__ float scratch[kSumGroups][kSumWeights];
+    const int i = blockIdx.x * kSumWeights + (int)(threadIdx.x % kSumWeights);
     const uint32_t step = steps[0] + 1u;
-    if (i < kWeights) {
-        float g = 0.0f;
-        for (uint32_t c = 0; c < parts; ++c) g += partials[(size_t)c * kPartial + i];
+    const float g = sum_partials(partials, parts, i, scratch);
+    if (threadIdx.x < (unsigned)kSumWeights && i < kWeights) {
         const float mi = beta1 * m[i] + (1.0f - beta1) * g;
         const float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
         m[i] = mi;
@@ -756,10 +812,8 @@ __global__ void adam_kernel(float* master, float* m, float* v, const float* part
         const __nv_bfloat16 b = __float2bfloat16_rn(w);
         *reinterpret_cast<__nv_bfloat16*>(image_f + fwd) = b;
         *reinterpret_cast<__nv_bfloat16*>(image_b + bwd) = b;
-    } else if (i == kWeights) {
-        float l = 0.0f;
-        for (uint32_t c = 0; c < parts; ++c) l += partials[(size_t)c * kPartial + kWeights];
-        *loss = l;
+    } else if (threadIdx.x < (unsigned)kSumWeights && i == kWeights) {
+        *loss = g;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -787,19 +841,19 @@ uint32_t mlp_partial_floats() { return (uint32_t)mlp::kPartial; }
 cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
                              float* partials, uint32_t* error, uint32_t ctas, cudaStream_t s, uint32_t wait_polls) {
     if (batch == 0) return cudaSuccess;
-    mlp::train_kernel<<<mlp_train_parts(batch, ctas), mlp::kThreads, mlp::kTrainSmem, s>>>(features, targets, batch, image_f, image_b,
+    mlp::train_kernel<<<mlp_train_parts(batch, ctas), mlp::kTrainThreads, mlp::kTrainSmem, s>>>(features, targets, batch, image_f, image_b,
                                                                                            partials, error, wait_polls);
     return cudaGetLastError();
 }
 
 void launch_mlp_reduce(const float* partials, uint32_t parts, float* grads, float* loss, cudaStream_t s) {
-    mlp::reduce_kernel<<<(mlp::kWeights + 256) / 256, 256, 0, s>>>(partials, parts, grads, loss);
+    mlp::reduce_kernel<<<mlp::kSumBlocks, mlp::kSumThreads, 0, s>>>(partials, parts, grads, loss);
 }
 
 void launch_mlp_adam(float* master, float* m, float* v, const float* partials, uint32_t parts, float lr, float beta1, float beta2, float eps,
                      uint32_t* steps, uint8_t* image_f, uint8_t* image_b, float* loss, cudaStream_t s) {
-    mlp::adam_kernel<<<(mlp::kWeights + 256) / 256, 256, 0, s>>>(master, m, v, partials, parts, lr, beta1, beta2, eps, steps, image_f,
-                                                                  image_b, loss);
+    mlp::adam_kernel<<<mlp::kSumBlocks, mlp::kSumThreads, 0, s>>>(master, m, v, partials, parts, lr, beta1, beta2, eps, steps, image_f,
+                                                                   image_b, loss);
 }
 
 

@@ -264,6 +264,7 @@ _SIGNATURES = {
     "vgi_mlp_apply_gradients": (_INT, [_P, _P, ctypes.c_float, ctypes.c_float, _INT]),
     "vgi_mlp_encode": (_INT, [_P, _P, _U32, _P]),
     "vgi_set_mlp_cache": (_INT, [_P, ctypes.c_int, _U32, _U32, _U32, ctypes.c_float]),
+    "vgi_set_mlp_schedule": (_INT, [_P, _U32, ctypes.c_float]),
     "vgi_mlp_stats": (_INT, [_P, _P]),
     "vgi_frame_shard": (_INT, [_P, _U32, _U32, _U32, _U32]),
     "vgi_submit_batch": (_INT, [_P, _P, _U32, _U32, _U32, _P, _P]),
@@ -937,6 +938,12 @@ class GpuTracer:
         frame over `steps_per_frame` Adam steps, and after warm_frames
         frames the network ends uncached first hits."""
         self._check(self._lib.vgi_set_mlp_cache(self._h, 1 if enable else 0, warm_frames, samples, steps_per_frame, float(lr)))
+
+    def set_mlp_schedule(self, rows_per_step: int = 0, history_share: float = 0.0) -> None:
+        """MLP cache mode: rows of one Adam step (0: the frame's samples over
+        its steps) and the averaging window, a share of the samples taken
+        since the network began ending paths (0: the transport's limit)."""
+        self._check(self._lib.vgi_set_mlp_schedule(self._h, int(rows_per_step), float(history_share)))
 
     def mlp_stats(self) -> dict:
         st = MlpStatus()

@@ -380,6 +380,20 @@ int vgi_mlp_encode(vgi_ctx* ctx, const vgi_face* faces, uint32_t n, float* featu
  * faces of their own, 4 paths each. In the single-kernel layout frames trace
  * plainly. Resets the frame count; the weights and Adam state stay. */
 int vgi_set_mlp_cache(vgi_ctx* ctx, int enable, uint32_t warm_frames, uint32_t samples, uint32_t steps_per_frame, float lr);
+/* The MLP cache mode's training batches and averaging window. No
+ * counterpart in the reference.
+ * rows_per_step: the rows of one Adam step; 0 (the default) splits the
+ * frame's samples over its steps. A larger batch cycles through the
+ * frame's samples (step k starts at k x rows_per_step modulo the samples),
+ * so the frame takes the same steps on bigger batches of the same data.
+ * history_share: with share > 0, every frame in which the network ends
+ * paths caps the faces' sample count (the accumulation's history limit) at
+ * share x the samples a face has taken in such frames, this one included,
+ * and at least 32 (above the cache's binding count of 16), so the means
+ * weight late frames, whose network is trained, above the first ones; the
+ * transport's history limit still caps it. 0 (the default) keeps the
+ * transport's limit. */
+int vgi_set_mlp_schedule(vgi_ctx* ctx, uint32_t rows_per_step, float history_share);
 typedef struct vgi_mlp_status {
     uint32_t frames;       /* frames traced since vgi_set_mlp_cache */
     uint32_t steps;        /* Adam steps taken since vgi_mlp_set_weights */

@@ -176,10 +176,10 @@ def test_mlp_graph_frames_match_direct_frames(gpu):
             gpu.set_graph(False)
     (r0, w0, s0), (r1, w1, s1) = outs
     assert s0["steps"] == s1["steps"] == 5 and s0["error"] == s1["error"] == 0
-    # The weight gradients are summed with atomics, so their last bits vary;
-    # Adam turns a gradient within that noise of 0 into a step of up to lr
-    # either way, and the next frames train on what the moved network
-    # predicted. The two runs stay close as a whole.
+    # The frame's queries are queued by atomic appends, so the training
+    # rows drawn from the queue differ between runs; Adam turns a gradient
+    # near 0 into a step of up to lr either way, and the next frames train on
+    # what the moved network predicted. The two runs stay close as a whole.
     rel = np.linalg.norm(w0 - w1) / np.linalg.norm(w0)
     assert rel < 2e-2, rel
     g, w = r0[:, :3].view(np.float32), r1[:, :3].view(np.float32)
@@ -219,3 +219,37 @@ def test_trained_network_gains_over_the_method_without_it(gpu):
             gpu.set_mlp_cache(False)
     print("relMSE vs FP64:", errors)
     assert errors["mlp"] < 0.7 * errors["plain"], errors
+
+
+def test_mlp_schedule_refuses_bad_settings_caps_counts_and_cycles_batches(gpu):
+    """vgi_set_mlp_schedule: a history share outside [0, 1] or more than
+    2^22 rows a step is refused. With share 0.5 at 2 samples a frame, the
+    k-th frame the network answers caps every face's count at max(32, k);
+    faces traced every frame sit at the cap. Steps of 4,096 rows over a
+    frame's 4,096 samples (every step a full pass) take the frame's steps
+    without a tensor-core error."""
+    case = terrain_case(bounces=2)
+    case.load(gpu)
+    gpu.mlp_set_weights(random_weights(7))
+    for bad in ((0, -0.5), (0, 1.5), (1 << 23, 0.0)):
+        with pytest.raises(vgi.VgiError) as err:
+            gpu.set_mlp_schedule(*bad)
+        assert err.value.status == vgi.ERR_INVALID
+    spp, warm, frames = 2, 2, 40
+    gpu.set_mlp_cache(True, warm_frames=warm, samples=4096, steps_per_frame=2, lr=1e-3)
+    gpu.set_mlp_schedule(4096, 0.5)
+    try:
+        for f in range(warm + frames):
+            gpu.frame(spp, clock_ms=16 * f)
+            k = f - warm + 1
+            if k in (1, 20, 33, frames):
+                cap = max(32, int(np.ceil(0.5 * spp * k)))
+                counts = gpu.read_state()[:, 5] & 0x7fffffff
+                assert counts.max() <= cap, (k, counts.max(), cap)
+        assert (counts == frames).mean() > 0.5, np.bincount(counts)[-8:]
+        st = gpu.mlp_stats()
+        assert st["error"] == 0 and st["steps"] == 2 * (warm + frames) and np.isfinite(st["loss"])
+        assert np.isfinite(gpu.mlp_get_weights()).all()
+    finally:
+        gpu.set_mlp_cache(False)
+        gpu.set_mlp_schedule(0, 0.0)
