@@ -596,7 +596,7 @@ def cave_run(local, stream, flush, plain_frames=37):
 ROOM_SPP, ROOM_FRAMES = 4, 64
 
 
-def stone_room_run(local, stream):
+def stone_room_run(local):
     """The reference's stone-room fixture, run in full: the 32^3 room
     (8 regions) with its stone and emissive materials, every exposed face a
     world-cache slot, 4 paths a face a frame, 1 diffuse hit, 64 traversal
@@ -645,6 +645,8 @@ def stone_room_run(local, stream):
         shadow.frame(ROOM_SPP, 16 * f)
     shadow.close()
     g.set_graph(True)
+    # The events go on the room tracer's own stream, where its frames run.
+    stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     torch.cuda.synchronize()
     ev[0].record(stream)
@@ -1238,7 +1240,7 @@ def main():
         if args.batch_scenes > 0:
             batched = batch_comparison(local, stream, flush, args.batch_scenes, args.steps, args.warmup)
         beside = None if args.no_next_rows else next_rows(g, stream)
-        room = None if args.no_room else stone_room_run(local, stream)
+        room = None if args.no_room else stone_room_run(local)
         cave = None if args.no_cave else cave_run(local, stream, flush)
         line = {
             "metric": METRIC,
