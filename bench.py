@@ -100,6 +100,24 @@ def profiled_traffic():
     return None
 
 
+def profiled_stage_traffic():
+    """DRAM bytes per frame of the stage kernels (begin, shade, scatter,
+    finalize) from the committed ncu summary of the small terrain, per stage
+    launch and in all, with that terrain's face count for scaling."""
+    path = os.path.join(ROOT, "profiles", "wave_stages_terrain.md")
+    out = {}
+    try:
+        for line in open(path):
+            if line.startswith("stage_dram_bytes:"):
+                name, value = line.split(":", 1)[1].split("=")
+                out[name.strip()] = float(value)
+            elif line.startswith("stage_faces:"):
+                out["_faces"] = float(line.split(":")[1])
+    except OSError:
+        return None
+    return out if "_faces" in out and len(out) > 1 else None
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clocks and throttle reasons during timing."""
 
@@ -1222,6 +1240,20 @@ def main():
     # Dominant kernel: the persistent traversal (BOUNCES + 1 launches per frame).
     achieved = traverse_bytes / (traverse_ms * 1e-3) / 1e9
     traffic = profiled_traffic()
+    stage_traffic = None
+    stages = profiled_stage_traffic()
+    if stages:
+        # Scaled from the small terrain by faces (paths per face and bounces are the bench's).
+        scale = n / stages["_faces"]
+        per_stage = {k: v * scale for k, v in stages.items() if k != "_faces"}
+        algorithmic = bytes_per_frame - traverse_bytes
+        stage_traffic = {"dram_bytes_per_frame": per_stage, "dram_bytes_per_frame_total": sum(per_stage.values()),
+                         "algorithmic_bytes_per_frame": algorithmic,
+                         "traffic_over_algorithmic": sum(per_stage.values()) / algorithmic,
+                         "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one frame's stage launches on the "
+                                   "256x128x256 terrain (profiles/wave_stages_terrain.md), scaled by faces",
+                         "algorithmic": "the frame's algorithmic bytes outside the traversal (counting pass: tasks, results, "
+                                        "materials, lights, emitter and tree reads, face-index probes, accepted cache states)"}
     # The whole frame's algorithmic bytes per second.
     frame_bytes = bytes_per_frame + n * (2 * 144 + 48)
     frame_gbs = frame_bytes / (total_ms / args.steps * 1e-3) / 1e9
@@ -1286,6 +1318,7 @@ def main():
                               "state read and write (2 x 144 B) and checkpoint (48 B) per face, over the CUDA-event frame time",
                 "note": "most of these bytes hit L2 (the geometry, face index and gather records stay resident); the DRAM traffic "
                         "of the frame's kernels is about a third of them (profiles)"},
+            "stage_traffic": stage_traffic,
             "clocks": clocks,
             "relmse": quality,
             "mlp_cache": mlp,
