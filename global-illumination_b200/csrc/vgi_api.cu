@@ -158,6 +158,10 @@ struct vgi_ctx {
     float env[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     DevBuf<uint4> emitters;
     DevBuf<float4> node_aux;
+    // Per slot, the light tree's top child probabilities at its receiver
+    // (TraceArgs::tree_rows), checked against the generation of the tree.
+    DevBuf<uint4> tree_rows;
+    uint32_t tree_generation = 1;
     float emitter_count = 0.0f, emitter_total = 0.0f;
     vgi_transport transport{};
 
@@ -396,6 +400,9 @@ TraceArgs trace_args(vgi_ctx* c, const uint4* tasks, uint4* results, uint32_t n,
     a.region_grid = c->has_grid ? c->grid.ptr : nullptr;
     a.region_headers = c->has_grid ? c->grid_headers.ptr : nullptr;
     a.face_index = with_cache ? c->face_index.ptr : nullptr;
+    // The kept tree rows follow the context's own face tasks only.
+    a.tree_rows = tasks == c->tasks.ptr ? c->tree_rows.ptr : nullptr;
+    a.tree_generation = c->tree_generation;
     a.cache = with_cache ? c->cache.ptr : nullptr;
     a.tasks = tasks;
     a.results = results;
@@ -691,7 +698,7 @@ int vgi_destroy(vgi_ctx* c) {
     drop_graph(c);
     c->directory.release(); c->headers.release(); c->cells.release(); c->voxels.release(); c->alloc.release();
     c->pack_error.release(); c->edit_buf.release(); c->zw.release(); c->region_list.release(); c->dedup_table.release();
-    c->materials.release(); c->lights.release(); c->emitters.release(); c->node_aux.release();
+    c->materials.release(); c->lights.release(); c->emitters.release(); c->node_aux.release(); c->tree_rows.release();
     c->tasks.release(); c->results.release(); c->state.release(); c->slot_meta.release(); c->checkpoint.release();
     c->face_index.release(); c->cache.release(); c->grid.release(); c->scratch_tasks.release(); c->scratch_results.release(); c->events.release();
     c->material_light.release(); c->measures.release(); c->measure_max.release();
@@ -1355,6 +1362,7 @@ int vgi_set_emitters(vgi_ctx* c, const uint32_t* words, uint64_t n_words, uint32
     const uint32_t nodes = (uint32_t)((n_words - records * 8) / 16);
     VGI_CUDA(c, c->node_aux.reserve(2 * (size_t)std::max<uint32_t>(nodes, 1)));
     launch_node_aux(c->emitters.ptr, (uint32_t)(records * 2), nodes, c->node_aux.ptr, c->stream);
+    c->tree_generation += 1u;  // every kept tree row is stale now
     VGI_CUDA(c, cudaGetLastError());
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->emitter_count = (float)n_faces;
@@ -1410,6 +1418,7 @@ int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, c->slot_meta.reserve(m * 3));
     VGI_CUDA(c, c->checkpoint.reserve(m * 3));
     VGI_CUDA(c, c->cache.reserve(m));
+    VGI_CUDA(c, c->tree_rows.reserve(m * kTreeRowWords));
     VGI_CUDA(c, c->face_index.reserve(index.size() / 4));
     VGI_CUDA(c, h2d(c->tasks.ptr, tasks.data(), (size_t)n * 32, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->results.ptr, 0, m * 96, c->stream));
@@ -1418,6 +1427,7 @@ int vgi_set_faces(vgi_ctx* c, const vgi_face* faces, uint32_t n) {
     VGI_CUDA(c, h2d(c->slot_meta.ptr, meta.data(), (size_t)n * 48, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->checkpoint.ptr, 0, m * 48, c->stream));
     VGI_CUDA(c, cudaMemsetAsync(c->cache.ptr, 0, m * 16, c->stream));
+    VGI_CUDA(c, cudaMemsetAsync(c->tree_rows.ptr, 0xff, m * kTreeRowWords * 16, c->stream));  // no key matches
     VGI_CUDA(c, h2d(c->face_index.ptr, index.data(), index.size() * 4, c->stream));
     VGI_CUDA(c, cudaStreamSynchronize(c->stream));
     c->n_slots = n;

@@ -371,9 +371,13 @@ __device__ float node_left_probability(const TraceArgs& A, uint32_t left_index, 
     return wclamp(__fadd_rn(__fmul_rn(0.05f, power), __fdiv_rn(__fmul_rn(0.95f, a), __fadd_rn(a, b))), 1e-6f, 0.999999f);
 }
 
+// `top`, when given, holds node_left_probability of the nodes at heap slots
+// 0..kTreeTopSlots-1 (slot s's children at 2s + 1 and 2s + 2) for this
+// position and normal, as wave_begin_kernel keeps them per receiver: the
+// same values, so the walk takes the same branches.
 template <bool C>
-__device__ Emissive tree_emitter(const TraceArgs& A, V3 position, V3 normal, float choice, Cnt<C>& cnt) {
-    uint32_t index = 0;
+__device__ Emissive tree_emitter(const TraceArgs& A, V3 position, V3 normal, float choice, Cnt<C>& cnt, const float* top = nullptr) {
+    uint32_t index = 0, slot = 0;
     float u = choice, probability = 1.0f;
     // Median splits keep the hierarchy balanced (depth <= 33); the host
     // checks that children follow their parent, so the walk ends. The bound
@@ -387,19 +391,40 @@ __device__ Emissive tree_emitter(const TraceArgs& A, V3 position, V3 normal, flo
             e.sampling.y = probability;
             return e;
         }
-        float p = node_left_probability(A, link.z, link.w, position, normal, cnt);
+        const float p = (top != nullptr && slot < kTreeTopSlots) ? top[slot] : node_left_probability(A, link.z, link.w, position, normal, cnt);
         if (u < p) {
             probability = __fmul_rn(probability, p);
             u = __fdiv_rn(u, p);
             index = link.z;
+            slot = slot < kTreeTopSlots ? 2u * slot + 1u : kTreeTopSlots;
         } else {
             probability = __fmul_rn(probability, __fsub_rn(1.0f, p));
             u = __fdiv_rn(__fsub_rn(u, p), __fsub_rn(1.0f, p));
             index = link.w;
+            slot = slot < kTreeTopSlots ? 2u * slot + 2u : kTreeTopSlots;
         }
         u = wmin(u, __uint_as_float(0x3f7fffffu));
     }
     return Emissive{I3{0, 0, 0}, 0u, make_float4(0.0f, 0.0f, 0.0f, 0.0f)};
+}
+
+// node_left_probability of the node at heap slot `slot` of the walk (the
+// bits of slot + 1 below its leading one, from the top: 0 left, 1 right),
+// or -1 when the walk never asks there (a leaf on the way, or the slot's
+// node is a leaf).
+__device__ float tree_slot_probability(const TraceArgs& A, uint32_t slot, V3 position, V3 normal) {
+    Cnt<false> none;
+    const uint32_t path = slot + 1u;
+    const int depth = 31 - __clz(path);
+    uint32_t index = 0;
+    for (int b = depth - 1; b >= 0; --b) {
+        const uint4 link = __ldg(reinterpret_cast<const uint4*>(A.node_aux) + 2u * index + 1u);
+        if (link.z == 0xffffffffu) return -1.0f;
+        index = ((path >> b) & 1u) ? link.w : link.z;
+    }
+    const uint4 link = __ldg(reinterpret_cast<const uint4*>(A.node_aux) + 2u * index + 1u);
+    if (link.z == 0xffffffffu) return -1.0f;
+    return node_left_probability(A, link.z, link.w, position, normal, none);
 }
 
 __device__ __forceinline__ int comp(I3 v, uint32_t i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }

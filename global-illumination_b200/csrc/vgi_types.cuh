@@ -42,7 +42,18 @@ struct TraceArgs {
     uint32_t path_steps;       // PATH_STEPS
     uint32_t lanes_log2;       // threads per face = 1 << lanes_log2
     unsigned long long* counters;  // 10 counters (counting variant only)
+    // Per task, the light tree's left-child probabilities of the top
+    // kTreeTopSlots nodes at the face's receiver point (null: none kept),
+    // valid while the row's key equals the task's first word and the tree
+    // generation (kTreeRowWords uint4 a task; see wave_begin_kernel).
+    uint4* tree_rows;
+    uint32_t tree_generation;
 };
+
+// The cached top of the light tree: heap slots 0..30 (depths 0-4), in a row
+// of a key (the task's first word), the generation, and 32 floats.
+constexpr uint32_t kTreeTopSlots = 31;
+constexpr uint32_t kTreeRowWords = 10;
 
 struct AccumArgs {
     uint4* state;         // 9 uint4 per slot

@@ -143,7 +143,7 @@ struct WaveTracer {
     // true with the ray and the value it would add (emission * factor) when a
     // ray is needed; the material is counted when the ray turns out visible.
     __device__ bool prepare_nee(V3 position, V3 normal, uint32_t source_stream, uint32_t sequence, uint32_t bounce, V3& so, V3& sdir,
-                                float& sdist, V3& pending) {
+                                float& sdist, V3& pending, const float* top = nullptr) {
         if (A.emitter_count == 0.0f) return false;
         uint32_t stream = source_stream ^ pcg(bounce + 0xa341316cu);
         // choose_emitter (voxel_path.wgsl:309-324)
@@ -152,7 +152,7 @@ struct WaveTracer {
             const float choice = sample_1d(stream, sequence, 12u);
             uint32_t count = f2u(A.emitter_count);
             if (load_emitter(A, 0u, cnt).sampling.w > 0.0f) {
-                em = tree_emitter(A, position, normal, choice, cnt);
+                em = tree_emitter(A, position, normal, choice, cnt, top);
             } else {
                 uint32_t low = 0, high = count;
 #pragma unroll 1
@@ -377,13 +377,44 @@ __global__ void __launch_bounds__(kWaveBlock, VGI_BEGIN_MIN_BLOCKS) wave_begin_k
     const uint32_t base = p * W.slots;
     uint32_t flags = valid ? kFlagValid : 0u;
     bool s0 = false, c0 = false;
+    // The receiver's position and normal are the task's, the same every
+    // frame, so the light tree's child probabilities on the top levels of
+    // its NEE walk are too. A face keeps them in its row (the timed passes;
+    // the counting pass walks as the reference does, to count the node
+    // reads): on a miss (new face, new tree) the face's lanes compute the
+    // row's slots between them, then every lane walks from it. The face's
+    // lanes share a warp when the sample count divides 32.
+    const float* top = nullptr;
+    if constexpr (!C) {
+        if (A.tree_rows != nullptr && A.samples != 0u && 32u % A.samples == 0u) {
+            uint4* row = A.tree_rows + (size_t)face * kTreeRowWords;
+            const bool tree = valid && A.emitter_count != 0.0f && __uint_as_float(__ldg(A.emitters + 1u).w) > 0.0f;
+            bool miss = false;
+            if (tree) {
+                const uint4 key = row[0];
+                miss = key.x != t0.x || key.y != t0.y || key.z != t0.z || key.w != t0.w || row[1].x != A.tree_generation;
+                if (miss) {
+                    float* slots = reinterpret_cast<float*>(row + 2);
+                    for (uint32_t j = sample; j < kTreeTopSlots; j += A.samples) slots[j] = tree_slot_probability(A, j, surface, normal);
+                }
+            }
+            __syncwarp();
+            if (tree) {
+                if (miss && sample == 0u) {
+                    row[0] = t0;
+                    row[1] = make_uint4(A.tree_generation, 0u, 0u, 0u);
+                }
+                top = reinterpret_cast<const float*>(row + 2);
+            }
+        }
+    }
     if (valid) {
         cnt.path();
         if (sample == 0u) cnt.bytes(32 + 96);
         V3 direction = hemisphere(normal, sample_1d(stream, sequence, 0u), sample_1d(stream, sequence, 1u));
         V3 so, sd, pending;
         float sdist;
-        s0 = T.prepare_nee(surface, normal, stream, sequence, 0u, so, sd, sdist, pending);
+        s0 = T.prepare_nee(surface, normal, stream, sequence, 0u, so, sd, sdist, pending, top);
         if (s0) {
             put_ray(W, base + 1u, so, sd, sdist, 0u);
             flags |= kFlagS0;
