@@ -569,8 +569,10 @@ def cave_run(local, stream, flush, plain_frames=37):
         t.set_faces(f)
         t.mlp_set_weights(init)
         share = max(MLP_STEPS * 128, int(MLP_SAMPLES * len(f) / sum(n_faces)))
+        # Each chunk's network trains on its share of the frame's samples
+        # (2k-7k), split over the steps: cycling such small batches through
+        # bigger steps, as the terrain's 65,536 samples do, measured worse here.
         t.set_mlp_cache(True, warm_frames=MLP_WARM, samples=share, steps_per_frame=MLP_STEPS, lr=MLP_LR)
-        t.set_mlp_schedule(min(share, max(128, MLP_STEP_ROWS * share // MLP_SAMPLES)), MLP_HISTORY)
     batch = vgi.GpuBatch(tracers)
     batch.set_graph(True)
     mlp_ms, curve, reached = [], [], None
