@@ -243,6 +243,7 @@ def mlp_comparison(g, faces, ref, stream, flush, plain, clock, max_frames):
     target = plain["relmse"]
     curve, frame_ms, reached = [], [], None
     at_equal_frames = at_equal_time = None
+    near = False
     total = 0.0
     for f in range(max_frames):
         with torch.cuda.stream(stream):
@@ -257,9 +258,12 @@ def mlp_comparison(g, faces, ref, stream, flush, plain, clock, max_frames):
         e.synchronize()
         frame_ms.append(s.elapsed_time(e))
         total += frame_ms[-1]
-        every = 2 if f < 64 else 4
+        # relMSE is read every 2 frames, every 4 after 64, and every frame
+        # once within 15% of the target, so the frame that reaches it is exact.
+        every = 1 if near else (2 if f < 64 else 4)
         value = relmse_now(g, ref) if (f + 1) % every == 0 or f + 1 == plain["frames"] else None
         if value is not None:
+            near = value <= 1.15 * target
             curve.append([f + 1, round(total, 2), round(value, 6)])
             if f + 1 == plain["frames"]:
                 at_equal_frames = value
