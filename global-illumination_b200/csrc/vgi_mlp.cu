@@ -551,13 +551,16 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(const float* featu
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t r = tid & (kRows - 1u), half = tid >> 7, col0 = half * 32u;
     const uint32_t bar_addr = smem_u32(bar), s0 = smem_u32(smem);
+    // Launched after the previous step's Adam as a programmatic dependent:
+    // the set-up below (barrier, zeroed tiles, TMEM) overlaps that kernel,
+    // and griddepcontrol.wait holds every read of its outputs (the weight
+    // images) and of the batch until it has finished. The next kernel may
+    // begin its own set-up as soon as every CTA here has started.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (tid == 0) {
         *abort_flag = 0u;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_addr), "r"(1u));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        bulk_expect(bar_addr, 2u * kImageBytes);
-        bulk_load(s0 + kWF, image_f, kImageBytes, bar_addr);
-        bulk_load(s0 + kWB, image_b, kImageBytes, bar_addr);
     }
     // Zero the transposed tiles once: rows past a tile's real features are
     // read by the M = 128 products.
@@ -565,6 +568,12 @@ __global__ void __launch_bounds__(kTrainThreads) train_kernel(const float* featu
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTrainColumns));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (tid == 0) {
+        bulk_expect(bar_addr, 2u * kImageBytes);
+        bulk_load(s0 + kWF, image_f, kImageBytes, bar_addr);
+        bulk_load(s0 + kWB, image_b, kImageBytes, bar_addr);
     }
     fence_before();
     __syncthreads();
@@ -796,6 +805,12 @@ __global__ void __launch_bounds__(kSumThreads) adam_kernel(float* master, float*
                                                           float beta1, float beta2, float eps, uint32_t* steps, uint8_t* image_f,
                                                           uint8_t* image_b, float* loss) {
     __shared__ float scratch[kSumGroups][kSumWeights];
+    // A programmatic dependent of the training kernel: nothing it wrote (the
+    // partial rows) or the step before it changed is read before
+    // griddepcontrol.wait, and the next step's training kernel may begin its
+    // set-up once every block here has started.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int i = blockIdx.x * kSumWeights + (int)(threadIdx.x % kSumWeights);
     const uint32_t step = steps[0] + 1u;
     const float g = sum_partials(partials, parts, i, scratch);
@@ -838,12 +853,29 @@ uint32_t mlp_train_parts(uint32_t batch, uint32_t ctas) {
 
 uint32_t mlp_partial_floats() { return (uint32_t)mlp::kPartial; }
 
+// A launch that may begin while the kernel before it on the stream is still
+// running (programmatic dependent launch); the kernel waits for it with
+// griddepcontrol.wait before reading anything it wrote.
+template <typename... Params, typename... Args>
+static cudaError_t launch_dependent(void (*kernel)(Params...), uint32_t grid, uint32_t block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+}
+
 cudaError_t launch_mlp_train(const float* features, const float4* targets, uint32_t batch, const uint8_t* image_f, const uint8_t* image_b,
                              float* partials, uint32_t* error, uint32_t ctas, cudaStream_t s, uint32_t wait_polls) {
     if (batch == 0) return cudaSuccess;
-    mlp::train_kernel<<<mlp_train_parts(batch, ctas), mlp::kTrainThreads, mlp::kTrainSmem, s>>>(features, targets, batch, image_f, image_b,
-                                                                                           partials, error, wait_polls);
-    return cudaGetLastError();
+    return launch_dependent(mlp::train_kernel, mlp_train_parts(batch, ctas), mlp::kTrainThreads, (size_t)mlp::kTrainSmem, s, features, targets,
+                            batch, image_f, image_b, partials, error, wait_polls);
 }
 
 void launch_mlp_reduce(const float* partials, uint32_t parts, float* grads, float* loss, cudaStream_t s) {
@@ -852,8 +884,8 @@ void launch_mlp_reduce(const float* partials, uint32_t parts, float* grads, floa
 
 void launch_mlp_adam(float* master, float* m, float* v, const float* partials, uint32_t parts, float lr, float beta1, float beta2, float eps,
                      uint32_t* steps, uint8_t* image_f, uint8_t* image_b, float* loss, cudaStream_t s) {
-    mlp::adam_kernel<<<mlp::kSumBlocks, mlp::kSumThreads, 0, s>>>(master, m, v, partials, parts, lr, beta1, beta2, eps, steps, image_f,
-                                                                   image_b, loss);
+    launch_dependent(mlp::adam_kernel, (uint32_t)mlp::kSumBlocks, (uint32_t)mlp::kSumThreads, 0, s, master, m, v, partials, parts, lr, beta1,
+                     beta2, eps, steps, image_f, image_b, loss);
 }
 
 
