@@ -334,3 +334,29 @@ def test_edits_match_oracle(gpu):
         d, h, cl, bounds = gpu.geometry()
         rd, rh, rcl, _ = ref.arrays()
         assert_words_equal(O.canonical(d, h, cl, case.coords), O.canonical(rd, rh, rcl, case.coords), f"geometry after edit {step}")
+
+
+@pytest.mark.parametrize("samples", [1, 3, 8, 32])
+def test_kept_light_tree_rows_follow_sample_counts_and_tree_changes(gpu, samples):
+    """The begin kernel keeps each face's top light-tree probabilities across
+    frames (filled by the face's lanes between them; not kept when the
+    sample count does not divide 32). Frames with 1, 3, 8 and 32 samples
+    match the oracle word for word, and so do frames after the emitters
+    change (new emission, so a new tree and stale rows)."""
+    case = terrain_case(bounces=1)
+    ref = run_frames(gpu, case, 2, samples)
+    assert_words_equal(gpu.read_results(), ref.results, f"frame results, {samples} samples")
+    # New emission on the emissive materials: new emitter weights and tree.
+    words = case.materials.copy().reshape(-1, 16)
+    words[8:, 4:7] *= 1.5
+    case.materials = words.reshape(-1)
+    case.emitters, case.n_emit, case.total = vgi.host_emitters(case.coords, case.vox, case.materials)
+    gpu.set_materials(case.materials)
+    gpu.build_emitters()
+    geometry = gpu.geometry()
+    ref.params_fn, ref.emitter_words, ref.materials = case.params_fn(geometry), case.emitters, case.materials
+    for f in range(2, 4):
+        gpu.frame(samples, clock_ms=16 * f)
+        ref.frame(samples, clock_ms=16 * f)
+    assert_words_equal(gpu.read_results(), ref.results, f"frame results after the tree changed, {samples} samples")
+    assert_words_equal(gpu.read_state(), ref.state, f"resident state after the tree changed, {samples} samples")
