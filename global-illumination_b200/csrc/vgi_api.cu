@@ -400,8 +400,13 @@ TraceArgs trace_args(vgi_ctx* c, const uint4* tasks, uint4* results, uint32_t n,
     a.region_grid = c->has_grid ? c->grid.ptr : nullptr;
     a.region_headers = c->has_grid ? c->grid_headers.ptr : nullptr;
     a.face_index = with_cache ? c->face_index.ptr : nullptr;
-    // The kept tree rows follow the context's own face tasks only.
-    a.tree_rows = tasks == c->tasks.ptr ? c->tree_rows.ptr : nullptr;
+    // The kept tree rows follow the context's own face tasks only (a shard
+    // of them from its first task's row).
+    a.tree_rows = nullptr;
+    if (tasks && c->tree_rows.ptr && tasks >= c->tasks.ptr && tasks < c->tasks.ptr + (size_t)c->n_slots * 2) {
+        const size_t first = (size_t)(tasks - c->tasks.ptr);
+        if (first % 2 == 0) a.tree_rows = c->tree_rows.ptr + first / 2 * kTreeRowWords;
+    }
     a.tree_generation = c->tree_generation;
     a.cache = with_cache ? c->cache.ptr : nullptr;
     a.tasks = tasks;
