@@ -50,10 +50,10 @@ struct TraceArgs {
     uint32_t tree_generation;
 };
 
-// The cached top of the light tree: heap slots 0..30 (depths 0-4), in a row
-// of a key (the task's first word), the generation, and 32 floats.
-constexpr uint32_t kTreeTopSlots = 31;
-constexpr uint32_t kTreeRowWords = 10;
+// The cached top of the light tree: heap slots 0..62 (depths 0-5), in a row
+// of a key (the task's first word), the generation, and 64 floats.
+constexpr uint32_t kTreeTopSlots = 63;
+constexpr uint32_t kTreeRowWords = 18;
 
 struct AccumArgs {
     uint4* state;         // 9 uint4 per slot
