@@ -2514,7 +2514,7 @@ int vgi_mlp_set_weights(vgi_ctx* c, const float* master, uint32_t count) {
     int sms = 148;
     VGI_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
     c->mlp_sms = (uint32_t)sms;
-    c->mlp_ctas = (uint32_t)sms * 3u;  // 62 KB of shared memory per forward CTA
+    c->mlp_ctas = (uint32_t)sms * 2u;  // 110 KB of shared memory per forward CTA (three 128-row groups)
     VGI_CUDA(c, c->mlp_partials.reserve((size_t)sms * mlp_partial_floats()));
     VGI_CUDA(c, c->mlp_adam.reserve((size_t)count * 2));
     VGI_CUDA(c, c->mlp_grads.reserve((size_t)count + 1));

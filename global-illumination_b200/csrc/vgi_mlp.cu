@@ -34,7 +34,6 @@ constexpr int kOut = 16;      // 3 used
 constexpr int kLayers = 5;
 constexpr int kRows = 128;    // queries per tile (MMA M)
 constexpr int kThreads = 128;
-constexpr int kTmemColumns = 64;
 
 __host__ __device__ constexpr int in_dim(int l) { return l == 0 ? kIn : kHidden; }
 __host__ __device__ constexpr int out_dim(int l) { return l == kLayers - 1 ? kOut : kHidden; }
@@ -48,7 +47,6 @@ __host__ __device__ constexpr int weight_offset(int l) {
 constexpr int kWeights = weight_offset(kLayers);          // 19456
 constexpr int kImageBytes = kWeights * 2;                 // 38912
 constexpr int kABytes = kRows * kIn * 2;                  // 24576
-constexpr int kSmemBytes = kImageBytes + kABytes + 64;    // + mbarrier, TMEM slot, flags
 
 // Byte offset of element (row n, column k) of an N x K K-major tile in the
 // no-swizzle canonical layout.
@@ -286,83 +284,108 @@ struct PathQueries {
 
 // The forward pass of CTA `cta` of `ctas` over `rows`' 128-row tiles, with
 // the network in `image` (the kernels below give each CTA its rows).
+//
+// A CTA holds one copy of the weight image and kGroups groups of 128
+// threads. Each group runs its own tiles (worker cta * kGroups + group of
+// ctas * kGroups) with its own A tile, mbarrier and 64 TMEM columns, and
+// synchronises on its own named barrier, so one group's epilogue overlaps
+// another's MMAs. Sharing the image lets 2 CTAs, 6 tiles, be in flight per
+// SM where one group per CTA fitted 3.
+constexpr int kGroups = 3;
+constexpr int kForwardThreads = kThreads * kGroups;                         // 384
+constexpr int kForwardTmem = 256;                                           // kGroups x 64 columns, a power of two
+constexpr int kForwardSmem = kImageBytes + kGroups * kABytes + 64;          // + mbarriers, TMEM slot, flags
+static_assert(kGroups * 64 <= kForwardTmem && 2 * kForwardTmem <= 512, "two CTAs' TMEM per SM");
+static_assert(2 * (kForwardSmem + 1024) <= 233472, "two CTAs' shared memory per SM");
+
+__device__ __forceinline__ void group_sync(uint32_t group) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1u + group), "r"((uint32_t)kThreads) : "memory");
+}
+
 template <class Rows>
 __device__ __forceinline__ void forward_tiles(const Rows& rows, const uint8_t* image, uint32_t cta, uint32_t ctas, uint32_t* error,
                                               uint32_t wait_polls) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* weights = smem;
-    uint8_t* tile = smem + kImageBytes;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kImageBytes + kABytes);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kImageBytes + kABytes + 8);
-    uint32_t* abort_flag = reinterpret_cast<uint32_t*>(smem + kImageBytes + kABytes + 12);
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, group = tid / kThreads, gtid = tid % kThreads;
+    uint8_t* tile = smem + kImageBytes + group * kABytes;
+    // bars[0]: the weight copy; bars[1 + g]: group g's MMAs. flags likewise.
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kImageBytes + kGroups * kABytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 1 + kGroups);
+    uint32_t* flags = tmem_slot + 1;
     const uint32_t n = rows.count();
     const uint32_t tiles = (n + kRows - 1) / kRows;
-    if (cta >= tiles) return;  // uniform per CTA: nothing allocated yet
+    if (cta * kGroups >= tiles) return;  // uniform per CTA: nothing allocated yet
 
-    const uint32_t bar_addr = smem_u32(bar);
     if (tid == 0) {
-        *abort_flag = 0u;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_addr), "r"(1u));
+        for (int g = 0; g <= kGroups; ++g) {
+            flags[g] = 0u;
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bars + g)), "r"(1u));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        bulk_expect(bar_addr, kImageBytes);
-        bulk_load(smem_u32(weights), image, kImageBytes, bar_addr);
+        bulk_expect(smem_u32(bars), kImageBytes);
+        bulk_load(smem_u32(weights), image, kImageBytes, smem_u32(bars));
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTmemColumns));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kForwardTmem));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     fence_before();
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t lane_base = tmem + ((warp * 32u) << 16);
-    // The weight image (phase 0 of the mbarrier), then one phase per layer.
-    if (!bar_wait(bar_addr, 0u, wait_polls)) give_up(bar_addr, 0u, abort_flag, error);
-    uint32_t phase = 1;
+    const uint32_t group_tmem = tmem + group * 64u;
+    const uint32_t lane_base = group_tmem + (((warp & 3u) * 32u) << 16);
+    // The weight image (phase 0 of bars[0]).
+    if (!bar_wait(smem_u32(bars), 0u, wait_polls)) give_up(smem_u32(bars), 0u, flags, error);
     __syncthreads();
-    const uint32_t first_tile = *abort_flag ? tiles : cta;
+    const uint32_t bar = smem_u32(bars + 1 + group);
+    uint32_t* abort_flag = flags + 1 + group;
+    uint32_t phase = 0;
+    const uint32_t workers = ctas * kGroups;
+    const uint32_t first_tile = flags[0] ? tiles : cta * kGroups + group;
 
-    for (uint32_t t = first_tile; t < tiles; t += ctas) {
-        const uint32_t row = t * kRows + tid;
-        rows.stage(tile, tid, row);
+    for (uint32_t t = first_tile; t < tiles; t += workers) {
+        const uint32_t row = t * kRows + gtid;
+        rows.stage(tile, gtid, row);
         bool ok = true;
         for (int l = 0; l < kLayers && ok; ++l) {
             const uint32_t K = in_dim(l), N = out_dim(l);
             fence_async_smem();
             fence_before();
-            __syncthreads();
-            if (tid == 0) {
+            group_sync(group);
+            if (gtid == 0) {
                 fence_after();
                 const uint32_t a0 = smem_u32(tile), b0 = smem_u32(weights + weight_offset(l) * 2);
                 const uint32_t idesc = instr_desc(N);
                 for (uint32_t kk = 0; kk < K / 16u; ++kk)
-                    mma_bf16(tmem, matrix_desc(a0 + kk * 256u, 128u, (K / 8u) * 128u), matrix_desc(b0 + kk * 256u, 128u, (K / 8u) * 128u),
-                             idesc, kk > 0 ? 1u : 0u);
-                mma_commit(bar_addr);
+                    mma_bf16(group_tmem, matrix_desc(a0 + kk * 256u, 128u, (K / 8u) * 128u),
+                             matrix_desc(b0 + kk * 256u, 128u, (K / 8u) * 128u), idesc, kk > 0 ? 1u : 0u);
+                mma_commit(bar);
             }
-            if (!bar_wait(bar_addr, phase, wait_polls)) give_up(bar_addr, phase, abort_flag, error);
+            if (!bar_wait(bar, phase, wait_polls)) give_up(bar, phase, abort_flag, error);
             phase ^= 1u;
-            __syncthreads();
+            group_sync(group);
             if (*abort_flag) {
                 ok = false;
                 break;
             }
             fence_after();
             if (l + 1 < kLayers) {
-                // The row's TMEM loads all in flight, then one wait.
-                float v[64];
+                // The row in two halves of 32 columns: each half's TMEM
+                // loads in flight, then one wait (two CTAs per SM leave 85
+                // registers a thread).
 #pragma unroll
-                for (uint32_t c0 = 0; c0 < 64u; c0 += 16u)
-                    if (c0 < N) tmem_ld16(lane_base + c0, v + c0);
-                tmem_wait_ld();
+                for (uint32_t h = 0; h < 64u; h += 32u) {
+                    if (h >= N) continue;
+                    float v[32];
+                    tmem_ld16(lane_base + h, v);
+                    tmem_ld16(lane_base + h + 16u, v + 16);
+                    tmem_wait_ld();
 #pragma unroll
-                for (uint32_t c0 = 0; c0 < 64u; c0 += 16u) {
-                    if (c0 >= N) continue;
+                    for (int j = 0; j < 32; ++j) v[j] = v[j] > 0.0f ? v[j] : 0.0f;
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) v[c0 + j] = v[c0 + j] > 0.0f ? v[c0 + j] : 0.0f;
-                    store8(tile, tid, c0 / 8u, N, v + c0);
-                    store8(tile, tid, c0 / 8u + 1u, N, v + c0 + 8);
+                    for (uint32_t c = 0; c < 4u; ++c) store8(tile, gtid, h / 8u + c, N, v + c * 8u);
                 }
             } else {
                 float v[16];
@@ -375,11 +398,11 @@ __device__ __forceinline__ void forward_tiles(const Rows& rows, const uint8_t* i
     }
     fence_before();
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kForwardTmem));
 }
 
 template <class Rows>
-__global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, const uint8_t* image, uint32_t* error, uint32_t wait_polls) {
+__global__ void __launch_bounds__(kForwardThreads, 2) forward_kernel(const Rows rows, const uint8_t* image, uint32_t* error, uint32_t wait_polls) {
     forward_tiles(rows, image, blockIdx.x, gridDim.x, error, wait_polls);
 }
 
@@ -390,7 +413,7 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(const Rows rows, cons
 // that scene's tiles. Every row's prediction is the one the scene's own
 // query launch gives: a row's outputs depend on its inputs and the weights
 // only, whatever tile it lands in.
-__global__ void __launch_bounds__(kThreads) forward_scenes_kernel(const MlpSceneQueries* scenes, uint32_t n_scenes, uint32_t wait_polls) {
+__global__ void __launch_bounds__(kForwardThreads, 2) forward_scenes_kernel(const MlpSceneQueries* scenes, uint32_t n_scenes, uint32_t wait_polls) {
     uint32_t lo = 0, hi = n_scenes - 1u;
     while (lo < hi) {
         const uint32_t mid = (lo + hi + 1u) >> 1;
@@ -893,12 +916,12 @@ void launch_mlp_queries(const float4* queue, const uint32_t* count, uint32_t cap
                         float4* out, uint32_t* error, uint32_t ctas, cudaStream_t s, uint32_t wait_polls) {
     if (capacity == 0) return;
     const mlp::PathQueries rows{queue, count, capacity, enc, out};
-    mlp::forward_kernel<mlp::PathQueries><<<ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error, wait_polls);
+    mlp::forward_kernel<mlp::PathQueries><<<ctas, mlp::kForwardThreads, mlp::kForwardSmem, s>>>(rows, image, error, wait_polls);
 }
 
 void launch_mlp_scene_queries(const MlpSceneQueries* scenes, uint32_t n_scenes, uint32_t ctas, cudaStream_t s, uint32_t wait_polls) {
     if (n_scenes == 0 || ctas == 0) return;
-    mlp::forward_scenes_kernel<<<ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(scenes, n_scenes, wait_polls);
+    mlp::forward_scenes_kernel<<<ctas, mlp::kForwardThreads, mlp::kForwardSmem, s>>>(scenes, n_scenes, wait_polls);
 }
 
 void launch_mlp_encode_training(const uint4* slot_meta, const uint4* results, const float4* materials, uint32_t n_slots,
@@ -926,11 +949,11 @@ void launch_mlp_query_targets(const uint4* results, uint32_t n, float4* targets,
 // Raises the dynamic shared-memory limit of the MLP kernels; called once per
 // context before their first launch (outside any stream capture).
 cudaError_t mlp_set_attributes() {
-    cudaError_t e = cudaFuncSetAttribute(mlp::forward_kernel<mlp::FeatureRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
+    cudaError_t e = cudaFuncSetAttribute(mlp::forward_kernel<mlp::FeatureRows>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kForwardSmem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(mlp::forward_kernel<mlp::PathQueries>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
+        e = cudaFuncSetAttribute(mlp::forward_kernel<mlp::PathQueries>, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kForwardSmem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(mlp::forward_scenes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kSmemBytes);
+        e = cudaFuncSetAttribute(mlp::forward_scenes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kForwardSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(mlp::train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
     return e;
 }
@@ -943,9 +966,10 @@ cudaError_t launch_mlp_forward(const float* features, const uint8_t* image, floa
                                cudaStream_t s, uint32_t wait_polls) {
     if (n == 0) return cudaSuccess;
     const uint32_t tiles = (n + mlp::kRows - 1) / mlp::kRows;
+    const uint32_t need = (tiles + mlp::kGroups - 1) / mlp::kGroups;  // CTAs with a tile for their first group
     const mlp::FeatureRows rows{features, outputs, n};
-    mlp::forward_kernel<mlp::FeatureRows><<<tiles < ctas ? tiles : ctas, mlp::kThreads, mlp::kSmemBytes, s>>>(rows, image, error,
-                                                                                                              wait_polls);
+    mlp::forward_kernel<mlp::FeatureRows><<<need < ctas ? need : ctas, mlp::kForwardThreads, mlp::kForwardSmem, s>>>(rows, image, error,
+                                                                                                                     wait_polls);
     return cudaGetLastError();
 }
 
