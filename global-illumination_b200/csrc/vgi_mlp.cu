@@ -133,9 +133,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Two values rounded to BF16 (round to nearest even) in one conversion, a
+// in the low half.
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
-    const __nv_bfloat16 x = __float2bfloat16_rn(a), y = __float2bfloat16_rn(b);
-    return (uint32_t)__bfloat16_as_ushort(x) | ((uint32_t)__bfloat16_as_ushort(y) << 16);
+    const __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&p);
 }
 
 // Writes 8 activations (columns c*8 .. c*8+7) of `row` into a K-major tile.
