@@ -476,7 +476,10 @@ __global__ void query_tasks_kernel(const float4* queue, const uint32_t* counter,
     int v[3];
     for (int a = 0; a < 3; ++a) v[a] = (int)floorf(centre[a] - 0.5f - ((uint32_t)a == axis ? side : 0.0f));
     tasks[2u * k] = make_uint4((uint32_t)v[0], (uint32_t)v[1], (uint32_t)v[2], face);
-    tasks[2u * k + 1u] = make_uint4(*step * samples, 0u, 0u, 0u);
+    // Each task's samples take their own stretch of the sequence (the step
+    // count times the rows, plus the row): a face drawn again in a later
+    // frame gets fresh directions, not the ones a shared base would repeat.
+    tasks[2u * k + 1u] = make_uint4((*step * n + k) * samples, 0u, 0u, 0u);
     encode_centre(centre, face, q1.x, q1.y, q1.z, enc, f);
 }
 
