@@ -2646,7 +2646,7 @@ static int mlp_frame_training(vgi_ctx* c) {
                            c->mlp_train_tasks.ptr, c->mlp_features.ptr, c->stream);
     const TraceArgs tr = trace_args(c, c->mlp_train_tasks.ptr, c->mlp_train_results.ptr, rows, kMlpTrainSamples, true);
     if (int e = run_trace(c, tr, false, false)) return e;
-    launch_mlp_query_targets(c->mlp_train_results.ptr, rows, c->mlp_targets.ptr, c->stream);
+    launch_mlp_query_targets(c->mlp_train_results.ptr, c->mlp_train_tasks.ptr, rows, c->mlp_targets.ptr, c->stream);
     for (uint32_t k = 0; k < steps; ++k) {
         uint32_t first = (uint32_t)(((uint64_t)k * batch) % rows);
         if (first + batch > rows) first = rows - batch;

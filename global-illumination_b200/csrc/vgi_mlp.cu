@@ -484,12 +484,18 @@ __global__ void query_tasks_kernel(const float4* queue, const uint32_t* counter,
 }
 
 // targets[k] = the traced mean of row k's face, NaN without a known sample.
-__global__ void query_targets_kernel(const uint4* results, uint32_t n, float4* targets) {
+// A task left empty by query_tasks_kernel (no queries this frame) gets no
+// result from the trace, so its row of `results` still holds an earlier
+// frame's (or freed memory's) words: its target is NaN, skipped by training,
+// whatever the row holds.
+__global__ void query_targets_kernel(const uint4* results, const uint4* tasks, uint32_t n, float4* targets) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const uint4 r0 = results[(size_t)k * 6u], r1 = results[(size_t)k * 6u + 1u];
     float4 target = make_float4(__int_as_float(0x7fc00000), 0.0f, 0.0f, 0.0f);
-    if (__uint_as_float(r1.y) > 0.0f) target = make_float4(__uint_as_float(r0.x), __uint_as_float(r0.y), __uint_as_float(r0.z), 0.0f);
+    if (tasks[2u * k].w != 0xffffffffu) {
+        const uint4 r0 = results[(size_t)k * 6u], r1 = results[(size_t)k * 6u + 1u];
+        if (__uint_as_float(r1.y) > 0.0f) target = make_float4(__uint_as_float(r0.x), __uint_as_float(r0.y), __uint_as_float(r0.z), 0.0f);
+    }
     targets[k] = target;
 }
 
@@ -947,8 +953,8 @@ void launch_mlp_query_tasks(const float4* queue, const uint32_t* count, uint32_t
     if (n) mlp::query_tasks_kernel<<<(n + 127) / 128, 128, 0, s>>>(queue, count, capacity, step, n, samples, enc, tasks, features);
 }
 
-void launch_mlp_query_targets(const uint4* results, uint32_t n, float4* targets, cudaStream_t s) {
-    if (n) mlp::query_targets_kernel<<<(n + 127) / 128, 128, 0, s>>>(results, n, targets);
+void launch_mlp_query_targets(const uint4* results, const uint4* tasks, uint32_t n, float4* targets, cudaStream_t s) {
+    if (n) mlp::query_targets_kernel<<<(n + 127) / 128, 128, 0, s>>>(results, tasks, n, targets);
 }
 
 // Raises the dynamic shared-memory limit of the MLP kernels; called once per

@@ -278,7 +278,7 @@ void launch_mlp_encode_training(const uint4* slot_meta, const uint4* results, co
                                 cudaStream_t s);
 void launch_mlp_query_tasks(const float4* queue, const uint32_t* count, uint32_t capacity, const uint32_t* step, uint32_t n,
                             uint32_t samples, const MlpEncoding& enc, uint4* tasks, float* features, cudaStream_t s);
-void launch_mlp_query_targets(const uint4* results, uint32_t n, float4* targets, cudaStream_t s);
+void launch_mlp_query_targets(const uint4* results, const uint4* tasks, uint32_t n, float4* targets, cudaStream_t s);
 void launch_mlp_encode_faces(const uint4* meta, uint32_t n, const float4* materials, const MlpEncoding& enc, float* features,
                              cudaStream_t s);
 void launch_mlp_pack(const float* master, uint8_t* image, cudaStream_t s);
